@@ -1,0 +1,366 @@
+#!/usr/bin/env python
+"""Benchmark of the Stratton-Chu field hot path on B200.
+
+Metric: E+H cell x point evaluations per second (one evaluation = one
+(observation point, cell, RHS) pair with both the K operator (E) and the R
+operator (H) accumulated), mixed form (complex FP32 far cells, FP64 near
+cells) at <= 1e-6 relative L2 against the FP64 form, which is itself within
+1e-12 of the reference's CPU output.
+
+Workload (one step): the refined PEC sphere, 64 x 128 = 8192 quads, k = 2 pi,
+20,000 observation points (18,000 on 2-5 m shells + 2,000 near-field points
+0.02-0.1 m above random cells, seed 1), one physical-optics RHS, default
+quadrature (n_start 8, p_max 1): 1.64e8 pairs per step, synthetic (seeded).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+
+For N > 1 (torchrun, one rank per GPU) every rank evaluates its own 20,000
+points against the replicated mesh (the points are independent: no
+collective on the data path), so the scaling is weak.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "E+H cell*point evals/s (mixed, <=1e-6 rel-L2 vs FP64)"
+UNIT = "pairs/s"
+# Algorithmic flops of one far pair with the default 8 x 8 split: 64 nodes x
+# 130 real flops for the fused K (F_RotRotSimplePot_H) + R (F_GradSimplePot_H)
+# integrand, transcendentals (sqrt, 1/r, sincos) not counted.
+FLOPS_PER_NODE = 130
+NODES_PER_PAIR = 64
+FLOPS_PER_FAR_PAIR = FLOPS_PER_NODE * NODES_PER_PAIR
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--fp64-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
+    return ap.parse_args()
+
+
+def workload():
+    from bielcc_b200 import workloads as W
+
+    return W.config2()
+
+
+def dist_init(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(ws, v, local):
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class Clocks:
+    """nvidia-smi samples (200 ms) during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                      stderr=subprocess.DEVNULL, text=True)
+        except FileNotFoundError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.p:
+            self.p.terminate()
+            try:
+                self.out = self.p.communicate(timeout=5)[0]
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        rows = [r.split(", ") for r in getattr(self, "out", "").strip().splitlines() if r.count(",") >= 8]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip() == "Active"})
+        pw = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows), "power_w_max": max(pw) if pw else None}
+
+
+# ---------------------------------------------------------------- CPU legs
+def cpu_sample(which, wl, target_s, threads):
+    """Times the CPU path (reference build or oracle port) on a bounded sample
+    of the workload's points (far and near in the workload's proportion)."""
+    import oracle
+
+    cells, J, k, pts = wl["cells"], wl["J"], wl["k"], wl["pts"]
+    n_far = 18000
+    # probe: 8 far + 1 near point
+    probe = np.concatenate([pts[:8], pts[n_far:n_far + 1]])
+    t0 = time.perf_counter()
+    oracle.field_EH(cells, J, k, probe, n_threads=threads, which=which)
+    dt = max(time.perf_counter() - t0, 1e-3)
+    per_pt = dt / len(probe)
+    m = int(max(18, min(4000, target_s / per_pt)))
+    m_near = max(2, m // 10)
+    sample = np.concatenate([pts[: m - m_near], pts[n_far: n_far + m_near]])
+    t0 = time.perf_counter()
+    oracle.field_EH(cells, J, k, sample, n_threads=threads, which=which)
+    dt = time.perf_counter() - t0
+    pairs = len(sample) * len(cells) * J.shape[0]
+    return pairs / dt, dt, f"{len(sample)} points ({m_near} near-field) x {len(cells)} cells x {J.shape[0]} RHS"
+
+
+def run_reference(args, ws, rank):
+    """CPU reference arm: the reference's own CPU implementation (compiled from
+    its sources into oracle/_ref) with every host thread, on bounded samples."""
+    if rank != 0:
+        return
+    import oracle
+
+    which = "ref" if oracle.available("ref") else "port"
+    kind = "reference" if which == "ref" else "port"
+    wl = workload()
+    threads = os.cpu_count() or 1
+    vals = []
+    for _ in range(max(0, args.warmup)):
+        cpu_sample(which, wl, 1.0, threads)
+    t_steps = []
+    sample = ""
+    for _ in range(args.steps):
+        v, dt, sample = cpu_sample(which, wl, 4.0, threads)
+        vals.append(v)
+        t_steps.append(dt)
+    value = float(np.mean(vals))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(t_steps)),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": wl["name"], "cells": 8192, "points": 20000, "rhs": 1, "k": "2pi",
+                       "sample_per_step": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- GPU arm
+def run_ours(args, ws, rank, local):
+    import torch
+
+    from bielcc_b200 import abi, gpu
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    wl = workload()
+    cells, J, k = wl["cells"], wl["J"], wl["k"]
+    pts = wl["pts"]
+    if ws > 1 and rank > 0:  # each rank: its own far points, same distribution (weak scaling)
+        from bielcc_b200 import workloads as W
+
+        rng = np.random.default_rng(1000 + rank)
+        pts = np.concatenate([W.shell_points(18000, 2.0, 5.0, rng), W.near_points(cells, 2000, 0.02, 0.1, rng)])
+    kv, e0, hs = wl["inc"]
+    inc = abi.PlaneWave.make(kv, e0, hs, True, True)
+    S, N, P = J.shape[0], len(cells), len(pts)
+    pairs_per_step = S * N * P
+
+    ctx = gpu.Context(local)
+    mesh = ctx.mesh(cells)
+    Jd = torch.from_numpy(np.ascontiguousarray(J)).to(dev)
+    Pd = torch.from_numpy(np.ascontiguousarray(pts)).to(dev)
+    Ed = torch.empty((S, P, 3), dtype=torch.complex128, device=dev)
+    Hd = torch.empty_like(Ed)
+    E64 = torch.empty_like(Ed)
+    H64 = torch.empty_like(Ed)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
+    stream = torch.cuda.current_stream(dev)
+
+    def step(prec, E, H):
+        ctx.field_EH_device(mesh, Jd.data_ptr(), k, Pd.data_ptr(), E.data_ptr(), H.data_ptr(), S, P, inc=inc,
+                            precision=prec, stream=stream.cuda_stream)
+
+    def timed(prec, E, H, n):
+        total = 0.0
+        for _ in range(n):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            step(prec, E, H)
+            b.record(stream)
+            b.synchronize()
+            total += a.elapsed_time(b)
+        return total
+
+    # FP64 form: reference values for the error of the mixed form, and its own speed
+    step("fp64", E64, H64)
+    torch.cuda.synchronize()
+    for _ in range(args.warmup):
+        step("mixed", Ed, Hd)
+    torch.cuda.synchronize()
+    barrier(ws)
+    ctx.stats(reset=True)
+    ctx.set_timing(True)
+    with Clocks(local) as clk:
+        torch.cuda.synchronize()
+        t_mixed = timed("mixed", Ed, Hd, args.steps)
+        torch.cuda.synchronize()
+    ctx.set_timing(False)
+    st = ctx.stats(reset=True)
+    barrier(ws)
+    t_mixed = max_over_ranks(ws, t_mixed, local)
+    ms_step = t_mixed / args.steps
+    value = ws * pairs_per_step / (ms_step * 1e-3)
+
+    rel = float(torch.sqrt((torch.sum(torch.abs(Ed - E64) ** 2) + torch.sum(torch.abs(Hd - H64) ** 2)) /
+                           (torch.sum(torch.abs(E64) ** 2) + torch.sum(torch.abs(H64) ** 2))).item())
+
+    # FP64 form timing (same step, FP64 far cells)
+    ctx.set_timing(True)
+    t64 = timed("fp64", E64, H64, args.fp64_steps)
+    ctx.set_timing(False)
+    st64 = ctx.stats(reset=True)
+    t64 = max_over_ranks(ws, t64, local)
+    value64 = ws * pairs_per_step / (t64 / args.fp64_steps * 1e-3)
+
+    # end to end through the host-buffer C-ABI call (pinned host memory)
+    Jh = torch.from_numpy(np.ascontiguousarray(J)).pin_memory().numpy()
+    Ph = torch.from_numpy(np.ascontiguousarray(pts)).pin_memory().numpy()
+    Eh = torch.empty((S, P, 3), dtype=torch.complex128).pin_memory().numpy()
+    Hh = torch.empty((S, P, 3), dtype=torch.complex128).pin_memory().numpy()
+    ctx.field_EH(mesh, Jh, k, Ph, inc=inc, precision="mixed", out=(Eh, Hh))
+    barrier(ws)
+    e2e_total = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.field_EH(mesh, Jh, k, Ph, inc=inc, precision="mixed", out=(Eh, Hh))
+        e2e_total += time.perf_counter() - t0
+    e2e_total = max_over_ranks(ws, e2e_total, local)
+    e2e_value = ws * pairs_per_step / (e2e_total / args.steps)
+
+    # roofline of the dominant kernel (the mixed far kernel)
+    peak32 = ctx.measure_fma_peak(False)
+    peak64 = ctx.measure_fma_peak(True)
+    far_ms = st["far_ms"] / max(1, st["far_launches"])
+    far_flops = FLOPS_PER_FAR_PAIR * st["far_pairs"] / max(1, st["far_launches"])
+    achieved = far_flops / (far_ms * 1e-3) / 1e12
+    far64_ms = st64["far_ms"] / max(1, st64["far_launches"])
+    achieved64 = FLOPS_PER_FAR_PAIR * st64["far_pairs"] / max(1, st64["far_launches"]) / (far64_ms * 1e-3) / 1e12
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "far_kernel_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get("bytes_per_launch")
+        except Exception:
+            traffic = None
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        import oracle
+
+        which = "ref" if oracle.available("ref") else "port"
+        threads = os.cpu_count() or 1
+        v, dt, sample = cpu_sample(which, wl, args.cpu_seconds, threads)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "reference" if which == "ref" else "port",
+               "sample": sample + f", {dt:.1f} s"}
+
+    launches = st["kernel_launches"]
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "c64 far / c128 near (f32 / f64)", "data": "synthetic (seeded)",
+        "config": {"workload": wl["name"], "cells": N, "points_per_gpu": P, "rhs": S, "k": "2pi",
+                   "quadrature": "n_start=8, n_start_seg=10, p_max=1", "parallelism": f"replicas x{ws}",
+                   "l2": "flushed (256 MB write) between timed steps"},
+        "rel_l2_vs_fp64": rel,
+        "fp64": {"value": value64, "unit": UNIT, "ms_per_step": t64 / args.fp64_steps,
+                 "roofline": {"bound": "fp64 CUDA-core pipe", "achieved": achieved64, "peak": peak64,
+                              "unit": "TFLOP/s", "frac": achieved64 / peak64 if peak64 else None,
+                              "peak_source": "measured FMA loop (bielcc_measure_fma_peak)"}},
+        "mixed_over_fp64": value / value64,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(Jh.nbytes + Ph.nbytes),
+                "d2h_bytes_per_step": int(Eh.nbytes + Hh.nbytes)},
+        "roofline": {"bound": "fp32 CUDA-core pipe (no tensor-core or HBM bound: compute-only kernel)",
+                     "kernel": "far_kernel<1,false,true>", "achieved": achieved, "peak": peak32, "unit": "TFLOP/s",
+                     "frac": achieved / peak32 if peak32 else None, "traffic": traffic,
+                     "algorithmic_flops_per_launch": far_flops, "far_ms_per_launch": far_ms,
+                     "peak_source": "measured FMA loop (bielcc_measure_fma_peak); MEASURED_PEAKS.json has no FP32 "
+                                    "CUDA-core figure"},
+        "cpu_baseline": cpu,
+        "clocks": clk.summary(),
+        "gpu_launches": launches,
+        "near_pairs_per_step": None,
+    }
+    rep = abi.Report()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    mesh.close()
+    ctx.close()
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_init(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, ws, rank)
+        else:
+            run_ours(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,742 @@
+// api.cu — the C ABI of libbielcc_gpu.so (include/bielcc_gpu.h): contexts,
+// resident meshes, workspaces, host<->device staging and kernel dispatch.
+// No C++ exception crosses the boundary; every entry point returns a status.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/bielcc_gpu.h"
+#include "internal.h"
+#include "ops.cuh"
+
+using namespace bielcc_gpu;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int set_error(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+int cuda_status(cudaError_t e, const char* what, int line) {
+    if (e == cudaSuccess) return BIELCC_OK;
+    int code = (e == cudaErrorMemoryAllocation) ? BIELCC_ERR_OOM : BIELCC_ERR_CUDA;
+    cudaGetLastError();  // clear a non-sticky error
+    return set_error(code, "%s (api.cu:%d): %s", what, line, cudaGetErrorString(e));
+}
+#define TRY_CUDA(call)                                      \
+    do {                                                    \
+        cudaError_t e_ = (call);                            \
+        if (e_ != cudaSuccess) return cuda_status(e_, #call, __LINE__); \
+    } while (0)
+#define TRY(call)                    \
+    do {                             \
+        int rc_ = (call);            \
+        if (rc_ != BIELCC_OK) return rc_; \
+    } while (0)
+
+// Grow-only device buffer.
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    int ensure(size_t bytes) {
+        if (bytes <= cap) return BIELCC_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = bytes + bytes / 4 + 256;
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(BIELCC_ERR_OOM, "device allocation of %zu bytes failed: %s", want, cudaGetErrorString(e));
+        }
+        cap = want;
+        return BIELCC_OK;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+}  // namespace
+
+struct bielcc_ctx_s {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ws_done = nullptr;  // last use of the shared workspaces
+    std::mutex mu;
+    std::map<int, MeshDev*> meshes;
+    int next_mesh = 1;
+    DevBuf ws, pair_ws, io, scratch_small;
+    long long* h_total = nullptr;  // pinned
+    unsigned long long* h_nonfinite = nullptr;
+    // counters / timing (bielcc_ctx_stats)
+    bool timing = false;
+    cudaEvent_t far_begin = nullptr, far_end = nullptr;
+    bielcc_stats stats = {0, 0, 0, 0.0};
+};
+
+namespace {
+
+NumParamH to_np(const bielcc_numparam* p) {
+    NumParamH n;
+    if (!p) {
+        n = {1e-6, 2.0, 2.0, 3.0, 8, 10, 1, 1};
+        return n;
+    }
+    n.eps = p->eps;
+    n.rs = p->rs;
+    n.rs_seg = p->rs_seg;
+    n.analytic_calc = p->analytic_calc;
+    n.n_start = p->n_start;
+    n.n_start_seg = p->n_start_seg;
+    n.p_max = p->p_max;
+    n.p_max_seg = p->p_max_seg;
+    return n;
+}
+
+int check_np(const NumParamH& n) {
+    if (n.n_start < 1 || n.n_start > 256 || n.n_start_seg < 1 || n.p_max < 1 || n.p_max > 20 || n.p_max_seg < 1 ||
+        n.p_max_seg > 20)
+        return set_error(BIELCC_ERR_ARG, "numparam out of range (n_start %d, n_start_seg %d, p_max %d, p_max_seg %d)",
+                         n.n_start, n.n_start_seg, n.p_max, n.p_max_seg);
+    return BIELCC_OK;
+}
+
+int enter(bielcc_ctx ctx) {
+    if (!ctx) return set_error(BIELCC_ERR_ARG, "null context");
+    TRY_CUDA(cudaSetDevice(ctx->device));
+    return BIELCC_OK;
+}
+
+int get_mesh(bielcc_ctx ctx, bielcc_mesh id, MeshDev** out) {
+    auto it = ctx->meshes.find(id);
+    if (it == ctx->meshes.end()) return set_error(BIELCC_ERR_NOT_FOUND, "unknown mesh %d", id);
+    *out = it->second;
+    return BIELCC_OK;
+}
+
+void free_mesh(MeshDev* m) {
+    cudaFree(m->verts);
+    cudaFree(m->geo);
+    cudaFree(m->nodes64);
+    cudaFree(m->nodes32);
+    cudaFree(m->rho32);
+    delete m;
+}
+
+// Node tables for split n, built on first use and cached on the mesh.
+int ensure_tables(MeshDev* m, int n, cudaStream_t s) {
+    if (m->table_n == n && m->nodes64) return BIELCC_OK;
+    cudaFree(m->nodes64);
+    cudaFree(m->nodes32);
+    cudaFree(m->rho32);
+    m->nodes64 = nullptr;
+    m->nodes32 = nullptr;
+    m->rho32 = nullptr;
+    m->table_n = 0;
+    size_t nn = (size_t)n * n * m->n_cells;
+    TRY_CUDA(cudaMalloc(&m->nodes64, nn * sizeof(double4) + 16));
+    TRY_CUDA(cudaMalloc(&m->nodes32, nn * sizeof(float4) + 16));
+    TRY_CUDA(cudaMalloc(&m->rho32, (size_t)m->n_cells * sizeof(float) + 16));
+    TRY_CUDA(launch_node_tables(m->verts, m->geo, m->nv, m->n_cells, n, m->nodes64, m->nodes32, m->rho32, s));
+    m->table_n = n;
+    return BIELCC_OK;
+}
+
+// Orders `s` after the previous use of the shared workspaces.
+int ws_acquire(bielcc_ctx ctx, cudaStream_t s) {
+    TRY_CUDA(cudaStreamWaitEvent(s, ctx->ws_done, 0));
+    return BIELCC_OK;
+}
+int ws_release(bielcc_ctx ctx, cudaStream_t s) {
+    TRY_CUDA(cudaEventRecord(ctx->ws_done, s));
+    return BIELCC_OK;
+}
+
+struct FieldArgs {
+    MeshDev* m;
+    int n_rhs;
+    const double* J;
+    cplx k, mult;
+    const bielcc_planewave* inc;
+    NumParamH np;
+    int n_pts;
+    const double* pts;
+    double* E;
+    double* H;
+    int precision;
+};
+
+// Enqueues a field evaluation on device buffers; one short host wait for the
+// near-pair count (sizes the FP64 near workspace).
+int field_device(bielcc_ctx ctx, const FieldArgs& a, cudaStream_t s, bielcc_report* rep,
+                 unsigned long long* d_nonfinite) {
+    TRY(ensure_tables(a.m, a.np.n_start, s));
+    FieldLaunch f;
+    f.mesh = a.m;
+    f.pts = a.pts;
+    f.n_pts = a.n_pts;
+    f.J = a.J;
+    f.n_rhs = a.n_rhs;
+    f.k = a.k;
+    f.mult = a.mult;
+    f.np = a.np;
+    f.precision = a.precision;
+    for (int g = 0; g < 3; g++) {
+        f.kvec[g] = a.inc ? a.inc->k_vec[g] : 0.;
+        f.e0[g] = a.inc ? a.inc->e0[g] : 0.;
+    }
+    f.h_scale = a.inc ? a.inc->h_scale : 0.;
+    f.add_E = a.inc ? a.inc->add_E : 0;
+    f.add_H = a.inc ? a.inc->add_H : 0;
+    f.E = a.E;
+    f.H = a.H;
+    int splits = 1;
+    size_t base = field_ws_base_bytes(f, &splits);
+    TRY(ctx->ws.ensure(base));
+    TRY(ctx->scratch_small.ensure(256));
+    long long* d_total = (long long*)ctx->scratch_small.p;
+    int l1 = 0, l2 = 0, lf = 0;
+    TRY_CUDA(field_stage1(f, ctx->ws.p, splits, d_total, s, &l1, ctx->timing ? ctx->far_begin : nullptr,
+                          ctx->timing ? ctx->far_end : nullptr, &lf));
+    TRY_CUDA(cudaMemcpyAsync(ctx->h_total, d_total, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    TRY_CUDA(cudaStreamSynchronize(s));
+    long long n_near = *ctx->h_total;
+    if (ctx->timing && lf > 0) {
+        float ms = 0.f;
+        TRY_CUDA(cudaEventElapsedTime(&ms, ctx->far_begin, ctx->far_end));
+        ctx->stats.far_ms += ms;
+    }
+    if (n_near > 0) TRY(ctx->pair_ws.ensure(field_pair_ws_bytes(n_near)));
+    TRY_CUDA(field_stage2(f, ctx->ws.p, splits, n_near, ctx->pair_ws.p, d_nonfinite, s, &l2));
+    ctx->stats.kernel_launches += l1 + l2;
+    ctx->stats.far_launches += lf;
+    ctx->stats.far_pairs += ((long long)a.n_pts * a.m->n_cells - n_near) * a.n_rhs;
+    if (rep) {
+        rep->n_pairs = (int64_t)a.n_pts * a.m->n_cells;
+        rep->n_near_pairs = n_near;
+    }
+    return BIELCC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void bielcc_numparam_default(bielcc_numparam* np) {
+    if (!np) return;
+    np->eps = 1e-6;
+    np->rs = 2.0;
+    np->rs_seg = 2.0;
+    np->analytic_calc = 3.0;
+    np->n_start = 8;
+    np->n_start_seg = 10;
+    np->p_max = 1;
+    np->p_max_seg = 1;
+}
+
+int bielcc_abi_version(void) { return BIELCC_ABI_VERSION; }
+
+const char* bielcc_last_error(void) { return g_last_error.c_str(); }
+
+int bielcc_ctx_create(int device, bielcc_ctx* out) {
+    if (!out) return set_error(BIELCC_ERR_ARG, "null output pointer");
+    *out = nullptr;
+    int n = 0;
+    TRY_CUDA(cudaGetDeviceCount(&n));
+    if (device < 0 || device >= n) return set_error(BIELCC_ERR_ARG, "device %d of %d", device, n);
+    TRY_CUDA(cudaSetDevice(device));
+    bielcc_ctx c = new (std::nothrow) bielcc_ctx_s;
+    if (!c) return set_error(BIELCC_ERR_OOM, "host allocation failed");
+    c->device = device;
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ws_done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaMallocHost(&c->h_total, 64);
+    if (e == cudaSuccess) e = cudaEventCreate(&c->far_begin);
+    if (e == cudaSuccess) e = cudaEventCreate(&c->far_end);
+    if (e != cudaSuccess) {
+        delete c;
+        return cuda_status(e, "context set-up", __LINE__);
+    }
+    c->h_nonfinite = reinterpret_cast<unsigned long long*>(c->h_total + 1);
+    TRY_CUDA(cudaEventRecord(c->ws_done, c->stream));
+    *out = c;
+    return BIELCC_OK;
+}
+
+int bielcc_ctx_destroy(bielcc_ctx ctx) {
+    if (!ctx) return BIELCC_OK;
+    cudaSetDevice(ctx->device);
+    cudaDeviceSynchronize();
+    for (auto& kv : ctx->meshes) free_mesh(kv.second);
+    ctx->ws.release();
+    ctx->pair_ws.release();
+    ctx->io.release();
+    ctx->scratch_small.release();
+    if (ctx->h_total) cudaFreeHost(ctx->h_total);
+    if (ctx->ws_done) cudaEventDestroy(ctx->ws_done);
+    if (ctx->far_begin) cudaEventDestroy(ctx->far_begin);
+    if (ctx->far_end) cudaEventDestroy(ctx->far_end);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return BIELCC_OK;
+}
+
+int bielcc_ctx_synchronize(bielcc_ctx ctx) {
+    TRY(enter(ctx));
+    TRY_CUDA(cudaDeviceSynchronize());
+    return BIELCC_OK;
+}
+
+int bielcc_ctx_set_timing(bielcc_ctx ctx, int on) {
+    if (!ctx) return set_error(BIELCC_ERR_ARG, "null context");
+    std::lock_guard<std::mutex> g(ctx->mu);
+    ctx->timing = on != 0;
+    return BIELCC_OK;
+}
+
+int bielcc_ctx_stats(bielcc_ctx ctx, bielcc_stats* out, int reset) {
+    if (!ctx || !out) return set_error(BIELCC_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> g(ctx->mu);
+    *out = ctx->stats;
+    if (reset) ctx->stats = bielcc_stats{0, 0, 0, 0.0};
+    return BIELCC_OK;
+}
+
+int bielcc_ctx_mem_used(bielcc_ctx ctx, int64_t* bytes) {
+    if (!ctx || !bytes) return set_error(BIELCC_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> g(ctx->mu);
+    int64_t b = ctx->ws.cap + ctx->pair_ws.cap + ctx->io.cap + ctx->scratch_small.cap;
+    for (auto& kv : ctx->meshes) {
+        const MeshDev* m = kv.second;
+        b += (int64_t)m->n_cells * (m->nv * 3 * 8 + sizeof(CellGeo));
+        if (m->table_n) b += (int64_t)m->n_cells * m->table_n * m->table_n * (32 + 16) + 4 * m->n_cells;
+    }
+    *bytes = b;
+    return BIELCC_OK;
+}
+
+int bielcc_mesh_create(bielcc_ctx ctx, int n_vert, int n_cells, const double* cells, bielcc_mesh* out) {
+    TRY(enter(ctx));
+    if (!out || (!cells && n_cells > 0)) return set_error(BIELCC_ERR_ARG, "null argument");
+    if (n_vert != 3 && n_vert != 4) return set_error(BIELCC_ERR_ARG, "n_vert must be 3 or 4, got %d", n_vert);
+    if (n_cells < 1) return set_error(BIELCC_ERR_ARG, "n_cells must be positive, got %d", n_cells);
+    std::lock_guard<std::mutex> g(ctx->mu);
+    MeshDev* m = new (std::nothrow) MeshDev;
+    if (!m) return set_error(BIELCC_ERR_OOM, "host allocation failed");
+    m->nv = n_vert;
+    m->n_cells = n_cells;
+    size_t vb = (size_t)n_cells * n_vert * 3 * sizeof(double);
+    cudaError_t e = cudaMalloc(&m->verts, vb);
+    if (e == cudaSuccess) e = cudaMalloc(&m->geo, (size_t)n_cells * sizeof(CellGeo));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(m->verts, cells, vb, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = launch_cell_geometry(m->verts, n_vert, n_cells, m->geo, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        free_mesh(m);
+        return cuda_status(e, "mesh upload", __LINE__);
+    }
+    int id = ctx->next_mesh++;
+    ctx->meshes[id] = m;
+    *out = id;
+    return BIELCC_OK;
+}
+
+int bielcc_mesh_destroy(bielcc_ctx ctx, bielcc_mesh mesh) {
+    TRY(enter(ctx));
+    std::lock_guard<std::mutex> g(ctx->mu);
+    MeshDev* m;
+    TRY(get_mesh(ctx, mesh, &m));
+    TRY_CUDA(cudaStreamSynchronize(ctx->stream));
+    free_mesh(m);
+    ctx->meshes.erase(mesh);
+    return BIELCC_OK;
+}
+
+int bielcc_field_EH_device(bielcc_ctx ctx, bielcc_mesh mesh, int n_rhs, const double* J_dev, double k_re, double k_im,
+                           double mult_re, double mult_im, const bielcc_planewave* inc, const bielcc_numparam* np,
+                           int n_pts, const double* pts_dev, double* E_dev, double* H_dev, int precision, void* stream,
+                           bielcc_report* report) {
+    TRY(enter(ctx));
+    std::lock_guard<std::mutex> g(ctx->mu);
+    MeshDev* m;
+    TRY(get_mesh(ctx, mesh, &m));
+    NumParamH n = to_np(np);
+    TRY(check_np(n));
+    if (n_rhs < 1 || n_pts < 0 || (n_pts > 0 && (!pts_dev || !E_dev)) || !J_dev)
+        return set_error(BIELCC_ERR_ARG, "bad field arguments (n_rhs %d, n_pts %d)", n_rhs, n_pts);
+    if (precision != BIELCC_PREC_FP64 && precision != BIELCC_PREC_MIXED)
+        return set_error(BIELCC_ERR_ARG, "unknown precision %d", precision);
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    TRY(ws_acquire(ctx, s));
+    FieldArgs a{m, n_rhs, J_dev, mk(k_re, k_im), mk(mult_re, mult_im), inc, n, n_pts, pts_dev, E_dev, H_dev,
+                precision};
+    if (report) memset(report, 0, sizeof(*report));
+    TRY(field_device(ctx, a, s, report, nullptr));
+    TRY(ws_release(ctx, s));
+    return BIELCC_OK;
+}
+
+int bielcc_field_EH(bielcc_ctx ctx, bielcc_mesh mesh, int n_rhs, const double* J, double k_re, double k_im,
+                    double mult_re, double mult_im, const bielcc_planewave* inc, const bielcc_numparam* np, int n_pts,
+                    const double* pts, double* E, double* H, int precision, bielcc_report* report) {
+    TRY(enter(ctx));
+    std::lock_guard<std::mutex> g(ctx->mu);
+    MeshDev* m;
+    TRY(get_mesh(ctx, mesh, &m));
+    NumParamH n = to_np(np);
+    TRY(check_np(n));
+    if (n_rhs < 1 || n_pts < 0 || !J || (n_pts > 0 && (!pts || !E)))
+        return set_error(BIELCC_ERR_ARG, "bad field arguments (n_rhs %d, n_pts %d)", n_rhs, n_pts);
+    if (precision != BIELCC_PREC_FP64 && precision != BIELCC_PREC_MIXED)
+        return set_error(BIELCC_ERR_ARG, "unknown precision %d", precision);
+    if (report) memset(report, 0, sizeof(*report));
+    cudaStream_t s = ctx->stream;
+    const size_t P = n_pts, N = m->n_cells, S = n_rhs;
+    const size_t bJ = S * N * 3 * 16, bP = P * 3 * 8, bO = S * P * 3 * 16;
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    TRY(ctx->io.ensure(al(bJ) + al(bP) + 2 * al(bO) + 256));
+    char* io = (char*)ctx->io.p;
+    double* dJ = (double*)io;
+    double* dP = (double*)(io + al(bJ));
+    double* dE = (double*)(io + al(bJ) + al(bP));
+    double* dH = H ? (double*)(io + al(bJ) + al(bP) + al(bO)) : nullptr;
+    unsigned long long* d_nf = (unsigned long long*)(io + al(bJ) + al(bP) + 2 * al(bO));
+    TRY(ws_acquire(ctx, s));
+    TRY_CUDA(cudaMemcpyAsync(dJ, J, bJ, cudaMemcpyHostToDevice, s));
+    if (P) TRY_CUDA(cudaMemcpyAsync(dP, pts, bP, cudaMemcpyHostToDevice, s));
+    TRY_CUDA(cudaMemsetAsync(d_nf, 0, sizeof(unsigned long long), s));
+    FieldArgs a{m, n_rhs, dJ, mk(k_re, k_im), mk(mult_re, mult_im), inc, n, n_pts, dP, dE, dH, precision};
+    if (P) TRY(field_device(ctx, a, s, report, d_nf));
+    if (P) TRY_CUDA(cudaMemcpyAsync(E, dE, bO, cudaMemcpyDeviceToHost, s));
+    if (P && H) TRY_CUDA(cudaMemcpyAsync(H, dH, bO, cudaMemcpyDeviceToHost, s));
+    TRY_CUDA(cudaMemcpyAsync(ctx->h_nonfinite, d_nf, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    TRY_CUDA(cudaStreamSynchronize(s));
+    TRY(ws_release(ctx, s));
+    int rc = BIELCC_OK;
+    unsigned long long nf = *ctx->h_nonfinite;
+    if (nf) rc = set_error(BIELCC_ERR_NAN, "%llu output points hold NaN/Inf", nf);
+    if (report) {
+        report->n_nonfinite = (int64_t)nf;
+        report->status = rc;
+    }
+    // Mixed form: relative L2 error against the FP64 form on a point sample.
+    if (report && precision == BIELCC_PREC_MIXED && P > 0) {
+        const int stride = (int)std::max<size_t>(1, P / 256);
+        std::vector<double> sp;
+        std::vector<size_t> idx;
+        for (size_t i = 0; i < P; i += stride) {
+            idx.push_back(i);
+            for (int g = 0; g < 3; g++) sp.push_back(pts[3 * i + g]);
+        }
+        const size_t Q = idx.size();
+        const size_t bQ = Q * 3 * 8, bQo = S * Q * 3 * 16;
+        TRY(ctx->io.ensure(al(bJ) + al(bQ) + 2 * al(bQo) + 256));
+        io = (char*)ctx->io.p;
+        dJ = (double*)io;
+        double* dQ = (double*)(io + al(bJ));
+        double* dEq = (double*)(io + al(bJ) + al(bQ));
+        double* dHq = (double*)(io + al(bJ) + al(bQ) + al(bQo));
+        TRY(ws_acquire(ctx, s));
+        TRY_CUDA(cudaMemcpyAsync(dJ, J, bJ, cudaMemcpyHostToDevice, s));
+        TRY_CUDA(cudaMemcpyAsync(dQ, sp.data(), bQ, cudaMemcpyHostToDevice, s));
+        FieldArgs b{m, n_rhs, dJ, mk(k_re, k_im), mk(mult_re, mult_im), inc, n, (int)Q, dQ, dEq, dHq,
+                    BIELCC_PREC_FP64};
+        TRY(field_device(ctx, b, s, nullptr, nullptr));
+        std::vector<double> e64(S * Q * 6), h64(S * Q * 6);
+        TRY_CUDA(cudaMemcpyAsync(e64.data(), dEq, bQo, cudaMemcpyDeviceToHost, s));
+        TRY_CUDA(cudaMemcpyAsync(h64.data(), dHq, bQo, cudaMemcpyDeviceToHost, s));
+        TRY_CUDA(cudaStreamSynchronize(s));
+        TRY(ws_release(ctx, s));
+        double num = 0, den = 0;
+        for (size_t r = 0; r < S; r++)
+            for (size_t q = 0; q < Q; q++)
+                for (int c = 0; c < 6; c++) {
+                    double ref = e64[(r * Q + q) * 6 + c], got = E[(r * P + idx[q]) * 6 + c];
+                    num += (got - ref) * (got - ref);
+                    den += ref * ref;
+                    if (H) {
+                        ref = h64[(r * Q + q) * 6 + c];
+                        got = H[(r * P + idx[q]) * 6 + c];
+                        num += (got - ref) * (got - ref);
+                        den += ref * ref;
+                    }
+                }
+        report->est_rel_l2 = den > 0 ? sqrt(num / den) : 0.;
+        report->est_sample = (int32_t)Q;
+    }
+    return rc;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- per-pair entry points
+namespace {
+
+// Host-buffer batch helper: copies `ins` to the device, runs `launch` with
+// their device pointers, copies `out_bytes` back into `out`.
+template <typename L>
+int run_batch(bielcc_ctx ctx, std::initializer_list<std::pair<const void*, size_t>> ins, void* out, size_t out_bytes,
+              L launch) {
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    size_t tot = al(out_bytes);
+    for (auto& in : ins) tot += al(in.second);
+    TRY(ctx->io.ensure(tot + 256));
+    cudaStream_t s = ctx->stream;
+    TRY(ws_acquire(ctx, s));
+    char* p = (char*)ctx->io.p;
+    std::vector<const void*> dptrs;
+    for (auto& in : ins) {
+        if (in.first && in.second) TRY_CUDA(cudaMemcpyAsync(p, in.first, in.second, cudaMemcpyHostToDevice, s));
+        dptrs.push_back(in.first ? p : nullptr);
+        p += al(in.second);
+    }
+    TRY_CUDA(launch(dptrs, (void*)p, s));
+    if (out_bytes) TRY_CUDA(cudaMemcpyAsync(out, p, out_bytes, cudaMemcpyDeviceToHost, s));
+    TRY_CUDA(cudaStreamSynchronize(s));
+    TRY(ws_release(ctx, s));
+    return BIELCC_OK;
+}
+
+int check_nv(int nv) {
+    if (nv != 3 && nv != 4) return set_error(BIELCC_ERR_ARG, "n_vert must be 3 or 4, got %d", nv);
+    return BIELCC_OK;
+}
+
+int check_quad_params(int n_start, int p_max) {
+    if (n_start < 1 || n_start > 4096 || p_max < 1 || p_max > 20)
+        return set_error(BIELCC_ERR_ARG, "n_start %d / p_max %d out of range", n_start, p_max);
+    return BIELCC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bielcc_pair_op(bielcc_ctx ctx, int op, int n_vert, int n_pairs, const double* cells, const double* x,
+                   const double* j, double k_re, double k_im, const bielcc_numparam* np, double* res) {
+    TRY(enter(ctx));
+    TRY(check_nv(n_vert));
+    if (op < 0 || op >= BIELCC_OP_COUNT) return set_error(BIELCC_ERR_ARG, "unknown operator %d", op);
+    if (n_pairs < 0 || (n_pairs > 0 && (!cells || !x || !j || !res))) return set_error(BIELCC_ERR_ARG, "null buffer");
+    NumParamH n = to_np(np);
+    TRY(check_np(n));
+    if (n_pairs == 0) return BIELCC_OK;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    size_t N = n_pairs;
+    return run_batch(ctx, {{cells, N * n_vert * 24}, {x, N * 24}, {j, N * 48}}, res, N * 48,
+                     [&](std::vector<const void*>& d, void* o, cudaStream_t s) {
+                         return launch_pair_op(op, n_vert, n_pairs, (const double*)d[0], (const double*)d[1],
+                                               (const double*)d[2], mk(k_re, k_im), n, (double*)o, s);
+                     });
+}
+
+int bielcc_integrand_info(int integrand, int* idim, int* is_complex) {
+    if (integrand < 0 || integrand >= BIELCC_F_COUNT) return set_error(BIELCC_ERR_ARG, "unknown integrand %d", integrand);
+    if (idim) *idim = integrand_dim(integrand);
+    if (is_complex) *is_complex = integrand_complex(integrand) ? 1 : 0;
+    return BIELCC_OK;
+}
+
+int bielcc_integral_pnt(bielcc_ctx ctx, int integrand, int n_vert, int n_pairs, const double* cells, const double* x,
+                        const bielcc_kernelparam* kp, int n_start, int p_max, double eps, double* res) {
+    TRY(enter(ctx));
+    TRY(check_nv(n_vert));
+    TRY(check_quad_params(n_start, p_max));
+    if (integrand < 0 || integrand >= BIELCC_F_COUNT) return set_error(BIELCC_ERR_ARG, "unknown integrand %d", integrand);
+    if (n_pairs < 0 || (n_pairs > 0 && (!cells || !x || !kp || !res))) return set_error(BIELCC_ERR_ARG, "null buffer");
+    if (n_pairs == 0) return BIELCC_OK;
+    static_assert(sizeof(bielcc_kernelparam) == sizeof(KParamDev), "kernel-parameter layouts differ");
+    std::lock_guard<std::mutex> g(ctx->mu);
+    size_t N = n_pairs;
+    int idim = integrand_dim(integrand);
+    size_t ob = N * idim * (integrand_complex(integrand) ? 16 : 8);
+    return run_batch(ctx, {{cells, N * n_vert * 24}, {x, N * 24}, {kp, N * sizeof(KParamDev)}}, res, ob,
+                     [&](std::vector<const void*>& d, void* o, cudaStream_t s) {
+                         return launch_integral_pnt(integrand, n_vert, n_pairs, (const double*)d[0],
+                                                    (const double*)d[1], (const KParamDev*)d[2], n_start, p_max, eps,
+                                                    (double*)o, s);
+                     });
+}
+
+int bielcc_integral_seg_pnt(bielcc_ctx ctx, int integrand, int n_pairs, const double* a, const double* b,
+                            const double* x, const bielcc_kernelparam* kp, int n_start, int p_max, double eps,
+                            double* res) {
+    TRY(enter(ctx));
+    TRY(check_quad_params(n_start, p_max));
+    if (integrand < 0 || integrand >= BIELCC_F_COUNT) return set_error(BIELCC_ERR_ARG, "unknown integrand %d", integrand);
+    if (n_pairs < 0 || (n_pairs > 0 && (!a || !b || !x || !kp || !res))) return set_error(BIELCC_ERR_ARG, "null buffer");
+    if (n_pairs == 0) return BIELCC_OK;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    size_t N = n_pairs;
+    int idim = integrand_dim(integrand);
+    size_t ob = N * idim * (integrand_complex(integrand) ? 16 : 8);
+    return run_batch(ctx, {{a, N * 24}, {b, N * 24}, {x, N * 24}, {kp, N * sizeof(KParamDev)}}, res, ob,
+                     [&](std::vector<const void*>& d, void* o, cudaStream_t s) {
+                         return launch_integral_seg(integrand, n_pairs, (const double*)d[0], (const double*)d[1],
+                                                    (const double*)d[2], (const KParamDev*)d[3], n_start, p_max, eps,
+                                                    (double*)o, s);
+                     });
+}
+
+int bielcc_k0(bielcc_ctx ctx, int integrand, int common, int n_vert, int n_pairs, const double* cells,
+              const double* x, const double* j, const bielcc_kernelparam* kp, int n_start_seg, int p_max_seg,
+              double eps, double* res) {
+    TRY(enter(ctx));
+    TRY(check_nv(n_vert));
+    TRY(check_quad_params(n_start_seg, p_max_seg));
+    if (integrand < 0 || integrand >= BIELCC_F_COUNT || !integrand_complex(integrand) || integrand_dim(integrand) != 3)
+        return set_error(BIELCC_ERR_ARG, "K0 needs a complex 3-vector integrand, got %d", integrand);
+    if (n_pairs < 0 || (n_pairs > 0 && (!cells || !x || !kp || !res || (!common && !j))))
+        return set_error(BIELCC_ERR_ARG, "null buffer");
+    if (n_pairs == 0) return BIELCC_OK;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    size_t N = n_pairs;
+    return run_batch(ctx, {{cells, N * n_vert * 24}, {x, N * 24}, {common ? nullptr : j, N * 48},
+                           {kp, N * sizeof(KParamDev)}},
+                     res, N * 48, [&](std::vector<const void*>& d, void* o, cudaStream_t s) {
+                         return launch_k0(integrand, common, n_vert, n_pairs, (const double*)d[0],
+                                          (const double*)d[1], (const double*)d[2], (const KParamDev*)d[3],
+                                          n_start_seg, p_max_seg, eps, (double*)o, s);
+                     });
+}
+
+int bielcc_integral_1divr(bielcc_ctx ctx, int n_vert, int n_pairs, const double* cells, const double* x,
+                          double* res) {
+    TRY(enter(ctx));
+    TRY(check_nv(n_vert));
+    if (n_pairs < 0 || (n_pairs > 0 && (!cells || !x || !res))) return set_error(BIELCC_ERR_ARG, "null buffer");
+    if (n_pairs == 0) return BIELCC_OK;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    size_t N = n_pairs;
+    return run_batch(ctx, {{cells, N * n_vert * 24}, {x, N * 24}}, res, N * 8,
+                     [&](std::vector<const void*>& d, void* o, cudaStream_t s) {
+                         return launch_analytic(0, n_vert, n_pairs, (const double*)d[0], nullptr, (const double*)d[1],
+                                                0., 1, 1, 0., mk(0, 0), (double*)o, s);
+                     });
+}
+
+int bielcc_integral_grad1divr_seg(bielcc_ctx ctx, int n_pairs, const double* a, const double* b, const double* x,
+                                  double* res) {
+    TRY(enter(ctx));
+    if (n_pairs < 0 || (n_pairs > 0 && (!a || !b || !x || !res))) return set_error(BIELCC_ERR_ARG, "null buffer");
+    if (n_pairs == 0) return BIELCC_OK;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    size_t N = n_pairs;
+    return run_batch(ctx, {{a, N * 24}, {b, N * 24}, {x, N * 24}}, res, N * 24,
+                     [&](std::vector<const void*>& d, void* o, cudaStream_t s) {
+                         return launch_analytic(1, 3, n_pairs, (const double*)d[0], (const double*)d[1],
+                                                (const double*)d[2], 0., 1, 1, 0., mk(0, 0), (double*)o, s);
+                     });
+}
+
+int bielcc_integral_surf_simplepot_h_hs(bielcc_ctx ctx, int n_vert, int n_pairs, const double* cells,
+                                        const double* x, double analytic_r, int n_start, int p_max, double eps,
+                                        double k_re, double k_im, double* res) {
+    TRY(enter(ctx));
+    TRY(check_nv(n_vert));
+    TRY(check_quad_params(n_start, p_max));
+    if (n_pairs < 0 || (n_pairs > 0 && (!cells || !x || !res))) return set_error(BIELCC_ERR_ARG, "null buffer");
+    if (n_pairs == 0) return BIELCC_OK;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    size_t N = n_pairs;
+    return run_batch(ctx, {{cells, N * n_vert * 24}, {x, N * 24}}, res, N * 16,
+                     [&](std::vector<const void*>& d, void* o, cudaStream_t s) {
+                         return launch_analytic(2, n_vert, n_pairs, (const double*)d[0], nullptr, (const double*)d[1],
+                                                analytic_r, n_start, p_max, eps, mk(k_re, k_im), (double*)o, s);
+                     });
+}
+
+int bielcc_integral_seg_gradsimplepot_h_hs(bielcc_ctx ctx, int n_pairs, const double* a, const double* b,
+                                           const double* x, double analytic_r, int n_start, int p_max, double eps,
+                                           double k_re, double k_im, double* res) {
+    TRY(enter(ctx));
+    TRY(check_quad_params(n_start, p_max));
+    if (n_pairs < 0 || (n_pairs > 0 && (!a || !b || !x || !res))) return set_error(BIELCC_ERR_ARG, "null buffer");
+    if (n_pairs == 0) return BIELCC_OK;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    size_t N = n_pairs;
+    return run_batch(ctx, {{a, N * 24}, {b, N * 24}, {x, N * 24}}, res, N * 48,
+                     [&](std::vector<const void*>& d, void* o, cudaStream_t s) {
+                         return launch_analytic(3, 3, n_pairs, (const double*)d[0], (const double*)d[1],
+                                                (const double*)d[2], analytic_r, n_start, p_max, eps, mk(k_re, k_im),
+                                                (double*)o, s);
+                     });
+}
+
+// Collocation assembly: implemented in assemble.cu's stages, driven here.
+int bielcc_assemble_K_device(bielcc_ctx ctx, bielcc_mesh mesh, double k_re, double k_im, const bielcc_numparam* np,
+                             int layout, int out_c64, int precision, void* A_dev, void* stream,
+                             bielcc_report* report) {
+    TRY(enter(ctx));
+    std::lock_guard<std::mutex> g(ctx->mu);
+    MeshDev* m;
+    TRY(get_mesh(ctx, mesh, &m));
+    NumParamH n = to_np(np);
+    TRY(check_np(n));
+    if (layout != BIELCC_LAYOUT_TAU2 && layout != BIELCC_LAYOUT_FULL3)
+        return set_error(BIELCC_ERR_ARG, "unknown layout %d", layout);
+    if (precision != BIELCC_PREC_FP64 && precision != BIELCC_PREC_MIXED)
+        return set_error(BIELCC_ERR_ARG, "unknown precision %d", precision);
+    if (!A_dev) return set_error(BIELCC_ERR_ARG, "null matrix");
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    TRY(ws_acquire(ctx, s));
+    TRY(ensure_tables(m, n.n_start, s));
+    AssembleLaunch a{m, mk(k_re, k_im), n, layout, out_c64 ? 1 : 0, precision, A_dev};
+    TRY(ctx->ws.ensure(assemble_ws_base_bytes(a)));
+    TRY(ctx->scratch_small.ensure(256));
+    long long* d_total = (long long*)ctx->scratch_small.p;
+    TRY_CUDA(assemble_stage1(a, ctx->ws.p, d_total, s));
+    TRY_CUDA(cudaMemcpyAsync(ctx->h_total, d_total, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    TRY_CUDA(cudaStreamSynchronize(s));
+    long long n_near = *ctx->h_total;
+    if (n_near > 0) TRY(ctx->pair_ws.ensure((size_t)n_near * (2 * sizeof(int)) + 1024));
+    TRY_CUDA(assemble_stage2(a, ctx->ws.p, n_near, ctx->pair_ws.p, s));
+    ctx->stats.kernel_launches += 3 + (n_near > 0 ? 2 : 0);
+    TRY(ws_release(ctx, s));
+    if (report) {
+        memset(report, 0, sizeof(*report));
+        report->n_pairs = (int64_t)m->n_cells * m->n_cells;
+        report->n_near_pairs = n_near;
+    }
+    return BIELCC_OK;
+}
+
+int bielcc_assemble_K(bielcc_ctx ctx, bielcc_mesh mesh, double k_re, double k_im, const bielcc_numparam* np,
+                      int layout, int out_c64, int precision, void* A_host, bielcc_report* report) {
+    TRY(enter(ctx));
+    MeshDev* m;
+    {
+        std::lock_guard<std::mutex> g(ctx->mu);
+        TRY(get_mesh(ctx, mesh, &m));
+    }
+    if (!A_host) return set_error(BIELCC_ERR_ARG, "null matrix");
+    size_t dim = (size_t)(layout == BIELCC_LAYOUT_FULL3 ? 3 : 2) * m->n_cells;
+    size_t bytes = dim * dim * (out_c64 ? 8 : 16);
+    void* dA = nullptr;
+    TRY_CUDA(cudaMalloc(&dA, bytes));
+    int rc = bielcc_assemble_K_device(ctx, mesh, k_re, k_im, np, layout, out_c64, precision, dA, nullptr, report);
+    if (rc == BIELCC_OK) {
+        cudaError_t e = cudaMemcpy(A_host, dA, bytes, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) rc = cuda_status(e, "matrix download", __LINE__);
+    }
+    cudaFree(dA);
+    return rc;
+}
+
+}  // extern "C"

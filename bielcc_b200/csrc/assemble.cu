@@ -1,0 +1,442 @@
+// assemble.cu — collocation-matrix assembly of the K operator:
+//   A[(i,a),(j,b)] = tau_a(i) . K[cell_j, tau_b(j)](c_i),  c_i = centre of cell i
+// (layout TAU2, 2N x 2N) or the full 3x3 blocks (layout FULL3, 3N x 3N).
+// K is linear in the cell current, so each (i, j) block is the 3x3 operator
+// matrix projected on the tangent bases (CellFill, mesh/cell.cpp).
+//   far  (|c_i - c_j| >= analytic_calc * diam_j): K_RotRot_Far (K.h:288-301)
+//        = (A1 I + T) / 4pi from the precomputed node tables; FP64 or FP32
+//        (phase split as in field.cu);
+//   near: K_RotRot_HS_Colloc (K.h:179-204) in FP64 = I_hs k^2/4pi I + M / 4pi,
+//        I_hs = IntegralSurf_SimplePot_H_HS (integrals_analytic.h:136-164),
+//        M = -sum_e ks_e nu_e^T from the unsmoothed K0 (K0.h:36-86).
+// Every entry is written exactly once (far kernel skips near pairs).
+#include <algorithm>
+#include <type_traits>
+
+#include "internal.h"
+#include "ops.cuh"
+#include "scan.cuh"
+
+namespace bielcc_gpu {
+
+constexpr int kAsmThreads = 128;
+constexpr int kAsmStageNodes = 256;
+constexpr int kAsmMaxCells = 32;
+
+struct AsmArgs {
+    const CellGeo* geo;
+    int n_cells;
+    const double4* nodes64;
+    const float4* nodes32;
+    const float* rho32;
+    int nn;
+    cplx k;
+    double analytic_calc;
+    int cols_per_split;
+    int m;  // 2 (tau) or 3 (full)
+    int c64;
+    void* A;
+};
+
+BIELCC_D bool asm_is_near(const double* x, const CellGeo& g, double analytic_calc, double* d) {
+    *d = dist3_rn(x, g.c);
+    return *d < __dmul_rn(analytic_calc, g.diam);
+}
+
+// Writes the m x m block of (row cell i, column cell j) from the 3x3 complex
+// operator matrix K (already / 4pi).
+BIELCC_D void write_block(const AsmArgs& a, int i, int j, const double (*Kr)[3], const double (*Ki)[3],
+                          const double* ti1, const double* ti2, const double* tj1, const double* tj2) {
+    const size_t dim = (size_t)a.m * a.n_cells;
+    const int m = a.m;
+    for (int aa = 0; aa < m; aa++) {
+        double rv[3][2];  // row vector: tau_a(i) or e_a
+        for (int b = 0; b < m; b++) {
+            double vr = 0., vi = 0.;
+            if (m == 3) {
+                vr = Kr[aa][b];
+                vi = Ki[aa][b];
+            } else {
+                const double* ta = aa == 0 ? ti1 : ti2;
+                const double* tb = b == 0 ? tj1 : tj2;
+                for (int p = 0; p < 3; p++) {
+                    double kr = Kr[p][0] * tb[0] + Kr[p][1] * tb[1] + Kr[p][2] * tb[2];
+                    double ki = Ki[p][0] * tb[0] + Ki[p][1] * tb[1] + Ki[p][2] * tb[2];
+                    vr += ta[p] * kr;
+                    vi += ta[p] * ki;
+                }
+            }
+            rv[b][0] = vr;
+            rv[b][1] = vi;
+        }
+        size_t off = ((size_t)i * m + aa) * dim + (size_t)j * m;
+        if (a.c64) {
+            float2* dst = reinterpret_cast<float2*>(a.A) + off;
+            for (int b = 0; b < m; b++) dst[b] = make_float2((float)rv[b][0], (float)rv[b][1]);
+        } else {
+            double2* dst = reinterpret_cast<double2*>(a.A) + off;
+            for (int b = 0; b < m; b++) dst[b] = make_double2(rv[b][0], rv[b][1]);
+        }
+    }
+}
+
+template <bool CK, bool MIXED>
+__global__ void __launch_bounds__(kAsmThreads) assemble_far_kernel(AsmArgs a) {
+    using NodeT = typename std::conditional<MIXED, float4, double4>::type;
+    __shared__ __align__(16) NodeT s_nodes[kAsmStageNodes];
+    __shared__ CellGeo s_geo[kAsmMaxCells];
+    __shared__ float s_rho[kAsmMaxCells];
+
+    const int i = blockIdx.x * kAsmThreads + threadIdx.x;
+    const bool live = i < a.n_cells;
+    CellGeo gi;
+    if (live) gi = a.geo[i];
+    else gi = a.geo[0];
+    const double* x = gi.c;
+    const int cb = blockIdx.y * a.cols_per_split;
+    const int ce = min(a.n_cells, cb + a.cols_per_split);
+    const int nn = a.nn;
+    const int cps = nn <= kAsmStageNodes ? max(1, min(kAsmMaxCells, kAsmStageNodes / nn)) : 1;
+    const int kchunk = nn <= kAsmStageNodes ? nn : kAsmStageNodes;
+    const double k2r = a.k.re * a.k.re - a.k.im * a.k.im, k2i = 2.0 * a.k.re * a.k.im;
+
+    using F = typename std::conditional<MIXED, float, double>::type;
+    F a1r = 0, a1i = 0, t[6][2];
+    bool far = false;
+    float Xf[3] = {0.f, 0.f, 0.f}, r0f = 0.f, r0sq = 0.f;
+    double P0r = 1., P0i = 0.;
+    int halvings = 0;
+
+    for (int c0 = cb; c0 < ce; c0 += cps) {
+        const int nc = min(cps, ce - c0);
+        for (int k0 = 0; k0 < nn; k0 += kchunk) {
+            const int kc = min(kchunk, nn - k0);
+            __syncthreads();
+            const int tot = nc * kc;
+            if constexpr (MIXED) {
+                const float4* src = a.nodes32 + (size_t)c0 * nn + k0;
+                for (int q = threadIdx.x; q < tot; q += kAsmThreads) {
+                    int cc = q / kc, kk = q - cc * kc;
+                    s_nodes[q] = __ldg(src + (size_t)cc * nn + kk);
+                }
+            } else {
+                const double2* src = reinterpret_cast<const double2*>(a.nodes64 + (size_t)c0 * nn + k0);
+                double2* dst = reinterpret_cast<double2*>(s_nodes);
+                for (int q = threadIdx.x; q < 2 * tot; q += kAsmThreads) {
+                    int node = q >> 1, cc = node / kc, kk = node - cc * kc;
+                    dst[q] = __ldg(src + 2 * ((size_t)cc * nn + kk) + (q & 1));
+                }
+            }
+            if (k0 == 0)
+                for (int q = threadIdx.x; q < nc; q += kAsmThreads) {
+                    s_geo[q] = a.geo[c0 + q];
+                    if (MIXED) s_rho[q] = a.rho32[c0 + q];
+                }
+            __syncthreads();
+            for (int cc = 0; cc < nc; cc++) {
+                const CellGeo& gj = s_geo[cc];
+                if (k0 == 0) {
+                    double d;
+                    far = live && !asm_is_near(x, gj, a.analytic_calc, &d);
+                    a1r = a1i = 0;
+                    for (int q = 0; q < 6; q++) t[q][0] = t[q][1] = 0;
+                    if (MIXED && far) {
+                        Xf[0] = (float)(x[0] - gj.c[0]);
+                        Xf[1] = (float)(x[1] - gj.c[1]);
+                        Xf[2] = (float)(x[2] - gj.c[2]);
+                        r0f = (float)d;
+                        r0sq = (float)(d * d);
+                        double sn, cs;
+                        sincos(a.k.re * d, &sn, &cs);
+                        if (CK) {
+                            double am = exp(-a.k.im * d);
+                            sn *= am;
+                            cs *= am;
+                        }
+                        P0r = cs;
+                        P0i = sn;
+                        float th = (float)fabs(a.k.re) * s_rho[cc];
+                        halvings = th <= 1.f ? 0 : (th <= 2.f ? 1 : (th <= 4.f ? 2 : 3));
+                    }
+                }
+                if (far) {
+                    const NodeT* nd = s_nodes + cc * kc;
+                    for (int q = 0; q < kc; q++) {
+                        F dx, dy, dz, w, ir, ir2, ir3, er, ei;
+                        if constexpr (MIXED) {
+                            float4 v = nd[q];
+                            float tx = fmaf(-2.f, Xf[0], v.x), ty = fmaf(-2.f, Xf[1], v.y), tz = fmaf(-2.f, Xf[2], v.z);
+                            float qq = fmaf(v.x, tx, fmaf(v.y, ty, v.z * tz));
+                            float r2 = r0sq + qq;
+                            ir = rsqrtf(r2);
+                            float r = r2 * ir;
+                            float dr = __fdividef(qq, r + r0f);
+                            float sn, cs;
+                            // e^{ik (r - r0)}; phase_f32 lives in field.cu: same polynomial inline here
+                            float th = (float)a.k.re * dr;
+                            if (halvings > 2) {
+                                sincosf(th, &sn, &cs);
+                            } else {
+                                float tt = th * (halvings == 0 ? 1.f : (halvings == 1 ? 0.5f : 0.25f));
+                                float t2 = tt * tt;
+                                float ps = fmaf(t2, 2.7557319e-6f, -1.9841270e-4f);
+                                ps = fmaf(t2, ps, 8.3333333e-3f);
+                                ps = fmaf(t2, ps, -1.6666667e-1f);
+                                ps = fmaf(t2, ps, 1.0f);
+                                sn = tt * ps;
+                                float pc = fmaf(t2, -2.7557319e-7f, 2.4801587e-5f);
+                                pc = fmaf(t2, pc, -1.3888889e-3f);
+                                pc = fmaf(t2, pc, 4.1666667e-2f);
+                                pc = fmaf(t2, pc, -0.5f);
+                                cs = fmaf(t2, pc, 1.0f);
+                                for (int h = 0; h < halvings; h++) {
+                                    float ns = 2.f * sn * cs;
+                                    cs = fmaf(cs, cs, -sn * sn);
+                                    sn = ns;
+                                }
+                            }
+                            w = v.w;
+                            if (CK) w *= __expf(-(float)a.k.im * dr);
+                            dx = Xf[0] - v.x;
+                            dy = Xf[1] - v.y;
+                            dz = Xf[2] - v.z;
+                            er = w * cs;
+                            ei = w * sn;
+                        } else {
+                            double4 v = nd[q];
+                            dx = x[0] - v.x;
+                            dy = x[1] - v.y;
+                            dz = x[2] - v.z;
+                            double r = sqrt(dx * dx + dy * dy + dz * dz);
+                            ir = 1.0 / r;
+                            double sn, cs;
+                            sincos(a.k.re * r, &sn, &cs);
+                            if (CK) {
+                                double am = exp(-a.k.im * r);
+                                sn *= am;
+                                cs *= am;
+                            }
+                            w = v.w;
+                            er = w * cs;
+                            ei = w * sn;
+                            if (!(r >= kMachineZero)) er = ei = 0.;  // F_RotRotSimplePot_H: 0 below MACHINE_ZERO
+                        }
+                        ir2 = ir * ir;
+                        ir3 = ir2 * ir;
+                        F f1r, f1i, f2r, f2i;
+                        if (CK) {
+                            f1r = (F)k2r * ir - ir3 - (F)a.k.im * ir2;
+                            f1i = (F)a.k.re * ir2 + (F)k2i * ir;
+                            f2r = (F)3 * ir3 + (F)3 * (F)a.k.im * ir2 - (F)k2r * ir;
+                            f2i = -(F)3 * (F)a.k.re * ir2 - (F)k2i * ir;
+                        } else {
+                            f1r = (F)k2r * ir - ir3;
+                            f1i = (F)a.k.re * ir2;
+                            f2r = (F)3 * ir3 - (F)k2r * ir;
+                            f2i = -(F)3 * (F)a.k.re * ir2;
+                        }
+                        a1r += er * f1r - ei * f1i;
+                        a1i += er * f1i + ei * f1r;
+                        F a2r = (er * f2r - ei * f2i) * ir2, a2i = (er * f2i + ei * f2r) * ir2;
+                        F dd[6] = {dx * dx, dx * dy, dx * dz, dy * dy, dy * dz, dz * dz};
+#pragma unroll
+                        for (int p = 0; p < 6; p++) {
+                            t[p][0] += a2r * dd[p];
+                            t[p][1] += a2i * dd[p];
+                        }
+                    }
+                }
+                if (k0 + kc == nn && far) {
+                    // K = (A1 I + T) * P0 / 4pi
+                    const int ti[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+                    double Kr[3][3], Ki[3][3];
+                    for (int p = 0; p < 3; p++)
+                        for (int q = 0; q < 3; q++) {
+                            double vr = (double)t[ti[p][q]][0] + (p == q ? (double)a1r : 0.);
+                            double vi = (double)t[ti[p][q]][1] + (p == q ? (double)a1i : 0.);
+                            Kr[p][q] = (vr * P0r - vi * P0i) * kInvFourPi;
+                            Ki[p][q] = (vr * P0i + vi * P0r) * kInvFourPi;
+                        }
+                    write_block(a, i, c0 + cc, Kr, Ki, gi.t1, gi.t2, gj.t1, gj.t2);
+                }
+            }
+        }
+    }
+}
+
+// Far entries with adaptive refinement (p_max > 1): K_RotRot_Far's
+// convergence depends on the current, so each column basis vector runs its
+// own adaptive quadrature (generic per-pair code, nodes on the fly).
+__global__ void assemble_far_adaptive_kernel(AsmArgs a, const double* __restrict__ verts, int nv, DNP np) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n_cells) return;
+    const CellGeo gi = a.geo[i];
+    const int cb = blockIdx.y * a.cols_per_split;
+    const int ce = min(a.n_cells, cb + a.cols_per_split);
+    for (int j = cb; j < ce; j++) {
+        const CellGeo& gj = a.geo[j];
+        double d;
+        if (asm_is_near(gi.c, gj, a.analytic_calc, &d)) continue;
+        DCell cl;
+        cl.nv = nv;
+        for (int v = 0; v < nv; v++)
+            for (int g = 0; g < 3; g++) cl.v[v][g] = verts[((size_t)j * nv + v) * 3 + g];
+        const int m = a.m;
+        cplx v[3][3];  // v[b] = K[J_b], J_b = tau_b(j) (TAU2) or e_b (FULL3)
+        for (int b = 0; b < m; b++) {
+            DKP kp;
+            dkp_zero(kp);
+            kp.smoothR = kMachineZero;
+            kp.smoothRMin = kMachineZero;
+            kp.k = a.k;
+            for (int g = 0; g < 3; g++)
+                kp.current[g] = mk(m == 3 ? (g == b ? 1. : 0.) : (b == 0 ? gj.t1[g] : gj.t2[g]), 0.);
+            integral_cell<cplx>(F_ROTROTSIMPLEPOT_H, gi.c, cl, kp, 3, np.n_start, np.p_max, np.eps, v[b]);
+        }
+        const size_t dim = (size_t)m * a.n_cells;
+        for (int aa = 0; aa < m; aa++) {
+            size_t off = ((size_t)i * m + aa) * dim + (size_t)j * m;
+            for (int b = 0; b < m; b++) {
+                cplx e = m == 3 ? v[b][aa]
+                                : (aa == 0 ? v[b][0] * gi.t1[0] + v[b][1] * gi.t1[1] + v[b][2] * gi.t1[2]
+                                           : v[b][0] * gi.t2[0] + v[b][1] * gi.t2[1] + v[b][2] * gi.t2[2]);
+                e = e * kInvFourPi;
+                if (a.c64) reinterpret_cast<float2*>(a.A)[off + b] = make_float2((float)e.re, (float)e.im);
+                else reinterpret_cast<double2*>(a.A)[off + b] = make_double2(e.re, e.im);
+            }
+        }
+    }
+}
+
+__global__ void asm_near_count_kernel(const CellGeo* __restrict__ geo, int n_cells, double analytic_calc,
+                                      long long* __restrict__ counts) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_cells) return;
+    const double* x = geo[i].c;
+    long long n = 0;
+    for (int j = 0; j < n_cells; j++) {
+        double d;
+        n += asm_is_near(x, geo[j], analytic_calc, &d);
+    }
+    counts[i] = n;
+}
+
+__global__ void asm_near_fill_kernel(const CellGeo* __restrict__ geo, int n_cells, double analytic_calc,
+                                     const long long* __restrict__ offs, int* __restrict__ pr, int* __restrict__ pc) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_cells) return;
+    const double* x = geo[i].c;
+    long long o = offs[i];
+    for (int j = 0; j < n_cells; j++) {
+        double d;
+        if (asm_is_near(x, geo[j], analytic_calc, &d)) {
+            pr[o] = i;
+            pc[o] = j;
+            o++;
+        }
+    }
+}
+
+// Near entries: K_RotRot_HS_Colloc as a 3x3 operator, FP64.
+__global__ void asm_near_kernel(AsmArgs a, const double* __restrict__ verts, int nv, const int* __restrict__ pr,
+                                const int* __restrict__ pc, long long n_pairs, DNP np) {
+    long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n_pairs) return;
+    int i = pr[q], j = pc[q];
+    const CellGeo gi = a.geo[i], gj = a.geo[j];
+    DCell cl;
+    cl.nv = nv;
+    for (int v = 0; v < nv; v++)
+        for (int g = 0; g < 3; g++) cl.v[v][g] = verts[((size_t)j * nv + v) * 3 + g];
+    const double* x = gi.c;
+    cplx I = surf_simplepot_h_hs_dev(cl, x, np.analytic_calc, np.n_start, np.p_max, np.eps, a.k);
+    cplx sI = I * a.k * a.k / kFourPi;
+    DKP ps;
+    dkp_zero(ps);
+    ps.smoothR = kMachineZero;
+    ps.smoothRMin = kMachineZero;
+    ps.k = a.k;
+    cplx M[3][3], dummy[3];
+    K0_dev(F_GRADSIMPLEPOT_H, nullptr, x, cl, ps, np.n_start_seg, np.p_max_seg, np.eps, dummy, M);
+    double Kr[3][3], Ki[3][3];
+    for (int p = 0; p < 3; p++)
+        for (int r = 0; r < 3; r++) {
+            cplx v = M[p][r] / kFourPi;
+            if (p == r) v += sI;
+            Kr[p][r] = v.re;
+            Ki[p][r] = v.im;
+        }
+    write_block(a, i, j, Kr, Ki, gi.t1, gi.t2, gj.t1, gj.t2);
+}
+
+static size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+size_t assemble_ws_base_bytes(const AssembleLaunch& a) {
+    size_t N = a.mesh->n_cells;
+    return 2 * al256((N + 1) * sizeof(long long)) + 256;
+}
+
+static AsmArgs make_args(const AssembleLaunch& a) {
+    const MeshDev& m = *a.mesh;
+    AsmArgs g;
+    g.geo = m.geo;
+    g.n_cells = m.n_cells;
+    g.nodes64 = m.nodes64;
+    g.nodes32 = m.nodes32;
+    g.rho32 = m.rho32;
+    g.nn = a.np.n_start * a.np.n_start;
+    g.k = a.k;
+    g.analytic_calc = a.np.analytic_calc;
+    g.m = a.layout == 1 ? 3 : 2;
+    g.c64 = a.out_c64;
+    g.A = a.A;
+    return g;
+}
+
+cudaError_t assemble_stage1(const AssembleLaunch& a, void* ws, long long* d_total, cudaStream_t s) {
+    const MeshDev& m = *a.mesh;
+    const int N = m.n_cells;
+    long long* counts = (long long*)ws;
+    long long* offs = (long long*)((char*)ws + al256((size_t)(N + 1) * sizeof(long long)));
+    AsmArgs g = make_args(a);
+    int tiles = (N + kAsmThreads - 1) / kAsmThreads;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int splits = std::max(1, std::min((8 * sms + tiles - 1) / tiles, std::max(1, N / 16)));
+    g.cols_per_split = (N + splits - 1) / splits;
+    bool ck = a.k.im != 0.;
+    dim3 grid(tiles, splits);
+    if (a.np.p_max > 1) {
+        DNP np{a.np.eps, a.np.rs, a.np.rs_seg, a.np.analytic_calc, a.np.n_start, a.np.n_start_seg, a.np.p_max,
+               a.np.p_max_seg};
+        assemble_far_adaptive_kernel<<<grid, kAsmThreads, 0, s>>>(g, m.verts, m.nv, np);
+    } else if (a.precision == 1) {
+        if (ck) assemble_far_kernel<true, true><<<grid, kAsmThreads, 0, s>>>(g);
+        else assemble_far_kernel<false, true><<<grid, kAsmThreads, 0, s>>>(g);
+    } else {
+        if (ck) assemble_far_kernel<true, false><<<grid, kAsmThreads, 0, s>>>(g);
+        else assemble_far_kernel<false, false><<<grid, kAsmThreads, 0, s>>>(g);
+    }
+    asm_near_count_kernel<<<tiles, kAsmThreads, 0, s>>>(m.geo, N, a.np.analytic_calc, counts);
+    scan_kernel<<<1, 1024, 0, s>>>(counts, N, offs, d_total);
+    return cudaGetLastError();
+}
+
+cudaError_t assemble_stage2(const AssembleLaunch& a, void* ws, long long n_near, void* pair_ws, cudaStream_t s) {
+    if (n_near <= 0) return cudaSuccess;
+    const MeshDev& m = *a.mesh;
+    const int N = m.n_cells;
+    long long* offs = (long long*)((char*)ws + al256((size_t)(N + 1) * sizeof(long long)));
+    int* pr = (int*)pair_ws;
+    int* pc = pr + n_near;
+    int tiles = (N + kAsmThreads - 1) / kAsmThreads;
+    asm_near_fill_kernel<<<tiles, kAsmThreads, 0, s>>>(m.geo, N, a.np.analytic_calc, offs, pr, pc);
+    AsmArgs g = make_args(a);
+    DNP np{a.np.eps, a.np.rs, a.np.rs_seg, a.np.analytic_calc, a.np.n_start, a.np.n_start_seg, a.np.p_max,
+           a.np.p_max_seg};
+    asm_near_kernel<<<(int)((n_near + 127) / 128), 128, 0, s>>>(g, m.verts, m.nv, pr, pc, n_near, np);
+    return cudaGetLastError();
+}
+
+}  // namespace bielcc_gpu

@@ -1,0 +1,774 @@
+// field.cu — E/H field over every observation-point x cell pair: the
+// GetFieldE_Ideal driver (electrodynamics/get_field.h:35-78) and its H
+// counterpart (examples/field/main0_field_test.cpp:237-311) on sm_100a.
+//
+// Pipeline (one stream, deterministic summation order):
+//   1. far kernel   — one observation point per thread, cell node tiles staged
+//                     in shared memory with 128-bit loads, cells split across
+//                     gridDim.y; far cells only (near cells skipped). Per cell
+//                     the J-independent moments A1 = sum w e f1,
+//                     T = sum w e f2 d^d^T, G = sum w grad F are accumulated and
+//                     contracted with each right-hand side once per cell:
+//                       K_RotRot_Far  (K.h:288-301)  = (A1 J + T J) / 4pi
+//                       R_Rot_Colloc  (R.h:89-111)   = (G x J) / 4pi
+//                     FP64 form: FP64 everywhere. Mixed form: nodes relative to
+//                     the cell centre in FP32, phase split e^{ikr} =
+//                     e^{ik r0} e^{ik (r - r0)} with r0 = |x - centre| and
+//                     e^{ik r0} in FP64, r - r0 = q / (r + r0) with
+//                     q = delta.(delta - 2X) (no cancellation), FP32 cell sums,
+//                     FP64 accumulation across cells.
+//   2. near count + scan + fill — per point, the cells with
+//                     |x - centre| < analytic_calc * diam (get_field.h:58), in
+//                     cell order.
+//   3. near pair kernel — FP64, one pair per thread: the J-independent parts of
+//                     K_RotRot_Near_Smooth (K.h:47-79) and R_Rot_Smooth
+//                     (R.h:46-61) with the reference's adaptive quadrature.
+//   4. finalize     — per (point, RHS): far partials over splits (in order) +
+//                     near pairs (in cell order), x mult, + incident field.
+#include <algorithm>
+#include <type_traits>
+
+#include "internal.h"
+#include "ops.cuh"
+#include "scan.cuh"
+
+namespace bielcc_gpu {
+
+constexpr int kFarThreads = 128;
+constexpr int kStageNodes = 256;
+constexpr int kMaxStageCells = 32;
+
+struct FarArgs {
+    const double* pts;
+    int n_pts;
+    const CellGeo* geo;
+    int n_cells;
+    const double4* nodes64;
+    const float4* nodes32;
+    const float* rho32;
+    int nn;  // nodes per cell
+    const cplx* J;  // [S][N][3]
+    int n_rhs, rhs0;
+    cplx k;
+    double analytic_calc;
+    int cells_per_split;
+    double* partial;  // [split][S][12][P]
+};
+
+// Near decision of get_field.h:58 with the reference's rounding.
+BIELCC_D bool is_near(const double* x, const double* c, double diam, double analytic_calc, double* d_out) {
+    double d = dist3_rn(x, c);
+    *d_out = d;
+    return d < __dmul_rn(analytic_calc, diam);
+}
+
+// Per-thread moment accumulators of one cell.
+template <typename F>
+struct Moments {
+    F a1r, a1i;
+    F t[6][2];  // xx, xy, xz, yy, yz, zz
+    F g[3][2];
+    BIELCC_D void zero() {
+        a1r = a1i = 0;
+        for (int i = 0; i < 6; i++) t[i][0] = t[i][1] = 0;
+        for (int i = 0; i < 3; i++) g[i][0] = g[i][1] = 0;
+    }
+};
+
+// One far node, FP64. dx = x - y; w = node weight. Real k (CK = false) or
+// complex k. F_RotRotSimplePot_H (kernel_lib.h:453-492) and
+// F_GradSimplePot_H (kernel_lib.h:295-313) share r, 1/r and e^{ikr}.
+template <bool CK>
+BIELCC_D void far_node_f64(Moments<double>& m, double dx, double dy, double dz, double w, cplx k, double k2r,
+                           double k2i) {
+    double r2 = dx * dx + dy * dy + dz * dz;
+    double r = sqrt(r2);
+    double ir = 1.0 / r;
+    double s, c;
+    sincos(k.re * r, &s, &c);
+    if (CK) {
+        double a = exp(-k.im * r);
+        s *= a;
+        c *= a;
+    }
+    double ir2 = ir * ir, ir3 = ir2 * ir;
+    double er = w * c, ei = w * s;
+    if (r >= kMachineZero) {  // F_RotRotSimplePot_H is 0 below MACHINE_ZERO
+        double f1r, f1i, f2r, f2i;
+        if (CK) {
+            f1r = k2r * ir - ir3 - k.im * ir2;
+            f1i = k.re * ir2 + k2i * ir;
+            f2r = 3.0 * ir3 + 3.0 * k.im * ir2 - k2r * ir;
+            f2i = -3.0 * k.re * ir2 - k2i * ir;
+        } else {
+            f1r = k2r * ir - ir3;
+            f1i = k.re * ir2;
+            f2r = 3.0 * ir3 - k2r * ir;
+            f2i = -3.0 * k.re * ir2;
+        }
+        m.a1r += er * f1r - ei * f1i;
+        m.a1i += er * f1i + ei * f1r;
+        double a2r = (er * f2r - ei * f2i) * ir2, a2i = (er * f2i + ei * f2r) * ir2;
+        double dd[6] = {dx * dx, dx * dy, dx * dz, dy * dy, dy * dz, dz * dz};
+#pragma unroll
+        for (int q = 0; q < 6; q++) {
+            m.t[q][0] += a2r * dd[q];
+            m.t[q][1] += a2i * dd[q];
+        }
+    }
+    // (ikr - 1) with ikr = (-k.im r, k.re r)
+    double ur = CK ? (-k.im * r - 1.0) : -1.0, ui = k.re * r;
+    double gr = (er * ur - ei * ui) * ir3, gi = (er * ui + ei * ur) * ir3;
+    m.g[0][0] += gr * dx;
+    m.g[0][1] += gi * dx;
+    m.g[1][0] += gr * dy;
+    m.g[1][1] += gi * dy;
+    m.g[2][0] += gr * dz;
+    m.g[2][1] += gi * dz;
+}
+
+// Taylor sine / cosine on |t| <= 1 (truncation below 2.6e-8), FP32.
+BIELCC_D void sincos_poly(float t, float* s, float* c) {
+    float t2 = t * t;
+    float ps = fmaf(t2, 2.7557319e-6f, -1.9841270e-4f);
+    ps = fmaf(t2, ps, 8.3333333e-3f);
+    ps = fmaf(t2, ps, -1.6666667e-1f);
+    ps = fmaf(t2, ps, 1.0f);
+    *s = t * ps;
+    float pc = fmaf(t2, -2.7557319e-7f, 2.4801587e-5f);
+    pc = fmaf(t2, pc, -1.3888889e-3f);
+    pc = fmaf(t2, pc, 4.1666667e-2f);
+    pc = fmaf(t2, pc, -0.5f);
+    *c = fmaf(t2, pc, 1.0f);
+}
+
+// e^{i theta} for |theta| <= 2^halvings: polynomial at theta / 2^h, then h
+// angle doublings; beyond 4 rad the accurate sincosf.
+BIELCC_D void phase_f32(float th, int halvings, float* s, float* c) {
+    if (halvings > 2) {
+        sincosf(th, s, c);
+        return;
+    }
+    float t = th * (halvings == 0 ? 1.f : (halvings == 1 ? 0.5f : 0.25f));
+    float ss, cc;
+    sincos_poly(t, &ss, &cc);
+    for (int h = 0; h < halvings; h++) {
+        float ns = 2.f * ss * cc;
+        cc = fmaf(cc, cc, -ss * ss);
+        ss = ns;
+    }
+    *s = ss;
+    *c = cc;
+}
+
+// One far node, FP32, relative to the cell centre: X = x - centre (FP32),
+// node delta = y - centre, r0 = |X| (FP64 rounded), phase relative to r0.
+template <bool CK>
+BIELCC_D void far_node_f32(Moments<float>& m, float Xx, float Xy, float Xz, float r0, float r0sq, float4 nd, float kr_,
+                           float ki_, float k2r, float k2i, int halvings) {
+    float tx = fmaf(-2.f, Xx, nd.x), ty = fmaf(-2.f, Xy, nd.y), tz = fmaf(-2.f, Xz, nd.z);
+    float q = fmaf(nd.x, tx, fmaf(nd.y, ty, nd.z * tz));  // |x-y|^2 - r0^2
+    float r2 = r0sq + q;
+    float ir = rsqrtf(r2);
+    float r = r2 * ir;
+    float dr = __fdividef(q, r + r0);
+    float s, c;
+    phase_f32(kr_ * dr, halvings, &s, &c);
+    float w = nd.w;
+    if (CK) w *= __expf(-ki_ * dr);
+    float dx = Xx - nd.x, dy = Xy - nd.y, dz = Xz - nd.z;
+    float ir2 = ir * ir, ir3 = ir2 * ir;
+    float er = w * c, ei = w * s;
+    float f1r, f1i, f2r, f2i;
+    if (CK) {
+        f1r = k2r * ir - ir3 - ki_ * ir2;
+        f1i = kr_ * ir2 + k2i * ir;
+        f2r = 3.f * ir3 + 3.f * ki_ * ir2 - k2r * ir;
+        f2i = -3.f * kr_ * ir2 - k2i * ir;
+    } else {
+        f1r = k2r * ir - ir3;
+        f1i = kr_ * ir2;
+        f2r = 3.f * ir3 - k2r * ir;
+        f2i = -3.f * kr_ * ir2;
+    }
+    m.a1r = fmaf(er, f1r, fmaf(-ei, f1i, m.a1r));
+    m.a1i = fmaf(er, f1i, fmaf(ei, f1r, m.a1i));
+    float a2r = (er * f2r - ei * f2i) * ir2, a2i = (er * f2i + ei * f2r) * ir2;
+    float bx_r = a2r * dx, bx_i = a2i * dx, by_r = a2r * dy, by_i = a2i * dy, bz_r = a2r * dz, bz_i = a2i * dz;
+    m.t[0][0] = fmaf(bx_r, dx, m.t[0][0]);
+    m.t[0][1] = fmaf(bx_i, dx, m.t[0][1]);
+    m.t[1][0] = fmaf(bx_r, dy, m.t[1][0]);
+    m.t[1][1] = fmaf(bx_i, dy, m.t[1][1]);
+    m.t[2][0] = fmaf(bx_r, dz, m.t[2][0]);
+    m.t[2][1] = fmaf(bx_i, dz, m.t[2][1]);
+    m.t[3][0] = fmaf(by_r, dy, m.t[3][0]);
+    m.t[3][1] = fmaf(by_i, dy, m.t[3][1]);
+    m.t[4][0] = fmaf(by_r, dz, m.t[4][0]);
+    m.t[4][1] = fmaf(by_i, dz, m.t[4][1]);
+    m.t[5][0] = fmaf(bz_r, dz, m.t[5][0]);
+    m.t[5][1] = fmaf(bz_i, dz, m.t[5][1]);
+    float ur = CK ? (-ki_ * r - 1.f) : -1.f, ui = kr_ * r;
+    float gr = (er * ur - ei * ui) * ir3, gi = (er * ui + ei * ur) * ir3;
+    m.g[0][0] = fmaf(gr, dx, m.g[0][0]);
+    m.g[0][1] = fmaf(gi, dx, m.g[0][1]);
+    m.g[1][0] = fmaf(gr, dy, m.g[1][0]);
+    m.g[1][1] = fmaf(gi, dy, m.g[1][1]);
+    m.g[2][0] = fmaf(gr, dz, m.g[2][0]);
+    m.g[2][1] = fmaf(gi, dz, m.g[2][1]);
+}
+
+// Contract one cell's moments (times the phase P = pr + i pi) with the RHS
+// currents and add into the FP64 accumulators acc[r][12] =
+// (Ex, Ey, Ez, Hx, Hy, Hz) x (re, im).
+template <int NRHS, typename F>
+BIELCC_D void contract(const Moments<F>& m, F pr, F pi, const cplx (*sj)[3], bool zeroR, double (*acc)[12]) {
+    // moments x phase
+    F A1r = m.a1r * pr - m.a1i * pi, A1i = m.a1r * pi + m.a1i * pr;
+    F T[6][2], G[3][2];
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        T[q][0] = m.t[q][0] * pr - m.t[q][1] * pi;
+        T[q][1] = m.t[q][0] * pi + m.t[q][1] * pr;
+    }
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        G[q][0] = m.g[q][0] * pr - m.g[q][1] * pi;
+        G[q][1] = m.g[q][0] * pi + m.g[q][1] * pr;
+    }
+    const int ti[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+#pragma unroll
+    for (int rr = 0; rr < NRHS; rr++) {
+        F jr[3], ji[3];
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            jr[a] = (F)sj[rr][a].re;
+            ji[a] = (F)sj[rr][a].im;
+        }
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            F er = A1r * jr[a] - A1i * ji[a], ei = A1r * ji[a] + A1i * jr[a];
+#pragma unroll
+            for (int b = 0; b < 3; b++) {
+                const F* t = T[ti[a][b]];
+                er += t[0] * jr[b] - t[1] * ji[b];
+                ei += t[0] * ji[b] + t[1] * jr[b];
+            }
+            acc[rr][2 * a] += (double)er;
+            acc[rr][2 * a + 1] += (double)ei;
+        }
+        if (!zeroR) {
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                int b = (a + 1) % 3, c = (a + 2) % 3;  // (G x J)_a = G_b J_c - G_c J_b
+                F hr = (G[b][0] * jr[c] - G[b][1] * ji[c]) - (G[c][0] * jr[b] - G[c][1] * ji[b]);
+                F hi = (G[b][0] * ji[c] + G[b][1] * jr[c]) - (G[c][0] * ji[b] + G[c][1] * jr[b]);
+                acc[rr][6 + 2 * a] += (double)hr;
+                acc[rr][6 + 2 * a + 1] += (double)hi;
+            }
+        }
+    }
+}
+
+// The far kernel. MIXED = false: FP64 nodes; true: FP32 nodes.
+template <int NRHS, bool CK, bool MIXED>
+__global__ void __launch_bounds__(kFarThreads) far_kernel(FarArgs a) {
+    using NodeT = typename std::conditional<MIXED, float4, double4>::type;
+    __shared__ __align__(16) NodeT s_nodes[kStageNodes];
+    __shared__ double4 s_cell[kMaxStageCells];  // centre xyz, near threshold
+    __shared__ cplx s_j[kMaxStageCells][NRHS][3];
+    __shared__ float s_rho[kMaxStageCells];
+
+    const int p = blockIdx.x * kFarThreads + threadIdx.x;
+    const bool live = p < a.n_pts;
+    double x[3] = {0., 0., 0.};
+    if (live)
+        for (int g = 0; g < 3; g++) x[g] = a.pts[3 * (size_t)p + g];
+    const int cb = blockIdx.y * a.cells_per_split;
+    const int ce = min(a.n_cells, cb + a.cells_per_split);
+    const int nn = a.nn;
+    const int cps = nn <= kStageNodes ? max(1, min(kMaxStageCells, kStageNodes / nn)) : 1;
+    const int kchunk = nn <= kStageNodes ? nn : kStageNodes;
+    const double k2r = a.k.re * a.k.re - a.k.im * a.k.im, k2i = 2.0 * a.k.re * a.k.im;
+
+    double acc[NRHS][12];
+#pragma unroll
+    for (int r = 0; r < NRHS; r++)
+#pragma unroll
+        for (int q = 0; q < 12; q++) acc[r][q] = 0.;
+
+    using F = typename std::conditional<MIXED, float, double>::type;
+    Moments<F> m;
+    m.zero();
+    bool far = false, zeroR = false;
+    // mixed-form per-pair state
+    float Xf[3] = {0.f, 0.f, 0.f}, r0f = 0.f, r0sq = 0.f;
+    double P0r = 1.0, P0i = 0.0;
+    int halvings = 0;
+
+    for (int c0 = cb; c0 < ce; c0 += cps) {
+        const int nc = min(cps, ce - c0);
+        for (int k0 = 0; k0 < nn; k0 += kchunk) {
+            const int kc = min(kchunk, nn - k0);
+            __syncthreads();
+            // stage nodes (contiguous when kc == nn) with 128-bit loads
+            {
+                const int tot = nc * kc;
+                if constexpr (MIXED) {
+                    const float4* src = a.nodes32 + (size_t)c0 * nn + k0;
+                    for (int i = threadIdx.x; i < tot; i += kFarThreads) {
+                        int cc = i / kc, kk = i - cc * kc;
+                        s_nodes[i] = __ldg(src + (size_t)cc * nn + kk);
+                    }
+                } else {
+                    const double2* src = reinterpret_cast<const double2*>(a.nodes64 + (size_t)c0 * nn + k0);
+                    double2* dst = reinterpret_cast<double2*>(s_nodes);
+                    for (int i = threadIdx.x; i < 2 * tot; i += kFarThreads) {
+                        int node = i >> 1, cc = node / kc, kk = node - cc * kc;
+                        dst[i] = __ldg(src + 2 * ((size_t)cc * nn + kk) + (i & 1));
+                    }
+                }
+            }
+            if (k0 == 0) {
+                for (int i = threadIdx.x; i < nc; i += kFarThreads) {
+                    const CellGeo& gg = a.geo[c0 + i];
+                    s_cell[i] = make_double4(gg.c[0], gg.c[1], gg.c[2], gg.diam);
+                    if (MIXED) s_rho[i] = a.rho32[c0 + i];
+                }
+                for (int i = threadIdx.x; i < nc * NRHS * 3; i += kFarThreads) {
+                    int cc = i / (NRHS * 3), rem = i - cc * NRHS * 3, rr = rem / 3, g = rem - rr * 3;
+                    int rhs = min(a.rhs0 + rr, a.n_rhs - 1);
+                    s_j[cc][rr][g] = a.J[((size_t)rhs * a.n_cells + (c0 + cc)) * 3 + g];
+                }
+            }
+            __syncthreads();
+            for (int cc = 0; cc < nc; cc++) {
+                if (k0 == 0) {
+                    double4 ci = s_cell[cc];
+                    double cen[3] = {ci.x, ci.y, ci.z}, d;
+                    far = !is_near(x, cen, ci.w, a.analytic_calc, &d) && live;
+                    zeroR = d < kMachineZero;  // R_Rot_Colloc: R = 0 at the cell centre
+                    m.zero();
+                    if (MIXED && far) {  // per-pair FP64 set-up of the phase split
+                        Xf[0] = (float)(x[0] - ci.x);
+                        Xf[1] = (float)(x[1] - ci.y);
+                        Xf[2] = (float)(x[2] - ci.z);
+                        r0f = (float)d;
+                        r0sq = (float)(d * d);
+                        double s, c;
+                        sincos(a.k.re * d, &s, &c);
+                        if (CK) {
+                            double am = exp(-a.k.im * d);
+                            s *= am;
+                            c *= am;
+                        }
+                        P0r = c;
+                        P0i = s;
+                        float th = (float)fabs(a.k.re) * s_rho[cc];
+                        halvings = th <= 1.f ? 0 : (th <= 2.f ? 1 : (th <= 4.f ? 2 : 3));
+                    }
+                }
+                if (far) {
+                    const NodeT* nd = s_nodes + cc * kc;
+                    if constexpr (MIXED) {
+                        const float kr_ = (float)a.k.re, ki_ = (float)a.k.im;
+                        const float k2rf = (float)k2r, k2if = (float)k2i;
+#pragma unroll 4
+                        for (int i = 0; i < kc; i++)
+                            far_node_f32<CK>(m, Xf[0], Xf[1], Xf[2], r0f, r0sq, nd[i], kr_, ki_, k2rf, k2if,
+                                             halvings);
+                    } else {
+#pragma unroll 2
+                        for (int i = 0; i < kc; i++) {
+                            double4 v = nd[i];
+                            far_node_f64<CK>(m, x[0] - v.x, x[1] - v.y, x[2] - v.z, v.w, a.k, k2r, k2i);
+                        }
+                    }
+                }
+                if (k0 + kc == nn && far) {
+                    if constexpr (MIXED) contract<NRHS, float>(m, (float)P0r, (float)P0i, s_j[cc], zeroR, acc);
+                    else contract<NRHS, double>(m, 1.0, 0.0, s_j[cc], zeroR, acc);
+                }
+            }
+        }
+    }
+    if (!live) return;
+    const size_t P = a.n_pts;
+#pragma unroll
+    for (int r = 0; r < NRHS; r++) {
+        if (a.rhs0 + r >= a.n_rhs) break;
+        double* dst = a.partial + (((size_t)blockIdx.y * a.n_rhs + (a.rhs0 + r)) * 12) * P + p;
+#pragma unroll
+        for (int q = 0; q < 12; q++) dst[(size_t)q * P] = acc[r][q];
+    }
+}
+
+// Far pairs with adaptive refinement (p_max > 1): the reference's
+// convergence test of K_RotRot_Far runs on F_RotRotSimplePot_H . J, so the
+// refinement depth depends on the current; one RHS per launch, generic
+// per-pair quadrature with nodes generated on the fly (ops.cuh). R_Rot_Colloc
+// is J-independent (moment G). Writes the same raw partials as far_kernel.
+__global__ void far_adaptive_kernel(FarArgs a, const double* __restrict__ verts, int nv, DNP np) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.n_pts) return;
+    const int rhs = a.rhs0;
+    double x[3] = {a.pts[3 * (size_t)p], a.pts[3 * (size_t)p + 1], a.pts[3 * (size_t)p + 2]};
+    const int cb = blockIdx.y * a.cells_per_split;
+    const int ce = min(a.n_cells, cb + a.cells_per_split);
+    double acc[12];
+    for (int q = 0; q < 12; q++) acc[q] = 0.;
+    for (int c = cb; c < ce; c++) {
+        const CellGeo& gg = a.geo[c];
+        double d;
+        if (is_near(x, gg.c, gg.diam, a.analytic_calc, &d)) continue;
+        DCell cl;
+        cl.nv = nv;
+        for (int v = 0; v < nv; v++)
+            for (int g = 0; g < 3; g++) cl.v[v][g] = verts[((size_t)c * nv + v) * 3 + g];
+        const cplx* j = a.J + ((size_t)rhs * a.n_cells + c) * 3;
+        DKP kp;
+        dkp_zero(kp);
+        kp.smoothR = kMachineZero;
+        kp.smoothRMin = kMachineZero;
+        kp.k = a.k;
+        for (int g = 0; g < 3; g++) kp.current[g] = j[g];
+        cplx K[3];
+        integral_cell<cplx>(F_ROTROTSIMPLEPOT_H, x, cl, kp, 3, np.n_start, np.p_max, np.eps, K);
+        for (int g = 0; g < 3; g++) {
+            acc[2 * g] += K[g].re;
+            acc[2 * g + 1] += K[g].im;
+        }
+        if (!(d < kMachineZero)) {  // R_Rot_Colloc: 0 at the cell centre
+            DKP kr;
+            dkp_zero(kr);
+            kr.smoothR = kMachineZero;
+            kr.smoothRMin = kMachineZero;
+            kr.k = a.k;
+            cplx G[3], h[3], jj[3] = {j[0], j[1], j[2]};
+            integral_cell<cplx>(F_GRADSIMPLEPOT_H, x, cl, kr, 3, np.n_start, np.p_max, np.eps, G);
+            ccross_cc(G, jj, h);
+            for (int g = 0; g < 3; g++) {
+                acc[6 + 2 * g] += h[g].re;
+                acc[6 + 2 * g + 1] += h[g].im;
+            }
+        }
+    }
+    const size_t P = a.n_pts;
+    double* dst = a.partial + (((size_t)blockIdx.y * a.n_rhs + rhs) * 12) * P + p;
+    for (int q = 0; q < 12; q++) dst[(size_t)q * P] = acc[q];
+}
+
+// ---------------------------------------------------------------- near classification
+__global__ void near_count_kernel(const double* __restrict__ pts, int n_pts, const CellGeo* __restrict__ geo,
+                                  int n_cells, double analytic_calc, long long* __restrict__ counts) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n_pts) return;
+    double x[3] = {pts[3 * (size_t)p], pts[3 * (size_t)p + 1], pts[3 * (size_t)p + 2]};
+    long long n = 0;
+    for (int c = 0; c < n_cells; c++) {
+        double d;
+        n += is_near(x, geo[c].c, geo[c].diam, analytic_calc, &d);
+    }
+    counts[p] = n;
+}
+
+__global__ void near_fill_kernel(const double* __restrict__ pts, int n_pts, const CellGeo* __restrict__ geo,
+                                 int n_cells, double analytic_calc, const long long* __restrict__ offs,
+                                 int* __restrict__ pair_cell, int* __restrict__ pair_pt) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n_pts) return;
+    double x[3] = {pts[3 * (size_t)p], pts[3 * (size_t)p + 1], pts[3 * (size_t)p + 2]};
+    long long o = offs[p];
+    for (int c = 0; c < n_cells; c++) {
+        double d;
+        if (is_near(x, geo[c].c, geo[c].diam, analytic_calc, &d)) {
+            pair_cell[o] = c;
+            pair_pt[o] = p;
+            o++;
+        }
+    }
+}
+
+// Near pair: J-independent parts of K_RotRot_Near_Smooth and R_Rot_Smooth,
+// scaled by 1/4pi: out[13] = { surf * k^2 / 4pi, M (3x3) / 4pi, g (3) / 4pi },
+// K = out0 * J + M J, R = g x J.
+__global__ void near_pair_kernel(const double* __restrict__ pts, const double* __restrict__ verts, int nv,
+                                 const int* __restrict__ pair_cell, const int* __restrict__ pair_pt, long long n_pairs,
+                                 cplx k, DNP np, cplx* __restrict__ out) {
+    long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n_pairs) return;
+    int c = pair_cell[q], p = pair_pt[q];
+    DCell cl;
+    cl.nv = nv;
+    for (int v = 0; v < nv; v++)
+        for (int g = 0; g < 3; g++) cl.v[v][g] = verts[((size_t)c * nv + v) * 3 + g];
+    double x[3] = {pts[3 * (size_t)p], pts[3 * (size_t)p + 1], pts[3 * (size_t)p + 2]};
+    double dm = cell_diam(cl);
+    // surface part of K_RotRot_Near_Smooth (K.h:51-67)
+    DKP pF;
+    dkp_zero(pF);
+    pF.smoothR = np.rs * dm / np.n_start;
+    pF.smoothRMin = np.eps;
+    pF.k = k;
+    cplx s[1];
+    integral_cell<cplx>(F_SIMPLEPOT_H, x, cl, pF, 1, np.n_start, np.p_max, np.eps, s);
+    cplx* o = out + q * 13;
+    o[0] = s[0] * k * k / kFourPi;
+    // contour part (K.h:56-72): K0 with the shared, shrinking segment radius
+    DKP pG;
+    dkp_zero(pG);
+    pG.smoothR = np.rs_seg * dm / np.n_start_seg;
+    pG.smoothRMin = np.eps;
+    pG.k = k;
+    cplx M[3][3], dummy[3];
+    K0_dev(F_GRADSIMPLEPOT_H, nullptr, x, cl, pG, np.n_start_seg, np.p_max_seg, np.eps, dummy, M);
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) o[1 + 3 * a + b] = M[a][b] / kFourPi;
+    // R_Rot_Smooth (R.h:46-61)
+    DKP pR;
+    dkp_zero(pR);
+    pR.smoothR = np.rs * dm / np.n_start;
+    pR.smoothRMin = dm / 100.;
+    pR.k = k;
+    cplx g[3];
+    integral_cell<cplx>(F_GRADSIMPLEPOT_H, x, cl, pR, 3, np.n_start, np.p_max, np.eps, g);
+    for (int a = 0; a < 3; a++) o[10 + a] = g[a] / kFourPi;
+}
+
+struct FinalArgs {
+    const double* pts;
+    int n_pts, n_rhs, n_cells, splits;
+    const double* partial;
+    const long long* offs;
+    const int* pair_cell;
+    const cplx* moments;
+    const cplx* J;
+    cplx mult;
+    double kvec[3], e0[3], h_scale;
+    int add_E, add_H;
+    double* E;
+    double* H;
+    unsigned long long* nonfinite;
+};
+
+__global__ void finalize_kernel(FinalArgs a) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    int s = blockIdx.y;
+    if (p >= a.n_pts) return;
+    const size_t P = a.n_pts;
+    double v[12];
+    for (int q = 0; q < 12; q++) v[q] = 0.;
+    for (int sp = 0; sp < a.splits; sp++) {
+        const double* src = a.partial + (((size_t)sp * a.n_rhs + s) * 12) * P + p;
+        for (int q = 0; q < 12; q++) v[q] += src[(size_t)q * P];
+    }
+    cplx E[3], H[3];
+    for (int g = 0; g < 3; g++) {
+        E[g] = mk(v[2 * g], v[2 * g + 1]) * kInvFourPi;
+        H[g] = mk(v[6 + 2 * g], v[6 + 2 * g + 1]) * kInvFourPi;
+    }
+    if (a.offs) {
+        for (long long q = a.offs[p]; q < a.offs[p + 1]; q++) {
+            int c = a.pair_cell[q];
+            const cplx* o = a.moments + q * 13;
+            const cplx* j = a.J + ((size_t)s * a.n_cells + c) * 3;
+            for (int g = 0; g < 3; g++) {
+                cplx kv = o[0] * j[g] + o[1 + 3 * g] * j[0] + o[2 + 3 * g] * j[1] + o[3 + 3 * g] * j[2];
+                E[g] += kv;
+            }
+            cplx h[3];
+            ccross_cc(o + 10, j, h);
+            for (int g = 0; g < 3; g++) H[g] += h[g];
+        }
+    }
+    for (int g = 0; g < 3; g++) E[g] = E[g] * a.mult;
+    const double* x = a.pts + 3 * (size_t)p;
+    if (a.add_E || a.add_H) {
+        double ph = a.kvec[0] * x[0] + a.kvec[1] * x[1] + a.kvec[2] * x[2];
+        double sn, cs;
+        sincos(ph, &sn, &cs);
+        if (a.add_E)
+            for (int g = 0; g < 3; g++) E[g] += mk(a.e0[g] * cs, a.e0[g] * sn);
+        if (a.add_H) {
+            double kx0[3];
+            cross3(a.kvec, a.e0, kx0);
+            for (int g = 0; g < 3; g++) H[g] += mk(kx0[g] * cs * a.h_scale, kx0[g] * sn * a.h_scale);
+        }
+    }
+    bool bad = false;
+    cplx* eo = reinterpret_cast<cplx*>(a.E) + ((size_t)s * P + p) * 3;
+    for (int g = 0; g < 3; g++) {
+        eo[g] = E[g];
+        bad |= !isfinite(E[g].re) || !isfinite(E[g].im);
+    }
+    if (a.H) {
+        cplx* ho = reinterpret_cast<cplx*>(a.H) + ((size_t)s * P + p) * 3;
+        for (int g = 0; g < 3; g++) {
+            ho[g] = H[g];
+            bad |= !isfinite(H[g].re) || !isfinite(H[g].im);
+        }
+    }
+    if (bad && a.nonfinite) atomicAdd(a.nonfinite, 1ull);
+}
+
+// ---------------------------------------------------------------- host launchers
+static int resident_far_ctas() {
+    static int cached = 0;
+    if (cached) return cached;
+    int dev = 0, sms = 148, per = 4;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, far_kernel<1, false, false>, kFarThreads, 0);
+    cached = std::max(1, sms * std::max(1, per));
+    return cached;
+}
+
+static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+size_t field_ws_base_bytes(const FieldLaunch& f, int* splits_out) {
+    int tiles = (f.n_pts + kFarThreads - 1) / kFarThreads;
+    int N = f.mesh->n_cells;
+    int target = 2 * resident_far_ctas();
+    int splits = std::max(1, (target + tiles - 1) / std::max(1, tiles));
+    splits = std::min(splits, std::max(1, N / 8));
+    *splits_out = splits;
+    size_t P = f.n_pts;
+    return align256((size_t)splits * f.n_rhs * 12 * P * sizeof(double)) + 2 * align256((P + 1) * sizeof(long long)) +
+           align256(sizeof(long long));
+}
+
+template <int NRHS, bool CK, bool MIXED>
+static void launch_far_t(const FarArgs& a, int tiles, int splits, cudaStream_t s) {
+    far_kernel<NRHS, CK, MIXED><<<dim3(tiles, splits), kFarThreads, 0, s>>>(a);
+}
+
+template <bool CK, bool MIXED>
+static int launch_far_rhs(FarArgs a, int tiles, int splits, cudaStream_t s) {
+    int n = 0;
+    for (int r0 = 0; r0 < a.n_rhs; n++) {
+        a.rhs0 = r0;
+        int left = a.n_rhs - r0;
+        if (left >= 4) { launch_far_t<4, CK, MIXED>(a, tiles, splits, s); r0 += 4; }
+        else if (left >= 2) { launch_far_t<2, CK, MIXED>(a, tiles, splits, s); r0 += 2; }
+        else { launch_far_t<1, CK, MIXED>(a, tiles, splits, s); r0 += 1; }
+    }
+    return n;
+}
+
+cudaError_t field_stage1(const FieldLaunch& f, void* ws, int splits, long long* d_total, cudaStream_t s,
+                         int* launches, cudaEvent_t far_begin, cudaEvent_t far_end, int* far_launches) {
+    const MeshDev& m = *f.mesh;
+    const size_t P = f.n_pts;
+    char* w = (char*)ws;
+    double* partial = (double*)w;
+    w += align256((size_t)splits * f.n_rhs * 12 * P * sizeof(double));
+    long long* counts = (long long*)w;
+    w += align256((P + 1) * sizeof(long long));
+    long long* offs = (long long*)w;
+
+    FarArgs a;
+    a.pts = f.pts;
+    a.n_pts = f.n_pts;
+    a.geo = m.geo;
+    a.n_cells = m.n_cells;
+    a.nodes64 = m.nodes64;
+    a.nodes32 = m.nodes32;
+    a.rho32 = m.rho32;
+    a.nn = f.np.n_start * f.np.n_start;
+    a.J = reinterpret_cast<const cplx*>(f.J);
+    a.n_rhs = f.n_rhs;
+    a.rhs0 = 0;
+    a.k = f.k;
+    a.analytic_calc = f.np.analytic_calc;
+    a.cells_per_split = (m.n_cells + splits - 1) / splits;
+    a.partial = partial;
+    int tiles = (f.n_pts + kFarThreads - 1) / kFarThreads;
+    bool ck = f.k.im != 0.0;
+    bool mixed = f.precision == 1;
+    int nl = 0;
+    if (far_begin) cudaEventRecord(far_begin, s);
+    if (tiles > 0 && f.np.p_max > 1) {
+        DNP np{f.np.eps, f.np.rs, f.np.rs_seg, f.np.analytic_calc, f.np.n_start, f.np.n_start_seg, f.np.p_max,
+               f.np.p_max_seg};
+        for (int r = 0; r < f.n_rhs; r++, nl++) {
+            a.rhs0 = r;
+            far_adaptive_kernel<<<dim3(tiles, splits), kFarThreads, 0, s>>>(a, m.verts, m.nv, np);
+        }
+    } else if (tiles > 0) {
+        if (mixed) nl = ck ? launch_far_rhs<true, true>(a, tiles, splits, s) : launch_far_rhs<false, true>(a, tiles, splits, s);
+        else nl = ck ? launch_far_rhs<true, false>(a, tiles, splits, s) : launch_far_rhs<false, false>(a, tiles, splits, s);
+    }
+    if (far_end) cudaEventRecord(far_end, s);
+    if (tiles > 0)
+        near_count_kernel<<<tiles, kFarThreads, 0, s>>>(f.pts, f.n_pts, m.geo, m.n_cells, f.np.analytic_calc,
+                                                        counts);
+    *far_launches = nl;
+    *launches = nl + (tiles > 0 ? 1 : 0) + 1;
+    scan_kernel<<<1, 1024, 0, s>>>(counts, f.n_pts, offs, d_total);
+    return cudaGetLastError();
+}
+
+cudaError_t field_stage2(const FieldLaunch& f, void* ws, int splits, long long n_near, void* pair_ws,
+                         unsigned long long* d_nonfinite, cudaStream_t s, int* launches) {
+    *launches = 0;
+    const MeshDev& m = *f.mesh;
+    const size_t P = f.n_pts;
+    char* w = (char*)ws;
+    double* partial = (double*)w;
+    w += align256((size_t)splits * f.n_rhs * 12 * P * sizeof(double));
+    w += align256((P + 1) * sizeof(long long));
+    long long* offs = (long long*)w;
+
+    int* pair_cell = nullptr;
+    int* pair_pt = nullptr;
+    cplx* moments = nullptr;
+    int tiles = (f.n_pts + kFarThreads - 1) / kFarThreads;
+    if (n_near > 0) {
+        char* pw = (char*)pair_ws;
+        moments = (cplx*)pw;
+        pw += align256((size_t)n_near * 13 * sizeof(cplx));
+        pair_cell = (int*)pw;
+        pw += align256((size_t)n_near * sizeof(int));
+        pair_pt = (int*)pw;
+        near_fill_kernel<<<tiles, kFarThreads, 0, s>>>(f.pts, f.n_pts, m.geo, m.n_cells, f.np.analytic_calc, offs,
+                                                       pair_cell, pair_pt);
+        DNP np{f.np.eps, f.np.rs, f.np.rs_seg, f.np.analytic_calc, f.np.n_start, f.np.n_start_seg, f.np.p_max,
+               f.np.p_max_seg};
+        int blocks = (int)((n_near + 127) / 128);
+        near_pair_kernel<<<blocks, 128, 0, s>>>(f.pts, m.verts, m.nv, pair_cell, pair_pt, n_near, f.k, np, moments);
+        *launches += 2;
+    }
+    FinalArgs fa;
+    fa.pts = f.pts;
+    fa.n_pts = f.n_pts;
+    fa.n_rhs = f.n_rhs;
+    fa.n_cells = m.n_cells;
+    fa.splits = splits;
+    fa.partial = partial;
+    fa.offs = n_near > 0 ? offs : nullptr;
+    fa.pair_cell = pair_cell;
+    fa.moments = moments;
+    fa.J = reinterpret_cast<const cplx*>(f.J);
+    fa.mult = f.mult;
+    for (int g = 0; g < 3; g++) {
+        fa.kvec[g] = f.kvec[g];
+        fa.e0[g] = f.e0[g];
+    }
+    fa.h_scale = f.h_scale;
+    fa.add_E = f.add_E;
+    fa.add_H = f.add_H;
+    fa.E = f.E;
+    fa.H = f.H;
+    fa.nonfinite = d_nonfinite;
+    if (tiles > 0 && f.n_rhs > 0) {
+        finalize_kernel<<<dim3(tiles, f.n_rhs), kFarThreads, 0, s>>>(fa);
+        *launches += 1;
+    }
+    return cudaGetLastError();
+}
+
+// Bytes of the stage-2 pair workspace for n_near pairs (matches the carving).
+size_t field_pair_ws_bytes(long long n_near) {
+    return align256((size_t)n_near * 13 * sizeof(cplx)) + 2 * align256((size_t)n_near * sizeof(int));
+}
+
+}  // namespace bielcc_gpu

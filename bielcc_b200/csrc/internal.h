@@ -1,0 +1,96 @@
+// internal.h — host-side declarations shared by the .cu files of
+// libbielcc_gpu.so (kernel launchers and workspace records). Not installed.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace bielcc_gpu {
+
+struct NumParamH {
+    double eps, rs, rs_seg, analytic_calc;
+    int n_start, n_start_seg, p_max, p_max_seg;
+};
+
+// Device-resident mesh with its per-cell geometry and cached node tables.
+struct MeshDev {
+    int nv = 0, n_cells = 0;
+    double* verts = nullptr;  // [N][nv][3]
+    CellGeo* geo = nullptr;   // [N]
+    // node tables for one split n (n^2 nodes per cell): FP64 absolute
+    // (x, y, z, weight) and FP32 relative to the centre (dx, dy, dz, weight)
+    int table_n = 0;
+    double4* nodes64 = nullptr;  // [N][n*n]
+    float4* nodes32 = nullptr;   // [N][n*n]
+    float* rho32 = nullptr;      // [N] max |node - centre|
+    size_t bytes = 0;
+};
+
+// ---- mesh.cu
+cudaError_t launch_cell_geometry(const double* verts, int nv, int n_cells, CellGeo* geo, cudaStream_t s);
+cudaError_t launch_node_tables(const double* verts, const CellGeo* geo, int nv, int n_cells, int n, double4* nodes64,
+                               float4* nodes32, float* rho32, cudaStream_t s);
+
+// ---- field.cu
+struct FieldLaunch {
+    const MeshDev* mesh;
+    const double* pts;  // [P][3] device
+    int n_pts;
+    const double* J;  // [S][N][3] complex device
+    int n_rhs;
+    cplx k;
+    cplx mult;
+    NumParamH np;
+    int precision;
+    // incident plane wave (add flags 0/1)
+    double kvec[3], e0[3], h_scale;
+    int add_E, add_H;
+    double* E;  // [S][P][3] complex device
+    double* H;  // may be null
+};
+// Workspace bytes a field call needs before the near-pair count is known
+// (partials, counts, offsets) and the per-near-pair bytes.
+size_t field_ws_base_bytes(const FieldLaunch& f, int* splits_out);
+size_t field_pair_ws_bytes(long long n_near);
+// Stage 1: far kernel + near counting + scan; writes total near pairs to
+// *d_total (device). Stage 2 (after the host knows the total): near fill,
+// near pair kernel, finalize.
+cudaError_t field_stage1(const FieldLaunch& f, void* ws, int splits, long long* d_total, cudaStream_t s,
+                         int* launches, cudaEvent_t far_begin, cudaEvent_t far_end, int* far_launches);
+cudaError_t field_stage2(const FieldLaunch& f, void* ws, int splits, long long n_near, void* pair_ws,
+                         unsigned long long* d_nonfinite, cudaStream_t s, int* launches);
+
+// ---- pairops.cu
+cudaError_t launch_pair_op(int op, int nv, int n, const double* cells, const double* x, const double* j, cplx k,
+                           NumParamH np, double* res, cudaStream_t s);
+struct KParamDev {
+    double smoothR, smoothRMin, k_re, k_im;
+    double current[3][2];
+    double vec_dbl[3];
+    double n[3];
+};
+cudaError_t launch_integral_pnt(int integrand, int nv, int n, const double* cells, const double* x,
+                                const KParamDev* kp, int n_start, int p_max, double eps, double* res, cudaStream_t s);
+cudaError_t launch_integral_seg(int integrand, int n, const double* a, const double* b, const double* x,
+                                const KParamDev* kp, int n_start, int p_max, double eps, double* res, cudaStream_t s);
+cudaError_t launch_k0(int integrand, int common, int nv, int n, const double* cells, const double* x, const double* j,
+                      const KParamDev* kp, int n_seg, int p_seg, double eps, double* res, cudaStream_t s);
+cudaError_t launch_analytic(int which, int nv, int n, const double* cells_or_a, const double* b, const double* x,
+                            double analytic_r, int n_start, int p_max, double eps, cplx k, double* res, cudaStream_t s);
+
+// ---- assemble.cu
+struct AssembleLaunch {
+    const MeshDev* mesh;
+    cplx k;
+    NumParamH np;
+    int layout;     // 0 tau2, 1 full3
+    int out_c64;    // complex64 storage
+    int precision;  // fp64 / mixed far entries
+    void* A;        // device
+};
+size_t assemble_ws_base_bytes(const AssembleLaunch& a);
+cudaError_t assemble_stage1(const AssembleLaunch& a, void* ws, long long* d_total, cudaStream_t s);
+cudaError_t assemble_stage2(const AssembleLaunch& a, void* ws, long long n_near, void* pair_ws, cudaStream_t s);
+
+}  // namespace bielcc_gpu

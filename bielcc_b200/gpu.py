@@ -1,0 +1,285 @@
+"""Python binding of libbielcc_gpu.so (include/bielcc_gpu.h) via ctypes.
+
+There is no CPU fallback: if the library is missing or no CUDA device is
+visible, constructing a Context raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libbielcc_gpu.so")
+
+_lib = None
+
+
+class BielccError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"bielcc error {code}: {msg}")
+        self.code = code
+
+
+def load(path=LIB_PATH):
+    """Loads the CUDA library (building it first when absent and nvcc exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        from . import build as _b
+
+        _b.build()
+    L = C.CDLL(path)
+    dp, vp, ip = C.POINTER(C.c_double), C.c_void_p, C.POINTER(C.c_int32)
+
+    def d(name, args, res=C.c_int):
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+
+    d("bielcc_abi_version", [])
+    d("bielcc_last_error", [], C.c_char_p)
+    d("bielcc_numparam_default", [C.POINTER(abi.NumParam)], None)
+    d("bielcc_ctx_create", [C.c_int, C.POINTER(vp)])
+    d("bielcc_ctx_destroy", [vp])
+    d("bielcc_ctx_synchronize", [vp])
+    d("bielcc_ctx_mem_used", [vp, C.POINTER(C.c_int64)])
+    d("bielcc_mesh_create", [vp, C.c_int, C.c_int, dp, ip])
+    d("bielcc_mesh_destroy", [vp, C.c_int32])
+    field_args = [vp, C.c_int32, C.c_int, dp, C.c_double, C.c_double, C.c_double, C.c_double,
+                  C.POINTER(abi.PlaneWave), C.POINTER(abi.NumParam), C.c_int, dp, dp, dp, C.c_int]
+    d("bielcc_field_EH", field_args + [C.POINTER(abi.Report)])
+    d("bielcc_field_EH_device", [vp, C.c_int32, C.c_int, vp, C.c_double, C.c_double, C.c_double, C.c_double,
+                                 C.POINTER(abi.PlaneWave), C.POINTER(abi.NumParam), C.c_int, vp, vp, vp, C.c_int, vp,
+                                 C.POINTER(abi.Report)])
+    d("bielcc_integrand_info", [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)])
+    d("bielcc_assemble_K", [vp, C.c_int32, C.c_double, C.c_double, C.POINTER(abi.NumParam), C.c_int, C.c_int, C.c_int,
+                            vp, C.POINTER(abi.Report)])
+    d("bielcc_assemble_K_device", [vp, C.c_int32, C.c_double, C.c_double, C.POINTER(abi.NumParam), C.c_int, C.c_int,
+                                   C.c_int, vp, vp, C.POINTER(abi.Report)])
+    d("bielcc_ctx_set_timing", [vp, C.c_int])
+    d("bielcc_measure_fma_peak", [C.c_int, C.POINTER(C.c_double)])
+    d("bielcc_ctx_stats", [vp, C.POINTER(abi.Stats), C.c_int])
+    abi.declare_common(L, "bielcc_")
+    if L.bielcc_abi_version() != abi.ABI_VERSION:
+        raise RuntimeError(f"{path}: ABI {L.bielcc_abi_version()} != {abi.ABI_VERSION}")
+    _lib = L
+    return L
+
+
+def _check(rc):
+    if rc != 0:
+        raise BielccError(rc, _lib.bielcc_last_error().decode(errors="replace"))
+    return rc
+
+
+def _c(a, dtype=np.float64):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+PREC = {"fp64": abi.PREC_FP64, "mixed": abi.PREC_MIXED}
+
+
+class Mesh:
+    def __init__(self, ctx, cells):
+        self.ctx = ctx
+        self.cells = _c(cells)
+        if self.cells.ndim != 3 or self.cells.shape[1] not in (3, 4) or self.cells.shape[2] != 3:
+            raise ValueError("cells must be [N][3|4][3]")
+        h = C.c_int32(0)
+        _check(_lib.bielcc_mesh_create(ctx.h, self.cells.shape[1], self.cells.shape[0], abi.dptr(self.cells),
+                                       C.byref(h)))
+        self.id = h.value
+        self.n_cells = self.cells.shape[0]
+        self.n_vert = self.cells.shape[1]
+
+    def close(self):
+        if self.id:
+            _check(_lib.bielcc_mesh_destroy(self.ctx.h, self.id))
+            self.id = 0
+
+
+class Context:
+    """One CUDA device, its stream and the resident meshes (bielcc_ctx)."""
+
+    def __init__(self, device=0):
+        load()
+        h = C.c_void_p()
+        _check(_lib.bielcc_ctx_create(int(device), C.byref(h)))
+        self.h = h
+        self.device = device
+
+    def close(self):
+        if self.h:
+            _lib.bielcc_ctx_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def synchronize(self):
+        _check(_lib.bielcc_ctx_synchronize(self.h))
+
+    def mem_used(self):
+        b = C.c_int64(0)
+        _check(_lib.bielcc_ctx_mem_used(self.h, C.byref(b)))
+        return b.value
+
+    def set_timing(self, on=True):
+        _check(_lib.bielcc_ctx_set_timing(self.h, int(bool(on))))
+
+    def stats(self, reset=False):
+        st = abi.Stats()
+        _check(_lib.bielcc_ctx_stats(self.h, C.byref(st), int(bool(reset))))
+        return {f: getattr(st, f) for f, _ in abi.Stats._fields_}
+
+    def mesh(self, cells):
+        return Mesh(self, cells)
+
+    def measure_fma_peak(self, fp64=False):
+        """FP32 / FP64 CUDA-core FMA peak of this device in TFLOP/s."""
+        t = C.c_double(0)
+        _check(_lib.bielcc_measure_fma_peak(int(bool(fp64)), C.byref(t)))
+        return t.value
+
+    # ------------------------------------------------------------------ field
+    def field_EH(self, mesh, J, k, pts, numparam=None, mult=1.0, inc=None, with_H=True, precision="fp64",
+                 check=True, out=None):
+        """E, H [S][M][3] complex128 and the report; J [S][N][3] or [N][3].
+        `out` = (E, H) preallocated C-contiguous complex128 arrays (e.g. pinned)."""
+        J = _c(J, np.complex128)
+        if J.ndim == 2:
+            J = J[None]
+        pts = _c(pts)
+        S, M = J.shape[0], pts.shape[0]
+        if J.shape[1] != mesh.n_cells:
+            raise ValueError("J has %d cells, mesh %d" % (J.shape[1], mesh.n_cells))
+        if out is not None:
+            E, H = out
+            assert E.shape == (S, M, 3) and E.dtype == np.complex128 and E.flags.c_contiguous
+            assert H is None or (H.shape == (S, M, 3) and H.dtype == np.complex128 and H.flags.c_contiguous)
+        else:
+            E = np.zeros((S, M, 3), np.complex128)
+            H = np.zeros((S, M, 3), np.complex128) if with_H else None
+        rep = abi.Report()
+        np_ = numparam if numparam is not None else abi.NumParam.default()
+        k = complex(k)
+        mult = complex(mult)
+        rc = _lib.bielcc_field_EH(self.h, mesh.id, S, abi.dptr(J), k.real, k.imag, mult.real, mult.imag,
+                                  C.byref(inc) if inc is not None else None, C.byref(np_), M, abi.dptr(pts),
+                                  abi.dptr(E), abi.dptr(H), PREC[precision], C.byref(rep))
+        if rc != 0 and (check or rc != abi.ERR_NAN):
+            _check(rc)
+        return E, H, rep
+
+    def field_EH_device(self, mesh, J_dev, k, pts_dev, E_dev, H_dev, n_rhs, n_pts, numparam=None, mult=1.0,
+                        inc=None, precision="fp64", stream=None):
+        """Device-buffer form: pointers are ints (e.g. torch tensor data_ptr())."""
+        rep = abi.Report()
+        np_ = numparam if numparam is not None else abi.NumParam.default()
+        k = complex(k)
+        mult = complex(mult)
+        _check(_lib.bielcc_field_EH_device(self.h, mesh.id, n_rhs, C.c_void_p(J_dev), k.real, k.imag, mult.real,
+                                           mult.imag, C.byref(inc) if inc is not None else None, C.byref(np_),
+                                           n_pts, C.c_void_p(pts_dev), C.c_void_p(E_dev),
+                                           C.c_void_p(H_dev) if H_dev else None, PREC[precision],
+                                           C.c_void_p(stream) if stream else None, C.byref(rep)))
+        return rep
+
+    # ------------------------------------------------------------------ per-pair operators
+    def pair_op(self, op, cells, x, j, k, numparam=None):
+        cells, x = _c(cells), _c(x)
+        j = _c(j, np.complex128)
+        n = cells.shape[0]
+        res = np.zeros((n, 3), np.complex128)
+        np_ = numparam if numparam is not None else abi.NumParam.default()
+        k = complex(k)
+        _check(_lib.bielcc_pair_op(self.h, op, cells.shape[1], n, abi.dptr(cells), abi.dptr(x), abi.dptr(j), k.real,
+                                   k.imag, C.byref(np_), abi.dptr(res)))
+        return res
+
+    def integral_pnt(self, integrand, cells, x, kp, n_start, p_max, eps):
+        cells, x = _c(cells), _c(x)
+        n = cells.shape[0]
+        _, idim, cplx = abi.INTEGRANDS[integrand]
+        res = np.zeros((n, idim), np.complex128 if cplx else np.float64)
+        _check(_lib.bielcc_integral_pnt(self.h, integrand, cells.shape[1], n, abi.dptr(cells), abi.dptr(x), kp,
+                                        n_start, p_max, eps, abi.dptr(res)))
+        return res
+
+    def integral_seg_pnt(self, integrand, a, b, x, kp, n_start, p_max, eps):
+        a, b, x = _c(a), _c(b), _c(x)
+        n = a.shape[0]
+        _, idim, cplx = abi.INTEGRANDS[integrand]
+        res = np.zeros((n, idim), np.complex128 if cplx else np.float64)
+        _check(_lib.bielcc_integral_seg_pnt(self.h, integrand, n, abi.dptr(a), abi.dptr(b), abi.dptr(x), kp, n_start,
+                                            p_max, eps, abi.dptr(res)))
+        return res
+
+    def k0(self, integrand, common, cells, x, j, kp, n_seg, p_seg, eps):
+        cells, x = _c(cells), _c(x)
+        j = _c(j, np.complex128)
+        n = cells.shape[0]
+        res = np.zeros((n, 3), np.complex128)
+        _check(_lib.bielcc_k0(self.h, integrand, int(common), cells.shape[1], n, abi.dptr(cells), abi.dptr(x),
+                              abi.dptr(j), kp, n_seg, p_seg, eps, abi.dptr(res)))
+        return res
+
+    def integral_1divr(self, cells, x):
+        cells, x = _c(cells), _c(x)
+        res = np.zeros(cells.shape[0])
+        _check(_lib.bielcc_integral_1divr(self.h, cells.shape[1], cells.shape[0], abi.dptr(cells), abi.dptr(x),
+                                          abi.dptr(res)))
+        return res
+
+    def integral_grad1divr_seg(self, a, b, x):
+        a, b, x = _c(a), _c(b), _c(x)
+        res = np.zeros((a.shape[0], 3))
+        _check(_lib.bielcc_integral_grad1divr_seg(self.h, a.shape[0], abi.dptr(a), abi.dptr(b), abi.dptr(x),
+                                                  abi.dptr(res)))
+        return res
+
+    def integral_surf_simplepot_h_hs(self, cells, x, analytic_r, n_start, p_max, eps, k):
+        cells, x = _c(cells), _c(x)
+        res = np.zeros(cells.shape[0], np.complex128)
+        k = complex(k)
+        _check(_lib.bielcc_integral_surf_simplepot_h_hs(self.h, cells.shape[1], cells.shape[0], abi.dptr(cells),
+                                                        abi.dptr(x), analytic_r, n_start, p_max, eps, k.real, k.imag,
+                                                        abi.dptr(res)))
+        return res
+
+    def integral_seg_gradsimplepot_h_hs(self, a, b, x, analytic_r, n_start, p_max, eps, k):
+        a, b, x = _c(a), _c(b), _c(x)
+        res = np.zeros((a.shape[0], 3), np.complex128)
+        k = complex(k)
+        _check(_lib.bielcc_integral_seg_gradsimplepot_h_hs(self.h, a.shape[0], abi.dptr(a), abi.dptr(b), abi.dptr(x),
+                                                           analytic_r, n_start, p_max, eps, k.real, k.imag,
+                                                           abi.dptr(res)))
+        return res
+
+    # ------------------------------------------------------------------ assembly
+    def assemble_K(self, mesh, k, numparam=None, layout=abi.LAYOUT_TAU2, c64=False, precision="fp64"):
+        m = 2 if layout == abi.LAYOUT_TAU2 else 3
+        dim = m * mesh.n_cells
+        A = np.zeros((dim, dim), np.complex64 if c64 else np.complex128)
+        rep = abi.Report()
+        np_ = numparam if numparam is not None else abi.NumParam.default()
+        k = complex(k)
+        _check(_lib.bielcc_assemble_K(self.h, mesh.id, k.real, k.imag, C.byref(np_), layout, int(c64),
+                                      PREC[precision], A.ctypes.data_as(C.c_void_p), C.byref(rep)))
+        return A, rep
+
+    def assemble_K_device(self, mesh, k, A_dev, numparam=None, layout=abi.LAYOUT_TAU2, c64=True, precision="mixed",
+                          stream=None):
+        rep = abi.Report()
+        np_ = numparam if numparam is not None else abi.NumParam.default()
+        k = complex(k)
+        _check(_lib.bielcc_assemble_K_device(self.h, mesh.id, k.real, k.imag, C.byref(np_), layout, int(c64),
+                                             PREC[precision], C.c_void_p(A_dev), C.c_void_p(stream) if stream else None,
+                                             C.byref(rep)))
+        return rep

@@ -1,0 +1,292 @@
+/*
+ * bielcc_gpu.h — C ABI of the B200 (sm_100a) implementation of BIELcc's
+ * Stratton-Chu hot path: the K, K0 and R operators, the cell/segment midpoint
+ * quadrature of the kernel_lib integrands, the analytic singular integrals,
+ * E/H field evaluation over every observation-point x cell pair
+ * (GetFieldE_Ideal and its H counterpart) and collocation-matrix assembly.
+ *
+ * Conventions (every entry point):
+ *   - plain C types only; complex numbers are interleaved (re, im) doubles,
+ *     i.e. the memory layout of std::complex<double>;
+ *   - cells are `double[n_cells][n_vert][3]` with n_vert = 4 (CellQuad) or
+ *     3 (CellTriangle), the layout of CellType::GetCellCoords();
+ *   - return value: BIELCC_OK (0) or a negative BIELCC_ERR_* code; the
+ *     message of the last failure on the calling thread is returned by
+ *     bielcc_last_error(); no C++ exception crosses this boundary;
+ *   - a context owns one CUDA device, one stream and the resident meshes;
+ *     calls on one context are serialised by an internal mutex.
+ *
+ * Reference interfaces each entry point replaces are cited as
+ * path:line inside AlenaSetukha/BIELcc.
+ */
+#ifndef BIELCC_GPU_H_
+#define BIELCC_GPU_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Exported with default visibility even when the library is built with
+ * -fvisibility=hidden. */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#define BIELCC_ABI_VERSION 1
+
+/* ---- status codes ---------------------------------------------------- */
+#define BIELCC_OK                 0
+#define BIELCC_ERR_ARG           -1  /* bad argument (null pointer, size, enum) */
+#define BIELCC_ERR_CUDA          -2  /* a CUDA runtime call failed */
+#define BIELCC_ERR_OOM           -3  /* device allocation failed / over budget */
+#define BIELCC_ERR_NAN           -4  /* result written, but holds NaN/Inf */
+#define BIELCC_ERR_TIMEOUT       -5  /* a bounded device wait gave up */
+#define BIELCC_ERR_UNSUPPORTED   -6  /* valid input outside what the GPU path covers */
+#define BIELCC_ERR_NOT_FOUND     -7  /* unknown mesh / request handle */
+#define BIELCC_ERR_BUSY          -8  /* admission refused (serving queue full) */
+
+/* ---- numerical parameters -------------------------------------------- */
+/* Mirrors NumParam (electrodynamics/num_param.h:28-55); defaults are the
+ * library's Calculation_Constants (electrodynamics/constants.h:17-27):
+ * eps=1e-6, rs=2, rs_seg=2, analytic_calc=3, n_start=8, n_start_seg=10,
+ * p_max=1, p_max_seg=1. */
+typedef struct bielcc_numparam {
+    double eps;            /* integral accuracy; also smoothRMin of K near  */
+    double rs;             /* surface smoothing radius, relative to diam/n_start */
+    double rs_seg;         /* segment smoothing radius, relative to diam/n_start_seg */
+    double analytic_calc;  /* near-zone radius, relative to cell diameter */
+    int32_t n_start;       /* initial n of the n x n cell split */
+    int32_t n_start_seg;   /* initial segment split */
+    int32_t p_max;         /* refinement levels of the cell quadrature */
+    int32_t p_max_seg;     /* refinement levels of the segment quadrature */
+} bielcc_numparam;
+
+/* Fills *np with the Calculation_Constants defaults. */
+void bielcc_numparam_default(bielcc_numparam* np);
+
+/* Plane-wave incident field, restating PlaneWaveFieldE / PlaneWaveFieldH
+ * (electrodynamics/incident_field.h:20-59):
+ *   E_inc(x) = e0 exp(i k_vec.x),  H_inc(x) = h_scale (k_vec x e0) exp(i k_vec.x).
+ * add_E / add_H select whether the incident field is added to the output. */
+typedef struct bielcc_planewave {
+    double k_vec[3];
+    double e0[3];
+    double h_scale;
+    int32_t add_E;
+    int32_t add_H;
+} bielcc_planewave;
+
+/* Integrand parameters: the fields of KernelParam<KType>
+ * (integrators/kernel_param.h:25-57) that the kernel_lib integrands read. */
+typedef struct bielcc_kernelparam {
+    double smoothR;
+    double smoothRMin;
+    double k_re, k_im;
+    double current[3][2];  /* KernelParam::current (complex) */
+    double vec_dbl[3];     /* KernelParam::vec_dbl */
+    double n[3];           /* KernelParam::n */
+} bielcc_kernelparam;
+
+/* Precision of the field / assembly path. */
+#define BIELCC_PREC_FP64   0  /* complex FP64 everywhere (parity form) */
+#define BIELCC_PREC_MIXED  1  /* complex FP32 far cells, FP64 near / singular cells */
+
+/* Result report of a field / assembly call. */
+typedef struct bielcc_report {
+    int64_t n_pairs;        /* point x cell pairs evaluated (per RHS) */
+    int64_t n_near_pairs;   /* pairs that took the FP64 near path */
+    int64_t n_nonfinite;    /* non-finite output components */
+    double  est_rel_l2;     /* mixed: rel-L2 vs FP64 on a point sample; FP64: 0 */
+    int32_t est_sample;     /* points in that sample */
+    int32_t status;         /* same as the return value */
+} bielcc_report;
+
+typedef struct bielcc_ctx_s* bielcc_ctx;
+typedef int32_t bielcc_mesh;
+
+/* ---- context ----------------------------------------------------------- */
+int bielcc_abi_version(void);
+const char* bielcc_last_error(void);
+int bielcc_ctx_create(int device, bielcc_ctx* out);
+int bielcc_ctx_destroy(bielcc_ctx ctx);
+int bielcc_ctx_synchronize(bielcc_ctx ctx);
+/* Device bytes currently held by the context (meshes + workspaces). */
+int bielcc_ctx_mem_used(bielcc_ctx ctx, int64_t* bytes);
+
+/* Counters of the kernels a context enqueued. With timing on, the far-field
+ * kernels of each field call are bracketed by CUDA events on the stream they
+ * run on and their elapsed time accumulates in far_ms (read back at the call's
+ * own synchronisation point). No counterpart in the reference (it has no
+ * device code); used by bench.py for the roofline figures. */
+typedef struct bielcc_stats {
+    int64_t kernel_launches;  /* all kernels enqueued by this context */
+    int64_t far_launches;     /* far-field kernel launches */
+    int64_t far_pairs;        /* far (point, cell, RHS) pairs those launches evaluated */
+    double  far_ms;           /* summed CUDA-event time of the far-field kernels */
+} bielcc_stats;
+int bielcc_ctx_set_timing(bielcc_ctx ctx, int on);
+int bielcc_ctx_stats(bielcc_ctx ctx, bielcc_stats* out, int reset);
+
+/* Measured FMA throughput (TFLOP/s, 2 flops per FMA) of the current device's
+ * FP32 (fp64 = 0) or FP64 (fp64 = 1) CUDA-core pipes: the roofline
+ * denominator of the field kernels. No counterpart in the reference. */
+int bielcc_measure_fma_peak(int fp64, double* tflops);
+
+/* ---- resident meshes -------------------------------------------------- */
+/* Uploads cells and precomputes per-cell geometry on the device: centre
+ * (get_center_mass, geometry/element_geom.cpp:320-342), diameter (get_diam,
+ * element_geom.cpp:275-317), normal (norm_func, element_geom.cpp:130-156),
+ * tangent basis tau1/tau2 (CellQuad/CellTriangle::CellFill, mesh/cell.cpp:8-51,
+ * 60-99). Replaces SurfMesh<CellType> (mesh/surf_mesh.h:47-302) as the input of
+ * the field driver; mesh parsing stays with the caller. */
+int bielcc_mesh_create(bielcc_ctx ctx, int n_vert, int n_cells, const double* cells,
+                       bielcc_mesh* out);
+int bielcc_mesh_destroy(bielcc_ctx ctx, bielcc_mesh mesh);
+
+/* ---- field evaluation ------------------------------------------------- */
+/* E(x_i) = mult * sum_j K[cell_j, J_j](x_i) + E_inc(x_i)
+ * H(x_i) =        sum_j R[cell_j, J_j](x_i) + H_inc(x_i)
+ * with the near/far split of GetFieldE_Ideal (electrodynamics/get_field.h:35-78):
+ * near iff |x - centre_j| < analytic_calc * diam_j; near K = K_RotRot_Near_Smooth
+ * (electrodynamics/K.h:47-79), far K = K_RotRot_Far (K.h:288-301); near R =
+ * R_Rot_Smooth (electrodynamics/R.h:46-61), far R = R_Rot_Colloc (R.h:89-111),
+ * the operator pairing of examples/field/main0_field_test.cpp:237-311.
+ *   J : [n_rhs][n_cells][3] complex   (the j_E argument, one set per RHS)
+ *   pts: [n_pts][3]                    (the points argument)
+ *   E, H: [n_rhs][n_pts][3] complex    (field_E and its H counterpart; H may be NULL)
+ * Host buffers; the copies are part of the call. */
+int bielcc_field_EH(bielcc_ctx ctx, bielcc_mesh mesh, int n_rhs, const double* J,
+                    double k_re, double k_im, double mult_re, double mult_im,
+                    const bielcc_planewave* inc, const bielcc_numparam* np,
+                    int n_pts, const double* pts, double* E, double* H,
+                    int precision, bielcc_report* report);
+
+/* Same computation on device buffers, enqueued on `stream` (a cudaStream_t,
+ * NULL = the context's stream); returns once enqueued. The report's
+ * n_nonfinite / est_rel_l2 are not filled (no host synchronisation). */
+int bielcc_field_EH_device(bielcc_ctx ctx, bielcc_mesh mesh, int n_rhs, const double* J_dev,
+                           double k_re, double k_im, double mult_re, double mult_im,
+                           const bielcc_planewave* inc, const bielcc_numparam* np,
+                           int n_pts, const double* pts_dev, double* E_dev, double* H_dev,
+                           int precision, void* stream, bielcc_report* report);
+
+/* ---- per-pair operators ----------------------------------------------- */
+/* One operator applied to n_pairs independent (cell, x, j) triples, each as
+ * the reference call op(j, x, cell, num_param, k, res):
+ *   cells: [n_pairs][n_vert][3], x: [n_pairs][3], j: [n_pairs][3] complex,
+ *   res:   [n_pairs][3] complex. Host buffers. */
+#define BIELCC_OP_K_NEAR_SMOOTH   0  /* K_RotRot_Near_Smooth  electrodynamics/K.h:47-79   */
+#define BIELCC_OP_K_HS            1  /* K_RotRot_HS           electrodynamics/K.h:119-145 */
+#define BIELCC_OP_K_HS_COLLOC     2  /* K_RotRot_HS_Colloc    electrodynamics/K.h:179-204 */
+#define BIELCC_OP_K_HS2_COLLOC    3  /* K_RotRot_HS2_Colloc   electrodynamics/K.h:230-252 */
+#define BIELCC_OP_K_FAR           4  /* K_RotRot_Far          electrodynamics/K.h:288-301 */
+#define BIELCC_OP_R_SMOOTH        5  /* R_Rot_Smooth          electrodynamics/R.h:46-61   */
+#define BIELCC_OP_R_COLLOC        6  /* R_Rot_Colloc          electrodynamics/R.h:89-111  */
+#define BIELCC_OP_R_NEAR          7  /* R_Rot_Near            electrodynamics/R.h:140-175 */
+#define BIELCC_OP_COUNT           8
+int bielcc_pair_op(bielcc_ctx ctx, int op, int n_vert, int n_pairs, const double* cells,
+                   const double* x, const double* j, double k_re, double k_im,
+                   const bielcc_numparam* np, double* res);
+
+/* ---- kernel_lib integrands under the universal quadratures ------------ */
+/* Integrand ids (electrodynamics/kernel_lib.h). Real-valued ones write
+ * doubles, complex ones interleaved complex. */
+#define BIELCC_F_SIMPLEPOT_L        0  /* F_SimplePot_L        kernel_lib.h:62-69   idim 1 real */
+#define BIELCC_F_GRADSIMPLEPOT_L    1  /* F_GradSimplePot_L    kernel_lib.h:87-98   idim 3 real */
+#define BIELCC_F_DOUBLEPOT_L        2  /* F_DoublePot_L        kernel_lib.h:117-129 idim 1 real */
+#define BIELCC_F_VECTORPOT_L        3  /* F_VectorPot_L        kernel_lib.h:149-177 idim 3 real */
+#define BIELCC_F_SIMPLEPOT_H        4  /* F_SimplePot_H        kernel_lib.h:209-217 idim 1 cplx */
+#define BIELCC_F_NU_SIMPLEPOT_H     5  /* nuF_SimplePot_H      kernel_lib.h:235-245 idim 3 cplx */
+#define BIELCC_F_SIMPLEPOT_HM1      6  /* F_SimplePot_Hm1      kernel_lib.h:262-278 idim 1 cplx */
+#define BIELCC_F_GRADSIMPLEPOT_H    7  /* F_GradSimplePot_H    kernel_lib.h:295-313 idim 3 cplx */
+#define BIELCC_F_GRADSIMPLEPOT_HM1  8  /* F_GradSimplePot_Hm1  kernel_lib.h:332-356 idim 3 cplx */
+#define BIELCC_F_DOUBLEPOT_H        9  /* F_DoublePot_H        kernel_lib.h:375-390 idim 1 cplx */
+#define BIELCC_F_N_DOUBLEPOT_H     10  /* nF_DoublePot_H       kernel_lib.h:409-419 idim 3 cplx */
+#define BIELCC_F_ROTROTSIMPLEPOT_H 11  /* F_RotRotSimplePot_H  kernel_lib.h:453-492 idim 3 cplx */
+#define BIELCC_F_ONE               12  /* F(x) = 1: IntegralUniversal area check   idim 1 real */
+#define BIELCC_F_COUNT             13
+
+/* Returns the value dimension (1 or 3) and whether it is complex. */
+int bielcc_integrand_info(int integrand, int* idim, int* is_complex);
+
+/* IntegralUniversalPnt (integrators/integral_universal.h:38-120 quad,
+ * :136-220 triangle) of one integrand over n_pairs (cell, x) pairs with the
+ * adaptive n -> 2n refinement and smoothing-radius halving of the reference.
+ * kp is per pair ([n_pairs]) so each pair has its own smoothR / current / n;
+ * its smoothR on return is NOT updated (the reference mutates it).
+ * res: [n_pairs][idim] (complex interleaved when the integrand is complex). */
+int bielcc_integral_pnt(bielcc_ctx ctx, int integrand, int n_vert, int n_pairs,
+                        const double* cells, const double* x,
+                        const bielcc_kernelparam* kp, int n_start, int p_max,
+                        double eps, double* res);
+
+/* IntegralUniversalSegPnt (integrators/integral_universal_seg.h:38-98):
+ * a, b, x: [n_pairs][3]. */
+int bielcc_integral_seg_pnt(bielcc_ctx ctx, int integrand, int n_pairs,
+                            const double* a, const double* b, const double* x,
+                            const bielcc_kernelparam* kp, int n_start, int p_max,
+                            double eps, double* res);
+
+/* K0 / K0_Common (electrodynamics/K0.h:36-86 / :112-166): contour integral
+ * of one integrand over the cell edges. common = 0: -sum_e (j.nu_e) int_e F;
+ * common = 1: sum_e int_e F nu_e (vec_dbl set to nu_e per edge). The
+ * kernel-parameter record is shared by the edges of a pair exactly as in the
+ * reference (its smoothR shrinks from edge to edge). */
+int bielcc_k0(bielcc_ctx ctx, int integrand, int common, int n_vert, int n_pairs,
+              const double* cells, const double* x, const double* j,
+              const bielcc_kernelparam* kp, int n_start_seg, int p_max_seg,
+              double eps, double* res);
+
+/* ---- analytic singular integrals -------------------------------------- */
+/* integral1Divr (integrators/integrals_analytic.cpp:218-235): exact
+ * integral of 1/|x-y| over a triangle, a quad = triangles (0,1,2)+(2,3,0). */
+int bielcc_integral_1divr(bielcc_ctx ctx, int n_vert, int n_pairs, const double* cells,
+                          const double* x, double* res);
+/* integralGrad1DivrSeg (integrals_analytic.cpp:240-257): closed-form
+ * integral over [A,B] of grad_x 1/|x-y|; res: [n_pairs][3]. */
+int bielcc_integral_grad1divr_seg(bielcc_ctx ctx, int n_pairs, const double* a,
+                                  const double* b, const double* x, double* res);
+/* IntegralSurf_SimplePot_H_HS (integrators/integrals_analytic.h:136-164):
+ * res [n_pairs] complex. */
+int bielcc_integral_surf_simplepot_h_hs(bielcc_ctx ctx, int n_vert, int n_pairs,
+                                        const double* cells, const double* x,
+                                        double analytic_r, int n_start, int p_max,
+                                        double eps, double k_re, double k_im, double* res);
+/* IntegralSeg_GradSimplePot_H_HS (integrals_analytic.h:193-221):
+ * res [n_pairs][3] complex. */
+int bielcc_integral_seg_gradsimplepot_h_hs(bielcc_ctx ctx, int n_pairs, const double* a,
+                                           const double* b, const double* x,
+                                           double analytic_r, int n_start, int p_max,
+                                           double eps, double k_re, double k_im, double* res);
+
+/* ---- collocation-matrix assembly -------------------------------------- */
+/* A[(i,a),(j,b)] = tau_a(i) . K[cell_j, tau_b(j)](c_i), c_i = centre of cell i
+ * (collocation points as SurfMesh::FormCollocPoints, mesh/surf_mesh.h:688-700),
+ * tau from CellFill (mesh/cell.cpp). Near (|c_i - c_j| < analytic_calc*diam_j)
+ * entries use K_RotRot_HS_Colloc (electrodynamics/K.h:179-204) in FP64, far
+ * entries K_RotRot_Far (K.h:288-301). The reference has no assembly loop,
+ * only the operator "for matrix assembly" (examples/ED_Operators/main0_K.cpp:60-69).
+ * layout BIELCC_LAYOUT_TAU2: A is (2N x 2N) row-major, row 2i+a, column 2j+b;
+ * layout BIELCC_LAYOUT_FULL3: A is (3N x 3N), the 3x3 block K_ij (x, y, z).
+ * out_c64 = 1: complex64 storage, 0: complex128. */
+#define BIELCC_LAYOUT_TAU2  0
+#define BIELCC_LAYOUT_FULL3 1
+int bielcc_assemble_K(bielcc_ctx ctx, bielcc_mesh mesh, double k_re, double k_im,
+                      const bielcc_numparam* np, int layout, int out_c64, int precision,
+                      void* A_host, bielcc_report* report);
+int bielcc_assemble_K_device(bielcc_ctx ctx, bielcc_mesh mesh, double k_re, double k_im,
+                             const bielcc_numparam* np, int layout, int out_c64,
+                             int precision, void* A_dev, void* stream,
+                             bielcc_report* report);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+#endif  /* BIELCC_GPU_H_ */

@@ -1,0 +1,145 @@
+"""GPU field path (GetFieldE_Ideal + H) through the C ABI against the
+reference's golden outputs and the oracle: FP64 within 1e-12 relative L2,
+mixed within 1e-6."""
+import numpy as np
+import pytest
+
+import oracle
+from bielcc_b200 import abi
+from bielcc_b200 import workloads as W
+from conftest import TOL_FP64, TOL_MIXED, golden, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _inc(g):
+    return abi.PlaneWave.make(g["kvec"], g["e0"], float(g["h_scale"]), True, True)
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", TOL_FP64), ("mixed", TOL_MIXED)])
+def test_golden_quad512(gctx, precision, tol):
+    g = golden("field_quad512.npz")
+    m = gctx.mesh(g["cells"])
+    E, H, rep = gctx.field_EH(m, g["J"], float(g["k"]), g["pts"], inc=_inc(g), precision=precision)
+    assert rel_l2(E, g["E"]) < tol
+    assert rel_l2(H, g["H"]) < tol
+    assert rep.n_near_pairs > 0 and rep.n_nonfinite == 0
+    if precision == "mixed":
+        assert 0 < rep.est_rel_l2 < tol
+    m.close()
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", TOL_FP64), ("mixed", TOL_MIXED)])
+def test_golden_tri80_complex_k_two_rhs(gctx, precision, tol):
+    g = golden("field_tri80.npz")
+    m = gctx.mesh(g["cells"])
+    E, H, _ = gctx.field_EH(m, g["J"], complex(g["k"]), g["pts"], mult=complex(g["mult"]), precision=precision)
+    assert E.shape == g["E"].shape
+    assert rel_l2(E, g["E"]) < tol
+    assert rel_l2(H, g["H"]) < tol
+
+
+def test_sphere512_1000_points_fp64(gctx):
+    c = W.config1()
+    kv, e0, hs = c["inc"]
+    inc = abi.PlaneWave.make(kv, e0, hs, True, True)
+    m = gctx.mesh(c["cells"])
+    E, H, rep = gctx.field_EH(m, c["J"], c["k"], c["pts"], inc=inc)
+    Eo, Ho = oracle.field_EH(c["cells"], c["J"], c["k"], c["pts"], inc=inc)
+    assert rel_l2(E, Eo) < TOL_FP64 and rel_l2(H, Ho) < TOL_FP64
+    assert rep.n_pairs == 512 * 1000 and rep.n_near_pairs == 0
+    Em, Hm, repm = gctx.field_EH(m, c["J"], c["k"], c["pts"], inc=inc, precision="mixed")
+    assert rel_l2(Em, Eo) < TOL_MIXED and rel_l2(Hm, Ho) < TOL_MIXED
+
+
+def test_sphere8192_near_and_far_subset(gctx):
+    c = W.config2()
+    rng = np.random.default_rng(0)
+    idx = np.concatenate([rng.choice(18000, 96, replace=False), 18000 + rng.choice(2000, 32, replace=False)])
+    pts = c["pts"][idx]
+    m = gctx.mesh(c["cells"])
+    E, H, rep = gctx.field_EH(m, c["J"], c["k"], pts)
+    Eo, Ho = oracle.field_EH(c["cells"], c["J"], c["k"], pts)
+    assert rep.n_near_pairs > 0
+    assert rel_l2(E, Eo) < TOL_FP64 and rel_l2(H, Ho) < TOL_FP64
+    Em, Hm, _ = gctx.field_EH(m, c["J"], c["k"], pts, precision="mixed")
+    assert rel_l2(Em, Eo) < TOL_MIXED and rel_l2(Hm, Ho) < TOL_MIXED
+
+
+@pytest.mark.parametrize("n_start,n_seg,p_max", [(4, 5, 1), (10, 12, 1), (20, 10, 1), (4, 6, 2), (3, 4, 3)])
+def test_quadrature_splits_and_adaptive(gctx, n_start, n_seg, p_max):
+    """Node tiles that fill one stage partially (n=4), several cells per stage
+    (n=10), chunked cells (n=20: 400 nodes > one stage) and adaptive refinement."""
+    cells = W.uv_sphere(8, 16)
+    J = W.po_currents(cells, 4.0, directions=3, seed=5)
+    rng = np.random.default_rng(n_start)
+    pts = np.concatenate([W.sphere_points(40, 2.0, n_start), W.near_points(cells, 12, 0.02, 0.3, rng)])
+    npm = abi.NumParam.default(n_start=n_start, n_start_seg=n_seg, p_max=p_max, p_max_seg=p_max)
+    m = gctx.mesh(cells)
+    E, H, _ = gctx.field_EH(m, J, 4.0, pts, numparam=npm)
+    Eo, Ho = oracle.field_EH(cells, J, 4.0, pts, npm)
+    assert rel_l2(E, Eo) < TOL_FP64 and rel_l2(H, Ho) < TOL_FP64
+    if p_max == 1:
+        Em, Hm, _ = gctx.field_EH(m, J, 4.0, pts, numparam=npm, precision="mixed")
+        assert rel_l2(Em, Eo) < TOL_MIXED and rel_l2(Hm, Ho) < TOL_MIXED
+
+
+def test_multi_rhs_chunks_and_large_k(gctx):
+    """7 RHS (chunks of 4 + 2 + 1) and a large k (mixed-form phase beyond 4 rad per cell)."""
+    cells = W.uv_sphere(12, 24)
+    J = W.po_currents(cells, 40.0, directions=7, seed=9)
+    pts = W.sphere_points(64, 2.5, 3)
+    m = gctx.mesh(cells)
+    for k in (2.0, 40.0, complex(6.0, 0.7)):
+        E, H, _ = gctx.field_EH(m, J, k, pts, mult=complex(0.5, 2.0))
+        Eo, Ho = oracle.field_EH(cells, J, k, pts, mult=complex(0.5, 2.0))
+        assert rel_l2(E, Eo) < TOL_FP64 and rel_l2(H, Ho) < TOL_FP64
+        Em, Hm, _ = gctx.field_EH(m, J, k, pts, mult=complex(0.5, 2.0), precision="mixed")
+        assert rel_l2(Em, Eo) < TOL_MIXED and rel_l2(Hm, Ho) < TOL_MIXED
+
+
+def test_edge_cases(gctx):
+    cells = W.uv_sphere(4, 8)
+    J = W.po_currents(cells, 1.0)
+    m = gctx.mesh(cells)
+    # no points
+    E, H, rep = gctx.field_EH(m, J, 1.0, np.zeros((0, 3)))
+    assert E.shape == (1, 0, 3)
+    # one point, one cell mesh
+    one = gctx.mesh(cells[5:6])
+    p = np.array([[3.0, 0.1, -0.2]])
+    E1, H1, _ = gctx.field_EH(one, J[:, 5:6], 1.0, p)
+    Eo, Ho = oracle.field_EH(cells[5:6], J[:, 5:6], 1.0, p)
+    assert rel_l2(E1, Eo) < TOL_FP64 and rel_l2(H1, Ho) < TOL_FP64
+    # a point at a cell centre: R_Rot_Colloc is 0 there, K near path smooths
+    pc = W.centres(cells)[[3]] + 0.0
+    E2, H2, _ = gctx.field_EH(m, J, 1.0, pc * 1.0000001)
+    Eo2, Ho2 = oracle.field_EH(cells, J, 1.0, pc * 1.0000001)
+    assert rel_l2(E2, Eo2) < TOL_FP64 and rel_l2(H2, Ho2) < TOL_FP64
+    # bad arguments fail with a status, not a crash
+    from bielcc_b200.gpu import BielccError
+
+    with pytest.raises(BielccError):
+        gctx.field_EH(m, J[:, :3], 1.0, p)
+    with pytest.raises(BielccError):
+        gctx.field_EH(m, J, 1.0, p, numparam=abi.NumParam.default(n_start=0))
+
+
+def test_device_buffers_through_torch(gctx):
+    """The device-pointer entry point on a torch stream matches the host one."""
+    torch = pytest.importorskip("torch")
+    c = W.config1()
+    m = gctx.mesh(c["cells"])
+    pts = c["pts"][:256]
+    E, H, _ = gctx.field_EH(m, c["J"], c["k"], pts)
+    dev = torch.device("cuda:0")
+    Jd = torch.from_numpy(np.ascontiguousarray(c["J"])).to(dev)
+    Pd = torch.from_numpy(np.ascontiguousarray(pts)).to(dev)
+    Ed = torch.zeros((1, 256, 3), dtype=torch.complex128, device=dev)
+    Hd = torch.zeros_like(Ed)
+    st = torch.cuda.current_stream()
+    gctx.field_EH_device(m, Jd.data_ptr(), c["k"], Pd.data_ptr(), Ed.data_ptr(), Hd.data_ptr(), 1, 256,
+                         stream=st.cuda_stream)
+    torch.cuda.synchronize()
+    assert rel_l2(Ed.cpu().numpy(), E) == 0.0
+    assert rel_l2(Hd.cpu().numpy(), H) == 0.0
