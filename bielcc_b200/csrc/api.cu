@@ -53,7 +53,10 @@ struct DevBuf {
     size_t cap = 0;
     int ensure(size_t bytes) {
         if (bytes <= cap) return BIELCC_OK;
-        if (p) cudaFree(p);
+        if (p) {
+            cudaDeviceSynchronize();  // the old buffer may still be in use on some stream
+            cudaFree(p);
+        }
         p = nullptr;
         cap = 0;
         size_t want = bytes + bytes / 4 + 256;
@@ -368,6 +371,30 @@ int bielcc_mesh_destroy(bielcc_ctx ctx, bielcc_mesh mesh) {
     return BIELCC_OK;
 }
 
+int bielcc_mesh_geometry(bielcc_ctx ctx, bielcc_mesh mesh, double* out) {
+    TRY(enter(ctx));
+    if (!out) return set_error(BIELCC_ERR_ARG, "null output");
+    std::lock_guard<std::mutex> g(ctx->mu);
+    MeshDev* m;
+    TRY(get_mesh(ctx, mesh, &m));
+    std::vector<CellGeo> rows(m->n_cells);
+    TRY_CUDA(cudaMemcpyAsync(rows.data(), m->geo, rows.size() * sizeof(CellGeo), cudaMemcpyDeviceToHost, ctx->stream));
+    TRY_CUDA(cudaStreamSynchronize(ctx->stream));
+    for (int c = 0; c < m->n_cells; c++) {
+        double* o = out + 14 * (size_t)c;
+        const CellGeo& r = rows[c];
+        for (int g2 = 0; g2 < 3; g2++) {
+            o[g2] = r.c[g2];
+            o[4 + g2] = r.n[g2];
+            o[7 + g2] = r.t1[g2];
+            o[10 + g2] = r.t2[g2];
+        }
+        o[3] = r.diam;
+        o[13] = r.area;
+    }
+    return BIELCC_OK;
+}
+
 int bielcc_field_EH_device(bielcc_ctx ctx, bielcc_mesh mesh, int n_rhs, const double* J_dev, double k_re, double k_im,
                            double mult_re, double mult_im, const bielcc_planewave* inc, const bielcc_numparam* np,
                            int n_pts, const double* pts_dev, double* E_dev, double* H_dev, int precision, void* stream,
@@ -490,9 +517,11 @@ namespace {
 
 // Host-buffer batch helper: copies `ins` to the device, runs `launch` with
 // their device pointers, copies `out_bytes` back into `out`.
+// `back` (optional): input index whose device copy is written back to
+// `back_host` after the launch (in/out records such as kernel parameters).
 template <typename L>
 int run_batch(bielcc_ctx ctx, std::initializer_list<std::pair<const void*, size_t>> ins, void* out, size_t out_bytes,
-              L launch) {
+              L launch, int back = -1, void* back_host = nullptr) {
     auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
     size_t tot = al(out_bytes);
     for (auto& in : ins) tot += al(in.second);
@@ -508,6 +537,10 @@ int run_batch(bielcc_ctx ctx, std::initializer_list<std::pair<const void*, size_
     }
     TRY_CUDA(launch(dptrs, (void*)p, s));
     if (out_bytes) TRY_CUDA(cudaMemcpyAsync(out, p, out_bytes, cudaMemcpyDeviceToHost, s));
+    if (back >= 0 && back_host) {
+        size_t b = (ins.begin() + back)->second;
+        TRY_CUDA(cudaMemcpyAsync(back_host, dptrs[back], b, cudaMemcpyDeviceToHost, s));
+    }
     TRY_CUDA(cudaStreamSynchronize(s));
     TRY(ws_release(ctx, s));
     return BIELCC_OK;
@@ -554,7 +587,7 @@ int bielcc_integrand_info(int integrand, int* idim, int* is_complex) {
 }
 
 int bielcc_integral_pnt(bielcc_ctx ctx, int integrand, int n_vert, int n_pairs, const double* cells, const double* x,
-                        const bielcc_kernelparam* kp, int n_start, int p_max, double eps, double* res) {
+                        bielcc_kernelparam* kp, int n_start, int p_max, double eps, double* res) {
     TRY(enter(ctx));
     TRY(check_nv(n_vert));
     TRY(check_quad_params(n_start, p_max));
@@ -569,13 +602,14 @@ int bielcc_integral_pnt(bielcc_ctx ctx, int integrand, int n_vert, int n_pairs, 
     return run_batch(ctx, {{cells, N * n_vert * 24}, {x, N * 24}, {kp, N * sizeof(KParamDev)}}, res, ob,
                      [&](std::vector<const void*>& d, void* o, cudaStream_t s) {
                          return launch_integral_pnt(integrand, n_vert, n_pairs, (const double*)d[0],
-                                                    (const double*)d[1], (const KParamDev*)d[2], n_start, p_max, eps,
+                                                    (const double*)d[1], (KParamDev*)d[2], n_start, p_max, eps,
                                                     (double*)o, s);
-                     });
+                     },
+                     2, kp);
 }
 
 int bielcc_integral_seg_pnt(bielcc_ctx ctx, int integrand, int n_pairs, const double* a, const double* b,
-                            const double* x, const bielcc_kernelparam* kp, int n_start, int p_max, double eps,
+                            const double* x, bielcc_kernelparam* kp, int n_start, int p_max, double eps,
                             double* res) {
     TRY(enter(ctx));
     TRY(check_quad_params(n_start, p_max));
@@ -589,13 +623,14 @@ int bielcc_integral_seg_pnt(bielcc_ctx ctx, int integrand, int n_pairs, const do
     return run_batch(ctx, {{a, N * 24}, {b, N * 24}, {x, N * 24}, {kp, N * sizeof(KParamDev)}}, res, ob,
                      [&](std::vector<const void*>& d, void* o, cudaStream_t s) {
                          return launch_integral_seg(integrand, n_pairs, (const double*)d[0], (const double*)d[1],
-                                                    (const double*)d[2], (const KParamDev*)d[3], n_start, p_max, eps,
+                                                    (const double*)d[2], (KParamDev*)d[3], n_start, p_max, eps,
                                                     (double*)o, s);
-                     });
+                     },
+                     3, kp);
 }
 
 int bielcc_k0(bielcc_ctx ctx, int integrand, int common, int n_vert, int n_pairs, const double* cells,
-              const double* x, const double* j, const bielcc_kernelparam* kp, int n_start_seg, int p_max_seg,
+              const double* x, const double* j, bielcc_kernelparam* kp, int n_start_seg, int p_max_seg,
               double eps, double* res) {
     TRY(enter(ctx));
     TRY(check_nv(n_vert));
@@ -611,9 +646,10 @@ int bielcc_k0(bielcc_ctx ctx, int integrand, int common, int n_vert, int n_pairs
                            {kp, N * sizeof(KParamDev)}},
                      res, N * 48, [&](std::vector<const void*>& d, void* o, cudaStream_t s) {
                          return launch_k0(integrand, common, n_vert, n_pairs, (const double*)d[0],
-                                          (const double*)d[1], (const double*)d[2], (const KParamDev*)d[3],
+                                          (const double*)d[1], (const double*)d[2], (KParamDev*)d[3],
                                           n_start_seg, p_max_seg, eps, (double*)o, s);
-                     });
+                     },
+                     3, kp);
 }
 
 int bielcc_integral_1divr(bielcc_ctx ctx, int n_vert, int n_pairs, const double* cells, const double* x,
@@ -732,9 +768,12 @@ int bielcc_assemble_K(bielcc_ctx ctx, bielcc_mesh mesh, double k_re, double k_im
     TRY_CUDA(cudaMalloc(&dA, bytes));
     int rc = bielcc_assemble_K_device(ctx, mesh, k_re, k_im, np, layout, out_c64, precision, dA, nullptr, report);
     if (rc == BIELCC_OK) {
-        cudaError_t e = cudaMemcpy(A_host, dA, bytes, cudaMemcpyDeviceToHost);
+        // the download runs on the context's (non-blocking) stream, after the kernels
+        cudaError_t e = cudaMemcpyAsync(A_host, dA, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
         if (e != cudaSuccess) rc = cuda_status(e, "matrix download", __LINE__);
     }
+    cudaStreamSynchronize(ctx->stream);
     cudaFree(dA);
     return rc;
 }

@@ -71,11 +71,11 @@ struct KParamDev {
     double n[3];
 };
 cudaError_t launch_integral_pnt(int integrand, int nv, int n, const double* cells, const double* x,
-                                const KParamDev* kp, int n_start, int p_max, double eps, double* res, cudaStream_t s);
+                                KParamDev* kp, int n_start, int p_max, double eps, double* res, cudaStream_t s);
 cudaError_t launch_integral_seg(int integrand, int n, const double* a, const double* b, const double* x,
-                                const KParamDev* kp, int n_start, int p_max, double eps, double* res, cudaStream_t s);
+                                KParamDev* kp, int n_start, int p_max, double eps, double* res, cudaStream_t s);
 cudaError_t launch_k0(int integrand, int common, int nv, int n, const double* cells, const double* x, const double* j,
-                      const KParamDev* kp, int n_seg, int p_seg, double eps, double* res, cudaStream_t s);
+                      KParamDev* kp, int n_seg, int p_seg, double eps, double* res, cudaStream_t s);
 cudaError_t launch_analytic(int which, int nv, int n, const double* cells_or_a, const double* b, const double* x,
                             double analytic_r, int n_start, int p_max, double eps, cplx k, double* res, cudaStream_t s);
 

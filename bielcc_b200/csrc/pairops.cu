@@ -38,7 +38,7 @@ __global__ void pair_op_kernel(int op, int nv, int n, const double* __restrict__
 }
 
 __global__ void integral_pnt_kernel(int id, int nv, int n, const double* __restrict__ cells,
-                                    const double* __restrict__ x, const KParamDev* __restrict__ kp, int n_start,
+                                    const double* __restrict__ x, KParamDev* __restrict__ kp, int n_start,
                                     int p_max, double eps, double* __restrict__ res) {
     int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= n) return;
@@ -57,10 +57,11 @@ __global__ void integral_pnt_kernel(int id, int nv, int n, const double* __restr
         integral_cell<double>(id, xp, c, p, idim, n_start, p_max, eps, r);
         for (int g = 0; g < idim; g++) res[(size_t)idim * q + g] = r[g];
     }
+    kp[q].smoothR = p.smoothR;  // the reference mutates its KernelParam
 }
 
 __global__ void integral_seg_kernel(int id, int n, const double* __restrict__ a, const double* __restrict__ b,
-                                    const double* __restrict__ x, const KParamDev* __restrict__ kp, int n_start,
+                                    const double* __restrict__ x, KParamDev* __restrict__ kp, int n_start,
                                     int p_max, double eps, double* __restrict__ res) {
     int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= n) return;
@@ -78,10 +79,11 @@ __global__ void integral_seg_kernel(int id, int n, const double* __restrict__ a,
         integral_seg<double>(id, A, B, X, p, idim, n_start, p_max, eps, r);
         for (int g = 0; g < idim; g++) res[(size_t)idim * q + g] = r[g];
     }
+    kp[q].smoothR = p.smoothR;
 }
 
 __global__ void k0_kernel(int id, int common, int nv, int n, const double* __restrict__ cells,
-                          const double* __restrict__ x, const cplx* __restrict__ j, const KParamDev* __restrict__ kp,
+                          const double* __restrict__ x, const cplx* __restrict__ j, KParamDev* __restrict__ kp,
                           int n_seg, int p_seg, double eps, cplx* __restrict__ res) {
     int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= n) return;
@@ -98,6 +100,7 @@ __global__ void k0_kernel(int id, int common, int nv, int n, const double* __res
         K0_dev(id, jj, xp, c, p, n_seg, p_seg, eps, r);
     }
     for (int g = 0; g < 3; g++) res[3 * (size_t)q + g] = r[g];
+    kp[q].smoothR = p.smoothR;
 }
 
 // which: 0 integral1Divr, 1 integralGrad1DivrSeg, 2 IntegralSurf_SimplePot_H_HS,
@@ -141,21 +144,21 @@ cudaError_t launch_pair_op(int op, int nv, int n, const double* cells, const dou
 }
 
 cudaError_t launch_integral_pnt(int integrand, int nv, int n, const double* cells, const double* x,
-                                const KParamDev* kp, int n_start, int p_max, double eps, double* res, cudaStream_t s) {
+                                KParamDev* kp, int n_start, int p_max, double eps, double* res, cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
     integral_pnt_kernel<<<blocks_for(n), 128, 0, s>>>(integrand, nv, n, cells, x, kp, n_start, p_max, eps, res);
     return cudaGetLastError();
 }
 
 cudaError_t launch_integral_seg(int integrand, int n, const double* a, const double* b, const double* x,
-                                const KParamDev* kp, int n_start, int p_max, double eps, double* res, cudaStream_t s) {
+                                KParamDev* kp, int n_start, int p_max, double eps, double* res, cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
     integral_seg_kernel<<<blocks_for(n), 128, 0, s>>>(integrand, n, a, b, x, kp, n_start, p_max, eps, res);
     return cudaGetLastError();
 }
 
 cudaError_t launch_k0(int integrand, int common, int nv, int n, const double* cells, const double* x, const double* j,
-                      const KParamDev* kp, int n_seg, int p_seg, double eps, double* res, cudaStream_t s) {
+                      KParamDev* kp, int n_seg, int p_seg, double eps, double* res, cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
     k0_kernel<<<blocks_for(n), 128, 0, s>>>(integrand, common, nv, n, cells, x, reinterpret_cast<const cplx*>(j), kp,
                                             n_seg, p_seg, eps, reinterpret_cast<cplx*>(res));

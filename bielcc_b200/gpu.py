@@ -48,6 +48,7 @@ def load(path=LIB_PATH):
     d("bielcc_ctx_mem_used", [vp, C.POINTER(C.c_int64)])
     d("bielcc_mesh_create", [vp, C.c_int, C.c_int, dp, ip])
     d("bielcc_mesh_destroy", [vp, C.c_int32])
+    d("bielcc_mesh_geometry", [vp, C.c_int32, dp])
     field_args = [vp, C.c_int32, C.c_int, dp, C.c_double, C.c_double, C.c_double, C.c_double,
                   C.POINTER(abi.PlaneWave), C.POINTER(abi.NumParam), C.c_int, dp, dp, dp, C.c_int]
     d("bielcc_field_EH", field_args + [C.POINTER(abi.Report)])
@@ -94,6 +95,12 @@ class Mesh:
         self.id = h.value
         self.n_cells = self.cells.shape[0]
         self.n_vert = self.cells.shape[1]
+
+    def geometry(self):
+        """[N][14]: centre(3), diam, normal(3), tau1(3), tau2(3), area computed on the device."""
+        out = np.zeros((self.n_cells, 14))
+        _check(_lib.bielcc_mesh_geometry(self.ctx.h, self.id, abi.dptr(out)))
+        return out
 
     def close(self):
         if self.id:

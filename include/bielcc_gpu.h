@@ -145,6 +145,12 @@ int bielcc_measure_fma_peak(int fp64, double* tflops);
 int bielcc_mesh_create(bielcc_ctx ctx, int n_vert, int n_cells, const double* cells,
                        bielcc_mesh* out);
 int bielcc_mesh_destroy(bielcc_ctx ctx, bielcc_mesh mesh);
+/* Per-cell geometry rows computed on the device, 14 doubles per cell:
+ * centre(3), diam, normal(3), tau1(3), tau2(3), area — the collocation points,
+ * normals and surface basis of SurfMesh::FormCollocPoints /
+ * FormNormalVectors / FormSurfaceBasis (mesh/surf_mesh.h:205-268) and
+ * get_diam, and the cell area of CellFill; out: [n_cells][14]. */
+int bielcc_mesh_geometry(bielcc_ctx ctx, bielcc_mesh mesh, double* out);
 
 /* ---- field evaluation ------------------------------------------------- */
 /* E(x_i) = mult * sum_j K[cell_j, J_j](x_i) + E_inc(x_i)
@@ -216,28 +222,29 @@ int bielcc_integrand_info(int integrand, int* idim, int* is_complex);
  * :136-220 triangle) of one integrand over n_pairs (cell, x) pairs with the
  * adaptive n -> 2n refinement and smoothing-radius halving of the reference.
  * kp is per pair ([n_pairs]) so each pair has its own smoothR / current / n;
- * its smoothR on return is NOT updated (the reference mutates it).
+ * on return each record's smoothR holds the value the reference leaves in its
+ * KernelParam (halved after every pass while above smoothRMin).
  * res: [n_pairs][idim] (complex interleaved when the integrand is complex). */
 int bielcc_integral_pnt(bielcc_ctx ctx, int integrand, int n_vert, int n_pairs,
                         const double* cells, const double* x,
-                        const bielcc_kernelparam* kp, int n_start, int p_max,
+                        bielcc_kernelparam* kp, int n_start, int p_max,
                         double eps, double* res);
 
 /* IntegralUniversalSegPnt (integrators/integral_universal_seg.h:38-98):
- * a, b, x: [n_pairs][3]. */
+ * a, b, x: [n_pairs][3]; kp in/out as for bielcc_integral_pnt. */
 int bielcc_integral_seg_pnt(bielcc_ctx ctx, int integrand, int n_pairs,
                             const double* a, const double* b, const double* x,
-                            const bielcc_kernelparam* kp, int n_start, int p_max,
+                            bielcc_kernelparam* kp, int n_start, int p_max,
                             double eps, double* res);
 
 /* K0 / K0_Common (electrodynamics/K0.h:36-86 / :112-166): contour integral
  * of one integrand over the cell edges. common = 0: -sum_e (j.nu_e) int_e F;
  * common = 1: sum_e int_e F nu_e (vec_dbl set to nu_e per edge). The
  * kernel-parameter record is shared by the edges of a pair exactly as in the
- * reference (its smoothR shrinks from edge to edge). */
+ * reference (its smoothR shrinks from edge to edge); kp in/out. */
 int bielcc_k0(bielcc_ctx ctx, int integrand, int common, int n_vert, int n_pairs,
               const double* cells, const double* x, const double* j,
-              const bielcc_kernelparam* kp, int n_start_seg, int p_max_seg,
+              bielcc_kernelparam* kp, int n_start_seg, int p_max_seg,
               double eps, double* res);
 
 /* ---- analytic singular integrals -------------------------------------- */

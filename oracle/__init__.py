@@ -194,9 +194,9 @@ def area_by_quadrature(cell, n_start=8, p_max=1, eps=1e-6, which="port"):
 
 
 def cell_geometry(cells, which="port"):
-    """[N][13]: centre(3), diam, normal(3), tau1(3), tau2(3), area."""
+    """[N][14]: centre(3), diam, normal(3), tau1(3), tau2(3), area."""
     cells = _c(cells)
-    out = np.zeros((cells.shape[0], 13))
+    out = np.zeros((cells.shape[0], 14))
     _f(which, "cell_geometry")(cells.shape[1], cells.shape[0], abi.dptr(cells), abi.dptr(out))
     return out
 

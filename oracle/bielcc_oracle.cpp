@@ -874,7 +874,7 @@ int oracle_pair_op(int op, int n_vert, int n_pairs, const double* cells, const d
 }
 
 int oracle_integral_pnt(int integrand, int n_vert, int n_pairs, const double* cells, const double* x,
-                        const bielcc_kernelparam* kp, int n_start, int p_max, double eps, double* res) {
+                        bielcc_kernelparam* kp, int n_start, int p_max, double eps, double* res) {
     if ((n_vert != 3 && n_vert != 4) || integrand < 0 || integrand >= BIELCC_F_COUNT) return BIELCC_ERR_ARG;
     int idim = integrand_dim(integrand);
     for (int p = 0; p < n_pairs; p++) {
@@ -887,12 +887,13 @@ int oracle_integral_pnt(int integrand, int n_vert, int n_pairs, const double* ce
         else
             integral_cell<double>(x + 3 * (size_t)p, cl, real_integrand(integrand), k, idim, n_start, p_max,
                                   eps, res + (size_t)idim * p);
+        kp[p].smoothR = k.smoothR;  // the reference leaves its KernelParam mutated
     }
     return BIELCC_OK;
 }
 
 int oracle_integral_seg_pnt(int integrand, int n_pairs, const double* a, const double* b, const double* x,
-                            const bielcc_kernelparam* kp, int n_start, int p_max, double eps, double* res) {
+                            bielcc_kernelparam* kp, int n_start, int p_max, double eps, double* res) {
     if (integrand < 0 || integrand >= BIELCC_F_COUNT) return BIELCC_ERR_ARG;
     int idim = integrand_dim(integrand);
     for (int p = 0; p < n_pairs; p++) {
@@ -905,12 +906,13 @@ int oracle_integral_seg_pnt(int integrand, int n_pairs, const double* a, const d
             integral_seg<double>(a + 3 * (size_t)p, b + 3 * (size_t)p, x + 3 * (size_t)p,
                                  real_integrand(integrand), k, idim, n_start, p_max, eps,
                                  res + (size_t)idim * p);
+        kp[p].smoothR = k.smoothR;
     }
     return BIELCC_OK;
 }
 
 int oracle_k0(int integrand, int common, int n_vert, int n_pairs, const double* cells, const double* x,
-              const double* j, const bielcc_kernelparam* kp, int n_seg, int p_seg, double eps, double* res) {
+              const double* j, bielcc_kernelparam* kp, int n_seg, int p_seg, double eps, double* res) {
     auto f = cplx_integrand(integrand);
     if (!f || integrand_dim(integrand) != 3) return BIELCC_ERR_ARG;
     for (int p = 0; p < n_pairs; p++) {
@@ -920,6 +922,7 @@ int oracle_k0(int integrand, int common, int n_vert, int n_pairs, const double* 
         cd* r = reinterpret_cast<cd*>(res) + 3 * (size_t)p;
         if (common) K0_Common(x + 3 * (size_t)p, cl, f, k, n_seg, p_seg, eps, r);
         else K0(reinterpret_cast<const cd*>(j) + 3 * (size_t)p, x + 3 * (size_t)p, cl, f, k, n_seg, p_seg, eps, r);
+        kp[p].smoothR = k.smoothR;
     }
     return BIELCC_OK;
 }
@@ -965,11 +968,11 @@ int oracle_area_by_quadrature(int n_vert, const double* cell, int n_start, int p
 }
 
 // Per-cell geometry rows as SurfMesh / CellFill expose them:
-// out[c] = centre(3), diam, normal(3), tau1(3), tau2(3), area = 13 doubles.
+// out[c] = centre(3), diam, normal(3), tau1(3), tau2(3), area = 14 doubles.
 int oracle_cell_geometry(int n_vert, int n_cells, const double* cells, double* out) {
     for (int c = 0; c < n_cells; c++) {
         Cell cl{n_vert, reinterpret_cast<const double(*)[3]>(cells + (size_t)c * n_vert * 3)};
-        double* o = out + 13 * (size_t)c;
+        double* o = out + 14 * (size_t)c;
         centre(cl, o);
         o[3] = diam(cl);
         normal(cl, o + 4);
@@ -983,9 +986,9 @@ int oracle_cell_geometry(int n_vert, int n_cells, const double* cells, double* o
                 ac[i] = mc[i] - ma[i]; bd[i] = md[i] - mb[i];
             }
             cross3(ac, bd, v);
-            o[12] = len3(v);
+            o[13] = len3(v);
         } else {
-            o[12] = tri_area(cl.v[0], cl.v[1], cl.v[2]);
+            o[13] = tri_area(cl.v[0], cl.v[1], cl.v[2]);
         }
     }
     return BIELCC_OK;
@@ -1004,16 +1007,16 @@ int oracle_assemble_K(int n_vert, int n_cells, const double* cells, double k_re,
     cd k(k_re, k_im);
     int m = layout == BIELCC_LAYOUT_TAU2 ? 2 : 3;
     size_t ncols = (size_t)m * n_cells;
-    std::vector<double> geo(13 * (size_t)n_cells);
+    std::vector<double> geo(14 * (size_t)n_cells);
     oracle_cell_geometry(n_vert, n_cells, cells, geo.data());
 #ifdef _OPENMP
 #pragma omp parallel for schedule(dynamic, 1)
 #endif
     for (int i = row_begin; i < row_end; i++) {
-        const double* ci = &geo[13 * (size_t)i];
+        const double* ci = &geo[14 * (size_t)i];
         for (int j = 0; j < n_cells; j++) {
             Cell cl{n_vert, reinterpret_cast<const double(*)[3]>(cells + (size_t)j * n_vert * 3)};
-            const double* gj = &geo[13 * (size_t)j];
+            const double* gj = &geo[14 * (size_t)j];
             bool near = dist3(ci, gj) < np.analytic_calc * gj[3];
             for (int b = 0; b < m; b++) {
                 cd jv[3];

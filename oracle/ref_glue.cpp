@@ -204,7 +204,7 @@ int with_integrand(int id, Fn fn) {
 
 template <typename KType>
 int integral_pnt_impl(int integrand, int n_vert, int n_pairs, const double* cells, const double* x,
-                      const bielcc_kernelparam* kp, int n_start, int p_max, double eps, double* res) {
+                      bielcc_kernelparam* kp, int n_start, int p_max, double eps, double* res) {
     return with_integrand<KType>(integrand, [&](auto fr, auto fc, int idim) {
         for (int p = 0; p < n_pairs; p++) {
             KernelParam<KType> k = make_kp<KType>(kp[p]);
@@ -219,13 +219,14 @@ int integral_pnt_impl(int integrand, int n_vert, int n_pairs, const double* cell
                 if (fc) IntegralUniversalPnt(xp, c, fc, k, ip, reinterpret_cast<cd*>(res) + (size_t)idim * p);
                 else IntegralUniversalPnt(xp, c, fr, k, ip, res + (size_t)idim * p);
             }
+            kp[p].smoothR = k.smoothR;
         }
     });
 }
 
 template <typename KType>
 int integral_seg_impl(int integrand, int n_pairs, const double* a, const double* b, const double* x,
-                      const bielcc_kernelparam* kp, int n_start, int p_max, double eps, double* res) {
+                      bielcc_kernelparam* kp, int n_start, int p_max, double eps, double* res) {
     return with_integrand<KType>(integrand, [&](auto fr, auto fc, int idim) {
         for (int p = 0; p < n_pairs; p++) {
             KernelParam<KType> k = make_kp<KType>(kp[p]);
@@ -233,13 +234,14 @@ int integral_seg_impl(int integrand, int n_pairs, const double* a, const double*
             size_t o = 3 * (size_t)p;
             if (fc) IntegralUniversalSegPnt(a + o, b + o, x + o, fc, k, ip, reinterpret_cast<cd*>(res) + (size_t)idim * p);
             else IntegralUniversalSegPnt(a + o, b + o, x + o, fr, k, ip, res + (size_t)idim * p);
+            kp[p].smoothR = k.smoothR;
         }
     });
 }
 
 template <typename KType>
 int k0_impl(int integrand, int common, int n_vert, int n_pairs, const double* cells, const double* x,
-            const double* j, const bielcc_kernelparam* kp, int n_seg, int p_seg, double eps, double* res) {
+            const double* j, bielcc_kernelparam* kp, int n_seg, int p_seg, double eps, double* res) {
     return with_integrand<KType>(integrand, [&](auto, auto fc, int idim) {
         if (!fc || idim != 3) return;
         for (int p = 0; p < n_pairs; p++) {
@@ -257,6 +259,7 @@ int k0_impl(int integrand, int common, int n_vert, int n_pairs, const double* ce
                 if (common) K0_Common(xp, c, fc, k, ip, r);
                 else K0(jp, xp, c, fc, k, ip, r);
             }
+            kp[p].smoothR = k.smoothR;
         }
     });
 }
@@ -308,7 +311,7 @@ int ref_pair_op(int op, int n_vert, int n_pairs, const double* cells, const doub
 }
 
 int ref_integral_pnt(int integrand, int n_vert, int n_pairs, const double* cells, const double* x,
-                     const bielcc_kernelparam* kp, int n_start, int p_max, double eps, double* res) {
+                     bielcc_kernelparam* kp, int n_start, int p_max, double eps, double* res) {
     if (n_vert != 3 && n_vert != 4) return BIELCC_ERR_ARG;
     bool cplx = false;
     for (int p = 0; p < n_pairs; p++) cplx = cplx || kp[p].k_im != 0.;
@@ -317,7 +320,7 @@ int ref_integral_pnt(int integrand, int n_vert, int n_pairs, const double* cells
 }
 
 int ref_integral_seg_pnt(int integrand, int n_pairs, const double* a, const double* b, const double* x,
-                         const bielcc_kernelparam* kp, int n_start, int p_max, double eps, double* res) {
+                         bielcc_kernelparam* kp, int n_start, int p_max, double eps, double* res) {
     bool cplx = false;
     for (int p = 0; p < n_pairs; p++) cplx = cplx || kp[p].k_im != 0.;
     if (cplx) return integral_seg_impl<cd>(integrand, n_pairs, a, b, x, kp, n_start, p_max, eps, res);
@@ -325,7 +328,7 @@ int ref_integral_seg_pnt(int integrand, int n_pairs, const double* a, const doub
 }
 
 int ref_k0(int integrand, int common, int n_vert, int n_pairs, const double* cells, const double* x,
-           const double* j, const bielcc_kernelparam* kp, int n_seg, int p_seg, double eps, double* res) {
+           const double* j, bielcc_kernelparam* kp, int n_seg, int p_seg, double eps, double* res) {
     bool cplx = false;
     for (int p = 0; p < n_pairs; p++) cplx = cplx || kp[p].k_im != 0.;
     if (cplx) return k0_impl<cd>(integrand, common, n_vert, n_pairs, cells, x, j, kp, n_seg, p_seg, eps, res);
@@ -392,10 +395,10 @@ int ref_area_by_quadrature(int n_vert, const double* cell, int n_start, int p_ma
 }
 
 // Cell geometry as the reference's CellFill / element_geom compute it:
-// centre(3), diam, norm_func normal(3), tau1(3), tau2(3), CellFill area.
+// centre(3), diam, norm_func normal(3), tau1(3), tau2(3), CellFill area (14).
 int ref_cell_geometry(int n_vert, int n_cells, const double* cells, double* out) {
     for (int c = 0; c < n_cells; c++) {
-        double* o = out + 13 * (size_t)c;
+        double* o = out + 14 * (size_t)c;
         if (n_vert == 4) {
             const auto& v = *reinterpret_cast<const double(*)[4][3]>(cells + (size_t)c * 12);
             CellQuad q;
@@ -404,7 +407,7 @@ int ref_cell_geometry(int n_vert, int n_cells, const double* cells, double* out)
             o[3] = get_diam(v);
             norm_func(v, o + 4);
             for (int g = 0; g < 3; g++) { o[7 + g] = q.GetTau1()[g]; o[10 + g] = q.GetTau2()[g]; }
-            o[12] = q.GetArea();
+            o[13] = q.GetArea();
         } else {
             const auto& v = *reinterpret_cast<const double(*)[3][3]>(cells + (size_t)c * 9);
             CellTriangle t;
@@ -413,7 +416,7 @@ int ref_cell_geometry(int n_vert, int n_cells, const double* cells, double* out)
             o[3] = get_diam(v);
             norm_func(v, o + 4);
             for (int g = 0; g < 3; g++) { o[7 + g] = t.GetTau1()[g]; o[10 + g] = t.GetTau2()[g]; }
-            o[12] = t.GetArea();
+            o[13] = t.GetArea();
         }
     }
     return BIELCC_OK;

@@ -86,8 +86,10 @@ def main():
             kk = np.where(rng.random(16) < 0.5, 2 * np.pi, 2 * np.pi + 0.3j)
             sR = 2.0 * dm / 8.0
             nrm = rng.normal(size=(16, 3))
-            kp = abi.kernelparam_array(16, smoothR=sR, smoothRMin=dm / 100, k=kk, current=j, vec_dbl=nrm, normal=nrm)
             for pm in (1, 2):
+                # fresh records per call: the call leaves smoothR mutated, as the reference does
+                kp = abi.kernelparam_array(16, smoothR=sR, smoothRMin=dm / 100, k=kk, current=j, vec_dbl=nrm,
+                                           normal=nrm)
                 r = oracle.integral_pnt(fid, cc, x, kp, 8, pm, 1e-6, which=REF)
                 key = f"{name}_f{fid}_p{pm}"
                 ints[key + "_cells"] = cc
@@ -104,9 +106,9 @@ def main():
         x = (a + b) / 2 + rng.normal(size=(16, 3)) * 0.2
         kk = np.where(rng.random(16) < 0.5, 2 * np.pi, 2 * np.pi + 0.3j)
         sR = np.full(16, 0.05)
-        kp = abi.kernelparam_array(16, smoothR=sR, smoothRMin=1e-3, k=kk, current=a + 1j * b, vec_dbl=b - a,
-                                   normal=b - a)
         for pm in (1, 3):
+            kp = abi.kernelparam_array(16, smoothR=sR, smoothRMin=1e-3, k=kk, current=a + 1j * b, vec_dbl=b - a,
+                                       normal=b - a)
             r = oracle.integral_seg_pnt(fid, a, b, x, kp, 10, pm, 1e-6, which=REF)
             key = f"seg_f{fid}_p{pm}"
             ints.update({key + "_a": a, key + "_b": b, key + "_x": x, key + "_sR": sR, key + "_k": kk,

@@ -119,7 +119,7 @@ def test_edge_cases(gctx):
     # bad arguments fail with a status, not a crash
     from bielcc_b200.gpu import BielccError
 
-    with pytest.raises(BielccError):
+    with pytest.raises((ValueError, BielccError)):
         gctx.field_EH(m, J[:, :3], 1.0, p)
     with pytest.raises(BielccError):
         gctx.field_EH(m, J, 1.0, p, numparam=abi.NumParam.default(n_start=0))
@@ -143,3 +143,14 @@ def test_device_buffers_through_torch(gctx):
     torch.cuda.synchronize()
     assert rel_l2(Ed.cpu().numpy(), E) == 0.0
     assert rel_l2(Hd.cpu().numpy(), H) == 0.0
+
+
+def test_mesh_geometry_rows(gctx):
+    """Centres, diameters, normals and the CellFill tangent basis computed on the device."""
+    for cells in (W.uv_sphere(16, 32), W.perturbed_icosphere(level=2, seed=2)):
+        m = gctx.mesh(cells)
+        g = m.geometry()
+        o = oracle.cell_geometry(cells)
+        assert np.abs(g[:, :13] - o[:, :13]).max() < 1e-14
+        assert np.abs(g[:, 13] - o[:, 13]).max() < 1e-14
+        m.close()

@@ -53,13 +53,15 @@ def test_k0_against_oracle(gctx):
     cc = cells[idx]
     x = W.centres(cc) + rng.normal(size=(40, 3)) * 0.2
     j = rng.normal(size=(40, 3)) + 1j * rng.normal(size=(40, 3))
-    kp = abi.kernelparam_array(40, smoothR=0.05, smoothRMin=1e-6, k=complex(2.0, 0.1))
     for fid in (abi.F_GRADSIMPLEPOT_H, abi.F_NU_SIMPLEPOT_H, abi.F_ROTROTSIMPLEPOT_H):
         for common in (0, 1):
             for pm in (1, 2):
-                a = gctx.k0(fid, common, cc, x, j, kp, 10, pm, 1e-6)
-                b = oracle.k0(fid, common, cc, x, j, kp, 10, pm, 1e-6)
+                kpa = abi.kernelparam_array(40, smoothR=0.05, smoothRMin=1e-6, k=complex(2.0, 0.1))
+                kpb = abi.kernelparam_array(40, smoothR=0.05, smoothRMin=1e-6, k=complex(2.0, 0.1))
+                a = gctx.k0(fid, common, cc, x, j, kpa, 10, pm, 1e-6)
+                b = oracle.k0(fid, common, cc, x, j, kpb, 10, pm, 1e-6)
                 assert rel_l2(a, b) < TOL_FP64
+                assert [r.smoothR for r in kpa] == [r.smoothR for r in kpb]  # KernelParam left as the reference does
 
 
 def test_analytic_golden(gctx):
