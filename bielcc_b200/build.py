@@ -19,6 +19,10 @@ FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxe
 # the C ABI symbols carry default visibility via extern "C" + this define
 DEFS = ["-DBIELCC_BUILDING"]
 HOST_CC = ["-ccbin", "/usr/bin/g++"] if os.path.exists("/usr/bin/g++") else []
+# FP32 kernels: flush FP32 denormals (values here are O(1e-10..1e3), far from
+# the denormal range), so rsqrt / reciprocal need no subnormal fix-ups. FP64
+# arithmetic is unaffected by this flag.
+PER_FILE = {"field.cu": ["-ftz=true"], "assemble.cu": ["-ftz=true"]}
 
 
 def _stale(obj, deps):
@@ -38,7 +42,7 @@ def build(verbose=False, force=False):
         o = os.path.join(BUILD, os.path.basename(s)[:-3] + ".o")
         objs.append(o)
         if force or _stale(o, [s] + headers):
-            cmd = [NVCC] + HOST_CC + ARCH + FLAGS + DEFS + ["-c", s, "-o", o]
+            cmd = [NVCC] + HOST_CC + ARCH + FLAGS + DEFS + PER_FILE.get(os.path.basename(s), []) + ["-c", s, "-o", o]
             if verbose:
                 print(" ".join(cmd), flush=True)
             procs.append((s, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))

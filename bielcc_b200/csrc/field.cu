@@ -51,8 +51,9 @@ struct FarArgs {
     int n_rhs, rhs0;
     cplx k;
     double analytic_calc;
-    int cells_per_split;
-    double* partial;  // [split][S][12][P]
+    int cells_per_split;  // a multiple of 32: near-mask words never straddle splits
+    double* partial;      // [split][S][12][P]
+    unsigned* nearmask;   // [ceil(N/32)][P]: bit c%32 of word c/32 set iff (p, c) is near
 };
 
 // Near decision of get_field.h:58 with the reference's rounding.
@@ -75,21 +76,47 @@ struct Moments {
     }
 };
 
+// e^{i t} in FP64 for |t| <= 0.5 from its Taylor series (sin to t^13, cos to
+// t^14: truncation below 3e-17).
+BIELCC_D void sincos_taylor64(double t, double* s, double* c) {
+    double t2 = t * t;
+    double ps = fma(t2, -1.6059043836821613e-10, 2.5052108385441720e-08);
+    ps = fma(t2, ps, -2.7557319223985893e-06);
+    ps = fma(t2, ps, 1.9841269841269841e-04);
+    ps = fma(t2, ps, -8.3333333333333333e-03);
+    ps = fma(t2, ps, 1.6666666666666667e-01);
+    *s = t - t * t2 * ps;
+    double pc = fma(t2, 1.1470745597729725e-11, -2.0876756987868099e-09);
+    pc = fma(t2, pc, 2.7557319223985891e-07);
+    pc = fma(t2, pc, -2.4801587301587302e-05);
+    pc = fma(t2, pc, 1.3888888888888889e-03);
+    pc = fma(t2, pc, -4.1666666666666667e-02);
+    pc = fma(t2, pc, 0.5);
+    *c = 1.0 - t2 * pc;
+}
+
 // One far node, FP64. dx = x - y; w = node weight. Real k (CK = false) or
 // complex k. F_RotRotSimplePot_H (kernel_lib.h:453-492) and
 // F_GradSimplePot_H (kernel_lib.h:295-313) share r, 1/r and e^{ikr}.
-template <bool CK>
+// SPLIT: the phase is taken relative to r0 = |x - centre| (the moments are
+// multiplied by e^{ik r0} once per cell) and e^{ik (r - r0)} comes from the
+// Taylor series; otherwise e^{ikr} from sincos per node.
+template <bool CK, bool SPLIT>
 BIELCC_D void far_node_f64(Moments<double>& m, double dx, double dy, double dz, double w, cplx k, double k2r,
-                           double k2i) {
+                           double k2i, double r0) {
     double r2 = dx * dx + dy * dy + dz * dz;
-    double r = sqrt(r2);
-    double ir = 1.0 / r;
+    double ir = rsqrt(r2);
+    double r = r2 * ir;
     double s, c;
-    sincos(k.re * r, &s, &c);
-    if (CK) {
-        double a = exp(-k.im * r);
-        s *= a;
-        c *= a;
+    if (SPLIT) {
+        sincos_taylor64(k.re * (r - r0), &s, &c);
+    } else {
+        sincos(k.re * r, &s, &c);
+        if (CK) {
+            double a = exp(-k.im * r);
+            s *= a;
+            c *= a;
+        }
     }
     double ir2 = ir * ir, ir3 = ir2 * ir;
     double er = w * c, ei = w * s;
@@ -142,30 +169,50 @@ BIELCC_D void sincos_poly(float t, float* s, float* c) {
     *c = fmaf(t2, pc, 1.0f);
 }
 
-// e^{i theta} for |theta| <= 2^halvings: polynomial at theta / 2^h, then h
-// angle doublings; beyond 4 rad the accurate sincosf.
-BIELCC_D void phase_f32(float th, int halvings, float* s, float* c) {
-    if (halvings > 2) {
+// Short Taylor sine / cosine for |t| <= 0.25 (truncation below 1.3e-8).
+BIELCC_D void sincos_short(float t, float* s, float* c) {
+    float t2 = t * t;
+    float ps = fmaf(t2, 8.3333333e-3f, -1.6666667e-1f);
+    *s = t * fmaf(t2, ps, 1.0f);
+    float pc = fmaf(t2, -1.3888889e-3f, 4.1666667e-2f);
+    pc = fmaf(t2, pc, -0.5f);
+    *c = fmaf(t2, pc, 1.0f);
+}
+
+// e^{i theta} for a per-cell bound on |theta| (uniform over the CTA, so the
+// mode is a template argument of the node loop): 0 -> |theta| <= 0.25 short
+// polynomial; 1 -> <= 1; 2 -> <= 2 (half angle, one doubling); 3 -> <= 4 (two
+// doublings); 4 -> accurate sincosf.
+template <int MODE>
+BIELCC_D void phase_f32(float th, float* s, float* c) {
+    if constexpr (MODE == 0) {
+        sincos_short(th, s, c);
+    } else if constexpr (MODE == 4) {
         sincosf(th, s, c);
-        return;
+    } else {
+        constexpr int H = MODE - 1;
+        float ss, cc;
+        sincos_poly(th * (H == 0 ? 1.f : (H == 1 ? 0.5f : 0.25f)), &ss, &cc);
+#pragma unroll
+        for (int h = 0; h < H; h++) {
+            float ns = 2.f * ss * cc;
+            cc = fmaf(cc, cc, -ss * ss);
+            ss = ns;
+        }
+        *s = ss;
+        *c = cc;
     }
-    float t = th * (halvings == 0 ? 1.f : (halvings == 1 ? 0.5f : 0.25f));
-    float ss, cc;
-    sincos_poly(t, &ss, &cc);
-    for (int h = 0; h < halvings; h++) {
-        float ns = 2.f * ss * cc;
-        cc = fmaf(cc, cc, -ss * ss);
-        ss = ns;
-    }
-    *s = ss;
-    *c = cc;
+}
+
+BIELCC_HD int phase_mode(float th) {
+    return th <= 0.25f ? 0 : (th <= 1.f ? 1 : (th <= 2.f ? 2 : (th <= 4.f ? 3 : 4)));
 }
 
 // One far node, FP32, relative to the cell centre: X = x - centre (FP32),
 // node delta = y - centre, r0 = |X| (FP64 rounded), phase relative to r0.
-template <bool CK>
+template <bool CK, int MODE>
 BIELCC_D void far_node_f32(Moments<float>& m, float Xx, float Xy, float Xz, float r0, float r0sq, float4 nd, float kr_,
-                           float ki_, float k2r, float k2i, int halvings) {
+                           float ki_, float k2r, float k2i) {
     float tx = fmaf(-2.f, Xx, nd.x), ty = fmaf(-2.f, Xy, nd.y), tz = fmaf(-2.f, Xz, nd.z);
     float q = fmaf(nd.x, tx, fmaf(nd.y, ty, nd.z * tz));  // |x-y|^2 - r0^2
     float r2 = r0sq + q;
@@ -173,7 +220,7 @@ BIELCC_D void far_node_f32(Moments<float>& m, float Xx, float Xy, float Xz, floa
     float r = r2 * ir;
     float dr = __fdividef(q, r + r0);
     float s, c;
-    phase_f32(kr_ * dr, halvings, &s, &c);
+    phase_f32<MODE>(kr_ * dr, &s, &c);
     float w = nd.w;
     if (CK) w *= __expf(-ki_ * dr);
     float dx = Xx - nd.x, dy = Xy - nd.y, dz = Xz - nd.z;
@@ -277,6 +324,7 @@ __global__ void __launch_bounds__(kFarThreads) far_kernel(FarArgs a) {
     __shared__ double4 s_cell[kMaxStageCells];  // centre xyz, near threshold
     __shared__ cplx s_j[kMaxStageCells][NRHS][3];
     __shared__ float s_rho[kMaxStageCells];
+    __shared__ double s_rho64[kMaxStageCells];
 
     const int p = blockIdx.x * kFarThreads + threadIdx.x;
     const bool live = p < a.n_pts;
@@ -300,10 +348,12 @@ __global__ void __launch_bounds__(kFarThreads) far_kernel(FarArgs a) {
     Moments<F> m;
     m.zero();
     bool far = false, zeroR = false;
+    unsigned nbits = 0;  // near bits of the current 32-cell word
     // mixed-form per-pair state
     float Xf[3] = {0.f, 0.f, 0.f}, r0f = 0.f, r0sq = 0.f;
-    double P0r = 1.0, P0i = 0.0;
-    int halvings = 0;
+    double P0r = 1.0, P0i = 0.0, r0d = 0.0;
+    int mode = 0;
+    bool split64 = false;
 
     for (int c0 = cb; c0 < ce; c0 += cps) {
         const int nc = min(cps, ce - c0);
@@ -333,6 +383,7 @@ __global__ void __launch_bounds__(kFarThreads) far_kernel(FarArgs a) {
                     const CellGeo& gg = a.geo[c0 + i];
                     s_cell[i] = make_double4(gg.c[0], gg.c[1], gg.c[2], gg.diam);
                     if (MIXED) s_rho[i] = a.rho32[c0 + i];
+                    else s_rho64[i] = (double)a.rho32[c0 + i] * (1.0 + 1e-6);
                 }
                 for (int i = threadIdx.x; i < nc * NRHS * 3; i += kFarThreads) {
                     int cc = i / (NRHS * 3), rem = i - cc * NRHS * 3, rr = rem / 3, g = rem - rr * 3;
@@ -345,9 +396,29 @@ __global__ void __launch_bounds__(kFarThreads) far_kernel(FarArgs a) {
                 if (k0 == 0) {
                     double4 ci = s_cell[cc];
                     double cen[3] = {ci.x, ci.y, ci.z}, d;
-                    far = !is_near(x, cen, ci.w, a.analytic_calc, &d) && live;
+                    const bool nr = is_near(x, cen, ci.w, a.analytic_calc, &d);
+                    far = !nr && live;
                     zeroR = d < kMachineZero;  // R_Rot_Colloc: R = 0 at the cell centre
                     m.zero();
+                    const int c = c0 + cc;
+                    nbits |= (nr ? 1u : 0u) << (c & 31);
+                    if ((c & 31) == 31 || c == ce - 1) {
+                        if (live && a.nearmask) a.nearmask[(size_t)(c >> 5) * a.n_pts + p] = nbits;
+                        nbits = 0;
+                    }
+                    if (!MIXED && far) {  // FP64 phase split when the cell's phase range is small
+                        split64 = !CK && fabs(a.k.re) * s_rho64[cc] <= 0.5;
+                        r0d = d;
+                        if (split64) {
+                            double sn, cs;
+                            sincos(a.k.re * d, &sn, &cs);
+                            P0r = cs;
+                            P0i = sn;
+                        } else {
+                            P0r = 1.0;
+                            P0i = 0.0;
+                        }
+                    }
                     if (MIXED && far) {  // per-pair FP64 set-up of the phase split
                         Xf[0] = (float)(x[0] - ci.x);
                         Xf[1] = (float)(x[1] - ci.y);
@@ -363,8 +434,7 @@ __global__ void __launch_bounds__(kFarThreads) far_kernel(FarArgs a) {
                         }
                         P0r = c;
                         P0i = s;
-                        float th = (float)fabs(a.k.re) * s_rho[cc];
-                        halvings = th <= 1.f ? 0 : (th <= 2.f ? 1 : (th <= 4.f ? 2 : 3));
+                        mode = phase_mode((float)fabs(a.k.re) * s_rho[cc]);
                     }
                 }
                 if (far) {
@@ -372,21 +442,38 @@ __global__ void __launch_bounds__(kFarThreads) far_kernel(FarArgs a) {
                     if constexpr (MIXED) {
                         const float kr_ = (float)a.k.re, ki_ = (float)a.k.im;
                         const float k2rf = (float)k2r, k2if = (float)k2i;
-#pragma unroll 4
-                        for (int i = 0; i < kc; i++)
-                            far_node_f32<CK>(m, Xf[0], Xf[1], Xf[2], r0f, r0sq, nd[i], kr_, ki_, k2rf, k2if,
-                                             halvings);
+#define BIELCC_NODE_LOOP(MODE_)                                                                        \
+    _Pragma("unroll 4") for (int i = 0; i < kc; i++)                                                    \
+        far_node_f32<CK, MODE_>(m, Xf[0], Xf[1], Xf[2], r0f, r0sq, nd[i], kr_, ki_, k2rf, k2if);
+                        switch (mode) {
+                            case 0: BIELCC_NODE_LOOP(0) break;
+                            case 1: BIELCC_NODE_LOOP(1) break;
+                            case 2: BIELCC_NODE_LOOP(2) break;
+                            case 3: BIELCC_NODE_LOOP(3) break;
+                            default: BIELCC_NODE_LOOP(4) break;
+                        }
+#undef BIELCC_NODE_LOOP
                     } else {
+                        if (split64) {
 #pragma unroll 2
-                        for (int i = 0; i < kc; i++) {
-                            double4 v = nd[i];
-                            far_node_f64<CK>(m, x[0] - v.x, x[1] - v.y, x[2] - v.z, v.w, a.k, k2r, k2i);
+                            for (int i = 0; i < kc; i++) {
+                                double4 v = nd[i];
+                                far_node_f64<CK, true>(m, x[0] - v.x, x[1] - v.y, x[2] - v.z, v.w, a.k, k2r, k2i,
+                                                       r0d);
+                            }
+                        } else {
+#pragma unroll 2
+                            for (int i = 0; i < kc; i++) {
+                                double4 v = nd[i];
+                                far_node_f64<CK, false>(m, x[0] - v.x, x[1] - v.y, x[2] - v.z, v.w, a.k, k2r, k2i,
+                                                        r0d);
+                            }
                         }
                     }
                 }
                 if (k0 + kc == nn && far) {
                     if constexpr (MIXED) contract<NRHS, float>(m, (float)P0r, (float)P0i, s_j[cc], zeroR, acc);
-                    else contract<NRHS, double>(m, 1.0, 0.0, s_j[cc], zeroR, acc);
+                    else contract<NRHS, double>(m, P0r, P0i, s_j[cc], zeroR, acc);
                 }
             }
         }
@@ -416,10 +503,17 @@ __global__ void far_adaptive_kernel(FarArgs a, const double* __restrict__ verts,
     const int ce = min(a.n_cells, cb + a.cells_per_split);
     double acc[12];
     for (int q = 0; q < 12; q++) acc[q] = 0.;
+    unsigned nbits = 0;
     for (int c = cb; c < ce; c++) {
         const CellGeo& gg = a.geo[c];
         double d;
-        if (is_near(x, gg.c, gg.diam, a.analytic_calc, &d)) continue;
+        const bool nr = is_near(x, gg.c, gg.diam, a.analytic_calc, &d);
+        nbits |= (nr ? 1u : 0u) << (c & 31);
+        if ((c & 31) == 31 || c == ce - 1) {
+            if (a.nearmask) a.nearmask[(size_t)(c >> 5) * a.n_pts + p] = nbits;
+            nbits = 0;
+        }
+        if (nr) continue;
         DCell cl;
         cl.nv = nv;
         for (int v = 0; v < nv; v++)
@@ -458,30 +552,31 @@ __global__ void far_adaptive_kernel(FarArgs a, const double* __restrict__ verts,
 }
 
 // ---------------------------------------------------------------- near classification
-__global__ void near_count_kernel(const double* __restrict__ pts, int n_pts, const CellGeo* __restrict__ geo,
-                                  int n_cells, double analytic_calc, long long* __restrict__ counts) {
+// The far kernels record, per point, which cells failed the far test
+// (get_field.h:58) in a bit mask; these two kernels turn it into per-point
+// counts and the cell lists in ascending cell order.
+__global__ void near_count_kernel(const unsigned* __restrict__ mask, int n_words, int n_pts,
+                                  long long* __restrict__ counts) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n_pts) return;
-    double x[3] = {pts[3 * (size_t)p], pts[3 * (size_t)p + 1], pts[3 * (size_t)p + 2]};
     long long n = 0;
-    for (int c = 0; c < n_cells; c++) {
-        double d;
-        n += is_near(x, geo[c].c, geo[c].diam, analytic_calc, &d);
-    }
+    for (int w = 0; w < n_words; w++) n += __popc(mask[(size_t)w * n_pts + p]);
     counts[p] = n;
 }
 
-__global__ void near_fill_kernel(const double* __restrict__ pts, int n_pts, const CellGeo* __restrict__ geo,
-                                 int n_cells, double analytic_calc, const long long* __restrict__ offs,
-                                 int* __restrict__ pair_cell, int* __restrict__ pair_pt) {
+__global__ void near_fill_kernel(const unsigned* __restrict__ mask, int n_words, int n_pts,
+                                 const long long* __restrict__ offs, int* __restrict__ pair_cell,
+                                 int* __restrict__ pair_pt) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n_pts) return;
-    double x[3] = {pts[3 * (size_t)p], pts[3 * (size_t)p + 1], pts[3 * (size_t)p + 2]};
     long long o = offs[p];
-    for (int c = 0; c < n_cells; c++) {
-        double d;
-        if (is_near(x, geo[c].c, geo[c].diam, analytic_calc, &d)) {
-            pair_cell[o] = c;
+    if (offs[p + 1] == o) return;
+    for (int w = 0; w < n_words; w++) {
+        unsigned b = mask[(size_t)w * n_pts + p];
+        while (b) {
+            int bit = __ffs(b) - 1;
+            b &= b - 1;
+            pair_cell[o] = w * 32 + bit;
             pair_pt[o] = p;
             o++;
         }
@@ -623,6 +718,12 @@ static int resident_far_ctas() {
 }
 
 static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+static size_t mask_words(int n_cells) { return (size_t)(n_cells + 31) / 32; }
+// Cells per split rounded up to a multiple of 32 (one near-mask word).
+static int round_cells_per_split(int n_cells, int splits) {
+    int cps = (n_cells + splits - 1) / splits;
+    return (cps + 31) / 32 * 32;
+}
 
 size_t field_ws_base_bytes(const FieldLaunch& f, int* splits_out) {
     int tiles = (f.n_pts + kFarThreads - 1) / kFarThreads;
@@ -630,10 +731,12 @@ size_t field_ws_base_bytes(const FieldLaunch& f, int* splits_out) {
     int target = 2 * resident_far_ctas();
     int splits = std::max(1, (target + tiles - 1) / std::max(1, tiles));
     splits = std::min(splits, std::max(1, N / 8));
+    int cps = round_cells_per_split(N, splits);
+    splits = (N + cps - 1) / cps;
     *splits_out = splits;
     size_t P = f.n_pts;
     return align256((size_t)splits * f.n_rhs * 12 * P * sizeof(double)) + 2 * align256((P + 1) * sizeof(long long)) +
-           align256(sizeof(long long));
+           align256(sizeof(long long)) + align256(mask_words(N) * P * sizeof(unsigned));
 }
 
 template <int NRHS, bool CK, bool MIXED>
@@ -664,6 +767,9 @@ cudaError_t field_stage1(const FieldLaunch& f, void* ws, int splits, long long* 
     long long* counts = (long long*)w;
     w += align256((P + 1) * sizeof(long long));
     long long* offs = (long long*)w;
+    w += align256((P + 1) * sizeof(long long)) + align256(sizeof(long long));
+    unsigned* mask = (unsigned*)w;
+    const int n_words = (int)mask_words(m.n_cells);
 
     FarArgs a;
     a.pts = f.pts;
@@ -679,8 +785,9 @@ cudaError_t field_stage1(const FieldLaunch& f, void* ws, int splits, long long* 
     a.rhs0 = 0;
     a.k = f.k;
     a.analytic_calc = f.np.analytic_calc;
-    a.cells_per_split = (m.n_cells + splits - 1) / splits;
+    a.cells_per_split = round_cells_per_split(m.n_cells, splits);
     a.partial = partial;
+    a.nearmask = mask;
     int tiles = (f.n_pts + kFarThreads - 1) / kFarThreads;
     bool ck = f.k.im != 0.0;
     bool mixed = f.precision == 1;
@@ -698,9 +805,7 @@ cudaError_t field_stage1(const FieldLaunch& f, void* ws, int splits, long long* 
         else nl = ck ? launch_far_rhs<true, false>(a, tiles, splits, s) : launch_far_rhs<false, false>(a, tiles, splits, s);
     }
     if (far_end) cudaEventRecord(far_end, s);
-    if (tiles > 0)
-        near_count_kernel<<<tiles, kFarThreads, 0, s>>>(f.pts, f.n_pts, m.geo, m.n_cells, f.np.analytic_calc,
-                                                        counts);
+    if (tiles > 0) near_count_kernel<<<tiles, kFarThreads, 0, s>>>(mask, n_words, f.n_pts, counts);
     *far_launches = nl;
     *launches = nl + (tiles > 0 ? 1 : 0) + 1;
     scan_kernel<<<1, 1024, 0, s>>>(counts, f.n_pts, offs, d_total);
@@ -717,6 +822,9 @@ cudaError_t field_stage2(const FieldLaunch& f, void* ws, int splits, long long n
     w += align256((size_t)splits * f.n_rhs * 12 * P * sizeof(double));
     w += align256((P + 1) * sizeof(long long));
     long long* offs = (long long*)w;
+    w += align256((P + 1) * sizeof(long long)) + align256(sizeof(long long));
+    const unsigned* mask = (const unsigned*)w;
+    const int n_words = (int)mask_words(m.n_cells);
 
     int* pair_cell = nullptr;
     int* pair_pt = nullptr;
@@ -729,8 +837,7 @@ cudaError_t field_stage2(const FieldLaunch& f, void* ws, int splits, long long n
         pair_cell = (int*)pw;
         pw += align256((size_t)n_near * sizeof(int));
         pair_pt = (int*)pw;
-        near_fill_kernel<<<tiles, kFarThreads, 0, s>>>(f.pts, f.n_pts, m.geo, m.n_cells, f.np.analytic_calc, offs,
-                                                       pair_cell, pair_pt);
+        near_fill_kernel<<<tiles, kFarThreads, 0, s>>>(mask, n_words, f.n_pts, offs, pair_cell, pair_pt);
         DNP np{f.np.eps, f.np.rs, f.np.rs_seg, f.np.analytic_calc, f.np.n_start, f.np.n_start_seg, f.np.p_max,
                f.np.p_max_seg};
         int blocks = (int)((n_near + 127) / 128);
