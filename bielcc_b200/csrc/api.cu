@@ -77,6 +77,10 @@ struct DevBuf {
 
 }  // namespace
 
+namespace bielcc_gpu {
+int set_api_error(int code, const char* msg) { return set_error(code, "%s", msg); }
+}  // namespace bielcc_gpu
+
 struct bielcc_ctx_s {
     int device = 0;
     cudaStream_t stream = nullptr;

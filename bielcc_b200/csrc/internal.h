@@ -27,6 +27,9 @@ struct MeshDev {
     size_t bytes = 0;
 };
 
+// ---- api.cu: records `msg` as this thread's bielcc_last_error() and returns code
+int set_api_error(int code, const char* msg);
+
 // ---- mesh.cu
 cudaError_t launch_cell_geometry(const double* verts, int nv, int n_cells, CellGeo* geo, cudaStream_t s);
 cudaError_t launch_node_tables(const double* verts, const CellGeo* geo, int nv, int n_cells, int n, double4* nodes64,

@@ -179,6 +179,32 @@ int bielcc_field_EH_device(bielcc_ctx ctx, bielcc_mesh mesh, int n_rhs, const do
                            int n_pts, const double* pts_dev, double* E_dev, double* H_dev,
                            int precision, void* stream, bielcc_report* report);
 
+/* Field evaluation that allocates nothing. No counterpart in the reference.
+ * For callers that must not call cudaMalloc while they run: applications that
+ * reserve (nearly) all device memory in their own pool up front, where a
+ * library allocation can fail or fragment that pool, and latency-critical
+ * loops, where cudaMalloc / cudaFree would stall the device. Same computation
+ * as bielcc_field_EH_device without a context or resident mesh: the caller
+ * passes device pointers for the cells ([n_cells][n_vert][3]), J, points and
+ * outputs, and the call's scratch memory (cell rows, node tables, partial
+ * sums, near lists) lives in one static device array of 64 MiB that every GPU
+ * loading the library holds until exit. Sizes whose scratch exceeds 64 MiB are
+ * rejected with BIELCC_ERR_ARG and a message giving the bytes needed (roughly:
+ * 2.6 KiB per cell at n_start = 8, 100 B per point per cell split, 216 B per
+ * near pair). The first call on each device looks up the array's device
+ * address (cudaGetSymbolAddress), so that first call should come before any
+ * stream capture. All calls share the array and leave its contents behind;
+ * each call rewrites what it reads, and calls that overlap on the GPU race on
+ * it. `stream` may be NULL (legacy default stream); like the _device call it
+ * waits once for the near-pair count. The report carries n_pairs and
+ * n_near_pairs only. */
+int bielcc_field_EH_noalloc(int n_vert, int n_cells, const double* cells_dev, int n_rhs,
+                            const double* J_dev, double k_re, double k_im, double mult_re,
+                            double mult_im, const bielcc_planewave* inc,
+                            const bielcc_numparam* np, int n_pts, const double* pts_dev,
+                            double* E_dev, double* H_dev, int precision, void* stream,
+                            bielcc_report* report);
+
 /* ---- per-pair operators ----------------------------------------------- */
 /* One operator applied to n_pairs independent (cell, x, j) triples, each as
  * the reference call op(j, x, cell, num_param, k, res):

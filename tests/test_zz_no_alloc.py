@@ -1,0 +1,95 @@
+"""bielcc_field_EH_noalloc: the field evaluation for callers that cannot
+allocate device memory while they run (they reserved the GPU's memory in their
+own pool, or cannot afford cudaMalloc's device-wide synchronisation). All of
+its scratch lives in a static 64 MiB device array; the caller passes device
+buffers only.
+
+Checked through the C ABI against the allocating entry point
+(bielcc_field_EH_device) on two calls in a row — the second with other points
+and precision, so leftovers of the first call in the shared array would show —
+plus the size limit. This file is collected last on purpose."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from bielcc_b200 import abi, gpu
+from bielcc_b200 import workloads as W
+from conftest import TOL_FP64, TOL_MIXED, golden, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _bind():
+    L = gpu.load()
+    f = L.bielcc_field_EH_noalloc
+    vp = C.c_void_p
+    f.argtypes = [C.c_int, C.c_int, vp, C.c_int, vp, C.c_double, C.c_double, C.c_double, C.c_double,
+                  C.POINTER(abi.PlaneWave), C.POINTER(abi.NumParam), C.c_int, vp, vp, vp, C.c_int, vp,
+                  C.POINTER(abi.Report)]
+    f.restype = C.c_int
+    return L, f
+
+
+def test_noalloc_matches_allocating_entry_point_twice():
+    torch = pytest.importorskip("torch")
+    L, noalloc = _bind()
+    g = golden("field_quad512.npz")
+    inc = abi.PlaneWave.make(g["kvec"], g["e0"], float(g["h_scale"]), True, True)
+    cells, J, k = g["cells"], g["J"], float(g["k"])
+    dev = torch.device("cuda:0")
+    ctx = gpu.Context(0)
+    mesh = ctx.mesh(cells)
+    stream = torch.cuda.current_stream(dev)
+    Cd = torch.from_numpy(np.ascontiguousarray(cells)).to(dev)
+    Jd = torch.from_numpy(np.ascontiguousarray(J)).to(dev)
+    np_ = abi.NumParam.default()
+
+    def run_both(pts, precision):
+        Pd = torch.from_numpy(np.ascontiguousarray(pts)).to(dev)
+        shape = (1, len(pts), 3)
+        Ea = torch.zeros(shape, dtype=torch.complex128, device=dev)
+        Ha = torch.zeros_like(Ea)
+        Eb = torch.full(shape, complex(7.0, 7.0), dtype=torch.complex128, device=dev)
+        Hb = torch.full(shape, complex(7.0, 7.0), dtype=torch.complex128, device=dev)
+        ctx.field_EH_device(mesh, Jd.data_ptr(), k, Pd.data_ptr(), Ea.data_ptr(), Ha.data_ptr(), 1, len(pts),
+                            inc=inc, precision=precision, stream=stream.cuda_stream)
+        rep = abi.Report()
+        rc = noalloc(4, len(cells), Cd.data_ptr(), 1, Jd.data_ptr(), k, 0.0, 1.0, 0.0, C.byref(inc), C.byref(np_),
+                     len(pts), Pd.data_ptr(), Eb.data_ptr(), Hb.data_ptr(), gpu.PREC[precision], stream.cuda_stream,
+                     C.byref(rep))
+        assert rc == 0, L.bielcc_last_error().decode()
+        torch.cuda.synchronize()
+        assert rep.n_pairs == len(pts) * len(cells)
+        return (Ea.cpu().numpy(), Ha.cpu().numpy()), (Eb.cpu().numpy(), Hb.cpu().numpy()), rep
+
+    # call 1: the golden far + near points, FP64
+    (Ea, Ha), (Eb, Hb), rep = run_both(g["pts"], "fp64")
+    assert rep.n_near_pairs > 0
+    assert rel_l2(Eb, Ea) < TOL_FP64 and rel_l2(Hb, Ha) < TOL_FP64
+    assert rel_l2(Eb, g["E"]) < TOL_FP64 and rel_l2(Hb, g["H"]) < TOL_FP64
+
+    # call 2: another point set and the mixed form, on the array call 1 left behind
+    rng = np.random.default_rng(42)
+    pts2 = np.concatenate([W.sphere_points(150, 2.2, 5), W.near_points(cells, 30, 0.03, 0.2, rng)])
+    (Ea, Ha), (Eb, Hb), rep = run_both(pts2, "mixed")
+    assert rep.n_near_pairs > 0
+    assert rel_l2(Eb, Ea) < TOL_MIXED and rel_l2(Hb, Ha) < TOL_MIXED
+
+    mesh.close()
+    ctx.close()
+
+
+def test_noalloc_rejects_sizes_beyond_its_scratch():
+    torch = pytest.importorskip("torch")
+    L, noalloc = _bind()
+    dev = torch.device("cuda:0")
+    cells = W.uv_sphere(128, 256)  # 32768 cells: node tables alone exceed 64 MiB
+    Cd = torch.from_numpy(np.ascontiguousarray(cells)).to(dev)
+    Jd = torch.zeros((1, len(cells), 3), dtype=torch.complex128, device=dev)
+    Pd = torch.zeros((4, 3), dtype=torch.float64, device=dev)
+    Ed = torch.zeros((1, 4, 3), dtype=torch.complex128, device=dev)
+    rc = noalloc(4, len(cells), Cd.data_ptr(), 1, Jd.data_ptr(), 1.0, 0.0, 1.0, 0.0, None, None, 4, Pd.data_ptr(),
+                 Ed.data_ptr(), None, 0, None, None)
+    assert rc == abi.ERR_ARG
+    assert "scratch" in L.bielcc_last_error().decode()
