@@ -136,6 +136,25 @@ class Report(C.Structure):
     ]
 
 
+class FieldJob(C.Structure):
+    """bielcc_field_job: one field evaluation of a batch (device pointers)."""
+
+    _fields_ = [
+        ("mesh", C.c_int32),
+        ("n_rhs", C.c_int32),
+        ("n_pts", C.c_int32),
+        ("J_dev", C.c_void_p),
+        ("pts_dev", C.c_void_p),
+        ("E_dev", C.c_void_p),
+        ("H_dev", C.c_void_p),
+        ("k_re", C.c_double),
+        ("k_im", C.c_double),
+        ("mult_re", C.c_double),
+        ("mult_im", C.c_double),
+        ("inc", PlaneWave),
+    ]
+
+
 class Stats(C.Structure):
     _fields_ = [
         ("kernel_launches", C.c_int64),

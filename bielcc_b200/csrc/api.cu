@@ -94,6 +94,7 @@ struct bielcc_ctx_s {
     // counters / timing (bielcc_ctx_stats)
     bool timing = false;
     cudaEvent_t far_begin = nullptr, far_end = nullptr;
+    double batch_item_cost = 4.0e6;  // node evaluations per batched work item (bielcc_batch_autotune)
     bielcc_stats stats = {0, 0, 0, 0.0};
 };
 
@@ -512,6 +513,148 @@ int bielcc_field_EH(bielcc_ctx ctx, bielcc_mesh mesh, int n_rhs, const double* J
         report->est_sample = (int32_t)Q;
     }
     return rc;
+}
+
+}  // extern "C"
+
+namespace {
+
+int field_batch_locked(bielcc_ctx ctx, int n_jobs, const bielcc_field_job* jobs, const NumParamH& n, int precision,
+                       cudaStream_t s, bielcc_report* report, double item_cost) {
+    std::vector<MeshDev*> meshes(n_jobs);
+    for (int i = 0; i < n_jobs; i++) {
+        const bielcc_field_job& j = jobs[i];
+        TRY(get_mesh(ctx, j.mesh, &meshes[i]));
+        if (j.n_rhs < 1 || j.n_pts < 0 || !j.J_dev || (j.n_pts > 0 && (!j.pts_dev || !j.E_dev)))
+            return set_error(BIELCC_ERR_ARG, "job %d: bad sizes or null buffers", i);
+    }
+    if (report) memset(report, 0, sizeof(*report));
+    TRY(ws_acquire(ctx, s));
+    if (n.p_max > 1 || n.n_start > kBatchMaxNStart) {  // outside the batched kernel: one call per job
+        for (int i = 0; i < n_jobs; i++) {
+            const bielcc_field_job& j = jobs[i];
+            FieldArgs a{meshes[i], j.n_rhs, j.J_dev, mk(j.k_re, j.k_im), mk(j.mult_re, j.mult_im), &j.inc, n,
+                        j.n_pts, j.pts_dev, j.E_dev, j.H_dev, precision};
+            bielcc_report r{};
+            TRY(field_device(ctx, a, s, &r, nullptr));
+            if (report) {
+                report->n_pairs += r.n_pairs * j.n_rhs;
+                report->n_near_pairs += r.n_near_pairs;
+            }
+        }
+        TRY(ws_release(ctx, s));
+        return BIELCC_OK;
+    }
+    std::vector<JobDev> jd(n_jobs);
+    bool ck = false;
+    int64_t pairs = 0;
+    for (int i = 0; i < n_jobs; i++) {
+        const bielcc_field_job& j = jobs[i];
+        MeshDev* m = meshes[i];
+        TRY(ensure_tables(m, n.n_start, s));
+        JobDev& d = jd[i];
+        memset(&d, 0, sizeof(d));
+        d.geo = m->geo;
+        d.nodes32 = m->nodes32;
+        d.nodes64 = m->nodes64;
+        d.rho32 = m->rho32;
+        d.verts = m->verts;
+        d.nv = m->nv;
+        d.n_cells = m->n_cells;
+        d.pts = j.pts_dev;
+        d.n_pts = j.n_pts;
+        d.J = reinterpret_cast<const cplx*>(j.J_dev);
+        d.n_rhs = j.n_rhs;
+        d.k = mk(j.k_re, j.k_im);
+        d.mult = mk(j.mult_re, j.mult_im);
+        for (int g = 0; g < 3; g++) {
+            d.kvec[g] = j.inc.k_vec[g];
+            d.e0[g] = j.inc.e0[g];
+        }
+        d.h_scale = j.inc.h_scale;
+        d.add_E = j.inc.add_E;
+        d.add_H = j.inc.add_H;
+        d.E = j.E_dev;
+        d.H = j.H_dev;
+        ck = ck || j.k_im != 0.;
+        pairs += (int64_t)j.n_pts * m->n_cells * j.n_rhs;
+    }
+    BatchPlan bp;
+    plan_batch(bp, jd, n.n_start, precision == BIELCC_PREC_MIXED, item_cost);
+    TRY(ctx->ws.ensure(bp.ws_bytes));
+    TRY(ctx->scratch_small.ensure(256));
+    BatchDevPtrs d;
+    int l1 = 0, l2 = 0;
+    TRY_CUDA(batch_stage1(bp, ctx->ws.p, n.analytic_calc, n.n_start, ck, s, &d, &l1));
+    TRY_CUDA(cudaMemcpyAsync(ctx->h_total, d.total, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    TRY_CUDA(cudaStreamSynchronize(s));
+    const long long n_near = *ctx->h_total;
+    if (n_near > 0) TRY(ctx->pair_ws.ensure(batch_pair_ws_bytes(n_near)));
+    DNP dn{n.eps, n.rs, n.rs_seg, n.analytic_calc, n.n_start, n.n_start_seg, n.p_max, n.p_max_seg};
+    TRY_CUDA(batch_stage2(bp, d, n_near, ctx->pair_ws.p, dn, nullptr, s, &l2));
+    ctx->stats.kernel_launches += l1 + l2;
+    ctx->stats.far_launches += 1;
+    ctx->stats.far_pairs += pairs;
+    TRY(ws_release(ctx, s));
+    if (report) {
+        report->n_pairs = pairs;
+        report->n_near_pairs = n_near;
+    }
+    return BIELCC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bielcc_field_EH_batch(bielcc_ctx ctx, int n_jobs, const bielcc_field_job* jobs, const bielcc_numparam* np,
+                          int precision, void* stream, bielcc_report* report) {
+    TRY(enter(ctx));
+    if (n_jobs < 0 || (n_jobs > 0 && !jobs)) return set_error(BIELCC_ERR_ARG, "bad job list");
+    if (precision != BIELCC_PREC_FP64 && precision != BIELCC_PREC_MIXED)
+        return set_error(BIELCC_ERR_ARG, "unknown precision %d", precision);
+    NumParamH n = to_np(np);
+    TRY(check_np(n));
+    std::lock_guard<std::mutex> g(ctx->mu);
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    return field_batch_locked(ctx, n_jobs, jobs, n, precision, s, report, ctx->batch_item_cost);
+}
+
+int bielcc_batch_autotune(bielcc_ctx ctx, int n_jobs, const bielcc_field_job* jobs, const bielcc_numparam* np,
+                          int precision, void* stream, double* item_cost) {
+    TRY(enter(ctx));
+    if (n_jobs < 1 || !jobs) return set_error(BIELCC_ERR_ARG, "autotuning needs a non-empty batch");
+    NumParamH n = to_np(np);
+    TRY(check_np(n));
+    std::lock_guard<std::mutex> g(ctx->mu);
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    cudaEvent_t e0, e1;
+    TRY_CUDA(cudaEventCreate(&e0));
+    TRY_CUDA(cudaEventCreate(&e1));
+    const double candidates[] = {0.5e6, 1e6, 2e6, 4e6, 8e6, 16e6};
+    double best = ctx->batch_item_cost, best_ms = 1e30;
+    int rc = BIELCC_OK;
+    for (int rep = 0; rep < 2 && rc == BIELCC_OK; rep++) {  // first sweep warms up
+        for (double c : candidates) {
+            cudaEventRecord(e0, s);
+            rc = field_batch_locked(ctx, n_jobs, jobs, n, precision, s, nullptr, c);
+            if (rc != BIELCC_OK) break;
+            cudaEventRecord(e1, s);
+            cudaEventSynchronize(e1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (rep == 1 && ms < best_ms) {
+                best_ms = ms;
+                best = c;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != BIELCC_OK) return rc;
+    ctx->batch_item_cost = best;
+    if (item_cost) *item_cost = best;
+    return BIELCC_OK;
 }
 
 }  // extern "C"

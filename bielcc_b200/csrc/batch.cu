@@ -1,0 +1,552 @@
+// batch.cu — many field evaluations (meshes of uneven sizes, each with its own
+// points, wave number and 1..S right-hand sides) in ONE persistent launch.
+//
+// Work is cut into items (job, 32-point tile, cell range) and ordered by
+// estimated cost (largest first); each CTA of the persistent grid pulls the
+// next item from a device counter. An item walks its cell range in chunks:
+//   phase A — warp w evaluates the far-field moments (A1, T, G: 20 values,
+//             farnode.cuh) of cells w, w+4, ... of the chunk for its 32 points
+//             and stores them in shared memory (node tiles staged with 128-bit
+//             loads, one observation point per lane);
+//   phase B — the same threads contract the chunk's moments with every
+//             right-hand side staged in shared memory, R RHS per thread held in
+//             registers, and add the result into the job's partial sums.
+// Extra right-hand sides therefore cost ~72 FP32 operations per pair instead
+// of the 64-node integrand. Near cells (get_field.h:58) are flagged in the
+// job's near mask and handled by the FP64 near-pair path afterwards, exactly
+// as in the single-job pipeline. Summation order depends only on the job
+// itself (its ranges and chunks), never on the other jobs of the batch.
+#include <algorithm>
+#include <cstring>
+#include <type_traits>
+#include <vector>
+
+#include "../../include/bielcc_gpu.h"
+#include "farnode.cuh"
+#include "internal.h"
+#include "ops.cuh"
+#include "scan.cuh"
+
+namespace bielcc_gpu {
+
+constexpr int kBT = 128;  // threads per CTA: 4 warps x 32 points
+constexpr int kBP = 32;   // points per item tile
+constexpr int kBW = 4;    // warps
+constexpr int kSP = 64;   // right-hand sides staged per pass
+
+
+template <bool MIXED>
+struct BatchCfg {
+    using F = typename std::conditional<MIXED, float, double>::type;
+    using NodeT = typename std::conditional<MIXED, float4, double4>::type;
+    static constexpr int CH = MIXED ? 16 : 8;             // cells per chunk (n_start <= 8)
+    static constexpr int NODES = MIXED ? 1024 : 512;      // staged nodes
+    static constexpr int R = MIXED ? 4 : 2;               // RHS per thread in phase B
+    static constexpr size_t smem_bytes() {
+        return sizeof(NodeT) * NODES + sizeof(F) * CH * 20 * kBP + sizeof(F) * 2 * CH * kSP * 3 +
+               sizeof(double4) * CH + sizeof(double) * CH + CH * kBP + 64;
+    }
+};
+
+// acc[12] += contraction of one cell's moments m[20] (a1r, a1i, t[6][2], g[3][2])
+// with the current J = (jr, ji): E = A1 J + T J, H = G x J.
+template <typename F>
+BIELCC_D void contract12(const F* m, const F* jr, const F* ji, F* acc) {
+    const F a1r = m[0], a1i = m[1];
+    const int ti[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        F er = a1r * jr[a] - a1i * ji[a], ei = a1r * ji[a] + a1i * jr[a];
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            const F tr = m[2 + 2 * ti[a][b]], tim = m[3 + 2 * ti[a][b]];
+            er += tr * jr[b] - tim * ji[b];
+            ei += tr * ji[b] + tim * jr[b];
+        }
+        acc[2 * a] += er;
+        acc[2 * a + 1] += ei;
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const int b = (a + 1) % 3, c = (a + 2) % 3;
+        const F gbr = m[14 + 2 * b], gbi = m[15 + 2 * b], gcr = m[14 + 2 * c], gci = m[15 + 2 * c];
+        acc[6 + 2 * a] += (gbr * jr[c] - gbi * ji[c]) - (gcr * jr[b] - gci * ji[b]);
+        acc[6 + 2 * a + 1] += (gbr * ji[c] + gbi * jr[c]) - (gcr * ji[b] + gci * jr[b]);
+    }
+}
+
+// Phase A of one (point, cell) pair: the 20 far moments times e^{ik r0}.
+// CK (complex k) is a property of the job, so every item of a job takes the
+// same code path whatever else is in the batch.
+template <bool MIXED, bool CK>
+BIELCC_D void batch_moments(const typename BatchCfg<MIXED>::NodeT* nd, int nn, const double* x, const double4& ci,
+                            double d, double rho, cplx k, double k2r, double k2i,
+                            typename BatchCfg<MIXED>::F* mom) {
+    using F = typename BatchCfg<MIXED>::F;
+    double P0r = 1.0, P0i = 0.0;
+    Moments<F> m;
+    m.zero();
+    if constexpr (MIXED) {
+        const float Xx = (float)(x[0] - ci.x), Xy = (float)(x[1] - ci.y), Xz = (float)(x[2] - ci.z);
+        const float r0f = (float)d, r0sq = (float)(d * d);
+        double sn, cs;
+        sincos(k.re * d, &sn, &cs);
+        if (CK) {
+            const double am = exp(-k.im * d);
+            sn *= am;
+            cs *= am;
+        }
+        P0r = cs;
+        P0i = sn;
+        const float kr_ = (float)k.re, ki_ = (float)k.im, k2rf = (float)k2r, k2if = (float)k2i;
+        const int mode = phase_mode((float)fabs(k.re) * (float)rho);
+#define BIELCC_BNODE(MODE_)                                                                            \
+    _Pragma("unroll 4") for (int i = 0; i < nn; i++)                                                    \
+        far_node_f32<CK, MODE_>(m, Xx, Xy, Xz, r0f, r0sq, nd[i], kr_, ki_, k2rf, k2if);
+        switch (mode) {
+            case 0: BIELCC_BNODE(0) break;
+            case 1: BIELCC_BNODE(1) break;
+            case 2: BIELCC_BNODE(2) break;
+            case 3: BIELCC_BNODE(3) break;
+            default: BIELCC_BNODE(4) break;
+        }
+#undef BIELCC_BNODE
+    } else {
+        const bool split = !CK && fabs(k.re) * rho * (1.0 + 1e-6) <= 0.5;
+        if (split) {
+            double sn, cs;
+            sincos(k.re * d, &sn, &cs);
+            P0r = cs;
+            P0i = sn;
+            for (int i = 0; i < nn; i++) {
+                const double4 v = nd[i];
+                far_node_f64<CK, true>(m, x[0] - v.x, x[1] - v.y, x[2] - v.z, v.w, k, k2r, k2i, d);
+            }
+        } else {
+            for (int i = 0; i < nn; i++) {
+                const double4 v = nd[i];
+                far_node_f64<CK, false>(m, x[0] - v.x, x[1] - v.y, x[2] - v.z, v.w, k, k2r, k2i, d);
+            }
+        }
+    }
+    // moments x e^{ik r0}; R_Rot_Colloc is 0 at the cell centre
+    const F pr = (F)P0r, pi = (F)P0i;
+    mom[0] = m.a1r * pr - m.a1i * pi;
+    mom[1] = m.a1r * pi + m.a1i * pr;
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        mom[2 + 2 * q] = m.t[q][0] * pr - m.t[q][1] * pi;
+        mom[3 + 2 * q] = m.t[q][0] * pi + m.t[q][1] * pr;
+    }
+    if (!(d < kMachineZero)) {
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            mom[14 + 2 * q] = m.g[q][0] * pr - m.g[q][1] * pi;
+            mom[15 + 2 * q] = m.g[q][0] * pi + m.g[q][1] * pr;
+        }
+    }
+}
+
+template <bool MIXED>
+__global__ void __launch_bounds__(kBT, 2) batch_far_kernel(const JobDev* __restrict__ jobs,
+                                                         const BatchItem* __restrict__ items, int n_items,
+                                                         int* __restrict__ counter, double analytic_calc, int n_start) {
+    using C = BatchCfg<MIXED>;
+    using F = typename C::F;
+    using NodeT = typename C::NodeT;
+    extern __shared__ __align__(16) unsigned char smem[];
+    NodeT* s_nodes = (NodeT*)smem;
+    F* s_mom = (F*)(s_nodes + C::NODES);                 // [CH][20][kBP]
+    F* s_j = s_mom + C::CH * 20 * kBP;                   // [CH][kSP][3][2]
+    double4* s_cell = (double4*)(s_j + C::CH * kSP * 6);  // centre, diam
+    double* s_rho = (double*)(s_cell + C::CH);
+    unsigned char* s_near = (unsigned char*)(s_rho + C::CH);  // [CH][kBP]
+    __shared__ int s_item;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nn = n_start * n_start;
+    const int ch = max(1, min(C::CH, C::NODES / nn));
+
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int it = s_item;
+        if (it >= n_items) break;
+        const BatchItem bi = items[it];
+        const JobDev& jb = jobs[bi.job];
+        const int P = jb.n_pts, N = jb.n_cells, S = jb.n_rhs;
+        const int p = bi.tile * kBP + lane;
+        const bool live = p < P;
+        double x[3] = {0., 0., 0.};
+        if (live)
+            for (int g = 0; g < 3; g++) x[g] = jb.pts[3 * (size_t)p + g];
+        const int cb = bi.range * jb.cells_per_range;
+        const int ce = min(N, cb + jb.cells_per_range);
+        const cplx k = jb.k;
+        const double k2r = k.re * k.re - k.im * k.im, k2i = 2.0 * k.re * k.im;
+        unsigned nbits = 0;
+
+        for (int s0 = 0; s0 < S; s0 += kSP) {
+            const int sp = min(kSP, S - s0);
+            for (int c0 = cb; c0 < ce; c0 += ch) {
+                const int nc = min(ch, ce - c0);
+                __syncthreads();
+                // stage node tables, cell rows and the chunk's currents
+                if constexpr (MIXED) {
+                    const float4* src = jb.nodes32 + (size_t)c0 * nn;
+                    for (int i = threadIdx.x; i < nc * nn; i += kBT) s_nodes[i] = __ldg(src + i);
+                } else {
+                    const double2* src = reinterpret_cast<const double2*>(jb.nodes64 + (size_t)c0 * nn);
+                    double2* dst = reinterpret_cast<double2*>(s_nodes);
+                    for (int i = threadIdx.x; i < 2 * nc * nn; i += kBT) dst[i] = __ldg(src + i);
+                }
+                for (int i = threadIdx.x; i < nc; i += kBT) {
+                    const CellGeo& gg = jb.geo[c0 + i];
+                    s_cell[i] = make_double4(gg.c[0], gg.c[1], gg.c[2], gg.diam);
+                    s_rho[i] = (double)jb.rho32[c0 + i];
+                }
+                for (int i = threadIdx.x; i < nc * sp * 3; i += kBT) {
+                    const int cc = i / (sp * 3), rem = i - cc * sp * 3, sl = rem / 3, g = rem - sl * 3;
+                    const cplx v = jb.J[((size_t)(s0 + sl) * N + (c0 + cc)) * 3 + g];
+                    F* d = s_j + ((size_t)(cc * kSP + sl) * 3 + g) * 2;
+                    d[0] = (F)v.re;
+                    d[1] = (F)v.im;
+                }
+                __syncthreads();
+                // phase A: moments of cells warp, warp+4, ... for this warp's 32 points
+                for (int cc = warp; cc < nc; cc += kBW) {
+                    const double4 ci = s_cell[cc];
+                    const double cen[3] = {ci.x, ci.y, ci.z};
+                    double d;
+                    const bool nr = is_near(x, cen, ci.w, analytic_calc, &d);
+                    const bool far = !nr && live;
+                    s_near[cc * kBP + lane] = nr ? 1 : 0;
+                    F mom[20];
+#pragma unroll
+                    for (int q = 0; q < 20; q++) mom[q] = 0;
+                    if (far) {
+                        const NodeT* nd = s_nodes + cc * nn;
+                        if (k.im != 0.0)
+                            batch_moments<MIXED, true>(nd, nn, x, ci, d, s_rho[cc], k, k2r, k2i, mom);
+                        else
+                            batch_moments<MIXED, false>(nd, nn, x, ci, d, s_rho[cc], k, k2r, k2i, mom);
+                    }
+#pragma unroll
+                    for (int q = 0; q < 20; q++) s_mom[(cc * 20 + q) * kBP + lane] = mom[q];
+                }
+                __syncthreads();
+                // near-cell mask (first RHS pass): warp 0 owns the words of its points
+                if (s0 == 0 && warp == 0) {
+                    for (int cc = 0; cc < nc; cc++) {
+                        const int c = c0 + cc;
+                        nbits |= (unsigned)s_near[cc * kBP + lane] << (c & 31);
+                        if ((c & 31) == 31 || c == ce - 1) {
+                            if (live) jb.mask[(size_t)(c >> 5) * P + p] = nbits;
+                            nbits = 0;
+                        }
+                    }
+                }
+                // phase B: RHS s = sb + warp + 4 j, j < R, contracted over the chunk's cells
+                for (int sb = 0; sb < sp; sb += kBW * C::R) {
+                    F acc[C::R][12];
+#pragma unroll
+                    for (int j = 0; j < C::R; j++)
+#pragma unroll
+                        for (int q = 0; q < 12; q++) acc[j][q] = 0;
+                    for (int cc = 0; cc < nc; cc++) {
+                        F m[20];
+#pragma unroll
+                        for (int q = 0; q < 20; q++) m[q] = s_mom[(cc * 20 + q) * kBP + lane];
+#pragma unroll
+                        for (int j = 0; j < C::R; j++) {
+                            const int sl = sb + warp + kBW * j;
+                            if (sl < sp) {
+                                const F* jj = s_j + (size_t)(cc * kSP + sl) * 6;
+                                const F jr[3] = {jj[0], jj[2], jj[4]}, ji[3] = {jj[1], jj[3], jj[5]};
+                                contract12<F>(m, jr, ji, acc[j]);
+                            }
+                        }
+                    }
+                    if (live) {
+#pragma unroll
+                        for (int j = 0; j < C::R; j++) {
+                            const int sl = sb + warp + kBW * j;
+                            if (sl >= sp) continue;
+                            double* dst =
+                                jb.partial + (((size_t)bi.range * S + (s0 + sl)) * 12) * (size_t)P + p;
+                            if (c0 == cb) {
+#pragma unroll
+                                for (int q = 0; q < 12; q++) dst[(size_t)q * P] = (double)acc[j][q];
+                            } else {
+#pragma unroll
+                                for (int q = 0; q < 12; q++) dst[(size_t)q * P] += (double)acc[j][q];
+                            }
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- batched near path + finalize
+__global__ void batch_near_count_kernel(const JobDev* __restrict__ jobs, const int* __restrict__ pt_job, int total,
+                                        long long* __restrict__ counts) {
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    const JobDev& jb = jobs[pt_job[g]];
+    const int p = g - jb.pt_off;
+    long long n = 0;
+    for (int w = 0; w < jb.n_words; w++) n += __popc(jb.mask[(size_t)w * jb.n_pts + p]);
+    counts[g] = n;
+}
+
+__global__ void batch_near_fill_kernel(const JobDev* __restrict__ jobs, const int* __restrict__ pt_job, int total,
+                                       const long long* __restrict__ offs, int* __restrict__ pair_cell,
+                                       int* __restrict__ pair_gpt) {
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    long long o = offs[g];
+    if (offs[g + 1] == o) return;
+    const JobDev& jb = jobs[pt_job[g]];
+    const int p = g - jb.pt_off;
+    for (int w = 0; w < jb.n_words; w++) {
+        unsigned b = jb.mask[(size_t)w * jb.n_pts + p];
+        while (b) {
+            const int bit = __ffs(b) - 1;
+            b &= b - 1;
+            pair_cell[o] = w * 32 + bit;
+            pair_gpt[o] = g;
+            o++;
+        }
+    }
+}
+
+__global__ void batch_near_pair_kernel(const JobDev* __restrict__ jobs, const int* __restrict__ pt_job,
+                                       const int* __restrict__ pair_cell, const int* __restrict__ pair_gpt,
+                                       long long n_pairs, DNP np, cplx* __restrict__ out) {
+    long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n_pairs) return;
+    const int g = pair_gpt[q], c = pair_cell[q];
+    const JobDev& jb = jobs[pt_job[g]];
+    const int p = g - jb.pt_off;
+    DCell cl;
+    cl.nv = jb.nv;
+    for (int v = 0; v < jb.nv; v++)
+        for (int a = 0; a < 3; a++) cl.v[v][a] = jb.verts[((size_t)c * jb.nv + v) * 3 + a];
+    double x[3] = {jb.pts[3 * (size_t)p], jb.pts[3 * (size_t)p + 1], jb.pts[3 * (size_t)p + 2]};
+    near_pair_moments(x, cl, jb.k, np, out + q * 13);
+}
+
+__global__ void batch_finalize_kernel(const JobDev* __restrict__ jobs, const int* __restrict__ pt_job, int total,
+                                      const long long* __restrict__ offs, const int* __restrict__ pair_cell,
+                                      const cplx* __restrict__ moments, unsigned long long* nonfinite) {
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    const JobDev& jb = jobs[pt_job[g]];
+    const int p = g - jb.pt_off;
+    const size_t P = jb.n_pts;
+    const double* x = jb.pts + 3 * (size_t)p;
+    double cs = 1., sn = 0.;
+    if (jb.add_E || jb.add_H) sincos(jb.kvec[0] * x[0] + jb.kvec[1] * x[1] + jb.kvec[2] * x[2], &sn, &cs);
+    double kx0[3];
+    cross3(jb.kvec, jb.e0, kx0);
+    bool bad = false;
+    for (int s = 0; s < jb.n_rhs; s++) {
+        double v[12];
+        for (int q = 0; q < 12; q++) v[q] = 0.;
+        for (int r = 0; r < jb.ranges; r++) {
+            const double* src = jb.partial + (((size_t)r * jb.n_rhs + s) * 12) * P + p;
+            for (int q = 0; q < 12; q++) v[q] += src[(size_t)q * P];
+        }
+        cplx E[3], H[3];
+        for (int a = 0; a < 3; a++) {
+            E[a] = mk(v[2 * a], v[2 * a + 1]) * kInvFourPi;
+            H[a] = mk(v[6 + 2 * a], v[6 + 2 * a + 1]) * kInvFourPi;
+        }
+        if (offs) {
+            for (long long q = offs[g]; q < offs[g + 1]; q++) {
+                const int c = pair_cell[q];
+                const cplx* o = moments + q * 13;
+                const cplx* j = jb.J + ((size_t)s * jb.n_cells + c) * 3;
+                for (int a = 0; a < 3; a++)
+                    E[a] += o[0] * j[a] + o[1 + 3 * a] * j[0] + o[2 + 3 * a] * j[1] + o[3 + 3 * a] * j[2];
+                cplx h[3];
+                ccross_cc(o + 10, j, h);
+                for (int a = 0; a < 3; a++) H[a] += h[a];
+            }
+        }
+        for (int a = 0; a < 3; a++) E[a] = E[a] * jb.mult;
+        if (jb.add_E)
+            for (int a = 0; a < 3; a++) E[a] += mk(jb.e0[a] * cs, jb.e0[a] * sn);
+        if (jb.add_H)
+            for (int a = 0; a < 3; a++) H[a] += mk(kx0[a] * cs * jb.h_scale, kx0[a] * sn * jb.h_scale);
+        cplx* eo = reinterpret_cast<cplx*>(jb.E) + ((size_t)s * P + p) * 3;
+        for (int a = 0; a < 3; a++) {
+            eo[a] = E[a];
+            bad |= !isfinite(E[a].re) || !isfinite(E[a].im);
+        }
+        if (jb.H) {
+            cplx* ho = reinterpret_cast<cplx*>(jb.H) + ((size_t)s * P + p) * 3;
+            for (int a = 0; a < 3; a++) {
+                ho[a] = H[a];
+                bad |= !isfinite(H[a].re) || !isfinite(H[a].im);
+            }
+        }
+    }
+    if (bad && nonfinite) atomicAdd(nonfinite, 1ull);
+}
+
+// ---------------------------------------------------------------- host side
+static size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+
+int batch_grid(bool mixed) {
+    // resident CTAs of the persistent grid (dynamic shared memory opted in once)
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    size_t smem = mixed ? BatchCfg<true>::smem_bytes() : BatchCfg<false>::smem_bytes();
+    if (mixed) {
+        cudaFuncSetAttribute(batch_far_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_far_kernel<true>, kBT, smem);
+    } else {
+        cudaFuncSetAttribute(batch_far_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_far_kernel<false>, kBT, smem);
+    }
+    return sms * std::max(1, per);
+}
+
+// Cuts every job into items (32-point tile, range of cells). The range length
+// depends only on the job itself and on `item_cost` (estimated node
+// evaluations per item, a per-context autotuned constant), never on the other
+// jobs of the batch, so a job's summation order - and its result - is the same
+// alone and in any mix. Ranges are multiples of 32 cells (near-mask words).
+void plan_batch(BatchPlan& bp, const std::vector<JobDev>& jobs_in, int n_start, bool mixed, double item_cost) {
+    bp.jobs = jobs_in;
+    bp.mixed = mixed;
+    bp.grid = batch_grid(mixed);
+    const double nodes = (double)n_start * n_start;
+    bp.items.clear();
+    bp.pt_job.clear();
+    std::vector<double> cost;
+    int pt_off = 0;
+    for (size_t ji = 0; ji < bp.jobs.size(); ji++) {
+        JobDev& j = bp.jobs[ji];
+        j.pt_off = pt_off;
+        pt_off += j.n_pts;
+        for (int p = 0; p < j.n_pts; p++) bp.pt_job.push_back((int)ji);
+        const double per_cell = (double)kBP * (nodes + 1.2 * j.n_rhs);
+        // at most kMaxRanges ranges per job: bounds the partial sums to kMaxRanges x (S x 12 x P) doubles
+        constexpr int kMaxRanges = 6;
+        int cpr = (int)std::min<double>(j.n_cells, std::max(32.0, item_cost / per_cell));
+        cpr = std::max(cpr, (j.n_cells + kMaxRanges - 1) / kMaxRanges);
+        cpr = (cpr + 31) / 32 * 32;
+        j.cells_per_range = cpr;
+        j.ranges = (j.n_cells + cpr - 1) / cpr;
+        j.n_words = (j.n_cells + 31) / 32;
+        const int tiles = (j.n_pts + kBP - 1) / kBP;
+        for (int t = 0; t < tiles; t++)
+            for (int r = 0; r < j.ranges; r++) {
+                bp.items.push_back(BatchItem{(int)ji, t, r, 0});
+                const int cells = std::min(cpr, j.n_cells - r * cpr);
+                cost.push_back((double)cells * per_cell);
+            }
+        bp.ws_bytes += al256((size_t)j.ranges * j.n_rhs * 12 * j.n_pts * sizeof(double)) +
+                       al256((size_t)j.n_words * j.n_pts * sizeof(unsigned));
+    }
+    bp.total_pts = pt_off;
+    std::vector<int> order(bp.items.size());
+    for (size_t i = 0; i < order.size(); i++) order[i] = (int)i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    std::vector<BatchItem> sorted(bp.items.size());
+    for (size_t i = 0; i < order.size(); i++) sorted[i] = bp.items[order[i]];
+    bp.items.swap(sorted);
+    const size_t T = bp.total_pts;
+    bp.ws_bytes += al256(bp.jobs.size() * sizeof(JobDev)) + al256(bp.items.size() * sizeof(BatchItem)) +
+                   al256(T * sizeof(int)) + 2 * al256((T + 1) * sizeof(long long)) + 3 * 256;
+}
+
+// Enqueues stage 1 (far kernel, near counting, scan) of a planned batch into
+// `ws`; `host_tables` receive the device table pointers for stage 2.
+
+cudaError_t batch_stage1(BatchPlan& bp, void* ws, double analytic_calc, int n_start, bool ck, cudaStream_t s,
+                         BatchDevPtrs* out, int* launches) {
+    char* w = (char*)ws;
+    for (auto& j : bp.jobs) {
+        j.partial = (double*)w;
+        w += al256((size_t)j.ranges * j.n_rhs * 12 * j.n_pts * sizeof(double));
+        j.mask = (unsigned*)w;
+        w += al256((size_t)j.n_words * j.n_pts * sizeof(unsigned));
+    }
+    const size_t T = bp.total_pts;
+    BatchDevPtrs d;
+    d.jobs = (JobDev*)w;
+    w += al256(bp.jobs.size() * sizeof(JobDev));
+    d.items = (BatchItem*)w;
+    w += al256(bp.items.size() * sizeof(BatchItem));
+    d.pt_job = (int*)w;
+    w += al256(T * sizeof(int));
+    d.counts = (long long*)w;
+    w += al256((T + 1) * sizeof(long long));
+    d.offs = (long long*)w;
+    w += al256((T + 1) * sizeof(long long));
+    d.total = (long long*)w;
+    w += 256;
+    d.counter = (int*)w;
+    cudaError_t e = cudaMemcpyAsync(d.jobs, bp.jobs.data(), bp.jobs.size() * sizeof(JobDev), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && !bp.items.empty())
+        e = cudaMemcpyAsync(d.items, bp.items.data(), bp.items.size() * sizeof(BatchItem), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && T) e = cudaMemcpyAsync(d.pt_job, bp.pt_job.data(), T * sizeof(int), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d.counter, 0, sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    const size_t smem = bp.mixed ? BatchCfg<true>::smem_bytes() : BatchCfg<false>::smem_bytes();
+    const int n_items = (int)bp.items.size();
+    if (n_items > 0) {
+        if (bp.mixed)
+            batch_far_kernel<true><<<bp.grid, kBT, smem, s>>>(d.jobs, d.items, n_items, d.counter, analytic_calc, n_start);
+        else
+            batch_far_kernel<false><<<bp.grid, kBT, smem, s>>>(d.jobs, d.items, n_items, d.counter, analytic_calc,
+                                                              n_start);
+    }
+    const int tb = (int)((T + 127) / 128);
+    if (T) batch_near_count_kernel<<<tb, 128, 0, s>>>(d.jobs, d.pt_job, (int)T, d.counts);
+    scan_kernel<<<1, 1024, 0, s>>>(d.counts, (int)T, d.offs, d.total);
+    *out = d;
+    *launches = (n_items > 0 ? 1 : 0) + (T ? 1 : 0) + 1;
+    return cudaGetLastError();
+}
+
+size_t batch_pair_ws_bytes(long long n_near) {
+    return al256((size_t)n_near * 13 * sizeof(cplx)) + 2 * al256((size_t)n_near * sizeof(int));
+}
+
+cudaError_t batch_stage2(BatchPlan& bp, const BatchDevPtrs& d, long long n_near, void* pair_ws, const DNP& np,
+                         unsigned long long* d_nonfinite, cudaStream_t s, int* launches) {
+    const size_t T = bp.total_pts;
+    const int tb = (int)((T + 127) / 128);
+    cplx* moments = nullptr;
+    int* pair_cell = nullptr;
+    *launches = 0;
+    if (n_near > 0) {
+        char* pw = (char*)pair_ws;
+        moments = (cplx*)pw;
+        pw += al256((size_t)n_near * 13 * sizeof(cplx));
+        pair_cell = (int*)pw;
+        pw += al256((size_t)n_near * sizeof(int));
+        int* pair_gpt = (int*)pw;
+        batch_near_fill_kernel<<<tb, 128, 0, s>>>(d.jobs, d.pt_job, (int)T, d.offs, pair_cell, pair_gpt);
+        batch_near_pair_kernel<<<(int)((n_near + 127) / 128), 128, 0, s>>>(d.jobs, d.pt_job, pair_cell, pair_gpt,
+                                                                          n_near, np, moments);
+        *launches += 2;
+    }
+    if (T) {
+        batch_finalize_kernel<<<tb, 128, 0, s>>>(d.jobs, d.pt_job, (int)T, n_near > 0 ? d.offs : nullptr, pair_cell,
+                                                  moments, d_nonfinite);
+        *launches += 1;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace bielcc_gpu

@@ -1,0 +1,221 @@
+// farnode.cuh — the per-node far-field integrand shared by the far kernels
+// (field.cu, batch.cu): F_RotRotSimplePot_H (kernel_lib.h:453-492) and
+// F_GradSimplePot_H (kernel_lib.h:295-313) evaluated together at one
+// quadrature node and accumulated as J-independent moments of one cell:
+//   A1 = sum w e f1,  T = sum w e f2 d^ d^T (6),  G = sum w e (ikr - 1)/r^3 d (3)
+// so that K_RotRot_Far = (A1 J + T J)/4pi and R_Rot_Colloc = (G x J)/4pi.
+// FP64 and FP32 (phase split relative to the cell centre) forms.
+#pragma once
+#include "common.cuh"
+
+namespace bielcc_gpu {
+
+// Near decision of get_field.h:58 with the reference's rounding.
+BIELCC_D bool is_near(const double* x, const double* c, double diam, double analytic_calc, double* d_out) {
+    double d = dist3_rn(x, c);
+    *d_out = d;
+    return d < __dmul_rn(analytic_calc, diam);
+}
+
+// Per-thread moment accumulators of one cell.
+template <typename F>
+struct Moments {
+    F a1r, a1i;
+    F t[6][2];  // xx, xy, xz, yy, yz, zz
+    F g[3][2];
+    BIELCC_D void zero() {
+        a1r = a1i = 0;
+        for (int i = 0; i < 6; i++) t[i][0] = t[i][1] = 0;
+        for (int i = 0; i < 3; i++) g[i][0] = g[i][1] = 0;
+    }
+};
+
+// e^{i t} in FP64 for |t| <= 0.5 from its Taylor series (sin to t^13, cos to
+// t^14: truncation below 3e-17).
+BIELCC_D void sincos_taylor64(double t, double* s, double* c) {
+    double t2 = t * t;
+    double ps = fma(t2, -1.6059043836821613e-10, 2.5052108385441720e-08);
+    ps = fma(t2, ps, -2.7557319223985893e-06);
+    ps = fma(t2, ps, 1.9841269841269841e-04);
+    ps = fma(t2, ps, -8.3333333333333333e-03);
+    ps = fma(t2, ps, 1.6666666666666667e-01);
+    *s = t - t * t2 * ps;
+    double pc = fma(t2, 1.1470745597729725e-11, -2.0876756987868099e-09);
+    pc = fma(t2, pc, 2.7557319223985891e-07);
+    pc = fma(t2, pc, -2.4801587301587302e-05);
+    pc = fma(t2, pc, 1.3888888888888889e-03);
+    pc = fma(t2, pc, -4.1666666666666667e-02);
+    pc = fma(t2, pc, 0.5);
+    *c = 1.0 - t2 * pc;
+}
+
+// One far node, FP64. dx = x - y; w = node weight. Real k (CK = false) or
+// complex k. F_RotRotSimplePot_H (kernel_lib.h:453-492) and
+// F_GradSimplePot_H (kernel_lib.h:295-313) share r, 1/r and e^{ikr}.
+// SPLIT: the phase is taken relative to r0 = |x - centre| (the moments are
+// multiplied by e^{ik r0} once per cell) and e^{ik (r - r0)} comes from the
+// Taylor series; otherwise e^{ikr} from sincos per node.
+template <bool CK, bool SPLIT>
+BIELCC_D void far_node_f64(Moments<double>& m, double dx, double dy, double dz, double w, cplx k, double k2r,
+                           double k2i, double r0) {
+    double r2 = dx * dx + dy * dy + dz * dz;
+    double ir = rsqrt(r2);
+    double r = r2 * ir;
+    double s, c;
+    if (SPLIT) {
+        sincos_taylor64(k.re * (r - r0), &s, &c);
+    } else {
+        sincos(k.re * r, &s, &c);
+        if (CK) {
+            double a = exp(-k.im * r);
+            s *= a;
+            c *= a;
+        }
+    }
+    double ir2 = ir * ir, ir3 = ir2 * ir;
+    double er = w * c, ei = w * s;
+    if (r >= kMachineZero) {  // F_RotRotSimplePot_H is 0 below MACHINE_ZERO
+        double f1r, f1i, f2r, f2i;
+        if (CK) {
+            f1r = k2r * ir - ir3 - k.im * ir2;
+            f1i = k.re * ir2 + k2i * ir;
+            f2r = 3.0 * ir3 + 3.0 * k.im * ir2 - k2r * ir;
+            f2i = -3.0 * k.re * ir2 - k2i * ir;
+        } else {
+            f1r = k2r * ir - ir3;
+            f1i = k.re * ir2;
+            f2r = 3.0 * ir3 - k2r * ir;
+            f2i = -3.0 * k.re * ir2;
+        }
+        m.a1r += er * f1r - ei * f1i;
+        m.a1i += er * f1i + ei * f1r;
+        double a2r = (er * f2r - ei * f2i) * ir2, a2i = (er * f2i + ei * f2r) * ir2;
+        double dd[6] = {dx * dx, dx * dy, dx * dz, dy * dy, dy * dz, dz * dz};
+#pragma unroll
+        for (int q = 0; q < 6; q++) {
+            m.t[q][0] += a2r * dd[q];
+            m.t[q][1] += a2i * dd[q];
+        }
+    }
+    // (ikr - 1) with ikr = (-k.im r, k.re r)
+    double ur = CK ? (-k.im * r - 1.0) : -1.0, ui = k.re * r;
+    double gr = (er * ur - ei * ui) * ir3, gi = (er * ui + ei * ur) * ir3;
+    m.g[0][0] += gr * dx;
+    m.g[0][1] += gi * dx;
+    m.g[1][0] += gr * dy;
+    m.g[1][1] += gi * dy;
+    m.g[2][0] += gr * dz;
+    m.g[2][1] += gi * dz;
+}
+
+// Taylor sine / cosine on |t| <= 1 (truncation below 2.6e-8), FP32.
+BIELCC_D void sincos_poly(float t, float* s, float* c) {
+    float t2 = t * t;
+    float ps = fmaf(t2, 2.7557319e-6f, -1.9841270e-4f);
+    ps = fmaf(t2, ps, 8.3333333e-3f);
+    ps = fmaf(t2, ps, -1.6666667e-1f);
+    ps = fmaf(t2, ps, 1.0f);
+    *s = t * ps;
+    float pc = fmaf(t2, -2.7557319e-7f, 2.4801587e-5f);
+    pc = fmaf(t2, pc, -1.3888889e-3f);
+    pc = fmaf(t2, pc, 4.1666667e-2f);
+    pc = fmaf(t2, pc, -0.5f);
+    *c = fmaf(t2, pc, 1.0f);
+}
+
+// Short Taylor sine / cosine for |t| <= 0.25 (truncation below 1.3e-8).
+BIELCC_D void sincos_short(float t, float* s, float* c) {
+    float t2 = t * t;
+    float ps = fmaf(t2, 8.3333333e-3f, -1.6666667e-1f);
+    *s = t * fmaf(t2, ps, 1.0f);
+    float pc = fmaf(t2, -1.3888889e-3f, 4.1666667e-2f);
+    pc = fmaf(t2, pc, -0.5f);
+    *c = fmaf(t2, pc, 1.0f);
+}
+
+// e^{i theta} for a per-cell bound on |theta| (uniform over the CTA, so the
+// mode is a template argument of the node loop): 0 -> |theta| <= 0.25 short
+// polynomial; 1 -> <= 1; 2 -> <= 2 (half angle, one doubling); 3 -> <= 4 (two
+// doublings); 4 -> accurate sincosf.
+template <int MODE>
+BIELCC_D void phase_f32(float th, float* s, float* c) {
+    if constexpr (MODE == 0) {
+        sincos_short(th, s, c);
+    } else if constexpr (MODE == 4) {
+        sincosf(th, s, c);
+    } else {
+        constexpr int H = MODE - 1;
+        float ss, cc;
+        sincos_poly(th * (H == 0 ? 1.f : (H == 1 ? 0.5f : 0.25f)), &ss, &cc);
+#pragma unroll
+        for (int h = 0; h < H; h++) {
+            float ns = 2.f * ss * cc;
+            cc = fmaf(cc, cc, -ss * ss);
+            ss = ns;
+        }
+        *s = ss;
+        *c = cc;
+    }
+}
+
+BIELCC_HD int phase_mode(float th) {
+    return th <= 0.25f ? 0 : (th <= 1.f ? 1 : (th <= 2.f ? 2 : (th <= 4.f ? 3 : 4)));
+}
+
+// One far node, FP32, relative to the cell centre: X = x - centre (FP32),
+// node delta = y - centre, r0 = |X| (FP64 rounded), phase relative to r0.
+template <bool CK, int MODE>
+BIELCC_D void far_node_f32(Moments<float>& m, float Xx, float Xy, float Xz, float r0, float r0sq, float4 nd, float kr_,
+                           float ki_, float k2r, float k2i) {
+    float tx = fmaf(-2.f, Xx, nd.x), ty = fmaf(-2.f, Xy, nd.y), tz = fmaf(-2.f, Xz, nd.z);
+    float q = fmaf(nd.x, tx, fmaf(nd.y, ty, nd.z * tz));  // |x-y|^2 - r0^2
+    float r2 = r0sq + q;
+    float ir = rsqrtf(r2);
+    float r = r2 * ir;
+    float dr = __fdividef(q, r + r0);
+    float s, c;
+    phase_f32<MODE>(kr_ * dr, &s, &c);
+    float w = nd.w;
+    if (CK) w *= __expf(-ki_ * dr);
+    float dx = Xx - nd.x, dy = Xy - nd.y, dz = Xz - nd.z;
+    float ir2 = ir * ir, ir3 = ir2 * ir;
+    float er = w * c, ei = w * s;
+    float f1r, f1i, f2r, f2i;
+    if (CK) {
+        f1r = k2r * ir - ir3 - ki_ * ir2;
+        f1i = kr_ * ir2 + k2i * ir;
+        f2r = 3.f * ir3 + 3.f * ki_ * ir2 - k2r * ir;
+        f2i = -3.f * kr_ * ir2 - k2i * ir;
+    } else {
+        f1r = k2r * ir - ir3;
+        f1i = kr_ * ir2;
+        f2r = 3.f * ir3 - k2r * ir;
+        f2i = -3.f * kr_ * ir2;
+    }
+    m.a1r = fmaf(er, f1r, fmaf(-ei, f1i, m.a1r));
+    m.a1i = fmaf(er, f1i, fmaf(ei, f1r, m.a1i));
+    float a2r = (er * f2r - ei * f2i) * ir2, a2i = (er * f2i + ei * f2r) * ir2;
+    float bx_r = a2r * dx, bx_i = a2i * dx, by_r = a2r * dy, by_i = a2i * dy, bz_r = a2r * dz, bz_i = a2i * dz;
+    m.t[0][0] = fmaf(bx_r, dx, m.t[0][0]);
+    m.t[0][1] = fmaf(bx_i, dx, m.t[0][1]);
+    m.t[1][0] = fmaf(bx_r, dy, m.t[1][0]);
+    m.t[1][1] = fmaf(bx_i, dy, m.t[1][1]);
+    m.t[2][0] = fmaf(bx_r, dz, m.t[2][0]);
+    m.t[2][1] = fmaf(bx_i, dz, m.t[2][1]);
+    m.t[3][0] = fmaf(by_r, dy, m.t[3][0]);
+    m.t[3][1] = fmaf(by_i, dy, m.t[3][1]);
+    m.t[4][0] = fmaf(by_r, dz, m.t[4][0]);
+    m.t[4][1] = fmaf(by_i, dz, m.t[4][1]);
+    m.t[5][0] = fmaf(bz_r, dz, m.t[5][0]);
+    m.t[5][1] = fmaf(bz_i, dz, m.t[5][1]);
+    float ur = CK ? (-ki_ * r - 1.f) : -1.f, ui = kr_ * r;
+    float gr = (er * ur - ei * ui) * ir3, gi = (er * ui + ei * ur) * ir3;
+    m.g[0][0] = fmaf(gr, dx, m.g[0][0]);
+    m.g[0][1] = fmaf(gi, dx, m.g[0][1]);
+    m.g[1][0] = fmaf(gr, dy, m.g[1][0]);
+    m.g[1][1] = fmaf(gi, dy, m.g[1][1]);
+    m.g[2][0] = fmaf(gr, dz, m.g[2][0]);
+    m.g[2][1] = fmaf(gi, dz, m.g[2][1]);
+}
+
+}  // namespace bielcc_gpu

@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "common.cuh"
 
 namespace bielcc_gpu {
@@ -95,5 +97,62 @@ struct AssembleLaunch {
 size_t assemble_ws_base_bytes(const AssembleLaunch& a);
 cudaError_t assemble_stage1(const AssembleLaunch& a, void* ws, long long* d_total, cudaStream_t s);
 cudaError_t assemble_stage2(const AssembleLaunch& a, void* ws, long long n_near, void* pair_ws, cudaStream_t s);
+
+
+// ---- batch.cu: many field jobs in one persistent launch
+struct JobDev {
+    const CellGeo* geo;
+    const float4* nodes32;
+    const double4* nodes64;
+    const float* rho32;
+    const double* verts;
+    int nv, n_cells;
+    const double* pts;
+    int n_pts, pt_off;
+    const cplx* J;
+    int n_rhs;
+    cplx k, mult;
+    double kvec[3], e0[3], h_scale;
+    int add_E, add_H;
+    double* E;
+    double* H;
+    double* partial;  // [ranges][S][12][P]
+    unsigned* mask;   // [words][P]
+    int n_words, ranges, cells_per_range;
+};
+
+struct BatchItem {
+    int job, tile, range, pad;
+};
+
+struct BatchPlan {
+    std::vector<JobDev> jobs;
+    std::vector<BatchItem> items;
+    std::vector<int> pt_job;
+    size_t ws_bytes = 0;  // per-job partials + masks + global tables
+    int total_pts = 0;
+    int grid = 0;
+    bool mixed = true, ck = false;
+};
+
+struct BatchDevPtrs {
+    JobDev* jobs;
+    BatchItem* items;
+    int* pt_job;
+    long long* counts;
+    long long* offs;
+    long long* total;
+    int* counter;
+};
+
+void plan_batch(BatchPlan& bp, const std::vector<JobDev>& jobs, int n_start, bool mixed, double item_cost);
+cudaError_t batch_stage1(BatchPlan& bp, void* ws, double analytic_calc, int n_start, bool ck, cudaStream_t s,
+                         BatchDevPtrs* out, int* launches);
+size_t batch_pair_ws_bytes(long long n_near);
+struct DNP;
+cudaError_t batch_stage2(BatchPlan& bp, const BatchDevPtrs& d, long long n_near, void* pair_ws, const DNP& np,
+                         unsigned long long* d_nonfinite, cudaStream_t s, int* launches);
+// largest n_start the batched kernel stages (node tile capacity)
+constexpr int kBatchMaxNStart = 22;
 
 }  // namespace bielcc_gpu

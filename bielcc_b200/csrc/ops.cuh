@@ -655,6 +655,42 @@ BIELCC_D void R_near_dev(const cplx* j, const double* x, const DCell& c, const D
     ccross_cc(j, t, res);
 }
 
+// J-independent parts of the near-field pair (x, cell) of the field driver,
+// scaled by 1/4pi: out[13] = { surf * k^2 / 4pi, M (3x3) / 4pi, g (3) / 4pi }
+// so that K_RotRot_Near_Smooth (K.h:47-79) = out0 * J + M J and
+// R_Rot_Smooth (R.h:46-61) = g x J.
+BIELCC_D void near_pair_moments(const double* x, const DCell& cl, cplx k, const DNP& np, cplx* o) {
+    double dm = cell_diam(cl);
+    // surface part of K_RotRot_Near_Smooth (K.h:51-67)
+    DKP pF;
+    dkp_zero(pF);
+    pF.smoothR = np.rs * dm / np.n_start;
+    pF.smoothRMin = np.eps;
+    pF.k = k;
+    cplx s[1];
+    integral_cell<cplx>(F_SIMPLEPOT_H, x, cl, pF, 1, np.n_start, np.p_max, np.eps, s);
+    o[0] = s[0] * k * k / kFourPi;
+    // contour part (K.h:56-72): K0 with the shared, shrinking segment radius
+    DKP pG;
+    dkp_zero(pG);
+    pG.smoothR = np.rs_seg * dm / np.n_start_seg;
+    pG.smoothRMin = np.eps;
+    pG.k = k;
+    cplx M[3][3], dummy[3];
+    K0_dev(F_GRADSIMPLEPOT_H, nullptr, x, cl, pG, np.n_start_seg, np.p_max_seg, np.eps, dummy, M);
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) o[1 + 3 * a + b] = M[a][b] / kFourPi;
+    // R_Rot_Smooth (R.h:46-61)
+    DKP pR;
+    dkp_zero(pR);
+    pR.smoothR = np.rs * dm / np.n_start;
+    pR.smoothRMin = dm / 100.;
+    pR.k = k;
+    cplx g[3];
+    integral_cell<cplx>(F_GRADSIMPLEPOT_H, x, cl, pR, 3, np.n_start, np.p_max, np.eps, g);
+    for (int a = 0; a < 3; a++) o[10 + a] = g[a] / kFourPi;
+}
+
 BIELCC_D void run_pair_op(int op, const cplx* j, const double* x, const DCell& c, const DNP& np, cplx k, cplx* res) {
     switch (op) {
         case 0: K_near_smooth_dev(j, x, c, np, k, res); break;

@@ -60,6 +60,10 @@ def load(path=LIB_PATH):
                             vp, C.POINTER(abi.Report)])
     d("bielcc_assemble_K_device", [vp, C.c_int32, C.c_double, C.c_double, C.POINTER(abi.NumParam), C.c_int, C.c_int,
                                    C.c_int, vp, vp, C.POINTER(abi.Report)])
+    d("bielcc_field_EH_batch", [vp, C.c_int, C.POINTER(abi.FieldJob), C.POINTER(abi.NumParam), C.c_int, vp,
+                                C.POINTER(abi.Report)])
+    d("bielcc_batch_autotune", [vp, C.c_int, C.POINTER(abi.FieldJob), C.POINTER(abi.NumParam), C.c_int, vp,
+                                C.POINTER(C.c_double)])
     d("bielcc_ctx_set_timing", [vp, C.c_int])
     d("bielcc_measure_fma_peak", [C.c_int, C.POINTER(C.c_double)])
     d("bielcc_ctx_stats", [vp, C.POINTER(abi.Stats), C.c_int])
@@ -197,6 +201,44 @@ class Context:
                                            C.c_void_p(H_dev) if H_dev else None, PREC[precision],
                                            C.c_void_p(stream) if stream else None, C.byref(rep)))
         return rep
+
+    # ------------------------------------------------------------------ batched field
+    @staticmethod
+    def make_jobs(specs):
+        """specs: dicts with mesh, n_rhs, n_pts, J, pts, E, H (device pointers as ints),
+        k, mult (optional), inc (optional PlaneWave)."""
+        arr = (abi.FieldJob * len(specs))()
+        for i, sp in enumerate(specs):
+            k = complex(sp["k"])
+            mult = complex(sp.get("mult", 1.0))
+            j = arr[i]
+            j.mesh = sp["mesh"].id
+            j.n_rhs = sp["n_rhs"]
+            j.n_pts = sp["n_pts"]
+            j.J_dev = sp["J"]
+            j.pts_dev = sp["pts"]
+            j.E_dev = sp["E"]
+            j.H_dev = sp.get("H") or None
+            j.k_re, j.k_im = k.real, k.imag
+            j.mult_re, j.mult_im = mult.real, mult.imag
+            if sp.get("inc") is not None:
+                j.inc = sp["inc"]
+        return arr
+
+    def field_EH_batch(self, jobs, numparam=None, precision="mixed", stream=None):
+        """Runs a batch built by make_jobs on device buffers; returns the report."""
+        rep = abi.Report()
+        np_ = numparam if numparam is not None else abi.NumParam.default()
+        _check(_lib.bielcc_field_EH_batch(self.h, len(jobs), jobs, C.byref(np_), PREC[precision],
+                                          C.c_void_p(stream) if stream else None, C.byref(rep)))
+        return rep
+
+    def batch_autotune(self, jobs, numparam=None, precision="mixed", stream=None):
+        c = C.c_double(0)
+        np_ = numparam if numparam is not None else abi.NumParam.default()
+        _check(_lib.bielcc_batch_autotune(self.h, len(jobs), jobs, C.byref(np_), PREC[precision],
+                                          C.c_void_p(stream) if stream else None, C.byref(c)))
+        return c.value
 
     # ------------------------------------------------------------------ per-pair operators
     def pair_op(self, op, cells, x, j, k, numparam=None):

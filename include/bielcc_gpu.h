@@ -205,6 +205,42 @@ int bielcc_field_EH_noalloc(int n_vert, int n_cells, const double* cells_dev, in
                             double* E_dev, double* H_dev, int precision, void* stream,
                             bielcc_report* report);
 
+/* ---- batched field evaluation ---------------------------------------- */
+/* One field evaluation of a batch: a resident mesh, its right-hand sides and
+ * points (device buffers, same layouts as bielcc_field_EH_device). */
+typedef struct bielcc_field_job {
+    bielcc_mesh mesh;
+    int32_t n_rhs;
+    int32_t n_pts;
+    const double* J_dev;    /* [n_rhs][n_cells][3] complex */
+    const double* pts_dev;  /* [n_pts][3] */
+    double* E_dev;          /* [n_rhs][n_pts][3] complex */
+    double* H_dev;          /* may be NULL */
+    double k_re, k_im, mult_re, mult_im;
+    bielcc_planewave inc;   /* add_E = add_H = 0 for no incident field */
+} bielcc_field_job;
+
+/* Many field evaluations (meshes of uneven sizes, their own k, 1..n RHS) in
+ * one persistent launch: the far field of every job in one kernel that pulls
+ * (job, 32-point tile, cell range) items from a device queue, largest first;
+ * per cell chunk the 20 far moments of each (point, cell) are staged in shared
+ * memory and contracted with every RHS, so extra RHS cost a contraction, not
+ * the quadrature. Near pairs take the FP64 path of bielcc_field_EH. Each
+ * job's result depends only on the job (never on the rest of the batch).
+ * Same per-job results as GetFieldE_Ideal + H (electrodynamics/get_field.h:35-78)
+ * within the precision's tolerance. p_max > 1 or n_start > 22 fall back to one
+ * bielcc_field_EH_device per job. report->n_pairs counts (point, cell, RHS). */
+int bielcc_field_EH_batch(bielcc_ctx ctx, int n_jobs, const bielcc_field_job* jobs,
+                          const bielcc_numparam* np, int precision, void* stream,
+                          bielcc_report* report);
+/* Times bielcc_field_EH_batch on the given batch for a set of item sizes
+ * (estimated node evaluations per work item) and keeps the fastest on the
+ * context for later batched calls; *item_cost receives it. The jobs' outputs
+ * are overwritten. No counterpart in the reference. */
+int bielcc_batch_autotune(bielcc_ctx ctx, int n_jobs, const bielcc_field_job* jobs,
+                          const bielcc_numparam* np, int precision, void* stream,
+                          double* item_cost);
+
 /* ---- per-pair operators ----------------------------------------------- */
 /* One operator applied to n_pairs independent (cell, x, j) triples, each as
  * the reference call op(j, x, cell, num_param, k, res):

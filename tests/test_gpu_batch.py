@@ -1,0 +1,89 @@
+"""Batched field evaluation (many meshes, uneven sizes, several RHS, one
+persistent launch) against the single-job path and the oracle; a job's
+result is the same alone and inside a mixed batch."""
+import numpy as np
+import pytest
+
+import oracle
+from bielcc_b200 import abi
+from bielcc_b200 import workloads as W
+from conftest import TOL_FP64, TOL_MIXED, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _batch(torch, gctx, specs_np, precision, numparam=None):
+    dev = torch.device("cuda:0")
+    keep, specs = [], []
+    for sp in specs_np:
+        Jd = torch.from_numpy(np.ascontiguousarray(sp["J"])).to(dev)
+        Pd = torch.from_numpy(np.ascontiguousarray(sp["pts"])).to(dev)
+        S, P = sp["J"].shape[0], len(sp["pts"])
+        Ed = torch.zeros((S, P, 3), dtype=torch.complex128, device=dev)
+        Hd = torch.zeros_like(Ed)
+        keep += [Jd, Pd, Ed, Hd]
+        specs.append(dict(mesh=sp["mesh"], n_rhs=S, n_pts=P, J=Jd.data_ptr(), pts=Pd.data_ptr(), E=Ed.data_ptr(),
+                          H=Hd.data_ptr(), k=sp["k"], mult=sp.get("mult", 1.0), inc=sp.get("inc"), out=(Ed, Hd)))
+    jobs = gctx.make_jobs(specs)
+    rep = gctx.field_EH_batch(jobs, numparam=numparam, precision=precision,
+                              stream=torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    outs = [(sp["out"][0].cpu().numpy(), sp["out"][1].cpu().numpy()) for sp in specs]
+    return outs, rep
+
+
+def _jobs(gctx, seed=0):
+    rng = np.random.default_rng(seed)
+    meshes = [W.uv_sphere(6, 12), W.perturbed_icosphere(1, seed=4), W.torus(18, 6), W.spheroid(5, 10, 1.0, 2.5)]
+    specs = []
+    for i, cells in enumerate(meshes):
+        k = [2.0, 5.0, complex(3.0, 0.2), 9.0][i]
+        S = [1, 5, 3, 7][i]
+        ext = float(np.max(np.linalg.norm(cells.reshape(-1, 3), axis=1)))
+        pts = np.concatenate([W.shell_points(40 + 13 * i, 1.6 * ext, 3 * ext, rng),
+                              W.near_points(cells, 6, 0.02, 0.2, rng)])
+        specs.append(dict(mesh=gctx.mesh(cells), cells=cells, J=W.po_currents(cells, abs(k), directions=S, seed=i),
+                          pts=pts, k=k, mult=complex(1.0, 0.5 * i)))
+    return specs
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", TOL_FP64), ("mixed", TOL_MIXED)])
+def test_batch_matches_oracle(gctx, precision, tol):
+    torch = pytest.importorskip("torch")
+    specs = _jobs(gctx)
+    outs, rep = _batch(torch, gctx, specs, precision)
+    assert rep.n_near_pairs > 0
+    for sp, (E, H) in zip(specs, outs):
+        Eo, Ho = oracle.field_EH(sp["cells"], sp["J"], sp["k"], sp["pts"], mult=sp["mult"])
+        assert rel_l2(E, Eo) < tol and rel_l2(H, Ho) < tol
+
+
+def test_batch_job_alone_equals_in_mix(gctx):
+    torch = pytest.importorskip("torch")
+    specs = _jobs(gctx, seed=3)
+    mix, _ = _batch(torch, gctx, specs, "mixed")
+    for i in (0, 3):
+        alone, _ = _batch(torch, gctx, [specs[i]], "mixed")
+        assert np.array_equal(alone[0][0], mix[i][0]) and np.array_equal(alone[0][1], mix[i][1])
+
+
+def test_batch_fallback_adaptive_and_autotune(gctx):
+    torch = pytest.importorskip("torch")
+    specs = _jobs(gctx, seed=5)[:2]
+    npm = abi.NumParam.default(n_start=4, n_start_seg=5, p_max=2, p_max_seg=2)
+    outs, _ = _batch(torch, gctx, specs, "fp64", numparam=npm)
+    for sp, (E, H) in zip(specs, outs):
+        Eo, Ho = oracle.field_EH(sp["cells"], sp["J"], sp["k"], sp["pts"], npm, mult=sp["mult"])
+        assert rel_l2(E, Eo) < TOL_FP64 and rel_l2(H, Ho) < TOL_FP64
+    dev = torch.device("cuda:0")
+    keep = []
+    s2 = []
+    for sp in specs:
+        Jd = torch.from_numpy(np.ascontiguousarray(sp["J"])).to(dev)
+        Pd = torch.from_numpy(np.ascontiguousarray(sp["pts"])).to(dev)
+        Ed = torch.zeros((sp["J"].shape[0], len(sp["pts"]), 3), dtype=torch.complex128, device=dev)
+        keep += [Jd, Pd, Ed]
+        s2.append(dict(mesh=sp["mesh"], n_rhs=sp["J"].shape[0], n_pts=len(sp["pts"]), J=Jd.data_ptr(),
+                       pts=Pd.data_ptr(), E=Ed.data_ptr(), k=sp["k"]))
+    c = gctx.batch_autotune(gctx.make_jobs(s2), precision="mixed")
+    assert c > 0
