@@ -52,6 +52,11 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
     ap.add_argument("--no-batched", action="store_true", help="skip the 256-mesh batched leg")
     ap.add_argument("--batch-meshes", type=int, default=256)
+    ap.add_argument("--no-assembly", action="store_true", help="skip the 20,480-triangle assembly leg")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream leg")
+    ap.add_argument("--serve-requests", type=int, default=400)
+    ap.add_argument("--serve-load", type=float, default=0.9, help="arrival rate / offline capacity")
+    ap.add_argument("--serve-slots", type=int, default=4)
     return ap.parse_args()
 
 
@@ -254,6 +259,211 @@ def run_batched(args, ctx, torch, dev, stream, flush, fp64_single_rhs_value):
                 st["kernel_launches"] / steps, "near_pairs": int(rep.n_near_pairs)}
 
 
+def run_assembly(args, ctx, torch, dev, stream, flush):
+    """Collocation assembly of K on the perturbed icosphere (level 5, 20,480
+    triangles, seed 2), k = 4 pi: the TAU2 matrix (40,960^2 complex64 entries,
+    13.4 GB) with FP64 near / self entries, timed on device-resident output;
+    its error is the relative L2 against the FP64 assembly (complex128) of the
+    same matrix, which is timed too."""
+    from bielcc_b200 import workloads as W
+
+    wl = W.config3()
+    cells, k = wl["cells"], wl["k"]
+    N = len(cells)
+    mesh = ctx.mesh(cells)
+    n = 2 * N
+    sc = stream.cuda_stream
+    A = torch.empty((n, n), dtype=torch.complex64, device=dev)
+
+    def timed(prec, out, steps):
+        total, rep = 0.0, None
+        for _ in range(steps):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            rep = ctx.assemble_K_device(mesh, k, out.data_ptr(), c64=out.dtype == torch.complex64, precision=prec,
+                                        stream=sc)
+            b.record(stream)
+            b.synchronize()
+            total += a.elapsed_time(b)
+        return total / steps, rep
+
+    timed("mixed", A, 1)  # warm-up: node tables, workspaces
+    steps = max(1, min(args.steps, 3))
+    ms, rep = timed("mixed", A, steps)
+    A64 = torch.empty((n, n), dtype=torch.complex128, device=dev)
+    ms64, _ = timed("fp64", A64, 1)
+    num = den = 0.0
+    for r0 in range(0, n, 4096):
+        d = A[r0:r0 + 4096].to(torch.complex128) - A64[r0:r0 + 4096]
+        num += float(torch.sum(d.real ** 2 + d.imag ** 2))
+        den += float(torch.sum(A64[r0:r0 + 4096].real ** 2 + A64[r0:r0 + 4096].imag ** 2))
+    del A64, A
+    torch.cuda.empty_cache()
+    mesh.close()
+    return {"workload": f"{wl['name']}: TAU2 {n}x{n} complex64, FP64 near/self entries",
+            "value": N * N / (ms * 1e-3), "unit": "(collocation point, cell) pairs/s", "ms": ms, "steps": steps,
+            "fp64_ms": ms64, "mixed_over_fp64": ms64 / ms, "rel_l2_vs_fp64": (num / den) ** 0.5,
+            "near_pairs": int(rep.n_near_pairs), "matrix_gb": n * n * 8 / 1e9,
+            "write_gbs": n * n * 8 / (ms * 1e-3) / 1e9}
+
+
+def _pct(v, q):
+    """Nearest-rank percentile."""
+    if not v:
+        return None
+    v = sorted(v)
+    return v[min(len(v) - 1, max(0, int(np.ceil(q * len(v))) - 1))]
+
+
+def run_serving(args, ctx, torch, dev, stream, item_cost):
+    """Serving stream: Poisson arrivals of field and assembly requests over 24
+    resident meshes drawn like the batched workload (seed 4); field requests
+    carry 100-50,000 points (log-uniform, 10% near-field) and 1-16 PO current
+    sets, complex64 E and H with FP64 near pairs; assembly requests build the
+    TAU2 complex64 matrix of a mesh of at most 2000 cells. The same requests
+    first run offline (device-resident inputs, field requests in batches of
+    64 through bielcc_field_EH_batch, assembly through
+    bielcc_assemble_K_device) to give the offline throughput; the stream then
+    arrives at --serve-load x that rate through bielcc_server_* with host
+    buffers, and its throughput, p50/p99 latency and agreement with the offline
+    results are reported."""
+    import threading
+
+    from bielcc_b200 import abi, gpu
+    from bielcc_b200 import workloads as W
+
+    meshes, reqs = W.serving_stream(n_requests=args.serve_requests, seed=4)
+    mh = [ctx.mesh(m["cells"]) for m in meshes]
+    Jd = [torch.from_numpy(m["J"]).to(dev) for m in meshes]
+    Pd = [torch.from_numpy(m["pts"]).to(dev) for m in meshes]
+    field = [r for r in reqs if r["type"] == "field"]
+    asm = [r for r in reqs if r["type"] == "assemble"]
+    pairs = sum(r["P"] * len(meshes[r["mesh"]]["cells"]) * r["S"] for r in field)
+    sc = stream.cuda_stream
+    # ---- offline
+    sample = set(range(0, len(reqs), max(1, len(reqs) // 16)))
+    ref = {}
+
+    def offline(keep_ref):
+        t = 0.0
+        for c0 in range(0, len(reqs), 64):
+            chunk = [(i, reqs[i]) for i in range(c0, min(len(reqs), c0 + 64))]
+            specs, outs = [], []
+            for i, r in chunk:
+                if r["type"] != "field":
+                    continue
+                E = torch.empty((r["S"], r["P"], 3), dtype=torch.complex128, device=dev)
+                H = torch.empty_like(E)
+                outs.append((i, E, H))
+                specs.append(dict(mesh=mh[r["mesh"]], n_rhs=r["S"], n_pts=r["P"], J=Jd[r["mesh"]].data_ptr(),
+                                  pts=Pd[r["mesh"]].data_ptr(), E=E.data_ptr(), H=H.data_ptr(),
+                                  k=meshes[r["mesh"]]["k"]))
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            if specs:
+                ctx.field_EH_batch(ctx.make_jobs(specs), precision="mixed", stream=sc)
+            for i, r in chunk:
+                if r["type"] == "assemble":
+                    n = 2 * mh[r["mesh"]].n_cells
+                    A = torch.empty((n, n), dtype=torch.complex64, device=dev)
+                    ctx.assemble_K_device(mh[r["mesh"]], meshes[r["mesh"]]["k"], A.data_ptr(), c64=True,
+                                          precision="mixed", stream=sc)
+                    if keep_ref and i in sample:
+                        outs.append((i, A, None))
+            b.record(stream)
+            b.synchronize()
+            t += a.elapsed_time(b) * 1e-3
+            if keep_ref:
+                for i, E, H in outs:
+                    if i in sample:
+                        ref[i] = (E.cpu().numpy(), None if H is None else H.cpu().numpy())
+        return t
+
+    offline(False)  # warm-up: node tables, allocations
+    t_off = offline(True)
+    off_pairs_per_s = pairs / t_off
+    rate = args.serve_load * len(reqs) / t_off  # requests/s
+    # ---- serving: the clients' output buffers are allocated and touched up
+    # front (a client reuses its buffers; first-touch page faults are not the
+    # server's cost)
+    outs = []
+    for r in reqs:
+        if r["type"] == "field":
+            E = np.ones((r["S"], r["P"], 3), np.complex64)
+            outs.append((E, np.ones_like(E)))
+        else:
+            n = 2 * mh[r["mesh"]].n_cells
+            outs.append(np.ones((n, n), np.complex64))
+    sv = gpu.Server(ctx, n_slots=args.serve_slots, precision="mixed", item_cost=item_cost)
+    res = [None] * len(reqs)
+    tickets = [None] * len(reqs)
+    ready = threading.Semaphore(0)
+
+    def collect():
+        for i in range(len(reqs)):
+            ready.acquire()
+            st_, lat_, out_ = sv.wait(tickets[i], timeout=600.0)
+            res[i] = (st_, lat_, out_ if i in sample else None)  # keep only the compared outputs
+
+    th = threading.Thread(target=collect)
+    th.start()
+    with Clocks(dev.index or 0) as clk:
+        t0 = time.perf_counter()
+        for i, r in enumerate(reqs):
+            due = t0 + r["t"] / rate
+            now = time.perf_counter()
+            if due > now:
+                time.sleep(due - now)
+            m = meshes[r["mesh"]]
+            if r["type"] == "field":
+                tickets[i] = sv.submit_field(mh[r["mesh"]], m["J"][:r["S"]], m["pts"][:r["P"]], m["k"],
+                                             out_c64=True, out=outs[i])
+            else:
+                tickets[i] = sv.submit_assemble(mh[r["mesh"]], m["k"], layout="tau2", out_c64=True, out=outs[i])
+            ready.release()
+        th.join()
+    st = sv.stats()
+    sv.close()
+    lat_f = [res[i][1] for i, r in enumerate(reqs) if r["type"] == "field"]
+    lat_a = [res[i][1] for i, r in enumerate(reqs) if r["type"] == "assemble"]
+    bad = sum(1 for x in res if x[0] != 0)
+    # served complex64 results against the offline run (complex128 rounded)
+    same = 0
+    for i in sorted(ref):
+        o = res[i][2]
+        if reqs[i]["type"] == "field":
+            ok = np.array_equal(o["E"], ref[i][0].astype(np.complex64)) and \
+                np.array_equal(o["H"], ref[i][1].astype(np.complex64))
+        else:
+            ok = np.array_equal(o["A"], ref[i][0])
+        same += int(ok)
+    served = pairs / st["wall_s"]
+    for m in mh:
+        m.close()
+    return {
+        "workload": f"{len(reqs)} requests ({len(field)} field, {len(asm)} assembly) over 24 resident meshes "
+                    f"(spheroids, rounded cubes, tori; 200-20000 cells; k 0.5-20; seed 4); field: 100-50000 "
+                    f"points log-uniform, 1-16 PO current sets, complex64 E+H, FP64 near pairs; assembly: TAU2 "
+                    f"complex64 on meshes <= 2000 cells; Poisson arrivals",
+        "arrival_rate_per_s": rate, "load": args.serve_load, "slots": args.serve_slots,
+        "hbm_budget_gb": st["budget"] / 2**30,
+        "offline_pairs_per_s": off_pairs_per_s, "offline_s": t_off,
+        "served_pairs_per_s": served, "served_wall_s": st["wall_s"],
+        "served_over_offline": served / off_pairs_per_s,
+        "p50_ms": _pct(lat_f + lat_a, 0.50), "p99_ms": _pct(lat_f + lat_a, 0.99),
+        "field_p50_ms": _pct(lat_f, 0.50), "field_p99_ms": _pct(lat_f, 0.99),
+        "assembly_p50_ms": _pct(lat_a, 0.50), "assembly_p99_ms": _pct(lat_a, 0.99),
+        "max_ms": max(lat_f + lat_a), "batches": st["batches"], "max_batch": st["max_batch"],
+        "priority_batches": st["priority_batches"], "peak_reserved_gb": st["peak_bytes_reserved"] / 2**30,
+        "host_stage_in_s": st["stage_in_s"], "host_copy_out_s": st["copy_out_s"],
+        "failed": bad, "sampled_identical_to_offline": f"{same}/{len(ref)}",
+        "unit": "(point, cell, RHS) pairs/s", "clocks": clk.summary(),
+    }
+
+
 # ---------------------------------------------------------------- GPU arm
 def run_ours(args, ws, rank, local):
     import torch
@@ -382,6 +592,12 @@ def run_ours(args, ws, rank, local):
     batched = None
     if not args.no_batched:
         batched = run_batched(args, ctx, torch, dev, stream, flush, value64)
+    assembly = None
+    if not args.no_assembly:
+        assembly = run_assembly(args, ctx, torch, dev, stream, flush)
+    serving = None
+    if not args.no_serving and rank == 0:
+        serving = run_serving(args, ctx, torch, dev, stream, batched["autotuned_item_cost"] if batched else None)
     launches = st["kernel_launches"]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
@@ -409,6 +625,8 @@ def run_ours(args, ws, rank, local):
         "gpu_launches": launches,
         "near_pairs_per_step": int(last["rep"].n_near_pairs),
         "batched": batched,
+        "assembly": assembly,
+        "serving": serving,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -16,6 +16,7 @@ ERR_TIMEOUT = -5
 ERR_UNSUPPORTED = -6
 ERR_NOT_FOUND = -7
 ERR_BUSY = -8
+ERR_CANCELLED = -9
 
 PREC_FP64 = 0
 PREC_MIXED = 1
@@ -153,6 +154,51 @@ class FieldJob(C.Structure):
         ("mult_im", C.c_double),
         ("inc", PlaneWave),
     ]
+
+
+class FieldRequest(C.Structure):
+    """bielcc_field_request: a serving request (host buffers, or resident J_dev)."""
+
+    _fields_ = [
+        ("mesh", C.c_int32),
+        ("n_rhs", C.c_int32),
+        ("n_pts", C.c_int32),
+        ("out_c64", C.c_int32),
+        ("J", C.c_void_p),
+        ("J_dev", C.c_void_p),
+        ("pts", C.c_void_p),
+        ("E", C.c_void_p),
+        ("H", C.c_void_p),
+        ("k_re", C.c_double),
+        ("k_im", C.c_double),
+        ("mult_re", C.c_double),
+        ("mult_im", C.c_double),
+        ("inc", PlaneWave),
+    ]
+
+
+class AssembleRequest(C.Structure):
+    _fields_ = [
+        ("mesh", C.c_int32),
+        ("layout", C.c_int32),
+        ("out_c64", C.c_int32),
+        ("A", C.c_void_p),
+        ("A_dev", C.c_void_p),
+        ("k_re", C.c_double),
+        ("k_im", C.c_double),
+    ]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(n, C.c_int64) for n in (
+        "submitted", "completed", "failed", "cancelled", "rejected", "queued", "running", "batches", "priority_batches",
+        "max_batch",
+        "bytes_reserved", "peak_bytes_reserved", "bytes_allocated", "budget", "pairs_done")] + \
+        [(n, C.c_double) for n in ("p50_ms", "p99_ms", "mean_ms", "max_ms", "wall_s", "pairs_per_s", "stage_in_s",
+                                   "copy_out_s")]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
 
 
 class Stats(C.Structure):

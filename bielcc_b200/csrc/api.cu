@@ -519,35 +519,12 @@ int bielcc_field_EH(bielcc_ctx ctx, bielcc_mesh mesh, int n_rhs, const double* J
 
 namespace {
 
-int field_batch_locked(bielcc_ctx ctx, int n_jobs, const bielcc_field_job* jobs, const NumParamH& n, int precision,
-                       cudaStream_t s, bielcc_report* report, double item_cost) {
-    std::vector<MeshDev*> meshes(n_jobs);
-    for (int i = 0; i < n_jobs; i++) {
-        const bielcc_field_job& j = jobs[i];
-        TRY(get_mesh(ctx, j.mesh, &meshes[i]));
-        if (j.n_rhs < 1 || j.n_pts < 0 || !j.J_dev || (j.n_pts > 0 && (!j.pts_dev || !j.E_dev)))
-            return set_error(BIELCC_ERR_ARG, "job %d: bad sizes or null buffers", i);
-    }
-    if (report) memset(report, 0, sizeof(*report));
-    TRY(ws_acquire(ctx, s));
-    if (n.p_max > 1 || n.n_start > kBatchMaxNStart) {  // outside the batched kernel: one call per job
-        for (int i = 0; i < n_jobs; i++) {
-            const bielcc_field_job& j = jobs[i];
-            FieldArgs a{meshes[i], j.n_rhs, j.J_dev, mk(j.k_re, j.k_im), mk(j.mult_re, j.mult_im), &j.inc, n,
-                        j.n_pts, j.pts_dev, j.E_dev, j.H_dev, precision};
-            bielcc_report r{};
-            TRY(field_device(ctx, a, s, &r, nullptr));
-            if (report) {
-                report->n_pairs += r.n_pairs * j.n_rhs;
-                report->n_near_pairs += r.n_near_pairs;
-            }
-        }
-        TRY(ws_release(ctx, s));
-        return BIELCC_OK;
-    }
-    std::vector<JobDev> jd(n_jobs);
-    bool ck = false;
-    int64_t pairs = 0;
+// bielcc_field_job records -> device job records (node tables built first).
+int jobs_to_dev(int n_jobs, const bielcc_field_job* jobs, const std::vector<MeshDev*>& meshes, const NumParamH& n,
+                cudaStream_t s, std::vector<JobDev>& jd, bool* ck, int64_t* pairs) {
+    jd.assign(n_jobs, JobDev{});
+    *ck = false;
+    *pairs = 0;
     for (int i = 0; i < n_jobs; i++) {
         const bielcc_field_job& j = jobs[i];
         MeshDev* m = meshes[i];
@@ -576,9 +553,48 @@ int field_batch_locked(bielcc_ctx ctx, int n_jobs, const bielcc_field_job* jobs,
         d.add_H = j.inc.add_H;
         d.E = j.E_dev;
         d.H = j.H_dev;
-        ck = ck || j.k_im != 0.;
-        pairs += (int64_t)j.n_pts * m->n_cells * j.n_rhs;
+        *ck = *ck || j.k_im != 0.;
+        *pairs += (int64_t)j.n_pts * m->n_cells * j.n_rhs;
     }
+    return BIELCC_OK;
+}
+
+int check_jobs(bielcc_ctx ctx, int n_jobs, const bielcc_field_job* jobs, std::vector<MeshDev*>& meshes) {
+    meshes.resize(n_jobs);
+    for (int i = 0; i < n_jobs; i++) {
+        const bielcc_field_job& j = jobs[i];
+        TRY(get_mesh(ctx, j.mesh, &meshes[i]));
+        if (j.n_rhs < 1 || j.n_pts < 0 || !j.J_dev || (j.n_pts > 0 && (!j.pts_dev || !j.E_dev)))
+            return set_error(BIELCC_ERR_ARG, "job %d: bad sizes or null buffers", i);
+    }
+    return BIELCC_OK;
+}
+
+int field_batch_locked(bielcc_ctx ctx, int n_jobs, const bielcc_field_job* jobs, const NumParamH& n, int precision,
+                       cudaStream_t s, bielcc_report* report, double item_cost) {
+    std::vector<MeshDev*> meshes;
+    TRY(check_jobs(ctx, n_jobs, jobs, meshes));
+    if (report) memset(report, 0, sizeof(*report));
+    TRY(ws_acquire(ctx, s));
+    if (n.p_max > 1 || n.n_start > kBatchMaxNStart) {  // outside the batched kernel: one call per job
+        for (int i = 0; i < n_jobs; i++) {
+            const bielcc_field_job& j = jobs[i];
+            FieldArgs a{meshes[i], j.n_rhs, j.J_dev, mk(j.k_re, j.k_im), mk(j.mult_re, j.mult_im), &j.inc, n,
+                        j.n_pts, j.pts_dev, j.E_dev, j.H_dev, precision};
+            bielcc_report r{};
+            TRY(field_device(ctx, a, s, &r, nullptr));
+            if (report) {
+                report->n_pairs += r.n_pairs * j.n_rhs;
+                report->n_near_pairs += r.n_near_pairs;
+            }
+        }
+        TRY(ws_release(ctx, s));
+        return BIELCC_OK;
+    }
+    std::vector<JobDev> jd;
+    bool ck = false;
+    int64_t pairs = 0;
+    TRY(jobs_to_dev(n_jobs, jobs, meshes, n, s, jd, &ck, &pairs));
     BatchPlan bp;
     plan_batch(bp, jd, n.n_start, precision == BIELCC_PREC_MIXED, item_cost);
     TRY(ctx->ws.ensure(bp.ws_bytes));
@@ -618,6 +634,126 @@ int bielcc_field_EH_batch(bielcc_ctx ctx, int n_jobs, const bielcc_field_job* jo
     std::lock_guard<std::mutex> g(ctx->mu);
     cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
     return field_batch_locked(ctx, n_jobs, jobs, n, precision, s, report, ctx->batch_item_cost);
+}
+
+}  // extern "C"
+
+// A batch planned once for repeated evaluation (bielcc_batch_plan_*): its
+// own workspaces (never shared with the context's), the near-pair list and
+// FP64 near moments of the first evaluation, and the CUDA graph of the
+// replay sequence.
+struct bielcc_batch_plan_s {
+    bielcc_ctx ctx = nullptr;
+    BatchPlan bp;
+    BatchDevPtrs d{};
+    void* ws = nullptr;
+    void* pair_ws = nullptr;
+    long long n_near = 0;
+    double analytic_calc = 3.0;
+    int n_start = 8;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int64_t pairs = 0;
+};
+
+namespace {
+
+void free_plan(bielcc_batch_plan p) {
+    if (!p) return;
+    if (p->exec) cudaGraphExecDestroy(p->exec);
+    if (p->graph) cudaGraphDestroy(p->graph);
+    cudaFree(p->ws);
+    cudaFree(p->pair_ws);
+    delete p;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bielcc_batch_plan_create(bielcc_ctx ctx, int n_jobs, const bielcc_field_job* jobs, const bielcc_numparam* np,
+                             int precision, void* stream, bielcc_batch_plan* out, bielcc_report* report) {
+    TRY(enter(ctx));
+    if (n_jobs < 1 || !jobs || !out) return set_error(BIELCC_ERR_ARG, "bad job list");
+    if (precision != BIELCC_PREC_FP64 && precision != BIELCC_PREC_MIXED)
+        return set_error(BIELCC_ERR_ARG, "unknown precision %d", precision);
+    NumParamH n = to_np(np);
+    TRY(check_np(n));
+    if (n.p_max > 1 || n.n_start > kBatchMaxNStart)
+        return set_error(BIELCC_ERR_UNSUPPORTED, "batch plans run the batched kernel: p_max = 1, n_start <= 22");
+    std::lock_guard<std::mutex> g(ctx->mu);
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    std::vector<MeshDev*> meshes;
+    TRY(check_jobs(ctx, n_jobs, jobs, meshes));
+    bielcc_batch_plan p = new (std::nothrow) bielcc_batch_plan_s;
+    if (!p) return set_error(BIELCC_ERR_OOM, "out of host memory");
+    p->ctx = ctx;
+    p->analytic_calc = n.analytic_calc;
+    p->n_start = n.n_start;
+    std::vector<JobDev> jd;
+    bool ck = false;
+    int rc = jobs_to_dev(n_jobs, jobs, meshes, n, s, jd, &ck, &p->pairs);
+    cudaError_t e = cudaSuccess;
+    int l1 = 0, l2 = 0;
+    if (rc == BIELCC_OK) {
+        plan_batch(p->bp, jd, n.n_start, precision == BIELCC_PREC_MIXED, ctx->batch_item_cost);
+        e = cudaMalloc(&p->ws, p->bp.ws_bytes);
+        if (e == cudaSuccess) e = batch_stage1(p->bp, p->ws, n.analytic_calc, n.n_start, ck, s, &p->d, &l1);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(ctx->h_total, p->d.total, sizeof(long long), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    }
+    if (rc == BIELCC_OK && e == cudaSuccess) {
+        p->n_near = *ctx->h_total;
+        if (p->n_near > 0) e = cudaMalloc(&p->pair_ws, batch_pair_ws_bytes(p->n_near));
+        DNP dn{n.eps, n.rs, n.rs_seg, n.analytic_calc, n.n_start, n.n_start_seg, n.p_max, n.p_max_seg};
+        if (e == cudaSuccess) e = batch_stage2(p->bp, p->d, p->n_near, p->pair_ws, dn, nullptr, s, &l2);
+    }
+    // capture the replay sequence on a private stream (capture needs a stream
+    // other than the legacy default one), then instantiate it
+    cudaStream_t cs = nullptr;
+    if (rc == BIELCC_OK && e == cudaSuccess) e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    if (rc == BIELCC_OK && e == cudaSuccess) {
+        e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            cudaError_t e1 = batch_replay(p->bp, p->d, p->n_near, p->pair_ws, n.analytic_calc, n.n_start, cs);
+            cudaError_t e2 = cudaStreamEndCapture(cs, &p->graph);
+            e = e1 != cudaSuccess ? e1 : e2;
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&p->exec, p->graph, 0);
+    }
+    if (cs) cudaStreamDestroy(cs);
+    if (rc == BIELCC_OK && e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (rc != BIELCC_OK || e != cudaSuccess) {
+        cudaGetLastError();
+        cudaStreamSynchronize(s);
+        free_plan(p);
+        return rc != BIELCC_OK ? rc : set_error(BIELCC_ERR_CUDA, "batch plan: %s", cudaGetErrorString(e));
+    }
+    ctx->stats.kernel_launches += l1 + l2;
+    if (report) {
+        memset(report, 0, sizeof(*report));
+        report->n_pairs = p->pairs;
+        report->n_near_pairs = p->n_near;
+    }
+    *out = p;
+    return BIELCC_OK;
+}
+
+int bielcc_batch_plan_launch(bielcc_batch_plan p, void* stream) {
+    if (!p) return set_error(BIELCC_ERR_ARG, "null plan");
+    TRY(enter(p->ctx));
+    cudaStream_t s = stream ? (cudaStream_t)stream : p->ctx->stream;
+    TRY_CUDA(cudaGraphLaunch(p->exec, s));
+    return BIELCC_OK;
+}
+
+int bielcc_batch_plan_destroy(bielcc_batch_plan p) {
+    if (!p) return BIELCC_OK;
+    TRY(enter(p->ctx));
+    TRY_CUDA(cudaDeviceSynchronize());
+    free_plan(p);
+    return BIELCC_OK;
 }
 
 int bielcc_batch_autotune(bielcc_ctx ctx, int n_jobs, const bielcc_field_job* jobs, const bielcc_numparam* np,
@@ -926,3 +1062,24 @@ int bielcc_assemble_K(bielcc_ctx ctx, bielcc_mesh mesh, double k_re, double k_im
 }
 
 }  // extern "C"
+
+namespace bielcc_gpu {
+
+// The server's view of a context's mesh: node tables built for `n_start`
+// (and finished) before the mesh joins a batch on another stream.
+int server_mesh(bielcc_ctx ctx, bielcc_mesh id, int n_start, MeshDev** out) {
+    TRY(enter(ctx));
+    std::lock_guard<std::mutex> g(ctx->mu);
+    MeshDev* m;
+    TRY(get_mesh(ctx, id, &m));
+    if (m->table_n != n_start || !m->nodes64) {
+        TRY(ensure_tables(m, n_start, ctx->stream));
+        TRY_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    *out = m;
+    return BIELCC_OK;
+}
+
+int server_device(bielcc_ctx ctx) { return ctx ? ctx->device : 0; }
+
+}  // namespace bielcc_gpu

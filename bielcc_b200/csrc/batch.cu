@@ -150,7 +150,8 @@ BIELCC_D void batch_moments(const typename BatchCfg<MIXED>::NodeT* nd, int nn, c
 template <bool MIXED>
 __global__ void __launch_bounds__(kBT, 2) batch_far_kernel(const JobDev* __restrict__ jobs,
                                                          const BatchItem* __restrict__ items, int n_items,
-                                                         int* __restrict__ counter, double analytic_calc, int n_start) {
+                                                         int* __restrict__ counter, double analytic_calc, int n_start,
+                                                         int max_items) {
     using C = BatchCfg<MIXED>;
     using F = typename C::F;
     using NodeT = typename C::NodeT;
@@ -167,7 +168,7 @@ __global__ void __launch_bounds__(kBT, 2) batch_far_kernel(const JobDev* __restr
     const int nn = n_start * n_start;
     const int ch = max(1, min(C::CH, C::NODES / nn));
 
-    for (;;) {
+    for (int taken = 0; taken < max_items; taken++) {
         __syncthreads();
         if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
         __syncthreads();
@@ -382,20 +383,29 @@ __global__ void batch_finalize_kernel(const JobDev* __restrict__ jobs, const int
             for (int a = 0; a < 3; a++) E[a] += mk(jb.e0[a] * cs, jb.e0[a] * sn);
         if (jb.add_H)
             for (int a = 0; a < 3; a++) H[a] += mk(kx0[a] * cs * jb.h_scale, kx0[a] * sn * jb.h_scale);
-        cplx* eo = reinterpret_cast<cplx*>(jb.E) + ((size_t)s * P + p) * 3;
-        for (int a = 0; a < 3; a++) {
-            eo[a] = E[a];
-            bad |= !isfinite(E[a].re) || !isfinite(E[a].im);
+        for (int a = 0; a < 3; a++) bad |= !isfinite(E[a].re) || !isfinite(E[a].im);
+        if (jb.E32) {
+            float2* eo = reinterpret_cast<float2*>(jb.E32) + ((size_t)s * P + p) * 3;
+            for (int a = 0; a < 3; a++) eo[a] = make_float2((float)E[a].re, (float)E[a].im);
+        } else {
+            cplx* eo = reinterpret_cast<cplx*>(jb.E) + ((size_t)s * P + p) * 3;
+            for (int a = 0; a < 3; a++) eo[a] = E[a];
         }
-        if (jb.H) {
-            cplx* ho = reinterpret_cast<cplx*>(jb.H) + ((size_t)s * P + p) * 3;
-            for (int a = 0; a < 3; a++) {
-                ho[a] = H[a];
-                bad |= !isfinite(H[a].re) || !isfinite(H[a].im);
+        if (jb.H || jb.H32) {
+            for (int a = 0; a < 3; a++) bad |= !isfinite(H[a].re) || !isfinite(H[a].im);
+            if (jb.H32) {
+                float2* ho = reinterpret_cast<float2*>(jb.H32) + ((size_t)s * P + p) * 3;
+                for (int a = 0; a < 3; a++) ho[a] = make_float2((float)H[a].re, (float)H[a].im);
+            } else {
+                cplx* ho = reinterpret_cast<cplx*>(jb.H) + ((size_t)s * P + p) * 3;
+                for (int a = 0; a < 3; a++) ho[a] = H[a];
             }
         }
     }
-    if (bad && nonfinite) atomicAdd(nonfinite, 1ull);
+    if (bad) {
+        if (nonfinite) atomicAdd(nonfinite, 1ull);
+        if (jb.nonfinite) atomicAdd(jb.nonfinite, 1ull);
+    }
 }
 
 // ---------------------------------------------------------------- host side
@@ -423,6 +433,15 @@ int batch_grid(bool mixed) {
 // evaluations per item, a per-context autotuned constant), never on the other
 // jobs of the batch, so a job's summation order - and its result - is the same
 // alone and in any mix. Ranges are multiples of 32 cells (near-mask words).
+int batch_cells_per_range(int n_cells, int n_rhs, int n_start, double item_cost) {
+    const double per_cell = (double)kBP * ((double)n_start * n_start + 1.2 * n_rhs);
+    // at most kMaxRanges ranges per job: bounds the partial sums to kMaxRanges x (S x 12 x P) doubles
+    constexpr int kMaxRanges = 6;
+    int cpr = (int)std::min<double>(n_cells, std::max(32.0, item_cost / per_cell));
+    cpr = std::max(cpr, (n_cells + kMaxRanges - 1) / kMaxRanges);
+    return (cpr + 31) / 32 * 32;
+}
+
 void plan_batch(BatchPlan& bp, const std::vector<JobDev>& jobs_in, int n_start, bool mixed, double item_cost) {
     bp.jobs = jobs_in;
     bp.mixed = mixed;
@@ -438,11 +457,7 @@ void plan_batch(BatchPlan& bp, const std::vector<JobDev>& jobs_in, int n_start, 
         pt_off += j.n_pts;
         for (int p = 0; p < j.n_pts; p++) bp.pt_job.push_back((int)ji);
         const double per_cell = (double)kBP * (nodes + 1.2 * j.n_rhs);
-        // at most kMaxRanges ranges per job: bounds the partial sums to kMaxRanges x (S x 12 x P) doubles
-        constexpr int kMaxRanges = 6;
-        int cpr = (int)std::min<double>(j.n_cells, std::max(32.0, item_cost / per_cell));
-        cpr = std::max(cpr, (j.n_cells + kMaxRanges - 1) / kMaxRanges);
-        cpr = (cpr + 31) / 32 * 32;
+        const int cpr = batch_cells_per_range(j.n_cells, j.n_rhs, n_start, item_cost);
         j.cells_per_range = cpr;
         j.ranges = (j.n_cells + cpr - 1) / cpr;
         j.n_words = (j.n_cells + 31) / 32;
@@ -466,6 +481,11 @@ void plan_batch(BatchPlan& bp, const std::vector<JobDev>& jobs_in, int n_start, 
     const size_t T = bp.total_pts;
     bp.ws_bytes += al256(bp.jobs.size() * sizeof(JobDev)) + al256(bp.items.size() * sizeof(BatchItem)) +
                    al256(T * sizeof(int)) + 2 * al256((T + 1) * sizeof(long long)) + 3 * 256;
+}
+
+void batch_make_preemptible(BatchPlan& bp) {
+    bp.max_items = 1;
+    bp.grid = std::max<int>(1, (int)std::min<size_t>(bp.items.size(), (size_t)INT32_MAX));
 }
 
 // Enqueues stage 1 (far kernel, near counting, scan) of a planned batch into
@@ -505,10 +525,11 @@ cudaError_t batch_stage1(BatchPlan& bp, void* ws, double analytic_calc, int n_st
     const int n_items = (int)bp.items.size();
     if (n_items > 0) {
         if (bp.mixed)
-            batch_far_kernel<true><<<bp.grid, kBT, smem, s>>>(d.jobs, d.items, n_items, d.counter, analytic_calc, n_start);
+            batch_far_kernel<true><<<bp.grid, kBT, smem, s>>>(d.jobs, d.items, n_items, d.counter, analytic_calc,
+                                                             n_start, bp.max_items);
         else
             batch_far_kernel<false><<<bp.grid, kBT, smem, s>>>(d.jobs, d.items, n_items, d.counter, analytic_calc,
-                                                              n_start);
+                                                              n_start, bp.max_items);
     }
     const int tb = (int)((T + 127) / 128);
     if (T) batch_near_count_kernel<<<tb, 128, 0, s>>>(d.jobs, d.pt_job, (int)T, d.counts);
@@ -545,6 +566,39 @@ cudaError_t batch_stage2(BatchPlan& bp, const BatchDevPtrs& d, long long n_near,
         batch_finalize_kernel<<<tb, 128, 0, s>>>(d.jobs, d.pt_job, (int)T, n_near > 0 ? d.offs : nullptr, pair_cell,
                                                   moments, d_nonfinite);
         *launches += 1;
+    }
+    return cudaGetLastError();
+}
+
+// The launch sequence of a repeated evaluation with fixed geometry: reset the
+// work queue, far kernel, finalize with the near-pair list and FP64 near-pair
+// moments that stage 2 left in pair_ws (they depend on geometry and k, not on
+// the currents). Captured once into a CUDA graph by bielcc_batch_plan_create.
+cudaError_t batch_replay(BatchPlan& bp, const BatchDevPtrs& d, long long n_near, void* pair_ws, double analytic_calc,
+                         int n_start, cudaStream_t s) {
+    const size_t T = bp.total_pts;
+    cudaError_t e = cudaMemsetAsync(d.counter, 0, sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    const size_t smem = bp.mixed ? BatchCfg<true>::smem_bytes() : BatchCfg<false>::smem_bytes();
+    const int n_items = (int)bp.items.size();
+    if (n_items > 0) {
+        if (bp.mixed)
+            batch_far_kernel<true><<<bp.grid, kBT, smem, s>>>(d.jobs, d.items, n_items, d.counter, analytic_calc,
+                                                             n_start, bp.max_items);
+        else
+            batch_far_kernel<false><<<bp.grid, kBT, smem, s>>>(d.jobs, d.items, n_items, d.counter, analytic_calc,
+                                                              n_start, bp.max_items);
+    }
+    if (T) {
+        const cplx* moments = nullptr;
+        const int* pair_cell = nullptr;
+        if (n_near > 0) {
+            moments = (const cplx*)pair_ws;
+            pair_cell = (const int*)((const char*)pair_ws + al256((size_t)n_near * 13 * sizeof(cplx)));
+        }
+        batch_finalize_kernel<<<(int)((T + 127) / 128), 128, 0, s>>>(d.jobs, d.pt_job, (int)T,
+                                                                      n_near > 0 ? d.offs : nullptr, pair_cell,
+                                                                      moments, nullptr);
     }
     return cudaGetLastError();
 }

@@ -8,6 +8,8 @@
 
 #include "common.cuh"
 
+struct bielcc_ctx_s;  // the C ABI's context (api.cu)
+
 namespace bielcc_gpu {
 
 struct NumParamH {
@@ -31,6 +33,9 @@ struct MeshDev {
 
 // ---- api.cu: records `msg` as this thread's bielcc_last_error() and returns code
 int set_api_error(int code, const char* msg);
+// a context's mesh with node tables ready for n_start; the context's device
+int server_mesh(::bielcc_ctx_s* ctx, int32_t id, int n_start, MeshDev** out);
+int server_device(::bielcc_ctx_s* ctx);
 
 // ---- mesh.cu
 cudaError_t launch_cell_geometry(const double* verts, int nv, int n_cells, CellGeo* geo, cudaStream_t s);
@@ -116,6 +121,9 @@ struct JobDev {
     int add_E, add_H;
     double* E;
     double* H;
+    float* E32;                     // complex64 outputs instead of E / H when set
+    float* H32;
+    unsigned long long* nonfinite;  // per-job count of points with a non-finite output (may be null)
     double* partial;  // [ranges][S][12][P]
     unsigned* mask;   // [words][P]
     int n_words, ranges, cells_per_range;
@@ -132,8 +140,14 @@ struct BatchPlan {
     size_t ws_bytes = 0;  // per-job partials + masks + global tables
     int total_pts = 0;
     int grid = 0;
+    // items a CTA takes before it exits: unbounded = persistent grid of
+    // resident CTAs; 1 with grid = items = every CTA retires after one item,
+    // so batches on higher-priority streams get SMs within one item's time
+    int max_items = 1 << 30;
     bool mixed = true, ck = false;
 };
+// Turns a planned batch into one CTA per item (see BatchPlan::max_items).
+void batch_make_preemptible(BatchPlan& bp);
 
 struct BatchDevPtrs {
     JobDev* jobs;
@@ -145,6 +159,9 @@ struct BatchDevPtrs {
     int* counter;
 };
 
+// Cells per item of one job (a multiple of 32; at most 6 ranges per job);
+// depends on the job and item_cost only.
+int batch_cells_per_range(int n_cells, int n_rhs, int n_start, double item_cost);
 void plan_batch(BatchPlan& bp, const std::vector<JobDev>& jobs, int n_start, bool mixed, double item_cost);
 cudaError_t batch_stage1(BatchPlan& bp, void* ws, double analytic_calc, int n_start, bool ck, cudaStream_t s,
                          BatchDevPtrs* out, int* launches);
@@ -152,6 +169,8 @@ size_t batch_pair_ws_bytes(long long n_near);
 struct DNP;
 cudaError_t batch_stage2(BatchPlan& bp, const BatchDevPtrs& d, long long n_near, void* pair_ws, const DNP& np,
                          unsigned long long* d_nonfinite, cudaStream_t s, int* launches);
+cudaError_t batch_replay(BatchPlan& bp, const BatchDevPtrs& d, long long n_near, void* pair_ws, double analytic_calc,
+                         int n_start, cudaStream_t s);
 // largest n_start the batched kernel stages (node tile capacity)
 constexpr int kBatchMaxNStart = 22;
 

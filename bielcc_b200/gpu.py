@@ -64,9 +64,25 @@ def load(path=LIB_PATH):
                                 C.POINTER(abi.Report)])
     d("bielcc_batch_autotune", [vp, C.c_int, C.POINTER(abi.FieldJob), C.POINTER(abi.NumParam), C.c_int, vp,
                                 C.POINTER(C.c_double)])
+    d("bielcc_batch_plan_create", [vp, C.c_int, C.POINTER(abi.FieldJob), C.POINTER(abi.NumParam), C.c_int, vp,
+                                   C.POINTER(vp), C.POINTER(abi.Report)])
+    d("bielcc_batch_plan_launch", [vp, vp])
+    d("bielcc_batch_plan_destroy", [vp])
     d("bielcc_ctx_set_timing", [vp, C.c_int])
     d("bielcc_measure_fma_peak", [C.c_int, C.POINTER(C.c_double)])
     d("bielcc_ctx_stats", [vp, C.POINTER(abi.Stats), C.c_int])
+    d("bielcc_server_create", [vp, C.c_int64, C.c_int, C.POINTER(abi.NumParam), C.c_int, C.POINTER(vp)])
+    d("bielcc_server_destroy", [vp])
+    d("bielcc_server_set_item_cost", [vp, C.c_double])
+    d("bielcc_server_set_max_batch", [vp, C.c_int])
+    d("bielcc_server_submit_field", [vp, C.POINTER(abi.FieldRequest), C.POINTER(C.c_int64)])
+    d("bielcc_server_submit_assemble", [vp, C.POINTER(abi.AssembleRequest), C.POINTER(C.c_int64)])
+    d("bielcc_server_poll", [vp, C.c_int64, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)])
+    d("bielcc_server_wait", [vp, C.c_int64, C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_double)])
+    d("bielcc_server_cancel", [vp, C.c_int64])
+    d("bielcc_server_pause", [vp, C.c_int])
+    d("bielcc_server_drain", [vp, C.c_double])
+    d("bielcc_server_get_stats", [vp, C.POINTER(abi.ServerStats), C.c_int])
     abi.declare_common(L, "bielcc_")
     if L.bielcc_abi_version() != abi.ABI_VERSION:
         raise RuntimeError(f"{path}: ABI {L.bielcc_abi_version()} != {abi.ABI_VERSION}")
@@ -240,6 +256,12 @@ class Context:
                                           C.c_void_p(stream) if stream else None, C.byref(c)))
         return c.value
 
+    def batch_plan(self, jobs, numparam=None, precision="mixed", stream=None):
+        """Plans a batch for repeated evaluation (fixed geometry, new currents in
+        place) and runs it once; returns a BatchPlan whose launch() replays the
+        captured CUDA graph."""
+        return BatchPlan(self, jobs, numparam, precision, stream)
+
     # ------------------------------------------------------------------ per-pair operators
     def pair_op(self, op, cells, x, j, k, numparam=None):
         cells, x = _c(cells), _c(x)
@@ -332,3 +354,135 @@ class Context:
                                              PREC[precision], C.c_void_p(A_dev), C.c_void_p(stream) if stream else None,
                                              C.byref(rep)))
         return rep
+
+
+class BatchPlan:
+    """bielcc_batch_plan: a batch captured once in a CUDA graph."""
+
+    def __init__(self, ctx, jobs, numparam=None, precision="mixed", stream=None):
+        self.ctx, self.jobs = ctx, jobs
+        np_ = numparam if numparam is not None else abi.NumParam.default()
+        h = C.c_void_p()
+        self.report = abi.Report()
+        _check(_lib.bielcc_batch_plan_create(ctx.h, len(jobs), jobs, C.byref(np_), PREC[precision],
+                                             C.c_void_p(stream) if stream else None, C.byref(h),
+                                             C.byref(self.report)))
+        self.h = h
+
+    def launch(self, stream=None):
+        _check(_lib.bielcc_batch_plan_launch(self.h, C.c_void_p(stream) if stream else None))
+
+    def close(self):
+        if self.h:
+            _check(_lib.bielcc_batch_plan_destroy(self.h))
+            self.h = None
+
+
+class Server:
+    """Continuous-batching request loop over a Context's resident meshes
+    (bielcc_server_*). Requests return a ticket at once; wait / poll hand back
+    (status, latency_ms, outputs) once the request finished."""
+
+    def __init__(self, ctx, hbm_budget=0, n_slots=2, numparam=None, precision="mixed", max_batch=None,
+                 item_cost=None):
+        self.ctx = ctx
+        np_ = numparam if numparam is not None else abi.NumParam.default()
+        h = C.c_void_p()
+        _check(_lib.bielcc_server_create(ctx.h, int(hbm_budget), int(n_slots), C.byref(np_), PREC[precision],
+                                         C.byref(h)))
+        self.h = h
+        self._live = {}
+        if max_batch is not None:
+            _check(_lib.bielcc_server_set_max_batch(self.h, int(max_batch)))
+        if item_cost is not None:
+            _check(_lib.bielcc_server_set_item_cost(self.h, float(item_cost)))
+
+    def submit_field(self, mesh, J, pts, k, mult=1.0, inc=None, with_H=True, out_c64=True, J_dev=None, n_rhs=None,
+                     out=None):
+        """J: complex [S][N][3] host array, or J=None with J_dev (device pointer) and n_rhs.
+        out: optional caller-owned (E, H) arrays ([S][P][3], complex64 or complex128 per out_c64)."""
+        pts = _c(pts)
+        if J is not None:
+            J = _c(J, np.complex128).reshape(-1, mesh.n_cells, 3)
+            n_rhs = J.shape[0]
+        elif not J_dev or not n_rhs:
+            raise ValueError("J or (J_dev, n_rhs) required")
+        P = pts.shape[0]
+        dt = np.complex64 if out_c64 else np.complex128
+        if out is not None:
+            E, H = out
+            for a in (E, H):
+                if a is not None and (a.dtype != dt or a.shape != (n_rhs, P, 3) or not a.flags.c_contiguous):
+                    raise ValueError("out arrays must be C-contiguous [S][P][3] of the output dtype")
+        else:
+            E = np.zeros((n_rhs, P, 3), dt)
+            H = np.zeros((n_rhs, P, 3), dt) if with_H else None
+        r = abi.FieldRequest()
+        r.mesh, r.n_rhs, r.n_pts, r.out_c64 = mesh.id, n_rhs, P, int(bool(out_c64))
+        r.J = J.ctypes.data if J is not None else None
+        r.J_dev = int(J_dev) if J is None else None
+        r.pts = pts.ctypes.data
+        r.E = E.ctypes.data
+        r.H = H.ctypes.data if H is not None else None
+        k, mult = complex(k), complex(mult)
+        r.k_re, r.k_im, r.mult_re, r.mult_im = k.real, k.imag, mult.real, mult.imag
+        if inc is not None:
+            r.inc = inc
+        t = C.c_int64(0)
+        _check(_lib.bielcc_server_submit_field(self.h, C.byref(r), C.byref(t)))
+        self._live[t.value] = (r, J, pts, {"E": E, "H": H})
+        return t.value
+
+    def submit_assemble(self, mesh, k, layout="tau2", out_c64=True, out=None):
+        m = 2 if layout == "tau2" else 3
+        dt = np.complex64 if out_c64 else np.complex128
+        shape = (m * mesh.n_cells, m * mesh.n_cells)
+        if out is not None:
+            if out.dtype != dt or out.shape != shape or not out.flags.c_contiguous:
+                raise ValueError("out must be a C-contiguous matrix of the output dtype")
+            A = out
+        else:
+            A = np.zeros(shape, dt)
+        r = abi.AssembleRequest()
+        r.mesh = mesh.id
+        r.layout = abi.LAYOUT_TAU2 if layout == "tau2" else abi.LAYOUT_FULL3
+        r.out_c64 = int(bool(out_c64))
+        r.A = A.ctypes.data
+        k = complex(k)
+        r.k_re, r.k_im = k.real, k.imag
+        t = C.c_int64(0)
+        _check(_lib.bielcc_server_submit_assemble(self.h, C.byref(r), C.byref(t)))
+        self._live[t.value] = (r, None, None, {"A": A})
+        return t.value
+
+    def poll(self, ticket):
+        done, st, lat = C.c_int(0), C.c_int(0), C.c_double(0)
+        _check(_lib.bielcc_server_poll(self.h, ticket, C.byref(done), C.byref(st), C.byref(lat)))
+        if not done.value:
+            return None
+        return st.value, lat.value, self._live.pop(ticket)[3]
+
+    def wait(self, ticket, timeout=120.0):
+        st, lat = C.c_int(0), C.c_double(0)
+        _check(_lib.bielcc_server_wait(self.h, ticket, float(timeout), C.byref(st), C.byref(lat)))
+        return st.value, lat.value, self._live.pop(ticket)[3]
+
+    def pause(self, paused=True):
+        _check(_lib.bielcc_server_pause(self.h, int(bool(paused))))
+
+    def cancel(self, ticket):
+        _check(_lib.bielcc_server_cancel(self.h, ticket))
+
+    def drain(self, timeout=600.0):
+        _check(_lib.bielcc_server_drain(self.h, float(timeout)))
+
+    def stats(self, reset=False):
+        st = abi.ServerStats()
+        _check(_lib.bielcc_server_get_stats(self.h, C.byref(st), int(bool(reset))))
+        return st.as_dict()
+
+    def close(self):
+        if self.h:
+            _check(_lib.bielcc_server_destroy(self.h))
+            self.h = None
+            self._live.clear()

@@ -258,3 +258,50 @@ def batch_meshes(n_meshes=256, seed=3, n_min=200, n_max=20000, pts_per_mesh=2000
         pts = shell_points(pts_per_mesh, 2.0 * extent, 4.0 * extent, rng)
         out.append(dict(cells=cells, k=k, J=J, pts=pts))
     return out
+
+
+def serving_stream(n_requests=400, seed=4, n_meshes=24, n_min=200, n_max=20000, p_min=100, p_max=50000,
+                   rhs_max=16, assembly_frac=0.1, max_assembly_cells=2000, near_frac=0.1):
+    """Request stream of the serving workload. Meshes are drawn like
+    batch_meshes (spheroids, rounded cubes, tori; 200-20000 cells log-uniform;
+    k log-uniform in [0.5, 20]) and stay resident; each carries rhs_max PO
+    current sets and a pool of p_max observation points (near_frac of them
+    0.02-0.1 x the mesh extent above random cells, the rest on a 1.5-4 x
+    extent shell). Requests arrive as a Poisson process of unit rate (arrival
+    times are scaled by the caller's rate); a field request takes 100-50000
+    points (log-uniform, the first P of its mesh's pool) and 1-16 current
+    sets (the first S); assembly requests (assembly_frac of them) go to meshes
+    of at most max_assembly_cells cells."""
+    rng = np.random.default_rng(seed)
+    meshes = []
+    for i in range(n_meshes):
+        kind = i % 3
+        target = float(np.exp(rng.uniform(np.log(n_min), np.log(n_max))))
+        if kind == 0:
+            n_lat = max(4, int(round((target / 2) ** 0.5)))
+            cells = spheroid(n_lat, 2 * n_lat, 1.0, rng.uniform(1.0, 4.0))
+        elif kind == 1:
+            cells = rounded_cube(max(4, int(round((target / 2) ** 0.5))), 0.1, 1.0)
+        else:
+            nv = max(4, int(round((target / 3) ** 0.5)))
+            cells = torus(3 * nv, nv, 1.5, 0.5)
+        k = float(np.exp(rng.uniform(np.log(0.5), np.log(20.0))))
+        extent = float(np.max(np.linalg.norm(cells.reshape(-1, 3), axis=1)))
+        n_near = int(near_frac * p_max)
+        pool = np.concatenate([shell_points(p_max - n_near, 1.5 * extent, 4.0 * extent, rng),
+                               near_points(cells, n_near, 0.02 * extent, 0.1 * extent, rng)])
+        pool = pool[rng.permutation(len(pool))]
+        J = po_currents(cells, k, directions=rhs_max, seed=int(rng.integers(1 << 31)))
+        meshes.append(dict(cells=cells, k=k, J=J, pts=np.ascontiguousarray(pool)))
+    small = [i for i, m in enumerate(meshes) if len(m["cells"]) <= max_assembly_cells]
+    t = 0.0
+    reqs = []
+    for _ in range(n_requests):
+        t += float(rng.exponential(1.0))
+        if small and rng.uniform() < assembly_frac:
+            reqs.append(dict(t=t, type="assemble", mesh=int(rng.choice(small))))
+        else:
+            P = int(round(np.exp(rng.uniform(np.log(p_min), np.log(p_max)))))
+            reqs.append(dict(t=t, type="field", mesh=int(rng.integers(n_meshes)), P=P,
+                             S=int(rng.integers(1, rhs_max + 1))))
+    return meshes, reqs

@@ -47,6 +47,7 @@ extern "C" {
 #define BIELCC_ERR_UNSUPPORTED   -6  /* valid input outside what the GPU path covers */
 #define BIELCC_ERR_NOT_FOUND     -7  /* unknown mesh / request handle */
 #define BIELCC_ERR_BUSY          -8  /* admission refused (serving queue full) */
+#define BIELCC_ERR_CANCELLED     -9  /* serving request cancelled before it ran */
 
 /* ---- numerical parameters -------------------------------------------- */
 /* Mirrors NumParam (electrodynamics/num_param.h:28-55); defaults are the
@@ -241,6 +242,27 @@ int bielcc_batch_autotune(bielcc_ctx ctx, int n_jobs, const bielcc_field_job* jo
                           const bielcc_numparam* np, int precision, void* stream,
                           double* item_cost);
 
+/* A batch planned once for repeated evaluation with fixed geometry: meshes,
+ * points, k, mult and incident field are fixed when the plan is made; the
+ * currents J (new contents at the same device addresses) may change between
+ * launches, as in an iterative solve or a sweep over incident fields.
+ * bielcc_batch_plan_create runs the full batch once (outputs valid when the
+ * stream reaches that point) and keeps its work items, workspaces, near-pair
+ * list and FP64 near-pair moments (they depend on geometry and k only); the
+ * sequence of every later evaluation (reset of the work queue, the
+ * persistent far kernel, finalize) is captured once in a CUDA graph, which
+ * bielcc_batch_plan_launch replays on a stream: no host planning, no host
+ * round trip, 3 graph nodes. Results are identical to bielcc_field_EH_batch
+ * with the same J. p_max must be 1 and n_start <= 22. The plan owns its
+ * device memory; the jobs' buffers must outlive it. No counterpart in the
+ * reference. */
+typedef struct bielcc_batch_plan_s* bielcc_batch_plan;
+int bielcc_batch_plan_create(bielcc_ctx ctx, int n_jobs, const bielcc_field_job* jobs,
+                             const bielcc_numparam* np, int precision, void* stream,
+                             bielcc_batch_plan* out, bielcc_report* report);
+int bielcc_batch_plan_launch(bielcc_batch_plan plan, void* stream);
+int bielcc_batch_plan_destroy(bielcc_batch_plan plan);
+
 /* ---- per-pair operators ----------------------------------------------- */
 /* One operator applied to n_pairs independent (cell, x, j) triples, each as
  * the reference call op(j, x, cell, num_param, k, res):
@@ -350,6 +372,97 @@ int bielcc_assemble_K_device(bielcc_ctx ctx, bielcc_mesh mesh, double k_re, doub
                              const bielcc_numparam* np, int layout, int out_c64,
                              int precision, void* A_dev, void* stream,
                              bielcc_report* report);
+
+/* ---- serving: continuous batching ---------------------------------------
+ * A server runs field and assembly requests submitted at any time, from any
+ * thread, against meshes resident in its context. It owns n_slots slots (a
+ * CUDA stream, device workspaces and pinned staging each) and a scheduler
+ * thread. Whenever a slot is idle the scheduler admits queued requests in
+ * arrival order while their device bytes fit the HBM budget: every field
+ * request admitted together runs as ONE bielcc_field_EH_batch launch, an
+ * assembly request runs alone. Requests that arrive while batches are on the
+ * GPU are admitted as soon as a slot and memory free up, and their work
+ * overlaps the running batches on the other slots' streams; a batch smaller
+ * than one already running goes to a high-priority stream and takes SMs as
+ * soon as the running batch's CTAs retire (each far-kernel CTA of a served
+ * batch handles one work item). A request's
+ * result depends only on the request (never on the rest of its batch), so it
+ * is the same alone and in any mix. No counterpart in the reference (it has
+ * no request loop). Meshes a server uses must stay alive, and must not be
+ * evaluated through the context with another n_start, while the server holds
+ * requests on them. */
+typedef struct bielcc_server_s* bielcc_server;
+
+typedef struct bielcc_field_request {
+    bielcc_mesh mesh;
+    int32_t n_rhs;
+    int32_t n_pts;
+    int32_t out_c64;        /* 1: E/H written as complex64, 0: complex128 */
+    const double* J;        /* host [n_rhs][n_cells][3] complex; or NULL and: */
+    const double* J_dev;    /* device-resident currents, same layout */
+    const double* pts;      /* host [n_pts][3] */
+    void* E;                /* host [n_rhs][n_pts][3] complex, written on completion */
+    void* H;                /* host, may be NULL */
+    double k_re, k_im, mult_re, mult_im;
+    bielcc_planewave inc;   /* add_E = add_H = 0 for no incident field */
+} bielcc_field_request;
+
+typedef struct bielcc_assemble_request {
+    bielcc_mesh mesh;
+    int32_t layout;         /* BIELCC_LAYOUT_TAU2 / BIELCC_LAYOUT_FULL3 */
+    int32_t out_c64;
+    void* A;                /* host matrix, written on completion; or NULL and: */
+    void* A_dev;            /* device matrix owned by the caller */
+    double k_re, k_im;
+} bielcc_assemble_request;
+
+typedef struct bielcc_server_stats {
+    int64_t submitted, completed, failed, cancelled, rejected, queued, running;
+    int64_t batches;              /* GPU batches launched */
+    int64_t priority_batches;     /* of which: launched at high priority to overtake a larger running batch */
+    int64_t max_batch;            /* most requests in one batch */
+    int64_t bytes_reserved;       /* device bytes held by admitted requests now */
+    int64_t peak_bytes_reserved;
+    int64_t bytes_allocated;      /* device bytes the slots hold now */
+    int64_t budget;
+    int64_t pairs_done;           /* (point, cell, RHS) pairs of completed field requests */
+    double p50_ms, p99_ms, mean_ms, max_ms;  /* submit -> result in the caller's buffer */
+    double wall_s;                /* first submit -> last completion */
+    double pairs_per_s;           /* pairs_done / wall_s */
+    double stage_in_s;            /* host time slots spent staging inputs and launching stage 1 */
+    double copy_out_s;            /* host time slots spent copying results into the callers' buffers */
+} bielcc_server_stats;
+
+/* hbm_budget <= 0 selects 150 GiB. np: NULL for the defaults; the server runs
+ * the batched kernel, so np->p_max must be 1 and np->n_start <= 22. */
+int bielcc_server_create(bielcc_ctx ctx, int64_t hbm_budget, int n_slots, const bielcc_numparam* np,
+                         int precision, bielcc_server* out);
+/* Drains the server (bounded wait), then frees it. */
+int bielcc_server_destroy(bielcc_server sv);
+/* Node evaluations per batched work item (bielcc_batch_autotune's result). */
+int bielcc_server_set_item_cost(bielcc_server sv, double item_cost);
+/* Most requests one batch admits (default 64). */
+int bielcc_server_set_max_batch(bielcc_server sv, int max_batch);
+/* paused = 1: queue requests without admitting any (running batches finish);
+ * 0: resume. Lets a caller release a burst of requests as one batch. */
+int bielcc_server_pause(bielcc_server sv, int paused);
+/* Queue a request; returns at once with a ticket. The host input buffers are
+ * read when the request is admitted, the output buffers written when it
+ * completes: keep them alive until bielcc_server_poll reports done.
+ * BIELCC_ERR_BUSY: the request alone exceeds the budget. */
+int bielcc_server_submit_field(bielcc_server sv, const bielcc_field_request* req, int64_t* ticket);
+int bielcc_server_submit_assemble(bielcc_server sv, const bielcc_assemble_request* req, int64_t* ticket);
+/* *done = 1 once the request finished; then *status is its result code and
+ * *latency_ms its submit-to-completion time, and the ticket is released. */
+int bielcc_server_poll(bielcc_server sv, int64_t ticket, int* done, int* status, double* latency_ms);
+/* Blocks (at most timeout_s) until the ticket's request finished; same outputs. */
+int bielcc_server_wait(bielcc_server sv, int64_t ticket, double timeout_s, int* status, double* latency_ms);
+/* Removes a request that is still queued (its status becomes
+ * BIELCC_ERR_CANCELLED); BIELCC_ERR_BUSY once it was admitted. */
+int bielcc_server_cancel(bielcc_server sv, int64_t ticket);
+/* Blocks (at most timeout_s) until nothing is queued or running. */
+int bielcc_server_drain(bielcc_server sv, double timeout_s);
+int bielcc_server_get_stats(bielcc_server sv, bielcc_server_stats* out, int reset);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop
