@@ -193,9 +193,11 @@ class ServerStats(C.Structure):
     _fields_ = [(n, C.c_int64) for n in (
         "submitted", "completed", "failed", "cancelled", "rejected", "queued", "running", "batches", "priority_batches",
         "max_batch",
-        "bytes_reserved", "peak_bytes_reserved", "bytes_allocated", "budget", "pairs_done")] + \
+        "bytes_reserved", "peak_bytes_reserved", "bytes_allocated", "budget", "pairs_done", "pool_mapped_bytes",
+        "pinned_bytes")] + \
         [(n, C.c_double) for n in ("p50_ms", "p99_ms", "mean_ms", "max_ms", "wall_s", "pairs_per_s", "stage_in_s",
-                                   "copy_out_s")]
+                                   "copy_out_s", "gpu_busy_s", "stage_alloc_s", "stage_copy_s", "stage_plan_s",
+                                   "stage_launch_s")]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}

@@ -25,6 +25,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <thread>
@@ -42,52 +43,107 @@ namespace {
 
 size_t al(size_t b) { return (b + 255) & ~(size_t)255; }
 
-// Stream-ordered device buffer: growing it never stalls the other slots.
-// Shrinks when a batch needs under a quarter of a large buffer, so an idle
-// slot does not hoard HBM that the budget has handed to other requests.
+// Device buffer of one batch, allocated stream-ordered from the server's
+// memory pool and returned to it when the batch's stream reaches its end. The
+// pool keeps its memory mapped (release threshold = unlimited), so a batch's
+// allocations reuse memory instead of mapping new pages, and memory freed by
+// one slot is reused by the others.
 struct SBuf {
     void* p = nullptr;
-    std::atomic<size_t> cap{0};  // read by bielcc_server_stats from other threads
+    cudaMemPool_t pool = nullptr;
     cudaError_t ensure(size_t b, cudaStream_t s) {
-        const size_t c = cap.load();
-        if (b <= c && !(c > 4 * b && c > ((size_t)256 << 20))) return cudaSuccess;
         release(s);
-        const size_t want = b + b / 4 + 4096;
-        cudaError_t e = cudaMallocAsync(&p, want, s);
-        if (e != cudaSuccess) {
-            p = nullptr;
-            return e;
-        }
-        cap = want;
-        return cudaSuccess;
+        if (!b) return cudaSuccess;
+        cudaError_t e = cudaMallocFromPoolAsync(&p, b, pool, s);
+        if (e != cudaSuccess) p = nullptr;
+        return e;
     }
     void release(cudaStream_t s) {
         if (p) cudaFreeAsync(p, s);
         p = nullptr;
-        cap = 0;
     }
 };
 
-// Pinned host staging; grow-only (pinning pages is slow).
-struct PinBuf {
+// Pinned host staging shared by the slots: large pinned regions (pinned once,
+// kept until the server is destroyed: pinning is slow and freeing pinned
+// memory synchronises the device), sub-allocated first-fit in 4 KiB units; a
+// slot holds one range per batch and returns it when the results are in the
+// callers' buffers. Free ranges are coalesced within their region.
+struct PinRef {
     void* p = nullptr;
     size_t cap = 0;
-    cudaError_t ensure(size_t b) {
-        if (b <= cap) return cudaSuccess;
-        release();
-        const size_t want = b + b / 4 + 4096;
-        cudaError_t e = cudaMallocHost(&p, want);
-        if (e != cudaSuccess) {
-            p = nullptr;
-            return e;
-        }
-        cap = want;
+};
+struct PinPool {
+    static constexpr size_t kMinRegion = (size_t)256 << 20;
+    std::mutex mu;
+    std::vector<std::pair<char*, size_t>> regions;
+    std::map<char*, size_t> free_;  // start -> bytes
+    size_t pinned = 0;
+    double alloc_s = 0;
+
+    bool same_region(const char* a, const char* b) const {
+        for (const auto& r : regions)
+            if (a >= r.first && a < r.first + r.second) return b >= r.first && b < r.first + r.second;
+        return false;
+    }
+    cudaError_t add_region(size_t bytes) {  // caller holds mu
+        char* p = nullptr;
+        const auto t0 = Clock::now();
+        cudaError_t e = cudaMallocHost((void**)&p, bytes);
+        alloc_s += std::chrono::duration<double>(Clock::now() - t0).count();
+        if (e != cudaSuccess) return e;
+        regions.emplace_back(p, bytes);
+        free_[p] = bytes;
+        pinned += bytes;
         return cudaSuccess;
     }
-    void release() {
-        if (p) cudaFreeHost(p);
-        p = nullptr;
-        cap = 0;
+    cudaError_t acquire(size_t b, PinRef& out) {
+        b = (std::max<size_t>(b, 1) + 4095) & ~(size_t)4095;
+        std::lock_guard<std::mutex> g(mu);
+        for (int pass = 0; pass < 2; pass++) {
+            for (auto it = free_.begin(); it != free_.end(); ++it) {
+                if (it->second < b) continue;
+                out.p = it->first;
+                out.cap = b;
+                if (it->second > b) free_[it->first + b] = it->second - b;
+                free_.erase(it);
+                return cudaSuccess;
+            }
+            if (pass == 0) {
+                cudaError_t e = add_region(std::max(b, kMinRegion));
+                if (e != cudaSuccess) return e;
+            }
+        }
+        return cudaErrorMemoryAllocation;
+    }
+    void release(PinRef& r) {
+        if (!r.p) return;
+        std::lock_guard<std::mutex> g(mu);
+        char* p = (char*)r.p;
+        size_t n = r.cap;
+        auto next = free_.lower_bound(p);
+        if (next != free_.end() && p + n == next->first && same_region(p, next->first)) {
+            n += next->second;
+            next = free_.erase(next);
+        }
+        if (next != free_.begin()) {
+            auto prev = std::prev(next);
+            if (prev->first + prev->second == p && same_region(prev->first, p)) {
+                prev->second += n;
+                r.p = nullptr;
+                r.cap = 0;
+                return;
+            }
+        }
+        free_[p] = n;
+        r.p = nullptr;
+        r.cap = 0;
+    }
+    void destroy() {
+        for (auto& r : regions) cudaFreeHost(r.first);
+        regions.clear();
+        free_.clear();
+        pinned = 0;
     }
 };
 
@@ -119,10 +175,11 @@ struct Slot {
     cudaStream_t s_hi = nullptr, s_lo = nullptr, s = nullptr;
     int64_t work = 0;  // pairs of the current batch
     cudaEvent_t ev_stage1 = nullptr, ev_done = nullptr;
+    cudaEvent_t ev_begin = nullptr, ev_end = nullptr;  // timed: the batch's span on the GPU
     std::atomic<int> state{kIdle};  // written by the scheduler and the completion thread
     std::vector<Req*> reqs;
     SBuf ws, pair_ws, io;
-    PinBuf pin;
+    PinRef pin;  // pinned staging block of the current batch
     long long* h_total = nullptr;  // pinned
     long long* d_total = nullptr;  // assembly near count
     BatchPlan bp;
@@ -147,16 +204,22 @@ struct bielcc_server_s {
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::vector<std::thread> workers;  // one per slot
+    cudaMemPool_t pool = nullptr;      // device memory of the batches
+    PinPool pins;
     std::atomic<bool> stop{false};
     int64_t next_ticket = 1;
     int max_batch = 64;
     bool paused = false;
+    bool preemptible = true;
+    cudaEvent_t ev_ref = nullptr;              // time origin of the batch spans
+    std::vector<std::pair<double, double>> spans;  // [begin, end] ms of every batch on the GPU
     double item_cost = 4.0e6;
     int running = 0;
     std::vector<double> lat_ms;
     int64_t submitted = 0, completed = 0, failed = 0, cancelled = 0, rejected = 0, batches = 0, max_in_batch = 0,
             pairs_done = 0, priority_batches = 0;
     double stage_in_s = 0, copy_out_s = 0;  // host time of input staging / result copies, summed over batches
+    double st_alloc = 0, st_copy = 0, st_plan = 0, st_launch = 0;  // parts of stage_in_s
     Clock::time_point t_first, t_last;
     bool any = false;
 };
@@ -235,9 +298,11 @@ cudaError_t start_field_batch(bielcc_server_s* sv, Slot& sl) {
     sl.nan_off = off;
     off += al(sl.reqs.size() * 8);
     sl.out_total = off - sl.out_base;
+    auto t0 = Clock::now();
     cudaError_t e = sl.io.ensure(off, sl.s);
-    if (e == cudaSuccess) e = sl.pin.ensure(off);
+    if (e == cudaSuccess) e = sv->pins.acquire(off, sl.pin);
     if (e != cudaSuccess) return e;
+    auto t1 = Clock::now();
     char* dev = (char*)sl.io.p;
     char* pin = (char*)sl.pin.p;
     for (Req* r : sl.reqs) {
@@ -245,7 +310,9 @@ cudaError_t start_field_batch(bielcc_server_s* sv, Slot& sl) {
         if (!r->f.J_dev) memcpy(pin + r->in_J, r->f.J, S * N * 48);
         memcpy(pin + r->in_P, r->f.pts, P * 24);
     }
-    if (in_bytes) e = cudaMemcpyAsync(dev, pin, in_bytes, cudaMemcpyHostToDevice, sl.s);
+    auto t2 = Clock::now();
+    e = cudaEventRecord(sl.ev_begin, sl.s);  // the batch's GPU span starts with its input copy
+    if (e == cudaSuccess && in_bytes) e = cudaMemcpyAsync(dev, pin, in_bytes, cudaMemcpyHostToDevice, sl.s);
     if (e == cudaSuccess) e = cudaMemsetAsync(dev + sl.nan_off, 0, sl.reqs.size() * 8, sl.s);
     if (e != cudaSuccess) return e;
     std::vector<JobDev> jd(sl.reqs.size());
@@ -284,13 +351,23 @@ cudaError_t start_field_batch(bielcc_server_s* sv, Slot& sl) {
         }
         d.nonfinite = (unsigned long long*)(dev + sl.nan_off) + i;
     }
+    auto t3 = Clock::now();
     plan_batch(sl.bp, jd, sv->np.n_start, sv->precision == BIELCC_PREC_MIXED, sv->item_cost);
-    batch_make_preemptible(sl.bp);
+    if (sv->preemptible) batch_make_preemptible(sl.bp);
+    auto t4 = Clock::now();
     e = sl.ws.ensure(sl.bp.ws_bytes, sl.s);
     if (e != cudaSuccess) return e;
+    auto t5 = Clock::now();
     int launches = 0;
     e = batch_stage1(sl.bp, sl.ws.p, sv->np.analytic_calc, sv->np.n_start, false, sl.s, &sl.d, &launches);
     if (e == cudaSuccess) e = cudaMemcpyAsync(sl.h_total, sl.d.total, sizeof(long long), cudaMemcpyDeviceToHost, sl.s);
+    auto t6 = Clock::now();
+    auto sec = [](Clock::time_point a, Clock::time_point b) { return std::chrono::duration<double>(b - a).count(); };
+    std::lock_guard<std::mutex> g(sv->mu);
+    sv->st_alloc += sec(t0, t1) + sec(t4, t5);
+    sv->st_copy += sec(t1, t2);
+    sv->st_plan += sec(t2, t4);
+    sv->st_launch += sec(t5, t6);
     return e;
 }
 
@@ -302,10 +379,10 @@ cudaError_t start_assemble(bielcc_server_s* sv, Slot& sl) {
     sl.out_base = 0;
     sl.out_total = r->a.A_dev ? 0 : r->out_bytes;
     void* target = r->a.A_dev;
-    cudaError_t e = cudaSuccess;
+    cudaError_t e = cudaEventRecord(sl.ev_begin, sl.s);
     if (!target) {
         e = sl.io.ensure(r->out_bytes, sl.s);
-        if (e == cudaSuccess) e = sl.pin.ensure(r->out_bytes);
+        if (e == cudaSuccess) e = sv->pins.acquire(r->out_bytes, sl.pin);
         target = sl.io.p;
     }
     if (e != cudaSuccess) return e;
@@ -357,6 +434,11 @@ cudaError_t finish_batch(bielcc_server_s* sv, Slot& sl, long long n_near, size_t
     if (e == cudaSuccess && sl.out_total)
         e = cudaMemcpyAsync((char*)sl.pin.p + sl.out_base, (char*)sl.io.p + sl.out_base, sl.out_total,
                             cudaMemcpyDeviceToHost, sl.s);
+    // the batch's device memory goes back to the pool when the stream gets here
+    sl.ws.release(sl.s);
+    sl.pair_ws.release(sl.s);
+    sl.io.release(sl.s);
+    if (e == cudaSuccess) e = cudaEventRecord(sl.ev_end, sl.s);
     if (e == cudaSuccess) e = cudaEventRecord(sl.ev_done, sl.s);
     return e;
 }
@@ -377,6 +459,7 @@ void complete_slot(bielcc_server_s* sv, Slot& sl) {
             memcpy(r->a.A, pin, r->out_bytes);
         }
     }
+    sv->pins.release(sl.pin);
     const auto now = Clock::now();
     std::lock_guard<std::mutex> g(sv->mu);
     sv->copy_out_s += std::chrono::duration<double>(now - t_out).count();
@@ -478,10 +561,20 @@ void slot_loop(bielcc_server_s* sv, Slot* slp) {
         }
         if (e == cudaSuccess) e = cudaEventSynchronize(sl.ev_done);
         if (e == cudaSuccess) {
+            float b = 0.f, t = 0.f;
+            if (cudaEventElapsedTime(&b, sv->ev_ref, sl.ev_begin) == cudaSuccess &&
+                cudaEventElapsedTime(&t, sv->ev_ref, sl.ev_end) == cudaSuccess) {
+                std::lock_guard<std::mutex> g(sv->mu);
+                sv->spans.emplace_back(b, t);
+            }
+            cudaGetLastError();
             sl.state = kCompleting;
             complete_slot(sv, sl);
         } else {
             cudaGetLastError();
+            cudaStreamSynchronize(sl.s);  // nothing of this batch may still write the pinned block
+            cudaGetLastError();
+            sv->pins.release(sl.pin);
             std::lock_guard<std::mutex> g(sv->mu);
             fail_slot_locked(sv, sl, e == cudaErrorMemoryAllocation ? BIELCC_ERR_OOM : BIELCC_ERR_CUDA);
             sv->cv_work.notify_all();
@@ -547,10 +640,23 @@ int bielcc_server_create(bielcc_ctx ctx, int64_t hbm_budget, int n_slots, const 
     sv->budget = hbm_budget > 0 ? hbm_budget : ((int64_t)150 << 30);
     sv->slot_mem.reset(new Slot[n_slots]);
     sv->n_slots = n_slots;
-    if (cudaSetDevice(sv->device) != cudaSuccess) {
-        delete sv;
-        return set_api_error(BIELCC_ERR_CUDA, "cudaSetDevice failed");
+    {
+        cudaMemPoolProps props;
+        memset(&props, 0, sizeof(props));
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = sv->device;
+        uint64_t keep = UINT64_MAX;  // never trim: batches reuse mapped memory
+        if (cudaSetDevice(sv->device) != cudaSuccess || cudaMemPoolCreate(&sv->pool, &props) != cudaSuccess ||
+            cudaMemPoolSetAttribute(sv->pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) {
+            cudaGetLastError();
+            if (sv->pool) cudaMemPoolDestroy(sv->pool);
+            delete sv;
+            return set_api_error(BIELCC_ERR_CUDA, "server memory pool set-up failed");
+        }
     }
+    for (Slot& sl : slots_of(sv)) sl.ws.pool = sl.pair_ws.pool = sl.io.pool = sv->pool;
     for (Slot& sl : slots_of(sv)) {
         int least = 0, greatest = 0;
         cudaDeviceGetStreamPriorityRange(&least, &greatest);
@@ -560,6 +666,8 @@ int bielcc_server_create(bielcc_ctx ctx, int64_t hbm_budget, int n_slots, const 
         const unsigned ef = cudaEventDisableTiming | cudaEventBlockingSync;
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.ev_stage1, ef);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.ev_done, ef);
+        if (e == cudaSuccess) e = cudaEventCreate(&sl.ev_begin);
+        if (e == cudaSuccess) e = cudaEventCreate(&sl.ev_end);
         if (e == cudaSuccess) e = cudaMallocHost(&sl.h_total, 64);
         if (e == cudaSuccess) e = cudaMalloc(&sl.d_total, 256);
         if (e != cudaSuccess) {
@@ -569,12 +677,20 @@ int bielcc_server_create(bielcc_ctx ctx, int64_t hbm_budget, int n_slots, const 
                 if (t.s_hi) cudaStreamDestroy(t.s_hi);
                 if (t.ev_stage1) cudaEventDestroy(t.ev_stage1);
                 if (t.ev_done) cudaEventDestroy(t.ev_done);
+                if (t.ev_begin) cudaEventDestroy(t.ev_begin);
+                if (t.ev_end) cudaEventDestroy(t.ev_end);
                 if (t.h_total) cudaFreeHost(t.h_total);
                 if (t.d_total) cudaFree(t.d_total);
             }
+            cudaMemPoolDestroy(sv->pool);
             delete sv;
             return set_api_error(BIELCC_ERR_CUDA, "server slot set-up failed");
         }
+    }
+    if (cudaEventCreate(&sv->ev_ref) != cudaSuccess || cudaEventRecord(sv->ev_ref, 0) != cudaSuccess ||
+        cudaEventSynchronize(sv->ev_ref) != cudaSuccess) {
+        cudaGetLastError();
+        sv->ev_ref = nullptr;
     }
     for (Slot& sl : slots_of(sv)) sv->workers.emplace_back(slot_loop, sv, &sl);
     *out = sv;
@@ -585,6 +701,39 @@ int bielcc_server_set_item_cost(bielcc_server sv, double item_cost) {
     if (!sv || !(item_cost > 0)) return set_api_error(BIELCC_ERR_ARG, "bad argument");
     std::lock_guard<std::mutex> g(sv->mu);
     sv->item_cost = item_cost;
+    return BIELCC_OK;
+}
+
+int bielcc_server_reserve(bielcc_server sv, int64_t device_bytes, int64_t pinned_bytes) {
+    if (!sv || device_bytes < 0 || pinned_bytes < 0) return set_api_error(BIELCC_ERR_ARG, "bad argument");
+    if (cudaSetDevice(sv->device) != cudaSuccess) return set_api_error(BIELCC_ERR_CUDA, "cudaSetDevice failed");
+    if (device_bytes > 0) {
+        // allocate and free once: the pool never trims, so the memory stays mapped for the batches
+        cudaStream_t s = slots_of(sv).begin()->s_lo;
+        void* p = nullptr;
+        cudaError_t e = cudaMallocFromPoolAsync(&p, (size_t)device_bytes, sv->pool, s);
+        if (e == cudaSuccess) e = cudaFreeAsync(p, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return set_api_error(e == cudaErrorMemoryAllocation ? BIELCC_ERR_OOM : BIELCC_ERR_CUDA,
+                                 "device reservation failed");
+        }
+    }
+    if (pinned_bytes > 0) {
+        std::lock_guard<std::mutex> g(sv->pins.mu);
+        if (sv->pins.add_region((size_t)pinned_bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return set_api_error(BIELCC_ERR_OOM, "pinned host reservation failed");
+        }
+    }
+    return BIELCC_OK;
+}
+
+int bielcc_server_set_preemptible(bielcc_server sv, int on) {
+    if (!sv) return set_api_error(BIELCC_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> g(sv->mu);
+    sv->preemptible = on != 0;
     return BIELCC_OK;
 }
 
@@ -710,11 +859,41 @@ int bielcc_server_get_stats(bielcc_server sv, bielcc_server_stats* st, int reset
     st->batches = sv->batches;
     st->priority_batches = sv->priority_batches;
     st->stage_in_s = sv->stage_in_s;
+    st->stage_alloc_s = sv->st_alloc;
+    {
+        std::lock_guard<std::mutex> gp(sv->pins.mu);
+        st->pinned_bytes = (int64_t)sv->pins.pinned;
+    }
+    uint64_t mapped = 0;
+    if (cudaMemPoolGetAttribute(sv->pool, cudaMemPoolAttrReservedMemCurrent, &mapped) == cudaSuccess)
+        st->pool_mapped_bytes = (int64_t)mapped;
+    st->stage_copy_s = sv->st_copy;
+    st->stage_plan_s = sv->st_plan;
+    st->stage_launch_s = sv->st_launch;
+    {
+        // union of the batch spans: time the GPU had at least one batch
+        std::vector<std::pair<double, double>> v = sv->spans;
+        std::sort(v.begin(), v.end());
+        double busy = 0, cb = 0, ce = -1e300;
+        for (const auto& iv : v) {
+            if (iv.first > ce) {
+                if (ce > cb) busy += ce - cb;
+                cb = iv.first;
+                ce = iv.second;
+            } else {
+                ce = std::max(ce, iv.second);
+            }
+        }
+        if (ce > cb) busy += ce - cb;
+        st->gpu_busy_s = busy * 1e-3;
+    }
     st->copy_out_s = sv->copy_out_s;
     st->max_batch = sv->max_in_batch;
     st->bytes_reserved = sv->reserved;
     st->peak_bytes_reserved = sv->peak_reserved;
-    for (const Slot& sl : slots_of(sv)) st->bytes_allocated += (int64_t)(sl.ws.cap + sl.pair_ws.cap + sl.io.cap);
+    uint64_t used = 0;
+    if (cudaMemPoolGetAttribute(sv->pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess)
+        st->bytes_allocated = (int64_t)used;
     st->budget = sv->budget;
     st->pairs_done = sv->pairs_done;
     std::vector<double> l = sv->lat_ms;
@@ -741,6 +920,8 @@ int bielcc_server_get_stats(bielcc_server sv, bielcc_server_stats* st, int reset
         sv->submitted = sv->completed = sv->failed = sv->cancelled = sv->rejected = 0;
         sv->batches = sv->max_in_batch = sv->pairs_done = sv->priority_batches = 0;
         sv->stage_in_s = sv->copy_out_s = 0;
+        sv->st_alloc = sv->st_copy = sv->st_plan = sv->st_launch = 0;
+        sv->spans.clear();
         sv->peak_reserved = sv->reserved;
         sv->any = false;
     }
@@ -764,15 +945,20 @@ int bielcc_server_destroy(bielcc_server sv) {
         sl.ws.release(sl.s_lo);
         sl.pair_ws.release(sl.s_lo);
         sl.io.release(sl.s_lo);
+        sv->pins.release(sl.pin);
         cudaStreamSynchronize(sl.s_lo);
-        sl.pin.release();
         cudaFreeHost(sl.h_total);
         cudaFree(sl.d_total);
         cudaEventDestroy(sl.ev_stage1);
         cudaEventDestroy(sl.ev_done);
+        cudaEventDestroy(sl.ev_begin);
+        cudaEventDestroy(sl.ev_end);
         cudaStreamDestroy(sl.s_lo);
         cudaStreamDestroy(sl.s_hi);
     }
+    sv->pins.destroy();
+    cudaMemPoolDestroy(sv->pool);
+    cudaEventDestroy(sv->ev_ref);
     for (auto& kv : sv->reqs) delete kv.second;
     delete sv;
     return rc;

@@ -75,6 +75,8 @@ def load(path=LIB_PATH):
     d("bielcc_server_destroy", [vp])
     d("bielcc_server_set_item_cost", [vp, C.c_double])
     d("bielcc_server_set_max_batch", [vp, C.c_int])
+    d("bielcc_server_set_preemptible", [vp, C.c_int])
+    d("bielcc_server_reserve", [vp, C.c_int64, C.c_int64])
     d("bielcc_server_submit_field", [vp, C.POINTER(abi.FieldRequest), C.POINTER(C.c_int64)])
     d("bielcc_server_submit_assemble", [vp, C.POINTER(abi.AssembleRequest), C.POINTER(C.c_int64)])
     d("bielcc_server_poll", [vp, C.c_int64, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)])
@@ -384,7 +386,7 @@ class Server:
     (status, latency_ms, outputs) once the request finished."""
 
     def __init__(self, ctx, hbm_budget=0, n_slots=2, numparam=None, precision="mixed", max_batch=None,
-                 item_cost=None):
+                 item_cost=None, preemptible=True, reserve=None):
         self.ctx = ctx
         np_ = numparam if numparam is not None else abi.NumParam.default()
         h = C.c_void_p()
@@ -396,6 +398,9 @@ class Server:
             _check(_lib.bielcc_server_set_max_batch(self.h, int(max_batch)))
         if item_cost is not None:
             _check(_lib.bielcc_server_set_item_cost(self.h, float(item_cost)))
+        _check(_lib.bielcc_server_set_preemptible(self.h, int(bool(preemptible))))
+        if reserve is not None:
+            _check(_lib.bielcc_server_reserve(self.h, int(reserve[0]), int(reserve[1])))
 
     def submit_field(self, mesh, J, pts, k, mult=1.0, inc=None, with_H=True, out_c64=True, J_dev=None, n_rhs=None,
                      out=None):

@@ -426,11 +426,16 @@ typedef struct bielcc_server_stats {
     int64_t bytes_allocated;      /* device bytes the slots hold now */
     int64_t budget;
     int64_t pairs_done;           /* (point, cell, RHS) pairs of completed field requests */
+    int64_t pool_mapped_bytes;    /* device memory the server's pool holds mapped */
+    int64_t pinned_bytes;         /* pinned host staging the server holds */
     double p50_ms, p99_ms, mean_ms, max_ms;  /* submit -> result in the caller's buffer */
     double wall_s;                /* first submit -> last completion */
     double pairs_per_s;           /* pairs_done / wall_s */
     double stage_in_s;            /* host time slots spent staging inputs and launching stage 1 */
     double copy_out_s;            /* host time slots spent copying results into the callers' buffers */
+    double gpu_busy_s;            /* union of the batches' spans on the GPU (first copy in to last copy out) */
+    double stage_alloc_s, stage_copy_s, stage_plan_s, stage_launch_s;  /* parts of stage_in_s (field batches):
+                                     buffer acquisition, host copies into pinned staging, planning, launches */
 } bielcc_server_stats;
 
 /* hbm_budget <= 0 selects 150 GiB. np: NULL for the defaults; the server runs
@@ -441,6 +446,15 @@ int bielcc_server_create(bielcc_ctx ctx, int64_t hbm_budget, int n_slots, const 
 int bielcc_server_destroy(bielcc_server sv);
 /* Node evaluations per batched work item (bielcc_batch_autotune's result). */
 int bielcc_server_set_item_cost(bielcc_server sv, double item_cost);
+/* Maps device_bytes of the server's memory pool and pins pinned_bytes of
+ * host staging up front, so that the first batches do not pay for mapping
+ * and pinning (the memory counts against nothing but the GPU / host; the
+ * HBM budget still bounds what admitted requests use). */
+int bielcc_server_reserve(bielcc_server sv, int64_t device_bytes, int64_t pinned_bytes);
+/* on = 1 (default): every far-kernel CTA of a served batch handles one work
+ * item and retires, so a batch on a higher-priority stream gets SMs at once;
+ * 0: persistent CTAs (no overtaking inside a running batch). */
+int bielcc_server_set_preemptible(bielcc_server sv, int on);
 /* Most requests one batch admits (default 64). */
 int bielcc_server_set_max_batch(bielcc_server sv, int max_batch);
 /* paused = 1: queue requests without admitting any (running batches finish);
