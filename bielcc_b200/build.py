@@ -22,7 +22,7 @@ HOST_CC = ["-ccbin", "/usr/bin/g++"] if os.path.exists("/usr/bin/g++") else []
 # FP32 kernels: flush FP32 denormals (values here are O(1e-10..1e3), far from
 # the denormal range), so rsqrt / reciprocal need no subnormal fix-ups. FP64
 # arithmetic is unaffected by this flag.
-PER_FILE = {"field.cu": ["-ftz=true"], "assemble.cu": ["-ftz=true"]}
+PER_FILE = {"field.cu": ["-ftz=true"], "assemble.cu": ["-ftz=true"], "batch.cu": ["-ftz=true"]}
 
 
 def _stale(obj, deps):

@@ -35,12 +35,23 @@ constexpr int kBW = 4;    // warps
 constexpr int kSP = 64;   // right-hand sides staged per pass
 
 
+// Mixed form: cells per chunk at n_start <= 8, and resident CTAs per SM the
+// kernel is compiled for. Measured on the 256-mesh batch (B200): 16 cells / 2
+// CTAs (248 registers, 81 KB smem) 959 ms per batch; 12 / 3 (162 registers)
+// 1029 ms; 8 / 4 (128 registers) 1538 ms.
+#ifndef BIELCC_BATCH_CH32
+#define BIELCC_BATCH_CH32 16
+#endif
+#ifndef BIELCC_BATCH_MINB
+#define BIELCC_BATCH_MINB 2
+#endif
+
 template <bool MIXED>
 struct BatchCfg {
     using F = typename std::conditional<MIXED, float, double>::type;
     using NodeT = typename std::conditional<MIXED, float4, double4>::type;
-    static constexpr int CH = MIXED ? 16 : 8;             // cells per chunk (n_start <= 8)
-    static constexpr int NODES = MIXED ? 1024 : 512;      // staged nodes
+    static constexpr int CH = MIXED ? BIELCC_BATCH_CH32 : 8;            // cells per chunk (n_start <= 8)
+    static constexpr int NODES = MIXED ? 64 * BIELCC_BATCH_CH32 : 512;  // staged nodes
     static constexpr int R = MIXED ? 4 : 2;               // RHS per thread in phase B
     static constexpr size_t smem_bytes() {
         return sizeof(NodeT) * NODES + sizeof(F) * CH * 20 * kBP + sizeof(F) * 2 * CH * kSP * 3 +
@@ -148,7 +159,7 @@ BIELCC_D void batch_moments(const typename BatchCfg<MIXED>::NodeT* nd, int nn, c
 }
 
 template <bool MIXED>
-__global__ void __launch_bounds__(kBT, 2) batch_far_kernel(const JobDev* __restrict__ jobs,
+__global__ void __launch_bounds__(kBT, MIXED ? BIELCC_BATCH_MINB : 2) batch_far_kernel(const JobDev* __restrict__ jobs,
                                                          const BatchItem* __restrict__ items, int n_items,
                                                          int* __restrict__ counter, double analytic_calc, int n_start,
                                                          int max_items) {
@@ -276,12 +287,15 @@ __global__ void __launch_bounds__(kBT, 2) batch_far_kernel(const JobDev* __restr
                             if (sl >= sp) continue;
                             double* dst =
                                 jb.partial + (((size_t)bi.range * S + (s0 + sl)) * 12) * (size_t)P + p;
+                            // one writer per address (this thread), so the adds land in chunk
+                            // order: the fire-and-forget reduction (no load to wait for) gives
+                            // the same sums as a load-add-store
                             if (c0 == cb) {
 #pragma unroll
                                 for (int q = 0; q < 12; q++) dst[(size_t)q * P] = (double)acc[j][q];
                             } else {
 #pragma unroll
-                                for (int q = 0; q < 12; q++) dst[(size_t)q * P] += (double)acc[j][q];
+                                for (int q = 0; q < 12; q++) atomicAdd(dst + (size_t)q * P, (double)acc[j][q]);
                             }
                         }
                     }
@@ -340,6 +354,41 @@ __global__ void batch_near_pair_kernel(const JobDev* __restrict__ jobs, const in
     near_pair_moments(x, cl, jb.k, np, out + q * 13);
 }
 
+// E and H of one (point, RHS): partial sums over the ranges in order, the
+// near pairs in cell order, the multiplier and the incident field. Not
+// inlined, so the arithmetic is compiled once and the complex64 and
+// complex128 outputs round the very same FP64 values.
+__device__ __noinline__ void finalize_values(const JobDev& jb, int p, int s, long long q0, long long q1,
+                                             const int* __restrict__ pair_cell, const cplx* __restrict__ moments,
+                                             double cs, double sn, const double* kx0, cplx* E, cplx* H) {
+    const size_t P = jb.n_pts;
+    double v[12];
+    for (int q = 0; q < 12; q++) v[q] = 0.;
+    for (int r = 0; r < jb.ranges; r++) {
+        const double* src = jb.partial + (((size_t)r * jb.n_rhs + s) * 12) * P + p;
+        for (int q = 0; q < 12; q++) v[q] += src[(size_t)q * P];
+    }
+    for (int a = 0; a < 3; a++) {
+        E[a] = mk(v[2 * a], v[2 * a + 1]) * kInvFourPi;
+        H[a] = mk(v[6 + 2 * a], v[6 + 2 * a + 1]) * kInvFourPi;
+    }
+    for (long long q = q0; q < q1; q++) {
+        const int c = pair_cell[q];
+        const cplx* o = moments + q * 13;
+        const cplx* j = jb.J + ((size_t)s * jb.n_cells + c) * 3;
+        for (int a = 0; a < 3; a++)
+            E[a] += o[0] * j[a] + o[1 + 3 * a] * j[0] + o[2 + 3 * a] * j[1] + o[3 + 3 * a] * j[2];
+        cplx h[3];
+        ccross_cc(o + 10, j, h);
+        for (int a = 0; a < 3; a++) H[a] += h[a];
+    }
+    for (int a = 0; a < 3; a++) E[a] = E[a] * jb.mult;
+    if (jb.add_E)
+        for (int a = 0; a < 3; a++) E[a] += mk(jb.e0[a] * cs, jb.e0[a] * sn);
+    if (jb.add_H)
+        for (int a = 0; a < 3; a++) H[a] += mk(kx0[a] * cs * jb.h_scale, kx0[a] * sn * jb.h_scale);
+}
+
 __global__ void batch_finalize_kernel(const JobDev* __restrict__ jobs, const int* __restrict__ pt_job, int total,
                                       const long long* __restrict__ offs, const int* __restrict__ pair_cell,
                                       const cplx* __restrict__ moments, unsigned long long* nonfinite) {
@@ -353,36 +402,11 @@ __global__ void batch_finalize_kernel(const JobDev* __restrict__ jobs, const int
     if (jb.add_E || jb.add_H) sincos(jb.kvec[0] * x[0] + jb.kvec[1] * x[1] + jb.kvec[2] * x[2], &sn, &cs);
     double kx0[3];
     cross3(jb.kvec, jb.e0, kx0);
+    const long long q0 = offs ? offs[g] : 0, q1 = offs ? offs[g + 1] : 0;
     bool bad = false;
     for (int s = 0; s < jb.n_rhs; s++) {
-        double v[12];
-        for (int q = 0; q < 12; q++) v[q] = 0.;
-        for (int r = 0; r < jb.ranges; r++) {
-            const double* src = jb.partial + (((size_t)r * jb.n_rhs + s) * 12) * P + p;
-            for (int q = 0; q < 12; q++) v[q] += src[(size_t)q * P];
-        }
         cplx E[3], H[3];
-        for (int a = 0; a < 3; a++) {
-            E[a] = mk(v[2 * a], v[2 * a + 1]) * kInvFourPi;
-            H[a] = mk(v[6 + 2 * a], v[6 + 2 * a + 1]) * kInvFourPi;
-        }
-        if (offs) {
-            for (long long q = offs[g]; q < offs[g + 1]; q++) {
-                const int c = pair_cell[q];
-                const cplx* o = moments + q * 13;
-                const cplx* j = jb.J + ((size_t)s * jb.n_cells + c) * 3;
-                for (int a = 0; a < 3; a++)
-                    E[a] += o[0] * j[a] + o[1 + 3 * a] * j[0] + o[2 + 3 * a] * j[1] + o[3 + 3 * a] * j[2];
-                cplx h[3];
-                ccross_cc(o + 10, j, h);
-                for (int a = 0; a < 3; a++) H[a] += h[a];
-            }
-        }
-        for (int a = 0; a < 3; a++) E[a] = E[a] * jb.mult;
-        if (jb.add_E)
-            for (int a = 0; a < 3; a++) E[a] += mk(jb.e0[a] * cs, jb.e0[a] * sn);
-        if (jb.add_H)
-            for (int a = 0; a < 3; a++) H[a] += mk(kx0[a] * cs * jb.h_scale, kx0[a] * sn * jb.h_scale);
+        finalize_values(jb, p, s, q0, q1, pair_cell, moments, cs, sn, kx0, E, H);
         for (int a = 0; a < 3; a++) bad |= !isfinite(E[a].re) || !isfinite(E[a].im);
         if (jb.E32) {
             float2* eo = reinterpret_cast<float2*>(jb.E32) + ((size_t)s * P + p) * 3;

@@ -158,3 +158,33 @@ def test_server_budget_cancel_and_errors(gctx):
         assert sv.stats()["peak_bytes_reserved"] <= 4 << 20
     finally:
         sv.close()
+
+
+def test_server_outputs_equal_the_batched_call(gctx):
+    """Served complex64 results are the complex128 batched results rounded;
+    served complex128 results are the batched results bit for bit."""
+    torch = pytest.importorskip("torch")
+    specs = _specs(gctx, 6)
+    dev = torch.device("cuda:0")
+    keep, jspecs = [], []
+    for sp in specs:
+        Jd = torch.from_numpy(np.ascontiguousarray(sp["J"])).to(dev)
+        Pd = torch.from_numpy(np.ascontiguousarray(sp["pts"])).to(dev)
+        S, P = sp["J"].shape[0], len(sp["pts"])
+        Ed = torch.zeros((S, P, 3), dtype=torch.complex128, device=dev)
+        Hd = torch.zeros_like(Ed)
+        keep.append((Jd, Pd, Ed, Hd))
+        jspecs.append(dict(mesh=sp["mesh"], n_rhs=S, n_pts=P, J=Jd.data_ptr(), pts=Pd.data_ptr(), E=Ed.data_ptr(),
+                           H=Hd.data_ptr(), k=sp["k"], mult=sp["mult"]))
+    gctx.field_EH_batch(gctx.make_jobs(jspecs), precision="mixed", stream=torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    sv = gpu.Server(gctx, n_slots=2, precision="mixed")
+    try:
+        for sp, (_, _, Ed, Hd) in zip(specs, keep):
+            E, H = Ed.cpu().numpy(), Hd.cpu().numpy()
+            _, _, o64 = sv.wait(_submit(sv, sp, out_c64=False))
+            _, _, o32 = sv.wait(_submit(sv, sp, out_c64=True))
+            assert np.array_equal(o64["E"], E) and np.array_equal(o64["H"], H)
+            assert np.array_equal(o32["E"], E.astype(np.complex64)) and np.array_equal(o32["H"], H.astype(np.complex64))
+    finally:
+        sv.close()
