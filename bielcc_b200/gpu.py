@@ -104,6 +104,20 @@ def _c(a, dtype=np.float64):
 
 PREC = {"fp64": abi.PREC_FP64, "mixed": abi.PREC_MIXED}
 
+# cudaStreamLegacy: the legacy default stream as an explicit handle
+_CUDA_STREAM_LEGACY = 0x1
+
+
+def _stream_arg(stream):
+    """cudaStream_t argument of the C ABI. None selects the context's own
+    stream; a raw handle (e.g. torch.cuda.Stream.cuda_stream) is passed as is,
+    except 0 — torch's handle of the legacy default stream — which is passed as
+    cudaStreamLegacy, so the work is ordered with everything on that stream
+    instead of going to the context's (non-blocking) stream."""
+    if stream is None:
+        return None
+    return C.c_void_p(int(stream) if int(stream) != 0 else _CUDA_STREAM_LEGACY)
+
 
 class Mesh:
     def __init__(self, ctx, cells):
@@ -170,10 +184,11 @@ class Context:
     def mesh(self, cells):
         return Mesh(self, cells)
 
-    def measure_fma_peak(self, fp64=False):
-        """FP32 / FP64 CUDA-core FMA peak of this device in TFLOP/s."""
+    def measure_fma_peak(self, fp64=False, packed=False):
+        """CUDA-core FMA peak of this device in TFLOP/s: FP32, FP64, or packed
+        FP32 pairs (fma.rn.f32x2) with packed=True."""
         t = C.c_double(0)
-        _check(_lib.bielcc_measure_fma_peak(int(bool(fp64)), C.byref(t)))
+        _check(_lib.bielcc_measure_fma_peak(2 if packed else int(bool(fp64)), C.byref(t)))
         return t.value
 
     # ------------------------------------------------------------------ field
@@ -217,7 +232,7 @@ class Context:
                                            mult.imag, C.byref(inc) if inc is not None else None, C.byref(np_),
                                            n_pts, C.c_void_p(pts_dev), C.c_void_p(E_dev),
                                            C.c_void_p(H_dev) if H_dev else None, PREC[precision],
-                                           C.c_void_p(stream) if stream else None, C.byref(rep)))
+                                           _stream_arg(stream), C.byref(rep)))
         return rep
 
     # ------------------------------------------------------------------ batched field
@@ -248,14 +263,14 @@ class Context:
         rep = abi.Report()
         np_ = numparam if numparam is not None else abi.NumParam.default()
         _check(_lib.bielcc_field_EH_batch(self.h, len(jobs), jobs, C.byref(np_), PREC[precision],
-                                          C.c_void_p(stream) if stream else None, C.byref(rep)))
+                                          _stream_arg(stream), C.byref(rep)))
         return rep
 
     def batch_autotune(self, jobs, numparam=None, precision="mixed", stream=None):
         c = C.c_double(0)
         np_ = numparam if numparam is not None else abi.NumParam.default()
         _check(_lib.bielcc_batch_autotune(self.h, len(jobs), jobs, C.byref(np_), PREC[precision],
-                                          C.c_void_p(stream) if stream else None, C.byref(c)))
+                                          _stream_arg(stream), C.byref(c)))
         return c.value
 
     def batch_plan(self, jobs, numparam=None, precision="mixed", stream=None):
@@ -353,7 +368,7 @@ class Context:
         np_ = numparam if numparam is not None else abi.NumParam.default()
         k = complex(k)
         _check(_lib.bielcc_assemble_K_device(self.h, mesh.id, k.real, k.imag, C.byref(np_), layout, int(c64),
-                                             PREC[precision], C.c_void_p(A_dev), C.c_void_p(stream) if stream else None,
+                                             PREC[precision], C.c_void_p(A_dev), _stream_arg(stream),
                                              C.byref(rep)))
         return rep
 
@@ -367,12 +382,12 @@ class BatchPlan:
         h = C.c_void_p()
         self.report = abi.Report()
         _check(_lib.bielcc_batch_plan_create(ctx.h, len(jobs), jobs, C.byref(np_), PREC[precision],
-                                             C.c_void_p(stream) if stream else None, C.byref(h),
+                                             _stream_arg(stream), C.byref(h),
                                              C.byref(self.report)))
         self.h = h
 
     def launch(self, stream=None):
-        _check(_lib.bielcc_batch_plan_launch(self.h, C.c_void_p(stream) if stream else None))
+        _check(_lib.bielcc_batch_plan_launch(self.h, _stream_arg(stream)))
 
     def close(self):
         if self.h:

@@ -132,9 +132,10 @@ int bielcc_ctx_set_timing(bielcc_ctx ctx, int on);
 int bielcc_ctx_stats(bielcc_ctx ctx, bielcc_stats* out, int reset);
 
 /* Measured FMA throughput (TFLOP/s, 2 flops per FMA) of the current device's
- * FP32 (fp64 = 0) or FP64 (fp64 = 1) CUDA-core pipes: the roofline
- * denominator of the field kernels. No counterpart in the reference. */
-int bielcc_measure_fma_peak(int fp64, double* tflops);
+ * CUDA-core pipes: kind 0 = scalar FP32 FMA, 1 = FP64 FMA, 2 = packed FP32
+ * pairs (fma.rn.f32x2, 4 flops per instruction): the roofline denominators of
+ * the field kernels. No counterpart in the reference. */
+int bielcc_measure_fma_peak(int kind, double* tflops);
 
 /* ---- resident meshes -------------------------------------------------- */
 /* Uploads cells and precomputes per-cell geometry on the device: centre
@@ -172,7 +173,8 @@ int bielcc_field_EH(bielcc_ctx ctx, bielcc_mesh mesh, int n_rhs, const double* J
                     int precision, bielcc_report* report);
 
 /* Same computation on device buffers, enqueued on `stream` (a cudaStream_t,
- * NULL = the context's stream); returns once enqueued. The report's
+ * NULL = the context's own non-blocking stream; pass cudaStreamLegacy for the
+ * legacy default stream); returns once enqueued. The report's
  * n_nonfinite / est_rel_l2 are not filled (no host synchronisation). */
 int bielcc_field_EH_device(bielcc_ctx ctx, bielcc_mesh mesh, int n_rhs, const double* J_dev,
                            double k_re, double k_im, double mult_re, double mult_im,
