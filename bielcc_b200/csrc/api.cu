@@ -89,6 +89,7 @@ struct bielcc_ctx_s {
     std::map<int, MeshDev*> meshes;
     int next_mesh = 1;
     DevBuf ws, pair_ws, io, scratch_small;
+    DevBuf full;  // [j_E; j_M] and the 2S-RHS outputs of bielcc_field_EH_full
     long long* h_total = nullptr;  // pinned
     unsigned long long* h_nonfinite = nullptr;
     // counters / timing (bielcc_ctx_stats)
@@ -296,7 +297,9 @@ int bielcc_ctx_destroy(bielcc_ctx ctx) {
     ctx->pair_ws.release();
     ctx->io.release();
     ctx->scratch_small.release();
+    ctx->full.release();
     if (ctx->h_total) cudaFreeHost(ctx->h_total);
+    if (ctx->h_nonfinite) cudaFreeHost(ctx->h_nonfinite);
     if (ctx->ws_done) cudaEventDestroy(ctx->ws_done);
     if (ctx->far_begin) cudaEventDestroy(ctx->far_begin);
     if (ctx->far_end) cudaEventDestroy(ctx->far_end);
@@ -422,6 +425,122 @@ int bielcc_field_EH_device(bielcc_ctx ctx, bielcc_mesh mesh, int n_rhs, const do
     TRY(field_device(ctx, a, s, report, nullptr));
     TRY(ws_release(ctx, s));
     return BIELCC_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Full Stratton-Chu on device buffers (caller holds ctx->mu and the shared
+// workspaces): [j_E; j_M] into ctx->full, one field evaluation over 2S
+// right-hand sides (mult 1, no incident field), then the combination.
+int field_full_core(bielcc_ctx ctx, MeshDev* m, int S, const double* JE, const double* JM, cplx k, cplx multE,
+                    cplx multH, const bielcc_planewave* inc, const NumParamH& n, int P, const double* pts, double* E,
+                    double* H, int precision, cudaStream_t s, bielcc_report* rep, unsigned long long* d_nf) {
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t N = m->n_cells, bJ = (size_t)S * N * 48, bO = (size_t)S * P * 48;
+    TRY(ctx->full.ensure(al(2 * bJ) + 2 * al(2 * bO) + 256));
+    char* b = (char*)ctx->full.p;
+    double* J2 = (double*)b;
+    double* E2 = (double*)(b + al(2 * bJ));
+    double* H2 = (double*)(b + al(2 * bJ) + al(2 * bO));
+    TRY_CUDA(cudaMemcpyAsync(J2, JE, bJ, cudaMemcpyDeviceToDevice, s));
+    TRY_CUDA(cudaMemcpyAsync((char*)J2 + bJ, JM, bJ, cudaMemcpyDeviceToDevice, s));
+    if (P == 0) return BIELCC_OK;
+    FieldArgs a{m, 2 * S, J2, k, mk(1.0, 0.0), nullptr, n, P, pts, E2, H2, precision};
+    TRY(field_device(ctx, a, s, rep, nullptr));
+    FullInc fi;
+    memset(&fi, 0, sizeof(fi));
+    if (inc) {
+        for (int g = 0; g < 3; g++) {
+            fi.kvec[g] = inc->k_vec[g];
+            fi.e0[g] = inc->e0[g];
+        }
+        fi.h_scale = inc->h_scale;
+        fi.add_E = inc->add_E;
+        fi.add_H = inc->add_H;
+    }
+    TRY_CUDA(launch_combine_full(E2, H2, S, P, multE, multH, pts, fi, E, H, d_nf, s));
+    ctx->stats.kernel_launches += 1;
+    return BIELCC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bielcc_field_EH_full_device(bielcc_ctx ctx, bielcc_mesh mesh, int n_rhs, const double* JE_dev,
+                                const double* JM_dev, double k_re, double k_im, double multE_re, double multE_im,
+                                double multH_re, double multH_im, const bielcc_planewave* inc,
+                                const bielcc_numparam* np, int n_pts, const double* pts_dev, double* E_dev,
+                                double* H_dev, int precision, void* stream, bielcc_report* report) {
+    TRY(enter(ctx));
+    std::lock_guard<std::mutex> g(ctx->mu);
+    MeshDev* m;
+    TRY(get_mesh(ctx, mesh, &m));
+    NumParamH n = to_np(np);
+    TRY(check_np(n));
+    if (n_rhs < 1 || n_pts < 0 || !JE_dev || !JM_dev || (n_pts > 0 && (!pts_dev || !E_dev || !H_dev)))
+        return set_error(BIELCC_ERR_ARG, "bad full-field arguments (n_rhs %d, n_pts %d)", n_rhs, n_pts);
+    if (precision != BIELCC_PREC_FP64 && precision != BIELCC_PREC_MIXED)
+        return set_error(BIELCC_ERR_ARG, "unknown precision %d", precision);
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    if (report) memset(report, 0, sizeof(*report));
+    TRY(ws_acquire(ctx, s));
+    TRY(field_full_core(ctx, m, n_rhs, JE_dev, JM_dev, mk(k_re, k_im), mk(multE_re, multE_im),
+                        mk(multH_re, multH_im), inc, n, n_pts, pts_dev, E_dev, H_dev, precision, s, report, nullptr));
+    TRY(ws_release(ctx, s));
+    return BIELCC_OK;
+}
+
+int bielcc_field_EH_full(bielcc_ctx ctx, bielcc_mesh mesh, int n_rhs, const double* J_E, const double* J_M,
+                         double k_re, double k_im, double multE_re, double multE_im, double multH_re,
+                         double multH_im, const bielcc_planewave* inc, const bielcc_numparam* np, int n_pts,
+                         const double* pts, double* E, double* H, int precision, bielcc_report* report) {
+    TRY(enter(ctx));
+    std::lock_guard<std::mutex> g(ctx->mu);
+    MeshDev* m;
+    TRY(get_mesh(ctx, mesh, &m));
+    NumParamH n = to_np(np);
+    TRY(check_np(n));
+    if (n_rhs < 1 || n_pts < 0 || !J_E || !J_M || (n_pts > 0 && (!pts || !E || !H)))
+        return set_error(BIELCC_ERR_ARG, "bad full-field arguments (n_rhs %d, n_pts %d)", n_rhs, n_pts);
+    if (precision != BIELCC_PREC_FP64 && precision != BIELCC_PREC_MIXED)
+        return set_error(BIELCC_ERR_ARG, "unknown precision %d", precision);
+    if (report) memset(report, 0, sizeof(*report));
+    cudaStream_t s = ctx->stream;
+    const size_t P = n_pts, N = m->n_cells, S = n_rhs;
+    const size_t bJ = S * N * 48, bP = P * 24, bO = S * P * 48;
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    TRY(ctx->io.ensure(2 * al(bJ) + al(bP) + 2 * al(bO) + 256));
+    char* io = (char*)ctx->io.p;
+    double* dJE = (double*)io;
+    double* dJM = (double*)(io + al(bJ));
+    double* dP = (double*)(io + 2 * al(bJ));
+    double* dE = (double*)(io + 2 * al(bJ) + al(bP));
+    double* dH = (double*)(io + 2 * al(bJ) + al(bP) + al(bO));
+    unsigned long long* d_nf = (unsigned long long*)(io + 2 * al(bJ) + al(bP) + 2 * al(bO));
+    TRY(ws_acquire(ctx, s));
+    TRY_CUDA(cudaMemcpyAsync(dJE, J_E, bJ, cudaMemcpyHostToDevice, s));
+    TRY_CUDA(cudaMemcpyAsync(dJM, J_M, bJ, cudaMemcpyHostToDevice, s));
+    if (P) TRY_CUDA(cudaMemcpyAsync(dP, pts, bP, cudaMemcpyHostToDevice, s));
+    TRY_CUDA(cudaMemsetAsync(d_nf, 0, sizeof(unsigned long long), s));
+    TRY(field_full_core(ctx, m, n_rhs, dJE, dJM, mk(k_re, k_im), mk(multE_re, multE_im), mk(multH_re, multH_im),
+                        inc, n, n_pts, dP, dE, dH, precision, s, report, d_nf));
+    if (P) {
+        TRY_CUDA(cudaMemcpyAsync(E, dE, bO, cudaMemcpyDeviceToHost, s));
+        TRY_CUDA(cudaMemcpyAsync(H, dH, bO, cudaMemcpyDeviceToHost, s));
+    }
+    TRY_CUDA(cudaMemcpyAsync(ctx->h_nonfinite, d_nf, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    TRY_CUDA(cudaStreamSynchronize(s));
+    TRY(ws_release(ctx, s));
+    const unsigned long long nf = *ctx->h_nonfinite;
+    int rc = nf ? set_error(BIELCC_ERR_NAN, "%llu output points hold NaN/Inf", nf) : BIELCC_OK;
+    if (report) {
+        report->n_nonfinite = (int64_t)nf;
+        report->status = rc;
+    }
+    return rc;
 }
 
 int bielcc_field_EH(bielcc_ctx ctx, bielcc_mesh mesh, int n_rhs, const double* J, double k_re, double k_im,

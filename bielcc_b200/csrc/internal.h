@@ -71,6 +71,17 @@ cudaError_t field_stage1(const FieldLaunch& f, void* ws, int splits, long long* 
 cudaError_t field_stage2(const FieldLaunch& f, void* ws, int splits, long long n_near, void* pair_ws,
                          unsigned long long* d_nonfinite, cudaStream_t s, int* launches);
 
+// ---- full.cu: E = multE K[j_E] - R[j_M] + E_inc, H = multH K[j_M] + R[j_E] + H_inc
+// from a field evaluation over [j_E, j_M] (2S right-hand sides, mult 1, no
+// incident field): E2 / H2 are its [2S][P][3] complex outputs.
+struct FullInc {
+    double kvec[3], e0[3], h_scale;
+    int add_E, add_H;
+};
+cudaError_t launch_combine_full(const double* E2, const double* H2, int S, int P, cplx multE, cplx multH,
+                                const double* pts, const FullInc& inc, double* E, double* H,
+                                unsigned long long* nonfinite, cudaStream_t s);
+
 // ---- pairops.cu
 cudaError_t launch_pair_op(int op, int nv, int n, const double* cells, const double* x, const double* j, cplx k,
                            NumParamH np, double* res, cudaStream_t s);

@@ -56,6 +56,10 @@ def load(path=LIB_PATH):
                                  C.POINTER(abi.PlaneWave), C.POINTER(abi.NumParam), C.c_int, vp, vp, vp, C.c_int, vp,
                                  C.POINTER(abi.Report)])
     d("bielcc_integrand_info", [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)])
+    full_args = [vp, C.c_int32, C.c_int, vp, vp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                 C.c_double, C.POINTER(abi.PlaneWave), C.POINTER(abi.NumParam), C.c_int, vp, vp, vp, C.c_int]
+    d("bielcc_field_EH_full", full_args + [C.POINTER(abi.Report)])
+    d("bielcc_field_EH_full_device", full_args + [vp, C.POINTER(abi.Report)])
     d("bielcc_assemble_K", [vp, C.c_int32, C.c_double, C.c_double, C.POINTER(abi.NumParam), C.c_int, C.c_int, C.c_int,
                             vp, C.POINTER(abi.Report)])
     d("bielcc_assemble_K_device", [vp, C.c_int32, C.c_double, C.c_double, C.POINTER(abi.NumParam), C.c_int, C.c_int,
@@ -233,6 +237,42 @@ class Context:
                                            n_pts, C.c_void_p(pts_dev), C.c_void_p(E_dev),
                                            C.c_void_p(H_dev) if H_dev else None, PREC[precision],
                                            _stream_arg(stream), C.byref(rep)))
+        return rep
+
+    def field_EH_full(self, mesh, J_E, J_M, k, pts, multE=1.0, multH=1.0, inc=None, numparam=None,
+                      precision="fp64"):
+        """Full Stratton-Chu E, H [S][M][3] of electric and magnetic currents
+        (bielcc_field_EH_full) and the report."""
+        JE = _c(J_E, np.complex128)
+        JM = _c(J_M, np.complex128)
+        if JE.ndim == 2:
+            JE, JM = JE[None], JM[None]
+        if JE.shape != JM.shape or JE.shape[1] != mesh.n_cells:
+            raise ValueError("J_E and J_M must both be [S][n_cells][3]")
+        pts = _c(pts)
+        S, P = JE.shape[0], pts.shape[0]
+        E = np.zeros((S, P, 3), np.complex128)
+        H = np.zeros_like(E)
+        rep = abi.Report()
+        np_ = numparam if numparam is not None else abi.NumParam.default()
+        k, multE, multH = complex(k), complex(multE), complex(multH)
+        _check(_lib.bielcc_field_EH_full(self.h, mesh.id, S, JE.ctypes.data, JM.ctypes.data, k.real, k.imag,
+                                         multE.real, multE.imag, multH.real, multH.imag,
+                                         C.byref(inc) if inc is not None else None, C.byref(np_), P,
+                                         pts.ctypes.data, E.ctypes.data, H.ctypes.data, PREC[precision],
+                                         C.byref(rep)))
+        return E, H, rep
+
+    def field_EH_full_device(self, mesh, JE_dev, JM_dev, k, pts_dev, E_dev, H_dev, n_rhs, n_pts, multE=1.0,
+                             multH=1.0, inc=None, numparam=None, precision="mixed", stream=None):
+        rep = abi.Report()
+        np_ = numparam if numparam is not None else abi.NumParam.default()
+        k, multE, multH = complex(k), complex(multE), complex(multH)
+        _check(_lib.bielcc_field_EH_full_device(self.h, mesh.id, n_rhs, C.c_void_p(JE_dev), C.c_void_p(JM_dev),
+                                                k.real, k.imag, multE.real, multE.imag, multH.real, multH.imag,
+                                                C.byref(inc) if inc is not None else None, C.byref(np_), n_pts,
+                                                C.c_void_p(pts_dev), C.c_void_p(E_dev), C.c_void_p(H_dev),
+                                                PREC[precision], _stream_arg(stream), C.byref(rep)))
         return rep
 
     # ------------------------------------------------------------------ batched field

@@ -182,6 +182,33 @@ int bielcc_field_EH_device(bielcc_ctx ctx, bielcc_mesh mesh, int n_rhs, const do
                            int n_pts, const double* pts_dev, double* E_dev, double* H_dev,
                            int precision, void* stream, bielcc_report* report);
 
+/* The full Stratton-Chu field of electric and magnetic surface currents, as
+ * examples/field/main0_field_test.cpp:237-319 forms it (field_E_SCH,
+ * field_H_SCH), with get_field.h:58's per-cell near test:
+ *   E = multE * sum_j K[j_E](x) - sum_j R[j_M](x) + E_inc(x),
+ *   H = multH * sum_j K[j_M](x) + sum_j R[j_E](x) + H_inc(x),
+ * K far = K_RotRot_Far, near = K_RotRot_Near_Smooth; R far = R_Rot_Colloc,
+ * near = R_Rot_Smooth. J_E, J_M: [n_rhs][n_cells][3] complex; E, H (both
+ * required): [n_rhs][n_pts][3] complex. For a dielectric body, multE / multH
+ * carry the medium's constants (the example's multE, multH). The four sums come
+ * from one evaluation over 2 n_rhs right-hand sides (the moments are shared),
+ * so the cost is that of bielcc_field_EH with twice the RHS. The host form
+ * fills report->n_nonfinite but no est_rel_l2. No library counterpart in the
+ * reference (only the example's loop). */
+int bielcc_field_EH_full(bielcc_ctx ctx, bielcc_mesh mesh, int n_rhs, const double* J_E,
+                         const double* J_M, double k_re, double k_im, double multE_re,
+                         double multE_im, double multH_re, double multH_im,
+                         const bielcc_planewave* inc, const bielcc_numparam* np, int n_pts,
+                         const double* pts, double* E, double* H, int precision,
+                         bielcc_report* report);
+int bielcc_field_EH_full_device(bielcc_ctx ctx, bielcc_mesh mesh, int n_rhs,
+                                const double* J_E_dev, const double* J_M_dev, double k_re,
+                                double k_im, double multE_re, double multE_im, double multH_re,
+                                double multH_im, const bielcc_planewave* inc,
+                                const bielcc_numparam* np, int n_pts, const double* pts_dev,
+                                double* E_dev, double* H_dev, int precision, void* stream,
+                                bielcc_report* report);
+
 /* Field evaluation that allocates nothing. No counterpart in the reference.
  * For callers that must not call cudaMalloc while they run: applications that
  * reserve (nearly) all device memory in their own pool up front, where a
