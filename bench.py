@@ -70,37 +70,23 @@ def workload():
 
 
 def dist_init(args):
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if ws > 1:
-        import datetime
+    from bielcc_b200 import replicas
 
-        import torch
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+    ws, rank, local = replicas.env()
+    replicas.init(ws, local)  # NCCL when a GPU is visible, gloo otherwise (the CPU reference arm)
     return ws, rank, local
 
 
 def barrier(ws):
-    if ws > 1:
-        import torch.distributed as dist
+    from bielcc_b200 import replicas
 
-        dist.barrier()
+    replicas.barrier(ws)
 
 
 def max_over_ranks(ws, v, local):
-    if ws == 1:
-        return v
-    import torch
-    import torch.distributed as dist
+    from bielcc_b200 import replicas
 
-    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return replicas.max_over_ranks(ws, v, local)
 
 
 class Clocks:
@@ -512,10 +498,9 @@ def run_ours(args, ws, rank, local):
     cells, J, k = wl["cells"], wl["J"], wl["k"]
     pts = wl["pts"]
     if ws > 1 and rank > 0:  # each rank: its own far points, same distribution (weak scaling)
-        from bielcc_b200 import workloads as W
+        from bielcc_b200 import replicas
 
-        rng = np.random.default_rng(1000 + rank)
-        pts = np.concatenate([W.shell_points(18000, 2.0, 5.0, rng), W.near_points(cells, 2000, 0.02, 0.1, rng)])
+        pts = replicas.rank_points(cells, rank)
     kv, e0, hs = wl["inc"]
     inc = abi.PlaneWave.make(kv, e0, hs, True, True)
     S, N, P = J.shape[0], len(cells), len(pts)
