@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--no-batched", action="store_true", help="skip the 256-mesh batched leg")
     ap.add_argument("--batch-meshes", type=int, default=256)
     ap.add_argument("--no-assembly", action="store_true", help="skip the 20,480-triangle assembly leg")
+    ap.add_argument("--assembly-level", type=int, default=5, help="icosphere level of the assembly leg (5: 20,480)")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream leg")
     ap.add_argument("--serve-requests", type=int, default=600)
     ap.add_argument("--serve-load", type=float, default=0.9, help="arrival rate / offline capacity")
@@ -268,7 +269,7 @@ def run_assembly(args, ctx, torch, dev, stream, flush):
     same matrix, which is timed too."""
     from bielcc_b200 import workloads as W
 
-    wl = W.config3()
+    wl = W.config3(args.assembly_level)
     cells, k = wl["cells"], wl["k"]
     N = len(cells)
     mesh = ctx.mesh(cells)

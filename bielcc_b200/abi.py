@@ -17,6 +17,7 @@ ERR_UNSUPPORTED = -6
 ERR_NOT_FOUND = -7
 ERR_BUSY = -8
 ERR_CANCELLED = -9
+ERR_IO = -10
 
 PREC_FP64 = 0
 PREC_MIXED = 1

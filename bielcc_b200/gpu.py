@@ -56,6 +56,9 @@ def load(path=LIB_PATH):
                                  C.POINTER(abi.PlaneWave), C.POINTER(abi.NumParam), C.c_int, vp, vp, vp, C.c_int, vp,
                                  C.POINTER(abi.Report)])
     d("bielcc_integrand_info", [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)])
+    d("bielcc_read_mesh_dat", [C.c_char_p, C.c_int, C.POINTER(C.c_int), dp])
+    d("bielcc_read_mesh_vtk", [C.c_char_p, C.c_int, C.POINTER(C.c_int), dp, C.POINTER(C.c_int)])
+    d("bielcc_read_currents", [C.c_char_p, C.c_char_p, C.POINTER(C.c_int), dp])
     full_args = [vp, C.c_int32, C.c_int, vp, vp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
                  C.c_double, C.POINTER(abi.PlaneWave), C.POINTER(abi.NumParam), C.c_int, vp, vp, vp, C.c_int]
     d("bielcc_field_EH_full", full_args + [C.POINTER(abi.Report)])
@@ -121,6 +124,36 @@ def _stream_arg(stream):
     if stream is None:
         return None
     return C.c_void_p(int(stream) if int(stream) != 0 else _CUDA_STREAM_LEGACY)
+
+
+def read_mesh_dat(path, n_vert):
+    """Cells [N][n_vert][3] of a geodat .dat mesh file (host reader, no GPU)."""
+    load()
+    n = C.c_int(0)
+    _check(_lib.bielcc_read_mesh_dat(os.fsencode(path), n_vert, C.byref(n), None))
+    cells = np.zeros((n.value, n_vert, 3))
+    _check(_lib.bielcc_read_mesh_dat(os.fsencode(path), n_vert, C.byref(n), abi.dptr(cells)))
+    return cells
+
+
+def read_mesh_vtk(path, n_vert):
+    """(cells [N][n_vert][3], polygons skipped) of a legacy ASCII VTK file."""
+    load()
+    n, sk = C.c_int(0), C.c_int(0)
+    _check(_lib.bielcc_read_mesh_vtk(os.fsencode(path), n_vert, C.byref(n), None, C.byref(sk)))
+    cells = np.zeros((n.value, n_vert, 3))
+    _check(_lib.bielcc_read_mesh_vtk(os.fsencode(path), n_vert, C.byref(n), abi.dptr(cells), C.byref(sk)))
+    return cells, sk.value
+
+
+def read_currents(path_re, path_im):
+    """J [N][3] complex128 from the real / imaginary current files."""
+    load()
+    n = C.c_int(0)
+    _check(_lib.bielcc_read_currents(os.fsencode(path_re), os.fsencode(path_im), C.byref(n), None))
+    J = np.zeros((n.value, 3), np.complex128)
+    _check(_lib.bielcc_read_currents(os.fsencode(path_re), os.fsencode(path_im), C.byref(n), abi.dptr(J)))
+    return J
 
 
 class Mesh:

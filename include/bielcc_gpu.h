@@ -48,6 +48,7 @@ extern "C" {
 #define BIELCC_ERR_NOT_FOUND     -7  /* unknown mesh / request handle */
 #define BIELCC_ERR_BUSY          -8  /* admission refused (serving queue full) */
 #define BIELCC_ERR_CANCELLED     -9  /* serving request cancelled before it ran */
+#define BIELCC_ERR_IO           -10  /* a mesh / current file is missing or malformed */
 
 /* ---- numerical parameters -------------------------------------------- */
 /* Mirrors NumParam (electrodynamics/num_param.h:28-55); defaults are the
@@ -401,6 +402,25 @@ int bielcc_assemble_K_device(bielcc_ctx ctx, bielcc_mesh mesh, double k_re, doub
                              const bielcc_numparam* np, int layout, int out_c64,
                              int precision, void* A_dev, void* stream,
                              bielcc_report* report);
+
+/* ---- mesh and current files --------------------------------------------
+ * Host-side readers of the reference's files, so that meshes and currents go
+ * from disk into bielcc_mesh_create / the field calls without the reference's
+ * SurfMesh classes. No GPU work. Each reader counts when its output pointer is
+ * NULL (first call: size the buffer), and fills a buffer of the counted size
+ * otherwise (on input *n_cells / *n is the buffer's capacity). File errors
+ * return BIELCC_ERR_IO, where the reference throws std::runtime_error.
+ *   bielcc_read_mesh_dat: geodat .dat, SurfMesh::ReadFromDatFile
+ *     (mesh/surf_mesh.cpp:18-175); n_vert 3 (CellTriangle) or 4 (CellQuad).
+ *   bielcc_read_mesh_vtk: legacy ASCII VTK, SurfMesh::ReadFromVtkFile +
+ *     FillMeshFromVTK (mesh/surf_mesh.h:382-560, surf_mesh.cpp:195-290):
+ *     POLYGONS or CELLS with exactly n_vert vertices, others skipped.
+ *   bielcc_read_currents: SurfaceCurrentsC_fromFiles
+ *     (electrodynamics/currents.cpp:74-109): J as interleaved complex [n][3].
+ * cells: [n_cells][n_vert][3] doubles, the layout bielcc_mesh_create takes. */
+int bielcc_read_mesh_dat(const char* path, int n_vert, int* n_cells, double* cells);
+int bielcc_read_mesh_vtk(const char* path, int n_vert, int* n_cells, double* cells, int* n_skipped);
+int bielcc_read_currents(const char* path_re, const char* path_im, int* n, double* J);
 
 /* ---- serving: continuous batching ---------------------------------------
  * A server runs field and assembly requests submitted at any time, from any
