@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <type_traits>
 
+#include "farnode.cuh"
 #include "internal.h"
 #include "ops.cuh"
 #include "scan.cuh"
@@ -43,22 +44,27 @@ BIELCC_D bool asm_is_near(const double* x, const CellGeo& g, double analytic_cal
     return *d < __dmul_rn(analytic_calc, g.diam);
 }
 
-// Writes the m x m block of (row cell i, column cell j) from the 3x3 complex
-// operator matrix K (already / 4pi).
-BIELCC_D void write_block(const AsmArgs& a, int i, int j, const double (*Kr)[3], const double (*Ki)[3],
-                          const double* ti1, const double* ti2, const double* tj1, const double* tj2) {
-    const size_t dim = (size_t)a.m * a.n_cells;
-    const int m = a.m;
-    for (int aa = 0; aa < m; aa++) {
-        double rv[3][2];  // row vector: tau_a(i) or e_a
-        for (int b = 0; b < m; b++) {
+// Writes the M x M block of (row cell i, column cell j) from the 3x3 complex
+// operator matrix K (already / 4pi): M = 2 projects on tau1, tau2 of both
+// cells, M = 3 keeps the Cartesian block. M is a template argument so that the
+// block stays in registers.
+template <int M>
+BIELCC_D void write_block_m(const AsmArgs& a, int i, int j, const double (&Kr)[3][3], const double (&Ki)[3][3],
+                            const double* ti1, const double* ti2, const double* tj1, const double* tj2) {
+    const size_t dim = (size_t)M * a.n_cells;
+#pragma unroll
+    for (int aa = 0; aa < M; aa++) {
+        double rv[M][2];
+#pragma unroll
+        for (int b = 0; b < M; b++) {
             double vr = 0., vi = 0.;
-            if (m == 3) {
+            if constexpr (M == 3) {
                 vr = Kr[aa][b];
                 vi = Ki[aa][b];
             } else {
                 const double* ta = aa == 0 ? ti1 : ti2;
                 const double* tb = b == 0 ? tj1 : tj2;
+#pragma unroll
                 for (int p = 0; p < 3; p++) {
                     double kr = Kr[p][0] * tb[0] + Kr[p][1] * tb[1] + Kr[p][2] * tb[2];
                     double ki = Ki[p][0] * tb[0] + Ki[p][1] * tb[1] + Ki[p][2] * tb[2];
@@ -69,15 +75,23 @@ BIELCC_D void write_block(const AsmArgs& a, int i, int j, const double (*Kr)[3],
             rv[b][0] = vr;
             rv[b][1] = vi;
         }
-        size_t off = ((size_t)i * m + aa) * dim + (size_t)j * m;
+        const size_t off = ((size_t)i * M + aa) * dim + (size_t)j * M;
         if (a.c64) {
             float2* dst = reinterpret_cast<float2*>(a.A) + off;
-            for (int b = 0; b < m; b++) dst[b] = make_float2((float)rv[b][0], (float)rv[b][1]);
+#pragma unroll
+            for (int b = 0; b < M; b++) dst[b] = make_float2((float)rv[b][0], (float)rv[b][1]);
         } else {
             double2* dst = reinterpret_cast<double2*>(a.A) + off;
-            for (int b = 0; b < m; b++) dst[b] = make_double2(rv[b][0], rv[b][1]);
+#pragma unroll
+            for (int b = 0; b < M; b++) dst[b] = make_double2(rv[b][0], rv[b][1]);
         }
     }
+}
+
+BIELCC_D void write_block(const AsmArgs& a, int i, int j, const double (&Kr)[3][3], const double (&Ki)[3][3],
+                          const double* ti1, const double* ti2, const double* tj1, const double* tj2) {
+    if (a.m == 2) write_block_m<2>(a, i, j, Kr, Ki, ti1, ti2, tj1, tj2);
+    else write_block_m<3>(a, i, j, Kr, Ki, ti1, ti2, tj1, tj2);
 }
 
 template <bool CK, bool MIXED>
@@ -105,7 +119,7 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_far_kernel(AsmArgs a) {
     bool far = false;
     float Xf[3] = {0.f, 0.f, 0.f}, r0f = 0.f, r0sq = 0.f;
     double P0r = 1., P0i = 0.;
-    int halvings = 0;
+    int mode = 0;  // phase polynomial of the current cell (farnode.cuh phase_mode)
 
     for (int c0 = cb; c0 < ce; c0 += cps) {
         const int nc = min(cps, ce - c0);
@@ -155,54 +169,29 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_far_kernel(AsmArgs a) {
                         }
                         P0r = cs;
                         P0i = sn;
-                        float th = (float)fabs(a.k.re) * s_rho[cc];
-                        halvings = th <= 1.f ? 0 : (th <= 2.f ? 1 : (th <= 4.f ? 2 : 3));
+                        mode = phase_mode((float)fabs(a.k.re) * s_rho[cc]);
                     }
                 }
                 if (far) {
                     const NodeT* nd = s_nodes + cc * kc;
+                    if constexpr (MIXED) {
+                        const float kr_ = (float)a.k.re, ki_ = (float)a.k.im;
+                        const float k2rf = (float)k2r, k2if = (float)k2i;
+#define BIELCC_ASM_LOOP(MODE_)                                                                         \
+    _Pragma("unroll 4") for (int q = 0; q < kc; q++)                                                    \
+        far_node_f32_K<CK, MODE_>(a1r, a1i, t, Xf[0], Xf[1], Xf[2], r0f, r0sq, nd[q], kr_, ki_, k2rf, k2if);
+                        switch (mode) {
+                            case 0: BIELCC_ASM_LOOP(0) break;
+                            case 1: BIELCC_ASM_LOOP(1) break;
+                            case 2: BIELCC_ASM_LOOP(2) break;
+                            case 3: BIELCC_ASM_LOOP(3) break;
+                            default: BIELCC_ASM_LOOP(4) break;
+                        }
+#undef BIELCC_ASM_LOOP
+                    } else {
                     for (int q = 0; q < kc; q++) {
-                        F dx, dy, dz, w, ir, ir2, ir3, er, ei;
-                        if constexpr (MIXED) {
-                            float4 v = nd[q];
-                            float tx = fmaf(-2.f, Xf[0], v.x), ty = fmaf(-2.f, Xf[1], v.y), tz = fmaf(-2.f, Xf[2], v.z);
-                            float qq = fmaf(v.x, tx, fmaf(v.y, ty, v.z * tz));
-                            float r2 = r0sq + qq;
-                            ir = rsqrtf(r2);
-                            float r = r2 * ir;
-                            float dr = __fdividef(qq, r + r0f);
-                            float sn, cs;
-                            // e^{ik (r - r0)}; phase_f32 lives in field.cu: same polynomial inline here
-                            float th = (float)a.k.re * dr;
-                            if (halvings > 2) {
-                                sincosf(th, &sn, &cs);
-                            } else {
-                                float tt = th * (halvings == 0 ? 1.f : (halvings == 1 ? 0.5f : 0.25f));
-                                float t2 = tt * tt;
-                                float ps = fmaf(t2, 2.7557319e-6f, -1.9841270e-4f);
-                                ps = fmaf(t2, ps, 8.3333333e-3f);
-                                ps = fmaf(t2, ps, -1.6666667e-1f);
-                                ps = fmaf(t2, ps, 1.0f);
-                                sn = tt * ps;
-                                float pc = fmaf(t2, -2.7557319e-7f, 2.4801587e-5f);
-                                pc = fmaf(t2, pc, -1.3888889e-3f);
-                                pc = fmaf(t2, pc, 4.1666667e-2f);
-                                pc = fmaf(t2, pc, -0.5f);
-                                cs = fmaf(t2, pc, 1.0f);
-                                for (int h = 0; h < halvings; h++) {
-                                    float ns = 2.f * sn * cs;
-                                    cs = fmaf(cs, cs, -sn * sn);
-                                    sn = ns;
-                                }
-                            }
-                            w = v.w;
-                            if (CK) w *= __expf(-(float)a.k.im * dr);
-                            dx = Xf[0] - v.x;
-                            dy = Xf[1] - v.y;
-                            dz = Xf[2] - v.z;
-                            er = w * cs;
-                            ei = w * sn;
-                        } else {
+                        double dx, dy, dz, w, ir, ir2, ir3, er, ei;
+                        {
                             double4 v = nd[q];
                             dx = x[0] - v.x;
                             dy = x[1] - v.y;
@@ -223,27 +212,28 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_far_kernel(AsmArgs a) {
                         }
                         ir2 = ir * ir;
                         ir3 = ir2 * ir;
-                        F f1r, f1i, f2r, f2i;
+                        double f1r, f1i, f2r, f2i;
                         if (CK) {
-                            f1r = (F)k2r * ir - ir3 - (F)a.k.im * ir2;
-                            f1i = (F)a.k.re * ir2 + (F)k2i * ir;
-                            f2r = (F)3 * ir3 + (F)3 * (F)a.k.im * ir2 - (F)k2r * ir;
-                            f2i = -(F)3 * (F)a.k.re * ir2 - (F)k2i * ir;
+                            f1r = k2r * ir - ir3 - a.k.im * ir2;
+                            f1i = a.k.re * ir2 + k2i * ir;
+                            f2r = 3.0 * ir3 + 3.0 * a.k.im * ir2 - k2r * ir;
+                            f2i = -3.0 * a.k.re * ir2 - k2i * ir;
                         } else {
-                            f1r = (F)k2r * ir - ir3;
-                            f1i = (F)a.k.re * ir2;
-                            f2r = (F)3 * ir3 - (F)k2r * ir;
-                            f2i = -(F)3 * (F)a.k.re * ir2;
+                            f1r = k2r * ir - ir3;
+                            f1i = a.k.re * ir2;
+                            f2r = 3.0 * ir3 - k2r * ir;
+                            f2i = -3.0 * a.k.re * ir2;
                         }
                         a1r += er * f1r - ei * f1i;
                         a1i += er * f1i + ei * f1r;
-                        F a2r = (er * f2r - ei * f2i) * ir2, a2i = (er * f2i + ei * f2r) * ir2;
-                        F dd[6] = {dx * dx, dx * dy, dx * dz, dy * dy, dy * dz, dz * dz};
+                        double a2r = (er * f2r - ei * f2i) * ir2, a2i = (er * f2i + ei * f2r) * ir2;
+                        double dd[6] = {dx * dx, dx * dy, dx * dz, dy * dy, dy * dz, dz * dz};
 #pragma unroll
                         for (int p = 0; p < 6; p++) {
                             t[p][0] += a2r * dd[p];
                             t[p][1] += a2i * dd[p];
                         }
+                    }
                     }
                 }
                 if (k0 + kc == nn && far) {

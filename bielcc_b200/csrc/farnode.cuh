@@ -218,4 +218,53 @@ BIELCC_D void far_node_f32(Moments<float>& m, float Xx, float Xy, float Xz, floa
     m.g[2][1] = fmaf(gi, dz, m.g[2][1]);
 }
 
+// The K moments only (A1, T; no grad F) of one far node, FP32: the node
+// arithmetic of far_node_f32 for the collocation matrix, whose entries need
+// K_RotRot_Far alone.
+template <bool CK, int MODE>
+BIELCC_D void far_node_f32_K(float& a1r, float& a1i, float (&t)[6][2], float Xx, float Xy, float Xz, float r0,
+                             float r0sq, float4 nd, float kr_, float ki_, float k2r, float k2i) {
+    float tx = fmaf(-2.f, Xx, nd.x), ty = fmaf(-2.f, Xy, nd.y), tz = fmaf(-2.f, Xz, nd.z);
+    float q = fmaf(nd.x, tx, fmaf(nd.y, ty, nd.z * tz));  // |x-y|^2 - r0^2
+    float r2 = r0sq + q;
+    float ir = rsqrtf(r2);
+    float r = r2 * ir;
+    float dr = __fdividef(q, r + r0);
+    float s, c;
+    phase_f32<MODE>(kr_ * dr, &s, &c);
+    float w = nd.w;
+    if (CK) w *= __expf(-ki_ * dr);
+    float dx = Xx - nd.x, dy = Xy - nd.y, dz = Xz - nd.z;
+    float ir2 = ir * ir, ir3 = ir2 * ir;
+    float er = w * c, ei = w * s;
+    float f1r, f1i, f2r, f2i;
+    if (CK) {
+        f1r = k2r * ir - ir3 - ki_ * ir2;
+        f1i = kr_ * ir2 + k2i * ir;
+        f2r = 3.f * ir3 + 3.f * ki_ * ir2 - k2r * ir;
+        f2i = -3.f * kr_ * ir2 - k2i * ir;
+    } else {
+        f1r = k2r * ir - ir3;
+        f1i = kr_ * ir2;
+        f2r = 3.f * ir3 - k2r * ir;
+        f2i = -3.f * kr_ * ir2;
+    }
+    a1r = fmaf(er, f1r, fmaf(-ei, f1i, a1r));
+    a1i = fmaf(er, f1i, fmaf(ei, f1r, a1i));
+    float a2r = (er * f2r - ei * f2i) * ir2, a2i = (er * f2i + ei * f2r) * ir2;
+    float bx_r = a2r * dx, bx_i = a2i * dx, by_r = a2r * dy, by_i = a2i * dy, bz_r = a2r * dz, bz_i = a2i * dz;
+    t[0][0] = fmaf(bx_r, dx, t[0][0]);
+    t[0][1] = fmaf(bx_i, dx, t[0][1]);
+    t[1][0] = fmaf(bx_r, dy, t[1][0]);
+    t[1][1] = fmaf(bx_i, dy, t[1][1]);
+    t[2][0] = fmaf(bx_r, dz, t[2][0]);
+    t[2][1] = fmaf(bx_i, dz, t[2][1]);
+    t[3][0] = fmaf(by_r, dy, t[3][0]);
+    t[3][1] = fmaf(by_i, dy, t[3][1]);
+    t[4][0] = fmaf(by_r, dz, t[4][0]);
+    t[4][1] = fmaf(by_i, dz, t[4][1]);
+    t[5][0] = fmaf(bz_r, dz, t[5][0]);
+    t[5][1] = fmaf(bz_i, dz, t[5][1]);
+}
+
 }  // namespace bielcc_gpu
