@@ -120,6 +120,8 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_far_kernel(AsmArgs a) {
     float Xf[3] = {0.f, 0.f, 0.f}, r0f = 0.f, r0sq = 0.f;
     double P0r = 1., P0i = 0.;
     int mode = 0;  // phase polynomial of the current cell (farnode.cuh phase_mode)
+    bool split64 = false;
+    double r0d = 0.;
 
     for (int c0 = cb; c0 < ce; c0 += cps) {
         const int nc = min(cps, ce - c0);
@@ -144,7 +146,7 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_far_kernel(AsmArgs a) {
             if (k0 == 0)
                 for (int q = threadIdx.x; q < nc; q += kAsmThreads) {
                     s_geo[q] = a.geo[c0 + q];
-                    if (MIXED) s_rho[q] = a.rho32[c0 + q];
+                    s_rho[q] = a.rho32[c0 + q];
                 }
             __syncthreads();
             for (int cc = 0; cc < nc; cc++) {
@@ -154,6 +156,19 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_far_kernel(AsmArgs a) {
                     far = live && !asm_is_near(x, gj, a.analytic_calc, &d);
                     a1r = a1i = 0;
                     for (int q = 0; q < 6; q++) t[q][0] = t[q][1] = 0;
+                    if (!MIXED && far) {  // FP64 phase split when the cell's phase range is small
+                        split64 = !CK && fabs(a.k.re) * (double)s_rho[cc] * (1.0 + 1e-6) <= 0.5;
+                        r0d = d;
+                        if (split64) {
+                            double sn, cs;
+                            sincos(a.k.re * d, &sn, &cs);
+                            P0r = cs;
+                            P0i = sn;
+                        } else {
+                            P0r = 1.0;
+                            P0i = 0.0;
+                        }
+                    }
                     if (MIXED && far) {
                         Xf[0] = (float)(x[0] - gj.c[0]);
                         Xf[1] = (float)(x[1] - gj.c[1]);
@@ -189,51 +204,32 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_far_kernel(AsmArgs a) {
                         }
 #undef BIELCC_ASM_LOOP
                     } else {
-                    for (int q = 0; q < kc; q++) {
-                        double dx, dy, dz, w, ir, ir2, ir3, er, ei;
-                        {
-                            double4 v = nd[q];
-                            dx = x[0] - v.x;
-                            dy = x[1] - v.y;
-                            dz = x[2] - v.z;
-                            double r = sqrt(dx * dx + dy * dy + dz * dz);
-                            ir = 1.0 / r;
-                            double sn, cs;
-                            sincos(a.k.re * r, &sn, &cs);
-                            if (CK) {
-                                double am = exp(-a.k.im * r);
-                                sn *= am;
-                                cs *= am;
+                        // FP64: the field kernel's node (phase relative to r0 with the Taylor
+                        // series when |k| rho <= 0.5); its grad-F moments are unused here
+                        Moments<double> mm;
+                        mm.zero();
+                        if (split64) {
+#pragma unroll 2
+                            for (int q = 0; q < kc; q++) {
+                                const double4 v = nd[q];
+                                far_node_f64<CK, true>(mm, x[0] - v.x, x[1] - v.y, x[2] - v.z, v.w, a.k, k2r, k2i,
+                                                       r0d);
                             }
-                            w = v.w;
-                            er = w * cs;
-                            ei = w * sn;
-                            if (!(r >= kMachineZero)) er = ei = 0.;  // F_RotRotSimplePot_H: 0 below MACHINE_ZERO
-                        }
-                        ir2 = ir * ir;
-                        ir3 = ir2 * ir;
-                        double f1r, f1i, f2r, f2i;
-                        if (CK) {
-                            f1r = k2r * ir - ir3 - a.k.im * ir2;
-                            f1i = a.k.re * ir2 + k2i * ir;
-                            f2r = 3.0 * ir3 + 3.0 * a.k.im * ir2 - k2r * ir;
-                            f2i = -3.0 * a.k.re * ir2 - k2i * ir;
                         } else {
-                            f1r = k2r * ir - ir3;
-                            f1i = a.k.re * ir2;
-                            f2r = 3.0 * ir3 - k2r * ir;
-                            f2i = -3.0 * a.k.re * ir2;
+#pragma unroll 2
+                            for (int q = 0; q < kc; q++) {
+                                const double4 v = nd[q];
+                                far_node_f64<CK, false>(mm, x[0] - v.x, x[1] - v.y, x[2] - v.z, v.w, a.k, k2r, k2i,
+                                                        r0d);
+                            }
                         }
-                        a1r += er * f1r - ei * f1i;
-                        a1i += er * f1i + ei * f1r;
-                        double a2r = (er * f2r - ei * f2i) * ir2, a2i = (er * f2i + ei * f2r) * ir2;
-                        double dd[6] = {dx * dx, dx * dy, dx * dz, dy * dy, dy * dz, dz * dz};
+                        a1r += mm.a1r;
+                        a1i += mm.a1i;
 #pragma unroll
                         for (int p = 0; p < 6; p++) {
-                            t[p][0] += a2r * dd[p];
-                            t[p][1] += a2i * dd[p];
+                            t[p][0] += mm.t[p][0];
+                            t[p][1] += mm.t[p][1];
                         }
-                    }
                     }
                 }
                 if (k0 + kc == nn && far) {
