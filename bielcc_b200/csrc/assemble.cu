@@ -37,6 +37,7 @@ struct AsmArgs {
     int m;  // 2 (tau) or 3 (full)
     int c64;
     void* A;
+    unsigned* mask;  // [ceil(N/32)][N] near bits of (row i, column word) written by the far kernel, or null
 };
 
 BIELCC_D bool asm_is_near(const double* x, const CellGeo& g, double analytic_calc, double* d) {
@@ -122,6 +123,7 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_far_kernel(AsmArgs a) {
     int mode = 0;  // phase polynomial of the current cell (farnode.cuh phase_mode)
     bool split64 = false;
     double r0d = 0.;
+    unsigned nbits = 0;  // near bits of the current 32-column word
 
     for (int c0 = cb; c0 < ce; c0 += cps) {
         const int nc = min(cps, ce - c0);
@@ -153,7 +155,16 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_far_kernel(AsmArgs a) {
                 const CellGeo& gj = s_geo[cc];
                 if (k0 == 0) {
                     double d;
-                    far = live && !asm_is_near(x, gj, a.analytic_calc, &d);
+                    const bool nr = asm_is_near(x, gj, a.analytic_calc, &d);
+                    far = live && !nr;
+                    if (a.mask) {
+                        const int c = c0 + cc;
+                        nbits |= (nr ? 1u : 0u) << (c & 31);
+                        if ((c & 31) == 31 || c == ce - 1) {
+                            if (live) a.mask[(size_t)(c >> 5) * a.n_cells + i] = nbits;
+                            nbits = 0;
+                        }
+                    }
                     a1r = a1i = 0;
                     for (int q = 0; q < 6; q++) t[q][0] = t[q][1] = 0;
                     if (!MIXED && far) {  // FP64 phase split when the cell's phase range is small
@@ -323,6 +334,36 @@ __global__ void asm_near_fill_kernel(const CellGeo* __restrict__ geo, int n_cell
     }
 }
 
+// Near pairs from the far kernel's bit mask (row i, word w: the near test of
+// get_field.h:58 for columns 32w..32w+31, evaluated there with the same
+// non-contracted FP64 arithmetic): counts per row, then the (row, column)
+// pairs in ascending column order.
+__global__ void asm_mask_count_kernel(const unsigned* __restrict__ mask, int n_words, int n_cells,
+                                      long long* __restrict__ counts) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_cells) return;
+    long long n = 0;
+    for (int w = 0; w < n_words; w++) n += __popc(mask[(size_t)w * n_cells + i]);
+    counts[i] = n;
+}
+
+__global__ void asm_mask_fill_kernel(const unsigned* __restrict__ mask, int n_words, int n_cells,
+                                     const long long* __restrict__ offs, int* __restrict__ pr, int* __restrict__ pc) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_cells) return;
+    long long o = offs[i];
+    for (int w = 0; w < n_words; w++) {
+        unsigned b = mask[(size_t)w * n_cells + i];
+        while (b) {
+            const int bit = __ffs(b) - 1;
+            b &= b - 1;
+            pr[o] = i;
+            pc[o] = w * 32 + bit;
+            o++;
+        }
+    }
+}
+
 // Near entries: K_RotRot_HS_Colloc as a 3x3 operator, FP64.
 __global__ void asm_near_kernel(AsmArgs a, const double* __restrict__ verts, int nv, const int* __restrict__ pr,
                                 const int* __restrict__ pc, long long n_pairs, DNP np) {
@@ -359,8 +400,12 @@ static size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 size_t assemble_ws_base_bytes(const AssembleLaunch& a) {
     size_t N = a.mesh->n_cells;
-    return 2 * al256((N + 1) * sizeof(long long)) + 256;
+    return 2 * al256((N + 1) * sizeof(long long)) + al256((N + 31) / 32 * N * sizeof(unsigned)) + 256;
 }
+
+// The far kernel writes the near mask (and count / fill read it) unless the
+// adaptive far kernel runs, which tests pairs on its own.
+static bool uses_mask(const AssembleLaunch& a) { return a.np.p_max <= 1; }
 
 static AsmArgs make_args(const AssembleLaunch& a) {
     const MeshDev& m = *a.mesh;
@@ -376,6 +421,7 @@ static AsmArgs make_args(const AssembleLaunch& a) {
     g.m = a.layout == 1 ? 3 : 2;
     g.c64 = a.out_c64;
     g.A = a.A;
+    g.mask = nullptr;
     return g;
 }
 
@@ -384,13 +430,18 @@ cudaError_t assemble_stage1(const AssembleLaunch& a, void* ws, long long* d_tota
     const int N = m.n_cells;
     long long* counts = (long long*)ws;
     long long* offs = (long long*)((char*)ws + al256((size_t)(N + 1) * sizeof(long long)));
+    unsigned* mask = (unsigned*)((char*)offs + al256((size_t)(N + 1) * sizeof(long long)));
+    const int n_words = (N + 31) / 32;
     AsmArgs g = make_args(a);
+    g.mask = uses_mask(a) ? mask : nullptr;
     int tiles = (N + kAsmThreads - 1) / kAsmThreads;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     int splits = std::max(1, std::min((8 * sms + tiles - 1) / tiles, std::max(1, N / 16)));
-    g.cols_per_split = (N + splits - 1) / splits;
+    // column splits in whole 32-column words, so every mask word has one writer
+    g.cols_per_split = ((N + splits - 1) / splits + 31) / 32 * 32;
+    splits = (N + g.cols_per_split - 1) / g.cols_per_split;
     bool ck = a.k.im != 0.;
     dim3 grid(tiles, splits);
     if (a.np.p_max > 1) {
@@ -404,7 +455,8 @@ cudaError_t assemble_stage1(const AssembleLaunch& a, void* ws, long long* d_tota
         if (ck) assemble_far_kernel<true, false><<<grid, kAsmThreads, 0, s>>>(g);
         else assemble_far_kernel<false, false><<<grid, kAsmThreads, 0, s>>>(g);
     }
-    asm_near_count_kernel<<<tiles, kAsmThreads, 0, s>>>(m.geo, N, a.np.analytic_calc, counts);
+    if (g.mask) asm_mask_count_kernel<<<tiles, kAsmThreads, 0, s>>>(mask, n_words, N, counts);
+    else asm_near_count_kernel<<<tiles, kAsmThreads, 0, s>>>(m.geo, N, a.np.analytic_calc, counts);
     scan_kernel<<<1, 1024, 0, s>>>(counts, N, offs, d_total);
     return cudaGetLastError();
 }
@@ -414,10 +466,14 @@ cudaError_t assemble_stage2(const AssembleLaunch& a, void* ws, long long n_near,
     const MeshDev& m = *a.mesh;
     const int N = m.n_cells;
     long long* offs = (long long*)((char*)ws + al256((size_t)(N + 1) * sizeof(long long)));
+    const unsigned* mask = (const unsigned*)((char*)offs + al256((size_t)(N + 1) * sizeof(long long)));
     int* pr = (int*)pair_ws;
     int* pc = pr + n_near;
     int tiles = (N + kAsmThreads - 1) / kAsmThreads;
-    asm_near_fill_kernel<<<tiles, kAsmThreads, 0, s>>>(m.geo, N, a.np.analytic_calc, offs, pr, pc);
+    if (uses_mask(a))
+        asm_mask_fill_kernel<<<tiles, kAsmThreads, 0, s>>>(mask, (N + 31) / 32, N, offs, pr, pc);
+    else
+        asm_near_fill_kernel<<<tiles, kAsmThreads, 0, s>>>(m.geo, N, a.np.analytic_calc, offs, pr, pc);
     AsmArgs g = make_args(a);
     DNP np{a.np.eps, a.np.rs, a.np.rs_seg, a.np.analytic_calc, a.np.n_start, a.np.n_start_seg, a.np.p_max,
            a.np.p_max_seg};

@@ -254,7 +254,7 @@ int64_t field_bytes(const Req& r, int n_start, double item_cost) {
 int64_t assemble_bytes(const Req& r) {
     const int64_t N = r.mesh->n_cells, m = r.a.layout == BIELCC_LAYOUT_FULL3 ? 3 : 2;
     const int64_t mat = r.a.A_dev ? 0 : al(m * N * m * N * (r.a.out_c64 ? 8 : 16));
-    return mat + 2 * al((N + 1) * 8) + 256 + r.near_est;
+    return mat + 2 * al((N + 1) * 8) + al((N + 31) / 32 * N * 4) + 256 + r.near_est;
 }
 
 // Marks a slot's requests done with `code` (caller holds the lock).
