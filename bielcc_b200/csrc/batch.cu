@@ -60,14 +60,15 @@ struct BatchCfg {
 };
 
 // acc[12] += contraction of one cell's moments m[20] (a1r, a1i, t[6][2], g[3][2])
-// with the current J = (jr, ji): E = A1 J + T J, H = G x J.
+// with the current J = (jr, ji): E = (A1 I + T) J, H = G x J. The caller has
+// folded A1 into T's diagonal (m[2..3], m[8..9], m[12..13]) once per cell, so
+// E is one complex 3x3 matrix-vector product per right-hand side.
 template <typename F>
 BIELCC_D void contract12(const F* m, const F* jr, const F* ji, F* acc) {
-    const F a1r = m[0], a1i = m[1];
     const int ti[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-        F er = a1r * jr[a] - a1i * ji[a], ei = a1r * ji[a] + a1i * jr[a];
+        F er = 0, ei = 0;
 #pragma unroll
         for (int b = 0; b < 3; b++) {
             const F tr = m[2 + 2 * ti[a][b]], tim = m[3 + 2 * ti[a][b]];
@@ -270,6 +271,13 @@ __global__ void __launch_bounds__(kBT, MIXED ? BIELCC_BATCH_MINB : 2) batch_far_
                         F m[20];
 #pragma unroll
                         for (int q = 0; q < 20; q++) m[q] = s_mom[(cc * 20 + q) * kBP + lane];
+                        // A1 I + T: A1 onto the diagonal t_xx, t_yy, t_zz
+                        m[2] += m[0];
+                        m[3] += m[1];
+                        m[8] += m[0];
+                        m[9] += m[1];
+                        m[12] += m[0];
+                        m[13] += m[1];
 #pragma unroll
                         for (int j = 0; j < C::R; j++) {
                             const int sl = sb + warp + kBW * j;
