@@ -75,3 +75,33 @@ def test_full_field_reduces_to_field_EH_and_device_form(gctx):
                               stream=torch.cuda.current_stream().cuda_stream)
     torch.cuda.synchronize()
     assert np.array_equal(tE.cpu().numpy(), Eh) and np.array_equal(tH.cpu().numpy(), Hh)
+
+
+def test_extinction_theorem_sphere(gctx):
+    """The known answer of examples/field/main0_field_test.cpp (its header,
+    steps 1-4): with j_E = -n x H_inc and j_M = n x E_inc on a closed surface,
+    the Stratton-Chu field is E_inc inside the body and zero outside. Units
+    with eps = mu = 1, omega = k (H_inc = k_hat x E_inc), so multE = multH =
+    i / k. Piecewise-constant currents on 8192 quads: a few per cent of
+    discretisation error."""
+    cells = W.uv_sphere(64, 128)
+    k = 2 * np.pi
+    kv, e0, hs = W.planewave(k)
+    c, n = W.centres(cells), W.normals(cells)
+    ph = np.exp(1j * (c @ kv))[:, None]
+    Einc = e0[None, :] * ph
+    Hinc = hs * np.cross(kv, e0)[None, :] * ph
+    JE = -np.cross(n, Hinc)[None]
+    JM = np.cross(n, Einc)[None]
+    rng = np.random.default_rng(3)
+    inside = W.shell_points(200, 0.0, 0.5, rng)
+    outside = W.shell_points(200, 2.0, 3.0, rng)
+    m = gctx.mesh(cells)
+    mult = 1j / k
+    Ei, Hi, _ = gctx.field_EH_full(m, JE, JM, k, inside, multE=mult, multH=mult, precision="mixed")
+    Eo, Ho, _ = gctx.field_EH_full(m, JE, JM, k, outside, multE=mult, multH=mult, precision="mixed")
+    pin = np.exp(1j * (inside @ kv))[:, None]
+    Ein = e0[None, :] * pin
+    Hin = hs * np.cross(kv, e0)[None, :] * pin
+    assert rel_l2(Ei[0], Ein) < 0.05 and rel_l2(Hi[0], Hin) < 0.05
+    assert np.sqrt(np.mean(np.abs(Eo[0]) ** 2)) < 0.05 and np.sqrt(np.mean(np.abs(Ho[0]) ** 2)) < 0.05
