@@ -301,10 +301,23 @@ def run_assembly(args, ctx, torch, dev, stream, flush):
         d = A[r0:r0 + 4096].to(torch.complex128) - A64[r0:r0 + 4096]
         num += float(torch.sum(d.real ** 2 + d.imag ** 2))
         den += float(torch.sum(A64[r0:r0 + 4096].real ** 2 + A64[r0:r0 + 4096].imag ** 2))
-    del A64, A
+    del A64
+    torch.cuda.empty_cache()
+    # the step after assembly: LU solve of this complex64 system (cuSOLVER, bielcc_solve_dense)
+    b = torch.randn(n, dtype=torch.complex64, device=dev)
+    a0 = torch.cuda.Event(enable_timing=True)
+    a1 = torch.cuda.Event(enable_timing=True)
+    a0.record(stream)
+    info = ctx.solve_dense(n, 1, True, A.data_ptr(), b.data_ptr(), stream=sc)
+    a1.record(stream)
+    a1.synchronize()
+    lu_ms = a0.elapsed_time(a1)
+    del A, b
     torch.cuda.empty_cache()
     mesh.close()
     return {"workload": f"{wl['name']}: TAU2 {n}x{n} complex64, FP64 near/self entries",
+            "lu_solve": {"n": n, "dtype": "c64", "ms": lu_ms, "info": info,
+                         "tflops": 8.0 * n ** 3 / 3.0 / (lu_ms * 1e-3) / 1e12, "library": "cuSOLVER getrf/getrs"},
             "value": N * N / (ms * 1e-3), "unit": "(collocation point, cell) pairs/s", "ms": ms, "steps": steps,
             "fp64_ms": ms64, "mixed_over_fp64": ms64 / ms, "rel_l2_vs_fp64": (num / den) ** 0.5,
             "near_pairs": int(rep.n_near_pairs), "matrix_gb": n * n * 8 / 1e9,

@@ -58,7 +58,7 @@ def build(verbose=False, force=False):
             sys.stderr.write(f"--- {s}\n{out}\n")
         raise RuntimeError("nvcc failed on " + ", ".join(os.path.basename(s) for s, _ in failed))
     if force or _stale(LIB, objs):
-        cmd = [NVCC] + HOST_CC + ARCH + ["-shared", "-o", LIB] + objs
+        cmd = [NVCC] + HOST_CC + ARCH + ["-shared", "-o", LIB] + objs + ["-ldl"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

@@ -1155,6 +1155,57 @@ int bielcc_assemble_K_device(bielcc_ctx ctx, bielcc_mesh mesh, double k_re, doub
     return BIELCC_OK;
 }
 
+int bielcc_solve_pec(bielcc_ctx ctx, bielcc_mesh mesh, double k_re, double k_im, double multE_re, double multE_im,
+                     const bielcc_planewave* inc, const bielcc_numparam* np, int precision, double* J_host,
+                     bielcc_report* report) {
+    TRY(enter(ctx));
+    if (!inc || !J_host) return set_error(BIELCC_ERR_ARG, "solve_pec: incident wave and J required");
+    if (multE_re == 0. && multE_im == 0.) return set_error(BIELCC_ERR_ARG, "solve_pec: multE must not be 0");
+    if (precision != BIELCC_PREC_FP64 && precision != BIELCC_PREC_MIXED)
+        return set_error(BIELCC_ERR_ARG, "unknown precision %d", precision);
+    MeshDev* m;
+    {
+        std::lock_guard<std::mutex> g(ctx->mu);
+        TRY(get_mesh(ctx, mesh, &m));
+    }
+    const int N = m->n_cells, dim = 2 * N;
+    const int c64 = precision == BIELCC_PREC_MIXED ? 1 : 0;
+    const size_t elt = c64 ? 8 : 16;
+    void* A = nullptr;
+    void* b = nullptr;
+    double* dJ = nullptr;
+    if (cudaMalloc(&A, (size_t)dim * dim * elt) != cudaSuccess || cudaMalloc(&b, (size_t)dim * elt) != cudaSuccess ||
+        cudaMalloc((void**)&dJ, (size_t)N * 48) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(A);
+        cudaFree(b);
+        return set_error(BIELCC_ERR_OOM, "solve_pec: device allocation of the %d x %d system failed", dim, dim);
+    }
+    int rc = bielcc_assemble_K_device(ctx, mesh, k_re, k_im, np, BIELCC_LAYOUT_TAU2, c64, precision, A, nullptr,
+                                      report);
+    int info = 0;
+    if (rc == BIELCC_OK) {
+        // b_(i,a) = -tau_a(i) . E_inc(c_i) / multE
+        const double m2 = multE_re * multE_re + multE_im * multE_im;
+        const cplx scale = mk(-multE_re / m2, multE_im / m2);  // -1 / multE
+        cudaError_t e = launch_efie_rhs(m->geo, N, inc->k_vec, inc->e0, scale, c64, b, ctx->stream);
+        if (e != cudaSuccess) rc = cuda_status(e, "efie rhs", __LINE__);
+    }
+    if (rc == BIELCC_OK) rc = bielcc_solve_dense(dim, 1, c64, A, b, ctx->stream, &info);
+    if (rc == BIELCC_OK) {
+        cudaError_t e = launch_basis_currents(m->geo, N, b, c64, dJ, ctx->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(J_host, dJ, (size_t)N * 48, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) rc = cuda_status(e, "solve_pec currents", __LINE__);
+    }
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(A);
+    cudaFree(b);
+    cudaFree(dJ);
+    if (report) report->status = rc;
+    return rc;
+}
+
 int bielcc_assemble_K(bielcc_ctx ctx, bielcc_mesh mesh, double k_re, double k_im, const bielcc_numparam* np,
                       int layout, int out_c64, int precision, void* A_host, bielcc_report* report) {
     TRY(enter(ctx));

@@ -82,6 +82,12 @@ cudaError_t launch_combine_full(const double* E2, const double* H2, int S, int P
                                 const double* pts, const FullInc& inc, double* E, double* H,
                                 unsigned long long* nonfinite, cudaStream_t s);
 
+// ---- solve.cu: right-hand side of the perfect-conductor collocation system and
+// the currents from its solution (TAU2 layout; c64 selects complex64 vectors)
+cudaError_t launch_efie_rhs(const CellGeo* geo, int n, const double* kvec, const double* e0, cplx scale, int c64,
+                            void* b, cudaStream_t s);
+cudaError_t launch_basis_currents(const CellGeo* geo, int n, const void* x, int c64, double* J, cudaStream_t s);
+
 // ---- pairops.cu
 cudaError_t launch_pair_op(int op, int nv, int n, const double* cells, const double* x, const double* j, cplx k,
                            NumParamH np, double* res, cudaStream_t s);

@@ -56,6 +56,9 @@ def load(path=LIB_PATH):
                                  C.POINTER(abi.PlaneWave), C.POINTER(abi.NumParam), C.c_int, vp, vp, vp, C.c_int, vp,
                                  C.POINTER(abi.Report)])
     d("bielcc_integrand_info", [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)])
+    d("bielcc_solve_dense", [C.c_int, C.c_int, C.c_int, vp, vp, vp, C.POINTER(C.c_int)])
+    d("bielcc_solve_pec", [vp, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double, C.POINTER(abi.PlaneWave),
+                           C.POINTER(abi.NumParam), C.c_int, dp, C.POINTER(abi.Report)])
     d("bielcc_read_mesh_dat", [C.c_char_p, C.c_int, C.POINTER(C.c_int), dp])
     d("bielcc_read_mesh_vtk", [C.c_char_p, C.c_int, C.POINTER(C.c_int), dp, C.POINTER(C.c_int)])
     d("bielcc_read_currents", [C.c_char_p, C.c_char_p, C.POINTER(C.c_int), dp])
@@ -307,6 +310,26 @@ class Context:
                                                 C.c_void_p(pts_dev), C.c_void_p(E_dev), C.c_void_p(H_dev),
                                                 PREC[precision], _stream_arg(stream), C.byref(rep)))
         return rep
+
+    # ------------------------------------------------------------------ solving the collocation system
+    def solve_pec(self, mesh, k, inc, multE, numparam=None, precision="fp64"):
+        """Currents J [N][3] of a perfect conductor under the plane wave `inc`
+        (bielcc_solve_pec): TAU2 assembly, LU solve, basis -> currents."""
+        J = np.zeros((mesh.n_cells, 3), np.complex128)
+        np_ = numparam if numparam is not None else abi.NumParam.default()
+        k, multE = complex(k), complex(multE)
+        rep = abi.Report()
+        _check(_lib.bielcc_solve_pec(self.h, mesh.id, k.real, k.imag, multE.real, multE.imag, C.byref(inc),
+                                     C.byref(np_), PREC[precision], abi.dptr(J), C.byref(rep)))
+        return J
+
+    @staticmethod
+    def solve_dense(n, nrhs, c64, A_dev, B_dev, stream=None):
+        """A X = B on device buffers (row-major A, B = [nrhs][n]); returns cuSOLVER's info."""
+        info = C.c_int(0)
+        _check(_lib.bielcc_solve_dense(n, nrhs, int(bool(c64)), C.c_void_p(A_dev), C.c_void_p(B_dev),
+                                       _stream_arg(stream), C.byref(info)))
+        return info.value
 
     # ------------------------------------------------------------------ batched field
     @staticmethod

@@ -527,6 +527,29 @@ int bielcc_server_cancel(bielcc_server sv, int64_t ticket);
 int bielcc_server_drain(bielcc_server sv, double timeout_s);
 int bielcc_server_get_stats(bielcc_server sv, bielcc_server_stats* out, int reset);
 
+/* ---- solving the collocation system ------------------------------------
+ * No counterpart in the reference (it assembles operators but has no solver).
+ * bielcc_solve_dense: A X = B for a dense complex n x n matrix in row-major
+ * order (the layout bielcc_assemble_K writes), B the nrhs right-hand sides,
+ * each contiguous ([nrhs][n]); LU with partial pivoting from cuSOLVER
+ * (getrf / getrs, loaded on first use; BIELCC_ERR_UNSUPPORTED without it).
+ * c64 = 1: complex64, 0: complex128. A is overwritten by its factors, B by X;
+ * *info is cuSOLVER's (0 = success); n^2 < 2^31. Device pointers, `stream` as
+ * in the _device calls (NULL = legacy default stream); returns after the
+ * solve has finished.
+ * bielcc_solve_pec: the perfectly conducting body under a plane wave. Builds
+ * the TAU2 matrix (bielcc_assemble_K), the right-hand side
+ * b_(i,a) = -tau_a(i) . E_inc(c_i) / multE (the tangential boundary condition
+ * E_inc + multE K[J] = 0 at the collocation points), solves, and writes the
+ * currents J_j = x_(j,1) tau1(j) + x_(j,2) tau2(j) (SurfaceCurrents_byBasis,
+ * electrodynamics/currents.h:22-33) as complex128 [n_cells][3] to J_host.
+ * MIXED: complex64 matrix and LU; FP64: complex128. The (2N)^2 matrix is
+ * allocated for the call (13.4 GB complex64 at N = 20,480). */
+int bielcc_solve_dense(int n, int nrhs, int c64, void* A_dev, void* B_dev, void* stream, int* info);
+int bielcc_solve_pec(bielcc_ctx ctx, bielcc_mesh mesh, double k_re, double k_im, double multE_re,
+                     double multE_im, const bielcc_planewave* inc, const bielcc_numparam* np,
+                     int precision, double* J_host, bielcc_report* report);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif
