@@ -53,8 +53,11 @@ struct BatchCfg {
     static constexpr int CH = MIXED ? BIELCC_BATCH_CH32 : 8;            // cells per chunk (n_start <= 8)
     static constexpr int NODES = MIXED ? 64 * BIELCC_BATCH_CH32 : 512;  // staged nodes
     static constexpr int R = MIXED ? 4 : 2;               // RHS per thread in phase B
+    // currents per (cell, RHS, component): FP32 (re, im, im, re) for the packed
+    // contraction, FP64 (re, im)
+    static constexpr int JW = MIXED ? 4 : 2;
     static constexpr size_t smem_bytes() {
-        return sizeof(NodeT) * NODES + sizeof(F) * CH * 20 * kBP + sizeof(F) * 2 * CH * kSP * 3 +
+        return sizeof(NodeT) * NODES + sizeof(F) * CH * 20 * kBP + sizeof(F) * JW * CH * kSP * 3 +
                sizeof(double4) * CH + sizeof(double) * CH + CH * kBP + 64;
     }
 };
@@ -84,6 +87,68 @@ BIELCC_D void contract12(const F* m, const F* jr, const F* ji, F* acc) {
         const F gbr = m[14 + 2 * b], gbi = m[15 + 2 * b], gcr = m[14 + 2 * c], gci = m[15 + 2 * c];
         acc[6 + 2 * a] += (gbr * jr[c] - gbi * ji[c]) - (gcr * jr[b] - gci * ji[b]);
         acc[6 + 2 * a + 1] += (gbr * ji[c] + gbi * jr[c]) - (gcr * ji[b] + gci * jr[b]);
+    }
+}
+
+// The FP32 contraction of one cell's moments (A1 already on T's diagonal) with
+// the RHS sl = sl0 + step * j (j < R, sl < sp), two lanes of a packed
+// fma.rn.f32x2 per complex multiply-add: (mr + i mi)(jr + i ji) =
+// (mr, mr) * (jr, ji) + (-mi, mi) * (ji, jr). The currents are staged as
+// (re, im, im, re), so both operand pairs come from one 128-bit load.
+BIELCC_D float2 f2(float v) { return make_float2(v, v); }
+
+template <int R>
+BIELCC_D void contract_packed_cell(const float* m, const float4* __restrict__ sj, int sl0, int step, int sp,
+                                   float (&acc)[R][12]) {
+    float2 P[9], Q[9];  // T (6 entries), G (3): (mr, mr), (-mi, mi)
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        P[q] = f2(m[2 + 2 * q]);
+        Q[q] = make_float2(-m[3 + 2 * q], m[3 + 2 * q]);
+    }
+    float2 NP[3], NQ[3];  // -G as pairs, for the subtracted half of G x J
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        P[6 + q] = f2(m[14 + 2 * q]);
+        Q[6 + q] = make_float2(-m[15 + 2 * q], m[15 + 2 * q]);
+        NP[q] = f2(-m[14 + 2 * q]);
+        NQ[q] = make_float2(m[15 + 2 * q], -m[15 + 2 * q]);
+    }
+    const int ti[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+#pragma unroll
+    for (int j = 0; j < R; j++) {
+        const int sl = sl0 + step * j;
+        if (sl >= sp) continue;
+        const float4* jj = sj + (size_t)sl * 3;
+        float2 jp[3], js[3];
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            const float4 v = jj[b];
+            jp[b] = make_float2(v.x, v.y);
+            js[b] = make_float2(v.z, v.w);
+        }
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            float2 e = make_float2(acc[j][2 * a], acc[j][2 * a + 1]);
+#pragma unroll
+            for (int b = 0; b < 3; b++) {
+                e = __ffma2_rn(P[ti[a][b]], jp[b], e);
+                e = __ffma2_rn(Q[ti[a][b]], js[b], e);
+            }
+            acc[j][2 * a] = e.x;
+            acc[j][2 * a + 1] = e.y;
+        }
+#pragma unroll
+        for (int a = 0; a < 3; a++) {  // H_a = G_b J_c - G_c J_b
+            const int b = (a + 1) % 3, c = (a + 2) % 3;
+            float2 h = make_float2(acc[j][6 + 2 * a], acc[j][7 + 2 * a]);
+            h = __ffma2_rn(P[6 + b], jp[c], h);
+            h = __ffma2_rn(Q[6 + b], js[c], h);
+            h = __ffma2_rn(NP[c], jp[b], h);
+            h = __ffma2_rn(NQ[c], js[b], h);
+            acc[j][6 + 2 * a] = h.x;
+            acc[j][7 + 2 * a] = h.y;
+        }
     }
 }
 
@@ -170,8 +235,8 @@ __global__ void __launch_bounds__(kBT, MIXED ? BIELCC_BATCH_MINB : 2) batch_far_
     extern __shared__ __align__(16) unsigned char smem[];
     NodeT* s_nodes = (NodeT*)smem;
     F* s_mom = (F*)(s_nodes + C::NODES);                 // [CH][20][kBP]
-    F* s_j = s_mom + C::CH * 20 * kBP;                   // [CH][kSP][3][2]
-    double4* s_cell = (double4*)(s_j + C::CH * kSP * 6);  // centre, diam
+    F* s_j = s_mom + C::CH * 20 * kBP;                   // [CH][kSP][3][JW]
+    double4* s_cell = (double4*)(s_j + C::CH * kSP * 3 * C::JW);  // centre, diam
     double* s_rho = (double*)(s_cell + C::CH);
     unsigned char* s_near = (unsigned char*)(s_rho + C::CH);  // [CH][kBP]
     __shared__ int s_item;
@@ -222,9 +287,13 @@ __global__ void __launch_bounds__(kBT, MIXED ? BIELCC_BATCH_MINB : 2) batch_far_
                 for (int i = threadIdx.x; i < nc * sp * 3; i += kBT) {
                     const int cc = i / (sp * 3), rem = i - cc * sp * 3, sl = rem / 3, g = rem - sl * 3;
                     const cplx v = jb.J[((size_t)(s0 + sl) * N + (c0 + cc)) * 3 + g];
-                    F* d = s_j + ((size_t)(cc * kSP + sl) * 3 + g) * 2;
+                    F* d = s_j + ((size_t)(cc * kSP + sl) * 3 + g) * C::JW;
                     d[0] = (F)v.re;
                     d[1] = (F)v.im;
+                    if constexpr (MIXED) {
+                        d[2] = (F)v.im;
+                        d[3] = (F)v.re;
+                    }
                 }
                 __syncthreads();
                 // phase A: moments of cells warp, warp+4, ... for this warp's 32 points
@@ -278,13 +347,18 @@ __global__ void __launch_bounds__(kBT, MIXED ? BIELCC_BATCH_MINB : 2) batch_far_
                         m[9] += m[1];
                         m[12] += m[0];
                         m[13] += m[1];
+                        if constexpr (MIXED) {
+                            contract_packed_cell<C::R>(m, reinterpret_cast<const float4*>(s_j) + (size_t)cc * kSP * 3,
+                                                       sb + warp, kBW, sp, acc);
+                        } else {
 #pragma unroll
-                        for (int j = 0; j < C::R; j++) {
-                            const int sl = sb + warp + kBW * j;
-                            if (sl < sp) {
-                                const F* jj = s_j + (size_t)(cc * kSP + sl) * 6;
-                                const F jr[3] = {jj[0], jj[2], jj[4]}, ji[3] = {jj[1], jj[3], jj[5]};
-                                contract12<F>(m, jr, ji, acc[j]);
+                            for (int j = 0; j < C::R; j++) {
+                                const int sl = sb + warp + kBW * j;
+                                if (sl < sp) {
+                                    const F* jj = s_j + (size_t)(cc * kSP + sl) * 6;
+                                    const F jr[3] = {jj[0], jj[2], jj[4]}, ji[3] = {jj[1], jj[3], jj[5]};
+                                    contract12<F>(m, jr, ji, acc[j]);
+                                }
                             }
                         }
                     }
