@@ -180,18 +180,43 @@ BIELCC_D void far_node_f32(Moments<float>& m, float Xx, float Xy, float Xz, floa
     float dx = Xx - nd.x, dy = Xy - nd.y, dz = Xz - nd.z;
     float ir2 = ir * ir, ir3 = ir2 * ir;
     float er = w * c, ei = w * s;
-    float f1r, f1i, f2r, f2i;
-    if (CK) {
-        f1r = k2r * ir - ir3 - ki_ * ir2;
-        f1i = kr_ * ir2 + k2i * ir;
-        f2r = 3.f * ir3 + 3.f * ki_ * ir2 - k2r * ir;
-        f2i = -3.f * kr_ * ir2 - k2i * ir;
-    } else {
-        f1r = k2r * ir - ir3;
-        f1i = kr_ * ir2;
-        f2r = 3.f * ir3 - k2r * ir;
-        f2i = -3.f * kr_ * ir2;
+    if (!CK) {
+        // real k: with alpha = 1/r^3 - i k/r^2 and u = k^2/r,
+        //   f1 = u - alpha, f2 = 3 alpha - u, (ikr - 1)/r^3 = -alpha,
+        // so one complex product e * alpha serves all three moment sets
+        const float beta = kr_ * ir2, u = k2r * ir;
+        const float ear = fmaf(ei, beta, er * ir3), eai = fmaf(-er, beta, ei * ir3);  // e alpha
+        const float ekr = er * u, eki = ei * u;                                          // e k^2 / r
+        m.a1r += ekr - ear;
+        m.a1i += eki - eai;
+        const float a2r = fmaf(3.f, ear, -ekr) * ir2, a2i = fmaf(3.f, eai, -eki) * ir2;
+        const float bx_r = a2r * dx, bx_i = a2i * dx, by_r = a2r * dy, by_i = a2i * dy, bz_r = a2r * dz,
+                    bz_i = a2i * dz;
+        m.t[0][0] = fmaf(bx_r, dx, m.t[0][0]);
+        m.t[0][1] = fmaf(bx_i, dx, m.t[0][1]);
+        m.t[1][0] = fmaf(bx_r, dy, m.t[1][0]);
+        m.t[1][1] = fmaf(bx_i, dy, m.t[1][1]);
+        m.t[2][0] = fmaf(bx_r, dz, m.t[2][0]);
+        m.t[2][1] = fmaf(bx_i, dz, m.t[2][1]);
+        m.t[3][0] = fmaf(by_r, dy, m.t[3][0]);
+        m.t[3][1] = fmaf(by_i, dy, m.t[3][1]);
+        m.t[4][0] = fmaf(by_r, dz, m.t[4][0]);
+        m.t[4][1] = fmaf(by_i, dz, m.t[4][1]);
+        m.t[5][0] = fmaf(bz_r, dz, m.t[5][0]);
+        m.t[5][1] = fmaf(bz_i, dz, m.t[5][1]);
+        m.g[0][0] = fmaf(-ear, dx, m.g[0][0]);
+        m.g[0][1] = fmaf(-eai, dx, m.g[0][1]);
+        m.g[1][0] = fmaf(-ear, dy, m.g[1][0]);
+        m.g[1][1] = fmaf(-eai, dy, m.g[1][1]);
+        m.g[2][0] = fmaf(-ear, dz, m.g[2][0]);
+        m.g[2][1] = fmaf(-eai, dz, m.g[2][1]);
+        return;
     }
+    float f1r, f1i, f2r, f2i;
+    f1r = k2r * ir - ir3 - ki_ * ir2;
+    f1i = kr_ * ir2 + k2i * ir;
+    f2r = 3.f * ir3 + 3.f * ki_ * ir2 - k2r * ir;
+    f2i = -3.f * kr_ * ir2 - k2i * ir;
     m.a1r = fmaf(er, f1r, fmaf(-ei, f1i, m.a1r));
     m.a1i = fmaf(er, f1i, fmaf(ei, f1r, m.a1i));
     float a2r = (er * f2r - ei * f2i) * ir2, a2i = (er * f2i + ei * f2r) * ir2;
@@ -208,7 +233,7 @@ BIELCC_D void far_node_f32(Moments<float>& m, float Xx, float Xy, float Xz, floa
     m.t[4][1] = fmaf(by_i, dz, m.t[4][1]);
     m.t[5][0] = fmaf(bz_r, dz, m.t[5][0]);
     m.t[5][1] = fmaf(bz_i, dz, m.t[5][1]);
-    float ur = CK ? (-ki_ * r - 1.f) : -1.f, ui = kr_ * r;
+    float ur = -ki_ * r - 1.f, ui = kr_ * r;
     float gr = (er * ur - ei * ui) * ir3, gi = (er * ui + ei * ur) * ir3;
     m.g[0][0] = fmaf(gr, dx, m.g[0][0]);
     m.g[0][1] = fmaf(gi, dx, m.g[0][1]);
