@@ -129,3 +129,35 @@ def test_batch_plan_graph_replay_with_new_currents(gctx):
         assert rel_l2(E, Eo) < TOL_MIXED and rel_l2(H, Ho) < TOL_MIXED
     assert plan.report.n_near_pairs > 0
     plan.close()
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", TOL_FP64), ("mixed", TOL_MIXED)])
+def test_batch_edge_cases(gctx, precision, tol):
+    """An empty batch; a job without points; a one-cell mesh; 70 right-hand
+    sides (more than one staged pass of 64); all in one launch, against the
+    oracle; and the largest staged split, n_start = 22."""
+    torch = pytest.importorskip("torch")
+    assert gctx.field_EH_batch(gctx.make_jobs([]), precision=precision).n_pairs == 0
+    rng = np.random.default_rng(9)
+    sph = W.uv_sphere(4, 8)
+    specs = [
+        dict(mesh=gctx.mesh(sph[7:8]), cells=sph[7:8], J=W.po_currents(sph, 2.0)[:, 7:8], pts=np.array([[2.5, 0.3, 0.1]]),
+             k=2.0, mult=1.0),
+        dict(mesh=gctx.mesh(sph), cells=sph, J=W.po_currents(sph, 3.0, directions=70, seed=4),
+             pts=np.concatenate([W.shell_points(20, 2.0, 3.0, rng), W.near_points(sph, 4, 0.02, 0.1, rng)]), k=3.0,
+             mult=complex(0.0, 1.0)),
+        dict(mesh=gctx.mesh(sph), cells=sph, J=W.po_currents(sph, 1.0), pts=np.zeros((0, 3)), k=1.0, mult=1.0),
+    ]
+    outs, _ = _batch(torch, gctx, specs, precision)
+    for sp, (E, H) in zip(specs, outs):
+        if len(sp["pts"]) == 0:
+            assert E.shape[1] == 0
+            continue
+        Eo, Ho = oracle.field_EH(sp["cells"], sp["J"], sp["k"], sp["pts"], mult=sp["mult"])
+        assert rel_l2(E, Eo) < tol and rel_l2(H, Ho) < tol
+    npm = abi.NumParam.default(n_start=22)
+    sp = specs[1]
+    sp22 = dict(sp, J=sp["J"][:3])
+    outs, _ = _batch(torch, gctx, [sp22], precision, numparam=npm)
+    Eo, Ho = oracle.field_EH(sp22["cells"], sp22["J"], sp22["k"], sp22["pts"], npm, mult=sp22["mult"])
+    assert rel_l2(outs[0][0], Eo) < tol and rel_l2(outs[0][1], Ho) < tol
