@@ -1,6 +1,7 @@
 // api.cu — the C ABI of libbielcc_gpu.so (include/bielcc_gpu.h): contexts,
 // resident meshes, workspaces, host<->device staging and kernel dispatch.
 // No C++ exception crosses the boundary; every entry point returns a status.
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -191,10 +192,77 @@ struct FieldArgs {
     int precision;
 };
 
+// More than 4 right-hand sides: the single-job far kernel takes at most 4 per
+// launch and repeats the quadrature for every group of 4, while the batched
+// kernel computes the J-independent moments once for up to 64 and contracts
+// them with each. The job runs as a one-job batch when the saved quadratures
+// (ceil(S/4) passes) outweigh the batched kernel's idle SMs on a small point
+// set (its work items over its resident CTAs). Returns false when the call is
+// left to the single-job path.
+int field_device_batched(bielcc_ctx ctx, const FieldArgs& a, cudaStream_t s, bielcc_report* rep,
+                         unsigned long long* d_nonfinite, bool* done) {
+    *done = false;
+    if (a.n_rhs <= 4 || a.np.p_max > 1 || a.np.n_start > kBatchMaxNStart || a.n_pts == 0) return BIELCC_OK;
+    TRY(ensure_tables(a.m, a.np.n_start, s));
+    JobDev d;
+    memset(&d, 0, sizeof(d));
+    d.geo = a.m->geo;
+    d.nodes32 = a.m->nodes32;
+    d.nodes64 = a.m->nodes64;
+    d.rho32 = a.m->rho32;
+    d.verts = a.m->verts;
+    d.nv = a.m->nv;
+    d.n_cells = a.m->n_cells;
+    d.pts = a.pts;
+    d.n_pts = a.n_pts;
+    d.J = reinterpret_cast<const cplx*>(a.J);
+    d.n_rhs = a.n_rhs;
+    d.k = a.k;
+    d.mult = a.mult;
+    if (a.inc) {
+        for (int g = 0; g < 3; g++) {
+            d.kvec[g] = a.inc->k_vec[g];
+            d.e0[g] = a.inc->e0[g];
+        }
+        d.h_scale = a.inc->h_scale;
+        d.add_E = a.inc->add_E;
+        d.add_H = a.inc->add_H;
+    }
+    d.E = a.E;
+    d.H = a.H;
+    BatchPlan bp;
+    plan_batch(bp, std::vector<JobDev>{d}, a.np.n_start, a.precision == BIELCC_PREC_MIXED, ctx->batch_item_cost);
+    const double busy = std::min(1.0, (double)bp.items.size() / std::max(1, bp.grid));
+    if ((double)((a.n_rhs + 3) / 4) * busy <= 1.5) return BIELCC_OK;
+    TRY(ctx->ws.ensure(bp.ws_bytes));
+    BatchDevPtrs dp;
+    int l1 = 0, l2 = 0;
+    TRY_CUDA(batch_stage1(bp, ctx->ws.p, a.np.analytic_calc, a.np.n_start, a.k.im != 0., s, &dp, &l1));
+    TRY_CUDA(cudaMemcpyAsync(ctx->h_total, dp.total, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    TRY_CUDA(cudaStreamSynchronize(s));
+    const long long n_near = *ctx->h_total;
+    if (n_near > 0) TRY(ctx->pair_ws.ensure(batch_pair_ws_bytes(n_near)));
+    DNP dn{a.np.eps, a.np.rs, a.np.rs_seg, a.np.analytic_calc, a.np.n_start, a.np.n_start_seg, a.np.p_max,
+           a.np.p_max_seg};
+    TRY_CUDA(batch_stage2(bp, dp, n_near, ctx->pair_ws.p, dn, d_nonfinite, s, &l2));
+    ctx->stats.kernel_launches += l1 + l2;
+    ctx->stats.far_launches += 1;
+    ctx->stats.far_pairs += ((long long)a.n_pts * a.m->n_cells - n_near) * a.n_rhs;
+    if (rep) {
+        rep->n_pairs = (int64_t)a.n_pts * a.m->n_cells;
+        rep->n_near_pairs = n_near;
+    }
+    *done = true;
+    return BIELCC_OK;
+}
+
 // Enqueues a field evaluation on device buffers; one short host wait for the
 // near-pair count (sizes the FP64 near workspace).
 int field_device(bielcc_ctx ctx, const FieldArgs& a, cudaStream_t s, bielcc_report* rep,
                  unsigned long long* d_nonfinite) {
+    bool done = false;
+    TRY(field_device_batched(ctx, a, s, rep, d_nonfinite, &done));
+    if (done) return BIELCC_OK;
     TRY(ensure_tables(a.m, a.np.n_start, s));
     FieldLaunch f;
     f.mesh = a.m;
