@@ -74,6 +74,31 @@ BIELCC_D void far_node_f64(Moments<double>& m, double dx, double dy, double dz, 
     }
     double ir2 = ir * ir, ir3 = ir2 * ir;
     double er = w * c, ei = w * s;
+    if (!CK) {
+        // real k: alpha = 1/r^3 - i k/r^2, u = k^2/r; f1 = u - alpha, f2 = 3 alpha - u,
+        // (ikr - 1)/r^3 = -alpha: one complex product e * alpha for all moment sets
+        const double beta = k.re * ir2, u = k2r * ir;
+        const double ear = fma(ei, beta, er * ir3), eai = fma(-er, beta, ei * ir3);
+        if (r >= kMachineZero) {  // F_RotRotSimplePot_H is 0 below MACHINE_ZERO
+            const double ekr = er * u, eki = ei * u;
+            m.a1r += ekr - ear;
+            m.a1i += eki - eai;
+            const double a2r = fma(3.0, ear, -ekr) * ir2, a2i = fma(3.0, eai, -eki) * ir2;
+            const double dd[6] = {dx * dx, dx * dy, dx * dz, dy * dy, dy * dz, dz * dz};
+#pragma unroll
+            for (int q = 0; q < 6; q++) {
+                m.t[q][0] += a2r * dd[q];
+                m.t[q][1] += a2i * dd[q];
+            }
+        }
+        m.g[0][0] -= ear * dx;
+        m.g[0][1] -= eai * dx;
+        m.g[1][0] -= ear * dy;
+        m.g[1][1] -= eai * dy;
+        m.g[2][0] -= ear * dz;
+        m.g[2][1] -= eai * dz;
+        return;
+    }
     if (r >= kMachineZero) {  // F_RotRotSimplePot_H is 0 below MACHINE_ZERO
         double f1r, f1i, f2r, f2i;
         if (CK) {
