@@ -118,7 +118,8 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_far_kernel(AsmArgs a) {
     using F = typename std::conditional<MIXED, float, double>::type;
     F a1r = 0, a1i = 0, t[6][2];
     bool far = false;
-    float Xf[3] = {0.f, 0.f, 0.f}, r0f = 0.f, r0sq = 0.f;
+    float Xf[3] = {0.f, 0.f, 0.f}, r0f = 0.f, r0sq = 0.f, r0k = 0.f;
+    const KF32 kf = KF32::make(a.k.re, a.k.im);
     double P0r = 1., P0i = 0.;
     int mode = 0;  // phase polynomial of the current cell (farnode.cuh phase_mode)
     bool split64 = false;
@@ -186,6 +187,7 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_far_kernel(AsmArgs a) {
                         Xf[2] = (float)(x[2] - gj.c[2]);
                         r0f = (float)d;
                         r0sq = (float)(d * d);
+                        r0k = r0f * kf.ikr;
                         double sn, cs;
                         sincos(a.k.re * d, &sn, &cs);
                         if (CK) {
@@ -201,11 +203,9 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_far_kernel(AsmArgs a) {
                 if (far) {
                     const NodeT* nd = s_nodes + cc * kc;
                     if constexpr (MIXED) {
-                        const float kr_ = (float)a.k.re, ki_ = (float)a.k.im;
-                        const float k2rf = (float)k2r, k2if = (float)k2i;
 #define BIELCC_ASM_LOOP(MODE_)                                                                         \
     _Pragma("unroll 4") for (int q = 0; q < kc; q++)                                                    \
-        far_node_f32_K<CK, MODE_>(a1r, a1i, t, Xf[0], Xf[1], Xf[2], r0f, r0sq, nd[q], kr_, ki_, k2rf, k2if);
+        far_node_f32_K<CK, MODE_>(a1r, a1i, t, Xf[0], Xf[1], Xf[2], r0f, r0sq, r0k, nd[q], kf);
                         switch (mode) {
                             case 0: BIELCC_ASM_LOOP(0) break;
                             case 1: BIELCC_ASM_LOOP(1) break;
@@ -234,6 +234,7 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_far_kernel(AsmArgs a) {
                                                         r0d);
                             }
                         }
+                        if (!CK) mm.finish_real_k();
                         a1r += mm.a1r;
                         a1i += mm.a1i;
 #pragma unroll
@@ -244,6 +245,7 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_far_kernel(AsmArgs a) {
                     }
                 }
                 if (k0 + kc == nn && far) {
+                    if constexpr (MIXED && !CK) finish_real_k<F>(a1r, a1i, t);
                     // K = (A1 I + T) * P0 / 4pi
                     const int ti[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
                     double Kr[3][3], Ki[3][3];

@@ -175,11 +175,12 @@ BIELCC_D void batch_moments(const typename BatchCfg<MIXED>::NodeT* nd, int nn, c
         }
         P0r = cs;
         P0i = sn;
-        const float kr_ = (float)k.re, ki_ = (float)k.im, k2rf = (float)k2r, k2if = (float)k2i;
+        const KF32 kf = KF32::make(k.re, k.im);
+        const float r0k = r0f * kf.ikr;
         const int mode = phase_mode((float)fabs(k.re) * (float)rho);
 #define BIELCC_BNODE(MODE_)                                                                            \
     _Pragma("unroll 4") for (int i = 0; i < nn; i++)                                                    \
-        far_node_f32<CK, MODE_>(m, Xx, Xy, Xz, r0f, r0sq, nd[i], kr_, ki_, k2rf, k2if);
+        far_node_f32<CK, MODE_>(m, Xx, Xy, Xz, r0f, r0sq, r0k, nd[i], kf);
         switch (mode) {
             case 0: BIELCC_BNODE(0) break;
             case 1: BIELCC_BNODE(1) break;
@@ -206,6 +207,7 @@ BIELCC_D void batch_moments(const typename BatchCfg<MIXED>::NodeT* nd, int nn, c
             }
         }
     }
+    if (!CK) m.finish_real_k();
     // moments x e^{ik r0}; R_Rot_Colloc is 0 at the cell centre
     const F pr = (F)P0r, pi = (F)P0i;
     mom[0] = m.a1r * pr - m.a1i * pi;

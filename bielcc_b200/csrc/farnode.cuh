@@ -5,6 +5,13 @@
 //   A1 = sum w e f1,  T = sum w e f2 d^ d^T (6),  G = sum w e (ikr - 1)/r^3 d (3)
 // so that K_RotRot_Far = (A1 J + T J)/4pi and R_Rot_Colloc = (G x J)/4pi.
 // FP64 and FP32 (phase split relative to the cell centre) forms.
+//
+// Real k: with alpha = 1/r^3 - i k/r^2 and u = k^2/r,
+//   f1 = u - alpha, f2 = 3 alpha - u, (ikr - 1)/r^3 = -alpha.
+// The node loop accumulates S = sum w e alpha in place of A1 and T/3 in place
+// of T; since |d|^2 = r^2, tr T = 3 S - sum w e u, so A1 = 2 S - tr T, which
+// finish_real_k recovers once per cell (two accumulators and the k^2/r
+// product leave the per-node work).
 #pragma once
 #include "common.cuh"
 
@@ -27,6 +34,44 @@ struct Moments {
         a1r = a1i = 0;
         for (int i = 0; i < 6; i++) t[i][0] = t[i][1] = 0;
         for (int i = 0; i < 3; i++) g[i][0] = g[i][1] = 0;
+    }
+    BIELCC_D void finish_real_k();
+};
+
+// Real-k node loops leave (S, T/3) in (a1, t): turn them into (A1, T).
+template <typename F>
+BIELCC_D void finish_real_k(F& a1r, F& a1i, F (&t)[6][2]) {
+    const F trr = t[0][0] + t[3][0] + t[5][0], tri = t[0][1] + t[3][1] + t[5][1];
+    a1r = F(2) * a1r - F(3) * trr;
+    a1i = F(2) * a1i - F(3) * tri;
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        t[q][0] *= F(3);
+        t[q][1] *= F(3);
+    }
+}
+
+template <typename F>
+BIELCC_D void Moments<F>::finish_real_k() {
+    bielcc_gpu::finish_real_k<F>(a1r, a1i, t);
+}
+
+// FP32 wavenumber constants of one launch (or one job).
+struct KF32 {
+    float kr, ki;    // k
+    float k2r, k2i;  // k^2
+    float ikr;       // 1 / Re k, 1e30 for Re k = 0 (phase k (r - r0) = q / ((r + r0) ikr) then rounds to 0)
+    float k2r3;      // Re k^2 / 3
+    static BIELCC_D KF32 make(double kre, double kim) {
+        KF32 f;
+        const double k2r = kre * kre - kim * kim;
+        f.kr = (float)kre;
+        f.ki = (float)kim;
+        f.k2r = (float)k2r;
+        f.k2i = (float)(2.0 * kre * kim);
+        f.ikr = kre != 0.0 ? (float)(1.0 / kre) : 1e30f;
+        f.k2r3 = (float)(k2r / 3.0);
+        return f;
     }
 };
 
@@ -75,15 +120,14 @@ BIELCC_D void far_node_f64(Moments<double>& m, double dx, double dy, double dz, 
     double ir2 = ir * ir, ir3 = ir2 * ir;
     double er = w * c, ei = w * s;
     if (!CK) {
-        // real k: alpha = 1/r^3 - i k/r^2, u = k^2/r; f1 = u - alpha, f2 = 3 alpha - u,
-        // (ikr - 1)/r^3 = -alpha: one complex product e * alpha for all moment sets
-        const double beta = k.re * ir2, u = k2r * ir;
+        // real k: S += e alpha, T/3 += e (alpha - u/3)/r^2 d d^T, G -= e alpha d
+        const double beta = k.re * ir2;
         const double ear = fma(ei, beta, er * ir3), eai = fma(-er, beta, ei * ir3);
         if (r >= kMachineZero) {  // F_RotRotSimplePot_H is 0 below MACHINE_ZERO
-            const double ekr = er * u, eki = ei * u;
-            m.a1r += ekr - ear;
-            m.a1i += eki - eai;
-            const double a2r = fma(3.0, ear, -ekr) * ir2, a2i = fma(3.0, eai, -eki) * ir2;
+            m.a1r += ear;
+            m.a1i += eai;
+            const double u3 = k2r * (1.0 / 3.0) * ir3;
+            const double a2r = fma(ear, ir2, -er * u3), a2i = fma(eai, ir2, -ei * u3);
             const double dd[6] = {dx * dx, dx * dy, dx * dz, dy * dy, dy * dz, dz * dz};
 #pragma unroll
             for (int q = 0; q < 6; q++) {
@@ -187,122 +231,37 @@ BIELCC_HD int phase_mode(float th) {
     return th <= 0.25f ? 0 : (th <= 1.f ? 1 : (th <= 2.f ? 2 : (th <= 4.f ? 3 : 4)));
 }
 
-// One far node, FP32, relative to the cell centre: X = x - centre (FP32),
-// node delta = y - centre, r0 = |X| (FP64 rounded), phase relative to r0.
+// Shared head of the FP32 far node, relative to the cell centre: X = x - centre
+// (FP32), node delta = y - centre, r0 = |X| (FP64 rounded), r0k = r0 / Re k.
+// Returns 1/r and sets r, the weighted phase factor e = w e^{ik(r - r0)} and d = x - y.
 template <bool CK, int MODE>
-BIELCC_D void far_node_f32(Moments<float>& m, float Xx, float Xy, float Xz, float r0, float r0sq, float4 nd, float kr_,
-                           float ki_, float k2r, float k2i) {
-    float tx = fmaf(-2.f, Xx, nd.x), ty = fmaf(-2.f, Xy, nd.y), tz = fmaf(-2.f, Xz, nd.z);
-    float q = fmaf(nd.x, tx, fmaf(nd.y, ty, nd.z * tz));  // |x-y|^2 - r0^2
-    float r2 = r0sq + q;
-    float ir = rsqrtf(r2);
-    float r = r2 * ir;
-    float dr = __fdividef(q, r + r0);
-    float s, c;
-    phase_f32<MODE>(kr_ * dr, &s, &c);
-    float w = nd.w;
-    if (CK) w *= __expf(-ki_ * dr);
-    float dx = Xx - nd.x, dy = Xy - nd.y, dz = Xz - nd.z;
-    float ir2 = ir * ir, ir3 = ir2 * ir;
-    float er = w * c, ei = w * s;
-    if (!CK) {
-        // real k: with alpha = 1/r^3 - i k/r^2 and u = k^2/r,
-        //   f1 = u - alpha, f2 = 3 alpha - u, (ikr - 1)/r^3 = -alpha,
-        // so one complex product e * alpha serves all three moment sets
-        const float beta = kr_ * ir2, u = k2r * ir;
-        const float ear = fmaf(ei, beta, er * ir3), eai = fmaf(-er, beta, ei * ir3);  // e alpha
-        const float ekr = er * u, eki = ei * u;                                          // e k^2 / r
-        m.a1r += ekr - ear;
-        m.a1i += eki - eai;
-        const float a2r = fmaf(3.f, ear, -ekr) * ir2, a2i = fmaf(3.f, eai, -eki) * ir2;
-        const float bx_r = a2r * dx, bx_i = a2i * dx, by_r = a2r * dy, by_i = a2i * dy, bz_r = a2r * dz,
-                    bz_i = a2i * dz;
-        m.t[0][0] = fmaf(bx_r, dx, m.t[0][0]);
-        m.t[0][1] = fmaf(bx_i, dx, m.t[0][1]);
-        m.t[1][0] = fmaf(bx_r, dy, m.t[1][0]);
-        m.t[1][1] = fmaf(bx_i, dy, m.t[1][1]);
-        m.t[2][0] = fmaf(bx_r, dz, m.t[2][0]);
-        m.t[2][1] = fmaf(bx_i, dz, m.t[2][1]);
-        m.t[3][0] = fmaf(by_r, dy, m.t[3][0]);
-        m.t[3][1] = fmaf(by_i, dy, m.t[3][1]);
-        m.t[4][0] = fmaf(by_r, dz, m.t[4][0]);
-        m.t[4][1] = fmaf(by_i, dz, m.t[4][1]);
-        m.t[5][0] = fmaf(bz_r, dz, m.t[5][0]);
-        m.t[5][1] = fmaf(bz_i, dz, m.t[5][1]);
-        m.g[0][0] = fmaf(-ear, dx, m.g[0][0]);
-        m.g[0][1] = fmaf(-eai, dx, m.g[0][1]);
-        m.g[1][0] = fmaf(-ear, dy, m.g[1][0]);
-        m.g[1][1] = fmaf(-eai, dy, m.g[1][1]);
-        m.g[2][0] = fmaf(-ear, dz, m.g[2][0]);
-        m.g[2][1] = fmaf(-eai, dz, m.g[2][1]);
-        return;
+BIELCC_D float far_head_f32(float Xx, float Xy, float Xz, float r0, float r0sq, float r0k, float4 nd, const KF32& kf,
+                            float& r_out, float& er, float& ei, float& dx, float& dy, float& dz) {
+    const float tx = fmaf(-2.f, Xx, nd.x), ty = fmaf(-2.f, Xy, nd.y), tz = fmaf(-2.f, Xz, nd.z);
+    const float q = fmaf(nd.x, tx, fmaf(nd.y, ty, nd.z * tz));  // |x-y|^2 - r0^2
+    const float r2 = r0sq + q;
+    const float ir = rsqrtf(r2);
+    const float r = r2 * ir;
+    float s, c, w = nd.w;
+    if (CK) {
+        const float dr = __fdividef(q, r + r0);  // r - r0 without cancellation
+        phase_f32<MODE>(kf.kr * dr, &s, &c);
+        w *= __expf(-kf.ki * dr);
+    } else {
+        phase_f32<MODE>(__fdividef(q, fmaf(r, kf.ikr, r0k)), &s, &c);  // k (r - r0)
     }
-    float f1r, f1i, f2r, f2i;
-    f1r = k2r * ir - ir3 - ki_ * ir2;
-    f1i = kr_ * ir2 + k2i * ir;
-    f2r = 3.f * ir3 + 3.f * ki_ * ir2 - k2r * ir;
-    f2i = -3.f * kr_ * ir2 - k2i * ir;
-    m.a1r = fmaf(er, f1r, fmaf(-ei, f1i, m.a1r));
-    m.a1i = fmaf(er, f1i, fmaf(ei, f1r, m.a1i));
-    float a2r = (er * f2r - ei * f2i) * ir2, a2i = (er * f2i + ei * f2r) * ir2;
-    float bx_r = a2r * dx, bx_i = a2i * dx, by_r = a2r * dy, by_i = a2i * dy, bz_r = a2r * dz, bz_i = a2i * dz;
-    m.t[0][0] = fmaf(bx_r, dx, m.t[0][0]);
-    m.t[0][1] = fmaf(bx_i, dx, m.t[0][1]);
-    m.t[1][0] = fmaf(bx_r, dy, m.t[1][0]);
-    m.t[1][1] = fmaf(bx_i, dy, m.t[1][1]);
-    m.t[2][0] = fmaf(bx_r, dz, m.t[2][0]);
-    m.t[2][1] = fmaf(bx_i, dz, m.t[2][1]);
-    m.t[3][0] = fmaf(by_r, dy, m.t[3][0]);
-    m.t[3][1] = fmaf(by_i, dy, m.t[3][1]);
-    m.t[4][0] = fmaf(by_r, dz, m.t[4][0]);
-    m.t[4][1] = fmaf(by_i, dz, m.t[4][1]);
-    m.t[5][0] = fmaf(bz_r, dz, m.t[5][0]);
-    m.t[5][1] = fmaf(bz_i, dz, m.t[5][1]);
-    float ur = -ki_ * r - 1.f, ui = kr_ * r;
-    float gr = (er * ur - ei * ui) * ir3, gi = (er * ui + ei * ur) * ir3;
-    m.g[0][0] = fmaf(gr, dx, m.g[0][0]);
-    m.g[0][1] = fmaf(gi, dx, m.g[0][1]);
-    m.g[1][0] = fmaf(gr, dy, m.g[1][0]);
-    m.g[1][1] = fmaf(gi, dy, m.g[1][1]);
-    m.g[2][0] = fmaf(gr, dz, m.g[2][0]);
-    m.g[2][1] = fmaf(gi, dz, m.g[2][1]);
+    dx = Xx - nd.x;
+    dy = Xy - nd.y;
+    dz = Xz - nd.z;
+    er = w * c;
+    ei = w * s;
+    r_out = r;
+    return ir;
 }
 
-// The K moments only (A1, T; no grad F) of one far node, FP32: the node
-// arithmetic of far_node_f32 for the collocation matrix, whose entries need
-// K_RotRot_Far alone.
-template <bool CK, int MODE>
-BIELCC_D void far_node_f32_K(float& a1r, float& a1i, float (&t)[6][2], float Xx, float Xy, float Xz, float r0,
-                             float r0sq, float4 nd, float kr_, float ki_, float k2r, float k2i) {
-    float tx = fmaf(-2.f, Xx, nd.x), ty = fmaf(-2.f, Xy, nd.y), tz = fmaf(-2.f, Xz, nd.z);
-    float q = fmaf(nd.x, tx, fmaf(nd.y, ty, nd.z * tz));  // |x-y|^2 - r0^2
-    float r2 = r0sq + q;
-    float ir = rsqrtf(r2);
-    float r = r2 * ir;
-    float dr = __fdividef(q, r + r0);
-    float s, c;
-    phase_f32<MODE>(kr_ * dr, &s, &c);
-    float w = nd.w;
-    if (CK) w *= __expf(-ki_ * dr);
-    float dx = Xx - nd.x, dy = Xy - nd.y, dz = Xz - nd.z;
-    float ir2 = ir * ir, ir3 = ir2 * ir;
-    float er = w * c, ei = w * s;
-    float f1r, f1i, f2r, f2i;
-    if (CK) {
-        f1r = k2r * ir - ir3 - ki_ * ir2;
-        f1i = kr_ * ir2 + k2i * ir;
-        f2r = 3.f * ir3 + 3.f * ki_ * ir2 - k2r * ir;
-        f2i = -3.f * kr_ * ir2 - k2i * ir;
-    } else {
-        f1r = k2r * ir - ir3;
-        f1i = kr_ * ir2;
-        f2r = 3.f * ir3 - k2r * ir;
-        f2i = -3.f * kr_ * ir2;
-    }
-    a1r = fmaf(er, f1r, fmaf(-ei, f1i, a1r));
-    a1i = fmaf(er, f1i, fmaf(ei, f1r, a1i));
-    float a2r = (er * f2r - ei * f2i) * ir2, a2i = (er * f2i + ei * f2r) * ir2;
-    float bx_r = a2r * dx, bx_i = a2i * dx, by_r = a2r * dy, by_i = a2i * dy, bz_r = a2r * dz, bz_i = a2i * dz;
+// T += b d^T over the 6 symmetric entries, b = a2 d (complex a2).
+BIELCC_D void acc_sym6(float (&t)[6][2], float a2r, float a2i, float dx, float dy, float dz) {
+    const float bx_r = a2r * dx, bx_i = a2i * dx, by_r = a2r * dy, by_i = a2i * dy, bz_r = a2r * dz, bz_i = a2i * dz;
     t[0][0] = fmaf(bx_r, dx, t[0][0]);
     t[0][1] = fmaf(bx_i, dx, t[0][1]);
     t[1][0] = fmaf(bx_r, dy, t[1][0]);
@@ -315,6 +274,75 @@ BIELCC_D void far_node_f32_K(float& a1r, float& a1i, float (&t)[6][2], float Xx,
     t[4][1] = fmaf(by_i, dz, t[4][1]);
     t[5][0] = fmaf(bz_r, dz, t[5][0]);
     t[5][1] = fmaf(bz_i, dz, t[5][1]);
+}
+
+// One far node, FP32 (E and H moments). Real k leaves (S, T/3) in (a1, t):
+// the caller runs finish_real_k once the cell's nodes are summed.
+template <bool CK, int MODE>
+BIELCC_D void far_node_f32(Moments<float>& m, float Xx, float Xy, float Xz, float r0, float r0sq, float r0k, float4 nd,
+                           const KF32& kf) {
+    float r, er, ei, dx, dy, dz;
+    const float ir = far_head_f32<CK, MODE>(Xx, Xy, Xz, r0, r0sq, r0k, nd, kf, r, er, ei, dx, dy, dz);
+    const float ir2 = ir * ir, ir3 = ir2 * ir;
+    if (!CK) {
+        const float beta = kf.kr * ir2;
+        const float ear = fmaf(ei, beta, er * ir3), eai = fmaf(-er, beta, ei * ir3);  // e alpha
+        m.a1r += ear;  // S
+        m.a1i += eai;
+        const float u3 = kf.k2r3 * ir3;                                               // k^2 / (3 r^3)
+        const float a2r = fmaf(ear, ir2, -er * u3), a2i = fmaf(eai, ir2, -ei * u3);  // e (alpha - u/3) / r^2
+        acc_sym6(m.t, a2r, a2i, dx, dy, dz);
+        m.g[0][0] = fmaf(-ear, dx, m.g[0][0]);
+        m.g[0][1] = fmaf(-eai, dx, m.g[0][1]);
+        m.g[1][0] = fmaf(-ear, dy, m.g[1][0]);
+        m.g[1][1] = fmaf(-eai, dy, m.g[1][1]);
+        m.g[2][0] = fmaf(-ear, dz, m.g[2][0]);
+        m.g[2][1] = fmaf(-eai, dz, m.g[2][1]);
+        return;
+    }
+    const float f1r = kf.k2r * ir - ir3 - kf.ki * ir2;
+    const float f1i = kf.kr * ir2 + kf.k2i * ir;
+    const float f2r = 3.f * ir3 + 3.f * kf.ki * ir2 - kf.k2r * ir;
+    const float f2i = -3.f * kf.kr * ir2 - kf.k2i * ir;
+    m.a1r = fmaf(er, f1r, fmaf(-ei, f1i, m.a1r));
+    m.a1i = fmaf(er, f1i, fmaf(ei, f1r, m.a1i));
+    const float a2r = (er * f2r - ei * f2i) * ir2, a2i = (er * f2i + ei * f2r) * ir2;
+    acc_sym6(m.t, a2r, a2i, dx, dy, dz);
+    const float ur = -kf.ki * r - 1.f, ui = kf.kr * r;
+    const float gr = (er * ur - ei * ui) * ir3, gi = (er * ui + ei * ur) * ir3;
+    m.g[0][0] = fmaf(gr, dx, m.g[0][0]);
+    m.g[0][1] = fmaf(gi, dx, m.g[0][1]);
+    m.g[1][0] = fmaf(gr, dy, m.g[1][0]);
+    m.g[1][1] = fmaf(gi, dy, m.g[1][1]);
+    m.g[2][0] = fmaf(gr, dz, m.g[2][0]);
+    m.g[2][1] = fmaf(gi, dz, m.g[2][1]);
+}
+
+// The K moments only (A1, T; no grad F) of one far node, FP32: the node
+// arithmetic of far_node_f32 for the collocation matrix, whose entries need
+// K_RotRot_Far alone. Real k leaves (S, T/3) as far_node_f32 does.
+template <bool CK, int MODE>
+BIELCC_D void far_node_f32_K(float& a1r, float& a1i, float (&t)[6][2], float Xx, float Xy, float Xz, float r0,
+                             float r0sq, float r0k, float4 nd, const KF32& kf) {
+    float r, er, ei, dx, dy, dz;
+    const float ir = far_head_f32<CK, MODE>(Xx, Xy, Xz, r0, r0sq, r0k, nd, kf, r, er, ei, dx, dy, dz);
+    const float ir2 = ir * ir, ir3 = ir2 * ir;
+    if (!CK) {
+        const float beta = kf.kr * ir2;
+        const float ear = fmaf(ei, beta, er * ir3), eai = fmaf(-er, beta, ei * ir3);
+        a1r += ear;
+        a1i += eai;
+        const float u3 = kf.k2r3 * ir3;
+        acc_sym6(t, fmaf(ear, ir2, -er * u3), fmaf(eai, ir2, -ei * u3), dx, dy, dz);
+        return;
+    }
+    const float f1r = kf.k2r * ir - ir3 - kf.ki * ir2;
+    const float f1i = kf.kr * ir2 + kf.k2i * ir;
+    const float f2r = 3.f * ir3 + 3.f * kf.ki * ir2 - kf.k2r * ir;
+    const float f2i = -3.f * kf.kr * ir2 - kf.k2i * ir;
+    a1r = fmaf(er, f1r, fmaf(-ei, f1i, a1r));
+    a1i = fmaf(er, f1i, fmaf(ei, f1r, a1i));
+    acc_sym6(t, (er * f2r - ei * f2i) * ir2, (er * f2i + ei * f2r) * ir2, dx, dy, dz);
 }
 
 }  // namespace bielcc_gpu

@@ -143,7 +143,8 @@ __global__ void __launch_bounds__(kFarThreads) far_kernel(FarArgs a) {
     bool far = false, zeroR = false;
     unsigned nbits = 0;  // near bits of the current 32-cell word
     // mixed-form per-pair state
-    float Xf[3] = {0.f, 0.f, 0.f}, r0f = 0.f, r0sq = 0.f;
+    float Xf[3] = {0.f, 0.f, 0.f}, r0f = 0.f, r0sq = 0.f, r0k = 0.f;
+    const KF32 kf = KF32::make(a.k.re, a.k.im);
     double P0r = 1.0, P0i = 0.0, r0d = 0.0;
     int mode = 0;
     bool split64 = false;
@@ -218,6 +219,7 @@ __global__ void __launch_bounds__(kFarThreads) far_kernel(FarArgs a) {
                         Xf[2] = (float)(x[2] - ci.z);
                         r0f = (float)d;
                         r0sq = (float)(d * d);
+                        r0k = r0f * kf.ikr;
                         double s, c;
                         sincos(a.k.re * d, &s, &c);
                         if (CK) {
@@ -233,11 +235,9 @@ __global__ void __launch_bounds__(kFarThreads) far_kernel(FarArgs a) {
                 if (far) {
                     const NodeT* nd = s_nodes + cc * kc;
                     if constexpr (MIXED) {
-                        const float kr_ = (float)a.k.re, ki_ = (float)a.k.im;
-                        const float k2rf = (float)k2r, k2if = (float)k2i;
 #define BIELCC_NODE_LOOP(MODE_)                                                                        \
     _Pragma("unroll 4") for (int i = 0; i < kc; i++)                                                    \
-        far_node_f32<CK, MODE_>(m, Xf[0], Xf[1], Xf[2], r0f, r0sq, nd[i], kr_, ki_, k2rf, k2if);
+        far_node_f32<CK, MODE_>(m, Xf[0], Xf[1], Xf[2], r0f, r0sq, r0k, nd[i], kf);
                         switch (mode) {
                             case 0: BIELCC_NODE_LOOP(0) break;
                             case 1: BIELCC_NODE_LOOP(1) break;
@@ -265,6 +265,7 @@ __global__ void __launch_bounds__(kFarThreads) far_kernel(FarArgs a) {
                     }
                 }
                 if (k0 + kc == nn && far) {
+                    if (!CK) m.finish_real_k();
                     if constexpr (MIXED) contract<NRHS, float>(m, (float)P0r, (float)P0i, s_j[cc], zeroR, acc);
                     else contract<NRHS, double>(m, P0r, P0i, s_j[cc], zeroR, acc);
                 }

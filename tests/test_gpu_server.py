@@ -188,3 +188,38 @@ def test_server_outputs_equal_the_batched_call(gctx):
             assert np.array_equal(o32["E"], E.astype(np.complex64)) and np.array_equal(o32["H"], H.astype(np.complex64))
     finally:
         sv.close()
+
+
+def test_server_concurrent_clients(gctx):
+    """Four client threads submit and wait at the same time (host threads of
+    one process, ctypes releasing the GIL); every result equals the same
+    request served alone."""
+    import threading
+
+    specs = _specs(gctx, 7)
+    sv = gpu.Server(gctx, n_slots=3, precision="mixed")
+    try:
+        alone = [sv.wait(_submit(sv, sp))[2] for sp in specs]
+        errors = []
+
+        def client(c):
+            try:
+                for rep in range(12):
+                    i = (c + rep) % len(specs)
+                    st, _, out = sv.wait(_submit(sv, specs[i]), timeout=120.0)
+                    if st != 0 or not (np.array_equal(out["E"], alone[i]["E"]) and
+                                       np.array_equal(out["H"], alone[i]["H"])):
+                        errors.append((c, rep, st))
+            except Exception as e:  # noqa: BLE001 - reported below
+                errors.append((c, repr(e)))
+
+        threads = [threading.Thread(target=client, args=(c,)) for c in range(4)]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join(timeout=300)
+        assert not errors, errors
+        s = sv.stats()
+        assert s["failed"] == 0 and s["completed"] == len(specs) + 48 and s["bytes_reserved"] == 0
+    finally:
+        sv.close()
