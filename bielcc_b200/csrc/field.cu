@@ -5,7 +5,9 @@
 // Pipeline (one stream, deterministic summation order):
 //   1. far kernel   — one observation point per thread, cell node tiles staged
 //                     in shared memory with 128-bit loads, cells split across
-//                     gridDim.y; far cells only (near cells skipped). Per cell
+//                     gridDim.y (the split count is chosen per launch so that
+//                     the last wave of CTAs fills the GPU: choose_far_splits);
+//                     far cells only (near cells skipped). Per cell
 //                     the J-independent moments A1 = sum w e f1,
 //                     T = sum w e f2 d^d^T, G = sum w grad F are accumulated and
 //                     contracted with each right-hand side once per cell:
@@ -26,7 +28,10 @@
 //   4. finalize     — per (point, RHS): far partials over splits (in order) +
 //                     near pairs (in cell order), x mult, + incident field.
 #include <algorithm>
+#include <atomic>
+#include <queue>
 #include <type_traits>
+#include <vector>
 
 #include "farnode.cuh"
 #include "internal.h"
@@ -470,17 +475,6 @@ __global__ void finalize_kernel(FinalArgs a) {
 }
 
 // ---------------------------------------------------------------- host launchers
-static int resident_far_ctas() {
-    static int cached = 0;
-    if (cached) return cached;
-    int dev = 0, sms = 148, per = 4;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, far_kernel<1, false, false>, kFarThreads, 0);
-    cached = std::max(1, sms * std::max(1, per));
-    return cached;
-}
-
 static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 static size_t mask_words(int n_cells) { return (size_t)(n_cells + 31) / 32; }
 // Cells per split rounded up to a multiple of 32 (one near-mask word).
@@ -489,17 +483,90 @@ static int round_cells_per_split(int n_cells, int splits) {
     return (cps + 31) / 32 * 32;
 }
 
+// Resident CTAs (whole GPU) of the far-kernel variant a launch starts with:
+// NRHS 4 / 2 / 1 (the first RHS chunk), real / complex k, FP64 / mixed, or
+// the adaptive kernel.
+static int far_slots(int n_rhs, bool ck, bool mixed, bool adaptive) {
+    static std::atomic<int> cache[2][2][3][2];
+    const int ri = n_rhs >= 4 ? 0 : (n_rhs >= 2 ? 1 : 2);
+    std::atomic<int>& c = cache[adaptive][ck][ri][mixed];
+    int v = c.load(std::memory_order_relaxed);
+    if (v) return v;
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const void* fn;
+    if (adaptive) fn = (const void*)far_adaptive_kernel;
+#define BIELCC_FK(R, C, M) (const void*)far_kernel<R, C, M>
+    else if (ri == 0) fn = ck ? (mixed ? BIELCC_FK(4, true, true) : BIELCC_FK(4, true, false))
+                              : (mixed ? BIELCC_FK(4, false, true) : BIELCC_FK(4, false, false));
+    else if (ri == 1) fn = ck ? (mixed ? BIELCC_FK(2, true, true) : BIELCC_FK(2, true, false))
+                              : (mixed ? BIELCC_FK(2, false, true) : BIELCC_FK(2, false, false));
+    else fn = ck ? (mixed ? BIELCC_FK(1, true, true) : BIELCC_FK(1, true, false))
+                 : (mixed ? BIELCC_FK(1, false, true) : BIELCC_FK(1, false, false));
+#undef BIELCC_FK
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, kFarThreads, 0);
+    v = std::max(1, sms * std::max(1, per));
+    c.store(v, std::memory_order_relaxed);
+    return v;
+}
+
+// Slot utilisation of a (tiles x splits) far grid on `slots` resident CTAs.
+// CTAs start in block order (tiles fastest) and run for a time proportional
+// to their cell count, so the grid is full waves of full-split CTAs, then a
+// tail: the remaining full-split CTAs and the CTAs of the last, shorter split,
+// each taking the earliest free slot.
+static double far_grid_utilisation(int tiles, int splits, int cps, int n_cells, int slots) {
+    const long long full = (long long)tiles * (splits - 1);
+    const long long fw = full / slots, r = full % slots;
+    const long long t0 = fw * cps, last = n_cells - (long long)(splits - 1) * cps;
+    // slots free at t0 (slots - r of them) and at t0 + cps (r of them)
+    std::priority_queue<long long, std::vector<long long>, std::greater<long long>> q;
+    for (long long i = 0; i < slots; i++) q.push(i < r ? t0 + cps : t0);
+    long long end = r ? t0 + cps : t0;
+    for (int t = 0; t < tiles; t++) {
+        const long long f = q.top() + last;
+        q.pop();
+        q.push(f);
+        end = std::max(end, f);
+    }
+    return (double)tiles * n_cells / ((double)slots * (double)end);
+}
+
+// Cell splits of the far grid: at least one full wave of CTAs, at most eight,
+// 32 cells per split at least and the partial sums within 256 MB; the count
+// with the highest slot utilisation wins (the fewest splits within 0.5 %).
+static int choose_far_splits(int tiles, int n_cells, int slots, size_t partial_bytes_per_split) {
+    if (tiles <= 0 || n_cells <= 32) return 1;
+    const int by_cells = std::max(1, n_cells / 32);
+    const int by_bytes = (int)std::max<size_t>(1, ((size_t)256 << 20) / std::max<size_t>(1, partial_bytes_per_split));
+    const int cap = std::min(by_cells, by_bytes);
+    const int lo = std::min(cap, std::max(1, (slots + tiles - 1) / tiles));
+    const int hi = std::min(cap, 8 * lo);
+    int best = 0;
+    double best_u = -1.0;
+    for (int s = lo; s <= hi; s++) {
+        const int cps = round_cells_per_split(n_cells, s);
+        const int sp = (n_cells + cps - 1) / cps;
+        if (sp != s) continue;  // the same grid as a smaller count
+        const double u = far_grid_utilisation(tiles, sp, cps, n_cells, slots);
+        if (u > best_u + 0.005) {
+            best_u = u;
+            best = sp;
+        }
+    }
+    return best > 0 ? best : (n_cells + round_cells_per_split(n_cells, lo) - 1) / round_cells_per_split(n_cells, lo);
+}
+
 size_t field_ws_base_bytes(const FieldLaunch& f, int* splits_out) {
-    int tiles = (f.n_pts + kFarThreads - 1) / kFarThreads;
-    int N = f.mesh->n_cells;
-    int target = 2 * resident_far_ctas();
-    int splits = std::max(1, (target + tiles - 1) / std::max(1, tiles));
-    splits = std::min(splits, std::max(1, N / 8));
-    int cps = round_cells_per_split(N, splits);
-    splits = (N + cps - 1) / cps;
+    const int tiles = (f.n_pts + kFarThreads - 1) / kFarThreads;
+    const int N = f.mesh->n_cells;
+    const size_t P = f.n_pts;
+    const size_t per_split = (size_t)f.n_rhs * 12 * P * sizeof(double);
+    const int slots = far_slots(f.n_rhs, f.k.im != 0.0, f.precision == 1, f.np.p_max > 1);
+    const int splits = choose_far_splits(tiles, N, slots, per_split);
     *splits_out = splits;
-    size_t P = f.n_pts;
-    return align256((size_t)splits * f.n_rhs * 12 * P * sizeof(double)) + 2 * align256((P + 1) * sizeof(long long)) +
+    return align256((size_t)splits * per_split) + 2 * align256((P + 1) * sizeof(long long)) +
            align256(sizeof(long long)) + align256(mask_words(N) * P * sizeof(unsigned));
 }
 
