@@ -11,9 +11,11 @@
 //        M = -sum_e ks_e nu_e^T from the unsmoothed K0 (K0.h:36-86).
 // Every entry is written exactly once (far kernel skips near pairs).
 #include <algorithm>
+#include <atomic>
 #include <type_traits>
 
 #include "farnode.cuh"
+#include "grid.h"
 #include "internal.h"
 #include "ops.cuh"
 #include "scan.cuh"
@@ -99,6 +101,7 @@ template <bool CK, bool MIXED>
 __global__ void __launch_bounds__(kAsmThreads) assemble_far_kernel(AsmArgs a) {
     using NodeT = typename std::conditional<MIXED, float4, double4>::type;
     __shared__ __align__(16) NodeT s_nodes[kAsmStageNodes];
+    __shared__ float s_yy[MIXED ? kAsmStageNodes : 1];  // |y - centre|^2 of the staged nodes (mixed form)
     __shared__ CellGeo s_geo[kAsmMaxCells];
     __shared__ float s_rho[kAsmMaxCells];
 
@@ -118,7 +121,7 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_far_kernel(AsmArgs a) {
     using F = typename std::conditional<MIXED, float, double>::type;
     F a1r = 0, a1i = 0, t[6][2];
     bool far = false;
-    float Xf[3] = {0.f, 0.f, 0.f}, r0f = 0.f, r0sq = 0.f, r0k = 0.f;
+    PairF32 pf{};
     const KF32 kf = KF32::make(a.k.re, a.k.im);
     double P0r = 1., P0i = 0.;
     int mode = 0;  // phase polynomial of the current cell (farnode.cuh phase_mode)
@@ -136,7 +139,9 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_far_kernel(AsmArgs a) {
                 const float4* src = a.nodes32 + (size_t)c0 * nn + k0;
                 for (int q = threadIdx.x; q < tot; q += kAsmThreads) {
                     int cc = q / kc, kk = q - cc * kc;
-                    s_nodes[q] = __ldg(src + (size_t)cc * nn + kk);
+                    const float4 v = __ldg(src + (size_t)cc * nn + kk);
+                    s_nodes[q] = v;
+                    s_yy[q] = node_yy(v);
                 }
             } else {
                 const double2* src = reinterpret_cast<const double2*>(a.nodes64 + (size_t)c0 * nn + k0);
@@ -182,12 +187,7 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_far_kernel(AsmArgs a) {
                         }
                     }
                     if (MIXED && far) {
-                        Xf[0] = (float)(x[0] - gj.c[0]);
-                        Xf[1] = (float)(x[1] - gj.c[1]);
-                        Xf[2] = (float)(x[2] - gj.c[2]);
-                        r0f = (float)d;
-                        r0sq = (float)(d * d);
-                        r0k = r0f * kf.ikr;
+                        pf.set(x, gj.c, d, kf);
                         double sn, cs;
                         sincos(a.k.re * d, &sn, &cs);
                         if (CK) {
@@ -203,9 +203,10 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_far_kernel(AsmArgs a) {
                 if (far) {
                     const NodeT* nd = s_nodes + cc * kc;
                     if constexpr (MIXED) {
-#define BIELCC_ASM_LOOP(MODE_)                                                                         \
-    _Pragma("unroll 4") for (int q = 0; q < kc; q++)                                                    \
-        far_node_f32_K<CK, MODE_>(a1r, a1i, t, Xf[0], Xf[1], Xf[2], r0f, r0sq, r0k, nd[q], kf);
+                        const float* yy = s_yy + cc * kc;
+#define BIELCC_ASM_LOOP(MODE_)         \
+    _Pragma("unroll 4") for (int q = 0; q < kc; q++) \
+        far_node_f32_K<CK, MODE_>(a1r, a1i, t, pf, nd[q], yy[q], kf);
                         switch (mode) {
                             case 0: BIELCC_ASM_LOOP(0) break;
                             case 1: BIELCC_ASM_LOOP(1) break;
@@ -427,6 +428,26 @@ static AsmArgs make_args(const AssembleLaunch& a) {
     return g;
 }
 
+// Resident CTAs (whole GPU) of the far assembly kernel variant.
+static int asm_slots(bool ck, bool mixed, bool adaptive) {
+    static std::atomic<int> cache[2][2][2];
+    std::atomic<int>& c = cache[adaptive][ck][mixed];
+    int v = c.load(std::memory_order_relaxed);
+    if (v) return v;
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const void* fn = adaptive ? (const void*)assemble_far_adaptive_kernel
+                              : (ck ? (mixed ? (const void*)assemble_far_kernel<true, true>
+                                             : (const void*)assemble_far_kernel<true, false>)
+                                    : (mixed ? (const void*)assemble_far_kernel<false, true>
+                                             : (const void*)assemble_far_kernel<false, false>));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, kAsmThreads, 0);
+    v = std::max(1, sms * std::max(1, per));
+    c.store(v, std::memory_order_relaxed);
+    return v;
+}
+
 cudaError_t assemble_stage1(const AssembleLaunch& a, void* ws, long long* d_total, cudaStream_t s) {
     const MeshDev& m = *a.mesh;
     const int N = m.n_cells;
@@ -437,14 +458,10 @@ cudaError_t assemble_stage1(const AssembleLaunch& a, void* ws, long long* d_tota
     AsmArgs g = make_args(a);
     g.mask = uses_mask(a) ? mask : nullptr;
     int tiles = (N + kAsmThreads - 1) / kAsmThreads;
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    int splits = std::max(1, std::min((8 * sms + tiles - 1) / tiles, std::max(1, N / 16)));
-    // column splits in whole 32-column words, so every mask word has one writer
-    g.cols_per_split = ((N + splits - 1) / splits + 31) / 32 * 32;
-    splits = (N + g.cols_per_split - 1) / g.cols_per_split;
     bool ck = a.k.im != 0.;
+    // column splits in whole 32-column words, so every mask word has one writer
+    int splits = choose_cell_splits(tiles, N, asm_slots(ck, a.precision == 1, a.np.p_max > 1), N);
+    g.cols_per_split = round_cells_per_split(N, splits);
     dim3 grid(tiles, splits);
     if (a.np.p_max > 1) {
         DNP np{a.np.eps, a.np.rs, a.np.rs_seg, a.np.analytic_calc, a.np.n_start, a.np.n_start_seg, a.np.p_max,

@@ -56,8 +56,9 @@ struct BatchCfg {
     // currents per (cell, RHS, component): FP32 (re, im, im, re) for the packed
     // contraction, FP64 (re, im)
     static constexpr int JW = MIXED ? 4 : 2;
+    static constexpr size_t YY = MIXED ? NODES : 0;  // |y - centre|^2 of the staged nodes (mixed form)
     static constexpr size_t smem_bytes() {
-        return sizeof(NodeT) * NODES + sizeof(F) * CH * 20 * kBP + sizeof(F) * JW * CH * kSP * 3 +
+        return sizeof(NodeT) * NODES + sizeof(float) * YY + sizeof(F) * CH * 20 * kBP + sizeof(F) * JW * CH * kSP * 3 +
                sizeof(double4) * CH + sizeof(double) * CH + CH * kBP + 64;
     }
 };
@@ -156,16 +157,18 @@ BIELCC_D void contract_packed_cell(const float* m, const float4* __restrict__ sj
 // CK (complex k) is a property of the job, so every item of a job takes the
 // same code path whatever else is in the batch.
 template <bool MIXED, bool CK>
-BIELCC_D void batch_moments(const typename BatchCfg<MIXED>::NodeT* nd, int nn, const double* x, const double4& ci,
-                            double d, double rho, cplx k, double k2r, double k2i,
+BIELCC_D void batch_moments(const typename BatchCfg<MIXED>::NodeT* nd, const float* yy, int nn, const double* x,
+                            const double4& ci, double d, double rho, cplx k, double k2r, double k2i,
                             typename BatchCfg<MIXED>::F* mom) {
     using F = typename BatchCfg<MIXED>::F;
     double P0r = 1.0, P0i = 0.0;
     Moments<F> m;
     m.zero();
     if constexpr (MIXED) {
-        const float Xx = (float)(x[0] - ci.x), Xy = (float)(x[1] - ci.y), Xz = (float)(x[2] - ci.z);
-        const float r0f = (float)d, r0sq = (float)(d * d);
+        const KF32 kf = KF32::make(k.re, k.im);
+        const double cen[3] = {ci.x, ci.y, ci.z};
+        PairF32 pf;
+        pf.set(x, cen, d, kf);
         double sn, cs;
         sincos(k.re * d, &sn, &cs);
         if (CK) {
@@ -175,12 +178,9 @@ BIELCC_D void batch_moments(const typename BatchCfg<MIXED>::NodeT* nd, int nn, c
         }
         P0r = cs;
         P0i = sn;
-        const KF32 kf = KF32::make(k.re, k.im);
-        const float r0k = r0f * kf.ikr;
         const int mode = phase_mode((float)fabs(k.re) * (float)rho);
-#define BIELCC_BNODE(MODE_)                                                                            \
-    _Pragma("unroll 4") for (int i = 0; i < nn; i++)                                                    \
-        far_node_f32<CK, MODE_>(m, Xx, Xy, Xz, r0f, r0sq, r0k, nd[i], kf);
+#define BIELCC_BNODE(MODE_) \
+    _Pragma("unroll 4") for (int i = 0; i < nn; i++) far_node_f32<CK, MODE_>(m, pf, nd[i], yy[i], kf);
         switch (mode) {
             case 0: BIELCC_BNODE(0) break;
             case 1: BIELCC_BNODE(1) break;
@@ -236,7 +236,8 @@ __global__ void __launch_bounds__(kBT, MIXED ? BIELCC_BATCH_MINB : 2) batch_far_
     using NodeT = typename C::NodeT;
     extern __shared__ __align__(16) unsigned char smem[];
     NodeT* s_nodes = (NodeT*)smem;
-    F* s_mom = (F*)(s_nodes + C::NODES);                 // [CH][20][kBP]
+    float* s_yy = (float*)(s_nodes + C::NODES);          // [NODES] (mixed form only)
+    F* s_mom = (F*)(s_yy + C::YY);                       // [CH][20][kBP]
     F* s_j = s_mom + C::CH * 20 * kBP;                   // [CH][kSP][3][JW]
     double4* s_cell = (double4*)(s_j + C::CH * kSP * 3 * C::JW);  // centre, diam
     double* s_rho = (double*)(s_cell + C::CH);
@@ -275,7 +276,11 @@ __global__ void __launch_bounds__(kBT, MIXED ? BIELCC_BATCH_MINB : 2) batch_far_
                 // stage node tables, cell rows and the chunk's currents
                 if constexpr (MIXED) {
                     const float4* src = jb.nodes32 + (size_t)c0 * nn;
-                    for (int i = threadIdx.x; i < nc * nn; i += kBT) s_nodes[i] = __ldg(src + i);
+                    for (int i = threadIdx.x; i < nc * nn; i += kBT) {
+                        const float4 v = __ldg(src + i);
+                        s_nodes[i] = v;
+                        s_yy[i] = node_yy(v);
+                    }
                 } else {
                     const double2* src = reinterpret_cast<const double2*>(jb.nodes64 + (size_t)c0 * nn);
                     double2* dst = reinterpret_cast<double2*>(s_nodes);
@@ -311,10 +316,11 @@ __global__ void __launch_bounds__(kBT, MIXED ? BIELCC_BATCH_MINB : 2) batch_far_
                     for (int q = 0; q < 20; q++) mom[q] = 0;
                     if (far) {
                         const NodeT* nd = s_nodes + cc * nn;
+                        const float* yy = s_yy + (MIXED ? cc * nn : 0);
                         if (k.im != 0.0)
-                            batch_moments<MIXED, true>(nd, nn, x, ci, d, s_rho[cc], k, k2r, k2i, mom);
+                            batch_moments<MIXED, true>(nd, yy, nn, x, ci, d, s_rho[cc], k, k2r, k2i, mom);
                         else
-                            batch_moments<MIXED, false>(nd, nn, x, ci, d, s_rho[cc], k, k2r, k2i, mom);
+                            batch_moments<MIXED, false>(nd, yy, nn, x, ci, d, s_rho[cc], k, k2r, k2i, mom);
                     }
 #pragma unroll
                     for (int q = 0; q < 20; q++) s_mom[(cc * 20 + q) * kBP + lane] = mom[q];

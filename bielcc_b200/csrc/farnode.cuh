@@ -231,28 +231,45 @@ BIELCC_HD int phase_mode(float th) {
     return th <= 0.25f ? 0 : (th <= 1.f ? 1 : (th <= 2.f ? 2 : (th <= 4.f ? 3 : 4)));
 }
 
-// Shared head of the FP32 far node, relative to the cell centre: X = x - centre
-// (FP32), node delta = y - centre, r0 = |X| (FP64 rounded), r0k = r0 / Re k.
+// Per-pair FP32 state of the mixed far node, relative to the cell centre:
+// X = x - centre, X2 = -2 X, r0 = |X| (FP64 rounded), r0sq = r0^2, r0k = r0 / Re k.
+struct PairF32 {
+    float X[3], X2[3], r0, r0sq, r0k;
+    BIELCC_D void set(const double* x, const double* centre, double d, const KF32& kf) {
+        for (int g = 0; g < 3; g++) {
+            X[g] = (float)(x[g] - centre[g]);
+            X2[g] = -2.f * X[g];
+        }
+        r0 = (float)d;
+        r0sq = (float)(d * d);
+        r0k = r0 * kf.ikr;
+    }
+};
+
+// |y - centre|^2 of a staged node (computed once per node and CTA).
+BIELCC_D float node_yy(float4 nd) { return fmaf(nd.x, nd.x, fmaf(nd.y, nd.y, nd.z * nd.z)); }
+
+// Shared head of the FP32 far node: nd = (y - centre, w), yy = |y - centre|^2.
+// q = |x - y|^2 - r0^2 = yy - 2 (y - centre).X carries no cancellation.
 // Returns 1/r and sets r, the weighted phase factor e = w e^{ik(r - r0)} and d = x - y.
 template <bool CK, int MODE>
-BIELCC_D float far_head_f32(float Xx, float Xy, float Xz, float r0, float r0sq, float r0k, float4 nd, const KF32& kf,
-                            float& r_out, float& er, float& ei, float& dx, float& dy, float& dz) {
-    const float tx = fmaf(-2.f, Xx, nd.x), ty = fmaf(-2.f, Xy, nd.y), tz = fmaf(-2.f, Xz, nd.z);
-    const float q = fmaf(nd.x, tx, fmaf(nd.y, ty, nd.z * tz));  // |x-y|^2 - r0^2
-    const float r2 = r0sq + q;
+BIELCC_D float far_head_f32(const PairF32& p, float4 nd, float yy, const KF32& kf, float& r_out, float& er, float& ei,
+                            float& dx, float& dy, float& dz) {
+    const float q = fmaf(nd.x, p.X2[0], fmaf(nd.y, p.X2[1], fmaf(nd.z, p.X2[2], yy)));
+    const float r2 = p.r0sq + q;
     const float ir = rsqrtf(r2);
     const float r = r2 * ir;
     float s, c, w = nd.w;
     if (CK) {
-        const float dr = __fdividef(q, r + r0);  // r - r0 without cancellation
+        const float dr = __fdividef(q, r + p.r0);  // r - r0 without cancellation
         phase_f32<MODE>(kf.kr * dr, &s, &c);
         w *= __expf(-kf.ki * dr);
     } else {
-        phase_f32<MODE>(__fdividef(q, fmaf(r, kf.ikr, r0k)), &s, &c);  // k (r - r0)
+        phase_f32<MODE>(__fdividef(q, fmaf(r, kf.ikr, p.r0k)), &s, &c);  // k (r - r0)
     }
-    dx = Xx - nd.x;
-    dy = Xy - nd.y;
-    dz = Xz - nd.z;
+    dx = p.X[0] - nd.x;
+    dy = p.X[1] - nd.y;
+    dz = p.X[2] - nd.z;
     er = w * c;
     ei = w * s;
     r_out = r;
@@ -279,10 +296,9 @@ BIELCC_D void acc_sym6(float (&t)[6][2], float a2r, float a2i, float dx, float d
 // One far node, FP32 (E and H moments). Real k leaves (S, T/3) in (a1, t):
 // the caller runs finish_real_k once the cell's nodes are summed.
 template <bool CK, int MODE>
-BIELCC_D void far_node_f32(Moments<float>& m, float Xx, float Xy, float Xz, float r0, float r0sq, float r0k, float4 nd,
-                           const KF32& kf) {
+BIELCC_D void far_node_f32(Moments<float>& m, const PairF32& p, float4 nd, float yy, const KF32& kf) {
     float r, er, ei, dx, dy, dz;
-    const float ir = far_head_f32<CK, MODE>(Xx, Xy, Xz, r0, r0sq, r0k, nd, kf, r, er, ei, dx, dy, dz);
+    const float ir = far_head_f32<CK, MODE>(p, nd, yy, kf, r, er, ei, dx, dy, dz);
     const float ir2 = ir * ir, ir3 = ir2 * ir;
     if (!CK) {
         const float beta = kf.kr * ir2;
@@ -322,10 +338,10 @@ BIELCC_D void far_node_f32(Moments<float>& m, float Xx, float Xy, float Xz, floa
 // arithmetic of far_node_f32 for the collocation matrix, whose entries need
 // K_RotRot_Far alone. Real k leaves (S, T/3) as far_node_f32 does.
 template <bool CK, int MODE>
-BIELCC_D void far_node_f32_K(float& a1r, float& a1i, float (&t)[6][2], float Xx, float Xy, float Xz, float r0,
-                             float r0sq, float r0k, float4 nd, const KF32& kf) {
+BIELCC_D void far_node_f32_K(float& a1r, float& a1i, float (&t)[6][2], const PairF32& p, float4 nd, float yy,
+                             const KF32& kf) {
     float r, er, ei, dx, dy, dz;
-    const float ir = far_head_f32<CK, MODE>(Xx, Xy, Xz, r0, r0sq, r0k, nd, kf, r, er, ei, dx, dy, dz);
+    const float ir = far_head_f32<CK, MODE>(p, nd, yy, kf, r, er, ei, dx, dy, dz);
     const float ir2 = ir * ir, ir3 = ir2 * ir;
     if (!CK) {
         const float beta = kf.kr * ir2;

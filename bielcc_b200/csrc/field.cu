@@ -6,7 +6,7 @@
 //   1. far kernel   — one observation point per thread, cell node tiles staged
 //                     in shared memory with 128-bit loads, cells split across
 //                     gridDim.y (the split count is chosen per launch so that
-//                     the last wave of CTAs fills the GPU: choose_far_splits);
+//                     the last wave of CTAs fills the GPU: grid.h);
 //                     far cells only (near cells skipped). Per cell
 //                     the J-independent moments A1 = sum w e f1,
 //                     T = sum w e f2 d^d^T, G = sum w grad F are accumulated and
@@ -29,11 +29,10 @@
 //                     near pairs (in cell order), x mult, + incident field.
 #include <algorithm>
 #include <atomic>
-#include <queue>
 #include <type_traits>
-#include <vector>
 
 #include "farnode.cuh"
+#include "grid.h"
 #include "internal.h"
 #include "ops.cuh"
 #include "scan.cuh"
@@ -119,6 +118,7 @@ template <int NRHS, bool CK, bool MIXED>
 __global__ void __launch_bounds__(kFarThreads) far_kernel(FarArgs a) {
     using NodeT = typename std::conditional<MIXED, float4, double4>::type;
     __shared__ __align__(16) NodeT s_nodes[kStageNodes];
+    __shared__ float s_yy[MIXED ? kStageNodes : 1];  // |y - centre|^2 of the staged nodes (mixed form)
     __shared__ double4 s_cell[kMaxStageCells];  // centre xyz, near threshold
     __shared__ cplx s_j[kMaxStageCells][NRHS][3];
     __shared__ float s_rho[kMaxStageCells];
@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(kFarThreads) far_kernel(FarArgs a) {
     bool far = false, zeroR = false;
     unsigned nbits = 0;  // near bits of the current 32-cell word
     // mixed-form per-pair state
-    float Xf[3] = {0.f, 0.f, 0.f}, r0f = 0.f, r0sq = 0.f, r0k = 0.f;
+    PairF32 pf{};
     const KF32 kf = KF32::make(a.k.re, a.k.im);
     double P0r = 1.0, P0i = 0.0, r0d = 0.0;
     int mode = 0;
@@ -166,7 +166,9 @@ __global__ void __launch_bounds__(kFarThreads) far_kernel(FarArgs a) {
                     const float4* src = a.nodes32 + (size_t)c0 * nn + k0;
                     for (int i = threadIdx.x; i < tot; i += kFarThreads) {
                         int cc = i / kc, kk = i - cc * kc;
-                        s_nodes[i] = __ldg(src + (size_t)cc * nn + kk);
+                        const float4 v = __ldg(src + (size_t)cc * nn + kk);
+                        s_nodes[i] = v;
+                        s_yy[i] = node_yy(v);
                     }
                 } else {
                     const double2* src = reinterpret_cast<const double2*>(a.nodes64 + (size_t)c0 * nn + k0);
@@ -219,12 +221,7 @@ __global__ void __launch_bounds__(kFarThreads) far_kernel(FarArgs a) {
                         }
                     }
                     if (MIXED && far) {  // per-pair FP64 set-up of the phase split
-                        Xf[0] = (float)(x[0] - ci.x);
-                        Xf[1] = (float)(x[1] - ci.y);
-                        Xf[2] = (float)(x[2] - ci.z);
-                        r0f = (float)d;
-                        r0sq = (float)(d * d);
-                        r0k = r0f * kf.ikr;
+                        pf.set(x, cen, d, kf);
                         double s, c;
                         sincos(a.k.re * d, &s, &c);
                         if (CK) {
@@ -240,9 +237,9 @@ __global__ void __launch_bounds__(kFarThreads) far_kernel(FarArgs a) {
                 if (far) {
                     const NodeT* nd = s_nodes + cc * kc;
                     if constexpr (MIXED) {
+                        const float* yy = s_yy + cc * kc;
 #define BIELCC_NODE_LOOP(MODE_)                                                                        \
-    _Pragma("unroll 4") for (int i = 0; i < kc; i++)                                                    \
-        far_node_f32<CK, MODE_>(m, Xf[0], Xf[1], Xf[2], r0f, r0sq, r0k, nd[i], kf);
+    _Pragma("unroll 4") for (int i = 0; i < kc; i++) far_node_f32<CK, MODE_>(m, pf, nd[i], yy[i], kf);
                         switch (mode) {
                             case 0: BIELCC_NODE_LOOP(0) break;
                             case 1: BIELCC_NODE_LOOP(1) break;
@@ -477,12 +474,6 @@ __global__ void finalize_kernel(FinalArgs a) {
 // ---------------------------------------------------------------- host launchers
 static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 static size_t mask_words(int n_cells) { return (size_t)(n_cells + 31) / 32; }
-// Cells per split rounded up to a multiple of 32 (one near-mask word).
-static int round_cells_per_split(int n_cells, int splits) {
-    int cps = (n_cells + splits - 1) / splits;
-    return (cps + 31) / 32 * 32;
-}
-
 // Resident CTAs (whole GPU) of the far-kernel variant a launch starts with:
 // NRHS 4 / 2 / 1 (the first RHS chunk), real / complex k, FP64 / mixed, or
 // the adaptive kernel.
@@ -511,60 +502,15 @@ static int far_slots(int n_rhs, bool ck, bool mixed, bool adaptive) {
     return v;
 }
 
-// Slot utilisation of a (tiles x splits) far grid on `slots` resident CTAs.
-// CTAs start in block order (tiles fastest) and run for a time proportional
-// to their cell count, so the grid is full waves of full-split CTAs, then a
-// tail: the remaining full-split CTAs and the CTAs of the last, shorter split,
-// each taking the earliest free slot.
-static double far_grid_utilisation(int tiles, int splits, int cps, int n_cells, int slots) {
-    const long long full = (long long)tiles * (splits - 1);
-    const long long fw = full / slots, r = full % slots;
-    const long long t0 = fw * cps, last = n_cells - (long long)(splits - 1) * cps;
-    // slots free at t0 (slots - r of them) and at t0 + cps (r of them)
-    std::priority_queue<long long, std::vector<long long>, std::greater<long long>> q;
-    for (long long i = 0; i < slots; i++) q.push(i < r ? t0 + cps : t0);
-    long long end = r ? t0 + cps : t0;
-    for (int t = 0; t < tiles; t++) {
-        const long long f = q.top() + last;
-        q.pop();
-        q.push(f);
-        end = std::max(end, f);
-    }
-    return (double)tiles * n_cells / ((double)slots * (double)end);
-}
-
-// Cell splits of the far grid: at least one full wave of CTAs, at most eight,
-// 32 cells per split at least and the partial sums within 256 MB; the count
-// with the highest slot utilisation wins (the fewest splits within 0.5 %).
-static int choose_far_splits(int tiles, int n_cells, int slots, size_t partial_bytes_per_split) {
-    if (tiles <= 0 || n_cells <= 32) return 1;
-    const int by_cells = std::max(1, n_cells / 32);
-    const int by_bytes = (int)std::max<size_t>(1, ((size_t)256 << 20) / std::max<size_t>(1, partial_bytes_per_split));
-    const int cap = std::min(by_cells, by_bytes);
-    const int lo = std::min(cap, std::max(1, (slots + tiles - 1) / tiles));
-    const int hi = std::min(cap, 8 * lo);
-    int best = 0;
-    double best_u = -1.0;
-    for (int s = lo; s <= hi; s++) {
-        const int cps = round_cells_per_split(n_cells, s);
-        const int sp = (n_cells + cps - 1) / cps;
-        if (sp != s) continue;  // the same grid as a smaller count
-        const double u = far_grid_utilisation(tiles, sp, cps, n_cells, slots);
-        if (u > best_u + 0.005) {
-            best_u = u;
-            best = sp;
-        }
-    }
-    return best > 0 ? best : (n_cells + round_cells_per_split(n_cells, lo) - 1) / round_cells_per_split(n_cells, lo);
-}
-
 size_t field_ws_base_bytes(const FieldLaunch& f, int* splits_out) {
     const int tiles = (f.n_pts + kFarThreads - 1) / kFarThreads;
     const int N = f.mesh->n_cells;
     const size_t P = f.n_pts;
     const size_t per_split = (size_t)f.n_rhs * 12 * P * sizeof(double);
     const int slots = far_slots(f.n_rhs, f.k.im != 0.0, f.precision == 1, f.np.p_max > 1);
-    const int splits = choose_far_splits(tiles, N, slots, per_split);
+    // partial sums within 256 MB
+    const int max_splits = (int)std::max<size_t>(1, ((size_t)256 << 20) / std::max<size_t>(1, per_split));
+    const int splits = choose_cell_splits(tiles, N, slots, max_splits);
     *splits_out = splits;
     return align256((size_t)splits * per_split) + 2 * align256((P + 1) * sizeof(long long)) +
            align256(sizeof(long long)) + align256(mask_words(N) * P * sizeof(unsigned));
