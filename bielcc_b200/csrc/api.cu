@@ -92,6 +92,12 @@ struct bielcc_ctx_s {
     DevBuf ws, pair_ws, io, scratch_small;
     DevBuf full;  // [j_E; j_M] and the 2S-RHS outputs of bielcc_field_EH_full
     long long* h_total = nullptr;  // pinned
+    // side stream and workspaces of the mixed form's FP64 error sample, which
+    // runs beside the main evaluation (bielcc_field_EH)
+    cudaStream_t side = nullptr;
+    cudaEvent_t side_in = nullptr;
+    DevBuf side_ws, side_pair_ws, side_io, side_scratch;
+    long long* h_side_total = nullptr;  // pinned
     unsigned long long* h_nonfinite = nullptr;
     // counters / timing (bielcc_ctx_stats)
     bool timing = false;
@@ -178,6 +184,20 @@ int ws_release(bielcc_ctx ctx, cudaStream_t s) {
     return BIELCC_OK;
 }
 
+// The workspaces one field evaluation uses: the context's shared set, or the
+// side set of the error sample.
+struct WsSet {
+    DevBuf* ws;
+    DevBuf* pair_ws;
+    DevBuf* scratch;
+    long long* h_total;  // pinned near-pair count
+    bool timed;          // far-kernel events into the context's stats
+};
+WsSet main_ws(bielcc_ctx ctx) { return {&ctx->ws, &ctx->pair_ws, &ctx->scratch_small, ctx->h_total, ctx->timing}; }
+WsSet side_ws(bielcc_ctx ctx) {
+    return {&ctx->side_ws, &ctx->side_pair_ws, &ctx->side_scratch, ctx->h_side_total, false};
+}
+
 struct FieldArgs {
     MeshDev* m;
     int n_rhs;
@@ -200,7 +220,7 @@ struct FieldArgs {
 // set (its work items over its resident CTAs). Returns false when the call is
 // left to the single-job path.
 int field_device_batched(bielcc_ctx ctx, const FieldArgs& a, cudaStream_t s, bielcc_report* rep,
-                         unsigned long long* d_nonfinite, bool* done) {
+                         unsigned long long* d_nonfinite, bool* done, const WsSet& w) {
     *done = false;
     if (a.n_rhs <= 4 || a.np.p_max > 1 || a.np.n_start > kBatchMaxNStart || a.n_pts == 0) return BIELCC_OK;
     TRY(ensure_tables(a.m, a.np.n_start, s));
@@ -234,17 +254,17 @@ int field_device_batched(bielcc_ctx ctx, const FieldArgs& a, cudaStream_t s, bie
     plan_batch(bp, std::vector<JobDev>{d}, a.np.n_start, a.precision == BIELCC_PREC_MIXED, ctx->batch_item_cost);
     const double busy = std::min(1.0, (double)bp.items.size() / std::max(1, bp.grid));
     if ((double)((a.n_rhs + 3) / 4) * busy <= 1.5) return BIELCC_OK;
-    TRY(ctx->ws.ensure(bp.ws_bytes));
+    TRY(w.ws->ensure(bp.ws_bytes));
     BatchDevPtrs dp;
     int l1 = 0, l2 = 0;
-    TRY_CUDA(batch_stage1(bp, ctx->ws.p, a.np.analytic_calc, a.np.n_start, a.k.im != 0., s, &dp, &l1));
-    TRY_CUDA(cudaMemcpyAsync(ctx->h_total, dp.total, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    TRY_CUDA(batch_stage1(bp, w.ws->p, a.np.analytic_calc, a.np.n_start, a.k.im != 0., s, &dp, &l1));
+    TRY_CUDA(cudaMemcpyAsync(w.h_total, dp.total, sizeof(long long), cudaMemcpyDeviceToHost, s));
     TRY_CUDA(cudaStreamSynchronize(s));
-    const long long n_near = *ctx->h_total;
-    if (n_near > 0) TRY(ctx->pair_ws.ensure(batch_pair_ws_bytes(n_near)));
+    const long long n_near = *w.h_total;
+    if (n_near > 0) TRY(w.pair_ws->ensure(batch_pair_ws_bytes(n_near)));
     DNP dn{a.np.eps, a.np.rs, a.np.rs_seg, a.np.analytic_calc, a.np.n_start, a.np.n_start_seg, a.np.p_max,
            a.np.p_max_seg};
-    TRY_CUDA(batch_stage2(bp, dp, n_near, ctx->pair_ws.p, dn, d_nonfinite, s, &l2));
+    TRY_CUDA(batch_stage2(bp, dp, n_near, w.pair_ws->p, dn, d_nonfinite, s, &l2));
     ctx->stats.kernel_launches += l1 + l2;
     ctx->stats.far_launches += 1;
     ctx->stats.far_pairs += ((long long)a.n_pts * a.m->n_cells - n_near) * a.n_rhs;
@@ -256,15 +276,24 @@ int field_device_batched(bielcc_ctx ctx, const FieldArgs& a, cudaStream_t s, bie
     return BIELCC_OK;
 }
 
-// Enqueues a field evaluation on device buffers; one short host wait for the
-// near-pair count (sizes the FP64 near workspace).
-int field_device(bielcc_ctx ctx, const FieldArgs& a, cudaStream_t s, bielcc_report* rep,
-                 unsigned long long* d_nonfinite) {
-    bool done = false;
-    TRY(field_device_batched(ctx, a, s, rep, d_nonfinite, &done));
-    if (done) return BIELCC_OK;
-    TRY(ensure_tables(a.m, a.np.n_start, s));
+// A single-job field evaluation between its two halves: stage 1 (far kernel,
+// near counting) is enqueued and the near-pair count is on its way to the host.
+struct FieldPending {
+    FieldArgs a;
     FieldLaunch f;
+    int splits = 1, l1 = 0, lf = 0;
+    bool batched = false;  // ran whole as a one-job batch
+};
+
+// Enqueues stage 1 of a field evaluation on device buffers (or the whole
+// evaluation, when it runs as a one-job batch).
+int field_begin(bielcc_ctx ctx, const FieldArgs& a, cudaStream_t s, bielcc_report* rep,
+                unsigned long long* d_nonfinite, const WsSet& w, FieldPending* p) {
+    p->a = a;
+    TRY(field_device_batched(ctx, a, s, rep, d_nonfinite, &p->batched, w));
+    if (p->batched) return BIELCC_OK;
+    TRY(ensure_tables(a.m, a.np.n_start, s));
+    FieldLaunch& f = p->f;
     f.mesh = a.m;
     f.pts = a.pts;
     f.n_pts = a.n_pts;
@@ -283,32 +312,50 @@ int field_device(bielcc_ctx ctx, const FieldArgs& a, cudaStream_t s, bielcc_repo
     f.add_H = a.inc ? a.inc->add_H : 0;
     f.E = a.E;
     f.H = a.H;
-    int splits = 1;
-    size_t base = field_ws_base_bytes(f, &splits);
-    TRY(ctx->ws.ensure(base));
-    TRY(ctx->scratch_small.ensure(256));
-    long long* d_total = (long long*)ctx->scratch_small.p;
-    int l1 = 0, l2 = 0, lf = 0;
-    TRY_CUDA(field_stage1(f, ctx->ws.p, splits, d_total, s, &l1, ctx->timing ? ctx->far_begin : nullptr,
-                          ctx->timing ? ctx->far_end : nullptr, &lf));
-    TRY_CUDA(cudaMemcpyAsync(ctx->h_total, d_total, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    size_t base = field_ws_base_bytes(f, &p->splits);
+    TRY(w.ws->ensure(base));
+    TRY(w.scratch->ensure(256));
+    long long* d_total = (long long*)w.scratch->p;
+    TRY_CUDA(field_stage1(f, w.ws->p, p->splits, d_total, s, &p->l1, w.timed ? ctx->far_begin : nullptr,
+                          w.timed ? ctx->far_end : nullptr, &p->lf));
+    TRY_CUDA(cudaMemcpyAsync(w.h_total, d_total, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    return BIELCC_OK;
+}
+
+// Waits for the near-pair count (sizes the FP64 near workspace) and enqueues
+// stage 2 (near pairs, finalize).
+int field_finish(bielcc_ctx ctx, FieldPending& p, cudaStream_t s, bielcc_report* rep,
+                 unsigned long long* d_nonfinite, const WsSet& w) {
+    if (p.batched) return BIELCC_OK;
+    const FieldArgs& a = p.a;
     TRY_CUDA(cudaStreamSynchronize(s));
-    long long n_near = *ctx->h_total;
-    if (ctx->timing && lf > 0) {
+    long long n_near = *w.h_total;
+    if (w.timed && p.lf > 0) {
         float ms = 0.f;
         TRY_CUDA(cudaEventElapsedTime(&ms, ctx->far_begin, ctx->far_end));
         ctx->stats.far_ms += ms;
     }
-    if (n_near > 0) TRY(ctx->pair_ws.ensure(field_pair_ws_bytes(n_near)));
-    TRY_CUDA(field_stage2(f, ctx->ws.p, splits, n_near, ctx->pair_ws.p, d_nonfinite, s, &l2));
-    ctx->stats.kernel_launches += l1 + l2;
-    ctx->stats.far_launches += lf;
+    int l2 = 0;
+    if (n_near > 0) TRY(w.pair_ws->ensure(field_pair_ws_bytes(n_near)));
+    TRY_CUDA(field_stage2(p.f, w.ws->p, p.splits, n_near, w.pair_ws->p, d_nonfinite, s, &l2));
+    ctx->stats.kernel_launches += p.l1 + l2;
+    ctx->stats.far_launches += p.lf;
     ctx->stats.far_pairs += ((long long)a.n_pts * a.m->n_cells - n_near) * a.n_rhs;
     if (rep) {
         rep->n_pairs = (int64_t)a.n_pts * a.m->n_cells;
         rep->n_near_pairs = n_near;
     }
     return BIELCC_OK;
+}
+
+// Enqueues a field evaluation on device buffers; one short host wait for the
+// near-pair count (sizes the FP64 near workspace).
+int field_device(bielcc_ctx ctx, const FieldArgs& a, cudaStream_t s, bielcc_report* rep,
+                 unsigned long long* d_nonfinite) {
+    const WsSet w = main_ws(ctx);
+    FieldPending p;
+    TRY(field_begin(ctx, a, s, rep, d_nonfinite, w, &p));
+    return field_finish(ctx, p, s, rep, d_nonfinite, w);
 }
 
 }  // namespace
@@ -346,7 +393,18 @@ int bielcc_ctx_create(int device, bielcc_ctx* out) {
     if (e == cudaSuccess) e = cudaMallocHost(&c->h_total, 64);
     if (e == cudaSuccess) e = cudaEventCreate(&c->far_begin);
     if (e == cudaSuccess) e = cudaEventCreate(&c->far_end);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->side_in, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaMallocHost(&c->h_side_total, 64);
     if (e != cudaSuccess) {
+        if (c->h_total) cudaFreeHost(c->h_total);
+        if (c->h_side_total) cudaFreeHost(c->h_side_total);
+        if (c->ws_done) cudaEventDestroy(c->ws_done);
+        if (c->far_begin) cudaEventDestroy(c->far_begin);
+        if (c->far_end) cudaEventDestroy(c->far_end);
+        if (c->side_in) cudaEventDestroy(c->side_in);
+        if (c->side) cudaStreamDestroy(c->side);
+        if (c->stream) cudaStreamDestroy(c->stream);
         delete c;
         return cuda_status(e, "context set-up", __LINE__);
     }
@@ -366,6 +424,13 @@ int bielcc_ctx_destroy(bielcc_ctx ctx) {
     ctx->io.release();
     ctx->scratch_small.release();
     ctx->full.release();
+    ctx->side_ws.release();
+    ctx->side_pair_ws.release();
+    ctx->side_io.release();
+    ctx->side_scratch.release();
+    if (ctx->h_side_total) cudaFreeHost(ctx->h_side_total);
+    if (ctx->side_in) cudaEventDestroy(ctx->side_in);
+    if (ctx->side) cudaStreamDestroy(ctx->side);
     if (ctx->h_total) cudaFreeHost(ctx->h_total);
     if (ctx->h_nonfinite) cudaFreeHost(ctx->h_nonfinite);
     if (ctx->ws_done) cudaEventDestroy(ctx->ws_done);
@@ -641,10 +706,46 @@ int bielcc_field_EH(bielcc_ctx ctx, bielcc_mesh mesh, int n_rhs, const double* J
     if (P) TRY_CUDA(cudaMemcpyAsync(dP, pts, bP, cudaMemcpyHostToDevice, s));
     TRY_CUDA(cudaMemsetAsync(d_nf, 0, sizeof(unsigned long long), s));
     FieldArgs a{m, n_rhs, dJ, mk(k_re, k_im), mk(mult_re, mult_im), inc, n, n_pts, dP, dE, dH, precision};
-    if (P) TRY(field_device(ctx, a, s, report, d_nf));
+    // Mixed form: its relative L2 error against the FP64 form on a sample of
+    // Q = min(P, 256) points spread over the set (two full point tiles),
+    // evaluated on the side stream beside the main evaluation.
+    const bool sample = report && precision == BIELCC_PREC_MIXED && P > 0;
+    const size_t Q = sample ? std::min<size_t>(P, 256) : 0;
+    std::vector<size_t> idx(Q);
+    for (size_t q = 0; q < Q; q++) idx[q] = q * P / Q;
+    const size_t bQ = Q * 3 * 8, bQo = S * Q * 3 * 16;
+    double *dQ = nullptr, *dEq = nullptr, *dHq = nullptr;
+    std::vector<double> e64(S * Q * 6), h64(S * Q * 6);
+    FieldPending pm, ps;
+    const WsSet wm = main_ws(ctx), wsd = side_ws(ctx);
+    std::vector<double> sp(Q * 3);
+    if (sample) {
+        for (size_t q = 0; q < Q; q++)
+            for (int g = 0; g < 3; g++) sp[3 * q + g] = pts[3 * idx[q] + g];
+        TRY(ctx->side_io.ensure(al(bQ) + 2 * al(bQo) + 256));
+        char* sio = (char*)ctx->side_io.p;
+        dQ = (double*)sio;
+        dEq = (double*)(sio + al(bQ));
+        dHq = (double*)(sio + al(bQ) + al(bQo));
+        TRY(ensure_tables(m, n.n_start, s));
+        TRY_CUDA(cudaEventRecord(ctx->side_in, s));  // currents and node tables on the device
+        TRY_CUDA(cudaStreamWaitEvent(ctx->side, ctx->side_in, 0));
+        TRY_CUDA(cudaMemcpyAsync(dQ, sp.data(), bQ, cudaMemcpyHostToDevice, ctx->side));
+    }
+    FieldArgs b{m, n_rhs, dJ, mk(k_re, k_im), mk(mult_re, mult_im), inc, n, (int)Q, dQ, dEq, H ? dHq : nullptr,
+                BIELCC_PREC_FP64};
+    if (P) TRY(field_begin(ctx, a, s, report, d_nf, wm, &pm));
+    if (sample) TRY(field_begin(ctx, b, ctx->side, nullptr, nullptr, wsd, &ps));
+    if (P) TRY(field_finish(ctx, pm, s, report, d_nf, wm));
     if (P) TRY_CUDA(cudaMemcpyAsync(E, dE, bO, cudaMemcpyDeviceToHost, s));
     if (P && H) TRY_CUDA(cudaMemcpyAsync(H, dH, bO, cudaMemcpyDeviceToHost, s));
     TRY_CUDA(cudaMemcpyAsync(ctx->h_nonfinite, d_nf, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    if (sample) {
+        TRY(field_finish(ctx, ps, ctx->side, nullptr, nullptr, wsd));
+        TRY_CUDA(cudaMemcpyAsync(e64.data(), dEq, bQo, cudaMemcpyDeviceToHost, ctx->side));
+        if (H) TRY_CUDA(cudaMemcpyAsync(h64.data(), dHq, bQo, cudaMemcpyDeviceToHost, ctx->side));
+        TRY_CUDA(cudaStreamSynchronize(ctx->side));
+    }
     TRY_CUDA(cudaStreamSynchronize(s));
     TRY(ws_release(ctx, s));
     int rc = BIELCC_OK;
@@ -654,34 +755,7 @@ int bielcc_field_EH(bielcc_ctx ctx, bielcc_mesh mesh, int n_rhs, const double* J
         report->n_nonfinite = (int64_t)nf;
         report->status = rc;
     }
-    // Mixed form: relative L2 error against the FP64 form on a point sample.
-    if (report && precision == BIELCC_PREC_MIXED && P > 0) {
-        const int stride = (int)std::max<size_t>(1, P / 256);
-        std::vector<double> sp;
-        std::vector<size_t> idx;
-        for (size_t i = 0; i < P; i += stride) {
-            idx.push_back(i);
-            for (int g = 0; g < 3; g++) sp.push_back(pts[3 * i + g]);
-        }
-        const size_t Q = idx.size();
-        const size_t bQ = Q * 3 * 8, bQo = S * Q * 3 * 16;
-        TRY(ctx->io.ensure(al(bJ) + al(bQ) + 2 * al(bQo) + 256));
-        io = (char*)ctx->io.p;
-        dJ = (double*)io;
-        double* dQ = (double*)(io + al(bJ));
-        double* dEq = (double*)(io + al(bJ) + al(bQ));
-        double* dHq = (double*)(io + al(bJ) + al(bQ) + al(bQo));
-        TRY(ws_acquire(ctx, s));
-        TRY_CUDA(cudaMemcpyAsync(dJ, J, bJ, cudaMemcpyHostToDevice, s));
-        TRY_CUDA(cudaMemcpyAsync(dQ, sp.data(), bQ, cudaMemcpyHostToDevice, s));
-        FieldArgs b{m, n_rhs, dJ, mk(k_re, k_im), mk(mult_re, mult_im), inc, n, (int)Q, dQ, dEq, dHq,
-                    BIELCC_PREC_FP64};
-        TRY(field_device(ctx, b, s, nullptr, nullptr));
-        std::vector<double> e64(S * Q * 6), h64(S * Q * 6);
-        TRY_CUDA(cudaMemcpyAsync(e64.data(), dEq, bQo, cudaMemcpyDeviceToHost, s));
-        TRY_CUDA(cudaMemcpyAsync(h64.data(), dHq, bQo, cudaMemcpyDeviceToHost, s));
-        TRY_CUDA(cudaStreamSynchronize(s));
-        TRY(ws_release(ctx, s));
+    if (sample) {
         double num = 0, den = 0;
         for (size_t r = 0; r < S; r++)
             for (size_t q = 0; q < Q; q++)

@@ -175,3 +175,22 @@ def test_many_rhs_single_job_routes_through_batched_kernel(gctx, precision, tol)
     Eo, Ho = oracle.field_EH(cells, J, k, pts[sub], mult=complex(0.3, 0.7))
     assert rel_l2(E[:, sub], Eo) < tol and rel_l2(H[:, sub], Ho) < tol
     assert rep.n_near_pairs > 0
+
+
+def test_mixed_error_estimate_is_the_sample_error(gctx):
+    """The mixed form's est_rel_l2 is its relative L2 error against the FP64
+    form over min(P, 256) points spread over the set (evaluated beside the
+    main evaluation): equal to the error measured against a full FP64 run at
+    those points."""
+    c = W.config1()
+    m = gctx.mesh(c["cells"])
+    for P in (1000, 100):
+        pts = c["pts"][:P]
+        Em, Hm, rep = gctx.field_EH(m, c["J"], c["k"], pts, precision="mixed")
+        E6, H6, _ = gctx.field_EH(m, c["J"], c["k"], pts, precision="fp64")
+        Q = min(P, 256)
+        idx = np.arange(Q) * P // Q
+        num = np.sum(np.abs(Em[:, idx] - E6[:, idx]) ** 2) + np.sum(np.abs(Hm[:, idx] - H6[:, idx]) ** 2)
+        den = np.sum(np.abs(E6[:, idx]) ** 2) + np.sum(np.abs(H6[:, idx]) ** 2)
+        assert rep.est_sample == Q
+        assert rep.est_rel_l2 == pytest.approx(np.sqrt(num / den), rel=1e-6)
