@@ -153,6 +153,47 @@ BIELCC_D void contract_packed_cell(const float* m, const float4* __restrict__ sj
     }
 }
 
+// Moments of one cell, real-k form finished, times e^{ik r0} into mom[20];
+// R_Rot_Colloc is 0 at the cell centre.
+template <bool CK, typename F>
+BIELCC_D void store_moments(Moments<F>& m, double P0r, double P0i, double d, F* mom) {
+    if (!CK) m.finish_real_k();
+    const F pr = (F)P0r, pi = (F)P0i;
+    mom[0] = m.a1r * pr - m.a1i * pi;
+    mom[1] = m.a1r * pi + m.a1i * pr;
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        mom[2 + 2 * q] = m.t[q][0] * pr - m.t[q][1] * pi;
+        mom[3 + 2 * q] = m.t[q][0] * pi + m.t[q][1] * pr;
+    }
+    if (!(d < kMachineZero)) {
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            mom[14 + 2 * q] = m.g[q][0] * pr - m.g[q][1] * pi;
+            mom[15 + 2 * q] = m.g[q][0] * pi + m.g[q][1] * pr;
+        }
+    }
+}
+
+// Mixed-form set-up of one (point, cell) pair: FP32 pair state, e^{ik r0} in
+// FP64, and the phase polynomial for the cell's phase range |k| rho.
+template <bool CK>
+BIELCC_D int mixed_pair_setup(const double* x, const double4& ci, double d, double rho, cplx k, const KF32& kf,
+                              PairF32& pf, double& P0r, double& P0i) {
+    const double cen[3] = {ci.x, ci.y, ci.z};
+    pf.set(x, cen, d, kf);
+    double sn, cs;
+    sincos(k.re * d, &sn, &cs);
+    if (CK) {
+        const double am = exp(-k.im * d);
+        sn *= am;
+        cs *= am;
+    }
+    P0r = cs;
+    P0i = sn;
+    return phase_mode((float)fabs(k.re) * (float)rho);
+}
+
 // Phase A of one (point, cell) pair: the 20 far moments times e^{ik r0}.
 // CK (complex k) is a property of the job, so every item of a job takes the
 // same code path whatever else is in the batch.
@@ -166,19 +207,8 @@ BIELCC_D void batch_moments(const typename BatchCfg<MIXED>::NodeT* nd, const flo
     m.zero();
     if constexpr (MIXED) {
         const KF32 kf = KF32::make(k.re, k.im);
-        const double cen[3] = {ci.x, ci.y, ci.z};
         PairF32 pf;
-        pf.set(x, cen, d, kf);
-        double sn, cs;
-        sincos(k.re * d, &sn, &cs);
-        if (CK) {
-            const double am = exp(-k.im * d);
-            sn *= am;
-            cs *= am;
-        }
-        P0r = cs;
-        P0i = sn;
-        const int mode = phase_mode((float)fabs(k.re) * (float)rho);
+        const int mode = mixed_pair_setup<CK>(x, ci, d, rho, k, kf, pf, P0r, P0i);
 #define BIELCC_BNODE(MODE_) \
     _Pragma("unroll 4") for (int i = 0; i < nn; i++) far_node_f32<CK, MODE_>(m, pf, nd[i], yy[i], kf);
         switch (mode) {
@@ -207,23 +237,41 @@ BIELCC_D void batch_moments(const typename BatchCfg<MIXED>::NodeT* nd, const flo
             }
         }
     }
-    if (!CK) m.finish_real_k();
-    // moments x e^{ik r0}; R_Rot_Colloc is 0 at the cell centre
-    const F pr = (F)P0r, pi = (F)P0i;
-    mom[0] = m.a1r * pr - m.a1i * pi;
-    mom[1] = m.a1r * pi + m.a1i * pr;
-#pragma unroll
-    for (int q = 0; q < 6; q++) {
-        mom[2 + 2 * q] = m.t[q][0] * pr - m.t[q][1] * pi;
-        mom[3 + 2 * q] = m.t[q][0] * pi + m.t[q][1] * pr;
+    store_moments<CK, F>(m, P0r, P0i, d, mom);
+}
+
+// Phase A of two far pairs of the same point (cells A and B of one job, equal
+// node counts), mixed form: the two node loops are interleaved, so each thread
+// has two independent dependency chains per node. A cell's moments do not
+// depend on the other cell; the phase polynomial is the one for the larger
+// phase range of the two (exact over the smaller range too).
+template <bool CK>
+BIELCC_D void batch_moments2(const float4* ndA, const float* yyA, const float4* ndB, const float* yyB, int nn,
+                             const double* x, const double4& ciA, double dA, double rhoA, const double4& ciB,
+                             double dB, double rhoB, cplx k, float* momA, float* momB) {
+    const KF32 kf = KF32::make(k.re, k.im);
+    PairF32 pa, pb;
+    double PAr, PAi, PBr, PBi;
+    const int mode = max(mixed_pair_setup<CK>(x, ciA, dA, rhoA, k, kf, pa, PAr, PAi),
+                         mixed_pair_setup<CK>(x, ciB, dB, rhoB, k, kf, pb, PBr, PBi));
+    Moments<float> ma, mb;
+    ma.zero();
+    mb.zero();
+#define BIELCC_BNODE2(MODE_)                                 \
+    _Pragma("unroll 2") for (int i = 0; i < nn; i++) {       \
+        far_node_f32<CK, MODE_>(ma, pa, ndA[i], yyA[i], kf); \
+        far_node_f32<CK, MODE_>(mb, pb, ndB[i], yyB[i], kf); \
     }
-    if (!(d < kMachineZero)) {
-#pragma unroll
-        for (int q = 0; q < 3; q++) {
-            mom[14 + 2 * q] = m.g[q][0] * pr - m.g[q][1] * pi;
-            mom[15 + 2 * q] = m.g[q][0] * pi + m.g[q][1] * pr;
-        }
+    switch (mode) {
+        case 0: BIELCC_BNODE2(0) break;
+        case 1: BIELCC_BNODE2(1) break;
+        case 2: BIELCC_BNODE2(2) break;
+        case 3: BIELCC_BNODE2(3) break;
+        default: BIELCC_BNODE2(4) break;
     }
+#undef BIELCC_BNODE2
+    store_moments<CK, float>(ma, PAr, PAi, dA, momA);
+    store_moments<CK, float>(mb, PBr, PBi, dB, momB);
 }
 
 template <bool MIXED>
@@ -303,27 +351,69 @@ __global__ void __launch_bounds__(kBT, MIXED ? BIELCC_BATCH_MINB : 2) batch_far_
                     }
                 }
                 __syncthreads();
-                // phase A: moments of cells warp, warp+4, ... for this warp's 32 points
-                for (int cc = warp; cc < nc; cc += kBW) {
-                    const double4 ci = s_cell[cc];
-                    const double cen[3] = {ci.x, ci.y, ci.z};
-                    double d;
-                    const bool nr = is_near(x, cen, ci.w, analytic_calc, &d);
-                    const bool far = !nr && live;
-                    s_near[cc * kBP + lane] = nr ? 1 : 0;
-                    F mom[20];
+                // phase A: moments of cells warp, warp+4, ... for this warp's 32 points; the
+                // mixed form takes them two at a time (cells cc and cc + 4)
+                if constexpr (MIXED) {
+                    for (int cc = warp; cc < nc; cc += 2 * kBW) {
+                        const int cb2 = cc + kBW;
+                        const bool two = cb2 < nc;
+                        const double4 ca = s_cell[cc], cbb = s_cell[two ? cb2 : cc];
+                        const double cena[3] = {ca.x, ca.y, ca.z}, cenb[3] = {cbb.x, cbb.y, cbb.z};
+                        double da, db;
+                        const bool na = is_near(x, cena, ca.w, analytic_calc, &da);
+                        const bool nb = is_near(x, cenb, cbb.w, analytic_calc, &db);
+                        const bool fa = !na && live, fb = two && !nb && live;
+                        s_near[cc * kBP + lane] = na ? 1 : 0;
+                        if (two) s_near[cb2 * kBP + lane] = nb ? 1 : 0;
+                        F moa[20], mob[20];
 #pragma unroll
-                    for (int q = 0; q < 20; q++) mom[q] = 0;
-                    if (far) {
-                        const NodeT* nd = s_nodes + cc * nn;
-                        const float* yy = s_yy + (MIXED ? cc * nn : 0);
-                        if (k.im != 0.0)
-                            batch_moments<MIXED, true>(nd, yy, nn, x, ci, d, s_rho[cc], k, k2r, k2i, mom);
-                        else
-                            batch_moments<MIXED, false>(nd, yy, nn, x, ci, d, s_rho[cc], k, k2r, k2i, mom);
+                        for (int q = 0; q < 20; q++) moa[q] = mob[q] = 0;
+                        const NodeT *nda = s_nodes + cc * nn, *ndb = s_nodes + (two ? cb2 : cc) * nn;
+                        const float *ya = s_yy + cc * nn, *yb = s_yy + (two ? cb2 : cc) * nn;
+                        const bool ck = k.im != 0.0;
+                        if (fa && fb) {
+                            if (ck) batch_moments2<true>(nda, ya, ndb, yb, nn, x, ca, da, s_rho[cc], cbb, db,
+                                                         s_rho[cb2], k, moa, mob);
+                            else batch_moments2<false>(nda, ya, ndb, yb, nn, x, ca, da, s_rho[cc], cbb, db,
+                                                       s_rho[cb2], k, moa, mob);
+                        } else if (fa || fb) {
+                            const NodeT* nd = fa ? nda : ndb;
+                            const float* yy = fa ? ya : yb;
+                            const double4 ci = fa ? ca : cbb;
+                            const double d = fa ? da : db, rho = s_rho[fa ? cc : cb2];
+                            F* mo = fa ? moa : mob;
+                            if (ck) batch_moments<MIXED, true>(nd, yy, nn, x, ci, d, rho, k, k2r, k2i, mo);
+                            else batch_moments<MIXED, false>(nd, yy, nn, x, ci, d, rho, k, k2r, k2i, mo);
+                        }
+#pragma unroll
+                        for (int q = 0; q < 20; q++) s_mom[(cc * 20 + q) * kBP + lane] = moa[q];
+                        if (two) {
+#pragma unroll
+                            for (int q = 0; q < 20; q++) s_mom[(cb2 * 20 + q) * kBP + lane] = mob[q];
+                        }
                     }
+                } else {
+                    for (int cc = warp; cc < nc; cc += kBW) {
+                        const double4 ci = s_cell[cc];
+                        const double cen[3] = {ci.x, ci.y, ci.z};
+                        double d;
+                        const bool nr = is_near(x, cen, ci.w, analytic_calc, &d);
+                        const bool far = !nr && live;
+                        s_near[cc * kBP + lane] = nr ? 1 : 0;
+                        F mom[20];
 #pragma unroll
-                    for (int q = 0; q < 20; q++) s_mom[(cc * 20 + q) * kBP + lane] = mom[q];
+                        for (int q = 0; q < 20; q++) mom[q] = 0;
+                        if (far) {
+                            const NodeT* nd = s_nodes + cc * nn;
+                            const float* yy = s_yy + (MIXED ? cc * nn : 0);
+                            if (k.im != 0.0)
+                                batch_moments<MIXED, true>(nd, yy, nn, x, ci, d, s_rho[cc], k, k2r, k2i, mom);
+                            else
+                                batch_moments<MIXED, false>(nd, yy, nn, x, ci, d, s_rho[cc], k, k2r, k2i, mom);
+                        }
+#pragma unroll
+                        for (int q = 0; q < 20; q++) s_mom[(cc * 20 + q) * kBP + lane] = mom[q];
+                    }
                 }
                 __syncthreads();
                 // near-cell mask (first RHS pass): warp 0 owns the words of its points
