@@ -8,9 +8,10 @@
 //             farnode.cuh) of cells w, w+4, ... of the chunk for its 32 points
 //             and stores them in shared memory (node tiles staged with 128-bit
 //             loads, one observation point per lane);
-//   phase B — the same threads contract the chunk's moments with every
-//             right-hand side staged in shared memory, R RHS per thread held in
-//             registers, and add the result into the job's partial sums.
+//   phase B — the same threads contract the chunk's moments with the
+//             right-hand sides, staged in shared memory a pass of kSP at a time
+//             (the moments stay), R RHS per thread held in registers, and add
+//             the result into the job's partial sums.
 // Extra right-hand sides therefore cost ~72 FP32 operations per pair instead
 // of the 64-node integrand. Near cells (get_field.h:58) are flagged in the
 // job's near mask and handled by the FP64 near-pair path afterwards, exactly
@@ -32,19 +33,23 @@ namespace bielcc_gpu {
 constexpr int kBT = 128;  // threads per CTA: 4 warps x 32 points
 constexpr int kBP = 32;   // points per item tile
 constexpr int kBW = 4;    // warps
-constexpr int kSP = 64;   // right-hand sides staged per pass
-
-
-// Mixed form: cells per chunk at n_start <= 8, and resident CTAs per SM the
-// kernel is compiled for. Measured on the 256-mesh batch (B200): 16 cells / 2
-// CTAs (248 registers, 81 KB smem) 959 ms per batch; 12 / 3 (162 registers)
-// 1029 ms; 8 / 4 (128 registers) 1538 ms.
+// Mixed form: cells per chunk at n_start <= 8 (CH32), right-hand sides staged
+// per pass (SP; a chunk's moments are computed once and contracted pass by
+// pass), and resident CTAs per SM the kernel is compiled for (MINB).
+// Measured on the 256-mesh batch (B200), cells / RHS per pass / CTAs per SM:
+// 16 / 16 / 3 (168 registers, 73 KB smem) 680 ms; 12 / 16 / 3 709 ms;
+// 16 / 64 / 2 (234 registers, 109 KB) 760 ms; 12 / 16 / 4 787 ms;
+// 8 / 16 / 4 (128 registers) 888 ms.
 #ifndef BIELCC_BATCH_CH32
 #define BIELCC_BATCH_CH32 16
 #endif
-#ifndef BIELCC_BATCH_MINB
-#define BIELCC_BATCH_MINB 2
+#ifndef BIELCC_BATCH_SP
+#define BIELCC_BATCH_SP 16
 #endif
+#ifndef BIELCC_BATCH_MINB
+#define BIELCC_BATCH_MINB 3
+#endif
+constexpr int kSP = BIELCC_BATCH_SP;  // right-hand sides staged per pass (a multiple of kBW x R)
 
 template <bool MIXED>
 struct BatchCfg {
@@ -316,118 +321,11 @@ __global__ void __launch_bounds__(kBT, MIXED ? BIELCC_BATCH_MINB : 2) batch_far_
         const double k2r = k.re * k.re - k.im * k.im, k2i = 2.0 * k.re * k.im;
         unsigned nbits = 0;
 
-        for (int s0 = 0; s0 < S; s0 += kSP) {
-            const int sp = min(kSP, S - s0);
-            for (int c0 = cb; c0 < ce; c0 += ch) {
-                const int nc = min(ch, ce - c0);
-                __syncthreads();
-                // stage node tables, cell rows and the chunk's currents
-                if constexpr (MIXED) {
-                    const float4* src = jb.nodes32 + (size_t)c0 * nn;
-                    for (int i = threadIdx.x; i < nc * nn; i += kBT) {
-                        const float4 v = __ldg(src + i);
-                        s_nodes[i] = v;
-                        s_yy[i] = node_yy(v);
-                    }
-                } else {
-                    const double2* src = reinterpret_cast<const double2*>(jb.nodes64 + (size_t)c0 * nn);
-                    double2* dst = reinterpret_cast<double2*>(s_nodes);
-                    for (int i = threadIdx.x; i < 2 * nc * nn; i += kBT) dst[i] = __ldg(src + i);
-                }
-                for (int i = threadIdx.x; i < nc; i += kBT) {
-                    const CellGeo& gg = jb.geo[c0 + i];
-                    s_cell[i] = make_double4(gg.c[0], gg.c[1], gg.c[2], gg.diam);
-                    s_rho[i] = (double)jb.rho32[c0 + i];
-                }
-                for (int i = threadIdx.x; i < nc * sp * 3; i += kBT) {
-                    const int cc = i / (sp * 3), rem = i - cc * sp * 3, sl = rem / 3, g = rem - sl * 3;
-                    const cplx v = jb.J[((size_t)(s0 + sl) * N + (c0 + cc)) * 3 + g];
-                    F* d = s_j + ((size_t)(cc * kSP + sl) * 3 + g) * C::JW;
-                    d[0] = (F)v.re;
-                    d[1] = (F)v.im;
-                    if constexpr (MIXED) {
-                        d[2] = (F)v.im;
-                        d[3] = (F)v.re;
-                    }
-                }
-                __syncthreads();
-                // phase A: moments of cells warp, warp+4, ... for this warp's 32 points; the
-                // mixed form takes them two at a time (cells cc and cc + 4)
-                if constexpr (MIXED) {
-                    for (int cc = warp; cc < nc; cc += 2 * kBW) {
-                        const int cb2 = cc + kBW;
-                        const bool two = cb2 < nc;
-                        const double4 ca = s_cell[cc], cbb = s_cell[two ? cb2 : cc];
-                        const double cena[3] = {ca.x, ca.y, ca.z}, cenb[3] = {cbb.x, cbb.y, cbb.z};
-                        double da, db;
-                        const bool na = is_near(x, cena, ca.w, analytic_calc, &da);
-                        const bool nb = is_near(x, cenb, cbb.w, analytic_calc, &db);
-                        const bool fa = !na && live, fb = two && !nb && live;
-                        s_near[cc * kBP + lane] = na ? 1 : 0;
-                        if (two) s_near[cb2 * kBP + lane] = nb ? 1 : 0;
-                        F moa[20], mob[20];
-#pragma unroll
-                        for (int q = 0; q < 20; q++) moa[q] = mob[q] = 0;
-                        const NodeT *nda = s_nodes + cc * nn, *ndb = s_nodes + (two ? cb2 : cc) * nn;
-                        const float *ya = s_yy + cc * nn, *yb = s_yy + (two ? cb2 : cc) * nn;
-                        const bool ck = k.im != 0.0;
-                        if (fa && fb) {
-                            if (ck) batch_moments2<true>(nda, ya, ndb, yb, nn, x, ca, da, s_rho[cc], cbb, db,
-                                                         s_rho[cb2], k, moa, mob);
-                            else batch_moments2<false>(nda, ya, ndb, yb, nn, x, ca, da, s_rho[cc], cbb, db,
-                                                       s_rho[cb2], k, moa, mob);
-                        } else if (fa || fb) {
-                            const NodeT* nd = fa ? nda : ndb;
-                            const float* yy = fa ? ya : yb;
-                            const double4 ci = fa ? ca : cbb;
-                            const double d = fa ? da : db, rho = s_rho[fa ? cc : cb2];
-                            F* mo = fa ? moa : mob;
-                            if (ck) batch_moments<MIXED, true>(nd, yy, nn, x, ci, d, rho, k, k2r, k2i, mo);
-                            else batch_moments<MIXED, false>(nd, yy, nn, x, ci, d, rho, k, k2r, k2i, mo);
-                        }
-#pragma unroll
-                        for (int q = 0; q < 20; q++) s_mom[(cc * 20 + q) * kBP + lane] = moa[q];
-                        if (two) {
-#pragma unroll
-                            for (int q = 0; q < 20; q++) s_mom[(cb2 * 20 + q) * kBP + lane] = mob[q];
-                        }
-                    }
-                } else {
-                    for (int cc = warp; cc < nc; cc += kBW) {
-                        const double4 ci = s_cell[cc];
-                        const double cen[3] = {ci.x, ci.y, ci.z};
-                        double d;
-                        const bool nr = is_near(x, cen, ci.w, analytic_calc, &d);
-                        const bool far = !nr && live;
-                        s_near[cc * kBP + lane] = nr ? 1 : 0;
-                        F mom[20];
-#pragma unroll
-                        for (int q = 0; q < 20; q++) mom[q] = 0;
-                        if (far) {
-                            const NodeT* nd = s_nodes + cc * nn;
-                            const float* yy = s_yy + (MIXED ? cc * nn : 0);
-                            if (k.im != 0.0)
-                                batch_moments<MIXED, true>(nd, yy, nn, x, ci, d, s_rho[cc], k, k2r, k2i, mom);
-                            else
-                                batch_moments<MIXED, false>(nd, yy, nn, x, ci, d, s_rho[cc], k, k2r, k2i, mom);
-                        }
-#pragma unroll
-                        for (int q = 0; q < 20; q++) s_mom[(cc * 20 + q) * kBP + lane] = mom[q];
-                    }
-                }
-                __syncthreads();
-                // near-cell mask (first RHS pass): warp 0 owns the words of its points
-                if (s0 == 0 && warp == 0) {
-                    for (int cc = 0; cc < nc; cc++) {
-                        const int c = c0 + cc;
-                        nbits |= (unsigned)s_near[cc * kBP + lane] << (c & 31);
-                        if ((c & 31) == 31 || c == ce - 1) {
-                            if (live) jb.mask[(size_t)(c >> 5) * P + p] = nbits;
-                            nbits = 0;
-                        }
-                    }
-                }
-                // phase B: RHS s = sb + warp + 4 j, j < R, contracted over the chunk's cells
+        for (int c0 = cb; c0 < ce; c0 += ch) {
+            const int nc = min(ch, ce - c0);
+            // phase B: RHS s0 + sb + warp + 4 j (j < R) of the sp staged in s_j, contracted over
+            // the chunk's cells and added into the job's partial sums
+            auto phase_b = [&](int s0, int sp) {
                 for (int sb = 0; sb < sp; sb += kBW * C::R) {
                     F acc[C::R][12];
 #pragma unroll
@@ -480,6 +378,125 @@ __global__ void __launch_bounds__(kBT, MIXED ? BIELCC_BATCH_MINB : 2) batch_far_
                         }
                     }
                 }
+            };
+            // stage the currents of RHS s0 .. s0 + sp - 1
+            auto stage_j = [&](int s0, int sp) {
+                for (int i = threadIdx.x; i < nc * sp * 3; i += kBT) {
+                    const int cc = i / (sp * 3), rem = i - cc * sp * 3, sl = rem / 3, g = rem - sl * 3;
+                    const cplx v = jb.J[((size_t)(s0 + sl) * N + (c0 + cc)) * 3 + g];
+                    F* d = s_j + ((size_t)(cc * kSP + sl) * 3 + g) * C::JW;
+                    d[0] = (F)v.re;
+                    d[1] = (F)v.im;
+                    if constexpr (MIXED) {
+                        d[2] = (F)v.im;
+                        d[3] = (F)v.re;
+                    }
+                }
+            };
+            __syncthreads();
+            // stage node tables, cell rows and the first RHS pass's currents
+            if constexpr (MIXED) {
+                const float4* src = jb.nodes32 + (size_t)c0 * nn;
+                for (int i = threadIdx.x; i < nc * nn; i += kBT) {
+                    const float4 v = __ldg(src + i);
+                    s_nodes[i] = v;
+                    s_yy[i] = node_yy(v);
+                }
+            } else {
+                const double2* src = reinterpret_cast<const double2*>(jb.nodes64 + (size_t)c0 * nn);
+                double2* dst = reinterpret_cast<double2*>(s_nodes);
+                for (int i = threadIdx.x; i < 2 * nc * nn; i += kBT) dst[i] = __ldg(src + i);
+            }
+            for (int i = threadIdx.x; i < nc; i += kBT) {
+                const CellGeo& gg = jb.geo[c0 + i];
+                s_cell[i] = make_double4(gg.c[0], gg.c[1], gg.c[2], gg.diam);
+                s_rho[i] = (double)jb.rho32[c0 + i];
+            }
+            stage_j(0, min(kSP, S));
+            __syncthreads();
+            // phase A: moments of cells warp, warp+4, ... for this warp's 32 points; the
+            // mixed form takes them two at a time (cells cc and cc + 4)
+            if constexpr (MIXED) {
+                for (int cc = warp; cc < nc; cc += 2 * kBW) {
+                    const int cb2 = cc + kBW;
+                    const bool two = cb2 < nc;
+                    const double4 ca = s_cell[cc], cbb = s_cell[two ? cb2 : cc];
+                    const double cena[3] = {ca.x, ca.y, ca.z}, cenb[3] = {cbb.x, cbb.y, cbb.z};
+                    double da, db;
+                    const bool na = is_near(x, cena, ca.w, analytic_calc, &da);
+                    const bool nb = is_near(x, cenb, cbb.w, analytic_calc, &db);
+                    const bool fa = !na && live, fb = two && !nb && live;
+                    s_near[cc * kBP + lane] = na ? 1 : 0;
+                    if (two) s_near[cb2 * kBP + lane] = nb ? 1 : 0;
+                    F moa[20], mob[20];
+#pragma unroll
+                    for (int q = 0; q < 20; q++) moa[q] = mob[q] = 0;
+                    const NodeT *nda = s_nodes + cc * nn, *ndb = s_nodes + (two ? cb2 : cc) * nn;
+                    const float *ya = s_yy + cc * nn, *yb = s_yy + (two ? cb2 : cc) * nn;
+                    const bool ck = k.im != 0.0;
+                    if (fa && fb) {
+                        if (ck) batch_moments2<true>(nda, ya, ndb, yb, nn, x, ca, da, s_rho[cc], cbb, db,
+                                                     s_rho[cb2], k, moa, mob);
+                        else batch_moments2<false>(nda, ya, ndb, yb, nn, x, ca, da, s_rho[cc], cbb, db,
+                                                   s_rho[cb2], k, moa, mob);
+                    } else if (fa || fb) {
+                        const NodeT* nd = fa ? nda : ndb;
+                        const float* yy = fa ? ya : yb;
+                        const double4 ci = fa ? ca : cbb;
+                        const double d = fa ? da : db, rho = s_rho[fa ? cc : cb2];
+                        F* mo = fa ? moa : mob;
+                        if (ck) batch_moments<MIXED, true>(nd, yy, nn, x, ci, d, rho, k, k2r, k2i, mo);
+                        else batch_moments<MIXED, false>(nd, yy, nn, x, ci, d, rho, k, k2r, k2i, mo);
+                    }
+#pragma unroll
+                    for (int q = 0; q < 20; q++) s_mom[(cc * 20 + q) * kBP + lane] = moa[q];
+                    if (two) {
+#pragma unroll
+                        for (int q = 0; q < 20; q++) s_mom[(cb2 * 20 + q) * kBP + lane] = mob[q];
+                    }
+                }
+            } else {
+                for (int cc = warp; cc < nc; cc += kBW) {
+                    const double4 ci = s_cell[cc];
+                    const double cen[3] = {ci.x, ci.y, ci.z};
+                    double d;
+                    const bool nr = is_near(x, cen, ci.w, analytic_calc, &d);
+                    const bool far = !nr && live;
+                    s_near[cc * kBP + lane] = nr ? 1 : 0;
+                    F mom[20];
+#pragma unroll
+                    for (int q = 0; q < 20; q++) mom[q] = 0;
+                    if (far) {
+                        const NodeT* nd = s_nodes + cc * nn;
+                        const float* yy = s_yy + (MIXED ? cc * nn : 0);
+                        if (k.im != 0.0)
+                            batch_moments<MIXED, true>(nd, yy, nn, x, ci, d, s_rho[cc], k, k2r, k2i, mom);
+                        else
+                            batch_moments<MIXED, false>(nd, yy, nn, x, ci, d, s_rho[cc], k, k2r, k2i, mom);
+                    }
+#pragma unroll
+                    for (int q = 0; q < 20; q++) s_mom[(cc * 20 + q) * kBP + lane] = mom[q];
+                }
+            }
+            __syncthreads();
+            // near-cell mask: warp 0 owns the words of its points
+            if (warp == 0) {
+                for (int cc = 0; cc < nc; cc++) {
+                    const int c = c0 + cc;
+                    nbits |= (unsigned)s_near[cc * kBP + lane] << (c & 31);
+                    if ((c & 31) == 31 || c == ce - 1) {
+                        if (live) jb.mask[(size_t)(c >> 5) * P + p] = nbits;
+                        nbits = 0;
+                    }
+                }
+            }
+            phase_b(0, min(kSP, S));
+            // further RHS passes reuse the chunk's moments in shared memory
+            for (int s0 = kSP; s0 < S; s0 += kSP) {
+                __syncthreads();
+                stage_j(s0, min(kSP, S - s0));
+                __syncthreads();
+                phase_b(s0, min(kSP, S - s0));
             }
         }
     }
