@@ -251,7 +251,14 @@ int field_device_batched(bielcc_ctx ctx, const FieldArgs& a, cudaStream_t s, bie
     d.E = a.E;
     d.H = a.H;
     BatchPlan bp;
-    plan_batch(bp, std::vector<JobDev>{d}, a.np.n_start, a.precision == BIELCC_PREC_MIXED, ctx->batch_item_cost);
+    const bool mixed = a.precision == BIELCC_PREC_MIXED;
+    plan_batch(bp, std::vector<JobDev>{d}, a.np.n_start, mixed, ctx->batch_item_cost);
+    // The tuned item size suits batches of many jobs; one job alone is cut
+    // finer (up to its range limit) when its items would leave resident CTAs idle.
+    if ((int)bp.items.size() < 2 * bp.grid) {
+        const double finer = std::max(1.0e5, ctx->batch_item_cost * bp.items.size() / (2.0 * bp.grid));
+        if (finer < ctx->batch_item_cost) plan_batch(bp, std::vector<JobDev>{d}, a.np.n_start, mixed, finer);
+    }
     const double busy = std::min(1.0, (double)bp.items.size() / std::max(1, bp.grid));
     if ((double)((a.n_rhs + 3) / 4) * busy <= 1.5) return BIELCC_OK;
     TRY(w.ws->ensure(bp.ws_bytes));

@@ -50,6 +50,18 @@ constexpr int kBW = 4;    // warps
 #define BIELCC_BATCH_MINB 3
 #endif
 constexpr int kSP = BIELCC_BATCH_SP;  // right-hand sides staged per pass (a multiple of kBW x R)
+// Unrolling of the one-cell and two-cell phase-A node loops. Three CTAs of
+// different jobs (different phase polynomials) share an SM's instruction
+// cache: the two-cell loop, already two dependency chains wide, is not
+// unrolled (256-mesh batch: 681 ms unrolled x2, 661 ms not unrolled).
+#ifndef BIELCC_BATCH_U1
+#define BIELCC_BATCH_U1 4
+#endif
+#ifndef BIELCC_BATCH_U2
+#define BIELCC_BATCH_U2 1
+#endif
+#define BIELCC_PRAGMA_STR(x) #x
+#define BIELCC_UNROLL(n) _Pragma(BIELCC_PRAGMA_STR(unroll n))
 
 template <bool MIXED>
 struct BatchCfg {
@@ -215,7 +227,7 @@ BIELCC_D void batch_moments(const typename BatchCfg<MIXED>::NodeT* nd, const flo
         PairF32 pf;
         const int mode = mixed_pair_setup<CK>(x, ci, d, rho, k, kf, pf, P0r, P0i);
 #define BIELCC_BNODE(MODE_) \
-    _Pragma("unroll 4") for (int i = 0; i < nn; i++) far_node_f32<CK, MODE_>(m, pf, nd[i], yy[i], kf);
+    BIELCC_UNROLL(BIELCC_BATCH_U1) for (int i = 0; i < nn; i++) far_node_f32<CK, MODE_>(m, pf, nd[i], yy[i], kf);
         switch (mode) {
             case 0: BIELCC_BNODE(0) break;
             case 1: BIELCC_BNODE(1) break;
@@ -263,7 +275,7 @@ BIELCC_D void batch_moments2(const float4* ndA, const float* yyA, const float4* 
     ma.zero();
     mb.zero();
 #define BIELCC_BNODE2(MODE_)                                 \
-    _Pragma("unroll 2") for (int i = 0; i < nn; i++) {       \
+    BIELCC_UNROLL(BIELCC_BATCH_U2) for (int i = 0; i < nn; i++) { \
         far_node_f32<CK, MODE_>(ma, pa, ndA[i], yyA[i], kf); \
         far_node_f32<CK, MODE_>(mb, pb, ndB[i], yyB[i], kf); \
     }
