@@ -101,8 +101,8 @@ typedef struct bielcc_report {
     int64_t n_pairs;        /* point x cell pairs evaluated (per RHS) */
     int64_t n_near_pairs;   /* pairs that took the FP64 near path */
     int64_t n_nonfinite;    /* non-finite output components */
-    double  est_rel_l2;     /* mixed: rel-L2 vs FP64 on a point sample; FP64: 0 */
-    int32_t est_sample;     /* points in that sample */
+    double  est_rel_l2;     /* mixed, host-buffer call: rel-L2 vs FP64 on a point sample; otherwise 0 */
+    int32_t est_sample;     /* points in that sample: min(n_pts, 256), spread evenly over the set */
     int32_t status;         /* same as the return value */
 } bielcc_report;
 
