@@ -438,13 +438,13 @@ int bielcc_ctx_destroy(bielcc_ctx ctx) {
     if (ctx->h_side_total) cudaFreeHost(ctx->h_side_total);
     if (ctx->side_in) cudaEventDestroy(ctx->side_in);
     if (ctx->side) cudaStreamDestroy(ctx->side);
-    if (ctx->h_total) cudaFreeHost(ctx->h_total);
-    if (ctx->h_nonfinite) cudaFreeHost(ctx->h_nonfinite);
+    if (ctx->h_total) cudaFreeHost(ctx->h_total);  // h_nonfinite lives in the same pinned block
     if (ctx->ws_done) cudaEventDestroy(ctx->ws_done);
     if (ctx->far_begin) cudaEventDestroy(ctx->far_begin);
     if (ctx->far_end) cudaEventDestroy(ctx->far_end);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
+    cudaGetLastError();  // leave no error of the clean-up behind for the next call on this thread
     return BIELCC_OK;
 }
 

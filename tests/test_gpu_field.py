@@ -194,3 +194,21 @@ def test_mixed_error_estimate_is_the_sample_error(gctx):
         den = np.sum(np.abs(E6[:, idx]) ** 2) + np.sum(np.abs(H6[:, idx]) ** 2)
         assert rep.est_sample == Q
         assert rep.est_rel_l2 == pytest.approx(np.sqrt(num / den), rel=1e-6)
+
+
+def test_context_created_again_after_destroy():
+    """Destroying a context leaves no CUDA error behind: a context created
+    after it uploads a mesh and evaluates as the first did."""
+    from bielcc_b200 import gpu
+
+    c = W.config1()
+    pts = c["pts"][:64]
+    out = []
+    for _ in range(2):
+        ctx = gpu.Context(0)
+        m = ctx.mesh(c["cells"])
+        E, H, _ = ctx.field_EH(m, c["J"], c["k"], pts, precision="mixed")
+        out.append((E, H))
+        m.close()
+        ctx.close()
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
