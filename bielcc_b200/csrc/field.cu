@@ -502,14 +502,13 @@ static int far_slots(int n_rhs, bool ck, bool mixed, bool adaptive) {
     return v;
 }
 
-size_t field_ws_base_bytes(const FieldLaunch& f, int* splits_out) {
+size_t field_ws_base_bytes(const FieldLaunch& f, int* splits_out, size_t partial_cap) {
     const int tiles = (f.n_pts + kFarThreads - 1) / kFarThreads;
     const int N = f.mesh->n_cells;
     const size_t P = f.n_pts;
     const size_t per_split = (size_t)f.n_rhs * 12 * P * sizeof(double);
     const int slots = far_slots(f.n_rhs, f.k.im != 0.0, f.precision == 1, f.np.p_max > 1);
-    // partial sums within 256 MB
-    const int max_splits = (int)std::max<size_t>(1, ((size_t)256 << 20) / std::max<size_t>(1, per_split));
+    const int max_splits = (int)std::max<size_t>(1, partial_cap / std::max<size_t>(1, per_split));
     const int splits = choose_cell_splits(tiles, N, slots, max_splits);
     *splits_out = splits;
     return align256((size_t)splits * per_split) + 2 * align256((P + 1) * sizeof(long long)) +

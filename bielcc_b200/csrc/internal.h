@@ -61,7 +61,8 @@ struct FieldLaunch {
 };
 // Workspace bytes a field call needs before the near-pair count is known
 // (partials, counts, offsets) and the per-near-pair bytes.
-size_t field_ws_base_bytes(const FieldLaunch& f, int* splits_out);
+// partial_cap bounds the far partial sums (the split count), at least one split.
+size_t field_ws_base_bytes(const FieldLaunch& f, int* splits_out, size_t partial_cap = (size_t)256 << 20);
 size_t field_pair_ws_bytes(long long n_near);
 // Stage 1: far kernel + near counting + scan; writes total near pairs to
 // *d_total (device). Stage 2 (after the host knows the total): near fill,

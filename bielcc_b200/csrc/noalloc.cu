@@ -129,8 +129,15 @@ extern "C" int bielcc_field_EH_noalloc(int n_vert, int n_cells, const double* ce
     f.add_H = inc ? inc->add_H : 0;
     f.E = E_dev;
     f.H = H_dev;
+    // the far partial sums take at most half of the room left after the node
+    // tables and the one-split workspace (more cell splits fill the GPU better;
+    // the other half stays for the near pairs)
     int splits = 1;
-    const size_t b_ws = al(field_ws_base_bytes(f, &splits));
+    const size_t per_split = al((size_t)n_rhs * 12 * n_pts * sizeof(double));
+    const size_t b_one = al(field_ws_base_bytes(f, &splits, 0));
+    const size_t used = off + b_one + 256;
+    const size_t room = used < BIELCC_NOALLOC_SCRATCH_BYTES ? BIELCC_NOALLOC_SCRATCH_BYTES - used : 0;
+    const size_t b_ws = al(field_ws_base_bytes(f, &splits, per_split + room / 2));
     char* ws = sp + off;
     off += b_ws;
     long long* d_total = (long long*)(sp + off);

@@ -80,6 +80,41 @@ def test_noalloc_matches_allocating_entry_point_twice():
     ctx.close()
 
 
+def test_noalloc_large_far_point_set_fits():
+    """8192 cells x 18,000 far points (no near pairs): the far partial sums are
+    sized to the room the static array has left, so the call fits and matches
+    the allocating entry point."""
+    torch = pytest.importorskip("torch")
+    L, noalloc = _bind()
+    c = W.config2()
+    cells, J, k = c["cells"], c["J"], c["k"]
+    pts = c["pts"][:18000]
+    dev = torch.device("cuda:0")
+    ctx = gpu.Context(0)
+    mesh = ctx.mesh(cells)
+    stream = torch.cuda.current_stream(dev)
+    Cd = torch.from_numpy(np.ascontiguousarray(cells)).to(dev)
+    Jd = torch.from_numpy(np.ascontiguousarray(J)).to(dev)
+    Pd = torch.from_numpy(np.ascontiguousarray(pts)).to(dev)
+    shape = (1, len(pts), 3)
+    Ea = torch.zeros(shape, dtype=torch.complex128, device=dev)
+    Ha = torch.zeros_like(Ea)
+    Eb = torch.zeros_like(Ea)
+    Hb = torch.zeros_like(Ea)
+    ctx.field_EH_device(mesh, Jd.data_ptr(), k, Pd.data_ptr(), Ea.data_ptr(), Ha.data_ptr(), 1, len(pts),
+                        precision="mixed", stream=stream.cuda_stream)
+    rep = abi.Report()
+    rc = noalloc(4, len(cells), Cd.data_ptr(), 1, Jd.data_ptr(), k, 0.0, 1.0, 0.0, None, None, len(pts),
+                 Pd.data_ptr(), Eb.data_ptr(), Hb.data_ptr(), gpu.PREC["mixed"], stream.cuda_stream, C.byref(rep))
+    assert rc == 0, L.bielcc_last_error().decode()
+    torch.cuda.synchronize()
+    assert rep.n_near_pairs == 0
+    assert rel_l2(Eb.cpu().numpy(), Ea.cpu().numpy()) < TOL_MIXED
+    assert rel_l2(Hb.cpu().numpy(), Ha.cpu().numpy()) < TOL_MIXED
+    mesh.close()
+    ctx.close()
+
+
 def test_noalloc_rejects_sizes_beyond_its_scratch():
     torch = pytest.importorskip("torch")
     L, noalloc = _bind()
