@@ -39,7 +39,19 @@
 
 namespace bielcc_gpu {
 
-constexpr int kFarThreads = 128;
+#ifndef BIELCC_FAR_THREADS
+#define BIELCC_FAR_THREADS 128
+#endif
+constexpr int kFarThreads = BIELCC_FAR_THREADS;
+// Minimum resident CTAs per SM asked of the 1-RHS real-k mixed far kernel
+// (0: none, the compiler's own register choice, which the other variants
+// keep). 5 caps it at 96 registers without spills: 20 warps per SM instead of
+// 16 (far launch on 8192 cells x 20,000 points 25.87 -> 25.42 ms).
+#ifndef BIELCC_FAR_MINB
+#define BIELCC_FAR_MINB 5
+#endif
+#define BIELCC_FAR_BOUNDS(NRHS_, CK_, MIXED_) \
+    __launch_bounds__(kFarThreads, (NRHS_ == 1 && !CK_ && MIXED_) ? BIELCC_FAR_MINB : 0)
 constexpr int kStageNodes = 256;
 constexpr int kMaxStageCells = 32;
 
@@ -115,7 +127,7 @@ BIELCC_D void contract(const Moments<F>& m, F pr, F pi, const cplx (*sj)[3], boo
 
 // The far kernel. MIXED = false: FP64 nodes; true: FP32 nodes.
 template <int NRHS, bool CK, bool MIXED>
-__global__ void __launch_bounds__(kFarThreads) far_kernel(FarArgs a) {
+__global__ void BIELCC_FAR_BOUNDS(NRHS, CK, MIXED) far_kernel(FarArgs a) {
     using NodeT = typename std::conditional<MIXED, float4, double4>::type;
     __shared__ __align__(16) NodeT s_nodes[kStageNodes];
     __shared__ float s_yy[MIXED ? kStageNodes : 1];  // |y - centre|^2 of the staged nodes (mixed form)
