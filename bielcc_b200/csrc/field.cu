@@ -50,8 +50,13 @@ constexpr int kFarThreads = BIELCC_FAR_THREADS;
 #ifndef BIELCC_FAR_MINB
 #define BIELCC_FAR_MINB 5
 #endif
+// The same for the 1-RHS real-k FP64 far kernel: 4 (127 registers) measured
+// slower than the compiler's own 152 (FP64 step 63.1 against 58.7 ms).
+#ifndef BIELCC_FAR64_MINB
+#define BIELCC_FAR64_MINB 0
+#endif
 #define BIELCC_FAR_BOUNDS(NRHS_, CK_, MIXED_) \
-    __launch_bounds__(kFarThreads, (NRHS_ == 1 && !CK_ && MIXED_) ? BIELCC_FAR_MINB : 0)
+    __launch_bounds__(kFarThreads, NRHS_ == 1 && !CK_ ? (MIXED_ ? BIELCC_FAR_MINB : BIELCC_FAR64_MINB) : 0)
 constexpr int kStageNodes = 256;
 constexpr int kMaxStageCells = 32;
 
