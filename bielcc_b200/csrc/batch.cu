@@ -567,9 +567,61 @@ __global__ void batch_near_pair_kernel(const JobDev* __restrict__ jobs, const in
 // near pairs in cell order, the multiplier and the incident field. Not
 // inlined, so the arithmetic is compiled once and the complex64 and
 // complex128 outputs round the very same FP64 values.
-__device__ __noinline__ void finalize_values(const JobDev& jb, int p, int s, long long q0, long long q1,
-                                             const int* __restrict__ pair_cell, const cplx* __restrict__ moments,
-                                             double cs, double sn, const double* kx0, cplx* E, cplx* H) {
+// Near pairs of a point contracted with its job's currents: one warp per
+// point and RHS pass over the job's RHS. Lane l takes the point's pairs l,
+// l + 32, ... (cell order) and sums them in order; a fixed xor butterfly
+// combines the lanes, so the sum depends only on the point's own pair list.
+// Written to the job's partial-sum slot after its cell ranges:
+// partial[ranges][s][12][p], already / 4pi.
+__global__ void batch_near_sum_kernel(const JobDev* __restrict__ jobs, const int* __restrict__ pt_job, int total,
+                                      const long long* __restrict__ offs, const int* __restrict__ pair_cell,
+                                      const cplx* __restrict__ moments) {
+    const long long g = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (g >= total) return;  // whole warps
+    const long long q0 = offs[g], q1 = offs[g + 1];
+    if (q0 == q1) return;
+    const JobDev& jb = jobs[pt_job[g]];
+    const int p = (int)(g - jb.pt_off);
+    const size_t P = jb.n_pts;
+    for (int s = 0; s < jb.n_rhs; s++) {
+        double v[12];
+#pragma unroll
+        for (int i = 0; i < 12; i++) v[i] = 0.;
+        for (long long q = q0 + lane; q < q1; q += 32) {
+            const int c = pair_cell[q];
+            const cplx* o = moments + q * 13;
+            const cplx* j = jb.J + ((size_t)s * jb.n_cells + c) * 3;
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                const cplx kv = o[0] * j[a] + o[1 + 3 * a] * j[0] + o[2 + 3 * a] * j[1] + o[3 + 3 * a] * j[2];
+                v[2 * a] += kv.re;
+                v[2 * a + 1] += kv.im;
+            }
+            cplx h[3];
+            ccross_cc(o + 10, j, h);
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                v[6 + 2 * a] += h[a].re;
+                v[7 + 2 * a] += h[a].im;
+            }
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+            for (int i = 0; i < 12; i++) v[i] += __shfl_xor_sync(0xffffffffu, v[i], off);
+        if (lane < 12) {
+            double x = v[0];
+#pragma unroll
+            for (int i = 1; i < 12; i++)
+                if (lane == i) x = v[i];
+            jb.partial[(((size_t)jb.ranges * jb.n_rhs + s) * 12 + lane) * P + p] = x;
+        }
+    }
+}
+
+__device__ __noinline__ void finalize_values(const JobDev& jb, int p, int s, bool has_near, double cs, double sn,
+                                             const double* kx0, cplx* E, cplx* H) {
     const size_t P = jb.n_pts;
     double v[12];
     for (int q = 0; q < 12; q++) v[q] = 0.;
@@ -581,15 +633,12 @@ __device__ __noinline__ void finalize_values(const JobDev& jb, int p, int s, lon
         E[a] = mk(v[2 * a], v[2 * a + 1]) * kInvFourPi;
         H[a] = mk(v[6 + 2 * a], v[6 + 2 * a + 1]) * kInvFourPi;
     }
-    for (long long q = q0; q < q1; q++) {
-        const int c = pair_cell[q];
-        const cplx* o = moments + q * 13;
-        const cplx* j = jb.J + ((size_t)s * jb.n_cells + c) * 3;
-        for (int a = 0; a < 3; a++)
-            E[a] += o[0] * j[a] + o[1 + 3 * a] * j[0] + o[2 + 3 * a] * j[1] + o[3 + 3 * a] * j[2];
-        cplx h[3];
-        ccross_cc(o + 10, j, h);
-        for (int a = 0; a < 3; a++) H[a] += h[a];
+    if (has_near) {  // batch_near_sum_kernel's sums
+        const double* nv = jb.partial + (((size_t)jb.ranges * jb.n_rhs + s) * 12) * P + p;
+        for (int a = 0; a < 3; a++) {
+            E[a] += mk(nv[(size_t)(2 * a) * P], nv[(size_t)(2 * a + 1) * P]);
+            H[a] += mk(nv[(size_t)(6 + 2 * a) * P], nv[(size_t)(7 + 2 * a) * P]);
+        }
     }
     for (int a = 0; a < 3; a++) E[a] = E[a] * jb.mult;
     if (jb.add_E)
@@ -599,8 +648,7 @@ __device__ __noinline__ void finalize_values(const JobDev& jb, int p, int s, lon
 }
 
 __global__ void batch_finalize_kernel(const JobDev* __restrict__ jobs, const int* __restrict__ pt_job, int total,
-                                      const long long* __restrict__ offs, const int* __restrict__ pair_cell,
-                                      const cplx* __restrict__ moments, unsigned long long* nonfinite) {
+                                      const long long* __restrict__ offs, unsigned long long* nonfinite) {
     int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= total) return;
     const JobDev& jb = jobs[pt_job[g]];
@@ -615,7 +663,7 @@ __global__ void batch_finalize_kernel(const JobDev* __restrict__ jobs, const int
     bool bad = false;
     for (int s = 0; s < jb.n_rhs; s++) {
         cplx E[3], H[3];
-        finalize_values(jb, p, s, q0, q1, pair_cell, moments, cs, sn, kx0, E, H);
+        finalize_values(jb, p, s, q1 > q0, cs, sn, kx0, E, H);
         for (int a = 0; a < 3; a++) bad |= !isfinite(E[a].re) || !isfinite(E[a].im);
         if (jb.E32) {
             float2* eo = reinterpret_cast<float2*>(jb.E32) + ((size_t)s * P + p) * 3;
@@ -701,7 +749,7 @@ void plan_batch(BatchPlan& bp, const std::vector<JobDev>& jobs_in, int n_start, 
                 const int cells = std::min(cpr, j.n_cells - r * cpr);
                 cost.push_back((double)cells * per_cell);
             }
-        bp.ws_bytes += al256((size_t)j.ranges * j.n_rhs * 12 * j.n_pts * sizeof(double)) +
+        bp.ws_bytes += al256((size_t)(j.ranges + 1) * j.n_rhs * 12 * j.n_pts * sizeof(double)) +
                        al256((size_t)j.n_words * j.n_pts * sizeof(unsigned));
     }
     bp.total_pts = pt_off;
@@ -729,7 +777,7 @@ cudaError_t batch_stage1(BatchPlan& bp, void* ws, double analytic_calc, int n_st
     char* w = (char*)ws;
     for (auto& j : bp.jobs) {
         j.partial = (double*)w;
-        w += al256((size_t)j.ranges * j.n_rhs * 12 * j.n_pts * sizeof(double));
+        w += al256((size_t)(j.ranges + 1) * j.n_rhs * 12 * j.n_pts * sizeof(double));  // + the near sums
         j.mask = (unsigned*)w;
         w += al256((size_t)j.n_words * j.n_pts * sizeof(unsigned));
     }
@@ -793,11 +841,13 @@ cudaError_t batch_stage2(BatchPlan& bp, const BatchDevPtrs& d, long long n_near,
         batch_near_fill_kernel<<<tb, 128, 0, s>>>(d.jobs, d.pt_job, (int)T, d.offs, pair_cell, pair_gpt);
         batch_near_pair_kernel<<<(int)((n_near + 127) / 128), 128, 0, s>>>(d.jobs, d.pt_job, pair_cell, pair_gpt,
                                                                           n_near, np, moments);
-        *launches += 2;
+        batch_near_sum_kernel<<<(int)((T + 7) / 8), 256, 0, s>>>(d.jobs, d.pt_job, (int)T, d.offs, pair_cell,
+                                                                moments);
+        *launches += 3;
     }
     if (T) {
-        batch_finalize_kernel<<<tb, 128, 0, s>>>(d.jobs, d.pt_job, (int)T, n_near > 0 ? d.offs : nullptr, pair_cell,
-                                                  moments, d_nonfinite);
+        batch_finalize_kernel<<<tb, 128, 0, s>>>(d.jobs, d.pt_job, (int)T, n_near > 0 ? d.offs : nullptr,
+                                                  d_nonfinite);
         *launches += 1;
     }
     return cudaGetLastError();
@@ -825,13 +875,14 @@ cudaError_t batch_replay(BatchPlan& bp, const BatchDevPtrs& d, long long n_near,
     if (T) {
         const cplx* moments = nullptr;
         const int* pair_cell = nullptr;
-        if (n_near > 0) {
+        if (n_near > 0) {  // the near sums depend on the currents: recomputed every replay
             moments = (const cplx*)pair_ws;
             pair_cell = (const int*)((const char*)pair_ws + al256((size_t)n_near * 13 * sizeof(cplx)));
+            batch_near_sum_kernel<<<(int)((T + 7) / 8), 256, 0, s>>>(d.jobs, d.pt_job, (int)T, d.offs, pair_cell,
+                                                                    moments);
         }
         batch_finalize_kernel<<<(int)((T + 127) / 128), 128, 0, s>>>(d.jobs, d.pt_job, (int)T,
-                                                                      n_near > 0 ? d.offs : nullptr, pair_cell,
-                                                                      moments, nullptr);
+                                                                      n_near > 0 ? d.offs : nullptr, nullptr);
     }
     return cudaGetLastError();
 }

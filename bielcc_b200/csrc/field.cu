@@ -17,7 +17,7 @@
 //                     the cell centre in FP32, phase split e^{ikr} =
 //                     e^{ik r0} e^{ik (r - r0)} with r0 = |x - centre| and
 //                     e^{ik r0} in FP64, r - r0 = q / (r + r0) with
-//                     q = delta.(delta - 2X) (no cancellation), FP32 cell sums,
+//                     q = |delta|^2 - 2 delta.X (no cancellation), FP32 cell sums,
 //                     FP64 accumulation across cells.
 //   2. near count + scan + fill — per point, the cells with
 //                     |x - centre| < analytic_calc * diam (get_field.h:58), in
@@ -25,8 +25,11 @@
 //   3. near pair kernel — FP64, one pair per thread: the J-independent parts of
 //                     K_RotRot_Near_Smooth (K.h:47-79) and R_Rot_Smooth
 //                     (R.h:46-61) with the reference's adaptive quadrature.
-//   4. finalize     — per (point, RHS): far partials over splits (in order) +
-//                     near pairs (in cell order), x mult, + incident field.
+//   4. near sums    — one warp per (point, RHS): the point's near pairs
+//                     contracted with J, lane-strided in cell order, fixed
+//                     butterfly across the lanes.
+//   5. finalize     — per (point, RHS): far partials over splits (in order) +
+//                     the near sum, x mult, + incident field.
 #include <algorithm>
 #include <atomic>
 #include <type_traits>
@@ -412,14 +415,60 @@ __global__ void near_pair_kernel(const double* __restrict__ pts, const double* _
     near_pair_moments(x, cl, k, np, out + q * 13);
 }
 
+// Near pairs of a point contracted with one RHS: one warp per (point, RHS).
+// Lane l takes the point's pairs l, l + 32, ... (cell order) and sums them in
+// order; the 32 lane sums are combined by a fixed xor butterfly. The result
+// depends only on the point's own pair list, whatever else runs, and a point
+// with hundreds of near cells (small cells near a pole) no longer holds up a
+// whole point tile in one thread. near[s][12][p] = E, H (re, im), already / 4pi.
+__global__ void near_sum_kernel(const long long* __restrict__ offs, const int* __restrict__ pair_cell,
+                                const cplx* __restrict__ moments, const cplx* __restrict__ J, int n_pts, int n_cells,
+                                double* __restrict__ near) {
+    const int p = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    const int s = blockIdx.y;
+    if (p >= n_pts) return;  // whole warps
+    const long long q0 = offs[p], q1 = offs[p + 1];
+    if (q0 == q1) return;
+    double v[12];
+#pragma unroll
+    for (int i = 0; i < 12; i++) v[i] = 0.;
+    for (long long q = q0 + lane; q < q1; q += 32) {
+        const int c = pair_cell[q];
+        const cplx* o = moments + q * 13;
+        const cplx* j = J + ((size_t)s * n_cells + c) * 3;
+#pragma unroll
+        for (int g = 0; g < 3; g++) {
+            const cplx kv = o[0] * j[g] + o[1 + 3 * g] * j[0] + o[2 + 3 * g] * j[1] + o[3 + 3 * g] * j[2];
+            v[2 * g] += kv.re;
+            v[2 * g + 1] += kv.im;
+        }
+        cplx h[3];
+        ccross_cc(o + 10, j, h);
+#pragma unroll
+        for (int g = 0; g < 3; g++) {
+            v[6 + 2 * g] += h[g].re;
+            v[7 + 2 * g] += h[g].im;
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+        for (int i = 0; i < 12; i++) v[i] += __shfl_xor_sync(0xffffffffu, v[i], off);
+    if (lane < 12) {
+        double x = v[0];
+#pragma unroll
+        for (int i = 1; i < 12; i++)
+            if (lane == i) x = v[i];
+        near[((size_t)s * 12 + lane) * n_pts + p] = x;
+    }
+}
+
 struct FinalArgs {
     const double* pts;
     int n_pts, n_rhs, n_cells, splits;
     const double* partial;
-    const long long* offs;
-    const int* pair_cell;
-    const cplx* moments;
-    const cplx* J;
+    const long long* offs;  // near-pair offsets per point, or null without near pairs
+    const double* near;     // near_sum_kernel's sums
     cplx mult;
     double kvec[3], e0[3], h_scale;
     int add_E, add_H;
@@ -444,18 +493,11 @@ __global__ void finalize_kernel(FinalArgs a) {
         E[g] = mk(v[2 * g], v[2 * g + 1]) * kInvFourPi;
         H[g] = mk(v[6 + 2 * g], v[6 + 2 * g + 1]) * kInvFourPi;
     }
-    if (a.offs) {
-        for (long long q = a.offs[p]; q < a.offs[p + 1]; q++) {
-            int c = a.pair_cell[q];
-            const cplx* o = a.moments + q * 13;
-            const cplx* j = a.J + ((size_t)s * a.n_cells + c) * 3;
-            for (int g = 0; g < 3; g++) {
-                cplx kv = o[0] * j[g] + o[1 + 3 * g] * j[0] + o[2 + 3 * g] * j[1] + o[3 + 3 * g] * j[2];
-                E[g] += kv;
-            }
-            cplx h[3];
-            ccross_cc(o + 10, j, h);
-            for (int g = 0; g < 3; g++) H[g] += h[g];
+    if (a.offs && a.offs[p + 1] > a.offs[p]) {
+        const double* nv = a.near + (size_t)s * 12 * P + p;
+        for (int g = 0; g < 3; g++) {
+            E[g] += mk(nv[(size_t)(2 * g) * P], nv[(size_t)(2 * g + 1) * P]);
+            H[g] += mk(nv[(size_t)(6 + 2 * g) * P], nv[(size_t)(7 + 2 * g) * P]);
         }
     }
     for (int g = 0; g < 3; g++) E[g] = E[g] * a.mult;
@@ -529,7 +571,8 @@ size_t field_ws_base_bytes(const FieldLaunch& f, int* splits_out, size_t partial
     const int splits = choose_cell_splits(tiles, N, slots, max_splits);
     *splits_out = splits;
     return align256((size_t)splits * per_split) + 2 * align256((P + 1) * sizeof(long long)) +
-           align256(sizeof(long long)) + align256(mask_words(N) * P * sizeof(unsigned));
+           align256(sizeof(long long)) + align256(mask_words(N) * P * sizeof(unsigned)) +
+           align256((size_t)f.n_rhs * 12 * P * sizeof(double));
 }
 
 template <int NRHS, bool CK, bool MIXED>
@@ -618,6 +661,8 @@ cudaError_t field_stage2(const FieldLaunch& f, void* ws, int splits, long long n
     w += align256((P + 1) * sizeof(long long)) + align256(sizeof(long long));
     const unsigned* mask = (const unsigned*)w;
     const int n_words = (int)mask_words(m.n_cells);
+    w += align256(mask_words(m.n_cells) * P * sizeof(unsigned));
+    double* near = (double*)w;
 
     int* pair_cell = nullptr;
     int* pair_pt = nullptr;
@@ -635,7 +680,9 @@ cudaError_t field_stage2(const FieldLaunch& f, void* ws, int splits, long long n
                f.np.p_max_seg};
         int blocks = (int)((n_near + 127) / 128);
         near_pair_kernel<<<blocks, 128, 0, s>>>(f.pts, m.verts, m.nv, pair_cell, pair_pt, n_near, f.k, np, moments);
-        *launches += 2;
+        near_sum_kernel<<<dim3((f.n_pts + 7) / 8, f.n_rhs), 256, 0, s>>>(
+            offs, pair_cell, moments, reinterpret_cast<const cplx*>(f.J), f.n_pts, m.n_cells, near);
+        *launches += 3;
     }
     FinalArgs fa;
     fa.pts = f.pts;
@@ -645,9 +692,7 @@ cudaError_t field_stage2(const FieldLaunch& f, void* ws, int splits, long long n
     fa.splits = splits;
     fa.partial = partial;
     fa.offs = n_near > 0 ? offs : nullptr;
-    fa.pair_cell = pair_cell;
-    fa.moments = moments;
-    fa.J = reinterpret_cast<const cplx*>(f.J);
+    fa.near = near;
     fa.mult = f.mult;
     for (int g = 0; g < 3; g++) {
         fa.kvec[g] = f.kvec[g];

@@ -247,7 +247,7 @@ int64_t field_bytes(const Req& r, int n_start, double item_cost) {
     const int64_t out = al(S * P * 3 * (r.f.out_c64 ? 8 : 16) * (r.f.H ? 2 : 1)) + 8;
     const int64_t cpr = batch_cells_per_range((int)N, (int)S, n_start, item_cost);
     const int64_t ranges = (N + cpr - 1) / cpr, words = (N + 31) / 32;
-    const int64_t ws = al(ranges * S * 12 * P * 8) + al(words * P * 4) + P * 24 + 4096;
+    const int64_t ws = al((ranges + 1) * S * 12 * P * 8) + al(words * P * 4) + P * 24 + 4096;
     return in + out + ws + r.near_est;
 }
 
