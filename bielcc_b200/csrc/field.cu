@@ -28,7 +28,8 @@
 //   4. near sums    — one warp per (point, RHS): the point's near pairs
 //                     contracted with J, lane-strided in cell order, fixed
 //                     butterfly across the lanes.
-//   5. finalize     — per (point, RHS): far partials over splits (in order) +
+//   5. finalize     — per (point, RHS): far partials over splits (in order;
+//                     lane-strided with a fixed butterfly beyond 32 splits) +
 //                     the near sum, x mult, + incident field.
 #include <algorithm>
 #include <atomic>
@@ -477,16 +478,40 @@ struct FinalArgs {
     unsigned long long* nonfinite;
 };
 
+// Per (point, RHS): far partials over the splits, near sum, mult, incident
+// field. One thread per point sums the splits in order (coalesced over the
+// points); with many splits (a small point set spread over the whole GPU) one
+// warp per point takes splits lane-strided and combines the lanes with a fixed
+// xor butterfly, so the serial chain is splits / 32 loads long instead of splits.
+template <bool WARP>
 __global__ void finalize_kernel(FinalArgs a) {
-    int p = blockIdx.x * blockDim.x + threadIdx.x;
-    int s = blockIdx.y;
-    if (p >= a.n_pts) return;
+    const int s = blockIdx.y;
     const size_t P = a.n_pts;
     double v[12];
+#pragma unroll
     for (int q = 0; q < 12; q++) v[q] = 0.;
-    for (int sp = 0; sp < a.splits; sp++) {
-        const double* src = a.partial + (((size_t)sp * a.n_rhs + s) * 12) * P + p;
-        for (int q = 0; q < 12; q++) v[q] += src[(size_t)q * P];
+    int p;
+    if constexpr (WARP) {
+        p = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+        const int lane = threadIdx.x & 31;
+        if (p >= a.n_pts) return;  // whole warps
+        for (int sp = lane; sp < a.splits; sp += 32) {
+            const double* src = a.partial + (((size_t)sp * a.n_rhs + s) * 12) * P + p;
+#pragma unroll
+            for (int q = 0; q < 12; q++) v[q] += src[(size_t)q * P];
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+            for (int q = 0; q < 12; q++) v[q] += __shfl_xor_sync(0xffffffffu, v[q], off);
+        if (lane != 0) return;
+    } else {
+        p = blockIdx.x * blockDim.x + threadIdx.x;
+        if (p >= a.n_pts) return;
+        for (int sp = 0; sp < a.splits; sp++) {
+            const double* src = a.partial + (((size_t)sp * a.n_rhs + s) * 12) * P + p;
+            for (int q = 0; q < 12; q++) v[q] += src[(size_t)q * P];
+        }
     }
     cplx E[3], H[3];
     for (int g = 0; g < 3; g++) {
@@ -705,7 +730,8 @@ cudaError_t field_stage2(const FieldLaunch& f, void* ws, int splits, long long n
     fa.H = f.H;
     fa.nonfinite = d_nonfinite;
     if (tiles > 0 && f.n_rhs > 0) {
-        finalize_kernel<<<dim3(tiles, f.n_rhs), kFarThreads, 0, s>>>(fa);
+        if (splits > 32) finalize_kernel<true><<<dim3((f.n_pts + 7) / 8, f.n_rhs), 256, 0, s>>>(fa);
+        else finalize_kernel<false><<<dim3(tiles, f.n_rhs), kFarThreads, 0, s>>>(fa);
         *launches += 1;
     }
     return cudaGetLastError();
