@@ -526,22 +526,36 @@ __global__ void batch_near_count_kernel(const JobDev* __restrict__ jobs, const i
     counts[g] = n;
 }
 
+// Near list of a point in ascending cell order, one warp per point: lane l
+// takes a contiguous run of the point's mask words and writes after the lanes
+// before it (warp prefix sum of the bit counts).
 __global__ void batch_near_fill_kernel(const JobDev* __restrict__ jobs, const int* __restrict__ pt_job, int total,
                                        const long long* __restrict__ offs, int* __restrict__ pair_cell,
                                        int* __restrict__ pair_gpt) {
-    int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= total) return;
-    long long o = offs[g];
-    if (offs[g + 1] == o) return;
+    const long long g = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (g >= total) return;  // whole warps
+    const long long o0 = offs[g];
+    if (offs[g + 1] == o0) return;
     const JobDev& jb = jobs[pt_job[g]];
-    const int p = g - jb.pt_off;
-    for (int w = 0; w < jb.n_words; w++) {
+    const int p = (int)(g - jb.pt_off);
+    const int run = (jb.n_words + 31) / 32, w0 = min(jb.n_words, lane * run), w1 = min(jb.n_words, w0 + run);
+    int cnt = 0;
+    for (int w = w0; w < w1; w++) cnt += __popc(jb.mask[(size_t)w * jb.n_pts + p]);
+    int incl = cnt;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl += t;
+    }
+    long long o = o0 + (incl - cnt);
+    for (int w = w0; w < w1; w++) {
         unsigned b = jb.mask[(size_t)w * jb.n_pts + p];
         while (b) {
             const int bit = __ffs(b) - 1;
             b &= b - 1;
             pair_cell[o] = w * 32 + bit;
-            pair_gpt[o] = g;
+            pair_gpt[o] = (int)g;
             o++;
         }
     }
@@ -838,7 +852,8 @@ cudaError_t batch_stage2(BatchPlan& bp, const BatchDevPtrs& d, long long n_near,
         pair_cell = (int*)pw;
         pw += al256((size_t)n_near * sizeof(int));
         int* pair_gpt = (int*)pw;
-        batch_near_fill_kernel<<<tb, 128, 0, s>>>(d.jobs, d.pt_job, (int)T, d.offs, pair_cell, pair_gpt);
+        batch_near_fill_kernel<<<(int)((T + 7) / 8), 256, 0, s>>>(d.jobs, d.pt_job, (int)T, d.offs, pair_cell,
+                                                                  pair_gpt);
         batch_near_pair_kernel<<<(int)((n_near + 127) / 128), 128, 0, s>>>(d.jobs, d.pt_job, pair_cell, pair_gpt,
                                                                           n_near, np, moments);
         batch_near_sum_kernel<<<(int)((T + 7) / 8), 256, 0, s>>>(d.jobs, d.pt_job, (int)T, d.offs, pair_cell,

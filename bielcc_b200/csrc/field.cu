@@ -381,17 +381,31 @@ __global__ void near_count_kernel(const unsigned* __restrict__ mask, int n_words
     counts[p] = n;
 }
 
+// Near list of a point in ascending cell order: one warp per point. Lane l
+// takes a contiguous run of the point's mask words, counts its bits, and
+// writes its cells after those of the lanes before it (warp prefix sum), so a
+// point with hundreds of near cells does not run 256 words in one thread.
 __global__ void near_fill_kernel(const unsigned* __restrict__ mask, int n_words, int n_pts,
                                  const long long* __restrict__ offs, int* __restrict__ pair_cell,
                                  int* __restrict__ pair_pt) {
-    int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n_pts) return;
-    long long o = offs[p];
-    if (offs[p + 1] == o) return;
-    for (int w = 0; w < n_words; w++) {
+    const int p = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (p >= n_pts) return;  // whole warps
+    const long long o0 = offs[p];
+    if (offs[p + 1] == o0) return;
+    const int run = (n_words + 31) / 32, w0 = min(n_words, lane * run), w1 = min(n_words, w0 + run);
+    int cnt = 0;
+    for (int w = w0; w < w1; w++) cnt += __popc(mask[(size_t)w * n_pts + p]);
+    int incl = cnt;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl += t;
+    }
+    long long o = o0 + (incl - cnt);
+    for (int w = w0; w < w1; w++) {
         unsigned b = mask[(size_t)w * n_pts + p];
         while (b) {
-            int bit = __ffs(b) - 1;
+            const int bit = __ffs(b) - 1;
             b &= b - 1;
             pair_cell[o] = w * 32 + bit;
             pair_pt[o] = p;
@@ -700,7 +714,7 @@ cudaError_t field_stage2(const FieldLaunch& f, void* ws, int splits, long long n
         pair_cell = (int*)pw;
         pw += align256((size_t)n_near * sizeof(int));
         pair_pt = (int*)pw;
-        near_fill_kernel<<<tiles, kFarThreads, 0, s>>>(mask, n_words, f.n_pts, offs, pair_cell, pair_pt);
+        near_fill_kernel<<<(f.n_pts + 7) / 8, 256, 0, s>>>(mask, n_words, f.n_pts, offs, pair_cell, pair_pt);
         DNP np{f.np.eps, f.np.rs, f.np.rs_seg, f.np.analytic_calc, f.np.n_start, f.np.n_start_seg, f.np.p_max,
                f.np.p_max_seg};
         int blocks = (int)((n_near + 127) / 128);
