@@ -91,14 +91,80 @@ BIELCC_D void write_block_m(const AsmArgs& a, int i, int j, const double (&Kr)[3
     }
 }
 
+// The mixed form's far block, in FP32 (the moments are FP32 sums already):
+// K = A1 I + T with T symmetric (xx, xy, xz, yy, yz, zz), projected on the two
+// cells' tangents (M = 2: u_b = K t_b, A_ab = t_a . u_b) or kept Cartesian
+// (M = 3), times ph = e^{ik r0} / 4pi.
+template <int M>
+BIELCC_D void write_block_f32(const AsmArgs& a, int i, int j, float a1r, float a1i, const float (&t)[6][2], float phr,
+                              float phi, const float (&ti)[2][3], const double* tj1, const double* tj2) {
+    const size_t dim = (size_t)M * a.n_cells;
+    const int sym[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+    float kr[6], ki[6];
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        const bool diag = q == 0 || q == 3 || q == 5;
+        kr[q] = diag ? t[q][0] + a1r : t[q][0];
+        ki[q] = diag ? t[q][1] + a1i : t[q][1];
+    }
+    float out[M][M][2];
+    if constexpr (M == 3) {
+#pragma unroll
+        for (int p = 0; p < 3; p++)
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                out[p][q][0] = kr[sym[p][q]] * phr - ki[sym[p][q]] * phi;
+                out[p][q][1] = kr[sym[p][q]] * phi + ki[sym[p][q]] * phr;
+            }
+    } else {
+        const float tb[2][3] = {{(float)tj1[0], (float)tj1[1], (float)tj1[2]},
+                                {(float)tj2[0], (float)tj2[1], (float)tj2[2]}};
+#pragma unroll
+        for (int b = 0; b < 2; b++) {
+            float ur[3], ui[3];
+#pragma unroll
+            for (int p = 0; p < 3; p++) {
+                ur[p] = kr[sym[p][0]] * tb[b][0] + kr[sym[p][1]] * tb[b][1] + kr[sym[p][2]] * tb[b][2];
+                ui[p] = ki[sym[p][0]] * tb[b][0] + ki[sym[p][1]] * tb[b][1] + ki[sym[p][2]] * tb[b][2];
+            }
+#pragma unroll
+            for (int aa = 0; aa < 2; aa++) {
+                const float vr = ti[aa][0] * ur[0] + ti[aa][1] * ur[1] + ti[aa][2] * ur[2];
+                const float vi = ti[aa][0] * ui[0] + ti[aa][1] * ui[1] + ti[aa][2] * ui[2];
+                out[aa][b][0] = vr * phr - vi * phi;
+                out[aa][b][1] = vr * phi + vi * phr;
+            }
+        }
+    }
+#pragma unroll
+    for (int aa = 0; aa < M; aa++) {
+        const size_t off = ((size_t)i * M + aa) * dim + (size_t)j * M;
+        if (a.c64) {
+            float2* dst = reinterpret_cast<float2*>(a.A) + off;
+#pragma unroll
+            for (int b = 0; b < M; b++) dst[b] = make_float2(out[aa][b][0], out[aa][b][1]);
+        } else {
+            double2* dst = reinterpret_cast<double2*>(a.A) + off;
+#pragma unroll
+            for (int b = 0; b < M; b++) dst[b] = make_double2(out[aa][b][0], out[aa][b][1]);
+        }
+    }
+}
+
 BIELCC_D void write_block(const AsmArgs& a, int i, int j, const double (&Kr)[3][3], const double (&Ki)[3][3],
                           const double* ti1, const double* ti2, const double* tj1, const double* tj2) {
     if (a.m == 2) write_block_m<2>(a, i, j, Kr, Ki, ti1, ti2, tj1, tj2);
     else write_block_m<3>(a, i, j, Kr, Ki, ti1, ti2, tj1, tj2);
 }
 
+// Minimum resident CTAs per SM asked of the real-k mixed far kernel (0: the
+// compiler's own register choice, which the other variants keep). 5 gives 96
+// registers without spills (20,480 triangles: 65.0 -> 62.4 ms).
+#ifndef BIELCC_ASM_MINB
+#define BIELCC_ASM_MINB 5
+#endif
 template <bool CK, bool MIXED>
-__global__ void __launch_bounds__(kAsmThreads) assemble_far_kernel(AsmArgs a) {
+__global__ void __launch_bounds__(kAsmThreads, (!CK && MIXED) ? BIELCC_ASM_MINB : 0) assemble_far_kernel(AsmArgs a) {
     using NodeT = typename std::conditional<MIXED, float4, double4>::type;
     __shared__ __align__(16) NodeT s_nodes[kAsmStageNodes];
     __shared__ float s_yy[MIXED ? kAsmStageNodes : 1];  // |y - centre|^2 of the staged nodes (mixed form)
@@ -123,6 +189,9 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_far_kernel(AsmArgs a) {
     bool far = false;
     PairF32 pf{};
     const KF32 kf = KF32::make(a.k.re, a.k.im);
+    // the row cell's tangents in FP32 (mixed-form block projection)
+    const float tif[2][3] = {{(float)gi.t1[0], (float)gi.t1[1], (float)gi.t1[2]},
+                             {(float)gi.t2[0], (float)gi.t2[1], (float)gi.t2[2]}};
     double P0r = 1., P0i = 0.;
     int mode = 0;  // phase polynomial of the current cell (farnode.cuh phase_mode)
     bool split64 = false;
@@ -246,18 +315,24 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_far_kernel(AsmArgs a) {
                     }
                 }
                 if (k0 + kc == nn && far) {
-                    if constexpr (MIXED && !CK) finish_real_k<F>(a1r, a1i, t);
-                    // K = (A1 I + T) * P0 / 4pi
-                    const int ti[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
-                    double Kr[3][3], Ki[3][3];
-                    for (int p = 0; p < 3; p++)
-                        for (int q = 0; q < 3; q++) {
-                            double vr = (double)t[ti[p][q]][0] + (p == q ? (double)a1r : 0.);
-                            double vi = (double)t[ti[p][q]][1] + (p == q ? (double)a1i : 0.);
-                            Kr[p][q] = (vr * P0r - vi * P0i) * kInvFourPi;
-                            Ki[p][q] = (vr * P0i + vi * P0r) * kInvFourPi;
-                        }
-                    write_block(a, i, c0 + cc, Kr, Ki, gi.t1, gi.t2, gj.t1, gj.t2);
+                    if constexpr (MIXED) {
+                        if constexpr (!CK) finish_real_k<F>(a1r, a1i, t);
+                        const float phr = (float)(P0r * kInvFourPi), phi = (float)(P0i * kInvFourPi);
+                        if (a.m == 2) write_block_f32<2>(a, i, c0 + cc, a1r, a1i, t, phr, phi, tif, gj.t1, gj.t2);
+                        else write_block_f32<3>(a, i, c0 + cc, a1r, a1i, t, phr, phi, tif, gj.t1, gj.t2);
+                    } else {
+                        // K = (A1 I + T) * P0 / 4pi
+                        const int ti[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+                        double Kr[3][3], Ki[3][3];
+                        for (int p = 0; p < 3; p++)
+                            for (int q = 0; q < 3; q++) {
+                                double vr = (double)t[ti[p][q]][0] + (p == q ? (double)a1r : 0.);
+                                double vi = (double)t[ti[p][q]][1] + (p == q ? (double)a1i : 0.);
+                                Kr[p][q] = (vr * P0r - vi * P0i) * kInvFourPi;
+                                Ki[p][q] = (vr * P0i + vi * P0r) * kInvFourPi;
+                            }
+                        write_block(a, i, c0 + cc, Kr, Ki, gi.t1, gi.t2, gj.t1, gj.t2);
+                    }
                 }
             }
         }
