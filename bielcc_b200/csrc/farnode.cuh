@@ -75,18 +75,25 @@ struct KF32 {
     }
 };
 
-// e^{i t} in FP64 for |t| <= 0.5 from its Taylor series (sin to t^13, cos to
-// t^14: truncation below 3e-17).
+// e^{i t} in FP64 from its Taylor series; the length follows a bound on |t|
+// (a template level, uniform over a cell): TD 0 |t| <= 0.5 (sin to t^13, cos
+// to t^14), TD 1 |t| <= 0.25 (t^11, t^12), TD 2 |t| <= 0.125 (t^9, t^10);
+// truncation below 3e-17 in each case. Coefficients are +-1/n!.
+template <int TD = 0>
 BIELCC_D void sincos_taylor64(double t, double* s, double* c) {
     double t2 = t * t;
-    double ps = fma(t2, -1.6059043836821613e-10, 2.5052108385441720e-08);
-    ps = fma(t2, ps, -2.7557319223985893e-06);
+    double ps;
+    if (TD == 0) ps = fma(fma(t2, -1.6059043836821613e-10, 2.5052108385441720e-08), t2, -2.7557319223985893e-06);
+    else if (TD == 1) ps = fma(t2, 2.5052108385441720e-08, -2.7557319223985893e-06);
+    else ps = -2.7557319223985893e-06;
     ps = fma(t2, ps, 1.9841269841269841e-04);
     ps = fma(t2, ps, -8.3333333333333333e-03);
     ps = fma(t2, ps, 1.6666666666666667e-01);
     *s = t - t * t2 * ps;
-    double pc = fma(t2, 1.1470745597729725e-11, -2.0876756987868099e-09);
-    pc = fma(t2, pc, 2.7557319223985891e-07);
+    double pc;
+    if (TD == 0) pc = fma(fma(t2, 1.1470745597729725e-11, -2.0876756987868099e-09), t2, 2.7557319223985891e-07);
+    else if (TD == 1) pc = fma(t2, -2.0876756987868099e-09, 2.7557319223985891e-07);
+    else pc = 2.7557319223985891e-07;
     pc = fma(t2, pc, -2.4801587301587302e-05);
     pc = fma(t2, pc, 1.3888888888888889e-03);
     pc = fma(t2, pc, -4.1666666666666667e-02);
@@ -100,7 +107,7 @@ BIELCC_D void sincos_taylor64(double t, double* s, double* c) {
 // SPLIT: the phase is taken relative to r0 = |x - centre| (the moments are
 // multiplied by e^{ik r0} once per cell) and e^{ik (r - r0)} comes from the
 // Taylor series; otherwise e^{ikr} from sincos per node.
-template <bool CK, bool SPLIT>
+template <bool CK, bool SPLIT, int TD = 0>
 BIELCC_D void far_node_f64(Moments<double>& m, double dx, double dy, double dz, double w, cplx k, double k2r,
                            double k2i, double r0) {
     double r2 = dx * dx + dy * dy + dz * dz;
@@ -108,7 +115,7 @@ BIELCC_D void far_node_f64(Moments<double>& m, double dx, double dy, double dz, 
     double r = r2 * ir;
     double s, c;
     if (SPLIT) {
-        sincos_taylor64(k.re * (r - r0), &s, &c);
+        sincos_taylor64<TD>(k.re * (r - r0), &s, &c);
     } else {
         sincos(k.re * r, &s, &c);
         if (CK) {

@@ -174,6 +174,7 @@ __global__ void BIELCC_FAR_BOUNDS(NRHS, CK, MIXED) far_kernel(FarArgs a) {
     double P0r = 1.0, P0i = 0.0, r0d = 0.0;
     int mode = 0;
     bool split64 = false;
+    int td64 = 0;  // Taylor length of the FP64 phase split (farnode.cuh sincos_taylor64)
 
     for (int c0 = cb; c0 < ce; c0 += cps) {
         const int nc = min(cps, ce - c0);
@@ -229,7 +230,9 @@ __global__ void BIELCC_FAR_BOUNDS(NRHS, CK, MIXED) far_kernel(FarArgs a) {
                         nbits = 0;
                     }
                     if (!MIXED && far) {  // FP64 phase split when the cell's phase range is small
-                        split64 = !CK && fabs(a.k.re) * s_rho64[cc] <= 0.5;
+                        const double th64 = fabs(a.k.re) * s_rho64[cc];
+                        split64 = !CK && th64 <= 0.5;
+                        td64 = th64 <= 0.125 ? 2 : (th64 <= 0.25 ? 1 : 0);
                         r0d = d;
                         if (split64) {
                             double sn, cs;
@@ -271,12 +274,17 @@ __global__ void BIELCC_FAR_BOUNDS(NRHS, CK, MIXED) far_kernel(FarArgs a) {
 #undef BIELCC_NODE_LOOP
                     } else {
                         if (split64) {
-#pragma unroll 2
-                            for (int i = 0; i < kc; i++) {
-                                double4 v = nd[i];
-                                far_node_f64<CK, true>(m, x[0] - v.x, x[1] - v.y, x[2] - v.z, v.w, a.k, k2r, k2i,
-                                                       r0d);
+#define BIELCC_NODE64_LOOP(TD_)                                                                       \
+    _Pragma("unroll 2") for (int i = 0; i < kc; i++) {                                                 \
+        const double4 v = nd[i];                                                                       \
+        far_node_f64<CK, true, TD_>(m, x[0] - v.x, x[1] - v.y, x[2] - v.z, v.w, a.k, k2r, k2i, r0d); \
+    }
+                            switch (td64) {
+                                case 2: BIELCC_NODE64_LOOP(2) break;
+                                case 1: BIELCC_NODE64_LOOP(1) break;
+                                default: BIELCC_NODE64_LOOP(0) break;
                             }
+#undef BIELCC_NODE64_LOOP
                         } else {
 #pragma unroll 2
                             for (int i = 0; i < kc; i++) {
