@@ -59,7 +59,7 @@ def parse():
     ap.add_argument("--serve-load", type=float, default=0.9, help="arrival rate / offline capacity")
     ap.add_argument("--serve-slots", type=int, default=4)
     ap.add_argument("--serve-max-batch", type=int, default=64)
-    ap.add_argument("--serve-reserve-gb", type=int, default=16, help="device memory the server maps up front")
+    ap.add_argument("--serve-reserve-gb", type=int, default=32, help="device memory the server maps up front")
     ap.add_argument("--serve-persistent", action="store_true", help="persistent far-kernel CTAs in served batches")
     return ap.parse_args()
 
