@@ -219,6 +219,18 @@ BIELCC_D void eval_cplx(int id, const double* x, const double* y, const DKP& p, 
     }
 }
 
+// F_SimplePot_H and F_GradSimplePot_H at one node together: the same r, t and
+// e^{ikr}, each output by the expression eval_cplx uses for it alone.
+BIELCC_D void eval_pot_and_grad(const double* x, const double* y, const DKP& p, cplx* f, cplx* g) {
+    double r = dist3(x, y);
+    double t = r / p.smoothR;
+    cplx e = eikr(r, p.k);
+    f[0] = e * w_pot(t, r, p.smoothR);
+    double w = w_grad(t, r, p.smoothR);
+    cplx ikr_m1 = mk(-r * p.k.im - 1., r * p.k.re);
+    for (int i = 0; i < 3; i++) g[i] = ((x[i] - y[i]) * e) * ikr_m1 * w;
+}
+
 template <typename T> struct Eval;
 template <> struct Eval<double> {
     BIELCC_D static void run(int id, const double* x, const double* y, const DKP& p, double* o) { eval_real(id, x, y, p, o); }
@@ -343,6 +355,55 @@ BIELCC_D void integral_cell(int id, const double* x, const DCell& c, DKP& kp, in
                             double eps, T* res) {
     if (c.nv == 4) integral_quad<T>(id, x, c.v, kp, idim, n_start, p_max, eps, res);
     else integral_tri<T>(id, x, c.v, kp, idim, n_start, p_max, eps, res);
+}
+
+// One pass (p_max = 1) of IntegralUniversalPnt for F_SimplePot_H (F) and
+// F_GradSimplePot_H (G) over one cell with the same smoothing radius: the
+// nodes, weights and accumulation order of integral_quad / integral_tri, with
+// each node evaluated once for both integrands.
+BIELCC_D void integral_cell_pot_and_grad(const double* x, const DCell& c, const DKP& kp, int n, cplx* F, cplx* G) {
+    F[0] = mk(0, 0);
+    for (int g = 0; g < 3; g++) G[g] = mk(0, 0);
+    cplx f[1], gg[3];
+    if (c.nv == 4) {
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                double y[3], s;
+                quad_node(c.v, i, j, n, y, &s);
+                eval_pot_and_grad(x, y, kp, f, gg);
+                F[0] = madd(F[0], f[0], s);
+                for (int g = 0; g < 3; g++) G[g] = madd(G[g], gg[g], s);
+            }
+        return;
+    }
+    const double(*cv)[3] = c.v;
+    double area = tri_area(cv[0], cv[1], cv[2]);
+    double pv[3], qv[3], rv[3];
+    for (int k = 0; k < 3; k++) {
+        pv[k] = (cv[1][k] - cv[0][k]) / n;
+        qv[k] = (cv[2][k] - cv[0][k]) / n;
+        rv[k] = (cv[2][k] - cv[1][k]) / n;
+    }
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < n - i; j++) {
+            double B[3], y[3];
+            for (int k = 0; k < 3; k++) {
+                B[k] = cv[0][k] + (i + 1) * pv[k] + j * qv[k];
+                double A = B[k] - pv[k];
+                y[k] = (B[k] + A + (A + qv[k])) / 3.0;
+            }
+            eval_pot_and_grad(x, y, kp, f, gg);
+            F[0] = madd(F[0], f[0], 1.0);
+            for (int g = 0; g < 3; g++) G[g] = madd(G[g], gg[g], 1.0);
+            if (j < n - 1 - i) {
+                for (int k = 0; k < 3; k++) y[k] = (B[k] + (B[k] + rv[k]) + (B[k] + qv[k])) / 3.0;
+                eval_pot_and_grad(x, y, kp, f, gg);
+                F[0] = madd(F[0], f[0], 1.0);
+                for (int g = 0; g < 3; g++) G[g] = madd(G[g], gg[g], 1.0);
+            }
+        }
+    F[0] = F[0] * area / (double)n / (double)n;
+    for (int g = 0; g < 3; g++) G[g] = G[g] * area / (double)n / (double)n;
 }
 
 // IntegralUniversalSegPnt (integral_universal_seg.h:38-98).
@@ -661,6 +722,30 @@ BIELCC_D void R_near_dev(const cplx* j, const double* x, const DCell& c, const D
 // R_Rot_Smooth (R.h:46-61) = g x J.
 BIELCC_D void near_pair_moments(const double* x, const DCell& cl, cplx k, const DNP& np, cplx* o) {
     double dm = cell_diam(cl);
+    if (np.p_max == 1) {
+        // one quadrature pass for both surface integrals: K_RotRot_Near_Smooth's
+        // int F (K.h:51-67) and R_Rot_Smooth's int grad F (R.h:46-61) start from
+        // the same smoothing radius rs diam / n_start, and without refinement
+        // their different smoothRMin never applies
+        DKP pS;
+        dkp_zero(pS);
+        pS.smoothR = np.rs * dm / np.n_start;
+        pS.k = k;
+        cplx sF[1], g[3];
+        integral_cell_pot_and_grad(x, cl, pS, np.n_start, sF, g);
+        o[0] = sF[0] * k * k / kFourPi;
+        DKP pG;
+        dkp_zero(pG);
+        pG.smoothR = np.rs_seg * dm / np.n_start_seg;
+        pG.smoothRMin = np.eps;
+        pG.k = k;
+        cplx M[3][3], dummy[3];
+        K0_dev(F_GRADSIMPLEPOT_H, nullptr, x, cl, pG, np.n_start_seg, np.p_max_seg, np.eps, dummy, M);
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) o[1 + 3 * a + b] = M[a][b] / kFourPi;
+        for (int a = 0; a < 3; a++) o[10 + a] = g[a] / kFourPi;
+        return;
+    }
     // surface part of K_RotRot_Near_Smooth (K.h:51-67)
     DKP pF;
     dkp_zero(pF);
