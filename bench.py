@@ -39,6 +39,10 @@ UNIT = "pairs/s"
 FLOPS_PER_NODE = 130
 NODES_PER_PAIR = 64
 FLOPS_PER_FAR_PAIR = FLOPS_PER_NODE * NODES_PER_PAIR
+# Algorithmic flops of one moment contraction per (point, cell, RHS) in the
+# batched kernel: (A1 I + T) J is 9 complex multiply-adds (72 flops), G x J
+# three components of two complex products and a difference (42 flops).
+FLOPS_PER_RHS_CONTRACTION = 114
 
 
 def parse():
@@ -188,7 +192,7 @@ def run_reference(args, ws, rank):
 
 
 # ---------------------------------------------------------------- batched leg
-def run_batched(args, ctx, torch, dev, stream, flush, fp64_single_rhs_value):
+def run_batched(args, ctx, torch, dev, stream, flush, fp64_single_rhs_value, peak32):
     """256 meshes of uneven sizes (spheroids, rounded cubes, tori; 200-20,000
     cells log-uniform; k log-uniform in [0.5, 20]; 1-64 PO right-hand sides;
     2,000 far points each, seed 3) in one persistent launch, mixed precision,
@@ -267,11 +271,17 @@ def run_batched(args, ctx, torch, dev, stream, flush, fp64_single_rhs_value):
     for m, _, _ in keep:
         m.close()
     value = rhs_pairs / (ms * 1e-3)
+    # whole batch (far kernel, near pairs, finalize) against the FP32 FMA peak
+    achieved = (geo_pairs * FLOPS_PER_FAR_PAIR + rhs_pairs * FLOPS_PER_RHS_CONTRACTION) / (ms * 1e-3) / 1e12
+    roofline = {"bound": "fp32 CUDA-core pipe", "kernel": "batch_far_kernel<mixed> (whole batch, one launch)",
+                "achieved": achieved, "peak": peak32, "unit": "TFLOP/s", "frac": achieved / peak32,
+                "flops": f"{FLOPS_PER_FAR_PAIR} per (point, cell) quadrature + {FLOPS_PER_RHS_CONTRACTION} per "
+                         f"(point, cell, RHS) contraction", "peak_source": "measured FMA loop (bielcc_measure_fma_peak)"}
     return {"workload": f"{len(jobs_np)} meshes (spheroids, rounded cubes, tori), 200-20000 cells, k 0.5-20, "
                         f"1-64 PO RHS, 2000 far points each, seed 3",
             "value": value, "unit": "(point, cell, RHS) pairs/s", "geometry_pairs_per_s": geo_pairs / (ms * 1e-3),
             "ms_per_step": ms, "steps": steps, "rhs_pairs_per_step": rhs_pairs, "geometry_pairs_per_step": geo_pairs,
-            "rel_l2_vs_fp64": (num / den) ** 0.5, "autotuned_item_cost": item_cost,
+            "rel_l2_vs_fp64": (num / den) ** 0.5, "autotuned_item_cost": item_cost, "roofline": roofline,
             "over_plain_fp64_single_rhs": value / fp64_single_rhs_value,
             "sequential_single_job_ms": ms_seq, "batched_over_sequential": ms_seq / ms,
             "graph_replay_ms": ms_graph, "graph_replay_value": rhs_pairs / (ms_graph * 1e-3), "gpu_launches_per_step":
@@ -644,7 +654,7 @@ def run_ours(args, ws, rank, local):
 
     batched = None
     if not args.no_batched:
-        batched = run_batched(args, ctx, torch, dev, stream, flush, value64)
+        batched = run_batched(args, ctx, torch, dev, stream, flush, value64, peak32)
     assembly = None
     if not args.no_assembly:
         assembly = run_assembly(args, ctx, torch, dev, stream, flush)
