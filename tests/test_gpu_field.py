@@ -213,3 +213,30 @@ def test_context_created_again_after_destroy():
         m.close()
         ctx.close()
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+def test_zero_wavenumber_static_limit(gctx):
+    """k = 0 (the static limit): the real-k far node folds k into its phase
+    denominator and the FP64 split takes its shortest Taylor level; both forms
+    match the oracle, single-job and batched."""
+    cells = W.uv_sphere(8, 16)
+    J = W.po_currents(cells, 2.0, directions=2, seed=11)
+    rng = np.random.default_rng(11)
+    pts = np.concatenate([W.shell_points(150, 2.0, 4.0, rng), W.near_points(cells, 20, 0.02, 0.2, rng)])
+    m = gctx.mesh(cells)
+    Eo, Ho = oracle.field_EH(cells, J, 0.0, pts)
+    assert np.all(np.isfinite(Eo)) and np.linalg.norm(Eo) > 0
+    for precision, tol in (("fp64", TOL_FP64), ("mixed", TOL_MIXED)):
+        E, H, _ = gctx.field_EH(m, J, 0.0, pts, precision=precision)
+        assert rel_l2(E, Eo) < tol and rel_l2(H, Ho) < tol
+    torch = pytest.importorskip("torch")
+    dev = torch.device("cuda:0")
+    Jd = torch.from_numpy(np.ascontiguousarray(J)).to(dev)
+    Pd = torch.from_numpy(np.ascontiguousarray(pts)).to(dev)
+    Ed = torch.zeros((2, len(pts), 3), dtype=torch.complex128, device=dev)
+    Hd = torch.zeros_like(Ed)
+    jobs = gctx.make_jobs([dict(mesh=m, n_rhs=2, n_pts=len(pts), J=Jd.data_ptr(), pts=Pd.data_ptr(), E=Ed.data_ptr(),
+                                H=Hd.data_ptr(), k=0.0)])
+    gctx.field_EH_batch(jobs, precision="mixed", stream=torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert rel_l2(Ed.cpu().numpy(), Eo) < TOL_MIXED and rel_l2(Hd.cpu().numpy(), Ho) < TOL_MIXED
