@@ -55,6 +55,12 @@ constexpr int kFarThreads = BIELCC_FAR_THREADS;
 #define BIELCC_FAR_STR(x) #x
 #define BIELCC_FAR_PRAGMA(x) _Pragma(BIELCC_FAR_STR(unroll x))
 #define BIELCC_FAR_UNROLL_PRAGMA BIELCC_FAR_PRAGMA(BIELCC_FAR_UNROLL)
+// Unrolling of the FP64 split node loop (FP64 step on 8192 cells x 20,000
+// points: x1 57.7, x2 56.4, x4 54.6, x8 53.3, x16 52.8 ms; registers 152-166).
+#ifndef BIELCC_FAR64_UNROLL
+#define BIELCC_FAR64_UNROLL 16
+#endif
+#define BIELCC_FAR64_UNROLL_PRAGMA BIELCC_FAR_PRAGMA(BIELCC_FAR64_UNROLL)
 // Minimum resident CTAs per SM asked of the 1-RHS real-k mixed far kernel
 // (0: none, the compiler's own register choice, which the other variants
 // keep). 5 caps it at 96 registers without spills: 20 warps per SM instead of
@@ -283,7 +289,7 @@ __global__ void BIELCC_FAR_BOUNDS(NRHS, CK, MIXED) far_kernel(FarArgs a) {
                     } else {
                         if (split64) {
 #define BIELCC_NODE64_LOOP(TD_)                                                                       \
-    _Pragma("unroll 2") for (int i = 0; i < kc; i++) {                                                 \
+    BIELCC_FAR64_UNROLL_PRAGMA for (int i = 0; i < kc; i++) {                                          \
         const double4 v = nd[i];                                                                       \
         far_node_f64<CK, true, TD_>(m, x[0] - v.x, x[1] - v.y, x[2] - v.z, v.w, a.k, k2r, k2i, r0d); \
     }
