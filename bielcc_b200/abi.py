@@ -5,7 +5,7 @@ shared object exporting functions with these argument layouts.
 """
 import ctypes as C
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 OK = 0
 ERR_ARG = -1
@@ -59,6 +59,7 @@ F_DOUBLEPOT_H = 9
 F_N_DOUBLEPOT_H = 10
 F_ROTROTSIMPLEPOT_H = 11
 F_ONE = 12
+F_PLANEWAVE_E = 13
 INTEGRANDS = {
     F_SIMPLEPOT_L: ("F_SimplePot_L", 1, False),
     F_GRADSIMPLEPOT_L: ("F_GradSimplePot_L", 3, False),
@@ -73,7 +74,13 @@ INTEGRANDS = {
     F_N_DOUBLEPOT_H: ("nF_DoublePot_H", 3, True),
     F_ROTROTSIMPLEPOT_H: ("F_RotRotSimplePot_H", 3, True),
     F_ONE: ("F_One", 1, False),
+    F_PLANEWAVE_E: ("PlaneWaveFieldE", 3, True),
 }
+# integrands of one point, F(x): the form IntegralUniversal and the segment
+# F(x) overload take (the rest are pair integrands F(x, y))
+FX_INTEGRANDS = (F_ONE, F_PLANEWAVE_E)
+# integrands the *_pnt and K0 forms take: the pair integrands and F = 1
+PAIR_INTEGRANDS = tuple(i for i in INTEGRANDS if i != F_PLANEWAVE_E)
 
 
 class NumParam(C.Structure):
@@ -124,6 +131,7 @@ class KernelParam(C.Structure):
         ("current", (C.c_double * 2) * 3),
         ("vec_dbl", C.c_double * 3),
         ("n", C.c_double * 3),
+        ("e0", C.c_double * 3),
     ]
 
 
@@ -213,7 +221,7 @@ class Stats(C.Structure):
     ]
 
 
-def kernelparam_array(n, smoothR=0.0, smoothRMin=0.0, k=0.0, current=None, vec_dbl=None, normal=None):
+def kernelparam_array(n, smoothR=0.0, smoothRMin=0.0, k=0.0, current=None, vec_dbl=None, normal=None, e0=None):
     """Array of n KernelParam records; array-valued arguments are per pair."""
     import numpy as np
 
@@ -224,6 +232,7 @@ def kernelparam_array(n, smoothR=0.0, smoothRMin=0.0, k=0.0, current=None, vec_d
     cur = None if current is None else np.broadcast_to(np.asarray(current, dtype=np.complex128), (n, 3))
     vd = None if vec_dbl is None else np.broadcast_to(np.asarray(vec_dbl, dtype=np.float64), (n, 3))
     nn = None if normal is None else np.broadcast_to(np.asarray(normal, dtype=np.float64), (n, 3))
+    ee = None if e0 is None else np.broadcast_to(np.asarray(e0, dtype=np.float64), (n, 3))
     for i in range(n):
         a = arr[i]
         a.smoothR = float(sR[i])
@@ -238,6 +247,8 @@ def kernelparam_array(n, smoothR=0.0, smoothRMin=0.0, k=0.0, current=None, vec_d
                 a.vec_dbl[g] = float(vd[i, g])
             if nn is not None:
                 a.n[g] = float(nn[i, g])
+            if ee is not None:
+                a.e0[g] = float(ee[i, g])
     return arr
 
 
@@ -261,6 +272,8 @@ def declare_common(lib, prefix):
     d("pair_op", ctx + [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, C.c_double, C.c_double, C.POINTER(NumParam), _dp])
     d("integral_pnt", ctx + [C.c_int, C.c_int, C.c_int, _dp, _dp, C.POINTER(KernelParam), C.c_int, C.c_int, C.c_double, _dp])
     d("integral_seg_pnt", ctx + [C.c_int, C.c_int, _dp, _dp, _dp, C.POINTER(KernelParam), C.c_int, C.c_int, C.c_double, _dp])
+    d("integral", ctx + [C.c_int, C.c_int, C.c_int, _dp, C.POINTER(KernelParam), C.c_int, C.c_int, C.c_double, _dp])
+    d("integral_seg", ctx + [C.c_int, C.c_int, _dp, _dp, C.POINTER(KernelParam), C.c_int, C.c_int, C.c_double, _dp])
     d("k0", ctx + [C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, C.POINTER(KernelParam), C.c_int, C.c_int, C.c_double, _dp])
     d("integral_1divr", ctx + [C.c_int, C.c_int, _dp, _dp, _dp])
     d("integral_grad1divr_seg", ctx + [C.c_int, _dp, _dp, _dp, _dp])

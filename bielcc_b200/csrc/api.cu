@@ -1142,12 +1142,66 @@ int bielcc_integrand_info(int integrand, int* idim, int* is_complex) {
     return BIELCC_OK;
 }
 
+// Pair integrands F(x, y), and F = 1, for the *_pnt forms.
+static int check_pair_integrand(int integrand) {
+    if (integrand < 0 || integrand >= BIELCC_F_COUNT) return set_error(BIELCC_ERR_ARG, "unknown integrand %d", integrand);
+    if (integrand_one_point(integrand) && integrand != BIELCC_F_ONE)
+        return set_error(BIELCC_ERR_ARG, "integrand %d is a function of one point: use bielcc_integral", integrand);
+    return BIELCC_OK;
+}
+
+// One-point integrands F(x) for IntegralUniversal and the segment F(x) overload.
+static int check_one_point_integrand(int integrand) {
+    if (integrand < 0 || integrand >= BIELCC_F_COUNT || !integrand_one_point(integrand))
+        return set_error(BIELCC_ERR_ARG, "integrand %d is not a function of one point F(x)", integrand);
+    return BIELCC_OK;
+}
+
+int bielcc_integral(bielcc_ctx ctx, int integrand, int n_vert, int n_cells, const double* cells,
+                    bielcc_kernelparam* kp, int n_start, int p_max, double eps, double* res) {
+    TRY(enter(ctx));
+    TRY(check_nv(n_vert));
+    TRY(check_quad_params(n_start, p_max));
+    TRY(check_one_point_integrand(integrand));
+    if (n_cells < 0 || (n_cells > 0 && (!cells || !kp || !res))) return set_error(BIELCC_ERR_ARG, "null buffer");
+    if (n_cells == 0) return BIELCC_OK;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    size_t N = n_cells;
+    int idim = integrand_dim(integrand);
+    size_t ob = N * idim * (integrand_complex(integrand) ? 16 : 8);
+    return run_batch(ctx, {{cells, N * n_vert * 24}, {kp, N * sizeof(KParamDev)}}, res, ob,
+                     [&](std::vector<const void*>& d, void* o, cudaStream_t s) {
+                         return launch_integral_pnt(integrand, n_vert, n_cells, (const double*)d[0], nullptr,
+                                                    (KParamDev*)d[1], n_start, p_max, eps, (double*)o, s);
+                     },
+                     1, kp);
+}
+
+int bielcc_integral_seg(bielcc_ctx ctx, int integrand, int n_segs, const double* a, const double* b,
+                        bielcc_kernelparam* kp, int n_start, int p_max, double eps, double* res) {
+    TRY(enter(ctx));
+    TRY(check_quad_params(n_start, p_max));
+    TRY(check_one_point_integrand(integrand));
+    if (n_segs < 0 || (n_segs > 0 && (!a || !b || !kp || !res))) return set_error(BIELCC_ERR_ARG, "null buffer");
+    if (n_segs == 0) return BIELCC_OK;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    size_t N = n_segs;
+    int idim = integrand_dim(integrand);
+    size_t ob = N * idim * (integrand_complex(integrand) ? 16 : 8);
+    return run_batch(ctx, {{a, N * 24}, {b, N * 24}, {kp, N * sizeof(KParamDev)}}, res, ob,
+                     [&](std::vector<const void*>& d, void* o, cudaStream_t s) {
+                         return launch_integral_seg(integrand, n_segs, (const double*)d[0], (const double*)d[1],
+                                                    nullptr, (KParamDev*)d[2], n_start, p_max, eps, (double*)o, s);
+                     },
+                     2, kp);
+}
+
 int bielcc_integral_pnt(bielcc_ctx ctx, int integrand, int n_vert, int n_pairs, const double* cells, const double* x,
                         bielcc_kernelparam* kp, int n_start, int p_max, double eps, double* res) {
     TRY(enter(ctx));
     TRY(check_nv(n_vert));
     TRY(check_quad_params(n_start, p_max));
-    if (integrand < 0 || integrand >= BIELCC_F_COUNT) return set_error(BIELCC_ERR_ARG, "unknown integrand %d", integrand);
+    TRY(check_pair_integrand(integrand));
     if (n_pairs < 0 || (n_pairs > 0 && (!cells || !x || !kp || !res))) return set_error(BIELCC_ERR_ARG, "null buffer");
     if (n_pairs == 0) return BIELCC_OK;
     static_assert(sizeof(bielcc_kernelparam) == sizeof(KParamDev), "kernel-parameter layouts differ");
@@ -1169,7 +1223,7 @@ int bielcc_integral_seg_pnt(bielcc_ctx ctx, int integrand, int n_pairs, const do
                             double* res) {
     TRY(enter(ctx));
     TRY(check_quad_params(n_start, p_max));
-    if (integrand < 0 || integrand >= BIELCC_F_COUNT) return set_error(BIELCC_ERR_ARG, "unknown integrand %d", integrand);
+    TRY(check_pair_integrand(integrand));
     if (n_pairs < 0 || (n_pairs > 0 && (!a || !b || !x || !kp || !res))) return set_error(BIELCC_ERR_ARG, "null buffer");
     if (n_pairs == 0) return BIELCC_OK;
     std::lock_guard<std::mutex> g(ctx->mu);
@@ -1191,7 +1245,8 @@ int bielcc_k0(bielcc_ctx ctx, int integrand, int common, int n_vert, int n_pairs
     TRY(enter(ctx));
     TRY(check_nv(n_vert));
     TRY(check_quad_params(n_start_seg, p_max_seg));
-    if (integrand < 0 || integrand >= BIELCC_F_COUNT || !integrand_complex(integrand) || integrand_dim(integrand) != 3)
+    if (integrand < 0 || integrand >= BIELCC_F_COUNT || integrand_one_point(integrand) ||
+        !integrand_complex(integrand) || integrand_dim(integrand) != 3)
         return set_error(BIELCC_ERR_ARG, "K0 needs a complex 3-vector integrand, got %d", integrand);
     if (n_pairs < 0 || (n_pairs > 0 && (!cells || !x || !kp || !res || (!common && !j))))
         return set_error(BIELCC_ERR_ARG, "null buffer");

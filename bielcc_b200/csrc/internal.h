@@ -97,11 +97,13 @@ struct KParamDev {
     double current[3][2];
     double vec_dbl[3];
     double n[3];
+    double e0[3];
 };
 cudaError_t launch_integral_pnt(int integrand, int nv, int n, const double* cells, const double* x,
                                 KParamDev* kp, int n_start, int p_max, double eps, double* res, cudaStream_t s);
 cudaError_t launch_integral_seg(int integrand, int n, const double* a, const double* b, const double* x,
                                 KParamDev* kp, int n_start, int p_max, double eps, double* res, cudaStream_t s);
+// x-free forms: x == nullptr (IntegralUniversal / the segment F(x) overload)
 cudaError_t launch_k0(int integrand, int common, int nv, int n, const double* cells, const double* x, const double* j,
                       KParamDev* kp, int n_seg, int p_seg, double eps, double* res, cudaStream_t s);
 cudaError_t launch_analytic(int which, int nv, int n, const double* cells_or_a, const double* b, const double* x,

@@ -21,7 +21,6 @@
 //     threads) race on the array: callers must order them.
 #include <cstdio>
 #include <cstring>
-#include <mutex>
 
 #include "../../include/bielcc_gpu.h"
 #include "internal.h"
@@ -34,33 +33,24 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[BIELCC_NOALLOC_
 
 namespace {
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-void* g_scratch_addr[kMaxDevices] = {};
-
 size_t al(size_t b) { return (b + 255) & ~(size_t)255; }
 
 // The message is returned by bielcc_last_error() on this thread.
 int fail(int code, const char* msg) { return set_api_error(code, msg); }
 
-// Device address of the scratch array for the current device. The first call
-// on each device looks it up (cudaGetSymbolAddress, current device); the host
-// symbol itself is only a stand-in and is never handed to a kernel.
+// Device address of the scratch array in the current context. The host symbol
+// is only a stand-in and is never handed to a kernel. The address is looked up
+// on every call rather than cached: after cudaDeviceReset, or under another
+// context on the same device, the module is loaded again and the array can
+// move, so a cached address could point at freed memory.
 int scratch_address(void** out) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
-        return fail(BIELCC_ERR_CUDA, "no current CUDA device");
-    std::lock_guard<std::mutex> g(g_mu);
-    if (!g_scratch_addr[dev]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
-            cudaGetLastError();
-            return fail(BIELCC_ERR_CUDA, "cudaGetSymbolAddress of the static scratch array failed");
-        }
-        g_scratch_addr[dev] = p;
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+        cudaGetLastError();
+        return fail(BIELCC_ERR_CUDA, "cudaGetSymbolAddress of the static scratch array failed");
     }
-    *out = g_scratch_addr[dev];
+    *out = p;
     return BIELCC_OK;
 }
 

@@ -26,6 +26,7 @@ struct DKP {
     cplx current[3];
     double vec_dbl[3];
     double n[3];
+    double e0[3];
 };
 
 BIELCC_D void dkp_zero(DKP& p) {
@@ -33,7 +34,7 @@ BIELCC_D void dkp_zero(DKP& p) {
     p.k = mk(0, 0);
     for (int i = 0; i < 3; i++) {
         p.current[i] = mk(0, 0);
-        p.vec_dbl[i] = p.n[i] = 0.;
+        p.vec_dbl[i] = p.n[i] = p.e0[i] = 0.;
     }
 }
 
@@ -98,8 +99,11 @@ BIELCC_D void edge_nu(const double* A, const double* B, const double* nrm, doubl
 enum Integrand {
     F_SIMPLEPOT_L = 0, F_GRADSIMPLEPOT_L, F_DOUBLEPOT_L, F_VECTORPOT_L, F_SIMPLEPOT_H, F_NU_SIMPLEPOT_H,
     F_SIMPLEPOT_HM1, F_GRADSIMPLEPOT_H, F_GRADSIMPLEPOT_HM1, F_DOUBLEPOT_H, F_N_DOUBLEPOT_H,
-    F_ROTROTSIMPLEPOT_H, F_ONE, F_COUNT
+    F_ROTROTSIMPLEPOT_H, F_ONE, F_PLANEWAVE_E, F_COUNT
 };
+// Integrands of one point, F(x) (IntegralUniversal, integral_universal.h:252-431):
+// evaluated at the node y, the pair point x unused.
+BIELCC_HD bool integrand_one_point(int id) { return id == F_ONE || id == F_PLANEWAVE_E; }
 BIELCC_HD int integrand_dim(int id) {
     return (id == F_SIMPLEPOT_L || id == F_DOUBLEPOT_L || id == F_SIMPLEPOT_H || id == F_SIMPLEPOT_HM1 ||
             id == F_DOUBLEPOT_H || id == F_ONE) ? 1 : 3;
@@ -197,6 +201,11 @@ BIELCC_D void eval_cplx(int id, const double* x, const double* y, const DKP& p, 
             cplx v = dot3(p.n, d) * eikr(r, p.k) * ikr_m1 * w_grad(t, r, p.smoothR);
             if (id == F_DOUBLEPOT_H) out[0] = v;
             else for (int i = 0; i < 3; i++) out[i] = p.n[i] * v;
+        } break;
+        case F_PLANEWAVE_E: {  // PlaneWaveFieldE (electrodynamics/incident_field.h:20-29), at the node y
+            double sn, cs;
+            sincos(dot3(p.vec_dbl, y), &sn, &cs);
+            for (int i = 0; i < 3; i++) out[i] = mk(p.e0[i] * cs, p.e0[i] * sn);
         } break;
         case F_ROTROTSIMPLEPOT_H: {  // kernel_lib.h:453-492
             if (r < kMachineZero) { out[0] = out[1] = out[2] = mk(0, 0); break; }

@@ -1,7 +1,9 @@
 // pairops.cu — batched per-pair kernels behind the drop-in operator calls:
 // one thread evaluates one reference call (K_RotRot_*, R_Rot_*, K0,
 // IntegralUniversalPnt, IntegralUniversalSegPnt, the analytic integrals) for
-// one (cell, x[, j]) triple, FP64, with the reference's adaptive quadrature.
+// one (cell, x[, j]) triple, FP64, with the reference's adaptive quadrature;
+// the x-free IntegralUniversal / segment F(x) forms run through the same
+// kernels with no point.
 #include "internal.h"
 #include "ops.cuh"
 
@@ -21,6 +23,7 @@ BIELCC_D void load_kp(DKP& p, const KParamDev& s) {
         p.current[i] = mk(s.current[i][0], s.current[i][1]);
         p.vec_dbl[i] = s.vec_dbl[i];
         p.n[i] = s.n[i];
+        p.e0[i] = s.e0[i];
     }
 }
 
@@ -46,7 +49,10 @@ __global__ void integral_pnt_kernel(int id, int nv, int n, const double* __restr
     load_cell(c, cells, nv, q);
     DKP p;
     load_kp(p, kp[q]);
-    double xp[3] = {x[3 * (size_t)q], x[3 * (size_t)q + 1], x[3 * (size_t)q + 2]};
+    // x == nullptr: IntegralUniversal, the F(x) form (the integrand reads the node only)
+    double xp[3] = {0., 0., 0.};
+    if (x)
+        for (int g = 0; g < 3; g++) xp[g] = x[3 * (size_t)q + g];
     int idim = integrand_dim(id);
     if (integrand_complex(id)) {
         cplx r[3];
@@ -68,7 +74,9 @@ __global__ void integral_seg_kernel(int id, int n, const double* __restrict__ a,
     DKP p;
     load_kp(p, kp[q]);
     size_t o = 3 * (size_t)q;
-    double A[3] = {a[o], a[o + 1], a[o + 2]}, B[3] = {b[o], b[o + 1], b[o + 2]}, X[3] = {x[o], x[o + 1], x[o + 2]};
+    double A[3] = {a[o], a[o + 1], a[o + 2]}, B[3] = {b[o], b[o + 1], b[o + 2]}, X[3] = {0., 0., 0.};
+    if (x)  // x == nullptr: the segment F(x) overload
+        for (int g = 0; g < 3; g++) X[g] = x[o + g];
     int idim = integrand_dim(id);
     if (integrand_complex(id)) {
         cplx r[3];

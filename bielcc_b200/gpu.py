@@ -405,6 +405,26 @@ class Context:
                                             p_max, eps, abi.dptr(res)))
         return res
 
+    def integral(self, integrand, cells, kp, n_start, p_max, eps):
+        """IntegralUniversal, the F(x) form (F_ONE or F_PLANEWAVE_E), per cell."""
+        cells = _c(cells)
+        n = cells.shape[0]
+        _, idim, cplx = abi.INTEGRANDS[integrand]
+        res = np.zeros((n, idim), np.complex128 if cplx else np.float64)
+        _check(_lib.bielcc_integral(self.h, integrand, cells.shape[1], n, abi.dptr(cells), kp, n_start, p_max, eps,
+                                    abi.dptr(res)))
+        return res
+
+    def integral_seg(self, integrand, a, b, kp, n_start, p_max, eps):
+        """IntegralUniversalSegPnt, the F(x) overload, per segment [a, b]."""
+        a, b = _c(a), _c(b)
+        n = a.shape[0]
+        _, idim, cplx = abi.INTEGRANDS[integrand]
+        res = np.zeros((n, idim), np.complex128 if cplx else np.float64)
+        _check(_lib.bielcc_integral_seg(self.h, integrand, n, abi.dptr(a), abi.dptr(b), kp, n_start, p_max, eps,
+                                        abi.dptr(res)))
+        return res
+
     def k0(self, integrand, common, cells, x, j, kp, n_seg, p_seg, eps):
         cells, x = _c(cells), _c(x)
         j = _c(j, np.complex128)

@@ -35,7 +35,7 @@ extern "C" {
 #pragma GCC visibility push(default)
 #endif
 
-#define BIELCC_ABI_VERSION 1
+#define BIELCC_ABI_VERSION 2
 
 /* ---- status codes ---------------------------------------------------- */
 #define BIELCC_OK                 0
@@ -90,6 +90,7 @@ typedef struct bielcc_kernelparam {
     double current[3][2];  /* KernelParam::current (complex) */
     double vec_dbl[3];     /* KernelParam::vec_dbl */
     double n[3];           /* KernelParam::n */
+    double e0[3];          /* KernelParam::e0 (read by PlaneWaveFieldE) */
 } bielcc_kernelparam;
 
 /* Precision of the field / assembly path. */
@@ -220,14 +221,20 @@ int bielcc_field_EH_full_device(bielcc_ctx ctx, bielcc_mesh mesh, int n_rhs,
  * outputs, and the call's scratch memory (cell rows, node tables, partial
  * sums, near lists) lives in one static device array of 64 MiB that every GPU
  * loading the library holds until exit. Sizes whose scratch exceeds 64 MiB are
- * rejected with BIELCC_ERR_ARG and a message giving the bytes needed (roughly:
- * 2.6 KiB per cell at n_start = 8, 100 B per point per cell split, 216 B per
- * near pair). The first call on each device looks up the array's device
- * address (cudaGetSymbolAddress), so that first call should come before any
- * stream capture. All calls share the array and leave its contents behind;
- * each call rewrites what it reads, and calls that overlap on the GPU race on
- * it. `stream` may be NULL (legacy default stream); like the _device call it
- * waits once for the near-pair count. The report carries n_pairs and
+ * rejected with BIELCC_ERR_ARG and a message giving the bytes needed. The
+ * scratch is, in bytes (each term rounded up to 256):
+ *   per cell:  128 + 48 n_start^2 + 4        (3204 B = 3.1 KiB at n_start = 8)
+ *   per point: 96 n_rhs per cell split + 96 n_rhs (near sums) + 16
+ *              + 4 ceil(n_cells / 32)        (near-cell mask: 1 KiB per point
+ *                                             at 8192 cells)
+ *   per near pair: 216
+ * The far partial sums take at most half of what is left after the cells and
+ * a one-split workspace; the cell-split count is capped to fit. Every call
+ * looks up the array's device address in the current context
+ * (cudaGetSymbolAddress). All calls share the array and leave its contents
+ * behind; each call rewrites what it reads, and calls that overlap on the GPU
+ * race on it. `stream` may be NULL (legacy default stream); like the _device
+ * call it waits once for the near-pair count. The report carries n_pairs and
  * n_near_pairs only. */
 int bielcc_field_EH_noalloc(int n_vert, int n_cells, const double* cells_dev, int n_rhs,
                             const double* J_dev, double k_re, double k_im, double mult_re,
@@ -327,7 +334,12 @@ int bielcc_pair_op(bielcc_ctx ctx, int op, int n_vert, int n_pairs, const double
 #define BIELCC_F_N_DOUBLEPOT_H     10  /* nF_DoublePot_H       kernel_lib.h:409-419 idim 3 cplx */
 #define BIELCC_F_ROTROTSIMPLEPOT_H 11  /* F_RotRotSimplePot_H  kernel_lib.h:453-492 idim 3 cplx */
 #define BIELCC_F_ONE               12  /* F(x) = 1: IntegralUniversal area check   idim 1 real */
-#define BIELCC_F_COUNT             13
+#define BIELCC_F_PLANEWAVE_E       13  /* PlaneWaveFieldE electrodynamics/incident_field.h:20-29:
+                                          F(x) = e0 exp(i vec_dbl . x)           idim 3 cplx */
+#define BIELCC_F_COUNT             14
+/* F_ONE and F_PLANEWAVE_E are functions of one point (the F(x) form); the
+ * others of a pair (x, y). The *_pnt and K0 entries take the pair form (and
+ * F_ONE), bielcc_integral / bielcc_integral_seg the F(x) form. */
 
 /* Returns the value dimension (1 or 3) and whether it is complex. */
 int bielcc_integrand_info(int integrand, int* idim, int* is_complex);
@@ -350,6 +362,21 @@ int bielcc_integral_seg_pnt(bielcc_ctx ctx, int integrand, int n_pairs,
                             const double* a, const double* b, const double* x,
                             bielcc_kernelparam* kp, int n_start, int p_max,
                             double eps, double* res);
+
+/* IntegralUniversal, the F(x) form (integrators/integral_universal.h:252-334
+ * quad, :347-431 triangle): the same adaptive sub-cell rule as
+ * bielcc_integral_pnt over n_cells cells, with an integrand of one point
+ * (BIELCC_F_ONE or BIELCC_F_PLANEWAVE_E); kp per cell, in/out as above.
+ * res: [n_cells][idim]. */
+int bielcc_integral(bielcc_ctx ctx, int integrand, int n_vert, int n_cells,
+                    const double* cells, bielcc_kernelparam* kp, int n_start, int p_max,
+                    double eps, double* res);
+
+/* IntegralUniversalSegPnt, the F(x) overload (integral_universal_seg.h:120-179):
+ * a, b: [n_segs][3]; integrand and kp as for bielcc_integral. */
+int bielcc_integral_seg(bielcc_ctx ctx, int integrand, int n_segs, const double* a,
+                        const double* b, bielcc_kernelparam* kp, int n_start, int p_max,
+                        double eps, double* res);
 
 /* K0 / K0_Common (electrodynamics/K0.h:36-86 / :112-166): contour integral
  * of one integrand over the cell edges. common = 0: -sum_e (j.nu_e) int_e F;

@@ -7,20 +7,23 @@
 //   R_Rot_Smooth / R_Rot_Colloc / R_Rot_Near                          electrodynamics/R.h:46-175
 //   K0 / K0_Common                                                    electrodynamics/K0.h:36-166
 //   IntegralUniversalPnt (quad, triangle)                             integrators/integral_universal.h:38-220
-//   IntegralUniversalSegPnt                                           integrators/integral_universal_seg.h:38-98
+//   IntegralUniversal, the F(x) form (quad, triangle)                 integrators/integral_universal.h:252-431
+//   IntegralUniversalSegPnt (F(x, y) and F(x) overloads)              integrators/integral_universal_seg.h:38-179
 //   integral1Divr / integralGrad1DivrSeg                              integrators/integrals_analytic.h:31-50
 //   IntegralSurf_SimplePot_H_HS / IntegralSeg_GradSimplePot_H_HS      integrators/integrals_analytic.h:136-221
 //   GetFieldE_Ideal                                                   electrodynamics/get_field.h:35-78
 // The parameter records are duck-typed: any NumParam with the fields eps, rs,
 // rs_seg, analytic_calc, n_start, n_start_seg, p_max, p_max_seg; any
-// KernelParam<KType> with smoothR, smoothRMin, k, current, vec_dbl, n; any
+// KernelParam<KType> with smoothR, smoothRMin, k, current, vec_dbl, n, e0; any
 // IntegralParam with GetIDim/GetNStart/GetPMax/GetEpsAccur; any SurfMesh with
 // GetNFrm() and GetCell(i).GetCellCoords(). The reference's own types work.
 //
 // Integrands are the kernel_lib functions. When the reference's kernel_lib.h
 // is included before this header, its function pointers (bielcc::F_*<KType>)
-// are recognised; otherwise pass the BIELCC_F_* id. A user-written integrand
-// cannot run on the device: such a call throws std::invalid_argument.
+// are recognised, and so is bielcc::PlaneWaveFieldE<KType> (incident_field.h)
+// as the F(x) integrand of IntegralUniversal; otherwise pass the BIELCC_F_* id.
+// A user-written integrand cannot run on the device: such a call throws
+// std::invalid_argument.
 //
 // Every call below is one batched GPU launch (the per-pair forms with a batch
 // of one); for throughput use the *_batch forms or bielcc_field_EH directly.
@@ -92,6 +95,7 @@ inline bielcc_kernelparam to_kernelparam(const KP& k) {
         p.current[i][1] = c.imag();
         p.vec_dbl[i] = k.vec_dbl[i];
         p.n[i] = k.n[i];
+        p.e0[i] = k.e0[i];
     }
     return p;
 }
@@ -172,6 +176,18 @@ inline int integrand_id(void (*f)(const double*, const double*, const bielcc::Ke
     throw std::invalid_argument("integrand is not a kernel_lib function: it cannot run on the GPU");
 }
 #endif
+#ifdef _INCIDENT_FIELD_H_
+// F(x) integrands of IntegralUniversal: PlaneWaveFieldE (incident_field.h:20-29).
+template <typename KType, typename P>
+inline int integrand_id(void (*f)(const double*, const bielcc::KernelParam<KType>&, P*)) {
+    using F = void (*)(const double*, const bielcc::KernelParam<KType>&, P*);
+    if constexpr (std::is_same<P, std::complex<double>>::value) {
+        if (f == (F)bielcc::PlaneWaveFieldE<KType>) return BIELCC_F_PLANEWAVE_E;
+    }
+    throw std::invalid_argument("F(x) integrand is not PlaneWaveFieldE: it cannot run on the GPU "
+                                "(pass BIELCC_F_ONE for F = 1)");
+}
+#endif
 
 // IntegralUniversalPnt: res receives idim values (double or complex); the
 // kernel parameter's smoothR is left as the reference leaves it.
@@ -192,6 +208,28 @@ inline void IntegralUniversalSegPnt(const double* a, const double* b, const doub
     bielcc_kernelparam kp = to_kernelparam(ker_param);
     check(bielcc_integral_seg_pnt(context(), id, 1, a, b, x, &kp, int_param.GetNStart(), int_param.GetPMax(),
                                   int_param.GetEpsAccur(), reinterpret_cast<double*>(res)));
+    ker_param.smoothR = kp.smoothR;
+}
+
+// IntegralUniversal, the F(x) form: f_0 is PlaneWaveFieldE or BIELCC_F_ONE.
+template <typename F, typename KP, typename IP, size_t CellPoints, typename P>
+inline void IntegralUniversal(const double (&cell)[CellPoints][3], F f_0, KP& ker_param, const IP& int_param,
+                              P* res) {
+    int id = integrand_id(f_0);
+    bielcc_kernelparam kp = to_kernelparam(ker_param);
+    check(bielcc_integral(context(), id, (int)CellPoints, 1, &cell[0][0], &kp, int_param.GetNStart(),
+                          int_param.GetPMax(), int_param.GetEpsAccur(), reinterpret_cast<double*>(res)));
+    ker_param.smoothR = kp.smoothR;
+}
+
+// IntegralUniversalSegPnt, the F(x) overload (integral_universal_seg.h:120-179).
+template <typename F, typename KP, typename IP, typename P>
+inline void IntegralUniversalSegPnt(const double* a, const double* b, F f_0, KP& ker_param, const IP& int_param,
+                                    P* res) {
+    int id = integrand_id(f_0);
+    bielcc_kernelparam kp = to_kernelparam(ker_param);
+    check(bielcc_integral_seg(context(), id, 1, a, b, &kp, int_param.GetNStart(), int_param.GetPMax(),
+                              int_param.GetEpsAccur(), reinterpret_cast<double*>(res)));
     ker_param.smoothR = kp.smoothR;
 }
 
@@ -279,11 +317,24 @@ inline void GetFieldE_Ideal(const Mesh& surf_mesh, const std::vector<std::array<
                             void (*EInc_Func)(const double*, const KP&, P*), const NP& num_param,
                             const std::vector<std::array<double, 3>>& points,
                             std::vector<std::array<std::complex<double>, 3>>& field_E) {
+    // the reference sums over the mesh's GetNFrm() cells, reading j_E[j] for each
+    // (get_field.h:47-55): extra currents are ignored, missing ones are an error
+    const int n_frm = surf_mesh.GetNFrm();
+    if (j_E.size() < (size_t)n_frm) throw std::invalid_argument("j_E holds fewer currents than the mesh has cells");
+    if (field_E.size() < points.size()) throw std::invalid_argument("field_E must be presized to points.size()");
     int nv = 0;
     std::vector<double> cells = mesh_cells(surf_mesh, &nv);
+    if (n_frm == 0) {  // no cells: the incident field alone
+        for (size_t i = 0; i < points.size(); i++) {
+            P e_inc[3] = {};
+            EInc_Func(points[i].data(), EInc_param, e_inc);
+            for (int g = 0; g < 3; g++) field_E[i][g] = e_inc[g];
+        }
+        return;
+    }
     bielcc_ctx ctx = context();
     bielcc_mesh m = 0;
-    check(bielcc_mesh_create(ctx, nv, (int)j_E.size(), cells.data(), &m));
+    check(bielcc_mesh_create(ctx, nv, n_frm, cells.data(), &m));
     double kr, ki;
     split_k(EInc_param.k, &kr, &ki);
     bielcc_numparam np = to_numparam(num_param);

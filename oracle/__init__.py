@@ -25,10 +25,13 @@ _libs = {}
 
 
 def build(ref=True):
-    """Builds liboracle.so (and the reference when its sources are present)."""
+    """Builds liboracle.so, and where the reference sources are present the
+    reference library and the drop-in checker (which links the GPU library)."""
     targets = ["oracle"]
     if ref and os.path.isdir(os.environ.get("BIELCC_REF_SRC", "/root/reference")):
         targets.append("ref")
+        if os.path.exists(os.path.join(HERE, "..", "bielcc_b200", "libbielcc_gpu.so")):
+            targets.append("dropin")
     env = dict(os.environ)
     if "BIELCC_REF_SRC" in env:
         targets.append("REF=" + env["BIELCC_REF_SRC"])
@@ -139,6 +142,30 @@ def integral_seg_pnt(integrand, a, b, x, kp, n_start, p_max, eps, which="port"):
                                        eps, abi.dptr(res))
     if rc != 0:
         raise RuntimeError(f"{which} integral_seg_pnt failed: {rc}")
+    return res
+
+
+def integral(integrand, cells, kp, n_start, p_max, eps, which="port"):
+    """IntegralUniversal, the F(x) form (integral_universal.h:252-431)."""
+    cells = _c(cells)
+    n = cells.shape[0]
+    _, idim, cplx = abi.INTEGRANDS[integrand]
+    res = np.zeros((n, idim), np.complex128 if cplx else np.float64)
+    rc = _f(which, "integral")(integrand, cells.shape[1], n, abi.dptr(cells), kp, n_start, p_max, eps, abi.dptr(res))
+    if rc != 0:
+        raise RuntimeError(f"{which} integral failed: {rc}")
+    return res
+
+
+def integral_seg(integrand, a, b, kp, n_start, p_max, eps, which="port"):
+    """IntegralUniversalSegPnt, the F(x) overload (integral_universal_seg.h:120-179)."""
+    a, b = _c(a), _c(b)
+    n = a.shape[0]
+    _, idim, cplx = abi.INTEGRANDS[integrand]
+    res = np.zeros((n, idim), np.complex128 if cplx else np.float64)
+    rc = _f(which, "integral_seg")(integrand, n, abi.dptr(a), abi.dptr(b), kp, n_start, p_max, eps, abi.dptr(res))
+    if rc != 0:
+        raise RuntimeError(f"{which} integral_seg failed: {rc}")
     return res
 
 

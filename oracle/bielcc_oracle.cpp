@@ -152,6 +152,7 @@ struct KP {
     cd current[3] = {0., 0., 0.};
     double vec_dbl[3] = {0, 0, 0};
     double n[3] = {0, 0, 0};
+    double e0[3] = {0, 0, 0};
 };
 
 // ---------------------------------------------------------------- integrands
@@ -273,6 +274,12 @@ static void F_RotRotSimplePot_H(const double* x, const double* y, const KP& p, c
 }
 // F = 1 (the f1 integrand of examples/integrators/main0_integrals.cpp:77-81)
 static void F_One(const double*, const double*, const KP&, double* out) { out[0] = 1.; }
+// PlaneWaveFieldE (electrodynamics/incident_field.h:20-29) as a one-point
+// integrand F(y) = e0 exp(i vec_dbl . y); the pair point is unused.
+static void PlaneWave_E(const double*, const double* y, const KP& p, cd* out) {
+    cd deg = std::exp(cd(0., 1.) * dot3(p.vec_dbl, y));
+    for (int i = 0; i < 3; i++) out[i] = p.e0[i] * deg;
+}
 
 // ---------------------------------------------------------------- universal quadrature
 // The adaptive driver shared by the three rules (integral_universal.h:58-119,
@@ -753,6 +760,7 @@ static void kp_from(const bielcc_kernelparam* s, KP& d) {
         d.current[i] = cd(s->current[i][0], s->current[i][1]);
         d.vec_dbl[i] = s->vec_dbl[i];
         d.n[i] = s->n[i];
+        d.e0[i] = s->e0[i];
     }
 }
 
@@ -766,6 +774,7 @@ static Integrand<cd> cplx_integrand(int id) {
         case BIELCC_F_DOUBLEPOT_H: return F_DoublePot_H;
         case BIELCC_F_N_DOUBLEPOT_H: return nF_DoublePot_H;
         case BIELCC_F_ROTROTSIMPLEPOT_H: return F_RotRotSimplePot_H;
+        case BIELCC_F_PLANEWAVE_E: return PlaneWave_E;
         default: return nullptr;
     }
 }
@@ -906,6 +915,50 @@ int oracle_integral_seg_pnt(int integrand, int n_pairs, const double* a, const d
             integral_seg<double>(a + 3 * (size_t)p, b + 3 * (size_t)p, x + 3 * (size_t)p,
                                  real_integrand(integrand), k, idim, n_start, p_max, eps,
                                  res + (size_t)idim * p);
+        kp[p].smoothR = k.smoothR;
+    }
+    return BIELCC_OK;
+}
+
+// IntegralUniversal, the F(x) form (integrators/integral_universal.h:252-334
+// quad, :347-431 triangle): the nodes and weights of IntegralUniversalPnt with
+// a one-point integrand (F = 1 or PlaneWaveFieldE).
+static bool one_point(int id) { return id == BIELCC_F_ONE || id == BIELCC_F_PLANEWAVE_E; }
+
+int oracle_integral(int integrand, int n_vert, int n_cells, const double* cells, bielcc_kernelparam* kp,
+                    int n_start, int p_max, double eps, double* res) {
+    if ((n_vert != 3 && n_vert != 4) || !one_point(integrand)) return BIELCC_ERR_ARG;
+    int idim = integrand_dim(integrand);
+    const double none[3] = {0, 0, 0};
+    for (int p = 0; p < n_cells; p++) {
+        Cell cl{n_vert, reinterpret_cast<const double(*)[3]>(cells + (size_t)p * n_vert * 3)};
+        KP k;
+        kp_from(kp + p, k);
+        if (auto fc = cplx_integrand(integrand))
+            integral_cell<cd>(none, cl, fc, k, idim, n_start, p_max, eps, reinterpret_cast<cd*>(res) + (size_t)idim * p);
+        else
+            integral_cell<double>(none, cl, real_integrand(integrand), k, idim, n_start, p_max, eps,
+                                  res + (size_t)idim * p);
+        kp[p].smoothR = k.smoothR;
+    }
+    return BIELCC_OK;
+}
+
+// IntegralUniversalSegPnt, the F(x) overload (integral_universal_seg.h:120-179).
+int oracle_integral_seg(int integrand, int n_segs, const double* a, const double* b, bielcc_kernelparam* kp,
+                        int n_start, int p_max, double eps, double* res) {
+    if (!one_point(integrand)) return BIELCC_ERR_ARG;
+    int idim = integrand_dim(integrand);
+    const double none[3] = {0, 0, 0};
+    for (int p = 0; p < n_segs; p++) {
+        KP k;
+        kp_from(kp + p, k);
+        if (auto fc = cplx_integrand(integrand))
+            integral_seg<cd>(a + 3 * (size_t)p, b + 3 * (size_t)p, none, fc, k, idim, n_start, p_max, eps,
+                             reinterpret_cast<cd*>(res) + (size_t)idim * p);
+        else
+            integral_seg<double>(a + 3 * (size_t)p, b + 3 * (size_t)p, none, real_integrand(integrand), k, idim,
+                                 n_start, p_max, eps, res + (size_t)idim * p);
         kp[p].smoothR = k.smoothR;
     }
     return BIELCC_OK;

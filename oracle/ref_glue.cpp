@@ -165,6 +165,7 @@ KernelParam<KType> make_kp(const bielcc_kernelparam& s) {
         p.current[i] = cd(s.current[i][0], s.current[i][1]);
         p.vec_dbl[i] = s.vec_dbl[i];
         p.n[i] = s.n[i];
+        p.e0[i] = s.e0[i];
     }
     return p;
 }
@@ -266,6 +267,40 @@ int k0_impl(int integrand, int common, int n_vert, int n_pairs, const double* ce
 
 }  // namespace
 
+namespace {
+// IntegralUniversal (integral_universal.h:252-431) and the segment F(x)
+// overload (integral_universal_seg.h:120-179) with F = 1 or PlaneWaveFieldE
+// (incident_field.h:20-29), the reference's own templates.
+template <typename KType>
+int integral_fx_impl(int integrand, int n_vert, int n_items, const double* cells, const double* a, const double* b,
+                     bielcc_kernelparam* kp, int n_start, int p_max, double eps, double* res) {
+    const int idim = integrand == BIELCC_F_ONE ? 1 : 3;
+    if (integrand != BIELCC_F_ONE && integrand != BIELCC_F_PLANEWAVE_E) return BIELCC_ERR_ARG;
+    for (int p = 0; p < n_items; p++) {
+        KernelParam<KType> k = make_kp<KType>(kp[p]);
+        IntegralParam ip(idim, n_start, p_max, eps);
+        double* rr = res + (size_t)idim * p;
+        cd* rc = reinterpret_cast<cd*>(res) + (size_t)idim * p;
+        if (cells && n_vert == 4) {
+            const auto& c = *reinterpret_cast<const double(*)[4][3]>(cells + (size_t)p * 12);
+            if (integrand == BIELCC_F_ONE) IntegralUniversal(c, f_one_x<KType>, k, ip, rr);
+            else IntegralUniversal(c, PlaneWaveFieldE<KType>, k, ip, rc);
+        } else if (cells) {
+            const auto& c = *reinterpret_cast<const double(*)[3][3]>(cells + (size_t)p * 9);
+            if (integrand == BIELCC_F_ONE) IntegralUniversal(c, f_one_x<KType>, k, ip, rr);
+            else IntegralUniversal(c, PlaneWaveFieldE<KType>, k, ip, rc);
+        } else {
+            size_t o = 3 * (size_t)p;
+            if (integrand == BIELCC_F_ONE) IntegralUniversalSegPnt(a + o, b + o, f_one_x<KType>, k, ip, rr);
+            else IntegralUniversalSegPnt(a + o, b + o, PlaneWaveFieldE<KType>, k, ip, rc);
+        }
+        kp[p].smoothR = k.smoothR;
+    }
+    return BIELCC_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 int ref_field_EH(int n_vert, int n_cells, const double* cells, int n_rhs, const double* J, double k_re,
@@ -325,6 +360,17 @@ int ref_integral_seg_pnt(int integrand, int n_pairs, const double* a, const doub
     for (int p = 0; p < n_pairs; p++) cplx = cplx || kp[p].k_im != 0.;
     if (cplx) return integral_seg_impl<cd>(integrand, n_pairs, a, b, x, kp, n_start, p_max, eps, res);
     return integral_seg_impl<double>(integrand, n_pairs, a, b, x, kp, n_start, p_max, eps, res);
+}
+
+int ref_integral(int integrand, int n_vert, int n_cells, const double* cells, bielcc_kernelparam* kp, int n_start,
+                 int p_max, double eps, double* res) {
+    if (n_vert != 3 && n_vert != 4) return BIELCC_ERR_ARG;
+    return integral_fx_impl<double>(integrand, n_vert, n_cells, cells, nullptr, nullptr, kp, n_start, p_max, eps, res);
+}
+
+int ref_integral_seg(int integrand, int n_segs, const double* a, const double* b, bielcc_kernelparam* kp, int n_start,
+                     int p_max, double eps, double* res) {
+    return integral_fx_impl<double>(integrand, 0, n_segs, nullptr, a, b, kp, n_start, p_max, eps, res);
 }
 
 int ref_k0(int integrand, int common, int n_vert, int n_pairs, const double* cells, const double* x,

@@ -3,7 +3,9 @@
 oracle/_ref/libbielcc_ref.so by oracle/Makefile) on small seeded cases.
 
 Run in a container where the reference sources exist:
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref && python tests/golden/make_golden.py [part ...]
+with parts "main" (field, pair operators, pair integrands, analytic, known
+answers) and "fx" (the one-point F(x) forms); no argument runs both.
 The fixtures pin the oracle (tests/test_oracle_golden.py) and the GPU path
 (tests/test_gpu_*.py) where the reference itself cannot travel.
 """
@@ -80,7 +82,7 @@ def main():
     # ---- universal quadratures of every integrand
     ints = {}
     for name, cells in (("quad", quad), ("tri", tri)):
-        for fid, (fname, idim, cplx) in abi.INTEGRANDS.items():
+        for fid in abi.PAIR_INTEGRANDS:
             cc, x, j = random_pairs(cells, 16, rng, 0.2)
             dm = W.diameters(cc)
             kk = np.where(rng.random(16) < 0.5, 2 * np.pi, 2 * np.pi + 0.3j)
@@ -100,7 +102,7 @@ def main():
                 ints[key + "_cur"] = j
                 ints[key + "_vec"] = nrm
                 ints[key + "_res"] = r
-    for fid, (fname, idim, cplx) in abi.INTEGRANDS.items():
+    for fid in abi.PAIR_INTEGRANDS:
         a = rng.normal(size=(16, 3))
         b = a + rng.normal(size=(16, 3)) * 0.3
         x = (a + b) / 2 + rng.normal(size=(16, 3)) * 0.2
@@ -160,5 +162,45 @@ def main():
         print(k_, v)
 
 
+def fx():
+    """IntegralUniversal (integral_universal.h:252-431) and the segment F(x)
+    overload (integral_universal_seg.h:120-179) with F = 1 and PlaneWaveFieldE
+    (incident_field.h:20-29), at p_max 1 and 3, on quads (incl. degenerate
+    pole quads), triangles and segments."""
+    rng = np.random.default_rng(20261204)
+    quad = W.uv_sphere(16, 32)
+    tri = W.perturbed_icosphere(level=1, seed=2)
+    out = {}
+    for name, cells in (("quad", quad), ("tri", tri)):
+        idx = np.concatenate([np.arange(4), rng.integers(0, len(cells), 20)])  # quads 0..3: a pole row
+        cc = cells[idx]
+        n = len(cc)
+        kv = rng.normal(size=(n, 3)) * 6.0
+        e0 = rng.normal(size=(n, 3))
+        for fid in abi.FX_INTEGRANDS:
+            for pm in (1, 3):
+                kp = abi.kernelparam_array(n, smoothR=0.1, smoothRMin=0.01, k=2 * np.pi, vec_dbl=kv, e0=e0)
+                r = oracle.integral(fid, cc, kp, 8, pm, 1e-6, which=REF)
+                key = f"{name}_f{fid}_p{pm}"
+                out.update({key + "_cells": cc, key + "_kv": kv, key + "_e0": e0, key + "_res": r,
+                            key + "_sR": np.array([kp[i].smoothR for i in range(n)])})
+    a = rng.normal(size=(16, 3))
+    b = a + rng.normal(size=(16, 3)) * 0.5
+    kv = rng.normal(size=(16, 3)) * 6.0
+    e0 = rng.normal(size=(16, 3))
+    for fid in abi.FX_INTEGRANDS:
+        for pm in (1, 3):
+            kp = abi.kernelparam_array(16, smoothR=0.1, smoothRMin=0.01, k=2 * np.pi, vec_dbl=kv, e0=e0)
+            r = oracle.integral_seg(fid, a, b, kp, 10, pm, 1e-6, which=REF)
+            key = f"seg_f{fid}_p{pm}"
+            out.update({key + "_a": a, key + "_b": b, key + "_kv": kv, key + "_e0": e0, key + "_res": r,
+                        key + "_sR": np.array([kp[i].smoothR for i in range(16)])})
+    np.savez_compressed(os.path.join(OUT, "integrals_fx.npz"), **out)
+
+
 if __name__ == "__main__":
-    main()
+    parts = sys.argv[1:] or ["main", "fx"]
+    if "main" in parts:
+        main()
+    if "fx" in parts:
+        fx()

@@ -25,7 +25,7 @@ def test_header_declares_the_boundary():
     names = declared_functions()
     for must in ("bielcc_ctx_create", "bielcc_mesh_create", "bielcc_field_EH", "bielcc_field_EH_device",
                  "bielcc_pair_op", "bielcc_integral_pnt", "bielcc_integral_seg_pnt", "bielcc_k0",
-                 "bielcc_integral_1divr", "bielcc_assemble_K"):
+                 "bielcc_integral_1divr", "bielcc_assemble_K", "bielcc_integral", "bielcc_integral_seg"):
         assert must in names
 
 
@@ -89,6 +89,7 @@ def test_checkers_export_the_same_calls():
         if not oracle.available(which) and which == "ref":
             continue
         L, prefix = oracle.lib(which)
-        for n in ("field_EH", "pair_op", "integral_pnt", "integral_seg_pnt", "k0", "integral_1divr",
+        for n in ("field_EH", "pair_op", "integral_pnt", "integral_seg_pnt", "integral", "integral_seg", "k0",
+                  "integral_1divr",
                   "integral_grad1divr_seg", "integral_surf_simplepot_h_hs", "integral_seg_gradsimplepot_h_hs"):
             assert hasattr(L, prefix + n)

@@ -4,7 +4,7 @@ import numpy as np
 import pytest
 
 import oracle
-from bielcc_b200 import abi
+from bielcc_b200 import abi, gpu
 from bielcc_b200 import workloads as W
 from conftest import TOL_FP64, golden, rel_l2
 
@@ -28,7 +28,7 @@ def test_pair_ops_golden(gctx):
 def test_integrals_golden(gctx):
     g = golden("integrals.npz")
     for name in ("quad", "tri"):
-        for fid in abi.INTEGRANDS:
+        for fid in abi.PAIR_INTEGRANDS:
             for pm in (1, 2):
                 key = f"{name}_f{fid}_p{pm}"
                 n = len(g[key + "_x"])
@@ -36,7 +36,7 @@ def test_integrals_golden(gctx):
                                            current=g[key + "_cur"], vec_dbl=g[key + "_vec"], normal=g[key + "_vec"])
                 r = gctx.integral_pnt(fid, g[key + "_cells"], g[key + "_x"], kp, 8, pm, 1e-6)
                 assert rel_l2(r, g[key + "_res"]) < TOL_FP64, key
-    for fid in abi.INTEGRANDS:
+    for fid in abi.PAIR_INTEGRANDS:
         for pm in (1, 3):
             key = f"seg_f{fid}_p{pm}"
             a, b = g[key + "_a"], g[key + "_b"]
@@ -44,6 +44,36 @@ def test_integrals_golden(gctx):
                                        current=a + 1j * b, vec_dbl=b - a, normal=b - a)
             r = gctx.integral_seg_pnt(fid, a, b, g[key + "_x"], kp, 10, pm, 1e-6)
             assert rel_l2(r, g[key + "_res"]) < TOL_FP64, key
+
+
+def test_integrals_one_point_form_golden(gctx):
+    """IntegralUniversal (F(x) form) and the segment F(x) overload on the GPU
+    against the reference's outputs, incl. the mutated smoothR; the pair and
+    one-point entry points refuse each other's integrands."""
+    g = golden("integrals_fx.npz")
+
+    def kp_for(key, n):
+        return abi.kernelparam_array(n, smoothR=0.1, smoothRMin=0.01, k=2 * np.pi, vec_dbl=g[key + "_kv"],
+                                     e0=g[key + "_e0"])
+
+    for fid in abi.FX_INTEGRANDS:
+        for pm in (1, 3):
+            for name in ("quad", "tri"):
+                key = f"{name}_f{fid}_p{pm}"
+                kp = kp_for(key, len(g[key + "_cells"]))
+                r = gctx.integral(fid, g[key + "_cells"], kp, 8, pm, 1e-6)
+                assert rel_l2(r, g[key + "_res"]) < TOL_FP64, key
+                assert np.array_equal([kp[i].smoothR for i in range(len(kp))], g[key + "_sR"]), key
+            key = f"seg_f{fid}_p{pm}"
+            kp = kp_for(key, len(g[key + "_a"]))
+            r = gctx.integral_seg(fid, g[key + "_a"], g[key + "_b"], kp, 10, pm, 1e-6)
+            assert rel_l2(r, g[key + "_res"]) < TOL_FP64, key
+    cells = g["quad_f12_p1_cells"][:2]
+    kp = abi.kernelparam_array(2)
+    with pytest.raises(gpu.BielccError):
+        gctx.integral(abi.F_SIMPLEPOT_H, cells, kp, 8, 1, 1e-6)
+    with pytest.raises(gpu.BielccError):
+        gctx.integral_pnt(abi.F_PLANEWAVE_E, cells, W.centres(cells), kp, 8, 1, 1e-6)
 
 
 def test_k0_against_oracle(gctx):

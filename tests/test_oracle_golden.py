@@ -50,7 +50,7 @@ def test_pair_ops():
 def test_integrals():
     g = golden("integrals.npz")
     for name in ("quad", "tri"):
-        for fid in abi.INTEGRANDS:
+        for fid in abi.PAIR_INTEGRANDS:
             for pm in (1, 2):
                 key = f"{name}_f{fid}_p{pm}"
                 n = len(g[key + "_x"])
@@ -58,7 +58,7 @@ def test_integrals():
                                            current=g[key + "_cur"], vec_dbl=g[key + "_vec"], normal=g[key + "_vec"])
                 r = oracle.integral_pnt(fid, g[key + "_cells"], g[key + "_x"], kp, 8, pm, 1e-6)
                 assert rel_l2(r, g[key + "_res"]) < TOL, key
-    for fid in abi.INTEGRANDS:
+    for fid in abi.PAIR_INTEGRANDS:
         for pm in (1, 3):
             key = f"seg_f{fid}_p{pm}"
             a, b = g[key + "_a"], g[key + "_b"]
@@ -66,6 +66,34 @@ def test_integrals():
                                        current=a + 1j * b, vec_dbl=b - a, normal=b - a)
             r = oracle.integral_seg_pnt(fid, a, b, g[key + "_x"], kp, 10, pm, 1e-6)
             assert rel_l2(r, g[key + "_res"]) < TOL, key
+
+
+def _fx_kp(g, key, n):
+    return abi.kernelparam_array(n, smoothR=0.1, smoothRMin=0.01, k=2 * np.pi, vec_dbl=g[key + "_kv"],
+                                 e0=g[key + "_e0"])
+
+
+def test_integrals_one_point_form():
+    """IntegralUniversal and the segment F(x) overload (F = 1, PlaneWaveFieldE)
+    against the reference's outputs, with the smoothR it leaves behind."""
+    g = golden("integrals_fx.npz")
+    for fid in abi.FX_INTEGRANDS:
+        for pm in (1, 3):
+            for name in ("quad", "tri"):
+                key = f"{name}_f{fid}_p{pm}"
+                kp = _fx_kp(g, key, len(g[key + "_cells"]))
+                r = oracle.integral(fid, g[key + "_cells"], kp, 8, pm, 1e-6)
+                assert rel_l2(r, g[key + "_res"]) < TOL, key
+                assert np.array_equal([kp[i].smoothR for i in range(len(kp))], g[key + "_sR"]), key
+            key = f"seg_f{fid}_p{pm}"
+            kp = _fx_kp(g, key, len(g[key + "_a"]))
+            r = oracle.integral_seg(fid, g[key + "_a"], g[key + "_b"], kp, 10, pm, 1e-6)
+            assert rel_l2(r, g[key + "_res"]) < TOL, key
+            assert np.array_equal([kp[i].smoothR for i in range(len(kp))], g[key + "_sR"]), key
+    # F = 1 over the trapezoid of the reference's Test0 is its area, 5
+    kp = abi.kernelparam_array(1)
+    rut1 = np.array([[[0., 0., 0.], [2., 0., 0.], [3., 2., 0.], [0., 2., 0.]]])
+    assert abs(oracle.integral(abi.F_ONE, rut1, kp, 8, 1, 1e-6)[0, 0] - 5.0) < 1e-12
 
 
 def test_analytic():

@@ -7,7 +7,8 @@ buffers only.
 Checked through the C ABI against the allocating entry point
 (bielcc_field_EH_device) on two calls in a row — the second with other points
 and precision, so leftovers of the first call in the shared array would show —
-plus the size limit. This file is collected last on purpose."""
+plus the size limit and the free device memory around a call (unchanged). This
+file is collected last on purpose."""
 import ctypes as C
 
 import numpy as np
@@ -128,3 +129,50 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
                  Ed.data_ptr(), None, 0, None, None)
     assert rc == abi.ERR_ARG
     assert "scratch" in L.bielcc_last_error().decode()
+
+
+def test_noalloc_allocates_no_device_memory():
+    """The point of the entry point: after a warm-up call (which may load the
+    library's kernels into the context), a call on a fresh stream leaves the
+    device's free memory unchanged, and so does a call rejected as too large."""
+    torch = pytest.importorskip("torch")
+    L, noalloc = _bind()
+    g = golden("field_quad512.npz")
+    cells, J, k = g["cells"], g["J"], float(g["k"])
+    dev = torch.device("cuda:0")
+    Cd = torch.from_numpy(np.ascontiguousarray(cells)).to(dev)
+    Jd = torch.from_numpy(np.ascontiguousarray(J)).to(dev)
+    Pd = torch.from_numpy(np.ascontiguousarray(g["pts"])).to(dev)
+    shape = (1, len(g["pts"]), 3)
+    Ed = torch.zeros(shape, dtype=torch.complex128, device=dev)
+    Hd = torch.zeros_like(Ed)
+    big = W.uv_sphere(128, 256)
+    Bd = torch.from_numpy(np.ascontiguousarray(big)).to(dev)
+    Jb = torch.zeros((1, len(big), 3), dtype=torch.complex128, device=dev)
+    stream = torch.cuda.Stream(dev)
+    np_ = abi.NumParam.default()
+
+    def call(precision):
+        rep = abi.Report()
+        rc = noalloc(4, len(cells), Cd.data_ptr(), 1, Jd.data_ptr(), k, 0.0, 1.0, 0.0, None, C.byref(np_),
+                     len(g["pts"]), Pd.data_ptr(), Ed.data_ptr(), Hd.data_ptr(), gpu.PREC[precision],
+                     stream.cuda_stream, C.byref(rep))
+        assert rc == 0, L.bielcc_last_error().decode()
+        stream.synchronize()
+        return rep
+
+    for prec in ("fp64", "mixed"):
+        call(prec)  # warm-up: kernels of this precision are loaded
+        torch.cuda.synchronize()
+        free0, _ = torch.cuda.mem_get_info(dev)
+        rep = call(prec)
+        free1, _ = torch.cuda.mem_get_info(dev)
+        assert rep.n_near_pairs > 0
+        assert free1 == free0, (prec, free0 - free1)
+
+    free0, _ = torch.cuda.mem_get_info(dev)
+    rc = noalloc(4, len(big), Bd.data_ptr(), 1, Jb.data_ptr(), 1.0, 0.0, 1.0, 0.0, None, None, 4, Pd.data_ptr(),
+                 Ed.data_ptr(), None, 0, stream.cuda_stream, None)
+    free1, _ = torch.cuda.mem_get_info(dev)
+    assert rc == abi.ERR_ARG
+    assert free1 == free0, free0 - free1
