@@ -262,8 +262,22 @@ def run_batched(args, ctx, torch, dev, stream, flush, fp64_single_rhs_value, pea
     b.record(stream)
     b.synchronize()
     ms_seq = a.elapsed_time(b)
-    ctx.field_EH_batch(jobs, precision="fp64", stream=sc)
+    # the same batch in FP64 (the plain form, batched the same way): the
+    # like-for-like reference for the mixed batch's speed and error
+    ctx.field_EH_batch(jobs, precision="fp64", stream=sc)  # warm-up; also the error reference
     torch.cuda.synchronize()
+    ms64 = 0.0
+    steps64 = max(1, min(args.steps, 2))
+    for _ in range(steps64):
+        flush.zero_()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        ctx.field_EH_batch(jobs, precision="fp64", stream=sc)
+        b.record(stream)
+        b.synchronize()
+        ms64 += a.elapsed_time(b)
+    ms64 /= steps64
     num = den = 0.0
     for (Em, Hm), (E6, H6) in zip(mixed, outs):
         num += float(torch.sum(torch.abs(Em - E6) ** 2) + torch.sum(torch.abs(Hm - H6) ** 2))
@@ -282,6 +296,8 @@ def run_batched(args, ctx, torch, dev, stream, flush, fp64_single_rhs_value, pea
             "value": value, "unit": "(point, cell, RHS) pairs/s", "geometry_pairs_per_s": geo_pairs / (ms * 1e-3),
             "ms_per_step": ms, "steps": steps, "rhs_pairs_per_step": rhs_pairs, "geometry_pairs_per_step": geo_pairs,
             "rel_l2_vs_fp64": (num / den) ** 0.5, "autotuned_item_cost": item_cost, "roofline": roofline,
+            "fp64_ms_per_step": ms64, "fp64_value": rhs_pairs / (ms64 * 1e-3),
+            "mixed_over_fp64_batched": ms64 / ms,
             "over_plain_fp64_single_rhs": value / fp64_single_rhs_value,
             "sequential_single_job_ms": ms_seq, "batched_over_sequential": ms_seq / ms,
             "graph_replay_ms": ms_graph, "graph_replay_value": rhs_pairs / (ms_graph * 1e-3), "gpu_launches_per_step":
@@ -633,7 +649,8 @@ def run_ours(args, ws, rank, local):
     achieved = far_flops / (far_ms * 1e-3) / 1e12
     far64_ms = st64["far_ms"] / max(1, st64["far_launches"])
     achieved64 = FLOPS_PER_FAR_PAIR * st64["far_pairs"] / max(1, st64["far_launches"]) / (far64_ms * 1e-3) / 1e12
-    # DRAM bytes per far-kernel launch, from the ncu capture summarised in profiles/
+    # DRAM bytes per far-kernel launch: a constant read from the ncu capture
+    # summarised in profiles/ (ncu does not run inside the bench)
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "far_kernel_mixed_sphere8192.md")
     if os.path.exists(tpath):
@@ -680,6 +697,9 @@ def run_ours(args, ws, rank, local):
         "roofline": {"bound": "fp32 CUDA-core pipe (no tensor-core or HBM bound: compute-only kernel)",
                      "kernel": "far_kernel<1,false,true>", "achieved": achieved, "peak": peak32, "unit": "TFLOP/s",
                      "frac": achieved / peak32 if peak32 else None, "traffic": traffic,
+                     "traffic_source": "ncu capture of the same launch summarised in "
+                                       "profiles/far_kernel_mixed_sphere8192.md (a constant from that capture, "
+                                       "not measured in this run)",
                      "algorithmic_flops_per_launch": far_flops, "far_ms_per_launch": far_ms,
                      "peak_source": "measured FMA loop (bielcc_measure_fma_peak); MEASURED_PEAKS.json has no FP32 "
                                     "CUDA-core figure"},

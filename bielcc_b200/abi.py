@@ -135,6 +135,42 @@ class KernelParam(C.Structure):
     ]
 
 
+DISPERSION_NONE = 0
+DISPERSION_REFRACT = 1
+
+
+class Material(C.Structure):
+    """bielcc_material: MaterialParam's description (electrodynamics/material.h)."""
+
+    _fields_ = [
+        ("dispersion", C.c_int32),
+        ("n_table", C.c_int32),
+        ("eps_r", C.c_double),
+        ("mu_r", C.c_double),
+        ("sigma", C.c_double),
+        ("table", C.POINTER(C.c_double)),
+    ]
+
+
+class Medium(C.Structure):
+    """bielcc_medium: eps, mu, k, multE, multH of a material at one frequency."""
+
+    _fields_ = [
+        ("eps", C.c_double * 2),
+        ("mu", C.c_double * 2),
+        ("k", C.c_double * 2),
+        ("k_source", C.c_double),
+        ("multE", C.c_double * 2),
+        ("multH", C.c_double * 2),
+        ("tand", C.c_double),
+        ("skin_depth", C.c_double),
+    ]
+
+    def cplx(self, name):
+        v = getattr(self, name)
+        return complex(v[0], v[1])
+
+
 class Report(C.Structure):
     _fields_ = [
         ("n_pairs", C.c_int64),

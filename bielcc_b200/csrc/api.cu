@@ -97,6 +97,7 @@ struct bielcc_ctx_s {
     cudaStream_t side = nullptr;
     cudaEvent_t side_in = nullptr;
     DevBuf side_ws, side_pair_ws, side_io, side_scratch;
+    bool batch_tc = true;               // mixed batches contract on the tensor cores when they qualify
     long long* h_side_total = nullptr;  // pinned
     unsigned long long* h_nonfinite = nullptr;
     // counters / timing (bielcc_ctx_stats)
@@ -193,6 +194,12 @@ struct WsSet {
     long long* h_total;  // pinned near-pair count
     bool timed;          // far-kernel events into the context's stats
 };
+}  // namespace
+
+bool ctx_batch_tensor_cores(bielcc_ctx_s* ctx) { return ctx->batch_tc; }
+
+namespace {
+
 WsSet main_ws(bielcc_ctx ctx) { return {&ctx->ws, &ctx->pair_ws, &ctx->scratch_small, ctx->h_total, ctx->timing}; }
 WsSet side_ws(bielcc_ctx ctx) {
     return {&ctx->side_ws, &ctx->side_pair_ws, &ctx->side_scratch, ctx->h_side_total, false};
@@ -255,12 +262,13 @@ int field_device_batched(bielcc_ctx ctx, const FieldArgs& a, cudaStream_t s, bie
     d.H = a.H;
     BatchPlan bp;
     const bool mixed = a.precision == BIELCC_PREC_MIXED;
-    plan_batch(bp, std::vector<JobDev>{d}, a.np.n_start, mixed, ctx->batch_item_cost);
+    plan_batch(bp, std::vector<JobDev>{d}, a.np.n_start, mixed, ctx->batch_item_cost, ctx->batch_tc);
     // The tuned item size suits batches of many jobs; one job alone is cut
     // finer (up to its range limit) when its items would leave resident CTAs idle.
     if ((int)bp.items.size() < 2 * bp.grid) {
         const double finer = std::max(1.0e5, ctx->batch_item_cost * bp.items.size() / (2.0 * bp.grid));
-        if (finer < ctx->batch_item_cost) plan_batch(bp, std::vector<JobDev>{d}, a.np.n_start, mixed, finer);
+        if (finer < ctx->batch_item_cost)
+            plan_batch(bp, std::vector<JobDev>{d}, a.np.n_start, mixed, finer, ctx->batch_tc);
     }
     const double busy = std::min(1.0, (double)bp.items.size() / std::max(1, bp.grid));
     const int S = a.n_rhs;
@@ -270,8 +278,9 @@ int field_device_batched(bielcc_ctx ctx, const FieldArgs& a, cudaStream_t s, bie
     BatchDevPtrs dp;
     int l1 = 0, l2 = 0;
     TRY_CUDA(batch_stage1(bp, w.ws->p, a.np.analytic_calc, a.np.n_start, a.k.im != 0., s, &dp, &l1));
-    TRY_CUDA(cudaMemcpyAsync(w.h_total, dp.total, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    TRY_CUDA(batch_status_to_host(dp, w.h_total, s));
     TRY_CUDA(cudaStreamSynchronize(s));
+    if (batch_timed_out(w.h_total)) return set_error(BIELCC_ERR_TIMEOUT, "batched far kernel: a bounded wait ran out");
     const long long n_near = *w.h_total;
     if (n_near > 0) TRY(w.pair_ws->ensure(batch_pair_ws_bytes(n_near)));
     DNP dn{a.np.eps, a.np.rs, a.np.rs_seg, a.np.analytic_calc, a.np.n_start, a.np.n_start_seg, a.np.p_max,
@@ -456,6 +465,13 @@ int bielcc_ctx_destroy(bielcc_ctx ctx) {
 int bielcc_ctx_synchronize(bielcc_ctx ctx) {
     TRY(enter(ctx));
     TRY_CUDA(cudaDeviceSynchronize());
+    return BIELCC_OK;
+}
+
+int bielcc_ctx_set_batch_tensor_cores(bielcc_ctx ctx, int on) {
+    TRY(enter(ctx));
+    std::lock_guard<std::mutex> g(ctx->mu);
+    ctx->batch_tc = on != 0;
     return BIELCC_OK;
 }
 
@@ -869,14 +885,15 @@ int field_batch_locked(bielcc_ctx ctx, int n_jobs, const bielcc_field_job* jobs,
     int64_t pairs = 0;
     TRY(jobs_to_dev(n_jobs, jobs, meshes, n, s, jd, &ck, &pairs));
     BatchPlan bp;
-    plan_batch(bp, jd, n.n_start, precision == BIELCC_PREC_MIXED, item_cost);
+    plan_batch(bp, jd, n.n_start, precision == BIELCC_PREC_MIXED, item_cost, ctx->batch_tc);
     TRY(ctx->ws.ensure(bp.ws_bytes));
     TRY(ctx->scratch_small.ensure(256));
     BatchDevPtrs d;
     int l1 = 0, l2 = 0;
     TRY_CUDA(batch_stage1(bp, ctx->ws.p, n.analytic_calc, n.n_start, ck, s, &d, &l1));
-    TRY_CUDA(cudaMemcpyAsync(ctx->h_total, d.total, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    TRY_CUDA(batch_status_to_host(d, ctx->h_total, s));
     TRY_CUDA(cudaStreamSynchronize(s));
+    if (batch_timed_out(ctx->h_total)) return set_error(BIELCC_ERR_TIMEOUT, "batched far kernel: a bounded wait ran out");
     const long long n_near = *ctx->h_total;
     if (n_near > 0) TRY(ctx->pair_ws.ensure(batch_pair_ws_bytes(n_near)));
     DNP dn{n.eps, n.rs, n.rs_seg, n.analytic_calc, n.n_start, n.n_start_seg, n.p_max, n.p_max_seg};
@@ -969,12 +986,13 @@ int bielcc_batch_plan_create(bielcc_ctx ctx, int n_jobs, const bielcc_field_job*
     cudaError_t e = cudaSuccess;
     int l1 = 0, l2 = 0;
     if (rc == BIELCC_OK) {
-        plan_batch(p->bp, jd, n.n_start, precision == BIELCC_PREC_MIXED, ctx->batch_item_cost);
+        plan_batch(p->bp, jd, n.n_start, precision == BIELCC_PREC_MIXED, ctx->batch_item_cost, ctx->batch_tc);
         e = cudaMalloc(&p->ws, p->bp.ws_bytes);
         if (e == cudaSuccess) e = batch_stage1(p->bp, p->ws, n.analytic_calc, n.n_start, ck, s, &p->d, &l1);
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(ctx->h_total, p->d.total, sizeof(long long), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = batch_status_to_host(p->d, ctx->h_total, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e == cudaSuccess && batch_timed_out(ctx->h_total))
+            rc = set_error(BIELCC_ERR_TIMEOUT, "batched far kernel: a bounded wait ran out");
     }
     if (rc == BIELCC_OK && e == cudaSuccess) {
         p->n_near = *ctx->h_total;

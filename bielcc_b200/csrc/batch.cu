@@ -27,6 +27,7 @@
 #include "internal.h"
 #include "ops.cuh"
 #include "scan.cuh"
+#include "umma.cuh"
 
 namespace bielcc_gpu {
 
@@ -514,6 +515,364 @@ __global__ void __launch_bounds__(kBT, MIXED ? BIELCC_BATCH_MINB : 2) batch_far_
     }
 }
 
+// ---------------------------------------------------------------- tensor-core contraction (mixed form)
+// batch_far_tc_kernel: the same items, phase A and summation boundaries as
+// batch_far_kernel<true>, with the contraction of phase B on the 5th-generation
+// tensor cores (tcgen05.mma kind::tf32, accumulators in tensor memory).
+//
+// Per item (job, 32-point tile, cell range) and chunk of 16 cells, in two
+// rounds of 8 cells, warp w evaluates the moments of cell w of the round for
+// the tile's 32 points (one point per lane) and writes them into the
+// operand A of the round,
+//     A[(a, p), (c, b, re|im)] = W_ab(p, c),   a = E x,y,z, H x,y,z;  b = x,y,z,
+// with W = A1 I + T for E and the cross-product matrix of G for H
+// (K_RotRot_Far = (A1 J + T J)/4pi, R_Rot_Colloc = (G x J)/4pi,
+// electrodynamics/K.h:288-301, R.h:89-111). The currents of 16 right-hand
+// sides at a time form the operand B, [[Jr, -Ji], [Ji, Jr]] per (cell, b), so
+// that D[(a, p), (s, re|im)] = sum_(c, b) W_ab(p, c) J_b(c, s) is one real GEMM
+// of M = 192 (two M = 128 MMAs, the second one's last 64 rows unused),
+// K = 48 per round and N = 2 S. FP32 operands are split into TF32 hi + lo and
+// each product is hi*hi + hi*lo + lo*hi, which keeps FP32-level accuracy. D
+// accumulates the chunk's 16 cells in tensor memory (FP32, as the CUDA-core
+// form accumulates them in registers) and is then added into the job's FP64
+// partial sums. A chunk's MMAs run while the warps evaluate the next round.
+namespace tcb {
+constexpr int kThreads = 256;  // 8 warps
+constexpr int kRound = 8;      // cells per round: one per warp
+constexpr int kK = 6 * kRound; // K of a round
+constexpr int kRows = 192;     // (component, point)
+constexpr int kSmax = 64;      // right-hand sides held in tensor memory
+constexpr int kG = 16;         // right-hand sides per staged B group
+constexpr uint32_t kTmemCols = 256, kBlock2Col = 128;
+constexpr uint32_t kAbytes = kRows * kK * 4;     // one of A hi / A lo
+constexpr uint32_t kBbytes = 2 * kG * kK * 4;    // one of B hi / B lo of one buffer
+constexpr uint32_t kSbo = (kK / 4) * 128;        // byte distance of 8-row groups
+constexpr int kNodes = kRound * 64;              // n_start <= 8
+// A hi, A lo, then B (2 buffers x hi, lo): the second M block of A lo reads
+// its 64 unused rows from the B buffers, which are larger than that.
+constexpr size_t kOffAl = kAbytes, kOffB = 2 * (size_t)kAbytes, kOffNodes = kOffB + 4 * (size_t)kBbytes;
+constexpr size_t kOffYY = kOffNodes + 16 * (size_t)kNodes, kOffCell = kOffYY + 4 * (size_t)kNodes;
+constexpr size_t kOffRho = kOffCell + 32 * kRound, kOffNear = kOffRho + 8 * kRound;
+constexpr size_t kSmem = kOffNear + kRound * 32;
+static_assert(64 * kK * 4 <= 4 * kBbytes, "the unused rows of the second M block must stay inside shared memory");
+// polls of one mbarrier wait before the kernel gives up (each poll blocks
+// for a bounded time; this is seconds, against microseconds of MMA work)
+constexpr long long kWaitPolls = 1ll << 22;
+}  // namespace tcb
+
+BIELCC_D void tc_put2(unsigned char* base, int row, int k, float v0, float v1) {
+    *reinterpret_cast<float2*>(base + umma::kmajor_offset(row, k, tcb::kK)) = make_float2(v0, v1);
+}
+
+// Writes one (point, cell) block of A: rows a * 32 + lane, K columns
+// 6 cl .. 6 cl + 5, hi and lo. m: the 20 moments times e^{ik r0}.
+BIELCC_D void tc_write_a(unsigned char* Ah, unsigned char* Al, int lane, int cl, const float* m) {
+    float tr[6], ti[6];
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        tr[q] = m[2 + 2 * q];
+        ti[q] = m[3 + 2 * q];
+    }
+    tr[0] += m[0];  // A1 onto the diagonal
+    ti[0] += m[1];
+    tr[3] += m[0];
+    ti[3] += m[1];
+    tr[5] += m[0];
+    ti[5] += m[1];
+    const float gr[3] = {m[14], m[16], m[18]}, gi[3] = {m[15], m[17], m[19]};
+    const int ti_[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+#pragma unroll
+    for (int a = 0; a < 6; a++) {
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            float wr, wi;
+            if (a < 3) {
+                wr = tr[ti_[a][b]];
+                wi = ti[ti_[a][b]];
+            } else {  // H_a = G_(a+1) J_(a+2) - G_(a+2) J_(a+1) (indices mod 3)
+                const int h = a - 3, b1 = (h + 1) % 3, b2 = (h + 2) % 3;
+                wr = b == b2 ? gr[b1] : (b == b1 ? -gr[b2] : 0.f);
+                wi = b == b2 ? gi[b1] : (b == b1 ? -gi[b2] : 0.f);
+            }
+            float hr, lr, hi, li;
+            umma::tf32_split(wr, hr, lr);
+            umma::tf32_split(wi, hi, li);
+            tc_put2(Ah, a * 32 + lane, 6 * cl + 2 * b, hr, hi);
+            tc_put2(Al, a * 32 + lane, 6 * cl + 2 * b, lr, li);
+        }
+    }
+}
+
+// TF32 hi / lo of an FP64 value.
+BIELCC_D void tc_split64(double v, float& hi, float& lo) {
+    uint32_t h, l;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"((float)v));
+    hi = __uint_as_float(h);
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"((float)(v - (double)hi)));
+    lo = __uint_as_float(l);
+}
+
+// Stages B of right-hand sides s0 .. s0 + 15 for the round's cells (zeros for
+// missing cells and right-hand sides): rows 2 s + (re|im of the output).
+BIELCC_D void tc_stage_b(unsigned char* Bh, unsigned char* Bl, const JobDev& jb, int c0, int nc, int s0) {
+    for (int i = threadIdx.x; i < tcb::kRound * tcb::kG * 3; i += tcb::kThreads) {
+        const int cl = i / (tcb::kG * 3), rem = i - cl * (tcb::kG * 3), sl = rem / 3, b = rem - sl * 3;
+        const int s = s0 + sl;
+        cplx v = mk(0., 0.);
+        if (cl < nc && s < jb.n_rhs) v = jb.J[((size_t)s * jb.n_cells + (c0 + cl)) * 3 + b];
+        float rh, rl, ih, il;
+        tc_split64(v.re, rh, rl);
+        tc_split64(v.im, ih, il);
+        const int k = 6 * cl + 2 * b;
+        tc_put2(Bh, 2 * sl, k, rh, -ih);
+        tc_put2(Bl, 2 * sl, k, rl, -il);
+        tc_put2(Bh, 2 * sl + 1, k, ih, rh);
+        tc_put2(Bl, 2 * sl + 1, k, il, rl);
+    }
+}
+
+// MMAs of one B group into D columns [32 g, 32 g + N) of both M blocks.
+BIELCC_D void tc_issue_group(uint32_t tmem, uint32_t sA, uint32_t sAl, uint32_t sBh, uint32_t sBl, int g, int n,
+                             bool first_round) {
+    const uint32_t id = umma::idesc_tf32(128, n);
+#pragma unroll
+    for (int blk = 0; blk < 2; blk++) {
+        const uint32_t d = tmem + blk * tcb::kBlock2Col + 32 * g;
+        const uint32_t ao = blk * 16 * tcb::kSbo;  // row 128
+#pragma unroll
+        for (int ks = 0; ks < tcb::kK / 8; ks++) {
+            const uint64_t ah = umma::smem_desc(sA + ao + 256 * ks, 128, tcb::kSbo);
+            const uint64_t al = umma::smem_desc(sAl + ao + 256 * ks, 128, tcb::kSbo);
+            const uint64_t bh = umma::smem_desc(sBh + 256 * ks, 128, tcb::kSbo);
+            const uint64_t bl = umma::smem_desc(sBl + 256 * ks, 128, tcb::kSbo);
+            umma::mma_tf32(d, ah, bh, id, !(first_round && ks == 0));
+            umma::mma_tf32(d, ah, bl, id, true);
+            umma::mma_tf32(d, al, bh, id, true);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(tcb::kThreads, 2)
+    batch_far_tc_kernel(const JobDev* __restrict__ jobs, const BatchItem* __restrict__ items, int n_items,
+                        int* __restrict__ counter, double analytic_calc, int n_start, int max_items,
+                        long long* __restrict__ err) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    unsigned char* sAh = smem;
+    unsigned char* sAl = smem + tcb::kOffAl;
+    unsigned char* sB = smem + tcb::kOffB;  // buffer q: hi at 2 q kBbytes, lo at (2 q + 1) kBbytes
+    float4* s_nodes = reinterpret_cast<float4*>(smem + tcb::kOffNodes);
+    float* s_yy = reinterpret_cast<float*>(smem + tcb::kOffYY);
+    double4* s_cell = reinterpret_cast<double4*>(smem + tcb::kOffCell);
+    double* s_rho = reinterpret_cast<double*>(smem + tcb::kOffRho);
+    unsigned char* s_near = smem + tcb::kOffNear;
+    __shared__ uint64_t bar[2];
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_item;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nn = n_start * n_start;
+    if (threadIdx.x == 0) {
+        umma::mbar_init(&bar[0], 1);
+        umma::mbar_init(&bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) umma::tmem_alloc(&s_tmem, tcb::kTmemCols);
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = s_tmem;
+    const uint32_t uA = umma::smem_u32(sAh), uAl = umma::smem_u32(sAl), uB = umma::smem_u32(sB);
+    // commits in flight per barrier (0 or 1) and the parity of the next phase to wait for
+    int inflight[2] = {0, 0};
+    uint32_t parity[2] = {0u, 0u};
+    bool abort = false;
+    // waits for every commit in flight; false on time-out (uniform over the CTA)
+    // (a timed-out commit stays recorded as in flight for the final wait)
+    auto wait_one_local = [&](int q) -> bool {
+        if (!inflight[q]) return true;
+        if (!umma::mbar_wait(&bar[q], parity[q], tcb::kWaitPolls)) return false;
+        parity[q] ^= 1u;
+        inflight[q] = 0;
+        return true;
+    };
+    auto wait_all = [&]() -> bool {
+        const bool ok0 = wait_one_local(0);
+        const bool ok1 = wait_one_local(1);
+        return !__syncthreads_or(!(ok0 && ok1));
+    };
+    auto wait_one = [&](int q) -> bool { return !__syncthreads_or(!wait_one_local(q)); };
+
+    // D of the last chunk, added to the partial sums once its MMAs completed
+    bool pend = false, pend_first = false;
+    int pend_range = 0;
+
+    for (int taken = 0; taken < max_items && !abort; taken++) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int it = s_item;
+        if (it >= n_items) break;
+        const BatchItem bi = items[it];
+        const JobDev& jb = jobs[bi.job];
+        const int P = jb.n_pts, N = jb.n_cells, S = jb.n_rhs;
+        const int p = bi.tile * kBP + lane;
+        const bool live = p < P;
+        double x[3] = {0., 0., 0.};
+        if (live)
+            for (int g = 0; g < 3; g++) x[g] = jb.pts[3 * (size_t)p + g];
+        const int cb = bi.range * jb.cells_per_range;
+        const int ce = min(N, cb + jb.cells_per_range);
+        const cplx k = jb.k;
+        const double k2r = k.re * k.re - k.im * k.im, k2i = 2.0 * k.re * k.im;
+        const bool ck = k.im != 0.0;
+        const int G = (S + tcb::kG - 1) / tcb::kG;
+        const int Spad = (S + 7) & ~7;
+        unsigned nbits = 0;
+
+        // adds D (the chunk just finished) into the job's partial sums:
+        // warps 0-3 hold E x,y,z and H x of their lane's point, warps 4-5 H y, H z
+        auto drain = [&]() {
+            if (warp < 6) {  // whole warps: tcgen05.ld is warp-collective
+                const int a = warp, q = warp & 3;
+                const uint32_t col0 = warp < 4 ? 0u : tcb::kBlock2Col;
+                for (int g = 0; g < G; g++) {
+                    float v[32];
+                    umma::tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + col0 + 32 * g, v);
+                    if (!live) continue;
+                    const int ns = min(tcb::kG, S - g * tcb::kG);
+#pragma unroll
+                    for (int sl = 0; sl < tcb::kG; sl++) {
+                        if (sl >= ns) break;
+                        const int s = g * tcb::kG + sl;
+                        double* dst = jb.partial + (((size_t)pend_range * S + s) * 12 + 2 * a) * (size_t)P + p;
+                        if (pend_first) {
+                            dst[0] = (double)v[2 * sl];
+                            dst[P] = (double)v[2 * sl + 1];
+                        } else {
+                            atomicAdd(dst, (double)v[2 * sl]);
+                            atomicAdd(dst + P, (double)v[2 * sl + 1]);
+                        }
+                    }
+                }
+            }
+            umma::fence_before_sync();
+            pend = false;
+        };
+
+        for (int c0 = cb; c0 < ce && !abort; c0 += 2 * tcb::kRound) {
+            for (int r = 0; r < 2 && !abort; r++) {
+                const int rc0 = c0 + r * tcb::kRound;
+                const int nc = min(tcb::kRound, ce - rc0);
+                if (nc <= 0) break;
+                __syncthreads();  // the previous round's reads of the staged nodes are done
+                {
+                    const float4* src = jb.nodes32 + (size_t)rc0 * nn;
+                    for (int i = threadIdx.x; i < nc * nn; i += tcb::kThreads) {
+                        const float4 v = __ldg(src + i);
+                        s_nodes[i] = v;
+                        s_yy[i] = node_yy(v);
+                    }
+                    for (int i = threadIdx.x; i < nc; i += tcb::kThreads) {
+                        const CellGeo& gg = jb.geo[rc0 + i];
+                        s_cell[i] = make_double4(gg.c[0], gg.c[1], gg.c[2], gg.diam);
+                        s_rho[i] = (double)jb.rho32[rc0 + i];
+                    }
+                }
+                __syncthreads();
+                // phase A: the moments of cell `warp` of the round for this warp's 32 points
+                float mom[20];
+#pragma unroll
+                for (int q = 0; q < 20; q++) mom[q] = 0.f;
+                if (warp < nc) {
+                    const double4 ci = s_cell[warp];
+                    const double cen[3] = {ci.x, ci.y, ci.z};
+                    double d;
+                    const bool nr = is_near(x, cen, ci.w, analytic_calc, &d);
+                    s_near[warp * 32 + lane] = nr ? 1 : 0;
+                    if (!nr && live) {
+                        const float4* nd = s_nodes + warp * nn;
+                        const float* yy = s_yy + warp * nn;
+                        if (ck) batch_moments<true, true>(nd, yy, nn, x, ci, d, s_rho[warp], k, k2r, k2i, mom);
+                        else batch_moments<true, false>(nd, yy, nn, x, ci, d, s_rho[warp], k, k2r, k2i, mom);
+                    }
+                }
+                // A and B are free once the previous round's MMAs completed; D of
+                // the previous chunk is added to the partial sums before this
+                // chunk's first MMA overwrites it
+                if (!wait_all()) {
+                    abort = true;
+                    break;
+                }
+                umma::fence_after_sync();
+                if (pend) drain();
+                tc_write_a(sAh, sAl, lane, warp, mom);
+                tc_stage_b(sB, sB + tcb::kBbytes, jb, rc0, nc, 0);
+                if (G > 1) tc_stage_b(sB + 2 * tcb::kBbytes, sB + 3 * tcb::kBbytes, jb, rc0, nc, tcb::kG);
+                umma::fence_async_smem();
+                umma::fence_before_sync();
+                __syncthreads();
+                umma::fence_after_sync();
+                // near-cell mask: warp 0 owns the words of its points
+                if (warp == 0) {
+                    for (int cc = 0; cc < nc; cc++) {
+                        const int c = rc0 + cc;
+                        nbits |= (unsigned)s_near[cc * 32 + lane] << (c & 31);
+                        if ((c & 31) == 31 || c == ce - 1) {
+                            if (live) jb.mask[(size_t)(c >> 5) * P + p] = nbits;
+                            nbits = 0;
+                        }
+                    }
+                }
+                for (int g = 0; g < G && !abort; g++) {
+                    const int q = g & 1;
+                    if (g >= 2) {  // buffer q is free once group g - 2's MMAs completed
+                        if (!wait_one(q)) {
+                            abort = true;
+                            break;
+                        }
+                        umma::fence_after_sync();
+                        tc_stage_b(sB + 2 * q * tcb::kBbytes, sB + (2 * q + 1) * tcb::kBbytes, jb, rc0, nc,
+                                   g * tcb::kG);
+                        umma::fence_async_smem();
+                        umma::fence_before_sync();
+                        __syncthreads();
+                        umma::fence_after_sync();
+                    }
+                    if (threadIdx.x == 0) {
+                        const int n = 2 * min(tcb::kG, Spad - g * tcb::kG);
+                        tc_issue_group(tmem, uA, uAl, uB + 2 * q * tcb::kBbytes, uB + (2 * q + 1) * tcb::kBbytes, g, n,
+                                       r == 0);
+                        umma::mma_commit(&bar[q]);
+                    }
+                    inflight[q] = 1;
+                }
+            }
+            pend = true;
+            pend_first = c0 == cb;
+            pend_range = bi.range;
+        }
+        // the item's last chunk: wait for its MMAs and add D
+        if (!abort) {
+            if (!wait_all()) abort = true;
+            umma::fence_after_sync();
+            if (!abort && pend) drain();
+        }
+    }
+    if (abort) {
+        if (threadIdx.x == 0) atomicExch(reinterpret_cast<unsigned long long*>(err), 1ull);
+        // MMAs still in flight: wait for them (bounded) before the tensor memory is released
+        for (int q = 0; q < 2; q++)
+            if (inflight[q]) umma::mbar_wait(&bar[q], parity[q], tcb::kWaitPolls);
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        umma::fence_after_sync();
+        umma::tmem_dealloc(tmem, tcb::kTmemCols);
+        umma::tmem_relinquish();
+    }
+}
+
 // ---------------------------------------------------------------- batched near path + finalize
 __global__ void batch_near_count_kernel(const JobDev* __restrict__ jobs, const int* __restrict__ pt_job, int total,
                                         long long* __restrict__ counts) {
@@ -707,11 +1066,18 @@ __global__ void batch_finalize_kernel(const JobDev* __restrict__ jobs, const int
 static size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 
-int batch_grid(bool mixed) {
+int batch_grid(bool mixed, bool tc) {
     // resident CTAs of the persistent grid (dynamic shared memory opted in once)
     int dev = 0, sms = 148, per = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (tc) {
+        cudaFuncSetAttribute(batch_far_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tcb::kSmem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_far_tc_kernel, tcb::kThreads, tcb::kSmem);
+        // every resident CTA holds kTmemCols of the SM's 512 tensor-memory columns
+        per = std::min(per, 512 / (int)tcb::kTmemCols);
+        return sms * std::max(1, per);
+    }
     size_t smem = mixed ? BatchCfg<true>::smem_bytes() : BatchCfg<false>::smem_bytes();
     if (mixed) {
         cudaFuncSetAttribute(batch_far_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -737,10 +1103,13 @@ int batch_cells_per_range(int n_cells, int n_rhs, int n_start, double item_cost)
     return (cpr + 31) / 32 * 32;
 }
 
-void plan_batch(BatchPlan& bp, const std::vector<JobDev>& jobs_in, int n_start, bool mixed, double item_cost) {
+void plan_batch(BatchPlan& bp, const std::vector<JobDev>& jobs_in, int n_start, bool mixed, double item_cost,
+                bool allow_tc) {
     bp.jobs = jobs_in;
     bp.mixed = mixed;
-    bp.grid = batch_grid(mixed);
+    bp.tc = mixed && allow_tc && n_start <= 8;
+    for (const JobDev& j : jobs_in) bp.tc = bp.tc && j.n_rhs <= tcb::kSmax;
+    bp.grid = batch_grid(mixed, bp.tc);
     const double nodes = (double)n_start * n_start;
     bp.items.clear();
     bp.pt_job.clear();
@@ -808,6 +1177,7 @@ cudaError_t batch_stage1(BatchPlan& bp, void* ws, double analytic_calc, int n_st
     d.offs = (long long*)w;
     w += al256((T + 1) * sizeof(long long));
     d.total = (long long*)w;
+    d.err = d.total + 1;
     w += 256;
     d.counter = (int*)w;
     cudaError_t e = cudaMemcpyAsync(d.jobs, bp.jobs.data(), bp.jobs.size() * sizeof(JobDev), cudaMemcpyHostToDevice, s);
@@ -815,11 +1185,15 @@ cudaError_t batch_stage1(BatchPlan& bp, void* ws, double analytic_calc, int n_st
         e = cudaMemcpyAsync(d.items, bp.items.data(), bp.items.size() * sizeof(BatchItem), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess && T) e = cudaMemcpyAsync(d.pt_job, bp.pt_job.data(), T * sizeof(int), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(d.counter, 0, sizeof(int), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d.total, 0, 2 * sizeof(long long), s);
     if (e != cudaSuccess) return e;
     const size_t smem = bp.mixed ? BatchCfg<true>::smem_bytes() : BatchCfg<false>::smem_bytes();
     const int n_items = (int)bp.items.size();
     if (n_items > 0) {
-        if (bp.mixed)
+        if (bp.tc)
+            batch_far_tc_kernel<<<bp.grid, tcb::kThreads, tcb::kSmem, s>>>(d.jobs, d.items, n_items, d.counter,
+                                                                          analytic_calc, n_start, bp.max_items, d.err);
+        else if (bp.mixed)
             batch_far_kernel<true><<<bp.grid, kBT, smem, s>>>(d.jobs, d.items, n_items, d.counter, analytic_calc,
                                                              n_start, bp.max_items);
         else
@@ -832,6 +1206,12 @@ cudaError_t batch_stage1(BatchPlan& bp, void* ws, double analytic_calc, int n_st
     *out = d;
     *launches = (n_items > 0 ? 1 : 0) + (T ? 1 : 0) + 1;
     return cudaGetLastError();
+}
+
+cudaError_t batch_status_to_host(const BatchDevPtrs& d, long long* h, cudaStream_t s) {
+    cudaError_t e = cudaMemcpyAsync(h, d.total, sizeof(long long), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h + 3, d.err, sizeof(long long), cudaMemcpyDeviceToHost, s);
+    return e;
 }
 
 size_t batch_pair_ws_bytes(long long n_near) {
@@ -880,7 +1260,10 @@ cudaError_t batch_replay(BatchPlan& bp, const BatchDevPtrs& d, long long n_near,
     const size_t smem = bp.mixed ? BatchCfg<true>::smem_bytes() : BatchCfg<false>::smem_bytes();
     const int n_items = (int)bp.items.size();
     if (n_items > 0) {
-        if (bp.mixed)
+        if (bp.tc)
+            batch_far_tc_kernel<<<bp.grid, tcb::kThreads, tcb::kSmem, s>>>(d.jobs, d.items, n_items, d.counter,
+                                                                          analytic_calc, n_start, bp.max_items, d.err);
+        else if (bp.mixed)
             batch_far_kernel<true><<<bp.grid, kBT, smem, s>>>(d.jobs, d.items, n_items, d.counter, analytic_calc,
                                                              n_start, bp.max_items);
         else

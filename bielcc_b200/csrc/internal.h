@@ -9,6 +9,8 @@
 #include "common.cuh"
 
 struct bielcc_ctx_s;  // the C ABI's context (api.cu)
+// Whether the context's mixed batches may use the tensor-core contraction (api.cu).
+bool ctx_batch_tensor_cores(bielcc_ctx_s* ctx);
 
 namespace bielcc_gpu {
 
@@ -165,6 +167,9 @@ struct BatchPlan {
     // so batches on higher-priority streams get SMs within one item's time
     int max_items = 1 << 30;
     bool mixed = true, ck = false;
+    // mixed batches whose jobs have at most 64 right-hand sides (n_start <= 8)
+    // contract their moments on the tensor cores (batch_far_tc_kernel)
+    bool tc = false;
 };
 // Turns a planned batch into one CTA per item (see BatchPlan::max_items).
 void batch_make_preemptible(BatchPlan& bp);
@@ -176,13 +181,21 @@ struct BatchDevPtrs {
     long long* counts;
     long long* offs;
     long long* total;
+    long long* err;  // nonzero: a bounded wait in the far kernel ran out (next to total)
     int* counter;
 };
+// Copies the near-pair count into h[0] and the far kernel's status into h[3]
+// (a 64-byte pinned block; h[1] may hold another count).
+cudaError_t batch_status_to_host(const BatchDevPtrs& d, long long* h, cudaStream_t s);
+inline bool batch_timed_out(const long long* h) { return h[3] != 0; }
 
 // Cells per item of one job (a multiple of 32; at most 6 ranges per job);
 // depends on the job and item_cost only.
 int batch_cells_per_range(int n_cells, int n_rhs, int n_start, double item_cost);
-void plan_batch(BatchPlan& bp, const std::vector<JobDev>& jobs, int n_start, bool mixed, double item_cost);
+// allow_tc: mixed batches that qualify run the tensor-core contraction
+// (bielcc_ctx_set_batch_tensor_cores); otherwise the CUDA-core kernel.
+void plan_batch(BatchPlan& bp, const std::vector<JobDev>& jobs, int n_start, bool mixed, double item_cost,
+                bool allow_tc = true);
 cudaError_t batch_stage1(BatchPlan& bp, void* ws, double analytic_calc, int n_start, bool ck, cudaStream_t s,
                          BatchDevPtrs* out, int* launches);
 size_t batch_pair_ws_bytes(long long n_near);

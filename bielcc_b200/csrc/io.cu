@@ -61,7 +61,8 @@ int bielcc_read_mesh_dat(const char* path, int n_vert, int* n_cells, double* cel
 // mesh/surf_mesh.cpp:195-290): legacy ASCII VTK, POINTS and POLYGONS (POLYDATA)
 // or CELLS (UNSTRUCTURED_GRID); polygons with exactly n_vert vertices become
 // cells in file order, others are skipped (their count in *n_skipped, may be
-// NULL); an index outside the point list is an error.
+// NULL); an index outside the point list, and a file without any polygon of
+// n_vert vertices, are errors, as the reference throws for both.
 int bielcc_read_mesh_vtk(const char* path, int n_vert, int* n_cells, double* cells, int* n_skipped) {
     if (!path || !n_cells || (n_vert != 3 && n_vert != 4))
         return set_api_error(BIELCC_ERR_ARG, "read_mesh_vtk: path, n_cells and n_vert 3 or 4 required");
@@ -116,8 +117,10 @@ int bielcc_read_mesh_vtk(const char* path, int n_vert, int* n_cells, double* cel
         }
         count++;
     }
-    *n_cells = count;
     if (n_skipped) *n_skipped = skipped;
+    // FillMeshFromVTK throws when no polygon has the cell's vertex count
+    if (count == 0) return io_error("read_mesh_vtk: no polygon with " + std::to_string(n_vert) + " vertices");
+    *n_cells = count;
     return BIELCC_OK;
 }
 

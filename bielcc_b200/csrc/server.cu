@@ -352,7 +352,8 @@ cudaError_t start_field_batch(bielcc_server_s* sv, Slot& sl) {
         d.nonfinite = (unsigned long long*)(dev + sl.nan_off) + i;
     }
     auto t3 = Clock::now();
-    plan_batch(sl.bp, jd, sv->np.n_start, sv->precision == BIELCC_PREC_MIXED, sv->item_cost);
+    plan_batch(sl.bp, jd, sv->np.n_start, sv->precision == BIELCC_PREC_MIXED, sv->item_cost,
+               ctx_batch_tensor_cores(sv->ctx));
     if (sv->preemptible) batch_make_preemptible(sl.bp);
     auto t4 = Clock::now();
     e = sl.ws.ensure(sl.bp.ws_bytes, sl.s);
@@ -360,7 +361,7 @@ cudaError_t start_field_batch(bielcc_server_s* sv, Slot& sl) {
     auto t5 = Clock::now();
     int launches = 0;
     e = batch_stage1(sl.bp, sl.ws.p, sv->np.analytic_calc, sv->np.n_start, false, sl.s, &sl.d, &launches);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(sl.h_total, sl.d.total, sizeof(long long), cudaMemcpyDeviceToHost, sl.s);
+    if (e == cudaSuccess) e = batch_status_to_host(sl.d, sl.h_total, sl.s);
     auto t6 = Clock::now();
     auto sec = [](Clock::time_point a, Clock::time_point b) { return std::chrono::duration<double>(b - a).count(); };
     std::lock_guard<std::mutex> g(sv->mu);
@@ -549,6 +550,8 @@ void slot_loop(bielcc_server_s* sv, Slot* slp) {
             sv->stage_in_s += in_s;
         }
         if (e == cudaSuccess) e = cudaEventSynchronize(sl.ev_stage1);
+        if (e == cudaSuccess && take[0]->type == kField && batch_timed_out(sl.h_total))
+            e = cudaErrorTimeout;  // a bounded wait in the far kernel ran out: the batch fails
         if (e == cudaSuccess) {
             const long long n_near = *sl.h_total;
             const size_t pb = pair_ws_bytes(sl, n_near);

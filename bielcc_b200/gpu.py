@@ -79,6 +79,10 @@ def load(path=LIB_PATH):
     d("bielcc_batch_plan_launch", [vp, vp])
     d("bielcc_batch_plan_destroy", [vp])
     d("bielcc_ctx_set_timing", [vp, C.c_int])
+    d("bielcc_ctx_set_batch_tensor_cores", [vp, C.c_int])
+    d("bielcc_medium_at", [C.POINTER(abi.Material), C.c_double, C.POINTER(abi.Medium)])
+    d("bielcc_planewave_in_medium", [C.POINTER(abi.Medium), C.c_double, C.POINTER(C.c_double),
+                                     C.POINTER(C.c_double), C.c_int, C.c_int, C.POINTER(abi.PlaneWave)])
     d("bielcc_measure_fma_peak", [C.c_int, C.POINTER(C.c_double)])
     d("bielcc_ctx_stats", [vp, C.POINTER(abi.Stats), C.c_int])
     d("bielcc_server_create", [vp, C.c_int64, C.c_int, C.POINTER(abi.NumParam), C.c_int, C.POINTER(vp)])
@@ -159,6 +163,40 @@ def read_currents(path_re, path_im):
     return J
 
 
+def material(eps_r=1.0, mu_r=1.0, sigma=0.0, table=None):
+    """bielcc_material: NonDispersive (eps_r, mu_r, sigma), or, with `table`
+    rows (frequency, n, absorption index), DispersiveByRefractIndex. The
+    returned record keeps its table alive."""
+    m = abi.Material()
+    m.eps_r, m.mu_r, m.sigma = float(eps_r), float(mu_r), float(sigma)
+    if table is not None:
+        t = _c(table).reshape(-1, 3)
+        m.dispersion, m.n_table = abi.DISPERSION_REFRACT, len(t)
+        m.table = abi.dptr(t)
+        m._table = t
+    else:
+        m.dispersion, m.n_table = abi.DISPERSION_NONE, 0
+    return m
+
+
+def medium_at(mat, freq):
+    """bielcc_medium of a material at a frequency (host only, no GPU)."""
+    load()
+    md = abi.Medium()
+    _check(_lib.bielcc_medium_at(C.byref(mat), float(freq), C.byref(md)))
+    return md
+
+
+def planewave_in_medium(md, freq, direction=(0.0, 0.0, 1.0), e0=(1.0, 0.0, 0.0), add_E=True, add_H=True):
+    """The incident plane wave of RadiationSource in that medium."""
+    load()
+    pw = abi.PlaneWave()
+    d = (C.c_double * 3)(*direction)
+    e = (C.c_double * 3)(*e0)
+    _check(_lib.bielcc_planewave_in_medium(C.byref(md), float(freq), d, e, int(add_E), int(add_H), C.byref(pw)))
+    return pw
+
+
 class Mesh:
     def __init__(self, ctx, cells):
         self.ctx = ctx
@@ -215,6 +253,10 @@ class Context:
 
     def set_timing(self, on=True):
         _check(_lib.bielcc_ctx_set_timing(self.h, int(bool(on))))
+
+    def set_batch_tensor_cores(self, on=True):
+        """Mixed batches contract moments and currents on the tensor cores (default) or the CUDA cores."""
+        _check(_lib.bielcc_ctx_set_batch_tensor_cores(self.h, int(bool(on))))
 
     def stats(self, reset=False):
         st = abi.Stats()

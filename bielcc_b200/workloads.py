@@ -131,6 +131,33 @@ def rounded_cube(n, edge_radius=0.1, half=1.0):
 
 
 # ---------------------------------------------------------------- cell geometry (numpy)
+def triangulate(cells):
+    """Each quad split into triangles (v0, v1, v2) and (v2, v3, v0); triangles
+    of (near) zero area, the collapsed halves of pole quads, are dropped."""
+    cells = np.asarray(cells, np.float64)
+    tri = np.concatenate([cells[:, [0, 1, 2]], cells[:, [2, 3, 0]]], axis=0)
+    order = np.stack([np.arange(len(cells)), np.arange(len(cells)) + len(cells)], 1).ravel()
+    tri = tri[order]  # the two halves of a quad next to each other
+    area = 0.5 * np.linalg.norm(np.cross(tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0]), axis=1)
+    return np.ascontiguousarray(tri[area > 1e-9 * area.max()])
+
+
+def _mixed_shape(kind, target, triangles, rng):
+    """One mesh of the batched / serving distributions: a spheroid (axis ratio
+    1-4), a rounded cube (edge radius 0.1) or a torus (R/r = 3) of about
+    `target` cells, as quads or (triangles=True) as their triangulation."""
+    t = target / 2 if triangles else target
+    if kind == 0:
+        n_lat = max(4, int(round((t / 2) ** 0.5)))
+        cells = spheroid(n_lat, 2 * n_lat, 1.0, rng.uniform(1.0, 4.0))
+    elif kind == 1:
+        cells = rounded_cube(max(4, int(round((t / 2) ** 0.5))), 0.1, 1.0)
+    else:
+        nv = max(4, int(round((t / 3) ** 0.5)))
+        cells = torus(3 * nv, nv, 1.5, 0.5)
+    return triangulate(cells) if triangles else cells
+
+
 def centres(cells):
     if cells.shape[1] == 4:
         return (cells[:, 0] + cells[:, 1] + cells[:, 2] + cells[:, 3]) * 0.25
@@ -233,7 +260,8 @@ def config3(level=5):
 
 def batch_meshes(n_meshes=256, seed=3, n_min=200, n_max=20000, pts_per_mesh=2000, rhs_max=64):
     """The 256-mesh batch: spheroids (axis ratio 1-4), rounded cubes (edge
-    radius 0.1), tori (R/r = 3); 200-20000 cells log-uniform; k log-uniform in
+    radius 0.1), tori (R/r = 3), every other triple of meshes as triangles
+    (the quads split in two); 200-20000 cells log-uniform; k log-uniform in
     [0.5, 20]; 1-rhs_max PO right-hand sides from uniform S^2 directions;
     pts_per_mesh far points (on a shell at 2-4 x the mesh extent)."""
     rng = np.random.default_rng(seed)
@@ -241,16 +269,7 @@ def batch_meshes(n_meshes=256, seed=3, n_min=200, n_max=20000, pts_per_mesh=2000
     for i in range(n_meshes):
         kind = i % 3
         target = float(np.exp(rng.uniform(np.log(n_min), np.log(n_max))))
-        if kind == 0:
-            n_lat = max(4, int(round((target / 2) ** 0.5)))
-            ratio = rng.uniform(1.0, 4.0)
-            cells = spheroid(n_lat, 2 * n_lat, 1.0, ratio)
-        elif kind == 1:
-            n = max(4, int(round((target / 2) ** 0.5)))
-            cells = rounded_cube(n, 0.1, 1.0)
-        else:
-            nv = max(4, int(round((target / 3) ** 0.5)))
-            cells = torus(3 * nv, nv, 1.5, 0.5)
+        cells = _mixed_shape(kind, target, (i // 3) % 2 == 1, rng)
         k = float(np.exp(rng.uniform(np.log(0.5), np.log(20.0))))
         S = int(rng.integers(1, rhs_max + 1))
         J = po_currents(cells, k, directions=S, seed=int(rng.integers(1 << 31)))
@@ -263,7 +282,8 @@ def batch_meshes(n_meshes=256, seed=3, n_min=200, n_max=20000, pts_per_mesh=2000
 def serving_stream(n_requests=400, seed=4, n_meshes=24, n_min=200, n_max=20000, p_min=100, p_max=50000,
                    rhs_max=16, assembly_frac=0.1, max_assembly_cells=2000, near_frac=0.1):
     """Request stream of the serving workload. Meshes are drawn like
-    batch_meshes (spheroids, rounded cubes, tori; 200-20000 cells log-uniform;
+    batch_meshes (spheroids, rounded cubes, tori, quads or triangles; 200-20000
+    cells log-uniform;
     k log-uniform in [0.5, 20]) and stay resident; each carries rhs_max PO
     current sets and a pool of p_max observation points (near_frac of them
     0.02-0.1 x the mesh extent above random cells, the rest on a 1.5-4 x
@@ -277,14 +297,7 @@ def serving_stream(n_requests=400, seed=4, n_meshes=24, n_min=200, n_max=20000, 
     for i in range(n_meshes):
         kind = i % 3
         target = float(np.exp(rng.uniform(np.log(n_min), np.log(n_max))))
-        if kind == 0:
-            n_lat = max(4, int(round((target / 2) ** 0.5)))
-            cells = spheroid(n_lat, 2 * n_lat, 1.0, rng.uniform(1.0, 4.0))
-        elif kind == 1:
-            cells = rounded_cube(max(4, int(round((target / 2) ** 0.5))), 0.1, 1.0)
-        else:
-            nv = max(4, int(round((target / 3) ** 0.5)))
-            cells = torus(3 * nv, nv, 1.5, 0.5)
+        cells = _mixed_shape(kind, target, (i // 3) % 2 == 1, rng)
         k = float(np.exp(rng.uniform(np.log(0.5), np.log(20.0))))
         extent = float(np.max(np.linalg.norm(cells.reshape(-1, 3), axis=1)))
         n_near = int(near_frac * p_max)

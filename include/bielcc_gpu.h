@@ -131,6 +131,14 @@ typedef struct bielcc_stats {
     double  far_ms;           /* summed CUDA-event time of the far-field kernels */
 } bielcc_stats;
 int bielcc_ctx_set_timing(bielcc_ctx ctx, int on);
+/* Mixed-precision batches (bielcc_field_EH_batch, batch plans, served
+ * batches, single-job calls routed as one-job batches) whose jobs have at most
+ * 64 right-hand sides and n_start <= 8 contract their far moments with the
+ * currents on the tensor cores (tcgen05, TF32 split into hi + lo, FP32
+ * accumulation over 16 cells, FP64 across) when on = 1 (the default);
+ * on = 0 keeps that contraction on the CUDA cores. No counterpart in the
+ * reference. */
+int bielcc_ctx_set_batch_tensor_cores(bielcc_ctx ctx, int on);
 int bielcc_ctx_stats(bielcc_ctx ctx, bielcc_stats* out, int reset);
 
 /* Measured FMA throughput (TFLOP/s, 2 flops per FMA) of the current device's
@@ -155,6 +163,42 @@ int bielcc_mesh_destroy(bielcc_ctx ctx, bielcc_mesh mesh);
  * FormNormalVectors / FormSurfaceBasis (mesh/surf_mesh.h:205-268) and
  * get_diam, and the cell area of CellFill; out: [n_cells][14]. */
 int bielcc_mesh_geometry(bielcc_ctx ctx, bielcc_mesh mesh, double* out);
+
+/* ---- media ---------------------------------------------------------------
+ * Constants of a field evaluation inside a material at one frequency, from
+ * the reference's material description: MaterialParam::Calc
+ * (electrodynamics/material.cpp:60-128), RadiationSource::CalcK
+ * (electrodynamics/radiation_source.cpp:159-180) and the Stratton-Chu
+ * multipliers of examples/field/main0_field_test.cpp:185-199. Host only.
+ * For a lossy material (complex eps) k is the complex omega sqrt(eps mu)
+ * with Im k > 0, which bielcc_field_EH_full takes as (k_re, k_im); the
+ * reference's CalcK throws there (it reads its real mu as complex). */
+#define BIELCC_DISPERSION_NONE     0  /* NonDispersive / Dispersive: eps_r, mu_r, sigma */
+#define BIELCC_DISPERSION_REFRACT  1  /* DispersiveByRefractIndex: table of (freq, n, k_absorb) */
+typedef struct bielcc_material {
+    int32_t dispersion;
+    int32_t n_table;        /* rows of table (BIELCC_DISPERSION_REFRACT) */
+    double eps_r, mu_r;     /* relative permittivity / permeability */
+    double sigma;           /* conductivity, S/m (0: lossless) */
+    const double* table;    /* [n_table][3]: frequency, refractive index n, absorption index
+                               (0: CalcEpsN, else CalcEpsNK); the frequency must be listed */
+} bielcc_material;
+typedef struct bielcc_medium {
+    double eps[2];          /* absolute permittivity, complex (F/m) */
+    double mu[2];           /* absolute permeability (H/m); real, as CalcMu */
+    double k[2];            /* omega sqrt(eps mu), Im >= 0 */
+    double k_source;        /* RadiationSource's real wave number, Re k */
+    double multE[2];        /* i / (omega eps) */
+    double multH[2];        /* i / (omega mu) */
+    double tand;            /* electric loss tangent, as Calc leaves it */
+    double skin_depth;      /* sqrt(2 / (omega mu sigma)); 0 without sigma */
+} bielcc_medium;
+int bielcc_medium_at(const bielcc_material* mat, double freq, bielcc_medium* out);
+/* Plane wave of RadiationSource in that medium, PlaneWaveFieldE / H
+ * (incident_field.h:20-59): k_vec = k_source * direction / |direction|,
+ * h_scale = 1 / (2 pi f mu). */
+int bielcc_planewave_in_medium(const bielcc_medium* md, double freq, const double* direction,
+                               const double* e0, int add_E, int add_H, bielcc_planewave* out);
 
 /* ---- field evaluation ------------------------------------------------- */
 /* E(x_i) = mult * sum_j K[cell_j, J_j](x_i) + E_inc(x_i)

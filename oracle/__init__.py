@@ -65,6 +65,16 @@ def lib(which="port"):
     f = getattr(L, prefix + "cell_geometry")
     f.argtypes = [C.c_int, C.c_int, dp, dp]
     f.restype = C.c_int
+    if which == "ref":
+        f = L.ref_read_mesh
+        f.argtypes = [C.c_int, C.c_int, C.c_char_p, C.POINTER(C.c_int), dp]
+        f.restype = C.c_int
+        f = L.ref_read_currents
+        f.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(C.c_int), dp]
+        f.restype = C.c_int
+        f = L.ref_material
+        f.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, dp, C.c_double, dp]
+        f.restype = C.c_int
     if which == "port":
         f = L.oracle_assemble_K
         f.argtypes = [C.c_int, C.c_int, dp, C.c_double, C.c_double, C.POINTER(abi.NumParam), C.c_int,
@@ -242,3 +252,46 @@ def assemble_K(cells, k, numparam=None, layout=abi.LAYOUT_TAU2, rows=None):
     if rc != 0:
         raise RuntimeError(f"oracle assemble_K failed: {rc}")
     return A
+
+
+def ref_material(freq, eps_r=1.0, mu_r=1.0, sigma=0.0, table=None):
+    """The reference's MaterialParam::Calc and RadiationSource::CalcK at freq:
+    dict of eps, mu (complex), skin_depth, k (CalcK) and calck_threw."""
+    L, _ = lib("ref")
+    out = np.zeros(7)
+    t = None if table is None else _c(table).reshape(-1, 3)
+    disp = abi.DISPERSION_NONE if t is None else abi.DISPERSION_REFRACT
+    L.ref_material(disp, float(eps_r), float(mu_r), float(sigma), 0 if t is None else len(t),
+                   None if t is None else abi.dptr(t), float(freq), abi.dptr(out))
+    return {"eps": complex(out[0], out[1]), "mu": complex(out[2], out[3]), "skin_depth": out[4], "k": out[5],
+            "calck_threw": bool(out[6])}
+
+
+def ref_read_mesh(path, n_vert, fmt):
+    """Cells [N][n_vert][3] as the reference's SurfMesh reader fills them
+    (fmt "dat" or "vtk"); raises on a reader error."""
+    L, _ = lib("ref")
+    n = C.c_int(0)
+    f = 0 if fmt == "dat" else 1
+    rc = L.ref_read_mesh(f, n_vert, os.fsencode(path), C.byref(n), None)
+    if rc != 0:
+        raise RuntimeError(f"reference reader failed on {path}: {rc}")
+    cells = np.zeros((n.value, n_vert, 3))
+    rc = L.ref_read_mesh(f, n_vert, os.fsencode(path), C.byref(n), abi.dptr(cells))
+    if rc != 0:
+        raise RuntimeError(f"reference reader failed on {path}: {rc}")
+    return cells
+
+
+def ref_read_currents(path_re, path_im):
+    """J [N][3] complex as SurfaceCurrentsC_fromFiles reads it."""
+    L, _ = lib("ref")
+    n = C.c_int(0)
+    rc = L.ref_read_currents(os.fsencode(path_re), os.fsencode(path_im), C.byref(n), None)
+    if rc != 0:
+        raise RuntimeError(f"reference current reader failed: {rc}")
+    J = np.zeros((n.value, 3), np.complex128)
+    rc = L.ref_read_currents(os.fsencode(path_re), os.fsencode(path_im), C.byref(n), abi.dptr(J))
+    if rc != 0:
+        raise RuntimeError(f"reference current reader failed: {rc}")
+    return J

@@ -29,6 +29,11 @@
 #include "kernel_lib.h"
 #include "num_param.h"
 #include "incident_field.h"
+#include "material.h"
+#include "radiation_source.h"
+#include "currents.h"
+#include <fstream>
+#include <stdexcept>
 
 #include "../include/bielcc_gpu.h"
 
@@ -464,6 +469,114 @@ int ref_cell_geometry(int n_vert, int n_cells, const double* cells, double* out)
             for (int g = 0; g < 3; g++) { o[7 + g] = t.GetTau1()[g]; o[10 + g] = t.GetTau2()[g]; }
             o[13] = t.GetArea();
         }
+    }
+    return BIELCC_OK;
+}
+
+// The reference's own readers, through their public entry
+// SurfMesh<CellType>::ReadFromFile (mesh/surf_mesh.h:352-363), which picks
+// ReadFromDatFile (mesh/surf_mesh.cpp:18-175) or ReadFromVtkFile
+// (mesh/surf_mesh.h:388-555) by the file's extension; cells as
+// GetCell(i).GetCellCoords(). Counts when cells is NULL; returns -10 when the
+// reader throws. (fmt is the caller's expectation of the format.)
+int ref_read_mesh(int fmt, int n_vert, const char* path, int* n_cells, double* cells) {
+    (void)fmt;
+    try {
+        auto run = [&](auto& m) {
+            m.ReadFromFile(path);
+            const int n = m.GetNFrm();
+            if (cells && *n_cells < n) return BIELCC_ERR_ARG;
+            *n_cells = n;
+            if (cells)
+                for (int c = 0; c < n; c++) {
+                    const auto& v = m.GetCell(c).GetCellCoords();
+                    for (int a = 0; a < n_vert; a++)
+                        for (int g = 0; g < 3; g++) cells[((size_t)c * n_vert + a) * 3 + g] = v[a][g];
+                }
+            return BIELCC_OK;
+        };
+        if (n_vert == 4) {
+            SurfMesh<CellQuad> m;
+            return run(m);
+        }
+        SurfMesh<CellTriangle> m;
+        return run(m);
+    } catch (const std::exception&) {
+        return BIELCC_ERR_IO;
+    }
+}
+
+// SurfaceCurrentsC_fromFiles (electrodynamics/currents.cpp:74-109): J as
+// interleaved complex [n][3]; the vector is presized from the files' header
+// (n1 x n2 values), since the reference writes into it by index.
+int ref_read_currents(const char* path_re, const char* path_im, int* n, double* J) {
+    std::ifstream f(path_re);
+    int n1 = 0, n2 = 0;
+    if (!(f >> n1 >> n2)) return BIELCC_ERR_IO;
+    const int cnt = n1 * n2;
+    if (!J) {
+        *n = cnt;
+        return BIELCC_OK;
+    }
+    if (*n < cnt) return BIELCC_ERR_ARG;
+    std::vector<std::array<cd, 3>> j((size_t)cnt);
+    try {
+        SurfaceCurrentsC_fromFiles(path_re, path_im, j);
+    } catch (const std::exception&) {
+        return BIELCC_ERR_IO;
+    }
+    for (int i = 0; i < cnt; i++)
+        for (int g = 0; g < 3; g++) {
+            J[(6 * (size_t)i) + 2 * g] = j[i][g].real();
+            J[(6 * (size_t)i) + 2 * g + 1] = j[i][g].imag();
+        }
+    *n = cnt;
+    return BIELCC_OK;
+}
+
+// MaterialParam::Calc (electrodynamics/material.cpp:60-128) and
+// RadiationSource::CalcK (radiation_source.cpp:159-180) of the reference.
+// out: eps (re, im), mu (re, im), skin depth (0 if none), k of CalcK, and
+// 1 if CalcK threw (it does for complex eps with its real mu), else 0.
+int ref_material(int dispersion, double eps_r, double mu_r, double sigma, int n_table, const double* table,
+                 double freq, double* out) {
+    MaterialParam m;
+    if (dispersion == BIELCC_DISPERSION_REFRACT) {
+        std::map<double, double> n, ka;
+        bool absorb = false;
+        for (int i = 0; i < n_table; i++) {
+            n[table[3 * i]] = table[3 * i + 1];
+            ka[table[3 * i]] = table[3 * i + 2];
+            absorb = absorb || table[3 * i + 2] != 0.;
+        }
+        if (absorb)
+            m = MaterialParam("m", ChangeMaterialTypeDir::Isotropic, ChangeMaterialTypeFreq::DispersiveByRefractIndex,
+                              n, ka, mu_r);
+        else
+            m = MaterialParam("m", ChangeMaterialTypeDir::Isotropic, ChangeMaterialTypeFreq::DispersiveByRefractIndex,
+                              n, mu_r);
+    } else {
+        m = MaterialParam("m", ChangeMaterialTypeDir::Isotropic, ChangeMaterialTypeFreq::NonDispersive, eps_r, mu_r,
+                          sigma, 0., 0.);
+    }
+    m.Calc(freq);
+    const auto eps = m.GetEps(), mu = m.GetMu();
+    const cd e = std::holds_alternative<double>(eps) ? cd(std::get<double>(eps), 0.) : std::get<cd>(eps);
+    const cd u = std::holds_alternative<double>(mu) ? cd(std::get<double>(mu), 0.) : std::get<cd>(mu);
+    out[0] = e.real();
+    out[1] = e.imag();
+    out[2] = u.real();
+    out[3] = u.imag();
+    out[4] = m.GetSkinDepth() ? *m.GetSkinDepth() : 0.;
+    const double ort[3] = {0., 0., 1.}, e0[3] = {1., 0., 0.};
+    RadiationSource src(RadiationSourceType::PlaneWave, ort, e0);
+    out[5] = 0.;
+    out[6] = 0.;
+    try {
+        src.CalcK(freq, m);
+        out[5] = src.GetK();
+    } catch (const std::bad_variant_access&) {
+        out[6] = 1.;
     }
     return BIELCC_OK;
 }

@@ -161,3 +161,43 @@ def test_batch_edge_cases(gctx, precision, tol):
     outs, _ = _batch(torch, gctx, [sp22], precision, numparam=npm)
     Eo, Ho = oracle.field_EH(sp22["cells"], sp22["J"], sp22["k"], sp22["pts"], npm, mult=sp22["mult"])
     assert rel_l2(outs[0][0], Eo) < tol and rel_l2(outs[0][1], Ho) < tol
+
+
+def test_batch_tensor_core_contraction_matches_cuda_cores(gctx):
+    """Mixed batches contract the far moments with the currents on the tensor
+    cores (TF32 hi + lo, FP32 over 16 cells, FP64 across): the result agrees
+    with the CUDA-core contraction and the oracle within the mixed tolerance,
+    for 1, 5, 16, 17, 33 and 64 right-hand sides (one, two, three and four
+    staged current groups), quads and triangles, real and complex k; a job
+    with more than 64 right-hand sides takes the CUDA-core contraction."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(11)
+    meshes = [W.uv_sphere(8, 16), W.perturbed_icosphere(2, seed=5), W.torus(24, 8), W.rounded_cube(6, 0.1, 1.0),
+              W.spheroid(6, 12, 1.0, 3.0), W.triangulate(W.uv_sphere(6, 12))]
+    specs = []
+    for i, cells in enumerate(meshes):
+        k = [2.0, 6.0, complex(3.0, 0.3), 9.0, 1.5, 4.0][i]
+        S = [1, 5, 16, 17, 33, 64][i]
+        ext = float(np.max(np.linalg.norm(cells.reshape(-1, 3), axis=1)))
+        pts = np.concatenate([W.shell_points(45 + 7 * i, 1.6 * ext, 3 * ext, rng),
+                              W.near_points(cells, 5, 0.02, 0.2, rng)])
+        specs.append(dict(mesh=gctx.mesh(cells), cells=cells, J=W.po_currents(cells, abs(k), directions=S, seed=i),
+                          pts=pts, k=k, mult=complex(0.5, 1.0)))
+    try:
+        gctx.set_batch_tensor_cores(True)
+        tc, rep = _batch(torch, gctx, specs, "mixed")
+        gctx.set_batch_tensor_cores(False)
+        cc, _ = _batch(torch, gctx, specs, "mixed")
+    finally:
+        gctx.set_batch_tensor_cores(True)
+    assert rep.n_near_pairs > 0
+    for sp, (E, H), (Ec, Hc) in zip(specs, tc, cc):
+        assert rel_l2(E, Ec) < TOL_MIXED and rel_l2(H, Hc) < TOL_MIXED
+        s2 = min(3, sp["J"].shape[0])
+        Eo, Ho = oracle.field_EH(sp["cells"], sp["J"][:s2], sp["k"], sp["pts"], mult=sp["mult"])
+        assert rel_l2(E[:s2], Eo) < TOL_MIXED and rel_l2(H[:s2], Ho) < TOL_MIXED
+    # more than 64 right-hand sides: the CUDA-core contraction, same results as per-job calls
+    big = dict(specs[0], J=W.po_currents(meshes[0], 2.0, directions=70, seed=3))
+    out, _ = _batch(torch, gctx, [big], "mixed")
+    Eo, Ho = oracle.field_EH(big["cells"], big["J"][::23], big["k"], big["pts"], mult=big["mult"])
+    assert rel_l2(out[0][0][::23], Eo) < TOL_MIXED and rel_l2(out[0][1][::23], Ho) < TOL_MIXED

@@ -27,12 +27,12 @@ def _case():
     return cells, k, pts, JE, JM
 
 
-def _reference(cells, k, pts, JE, JM, inc):
+def _reference(cells, k, pts, JE, JM, inc, mult_e=MULT_E, mult_h=MULT_H):
     which = "ref" if oracle.available("ref") else "port"
     KE, RE = oracle.field_EH(cells, JE, k, pts, which=which)
     KM, RM = oracle.field_EH(cells, JM, k, pts, which=which)
-    E = MULT_E * KE - RM
-    H = MULT_H * KM + RE
+    E = mult_e * KE - RM
+    H = mult_h * KM + RE
     if inc is not None:
         kvec = np.array(inc.k_vec[:])
         e0 = np.array(inc.e0[:])
@@ -105,3 +105,29 @@ def test_extinction_theorem_sphere(gctx):
     Hin = hs * np.cross(kv, e0)[None, :] * pin
     assert rel_l2(Ei[0], Ein) < 0.05 and rel_l2(Hi[0], Hin) < 0.05
     assert np.sqrt(np.mean(np.abs(Eo[0]) ** 2)) < 0.05 and np.sqrt(np.mean(np.abs(Ho[0]) ** 2)) < 0.05
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", TOL_FP64), ("mixed", TOL_MIXED)])
+def test_full_field_in_lossy_medium(gctx, precision, tol):
+    """A body in a lossy dielectric (eps_r = 2, sigma = 2 mS/m at the frequency
+    where Re k = 2 pi): the medium's complex wave number (Im k > 0), multE =
+    i / (omega eps), multH = i / (omega mu) and incident plane wave from
+    bielcc_medium_at / bielcc_planewave_in_medium (MaterialParam::Calc,
+    RadiationSource::CalcK, main0_field_test.cpp:185-199), through
+    bielcc_field_EH_full, against the reference's own field sums with that
+    complex k (KType = std::complex<double>) combined as the example does."""
+    from bielcc_b200 import gpu
+
+    c0 = 299792458.0
+    freq = c0 / np.sqrt(2.0)  # Re k ~ 2 pi in eps_r = 2
+    md = gpu.medium_at(gpu.material(eps_r=2.0, sigma=2e-3), freq)
+    k = md.cplx("k")
+    assert k.imag > 0.05 and abs(k.real - 2 * np.pi) < 0.2
+    inc = gpu.planewave_in_medium(md, freq, direction=(0, 0, 1), e0=(1, 0, 0))
+    cells, _, pts, JE, JM = _case()
+    multE, multH = md.cplx("multE"), md.cplx("multH")
+    m = gctx.mesh(cells)
+    E, H, rep = gctx.field_EH_full(m, JE, JM, k, pts, multE=multE, multH=multH, inc=inc, precision=precision)
+    Er, Hr = _reference(cells, k, pts, JE, JM, inc, multE, multH)
+    assert rep.n_near_pairs > 0 and rep.n_nonfinite == 0
+    assert rel_l2(E, Er) < tol and rel_l2(H, Hr) < tol

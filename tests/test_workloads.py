@@ -39,3 +39,21 @@ def test_config_points():
     assert c2["pts"].shape == (20000, 3)
     r = np.linalg.norm(c2["pts"][:18000], axis=1)
     assert r.min() >= 2.0 and r.max() <= 5.0
+
+
+def test_batch_meshes_mix_quads_and_triangles():
+    """The batched workload draws quads and triangles (config 4: "quad or
+    triangle cells"), 200-20,000 cells, no degenerate triangles."""
+    js = W.batch_meshes(n_meshes=24, seed=3)
+    nv = {j["cells"].shape[1] for j in js}
+    assert nv == {3, 4}
+    for j in js:
+        c = j["cells"]
+        assert 150 <= len(c) <= 21000
+        assert np.isfinite(W.normals(c)).all()
+    q = W.uv_sphere(8, 16)
+    t = W.triangulate(q)
+    # the pole quads lose their collapsed halves; every other quad gives two triangles
+    assert len(t) == 2 * len(q) - 2 * 16
+    area = lambda c: 0.5 * np.linalg.norm(np.cross(c[:, 1] - c[:, 0], c[:, 2] - c[:, 0]), axis=1).sum()
+    assert abs(area(t) - sum(area(q[:, [0, 1, 2]]) + area(q[:, [2, 3, 0]]) for _ in [0])) < 1e-9
