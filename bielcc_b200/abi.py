@@ -198,6 +198,7 @@ class FieldJob(C.Structure):
         ("mult_re", C.c_double),
         ("mult_im", C.c_double),
         ("inc", PlaneWave),
+        ("est_dev", C.c_void_p),
     ]
 
 
@@ -219,6 +220,7 @@ class FieldRequest(C.Structure):
         ("mult_re", C.c_double),
         ("mult_im", C.c_double),
         ("inc", PlaneWave),
+        ("est", C.c_void_p),
     ]
 
 

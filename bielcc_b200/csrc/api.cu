@@ -96,6 +96,7 @@ struct bielcc_ctx_s {
     // runs beside the main evaluation (bielcc_field_EH)
     cudaStream_t side = nullptr;
     cudaEvent_t side_in = nullptr;
+    cudaEvent_t side_out = nullptr;  // the side stream's error sample is complete
     DevBuf side_ws, side_pair_ws, side_io, side_scratch;
     bool batch_tc = true;               // mixed batches contract on the tensor cores when they qualify
     long long* h_side_total = nullptr;  // pinned
@@ -379,6 +380,102 @@ int field_device(bielcc_ctx ctx, const FieldArgs& a, cudaStream_t s, bielcc_repo
     return field_finish(ctx, p, s, rep, d_nonfinite, w);
 }
 
+// Error sample of a single-job mixed evaluation: the FP64 field at
+// Q = min(P, 256) points spread over the set (two full point tiles), all
+// right-hand sides, evaluated on the side stream beside the main evaluation
+// and compared with the mixed outputs on the device (estimate.cu). `full`:
+// the outputs are the full Stratton-Chu combination of a 2S-RHS evaluation,
+// so the sample is combined the same way before the comparison.
+struct SingleEst {
+    bool on = false;
+    int Q = 0;
+    ErrJob* d_job = nullptr;
+    double *spts = nullptr, *Eq = nullptr, *Hq = nullptr, *Ec = nullptr, *Hc = nullptr, *nd = nullptr,
+           *sums = nullptr;
+    FieldPending ps;
+    bool full = false;
+    cplx multE, multH;
+    const bielcc_planewave* inc = nullptr;
+    int S_out = 0;
+};
+
+// a: the main evaluation's arguments (precision mixed); E_out / H_out: the
+// outputs compared (a.E / a.H, or the full-field combination), S_out right-hand
+// sides each.
+int est_single_begin(bielcc_ctx ctx, const FieldArgs& a, cudaStream_t s, SingleEst& e, const double* E_out,
+                     const double* H_out, int S_out) {
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    e.on = true;
+    e.Q = std::min(a.n_pts, 256);
+    e.S_out = S_out;
+    const size_t Q = e.Q, Sa = a.n_rhs;
+    const size_t bQ = Q * 24, bQo = Sa * Q * 48, bC = (size_t)S_out * Q * 48;
+    TRY(ctx->side_io.ensure(3 * 256 + al(bQ) + 2 * al(bQo) + 2 * al(bC)));
+    char* b = (char*)ctx->side_io.p;
+    e.d_job = (ErrJob*)b;
+    e.nd = (double*)(b + 256);
+    e.sums = (double*)(b + 512);
+    e.spts = (double*)(b + 768);
+    e.Eq = (double*)(b + 768 + al(bQ));
+    e.Hq = (double*)(b + 768 + al(bQ) + al(bQo));
+    e.Ec = (double*)(b + 768 + al(bQ) + 2 * al(bQo));
+    e.Hc = (double*)(b + 768 + al(bQ) + 2 * al(bQo) + al(bC));
+    ErrJob j{};
+    j.pts = a.pts;
+    j.P = a.n_pts;
+    j.Q = e.Q;
+    j.S = S_out;
+    j.Ss = S_out;
+    j.off = 0;
+    j.E = E_out;
+    j.H = H_out;
+    j.Eq = e.full ? e.Ec : e.Eq;
+    j.Hq = H_out ? (e.full ? e.Hc : e.Hq) : nullptr;
+    TRY(ensure_tables(a.m, a.np.n_start, s));
+    TRY_CUDA(cudaEventRecord(ctx->side_in, s));  // inputs and node tables on the device
+    TRY_CUDA(cudaStreamWaitEvent(ctx->side, ctx->side_in, 0));
+    TRY_CUDA(cudaMemcpyAsync(e.d_job, &j, sizeof(j), cudaMemcpyHostToDevice, ctx->side));
+    TRY_CUDA(err_gather(e.d_job, 1, e.spts, ctx->side));
+    FieldArgs b64{a.m, a.n_rhs, a.J, a.k, a.mult, a.inc, a.np, e.Q, e.spts, e.Eq, (H_out || e.full) ? e.Hq : nullptr,
+                  BIELCC_PREC_FP64};
+    return field_begin(ctx, b64, ctx->side, nullptr, nullptr, side_ws(ctx), &e.ps);
+}
+
+// Completes the sample on the side stream and enqueues the comparison on s
+// (after the main evaluation's outputs); the sums land in h_total[4], [5].
+int est_single_finish(bielcc_ctx ctx, cudaStream_t s, SingleEst& e) {
+    TRY(field_finish(ctx, e.ps, ctx->side, nullptr, nullptr, side_ws(ctx)));
+    if (e.full) {
+        FullInc fi;
+        memset(&fi, 0, sizeof(fi));
+        if (e.inc) {
+            for (int g = 0; g < 3; g++) {
+                fi.kvec[g] = e.inc->k_vec[g];
+                fi.e0[g] = e.inc->e0[g];
+            }
+            fi.h_scale = e.inc->h_scale;
+            fi.add_E = e.inc->add_E;
+            fi.add_H = e.inc->add_H;
+        }
+        TRY_CUDA(launch_combine_full(e.Eq, e.Hq, e.S_out, e.Q, e.multE, e.multH, e.spts, fi, e.Ec, e.Hc, nullptr,
+                                     ctx->side));
+    }
+    TRY_CUDA(cudaEventRecord(ctx->side_out, ctx->side));
+    TRY_CUDA(cudaStreamWaitEvent(s, ctx->side_out, 0));
+    TRY_CUDA(err_compare(e.d_job, 1, e.nd, e.sums, s));
+    TRY_CUDA(cudaMemcpyAsync(ctx->h_total + 4, e.sums, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    ctx->stats.kernel_launches += 3 + (e.full ? 1 : 0);
+    return BIELCC_OK;
+}
+
+// After the stream has been synchronised: the estimate into the report.
+void est_single_report(bielcc_ctx ctx, const SingleEst& e, bielcc_report* rep) {
+    if (!e.on || !rep) return;
+    const double* v = reinterpret_cast<const double*>(ctx->h_total + 4);
+    rep->est_rel_l2 = v[1] > 0. ? sqrt(v[0] / v[1]) : 0.;
+    rep->est_sample = e.Q;
+}
+
 }  // namespace
 
 extern "C" {
@@ -416,6 +513,7 @@ int bielcc_ctx_create(int device, bielcc_ctx* out) {
     if (e == cudaSuccess) e = cudaEventCreate(&c->far_end);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->side_in, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->side_out, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaMallocHost(&c->h_side_total, 64);
     if (e != cudaSuccess) {
         if (c->h_total) cudaFreeHost(c->h_total);
@@ -424,6 +522,7 @@ int bielcc_ctx_create(int device, bielcc_ctx* out) {
         if (c->far_begin) cudaEventDestroy(c->far_begin);
         if (c->far_end) cudaEventDestroy(c->far_end);
         if (c->side_in) cudaEventDestroy(c->side_in);
+        if (c->side_out) cudaEventDestroy(c->side_out);
         if (c->side) cudaStreamDestroy(c->side);
         if (c->stream) cudaStreamDestroy(c->stream);
         delete c;
@@ -451,6 +550,7 @@ int bielcc_ctx_destroy(bielcc_ctx ctx) {
     ctx->side_scratch.release();
     if (ctx->h_side_total) cudaFreeHost(ctx->h_side_total);
     if (ctx->side_in) cudaEventDestroy(ctx->side_in);
+    if (ctx->side_out) cudaEventDestroy(ctx->side_out);
     if (ctx->side) cudaStreamDestroy(ctx->side);
     if (ctx->h_total) cudaFreeHost(ctx->h_total);  // h_nonfinite lives in the same pinned block
     if (ctx->ws_done) cudaEventDestroy(ctx->ws_done);
@@ -583,7 +683,17 @@ int bielcc_field_EH_device(bielcc_ctx ctx, bielcc_mesh mesh, int n_rhs, const do
     FieldArgs a{m, n_rhs, J_dev, mk(k_re, k_im), mk(mult_re, mult_im), inc, n, n_pts, pts_dev, E_dev, H_dev,
                 precision};
     if (report) memset(report, 0, sizeof(*report));
+    // mixed with a report: the error sample runs beside the evaluation and the
+    // call waits for the stream to fill est_rel_l2
+    const bool sample = report && precision == BIELCC_PREC_MIXED && n_pts > 0;
+    SingleEst es;
+    if (sample) TRY(est_single_begin(ctx, a, s, es, E_dev, H_dev, n_rhs));
     TRY(field_device(ctx, a, s, report, nullptr));
+    if (sample) {
+        TRY(est_single_finish(ctx, s, es));
+        TRY_CUDA(cudaStreamSynchronize(s));
+        est_single_report(ctx, es, report);
+    }
     TRY(ws_release(ctx, s));
     return BIELCC_OK;
 }
@@ -597,7 +707,8 @@ namespace {
 // right-hand sides (mult 1, no incident field), then the combination.
 int field_full_core(bielcc_ctx ctx, MeshDev* m, int S, const double* JE, const double* JM, cplx k, cplx multE,
                     cplx multH, const bielcc_planewave* inc, const NumParamH& n, int P, const double* pts, double* E,
-                    double* H, int precision, cudaStream_t s, bielcc_report* rep, unsigned long long* d_nf) {
+                    double* H, int precision, cudaStream_t s, bielcc_report* rep, unsigned long long* d_nf,
+                    SingleEst* es) {
     auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
     const size_t N = m->n_cells, bJ = (size_t)S * N * 48, bO = (size_t)S * P * 48;
     TRY(ctx->full.ensure(al(2 * bJ) + 2 * al(2 * bO) + 256));
@@ -609,6 +720,13 @@ int field_full_core(bielcc_ctx ctx, MeshDev* m, int S, const double* JE, const d
     TRY_CUDA(cudaMemcpyAsync((char*)J2 + bJ, JM, bJ, cudaMemcpyDeviceToDevice, s));
     if (P == 0) return BIELCC_OK;
     FieldArgs a{m, 2 * S, J2, k, mk(1.0, 0.0), nullptr, n, P, pts, E2, H2, precision};
+    if (es) {  // the error sample of the combined field (the caller reports it after its sync)
+        es->full = true;
+        es->multE = multE;
+        es->multH = multH;
+        es->inc = inc;
+        TRY(est_single_begin(ctx, a, s, *es, E, H, S));
+    }
     TRY(field_device(ctx, a, s, rep, nullptr));
     FullInc fi;
     memset(&fi, 0, sizeof(fi));
@@ -623,6 +741,7 @@ int field_full_core(bielcc_ctx ctx, MeshDev* m, int S, const double* JE, const d
     }
     TRY_CUDA(launch_combine_full(E2, H2, S, P, multE, multH, pts, fi, E, H, d_nf, s));
     ctx->stats.kernel_launches += 1;
+    if (es) TRY(est_single_finish(ctx, s, *es));
     return BIELCC_OK;
 }
 
@@ -648,8 +767,15 @@ int bielcc_field_EH_full_device(bielcc_ctx ctx, bielcc_mesh mesh, int n_rhs, con
     cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
     if (report) memset(report, 0, sizeof(*report));
     TRY(ws_acquire(ctx, s));
+    const bool sample = report && precision == BIELCC_PREC_MIXED && n_pts > 0;
+    SingleEst es;
     TRY(field_full_core(ctx, m, n_rhs, JE_dev, JM_dev, mk(k_re, k_im), mk(multE_re, multE_im),
-                        mk(multH_re, multH_im), inc, n, n_pts, pts_dev, E_dev, H_dev, precision, s, report, nullptr));
+                        mk(multH_re, multH_im), inc, n, n_pts, pts_dev, E_dev, H_dev, precision, s, report, nullptr,
+                        sample ? &es : nullptr));
+    if (sample) {
+        TRY_CUDA(cudaStreamSynchronize(s));
+        est_single_report(ctx, es, report);
+    }
     TRY(ws_release(ctx, s));
     return BIELCC_OK;
 }
@@ -686,8 +812,10 @@ int bielcc_field_EH_full(bielcc_ctx ctx, bielcc_mesh mesh, int n_rhs, const doub
     TRY_CUDA(cudaMemcpyAsync(dJM, J_M, bJ, cudaMemcpyHostToDevice, s));
     if (P) TRY_CUDA(cudaMemcpyAsync(dP, pts, bP, cudaMemcpyHostToDevice, s));
     TRY_CUDA(cudaMemsetAsync(d_nf, 0, sizeof(unsigned long long), s));
+    const bool sample = report && precision == BIELCC_PREC_MIXED && n_pts > 0;
+    SingleEst es;
     TRY(field_full_core(ctx, m, n_rhs, dJE, dJM, mk(k_re, k_im), mk(multE_re, multE_im), mk(multH_re, multH_im),
-                        inc, n, n_pts, dP, dE, dH, precision, s, report, d_nf));
+                        inc, n, n_pts, dP, dE, dH, precision, s, report, d_nf, sample ? &es : nullptr));
     if (P) {
         TRY_CUDA(cudaMemcpyAsync(E, dE, bO, cudaMemcpyDeviceToHost, s));
         TRY_CUDA(cudaMemcpyAsync(H, dH, bO, cudaMemcpyDeviceToHost, s));
@@ -701,6 +829,7 @@ int bielcc_field_EH_full(bielcc_ctx ctx, bielcc_mesh mesh, int n_rhs, const doub
         report->n_nonfinite = (int64_t)nf;
         report->status = rc;
     }
+    est_single_report(ctx, es, report);
     return rc;
 }
 
@@ -735,45 +864,18 @@ int bielcc_field_EH(bielcc_ctx ctx, bielcc_mesh mesh, int n_rhs, const double* J
     TRY_CUDA(cudaMemsetAsync(d_nf, 0, sizeof(unsigned long long), s));
     FieldArgs a{m, n_rhs, dJ, mk(k_re, k_im), mk(mult_re, mult_im), inc, n, n_pts, dP, dE, dH, precision};
     // Mixed form: its relative L2 error against the FP64 form on a sample of
-    // Q = min(P, 256) points spread over the set (two full point tiles),
-    // evaluated on the side stream beside the main evaluation.
+    // min(P, 256) points, evaluated on the side stream beside the main one.
     const bool sample = report && precision == BIELCC_PREC_MIXED && P > 0;
-    const size_t Q = sample ? std::min<size_t>(P, 256) : 0;
-    std::vector<size_t> idx(Q);
-    for (size_t q = 0; q < Q; q++) idx[q] = q * P / Q;
-    const size_t bQ = Q * 3 * 8, bQo = S * Q * 3 * 16;
-    double *dQ = nullptr, *dEq = nullptr, *dHq = nullptr;
-    std::vector<double> e64(S * Q * 6), h64(S * Q * 6);
-    FieldPending pm, ps;
-    const WsSet wm = main_ws(ctx), wsd = side_ws(ctx);
-    std::vector<double> sp(Q * 3);
-    if (sample) {
-        for (size_t q = 0; q < Q; q++)
-            for (int g = 0; g < 3; g++) sp[3 * q + g] = pts[3 * idx[q] + g];
-        TRY(ctx->side_io.ensure(al(bQ) + 2 * al(bQo) + 256));
-        char* sio = (char*)ctx->side_io.p;
-        dQ = (double*)sio;
-        dEq = (double*)(sio + al(bQ));
-        dHq = (double*)(sio + al(bQ) + al(bQo));
-        TRY(ensure_tables(m, n.n_start, s));
-        TRY_CUDA(cudaEventRecord(ctx->side_in, s));  // currents and node tables on the device
-        TRY_CUDA(cudaStreamWaitEvent(ctx->side, ctx->side_in, 0));
-        TRY_CUDA(cudaMemcpyAsync(dQ, sp.data(), bQ, cudaMemcpyHostToDevice, ctx->side));
-    }
-    FieldArgs b{m, n_rhs, dJ, mk(k_re, k_im), mk(mult_re, mult_im), inc, n, (int)Q, dQ, dEq, H ? dHq : nullptr,
-                BIELCC_PREC_FP64};
+    FieldPending pm;
+    SingleEst es;
+    const WsSet wm = main_ws(ctx);
+    if (sample) TRY(est_single_begin(ctx, a, s, es, dE, dH, n_rhs));
     if (P) TRY(field_begin(ctx, a, s, report, d_nf, wm, &pm));
-    if (sample) TRY(field_begin(ctx, b, ctx->side, nullptr, nullptr, wsd, &ps));
     if (P) TRY(field_finish(ctx, pm, s, report, d_nf, wm));
+    if (sample) TRY(est_single_finish(ctx, s, es));
     if (P) TRY_CUDA(cudaMemcpyAsync(E, dE, bO, cudaMemcpyDeviceToHost, s));
     if (P && H) TRY_CUDA(cudaMemcpyAsync(H, dH, bO, cudaMemcpyDeviceToHost, s));
     TRY_CUDA(cudaMemcpyAsync(ctx->h_nonfinite, d_nf, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
-    if (sample) {
-        TRY(field_finish(ctx, ps, ctx->side, nullptr, nullptr, wsd));
-        TRY_CUDA(cudaMemcpyAsync(e64.data(), dEq, bQo, cudaMemcpyDeviceToHost, ctx->side));
-        if (H) TRY_CUDA(cudaMemcpyAsync(h64.data(), dHq, bQo, cudaMemcpyDeviceToHost, ctx->side));
-        TRY_CUDA(cudaStreamSynchronize(ctx->side));
-    }
     TRY_CUDA(cudaStreamSynchronize(s));
     TRY(ws_release(ctx, s));
     int rc = BIELCC_OK;
@@ -783,24 +885,7 @@ int bielcc_field_EH(bielcc_ctx ctx, bielcc_mesh mesh, int n_rhs, const double* J
         report->n_nonfinite = (int64_t)nf;
         report->status = rc;
     }
-    if (sample) {
-        double num = 0, den = 0;
-        for (size_t r = 0; r < S; r++)
-            for (size_t q = 0; q < Q; q++)
-                for (int c = 0; c < 6; c++) {
-                    double ref = e64[(r * Q + q) * 6 + c], got = E[(r * P + idx[q]) * 6 + c];
-                    num += (got - ref) * (got - ref);
-                    den += ref * ref;
-                    if (H) {
-                        ref = h64[(r * Q + q) * 6 + c];
-                        got = H[(r * P + idx[q]) * 6 + c];
-                        num += (got - ref) * (got - ref);
-                        den += ref * ref;
-                    }
-                }
-        report->est_rel_l2 = den > 0 ? sqrt(num / den) : 0.;
-        report->est_sample = (int32_t)Q;
-    }
+    est_single_report(ctx, es, report);
     return rc;
 }
 
@@ -859,6 +944,104 @@ int check_jobs(bielcc_ctx ctx, int n_jobs, const bielcc_field_job* jobs, std::ve
     return BIELCC_OK;
 }
 
+// Error sample of a mixed batch: per job min(P, 32) points spread over its set
+// and its first min(S, 4) right-hand sides, evaluated as one FP64 batch on the
+// side stream (side workspaces) beside the main batch, then compared with the
+// main outputs on the device: each job's estimate to its est_dev, the sums
+// over all jobs to h_total[4], [5].
+struct BatchEst {
+    bool on = false;
+    int n_jobs = 0, total_q = 0;
+    std::vector<ErrJob> ej;
+    std::vector<JobDev> js;
+    ErrJob* d_ej = nullptr;
+    double *spts = nullptr, *nd = nullptr, *sums = nullptr;
+    BatchPlan bp;
+    BatchDevPtrs d{};
+    int l1 = 0;
+};
+
+int batch_est_begin(bielcc_ctx ctx, const std::vector<JobDev>& jd, const bielcc_field_job* jobs, const NumParamH& n,
+                    bool ck, double item_cost, cudaStream_t s, BatchEst& e) {
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    e.on = true;
+    e.n_jobs = (int)jd.size();
+    e.ej.assign(jd.size(), ErrJob{});
+    size_t tq = 0, tout = 0;
+    for (size_t i = 0; i < jd.size(); i++) {
+        const int Q = std::min(jd[i].n_pts, 32), Ss = std::min(jd[i].n_rhs, 4);
+        tq += Q;
+        tout += (size_t)Ss * Q;
+    }
+    e.total_q = (int)tq;
+    const size_t b_ej = al(jd.size() * sizeof(ErrJob)), b_nd = al(jd.size() * 16 + 16), b_p = al(tq * 24),
+                 b_o = al(tout * 48);
+    TRY(ctx->side_io.ensure(b_ej + b_nd + b_p + 2 * b_o + 256));
+    char* b = (char*)ctx->side_io.p;
+    e.d_ej = (ErrJob*)b;
+    e.nd = (double*)(b + b_ej);
+    e.sums = e.nd + 2 * jd.size();
+    e.spts = (double*)(b + b_ej + b_nd);
+    double* Eq = (double*)(b + b_ej + b_nd + b_p);
+    double* Hq = (double*)(b + b_ej + b_nd + b_p + b_o);
+    e.js.assign(jd.begin(), jd.end());
+    size_t oq = 0, oo = 0;
+    for (size_t i = 0; i < jd.size(); i++) {
+        const JobDev& j = jd[i];
+        const int Q = std::min(j.n_pts, 32), Ss = std::min(j.n_rhs, 4);
+        ErrJob& r = e.ej[i];
+        r.pts = j.pts;
+        r.P = j.n_pts;
+        r.Q = Q;
+        r.S = j.n_rhs;
+        r.Ss = Ss;
+        r.off = (int)oq;
+        r.E = j.E;
+        r.H = j.H;
+        r.E32 = j.E32;
+        r.H32 = j.H32;
+        r.Eq = Eq + 2 * 3 * oo;
+        r.Hq = (j.H || j.H32) ? Hq + 2 * 3 * oo : nullptr;
+        r.est_dev = jobs ? jobs[i].est_dev : nullptr;
+        JobDev& q = e.js[i];
+        q.pts = e.spts + 3 * oq;
+        q.n_pts = Q;
+        q.n_rhs = Ss;  // the first Ss right-hand sides: the leading part of J
+        q.E = const_cast<double*>(r.Eq);
+        q.H = const_cast<double*>(r.Hq);
+        q.E32 = q.H32 = nullptr;
+        q.nonfinite = nullptr;
+        oq += Q;
+        oo += (size_t)Ss * Q;
+    }
+    TRY_CUDA(cudaEventRecord(ctx->side_in, s));
+    TRY_CUDA(cudaStreamWaitEvent(ctx->side, ctx->side_in, 0));
+    TRY_CUDA(cudaMemcpyAsync(e.d_ej, e.ej.data(), jd.size() * sizeof(ErrJob), cudaMemcpyHostToDevice, ctx->side));
+    TRY_CUDA(err_gather(e.d_ej, e.n_jobs, e.spts, ctx->side));
+    plan_batch(e.bp, e.js, n.n_start, false, item_cost, false);
+    TRY(ctx->side_ws.ensure(e.bp.ws_bytes));
+    TRY_CUDA(batch_stage1(e.bp, ctx->side_ws.p, n.analytic_calc, n.n_start, ck, ctx->side, &e.d, &e.l1));
+    TRY_CUDA(batch_status_to_host(e.d, ctx->h_side_total, ctx->side));
+    return BIELCC_OK;
+}
+
+int batch_est_finish(bielcc_ctx ctx, const NumParamH& n, cudaStream_t s, BatchEst& e) {
+    TRY_CUDA(cudaStreamSynchronize(ctx->side));
+    if (batch_timed_out(ctx->h_side_total))
+        return set_error(BIELCC_ERR_TIMEOUT, "batched far kernel: a bounded wait ran out");
+    const long long n_near = *ctx->h_side_total;
+    if (n_near > 0) TRY(ctx->side_pair_ws.ensure(batch_pair_ws_bytes(n_near)));
+    DNP dn{n.eps, n.rs, n.rs_seg, n.analytic_calc, n.n_start, n.n_start_seg, n.p_max, n.p_max_seg};
+    int l2 = 0;
+    TRY_CUDA(batch_stage2(e.bp, e.d, n_near, ctx->side_pair_ws.p, dn, nullptr, ctx->side, &l2));
+    TRY_CUDA(cudaEventRecord(ctx->side_out, ctx->side));
+    TRY_CUDA(cudaStreamWaitEvent(s, ctx->side_out, 0));
+    TRY_CUDA(err_compare(e.d_ej, e.n_jobs, e.nd, e.sums, s));
+    TRY_CUDA(cudaMemcpyAsync(ctx->h_total + 4, e.sums, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    ctx->stats.kernel_launches += e.l1 + l2 + 3;
+    return BIELCC_OK;
+}
+
 int field_batch_locked(bielcc_ctx ctx, int n_jobs, const bielcc_field_job* jobs, const NumParamH& n, int precision,
                        cudaStream_t s, bielcc_report* report, double item_cost) {
     std::vector<MeshDev*> meshes;
@@ -884,6 +1067,12 @@ int field_batch_locked(bielcc_ctx ctx, int n_jobs, const bielcc_field_job* jobs,
     bool ck = false;
     int64_t pairs = 0;
     TRY(jobs_to_dev(n_jobs, jobs, meshes, n, s, jd, &ck, &pairs));
+    // mixed: the error sample, with a report or when a job asks for its estimate
+    bool want_est = report != nullptr;
+    for (int i = 0; i < n_jobs; i++) want_est = want_est || jobs[i].est_dev;
+    BatchEst es;
+    if (precision == BIELCC_PREC_MIXED && want_est && n_jobs > 0)
+        TRY(batch_est_begin(ctx, jd, jobs, n, ck, item_cost, s, es));
     BatchPlan bp;
     plan_batch(bp, jd, n.n_start, precision == BIELCC_PREC_MIXED, item_cost, ctx->batch_tc);
     TRY(ctx->ws.ensure(bp.ws_bytes));
@@ -898,14 +1087,21 @@ int field_batch_locked(bielcc_ctx ctx, int n_jobs, const bielcc_field_job* jobs,
     if (n_near > 0) TRY(ctx->pair_ws.ensure(batch_pair_ws_bytes(n_near)));
     DNP dn{n.eps, n.rs, n.rs_seg, n.analytic_calc, n.n_start, n.n_start_seg, n.p_max, n.p_max_seg};
     TRY_CUDA(batch_stage2(bp, d, n_near, ctx->pair_ws.p, dn, nullptr, s, &l2));
+    if (es.on) TRY(batch_est_finish(ctx, n, s, es));
     ctx->stats.kernel_launches += l1 + l2;
     ctx->stats.far_launches += 1;
     ctx->stats.far_pairs += pairs;
-    TRY(ws_release(ctx, s));
     if (report) {
         report->n_pairs = pairs;
         report->n_near_pairs = n_near;
+        if (es.on) {  // the estimate of the whole batch: wait for the stream
+            TRY_CUDA(cudaStreamSynchronize(s));
+            const double* v = reinterpret_cast<const double*>(ctx->h_total + 4);
+            report->est_rel_l2 = v[1] > 0. ? sqrt(v[0] / v[1]) : 0.;
+            report->est_sample = es.total_q;
+        }
     }
+    TRY(ws_release(ctx, s));
     return BIELCC_OK;
 }
 
@@ -1373,11 +1569,27 @@ int bielcc_assemble_K_device(bielcc_ctx ctx, bielcc_mesh mesh, double k_re, doub
     if (n_near > 0) TRY(ctx->pair_ws.ensure((size_t)n_near * (2 * sizeof(int)) + 1024));
     TRY_CUDA(assemble_stage2(a, ctx->ws.p, n_near, ctx->pair_ws.p, s));
     ctx->stats.kernel_launches += 3 + (n_near > 0 ? 2 : 0);
+    // mixed with a report: min(N, 16) sampled rows in FP64 against the stored
+    // matrix, and the call waits for the stream to fill est_rel_l2
+    const int R = (report && precision == BIELCC_PREC_MIXED) ? std::min(m->n_cells, 16) : 0;
+    if (R > 0) {
+        TRY(ctx->side_io.ensure(assemble_error_ws_bytes(a, R) + 256));
+        double* sums = (double*)((char*)ctx->side_io.p + assemble_error_ws_bytes(a, R));
+        TRY_CUDA(assemble_error_sample(a, R, ctx->side_io.p, sums, s));
+        TRY_CUDA(cudaMemcpyAsync(ctx->h_total + 4, sums, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        TRY_CUDA(cudaStreamSynchronize(s));
+        ctx->stats.kernel_launches += 2;
+    }
     TRY(ws_release(ctx, s));
     if (report) {
         memset(report, 0, sizeof(*report));
         report->n_pairs = (int64_t)m->n_cells * m->n_cells;
         report->n_near_pairs = n_near;
+        if (R > 0) {
+            const double* v = reinterpret_cast<const double*>(ctx->h_total + 4);
+            report->est_rel_l2 = v[1] > 0. ? sqrt(v[0] / v[1]) : 0.;
+            report->est_sample = R;
+        }
     }
     return BIELCC_OK;
 }

@@ -442,6 +442,27 @@ __global__ void asm_mask_fill_kernel(const unsigned* __restrict__ mask, int n_wo
     }
 }
 
+// K_RotRot_HS_Colloc (electrodynamics/K.h:179-204) at x as a 3x3 operator, FP64.
+BIELCC_D void near_operator(const DCell& cl, const double* x, cplx k, const DNP& np, double (&Kr)[3][3],
+                            double (&Ki)[3][3]) {
+    cplx I = surf_simplepot_h_hs_dev(cl, x, np.analytic_calc, np.n_start, np.p_max, np.eps, k);
+    cplx sI = I * k * k / kFourPi;
+    DKP ps;
+    dkp_zero(ps);
+    ps.smoothR = kMachineZero;
+    ps.smoothRMin = kMachineZero;
+    ps.k = k;
+    cplx M[3][3], dummy[3];
+    K0_dev(F_GRADSIMPLEPOT_H, nullptr, x, cl, ps, np.n_start_seg, np.p_max_seg, np.eps, dummy, M);
+    for (int p = 0; p < 3; p++)
+        for (int r = 0; r < 3; r++) {
+            cplx v = M[p][r] / kFourPi;
+            if (p == r) v += sI;
+            Kr[p][r] = v.re;
+            Ki[p][r] = v.im;
+        }
+}
+
 // Near entries: K_RotRot_HS_Colloc as a 3x3 operator, FP64.
 __global__ void asm_near_kernel(AsmArgs a, const double* __restrict__ verts, int nv, const int* __restrict__ pr,
                                 const int* __restrict__ pc, long long n_pairs, DNP np) {
@@ -454,24 +475,96 @@ __global__ void asm_near_kernel(AsmArgs a, const double* __restrict__ verts, int
     for (int v = 0; v < nv; v++)
         for (int g = 0; g < 3; g++) cl.v[v][g] = verts[((size_t)j * nv + v) * 3 + g];
     const double* x = gi.c;
-    cplx I = surf_simplepot_h_hs_dev(cl, x, np.analytic_calc, np.n_start, np.p_max, np.eps, a.k);
-    cplx sI = I * a.k * a.k / kFourPi;
-    DKP ps;
-    dkp_zero(ps);
-    ps.smoothR = kMachineZero;
-    ps.smoothRMin = kMachineZero;
-    ps.k = a.k;
-    cplx M[3][3], dummy[3];
-    K0_dev(F_GRADSIMPLEPOT_H, nullptr, x, cl, ps, np.n_start_seg, np.p_max_seg, np.eps, dummy, M);
     double Kr[3][3], Ki[3][3];
-    for (int p = 0; p < 3; p++)
-        for (int r = 0; r < 3; r++) {
-            cplx v = M[p][r] / kFourPi;
-            if (p == r) v += sI;
-            Kr[p][r] = v.re;
-            Ki[p][r] = v.im;
-        }
+    near_operator(cl, x, a.k, np, Kr, Ki);
     write_block(a, i, j, Kr, Ki, gi.t1, gi.t2, gj.t1, gj.t2);
+}
+
+// Error sample of a mixed assembly: rows of the cells i_r = r N / R
+// (r < R), every column, recomputed in FP64 with the per-pair operators
+// (K_RotRot_HS_Colloc near, K_RotRot_Far far, electrodynamics/K.h) and
+// projected as the stored entries are; each block sums |stored - FP64|^2
+// and |FP64|^2 of its (row, column) pairs into part[block] (fixed order).
+__global__ void asm_error_sample_kernel(AsmArgs a, const double* __restrict__ verts, int nv, int R, DNP np,
+                                        double2* __restrict__ part) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int N = a.n_cells, M = a.m;
+    double num = 0., den = 0.;
+    if (q < (long long)R * N) {
+        const int r = (int)(q / N), j = (int)(q - (long long)r * N);
+        const int i = (int)((long long)r * N / R);
+        const CellGeo gi = a.geo[i], gj = a.geo[j];
+        DCell cl;
+        cl.nv = nv;
+        for (int v = 0; v < nv; v++)
+            for (int g = 0; g < 3; g++) cl.v[v][g] = verts[((size_t)j * nv + v) * 3 + g];
+        const double* x = gi.c;
+        double d;
+        double Kr[3][3], Ki[3][3];
+        if (asm_is_near(x, gj, a.analytic_calc, &d)) {
+            near_operator(cl, x, a.k, np, Kr, Ki);
+        } else {
+            for (int b = 0; b < 3; b++) {  // K_RotRot_Far is linear in the current: one column per basis vector
+                cplx e[3] = {mk(b == 0, 0.), mk(b == 1, 0.), mk(b == 2, 0.)}, col[3];
+                K_far_dev(e, x, cl, np, a.k, col);
+                for (int p = 0; p < 3; p++) {
+                    Kr[p][b] = col[p].re;
+                    Ki[p][b] = col[p].im;
+                }
+            }
+        }
+        const size_t dim = (size_t)M * N;
+        for (int aa = 0; aa < M; aa++)
+            for (int b = 0; b < M; b++) {
+                double vr = 0., vi = 0.;
+                if (M == 3) {
+                    vr = Kr[aa][b];
+                    vi = Ki[aa][b];
+                } else {
+                    const double* ta = aa == 0 ? gi.t1 : gi.t2;
+                    const double* tb = b == 0 ? gj.t1 : gj.t2;
+                    for (int p = 0; p < 3; p++) {
+                        vr += ta[p] * (Kr[p][0] * tb[0] + Kr[p][1] * tb[1] + Kr[p][2] * tb[2]);
+                        vi += ta[p] * (Ki[p][0] * tb[0] + Ki[p][1] * tb[1] + Ki[p][2] * tb[2]);
+                    }
+                }
+                const size_t off = ((size_t)i * M + aa) * dim + (size_t)j * M + b;
+                double sr, si;
+                if (a.c64) {
+                    const float2 v = reinterpret_cast<const float2*>(a.A)[off];
+                    sr = v.x;
+                    si = v.y;
+                } else {
+                    const double2 v = reinterpret_cast<const double2*>(a.A)[off];
+                    sr = v.x;
+                    si = v.y;
+                }
+                num += (sr - vr) * (sr - vr) + (si - vi) * (si - vi);
+                den += vr * vr + vi * vi;
+            }
+    }
+    __shared__ double sn[128], sd[128];
+    sn[threadIdx.x] = num;
+    sd[threadIdx.x] = den;
+    __syncthreads();
+    for (int w = 64; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            sn[threadIdx.x] += sn[threadIdx.x + w];
+            sd[threadIdx.x] += sd[threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = make_double2(sn[0], sd[0]);
+}
+
+__global__ void asm_error_sum_kernel(const double2* __restrict__ part, int n, double* __restrict__ sums) {
+    double a = 0., b = 0.;
+    for (int i = 0; i < n; i++) {
+        a += part[i].x;
+        b += part[i].y;
+    }
+    sums[0] = a;
+    sums[1] = b;
 }
 
 static size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
@@ -572,6 +665,23 @@ cudaError_t assemble_stage2(const AssembleLaunch& a, void* ws, long long n_near,
     DNP np{a.np.eps, a.np.rs, a.np.rs_seg, a.np.analytic_calc, a.np.n_start, a.np.n_start_seg, a.np.p_max,
            a.np.p_max_seg};
     asm_near_kernel<<<(int)((n_near + 127) / 128), 128, 0, s>>>(g, m.verts, m.nv, pr, pc, n_near, np);
+    return cudaGetLastError();
+}
+
+size_t assemble_error_ws_bytes(const AssembleLaunch& a, int R) {
+    return al256((size_t)(((long long)R * a.mesh->n_cells + 127) / 128) * sizeof(double2)) + 256;
+}
+
+cudaError_t assemble_error_sample(const AssembleLaunch& a, int R, void* ws, double* sums, cudaStream_t s) {
+    const MeshDev& m = *a.mesh;
+    const long long tot = (long long)R * m.n_cells;
+    const int blocks = (int)((tot + 127) / 128);
+    AsmArgs g = make_args(a);
+    DNP np{a.np.eps, a.np.rs, a.np.rs_seg, a.np.analytic_calc, a.np.n_start, a.np.n_start_seg, a.np.p_max,
+           a.np.p_max_seg};
+    double2* part = (double2*)ws;
+    asm_error_sample_kernel<<<blocks, 128, 0, s>>>(g, m.verts, m.nv, R, np, part);
+    asm_error_sum_kernel<<<1, 1, 0, s>>>(part, blocks, sums);
     return cudaGetLastError();
 }
 

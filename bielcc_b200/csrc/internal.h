@@ -124,7 +124,30 @@ struct AssembleLaunch {
 size_t assemble_ws_base_bytes(const AssembleLaunch& a);
 cudaError_t assemble_stage1(const AssembleLaunch& a, void* ws, long long* d_total, cudaStream_t s);
 cudaError_t assemble_stage2(const AssembleLaunch& a, void* ws, long long n_near, void* pair_ws, cudaStream_t s);
+// Error sample of a mixed assembly: R rows (cells r N / R) recomputed in FP64
+// and compared with the stored matrix; sums[0] = sum |stored - FP64|^2,
+// sums[1] = sum |FP64|^2 (device), on stream s after the assembly.
+size_t assemble_error_ws_bytes(const AssembleLaunch& a, int R);
+cudaError_t assemble_error_sample(const AssembleLaunch& a, int R, void* ws, double* sums, cudaStream_t s);
 
+
+// ---- estimate.cu: error report of a mixed result against an FP64 sample
+struct ErrJob {
+    const double* pts;  // the job's points (device) [P][3]
+    int P, Q;           // points, sample points (point q * P / Q)
+    int S, Ss;          // right-hand sides of the outputs, sampled right-hand sides (the first Ss)
+    int off;            // first sample point of this job in the gathered array
+    const double* E;    // mixed outputs [S][P][3] complex128 (or E32 / H32 complex64)
+    const double* H;
+    const float* E32;
+    const float* H32;
+    const double* Eq;   // FP64 sample outputs [Ss][Q][3] complex128
+    const double* Hq;   // may be null
+    double* est_dev;    // receives sqrt(num / den) of this job (may be null)
+};
+cudaError_t err_gather(const ErrJob* d_jobs, int n_jobs, double* spts, cudaStream_t s);
+// per-job (num, den) into nd[2 n_jobs], their sums into sums[2]
+cudaError_t err_compare(const ErrJob* d_jobs, int n_jobs, double* nd, double* sums, cudaStream_t s);
 
 // ---- batch.cu: many field jobs in one persistent launch
 struct JobDev {

@@ -187,6 +187,15 @@ struct Slot {
     AssembleLaunch asl{};
     size_t out_base = 0, out_total = 0, nan_off = 0;
     int64_t extra = 0;  // reservation correction once the near count is known
+    // error sample of a mixed field batch (estimate.cu): per request min(P, 32)
+    // points and min(S, 4) right-hand sides in FP64, after the main stage 1
+    bool samp_on = false;
+    size_t est_off = 0, samp_off = 0;  // per-request estimates (copied back), sample scratch (device only)
+    SBuf samp_ws, samp_pair_ws;
+    BatchPlan samp_bp;
+    BatchDevPtrs samp_d{};
+    ErrJob* samp_ej = nullptr;
+    double *samp_nd = nullptr, *samp_sums = nullptr;
 };
 
 }  // namespace
@@ -248,7 +257,11 @@ int64_t field_bytes(const Req& r, int n_start, double item_cost) {
     const int64_t cpr = batch_cells_per_range((int)N, (int)S, n_start, item_cost);
     const int64_t ranges = (N + cpr - 1) / cpr, words = (N + 31) / 32;
     const int64_t ws = al((ranges + 1) * S * 12 * P * 8) + al(words * P * 4) + P * 24 + 4096;
-    return in + out + ws + r.near_est;
+    // the mixed form's error sample: its points, FP64 outputs, partial sums and near mask
+    const int64_t Q = std::min<int64_t>(P, 32), Ss = std::min<int64_t>(S, 4);
+    const int64_t samp = 3 * al(Q * 24 + Ss * Q * 96) + al((ranges + 1) * Ss * 12 * Q * 8) + al(words * Q * 4) +
+                         al(Q * 8 * 216) + 1024;
+    return in + out + ws + samp + r.near_est;
 }
 
 int64_t assemble_bytes(const Req& r) {
@@ -297,7 +310,20 @@ cudaError_t start_field_batch(bielcc_server_s* sv, Slot& sl) {
     }
     sl.nan_off = off;
     off += al(sl.reqs.size() * 8);
+    sl.samp_on = sv->precision == BIELCC_PREC_MIXED;
+    sl.est_off = off;
+    if (sl.samp_on) off += al(sl.reqs.size() * 8);
     sl.out_total = off - sl.out_base;
+    // sample scratch (device only): ErrJob records, per-job sums, points, FP64 outputs
+    sl.samp_off = off;
+    size_t samp_q = 0, samp_o = 0;
+    for (Req* r : sl.reqs) {
+        samp_q += std::min(r->f.n_pts, 32);
+        samp_o += (size_t)std::min(r->f.n_pts, 32) * std::min(r->f.n_rhs, 4);
+    }
+    if (sl.samp_on)
+        off += al(sl.reqs.size() * sizeof(ErrJob)) + al(sl.reqs.size() * 16 + 16) + al(samp_q * 24) +
+               2 * al(samp_o * 48);
     auto t0 = Clock::now();
     cudaError_t e = sl.io.ensure(off, sl.s);
     if (e == cudaSuccess) e = sv->pins.acquire(off, sl.pin);
@@ -362,6 +388,53 @@ cudaError_t start_field_batch(bielcc_server_s* sv, Slot& sl) {
     int launches = 0;
     e = batch_stage1(sl.bp, sl.ws.p, sv->np.analytic_calc, sv->np.n_start, false, sl.s, &sl.d, &launches);
     if (e == cudaSuccess) e = batch_status_to_host(sl.d, sl.h_total, sl.s);
+    if (e == cudaSuccess && sl.samp_on) {  // the error sample: gather, FP64 stage 1 (status in h_total[4], [7])
+        char* sb = dev + sl.samp_off;
+        const size_t n = sl.reqs.size();
+        sl.samp_ej = (ErrJob*)sb;
+        sb += al(n * sizeof(ErrJob));
+        sl.samp_nd = (double*)sb;
+        sl.samp_sums = sl.samp_nd + 2 * n;
+        sb += al(n * 16 + 16);
+        double* spts = (double*)sb;
+        size_t tq = 0, to = 0;
+        for (const JobDev& j : jd) {
+            tq += std::min(j.n_pts, 32);
+            to += (size_t)std::min(j.n_pts, 32) * std::min(j.n_rhs, 4);
+        }
+        sb += al(tq * 24);
+        double* Eq = (double*)sb;
+        double* Hq = (double*)(sb + al(to * 48));
+        std::vector<ErrJob> ej(n);
+        std::vector<JobDev> js(jd);
+        size_t oq = 0, oo = 0;
+        for (size_t i = 0; i < n; i++) {
+            const JobDev& j = jd[i];
+            const int Q = std::min(j.n_pts, 32), Ss = std::min(j.n_rhs, 4);
+            ej[i] = ErrJob{j.pts, j.n_pts, Q, j.n_rhs, Ss, (int)oq, j.E, j.H, j.E32, j.H32, Eq + 6 * oo,
+                           (j.H || j.H32) ? Hq + 6 * oo : nullptr, (double*)(dev + sl.est_off) + i};
+            js[i].pts = spts + 3 * oq;
+            js[i].n_pts = Q;
+            js[i].n_rhs = Ss;
+            js[i].E = Eq + 6 * oo;
+            js[i].H = (j.H || j.H32) ? Hq + 6 * oo : nullptr;
+            js[i].E32 = js[i].H32 = nullptr;
+            js[i].nonfinite = nullptr;
+            oq += Q;
+            oo += (size_t)Ss * Q;
+        }
+        e = cudaMemcpyAsync(sl.samp_ej, ej.data(), n * sizeof(ErrJob), cudaMemcpyHostToDevice, sl.s);
+        if (e == cudaSuccess) e = err_gather(sl.samp_ej, (int)n, spts, sl.s);
+        if (e == cudaSuccess) {
+            plan_batch(sl.samp_bp, js, sv->np.n_start, false, sv->item_cost, false);
+            e = sl.samp_ws.ensure(sl.samp_bp.ws_bytes, sl.s);
+        }
+        int l = 0;
+        if (e == cudaSuccess)
+            e = batch_stage1(sl.samp_bp, sl.samp_ws.p, sv->np.analytic_calc, sv->np.n_start, false, sl.s, &sl.samp_d,
+                             &l);
+        if (e == cudaSuccess) e = batch_status_to_host(sl.samp_d, sl.h_total + 4, sl.s);
+    }
     auto t6 = Clock::now();
     auto sec = [](Clock::time_point a, Clock::time_point b) { return std::chrono::duration<double>(b - a).count(); };
     std::lock_guard<std::mutex> g(sv->mu);
@@ -374,6 +447,7 @@ cudaError_t start_field_batch(bielcc_server_s* sv, Slot& sl) {
 
 cudaError_t start_assemble(bielcc_server_s* sv, Slot& sl) {
     Req* r = sl.reqs[0];
+    sl.samp_on = false;
     const size_t N = r->mesh->n_cells, m = r->a.layout == BIELCC_LAYOUT_FULL3 ? 3 : 2;
     r->out_bytes = m * N * m * N * (r->a.out_c64 ? 8 : 16);
     r->out_off = 0;
@@ -428,6 +502,13 @@ cudaError_t finish_batch(bielcc_server_s* sv, Slot& sl, long long n_near, size_t
                sv->np.p_max, sv->np.p_max_seg};
         int launches = 0;
         if (e == cudaSuccess) e = batch_stage2(sl.bp, sl.d, n_near, sl.pair_ws.p, dn, nullptr, sl.s, &launches);
+        if (e == cudaSuccess && sl.samp_on) {  // the error sample's stage 2, then the comparison
+            const long long sn = sl.h_total[4];
+            if (sn > 0) e = sl.samp_pair_ws.ensure(batch_pair_ws_bytes(sn), sl.s);
+            if (e == cudaSuccess)
+                e = batch_stage2(sl.samp_bp, sl.samp_d, sn, sl.samp_pair_ws.p, dn, nullptr, sl.s, &launches);
+            if (e == cudaSuccess) e = err_compare(sl.samp_ej, (int)sl.reqs.size(), sl.samp_nd, sl.samp_sums, sl.s);
+        }
     } else {
         if (pair_bytes) e = sl.pair_ws.ensure(pair_bytes, sl.s);
         if (e == cudaSuccess) e = assemble_stage2(sl.asl, sl.ws.p, n_near, sl.pair_ws.p, sl.s);
@@ -439,6 +520,8 @@ cudaError_t finish_batch(bielcc_server_s* sv, Slot& sl, long long n_near, size_t
     sl.ws.release(sl.s);
     sl.pair_ws.release(sl.s);
     sl.io.release(sl.s);
+    sl.samp_ws.release(sl.s);
+    sl.samp_pair_ws.release(sl.s);
     if (e == cudaSuccess) e = cudaEventRecord(sl.ev_end, sl.s);
     if (e == cudaSuccess) e = cudaEventRecord(sl.ev_done, sl.s);
     return e;
@@ -456,6 +539,7 @@ void complete_slot(bielcc_server_s* sv, Slot& sl) {
             if (r->f.H) memcpy(r->f.H, pin + r->out_off + r->e_bytes, r->e_bytes);
             const unsigned long long bad = ((const unsigned long long*)(pin + sl.nan_off))[i];
             if (bad) status[i] = BIELCC_ERR_NAN;
+            if (r->f.est) *r->f.est = sl.samp_on ? ((const double*)(pin + sl.est_off))[i] : 0.;
         } else if (!r->a.A_dev) {
             memcpy(r->a.A, pin, r->out_bytes);
         }
@@ -550,7 +634,8 @@ void slot_loop(bielcc_server_s* sv, Slot* slp) {
             sv->stage_in_s += in_s;
         }
         if (e == cudaSuccess) e = cudaEventSynchronize(sl.ev_stage1);
-        if (e == cudaSuccess && take[0]->type == kField && batch_timed_out(sl.h_total))
+        if (e == cudaSuccess && take[0]->type == kField &&
+            (batch_timed_out(sl.h_total) || (sl.samp_on && batch_timed_out(sl.h_total + 4))))
             e = cudaErrorTimeout;  // a bounded wait in the far kernel ran out: the batch fails
         if (e == cudaSuccess) {
             const long long n_near = *sl.h_total;

@@ -377,7 +377,8 @@ class Context:
     @staticmethod
     def make_jobs(specs):
         """specs: dicts with mesh, n_rhs, n_pts, J, pts, E, H (device pointers as ints),
-        k, mult (optional), inc (optional PlaneWave)."""
+        k, mult (optional), inc (optional PlaneWave), est (optional device address of
+        one double that receives the job's estimated mixed-precision error)."""
         arr = (abi.FieldJob * len(specs))()
         for i, sp in enumerate(specs):
             k = complex(sp["k"])
@@ -394,6 +395,7 @@ class Context:
             j.mult_re, j.mult_im = mult.real, mult.imag
             if sp.get("inc") is not None:
                 j.inc = sp["inc"]
+            j.est_dev = sp.get("est") or None
         return arr
 
     def field_EH_batch(self, jobs, numparam=None, precision="mixed", stream=None):
@@ -606,9 +608,11 @@ class Server:
         r.k_re, r.k_im, r.mult_re, r.mult_im = k.real, k.imag, mult.real, mult.imag
         if inc is not None:
             r.inc = inc
+        est = C.c_double(0.0)  # the mixed form's estimated error, written on completion
+        r.est = C.addressof(est)
         t = C.c_int64(0)
         _check(_lib.bielcc_server_submit_field(self.h, C.byref(r), C.byref(t)))
-        self._live[t.value] = (r, J, pts, {"E": E, "H": H})
+        self._live[t.value] = (r, J, pts, {"E": E, "H": H}, est)
         return t.value
 
     def submit_assemble(self, mesh, k, layout="tau2", out_c64=True, out=None):
@@ -643,7 +647,11 @@ class Server:
     def wait(self, ticket, timeout=120.0):
         st, lat = C.c_int(0), C.c_double(0)
         _check(_lib.bielcc_server_wait(self.h, ticket, float(timeout), C.byref(st), C.byref(lat)))
-        return st.value, lat.value, self._live.pop(ticket)[3]
+        live = self._live.pop(ticket)
+        out = live[3]
+        if len(live) > 4:
+            out["est"] = live[4].value
+        return st.value, lat.value, out
 
     def pause(self, paused=True):
         _check(_lib.bielcc_server_pause(self.h, int(bool(paused))))

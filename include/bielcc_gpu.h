@@ -97,13 +97,19 @@ typedef struct bielcc_kernelparam {
 #define BIELCC_PREC_FP64   0  /* complex FP64 everywhere (parity form) */
 #define BIELCC_PREC_MIXED  1  /* complex FP32 far cells, FP64 near / singular cells */
 
-/* Result report of a field / assembly call. */
+/* Result report of a field / assembly call. Every mixed-precision call given
+ * a report estimates its error against the FP64 form on a sample evaluated in
+ * FP64 beside it (and then waits for its stream to fill the estimate):
+ * single-job calls min(n_pts, 256) points spread over the set and all RHS;
+ * batches min(n_pts, 32) points and the first min(n_rhs, 4) RHS of every job
+ * (each job's own estimate also goes to its est_dev); assembly min(N, 16)
+ * rows spread over the matrix. FP64 calls report 0. */
 typedef struct bielcc_report {
     int64_t n_pairs;        /* point x cell pairs evaluated (per RHS) */
     int64_t n_near_pairs;   /* pairs that took the FP64 near path */
     int64_t n_nonfinite;    /* non-finite output components */
-    double  est_rel_l2;     /* mixed, host-buffer call: rel-L2 vs FP64 on a point sample; otherwise 0 */
-    int32_t est_sample;     /* points in that sample: min(n_pts, 256), spread evenly over the set */
+    double  est_rel_l2;     /* mixed: relative L2 difference from FP64 over the sample; FP64: 0 */
+    int32_t est_sample;     /* points (rows for assembly) in that sample */
     int32_t status;         /* same as the return value */
 } bielcc_report;
 
@@ -300,6 +306,8 @@ typedef struct bielcc_field_job {
     double* H_dev;          /* may be NULL */
     double k_re, k_im, mult_re, mult_im;
     bielcc_planewave inc;   /* add_E = add_H = 0 for no incident field */
+    double* est_dev;        /* mixed precision: device address that receives this job's estimated
+                               relative L2 error against FP64 (may be NULL) */
 } bielcc_field_job;
 
 /* Many field evaluations (meshes of uneven sizes, their own k, 1..n RHS) in
@@ -525,6 +533,8 @@ typedef struct bielcc_field_request {
     void* H;                /* host, may be NULL */
     double k_re, k_im, mult_re, mult_im;
     bielcc_planewave inc;   /* add_E = add_H = 0 for no incident field */
+    double* est;            /* mixed server: host address that receives the request's estimated
+                               relative L2 error against FP64 on completion (may be NULL) */
 } bielcc_field_request;
 
 typedef struct bielcc_assemble_request {
