@@ -65,6 +65,14 @@ def parse():
     ap.add_argument("--serve-max-batch", type=int, default=64)
     ap.add_argument("--serve-reserve-gb", type=int, default=32, help="device memory the server maps up front")
     ap.add_argument("--serve-persistent", action="store_true", help="persistent far-kernel CTAs in served batches")
+    ap.add_argument("--serve-max-batch-pairs", type=float, default=0.0,
+                    help="cap on a served batch's (point, cell, RHS) pairs (0: none)")
+    ap.add_argument("--serve-asm-max-cells", type=int, default=20000,
+                    help="largest mesh an assembly request draws (the config-5 mesh range)")
+    ap.add_argument("--serve-asm-host-cells", type=int, default=2000,
+                    help="assemblies of larger meshes write a caller-owned device matrix instead of host memory")
+    ap.add_argument("--serve-p99-target-ms", type=float, default=1000.0,
+                    help="stated p99 latency objective of the serving stream")
     return ap.parse_args()
 
 
@@ -380,24 +388,34 @@ def run_serving(args, ctx, torch, dev, stream, item_cost):
     resident meshes drawn like the batched workload (seed 4); field requests
     carry 100-50,000 points (log-uniform, 10% near-field) and 1-16 PO current
     sets, complex64 E and H with FP64 near pairs; assembly requests build the
-    TAU2 complex64 matrix of a mesh of at most 2000 cells. The same requests
+    TAU2 complex64 matrix of a mesh of the same distribution (matrices of
+    meshes above --serve-asm-host-cells cells go to caller-owned device
+    memory, as a solver on the GPU would take them). The same requests
     first run offline (device-resident inputs, field requests in batches of
     64 through bielcc_field_EH_batch, assembly through
     bielcc_assemble_K_device) to give the offline throughput; the stream then
     arrives at --serve-load x that rate through bielcc_server_* with host
-    buffers, and its throughput, p50/p99 latency and agreement with the offline
-    results are reported."""
+    buffers, and its throughput, p50/p99 latency, agreement with the offline
+    results and the stated objective (p99 <= --serve-p99-target-ms while
+    serving >= 0.8 x the offline throughput) are reported."""
     import threading
 
     from bielcc_b200 import abi, gpu
     from bielcc_b200 import workloads as W
 
-    meshes, reqs = W.serving_stream(n_requests=args.serve_requests, seed=4)
+    meshes, reqs = W.serving_stream(n_requests=args.serve_requests, seed=4,
+                                    max_assembly_cells=args.serve_asm_max_cells)
     mh = [ctx.mesh(m["cells"]) for m in meshes]
     Jd = [torch.from_numpy(m["J"]).to(dev) for m in meshes]
     Pd = [torch.from_numpy(m["pts"]).to(dev) for m in meshes]
     field = [r for r in reqs if r["type"] == "field"]
     asm = [r for r in reqs if r["type"] == "assemble"]
+    # assemblies of large meshes write a caller-owned device matrix (one per mesh,
+    # shared by its requests: they write the same values), small ones host memory
+    big_asm = {r["mesh"] for r in asm if mh[r["mesh"]].n_cells > args.serve_asm_host_cells}
+    asm_dev = {i: torch.empty((2 * mh[i].n_cells, 2 * mh[i].n_cells), dtype=torch.complex64, device=dev)
+               for i in sorted(big_asm)}
+    ROWS = 128  # rows of a device-held matrix compared with the offline run
     pairs = sum(r["P"] * len(meshes[r["mesh"]]["cells"]) * r["S"] for r in field)
     sc = stream.cuda_stream
     # ---- offline
@@ -426,11 +444,13 @@ def run_serving(args, ctx, torch, dev, stream, item_cost):
             for i, r in chunk:
                 if r["type"] == "assemble":
                     n = 2 * mh[r["mesh"]].n_cells
-                    A = torch.empty((n, n), dtype=torch.complex64, device=dev)
+                    A = asm_dev.get(r["mesh"])
+                    if A is None:
+                        A = torch.empty((n, n), dtype=torch.complex64, device=dev)
                     ctx.assemble_K_device(mh[r["mesh"]], meshes[r["mesh"]]["k"], A.data_ptr(), c64=True,
                                           precision="mixed", stream=sc)
                     if keep_ref and i in sample:
-                        outs.append((i, A, None))
+                        outs.append((i, A[:ROWS] if r["mesh"] in asm_dev else A, None))
             b.record(stream)
             b.synchronize()
             t += a.elapsed_time(b) * 1e-3
@@ -453,12 +473,21 @@ def run_serving(args, ctx, torch, dev, stream, item_cost):
         if r["type"] == "field":
             E = np.ones((r["S"], r["P"], 3), np.complex64)
             outs.append((E, np.ones_like(E)))
+        elif r["mesh"] in asm_dev:
+            outs.append(None)
         else:
             n = 2 * mh[r["mesh"]].n_cells
             outs.append(np.ones((n, n), np.complex64))
     sv = gpu.Server(ctx, n_slots=args.serve_slots, precision="mixed", item_cost=item_cost,
                     preemptible=not args.serve_persistent, max_batch=args.serve_max_batch,
-                    reserve=(args.serve_reserve_gb << 30, 4 << 30))
+                    reserve=(args.serve_reserve_gb << 30, 4 << 30),
+                    max_batch_pairs=int(args.serve_max_batch_pairs) or None)
+
+    def submit_asm(i, r):
+        if r["mesh"] in asm_dev:
+            return sv.submit_assemble(mh[r["mesh"]], meshes[r["mesh"]]["k"], layout="tau2", out_c64=True,
+                                      A_dev=asm_dev[r["mesh"]].data_ptr())
+        return sv.submit_assemble(mh[r["mesh"]], meshes[r["mesh"]]["k"], layout="tau2", out_c64=True, out=outs[i])
     # a long-running server is warm: one pass over every 8th request before the timed stream
     warm = [i for i in range(0, len(reqs), 8)]
     for i in warm:
@@ -467,7 +496,7 @@ def run_serving(args, ctx, torch, dev, stream, item_cost):
             sv.wait(sv.submit_field(mh[r["mesh"]], m["J"][:r["S"]], m["pts"][:r["P"]], m["k"], out_c64=True,
                                     out=outs[i]))
         else:
-            sv.wait(sv.submit_assemble(mh[r["mesh"]], m["k"], layout="tau2", out_c64=True, out=outs[i]))
+            sv.wait(submit_asm(i, r))
     sv.stats(reset=True)
     res = [None] * len(reqs)
     tickets = [None] * len(reqs)
@@ -493,7 +522,7 @@ def run_serving(args, ctx, torch, dev, stream, item_cost):
                 tickets[i] = sv.submit_field(mh[r["mesh"]], m["J"][:r["S"]], m["pts"][:r["P"]], m["k"],
                                              out_c64=True, out=outs[i])
             else:
-                tickets[i] = sv.submit_assemble(mh[r["mesh"]], m["k"], layout="tau2", out_c64=True, out=outs[i])
+                tickets[i] = submit_asm(i, r)
             ready.release()
         th.join()
     st = sv.stats()
@@ -507,6 +536,8 @@ def run_serving(args, ctx, torch, dev, stream, item_cost):
         o = res[i][2]
         if reqs[i]["type"] == "field":
             pairs_cmp = [(o["E"], ref[i][0].astype(np.complex64)), (o["H"], ref[i][1].astype(np.complex64))]
+        elif reqs[i]["mesh"] in asm_dev:
+            pairs_cmp = [(asm_dev[reqs[i]["mesh"]][:ROWS].cpu().numpy(), ref[i][0])]
         else:
             pairs_cmp = [(o["A"], ref[i][0])]
         ok = all(np.array_equal(a, b) for a, b in pairs_cmp)
@@ -518,11 +549,22 @@ def run_serving(args, ctx, torch, dev, stream, item_cost):
     served = pairs / st["wall_s"]
     for m in mh:
         m.close()
+    asm_dev.clear()
+    est = [res[i][2].get("est") for i in sorted(ref) if reqs[i]["type"] == "field" and res[i][2] is not None]
+    p99 = _pct(lat_f + lat_a, 0.99)
+    slo = {"p99_target_ms": args.serve_p99_target_ms, "p99_ms": p99, "p99_met": p99 <= args.serve_p99_target_ms,
+           "throughput_target": 0.8, "served_over_offline": served / off_pairs_per_s,
+           "throughput_met": served / off_pairs_per_s >= 0.8,
+           "met": p99 <= args.serve_p99_target_ms and served / off_pairs_per_s >= 0.8,
+           "statement": f"p99 latency <= {args.serve_p99_target_ms:.0f} ms (submission to result in the caller's "
+                        f"buffer) over all requests while serving >= 0.8 x the offline batched throughput at "
+                        f"{args.serve_load} x the offline rate"}
     return {
         "workload": f"{len(reqs)} requests ({len(field)} field, {len(asm)} assembly) over 24 resident meshes "
-                    f"(spheroids, rounded cubes, tori; 200-20000 cells; k 0.5-20; seed 4); field: 100-50000 "
-                    f"points log-uniform, 1-16 PO current sets, complex64 E+H, FP64 near pairs; assembly: TAU2 "
-                    f"complex64 on meshes <= 2000 cells; Poisson arrivals",
+                    f"(spheroids, rounded cubes, tori, quads or triangles; 200-20000 cells; k 0.5-20; seed 4); "
+                    f"field: 100-50000 points log-uniform, 1-16 PO current sets, complex64 E+H, FP64 near pairs; "
+                    f"assembly: TAU2 complex64 on meshes <= {args.serve_asm_max_cells} cells (device matrices "
+                    f"above {args.serve_asm_host_cells}); Poisson arrivals",
         "arrival_rate_per_s": rate, "load": args.serve_load, "slots": args.serve_slots,
         "hbm_budget_gb": st["budget"] / 2**30,
         "offline_pairs_per_s": off_pairs_per_s, "offline_s": t_off,
@@ -539,7 +581,12 @@ def run_serving(args, ctx, torch, dev, stream, item_cost):
         "arrival_window_s": reqs[-1]["t"] / rate, "offered_pairs_per_s": pairs / (reqs[-1]["t"] / rate),
         "failed": bad, "sampled_identical_to_offline": f"{same}/{len(ref)}",
         "sampled_mismatch": {"requests": bad_idx, "max_diff_over_max": worst},
-        "unit": "(point, cell, RHS) pairs/s", "clocks": clk.summary(),
+        "unit": "(point, cell, RHS) pairs/s", "clocks": clk.summary(), "slo": slo,
+        "max_batch_pairs": args.serve_max_batch_pairs,
+        "assembly_meshes": {"max_cells": args.serve_asm_max_cells, "device_output_above_cells":
+                            args.serve_asm_host_cells, "largest_assembled": max([mh_n for mh_n in
+                            [len(meshes[r["mesh"]]["cells"]) for r in asm]] or [0])},
+        "served_est_rel_l2_max": max(est) if est else None,
     }
 
 

@@ -555,9 +555,9 @@ constexpr size_t kOffYY = kOffNodes + 16 * (size_t)kNodes, kOffCell = kOffYY + 4
 constexpr size_t kOffRho = kOffCell + 32 * kRound, kOffNear = kOffRho + 8 * kRound;
 constexpr size_t kSmem = kOffNear + kRound * 32;
 static_assert(64 * kK * 4 <= 4 * kBbytes, "the unused rows of the second M block must stay inside shared memory");
-// polls of one mbarrier wait before the kernel gives up (each poll blocks
-// for a bounded time; this is seconds, against microseconds of MMA work)
-constexpr long long kWaitPolls = 1ll << 22;
+// longest wait for one group of MMAs before the kernel gives up: 2 s of the
+// global timer, against microseconds of MMA work
+constexpr uint64_t kWaitNs = 2000000000ull;
 }  // namespace tcb
 
 BIELCC_D void tc_put2(unsigned char* base, int row, int k, float v0, float v1) {
@@ -690,7 +690,7 @@ __global__ void __launch_bounds__(tcb::kThreads, 2)
     // (a timed-out commit stays recorded as in flight for the final wait)
     auto wait_one_local = [&](int q) -> bool {
         if (!inflight[q]) return true;
-        if (!umma::mbar_wait(&bar[q], parity[q], tcb::kWaitPolls)) return false;
+        if (!umma::mbar_wait(&bar[q], parity[q], tcb::kWaitNs)) return false;
         parity[q] ^= 1u;
         inflight[q] = 0;
         return true;
@@ -862,7 +862,7 @@ __global__ void __launch_bounds__(tcb::kThreads, 2)
         if (threadIdx.x == 0) atomicExch(reinterpret_cast<unsigned long long*>(err), 1ull);
         // MMAs still in flight: wait for them (bounded) before the tensor memory is released
         for (int q = 0; q < 2; q++)
-            if (inflight[q]) umma::mbar_wait(&bar[q], parity[q], tcb::kWaitPolls);
+            if (inflight[q]) umma::mbar_wait(&bar[q], parity[q], tcb::kWaitNs);
     }
     umma::fence_before_sync();
     __syncthreads();

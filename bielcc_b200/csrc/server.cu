@@ -218,6 +218,7 @@ struct bielcc_server_s {
     std::atomic<bool> stop{false};
     int64_t next_ticket = 1;
     int max_batch = 64;
+    int64_t max_batch_pairs = 0;  // 0: no cap on a batch's (point, cell, RHS) pairs
     bool paused = false;
     bool preemptible = true;
     cudaEvent_t ev_ref = nullptr;              // time origin of the batch spans
@@ -572,14 +573,19 @@ void complete_slot(bielcc_server_s* sv, Slot& sl) {
 // field requests in arrival order, or one assembly request, within budget.
 std::vector<Req*> admit_locked(bielcc_server_s* sv) {
     std::vector<Req*> take;
+    int64_t work = 0;
     while (!sv->paused && !sv->queue.empty()) {
         Req* r = sv->queue.front();
         if (r->type == kAssemble && !take.empty()) break;
+        // a batch's length bounds the latency of every request in it: past the
+        // cap, the rest waits for the next idle slot (an empty batch takes any one)
+        if (sv->max_batch_pairs > 0 && !take.empty() && work + r->pairs > sv->max_batch_pairs) break;
         const bool fits = sv->reserved + r->bytes <= sv->budget;
         if (!fits && !(sv->reserved == 0 && take.empty())) break;  // head of line waits for memory
         sv->queue.pop_front();
         sv->reserved += r->bytes;
         r->state = kRunning;
+        work += r->pairs;
         take.push_back(r);
         if (r->type == kAssemble || (int)take.size() >= sv->max_batch) break;
     }
@@ -829,6 +835,13 @@ int bielcc_server_set_max_batch(bielcc_server sv, int max_batch) {
     if (!sv || max_batch < 1) return set_api_error(BIELCC_ERR_ARG, "bad argument");
     std::lock_guard<std::mutex> g(sv->mu);
     sv->max_batch = max_batch;
+    return BIELCC_OK;
+}
+
+int bielcc_server_set_max_batch_pairs(bielcc_server sv, int64_t pairs) {
+    if (!sv || pairs < 0) return set_api_error(BIELCC_ERR_ARG, "bad argument");
+    std::lock_guard<std::mutex> g(sv->mu);
+    sv->max_batch_pairs = pairs;
     return BIELCC_OK;
 }
 

@@ -107,13 +107,21 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// Waits for the phase with the given parity to complete, at most `limit`
-// polls (each try_wait itself blocks for a bounded, implementation-defined
-// time). Returns false when the limit ran out.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long limit) {
-    for (long long i = 0; i < limit; i++)
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Waits for the phase with the given parity to complete, for at most
+// `limit_ns` nanoseconds of the global timer (each try_wait itself suspends
+// for a bounded, implementation-defined time). Returns false when the limit
+// ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
+    const uint64_t t0 = global_ns();
+    for (;;) {
         if (mbar_try_wait(bar, parity)) return true;
-    return false;
+        if (global_ns() - t0 > limit_ns) return false;
+    }
 }
 
 // ---- accumulator read-back: 32 consecutive 32-bit columns of this thread's

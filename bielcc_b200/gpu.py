@@ -98,6 +98,7 @@ def load(path=LIB_PATH):
     d("bielcc_server_cancel", [vp, C.c_int64])
     d("bielcc_server_pause", [vp, C.c_int])
     d("bielcc_server_drain", [vp, C.c_double])
+    d("bielcc_server_set_max_batch_pairs", [vp, C.c_int64])
     d("bielcc_server_get_stats", [vp, C.POINTER(abi.ServerStats), C.c_int])
     abi.declare_common(L, "bielcc_")
     if L.bielcc_abi_version() != abi.ABI_VERSION:
@@ -561,7 +562,7 @@ class Server:
     (status, latency_ms, outputs) once the request finished."""
 
     def __init__(self, ctx, hbm_budget=0, n_slots=2, numparam=None, precision="mixed", max_batch=None,
-                 item_cost=None, preemptible=True, reserve=None):
+                 item_cost=None, preemptible=True, reserve=None, max_batch_pairs=None):
         self.ctx = ctx
         np_ = numparam if numparam is not None else abi.NumParam.default()
         h = C.c_void_p()
@@ -571,6 +572,8 @@ class Server:
         self._live = {}
         if max_batch is not None:
             _check(_lib.bielcc_server_set_max_batch(self.h, int(max_batch)))
+        if max_batch_pairs is not None:
+            _check(_lib.bielcc_server_set_max_batch_pairs(self.h, int(max_batch_pairs)))
         if item_cost is not None:
             _check(_lib.bielcc_server_set_item_cost(self.h, float(item_cost)))
         _check(_lib.bielcc_server_set_preemptible(self.h, int(bool(preemptible))))
@@ -615,21 +618,26 @@ class Server:
         self._live[t.value] = (r, J, pts, {"E": E, "H": H}, est)
         return t.value
 
-    def submit_assemble(self, mesh, k, layout="tau2", out_c64=True, out=None):
+    def submit_assemble(self, mesh, k, layout="tau2", out_c64=True, out=None, A_dev=None):
+        """out: optional caller-owned host matrix; A_dev: a caller-owned device
+        matrix (device pointer) written instead of a host one."""
         m = 2 if layout == "tau2" else 3
         dt = np.complex64 if out_c64 else np.complex128
         shape = (m * mesh.n_cells, m * mesh.n_cells)
-        if out is not None:
-            if out.dtype != dt or out.shape != shape or not out.flags.c_contiguous:
-                raise ValueError("out must be a C-contiguous matrix of the output dtype")
-            A = out
-        else:
-            A = np.zeros(shape, dt)
+        A = None
+        if A_dev is None:
+            if out is not None:
+                if out.dtype != dt or out.shape != shape or not out.flags.c_contiguous:
+                    raise ValueError("out must be a C-contiguous matrix of the output dtype")
+                A = out
+            else:
+                A = np.zeros(shape, dt)
         r = abi.AssembleRequest()
         r.mesh = mesh.id
         r.layout = abi.LAYOUT_TAU2 if layout == "tau2" else abi.LAYOUT_FULL3
         r.out_c64 = int(bool(out_c64))
-        r.A = A.ctypes.data
+        r.A = A.ctypes.data if A is not None else None
+        r.A_dev = int(A_dev) if A_dev is not None else None
         k = complex(k)
         r.k_re, r.k_im = k.real, k.imag
         t = C.c_int64(0)

@@ -587,6 +587,11 @@ int bielcc_server_reserve(bielcc_server sv, int64_t device_bytes, int64_t pinned
 int bielcc_server_set_preemptible(bielcc_server sv, int on);
 /* Most requests one batch admits (default 64). */
 int bielcc_server_set_max_batch(bielcc_server sv, int max_batch);
+/* Most (point, cell, RHS) pairs one batch admits (0 = no cap, the default):
+ * a batch's length bounds the latency of every request in it, so a cap keeps
+ * large requests from lengthening the batches of small ones; a request larger
+ * than the cap runs in a batch of its own. */
+int bielcc_server_set_max_batch_pairs(bielcc_server sv, int64_t pairs);
 /* paused = 1: queue requests without admitting any (running batches finish);
  * 0: resume. Lets a caller release a burst of requests as one batch. */
 int bielcc_server_pause(bielcc_server sv, int paused);

@@ -88,7 +88,10 @@ def test_server_small_requests_overtake_a_large_batch(gctx):
     sv = gpu.Server(gctx, n_slots=2, precision="mixed")
     try:
         tb = _submit(sv, big)
-        time.sleep(0.005)  # the large request is admitted and on the GPU
+        t0 = time.monotonic()
+        while sv.stats()["running"] < 1:  # the server has admitted the large request into a slot
+            assert time.monotonic() - t0 < 60.0
+            time.sleep(0.0002)
         ts = [_submit(sv, small) for _ in range(4)]
         lat_small = [sv.wait(t)[1] for t in ts]
         st, lat_big, _ = sv.wait(tb)
