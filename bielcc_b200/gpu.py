@@ -305,9 +305,11 @@ class Context:
         return E, H, rep
 
     def field_EH_device(self, mesh, J_dev, k, pts_dev, E_dev, H_dev, n_rhs, n_pts, numparam=None, mult=1.0,
-                        inc=None, precision="fp64", stream=None):
-        """Device-buffer form: pointers are ints (e.g. torch tensor data_ptr())."""
-        rep = abi.Report()
+                        inc=None, precision="fp64", stream=None, report=True):
+        """Device-buffer form: pointers are ints (e.g. torch tensor data_ptr()).
+        report=False passes no report: no error sample, and the call returns
+        once enqueued (None is returned)."""
+        rep = abi.Report() if report else None
         np_ = numparam if numparam is not None else abi.NumParam.default()
         k = complex(k)
         mult = complex(mult)
@@ -315,7 +317,7 @@ class Context:
                                            mult.imag, C.byref(inc) if inc is not None else None, C.byref(np_),
                                            n_pts, C.c_void_p(pts_dev), C.c_void_p(E_dev),
                                            C.c_void_p(H_dev) if H_dev else None, PREC[precision],
-                                           _stream_arg(stream), C.byref(rep)))
+                                           _stream_arg(stream), C.byref(rep) if rep is not None else None))
         return rep
 
     def field_EH_full(self, mesh, J_E, J_M, k, pts, multE=1.0, multH=1.0, inc=None, numparam=None,
@@ -399,12 +401,13 @@ class Context:
             j.est_dev = sp.get("est") or None
         return arr
 
-    def field_EH_batch(self, jobs, numparam=None, precision="mixed", stream=None):
-        """Runs a batch built by make_jobs on device buffers; returns the report."""
+    def field_EH_batch(self, jobs, numparam=None, precision="mixed", stream=None, report=True):
+        """Runs a batch built by make_jobs on device buffers; returns the report
+        (report=False passes none: no error sample, the call returns once enqueued)."""
         rep = abi.Report()
         np_ = numparam if numparam is not None else abi.NumParam.default()
         _check(_lib.bielcc_field_EH_batch(self.h, len(jobs), jobs, C.byref(np_), PREC[precision],
-                                          _stream_arg(stream), C.byref(rep)))
+                                          _stream_arg(stream), C.byref(rep) if report else None))
         return rep
 
     def batch_autotune(self, jobs, numparam=None, precision="mixed", stream=None):
