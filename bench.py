@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--no-assembly", action="store_true", help="skip the 20,480-triangle assembly leg")
     ap.add_argument("--assembly-level", type=int, default=5, help="icosphere level of the assembly leg (5: 20,480)")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream leg")
+    ap.add_argument("--small", action="store_true",
+                    help="reduced case for profiler captures: 2048-cell sphere x 5000 points (not a bench line)")
     ap.add_argument("--serve-requests", type=int, default=600)
     ap.add_argument("--serve-load", type=float, default=0.9, help="arrival rate / offline capacity")
     ap.add_argument("--serve-slots", type=int, default=4)
@@ -76,10 +78,10 @@ def parse():
     return ap.parse_args()
 
 
-def workload():
+def workload(small=False):
     from bielcc_b200 import workloads as W
 
-    return W.config2()
+    return W.config2(4500, 500, 32) if small else W.config2()
 
 
 def dist_init(args):
@@ -623,7 +625,7 @@ def run_ours(args, ws, rank, local):
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    wl = workload()
+    wl = workload(args.small)
     cells, J, k = wl["cells"], wl["J"], wl["k"]
     pts = wl["pts"]
     if ws > 1 and rank > 0:  # each rank: its own far points, same distribution (weak scaling)
@@ -738,7 +740,7 @@ def run_ours(args, ws, rank, local):
         traffic = int(m.group(1)) if m else None
 
     cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline and not args.small:
         import oracle
 
         which = "ref" if oracle.available("ref") else "port"

@@ -241,15 +241,17 @@ def config1():
                 pts=sphere_points(1000, 3.0, 0), inc=planewave(k))
 
 
-def config2(n_far=18000, n_near=2000):
+def config2(n_far=18000, n_near=2000, n_lat=64):
     """8192-quad UV sphere (64 x 128), k = 2 pi, 18000 points on 2-5 m shells +
-    2000 near-field points 0.02-0.1 m along normals of random cells (seed 1)."""
-    cells = uv_sphere(64, 128)
+    2000 near-field points 0.02-0.1 m along normals of random cells (seed 1).
+    n_lat (and the point counts) give the same construction at another size,
+    for reduced profiling runs."""
+    cells = uv_sphere(n_lat, 2 * n_lat)
     k = 2.0 * np.pi
     rng = np.random.default_rng(1)
     pts = np.concatenate([shell_points(n_far, 2.0, 5.0, rng), near_points(cells, n_near, 0.02, 0.1, rng)])
-    return dict(name="sphere8192_k2pi_pts20000", cells=cells, k=k, J=po_currents(cells, k), pts=pts,
-                inc=planewave(k))
+    return dict(name=f"sphere{len(cells)}_k2pi_pts{n_far + n_near}", cells=cells, k=k, J=po_currents(cells, k),
+                pts=pts, inc=planewave(k))
 
 
 def config3(level=5):
