@@ -317,12 +317,38 @@ def run_batched(args, ctx, torch, dev, stream, flush, fp64_single_rhs_value, pea
     for m, _, _ in keep:
         m.close()
     value = rhs_pairs / (ms * 1e-3)
-    # whole batch (far kernel, near pairs, finalize) against the FP32 FMA peak
-    achieved = (geo_pairs * FLOPS_PER_FAR_PAIR + rhs_pairs * FLOPS_PER_RHS_CONTRACTION) / (ms * 1e-3) / 1e12
-    roofline = {"bound": "fp32 CUDA-core pipe", "kernel": "batch_far_kernel<mixed> (whole batch, one launch)",
-                "achieved": achieved, "peak": peak32, "unit": "TFLOP/s", "frac": achieved / peak32,
-                "flops": f"{FLOPS_PER_FAR_PAIR} per (point, cell) quadrature + {FLOPS_PER_RHS_CONTRACTION} per "
-                         f"(point, cell, RHS) contraction", "peak_source": "measured FMA loop (bielcc_measure_fma_peak)"}
+    # The moments (the quadrature) bound the FP32 pipe; the contraction runs on
+    # the tensor cores: per 32-point tile, cell and group of 16 RHS, two M = 128
+    # MMAs of K = 6 and N = 2 min(16, S8 - 16 g) (S8 = S rounded up to 8), three
+    # TF32 products each. Time without the error report (no FP64 sample).
+    tc_flops = 0.0
+    for j in jobs_np:
+        S = j["J"].shape[0]
+        s8 = (S + 7) // 8 * 8
+        n_sum = sum(2 * min(16, s8 - 16 * g) for g in range((S + 15) // 16))
+        tiles = (len(j["pts"]) + 31) // 32
+        tc_flops += tiles * len(j["cells"]) * 2 * 128 * 6 * n_sum * 3 * 2
+    quad = geo_pairs * FLOPS_PER_FAR_PAIR / (ms_no_est * 1e-3) / 1e12
+    peak_tf32 = None
+    try:
+        mp = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        peak_tf32 = mp["bf16_tflops"] / 2.0
+    except Exception:
+        pass
+    tc_achieved = tc_flops / (ms_no_est * 1e-3) / 1e12
+    roofline = {"bound": "fp32 CUDA-core pipe (the moments); the contraction runs on the tensor cores",
+                "kernel": "batch_far_tc_kernel (whole batch, one launch)",
+                "achieved": quad, "peak": peak32, "unit": "TFLOP/s", "frac": quad / peak32,
+                "flops": f"{FLOPS_PER_FAR_PAIR} per (point, cell) quadrature",
+                "peak_source": "measured FMA loop (bielcc_measure_fma_peak)",
+                "tensor": {"achieved": tc_achieved, "unit": "TFLOP/s (TF32, issued)",
+                           "peak": peak_tf32, "frac": tc_achieved / peak_tf32 if peak_tf32 else None,
+                           "peak_source": "half the measured dense bf16 rate (MEASURED_PEAKS.json bf16_tflops)",
+                           "flops": "2 M=128 MMAs x K=6 per (tile, cell) and 16-RHS group, 3 TF32 products"},
+                "cuda_core_form": {"achieved": (geo_pairs * FLOPS_PER_FAR_PAIR + rhs_pairs *
+                                                FLOPS_PER_RHS_CONTRACTION) / (ms_cuda_cores * 1e-3) / 1e12,
+                                   "flops": f"{FLOPS_PER_FAR_PAIR} per (point, cell) + "
+                                            f"{FLOPS_PER_RHS_CONTRACTION} per (point, cell, RHS)"}}
     return {"workload": f"{len(jobs_np)} meshes (spheroids, rounded cubes, tori), 200-20000 cells, k 0.5-20, "
                         f"1-64 PO RHS, 2000 far points each, seed 3",
             "value": value, "unit": "(point, cell, RHS) pairs/s", "geometry_pairs_per_s": geo_pairs / (ms * 1e-3),
