@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--no-assembly", action="store_true", help="skip the 20,480-triangle assembly leg")
     ap.add_argument("--assembly-level", type=int, default=5, help="icosphere level of the assembly leg (5: 20,480)")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream leg")
+    ap.add_argument("--no-tensor-cores", action="store_true",
+                    help="mixed batches contract on the CUDA cores (bielcc_ctx_set_batch_tensor_cores(ctx, 0))")
     ap.add_argument("--small", action="store_true",
                     help="reduced case for profiler captures: 2048-cell sphere x 5000 points (not a bench line)")
     ap.add_argument("--serve-requests", type=int, default=600)
@@ -266,7 +268,7 @@ def run_batched(args, ctx, torch, dev, stream, flush, fp64_single_rhs_value, pea
     ctx.set_batch_tensor_cores(False)
     ctx.field_EH_batch(jobs, precision="mixed", stream=sc, report=False)  # warm-up of the other kernel
     ms_cuda_cores = time_batch(max(1, min(steps, 2)), report=False)
-    ctx.set_batch_tensor_cores(True)
+    ctx.set_batch_tensor_cores(not args.no_tensor_cores)
     # the batch planned once and replayed from its CUDA graph (fixed geometry, currents in place)
     plan = ctx.batch_plan(jobs, precision="mixed", stream=sc)
     torch.cuda.synchronize()
@@ -357,7 +359,7 @@ def run_batched(args, ctx, torch, dev, stream, flush, fp64_single_rhs_value, pea
             "fp64_ms_per_step": ms64, "fp64_value": rhs_pairs / (ms64 * 1e-3),
             "mixed_over_fp64_batched": ms64 / ms,
             "est_rel_l2_reported": est_rel_l2, "ms_without_error_report": ms_no_est,
-            "contraction": "tensor cores (tcgen05 kind::tf32, TF32 hi+lo)",
+            "contraction": "CUDA cores" if args.no_tensor_cores else "tensor cores (tcgen05 kind::tf32, TF32 hi+lo)",
             "cuda_core_contraction_ms": ms_cuda_cores, "tensor_core_speedup": ms_cuda_cores / ms_no_est,
             "over_plain_fp64_single_rhs": value / fp64_single_rhs_value,
             "sequential_single_job_ms": ms_seq, "batched_over_sequential": ms_seq / ms,
@@ -664,6 +666,8 @@ def run_ours(args, ws, rank, local):
     pairs_per_step = S * N * P
 
     ctx = gpu.Context(local)
+    if args.no_tensor_cores:
+        ctx.set_batch_tensor_cores(False)
     mesh = ctx.mesh(cells)
     Jd = torch.from_numpy(np.ascontiguousarray(J)).to(dev)
     Pd = torch.from_numpy(np.ascontiguousarray(pts)).to(dev)
