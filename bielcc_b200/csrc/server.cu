@@ -750,7 +750,8 @@ int bielcc_server_create(bielcc_ctx ctx, int64_t hbm_budget, int n_slots, const 
             return set_api_error(BIELCC_ERR_CUDA, "server memory pool set-up failed");
         }
     }
-    for (Slot& sl : slots_of(sv)) sl.ws.pool = sl.pair_ws.pool = sl.io.pool = sv->pool;
+    for (Slot& sl : slots_of(sv)) sl.ws.pool = sl.pair_ws.pool = sl.io.pool = sl.samp_ws.pool = sl.samp_pair_ws.pool =
+        sv->pool;
     for (Slot& sl : slots_of(sv)) {
         int least = 0, greatest = 0;
         cudaDeviceGetStreamPriorityRange(&least, &greatest);
@@ -785,6 +786,22 @@ int bielcc_server_create(bielcc_ctx ctx, int64_t hbm_budget, int n_slots, const 
         cudaEventSynchronize(sv->ev_ref) != cudaSuccess) {
         cudaGetLastError();
         sv->ev_ref = nullptr;
+    }
+    // Map a quarter of the budget (at most half the free device memory) into the
+    // pool up front: growing the pool while other slots' kernels run can block a
+    // slot's thread for seconds. Best effort; bielcc_server_reserve adds more.
+    {
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+            const int64_t want = std::min<int64_t>(sv->budget / 4, (int64_t)(free_b / 2)) & ~((int64_t)(2 << 20) - 1);
+            cudaStream_t s0 = slots_of(sv).begin()->s_lo;
+            void* p = nullptr;
+            if (want > 0 && cudaMallocFromPoolAsync(&p, (size_t)want, sv->pool, s0) == cudaSuccess) {
+                cudaFreeAsync(p, s0);
+                cudaStreamSynchronize(s0);
+            }
+            cudaGetLastError();
+        }
     }
     for (Slot& sl : slots_of(sv)) sv->workers.emplace_back(slot_loop, sv, &sl);
     *out = sv;

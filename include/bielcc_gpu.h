@@ -569,7 +569,9 @@ typedef struct bielcc_server_stats {
 } bielcc_server_stats;
 
 /* hbm_budget <= 0 selects 150 GiB. np: NULL for the defaults; the server runs
- * the batched kernel, so np->p_max must be 1 and np->n_start <= 22. */
+ * the batched kernel, so np->p_max must be 1 and np->n_start <= 22. The
+ * server maps a quarter of its budget (at most half the free device memory)
+ * into its memory pool at creation. */
 int bielcc_server_create(bielcc_ctx ctx, int64_t hbm_budget, int n_slots, const bielcc_numparam* np,
                          int precision, bielcc_server* out);
 /* Drains the server (bounded wait), then frees it. */
