@@ -69,8 +69,8 @@ def parse():
     ap.add_argument("--serve-max-batch", type=int, default=64)
     ap.add_argument("--serve-reserve-gb", type=int, default=32, help="device memory the server maps up front")
     ap.add_argument("--serve-persistent", action="store_true", help="persistent far-kernel CTAs in served batches")
-    ap.add_argument("--serve-max-batch-pairs", type=float, default=0.0,
-                    help="cap on a served batch's (point, cell, RHS) pairs (0: none)")
+    ap.add_argument("--serve-max-batch-pairs", type=float, default=1e10,
+                    help="cap on a served batch's (point, cell, RHS) pairs (0: none); 1e10 is ~0.4 s of the GPU")
     ap.add_argument("--serve-asm-max-cells", type=int, default=20000,
                     help="largest mesh an assembly request draws (the config-5 mesh range)")
     ap.add_argument("--serve-asm-host-cells", type=int, default=2000,
@@ -267,8 +267,16 @@ def run_batched(args, ctx, torch, dev, stream, flush, fp64_single_rhs_value, pea
     ms_no_est = time_batch(steps, report=False)
     ctx.set_batch_tensor_cores(False)
     ctx.field_EH_batch(jobs, precision="mixed", stream=sc, report=False)  # warm-up of the other kernel
+    ctx.stats(reset=True)
     ms_cuda_cores = time_batch(max(1, min(steps, 2)), report=False)
+    ctas_cuda_cores = ctx.stats(reset=True)["far_ctas"]
+    other = [(E.clone(), H.clone()) for E, H in outs]
     ctx.set_batch_tensor_cores(not args.no_tensor_cores)
+    if args.no_tensor_cores:  # `other` holds the tensor-core form then
+        ctx.set_batch_tensor_cores(True)
+        ctx.field_EH_batch(jobs, precision="mixed", stream=sc, report=False)
+        other = [(E.clone(), H.clone()) for E, H in outs]
+        ctx.set_batch_tensor_cores(False)
     # the batch planned once and replayed from its CUDA graph (fixed geometry, currents in place)
     plan = ctx.batch_plan(jobs, precision="mixed", stream=sc)
     torch.cuda.synchronize()
@@ -312,10 +320,12 @@ def run_batched(args, ctx, torch, dev, stream, flush, fp64_single_rhs_value, pea
         b.synchronize()
         ms64 += a.elapsed_time(b)
     ms64 /= steps64
-    num = den = 0.0
-    for (Em, Hm), (E6, H6) in zip(mixed, outs):
+    num = den = num_o = 0.0
+    for (Em, Hm), (Eo, Ho), (E6, H6) in zip(mixed, other, outs):
         num += float(torch.sum(torch.abs(Em - E6) ** 2) + torch.sum(torch.abs(Hm - H6) ** 2))
+        num_o += float(torch.sum(torch.abs(Eo - E6) ** 2) + torch.sum(torch.abs(Ho - H6) ** 2))
         den += float(torch.sum(torch.abs(E6) ** 2) + torch.sum(torch.abs(H6) ** 2))
+    del mixed, other
     for m, _, _ in keep:
         m.close()
     value = rhs_pairs / (ms * 1e-3)
@@ -361,6 +371,8 @@ def run_batched(args, ctx, torch, dev, stream, flush, fp64_single_rhs_value, pea
             "est_rel_l2_reported": est_rel_l2, "ms_without_error_report": ms_no_est,
             "contraction": "CUDA cores" if args.no_tensor_cores else "tensor cores (tcgen05 kind::tf32, TF32 hi+lo)",
             "cuda_core_contraction_ms": ms_cuda_cores, "tensor_core_speedup": ms_cuda_cores / ms_no_est,
+            "far_ctas": st["far_ctas"], "cuda_core_far_ctas": ctas_cuda_cores,
+            "other_contraction_rel_l2_vs_fp64": (num_o / den) ** 0.5,
             "over_plain_fp64_single_rhs": value / fp64_single_rhs_value,
             "sequential_single_job_ms": ms_seq, "batched_over_sequential": ms_seq / ms,
             "graph_replay_ms": ms_graph, "graph_replay_value": rhs_pairs / (ms_graph * 1e-3), "gpu_launches_per_step":

@@ -256,6 +256,7 @@ class Stats(C.Structure):
         ("far_launches", C.c_int64),
         ("far_pairs", C.c_int64),
         ("far_ms", C.c_double),
+        ("far_ctas", C.c_int64),
     ]
 
 

@@ -105,7 +105,7 @@ struct bielcc_ctx_s {
     bool timing = false;
     cudaEvent_t far_begin = nullptr, far_end = nullptr;
     double batch_item_cost = 4.0e6;  // node evaluations per batched work item (bielcc_batch_autotune)
-    bielcc_stats stats = {0, 0, 0, 0.0};
+    bielcc_stats stats = {0, 0, 0, 0.0, 0};
 };
 
 namespace {
@@ -194,6 +194,7 @@ struct WsSet {
     DevBuf* scratch;
     long long* h_total;  // pinned near-pair count
     bool timed;          // far-kernel events into the context's stats
+    bool sample;         // an FP64 error sample: its far work stays out of far_launches / far_pairs
 };
 }  // namespace
 
@@ -201,9 +202,11 @@ bool ctx_batch_tensor_cores(bielcc_ctx_s* ctx) { return ctx->batch_tc; }
 
 namespace {
 
-WsSet main_ws(bielcc_ctx ctx) { return {&ctx->ws, &ctx->pair_ws, &ctx->scratch_small, ctx->h_total, ctx->timing}; }
+WsSet main_ws(bielcc_ctx ctx) {
+    return {&ctx->ws, &ctx->pair_ws, &ctx->scratch_small, ctx->h_total, ctx->timing, false};
+}
 WsSet side_ws(bielcc_ctx ctx) {
-    return {&ctx->side_ws, &ctx->side_pair_ws, &ctx->side_scratch, ctx->h_side_total, false};
+    return {&ctx->side_ws, &ctx->side_pair_ws, &ctx->side_scratch, ctx->h_side_total, false, true};
 }
 
 struct FieldArgs {
@@ -288,8 +291,10 @@ int field_device_batched(bielcc_ctx ctx, const FieldArgs& a, cudaStream_t s, bie
            a.np.p_max_seg};
     TRY_CUDA(batch_stage2(bp, dp, n_near, w.pair_ws->p, dn, d_nonfinite, s, &l2));
     ctx->stats.kernel_launches += l1 + l2;
-    ctx->stats.far_launches += 1;
-    ctx->stats.far_pairs += ((long long)a.n_pts * a.m->n_cells - n_near) * a.n_rhs;
+    if (!w.sample) {
+        ctx->stats.far_launches += 1;
+        ctx->stats.far_pairs += ((long long)a.n_pts * a.m->n_cells - n_near) * a.n_rhs;
+    }
     if (rep) {
         rep->n_pairs = (int64_t)a.n_pts * a.m->n_cells;
         rep->n_near_pairs = n_near;
@@ -361,8 +366,10 @@ int field_finish(bielcc_ctx ctx, FieldPending& p, cudaStream_t s, bielcc_report*
     if (n_near > 0) TRY(w.pair_ws->ensure(field_pair_ws_bytes(n_near)));
     TRY_CUDA(field_stage2(p.f, w.ws->p, p.splits, n_near, w.pair_ws->p, d_nonfinite, s, &l2));
     ctx->stats.kernel_launches += p.l1 + l2;
-    ctx->stats.far_launches += p.lf;
-    ctx->stats.far_pairs += ((long long)a.n_pts * a.m->n_cells - n_near) * a.n_rhs;
+    if (!w.sample) {
+        ctx->stats.far_launches += p.lf;
+        ctx->stats.far_pairs += ((long long)a.n_pts * a.m->n_cells - n_near) * a.n_rhs;
+    }
     if (rep) {
         rep->n_pairs = (int64_t)a.n_pts * a.m->n_cells;
         rep->n_near_pairs = n_near;
@@ -586,7 +593,7 @@ int bielcc_ctx_stats(bielcc_ctx ctx, bielcc_stats* out, int reset) {
     if (!ctx || !out) return set_error(BIELCC_ERR_ARG, "null argument");
     std::lock_guard<std::mutex> g(ctx->mu);
     *out = ctx->stats;
-    if (reset) ctx->stats = bielcc_stats{0, 0, 0, 0.0};
+    if (reset) ctx->stats = bielcc_stats{0, 0, 0, 0.0, 0};
     return BIELCC_OK;
 }
 
@@ -1091,6 +1098,7 @@ int field_batch_locked(bielcc_ctx ctx, int n_jobs, const bielcc_field_job* jobs,
     ctx->stats.kernel_launches += l1 + l2;
     ctx->stats.far_launches += 1;
     ctx->stats.far_pairs += pairs;
+    ctx->stats.far_ctas = bp.grid;
     if (report) {
         report->n_pairs = pairs;
         report->n_near_pairs = n_near;

@@ -1073,7 +1073,27 @@ int batch_grid(bool mixed, bool tc) {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (tc) {
         cudaFuncSetAttribute(batch_far_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tcb::kSmem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_far_tc_kernel, tcb::kThreads, tcb::kSmem);
+        // the whole shared-memory carveout: two CTAs of ~110 KB share one SM
+        cudaFuncSetAttribute(batch_far_tc_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_far_tc_kernel, tcb::kThreads, tcb::kSmem) !=
+            cudaSuccess) {
+            cudaGetLastError();
+            per = 1;
+        }
+        // the same bound from the kernel's registers and shared memory: the
+        // occupancy query can assume a smaller carveout than the launch gets
+        cudaFuncAttributes fa{};
+        int regs_sm = 65536, smem_sm = 0, resv = 0;
+        if (cudaFuncGetAttributes(&fa, batch_far_tc_kernel) == cudaSuccess &&
+            cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&resv, cudaDevAttrReservedSharedMemoryPerBlock, dev) == cudaSuccess) {
+            const int by_regs = regs_sm / std::max(1, fa.numRegs * tcb::kThreads);
+            const int by_smem = smem_sm / (int)(fa.sharedSizeBytes + tcb::kSmem + resv);
+            per = std::max(per, std::min(by_regs, by_smem));
+        }
+        cudaGetLastError();
         // every resident CTA holds kTmemCols of the SM's 512 tensor-memory columns
         per = std::min(per, 512 / (int)tcb::kTmemCols);
         return sms * std::max(1, per);

@@ -135,6 +135,7 @@ typedef struct bielcc_stats {
     int64_t far_launches;     /* far-field kernel launches */
     int64_t far_pairs;        /* far (point, cell, RHS) pairs those launches evaluated */
     double  far_ms;           /* summed CUDA-event time of the far-field kernels */
+    int64_t far_ctas;         /* CTAs of the last batched far launch (the persistent grid) */
 } bielcc_stats;
 int bielcc_ctx_set_timing(bielcc_ctx ctx, int on);
 /* Mixed-precision batches (bielcc_field_EH_batch, batch plans, served
