@@ -269,12 +269,12 @@ int field_device_batched(bielcc_ctx ctx, const FieldArgs& a, cudaStream_t s, bie
     plan_batch(bp, std::vector<JobDev>{d}, a.np.n_start, mixed, ctx->batch_item_cost, ctx->batch_tc);
     // The tuned item size suits batches of many jobs; one job alone is cut
     // finer (up to its range limit) when its items would leave resident CTAs idle.
-    if ((int)bp.items.size() < 2 * bp.grid) {
-        const double finer = std::max(1.0e5, ctx->batch_item_cost * bp.items.size() / (2.0 * bp.grid));
+    if ((int)bp.items.size() < 2 * bp.workers()) {
+        const double finer = std::max(1.0e5, ctx->batch_item_cost * bp.items.size() / (2.0 * bp.workers()));
         if (finer < ctx->batch_item_cost)
             plan_batch(bp, std::vector<JobDev>{d}, a.np.n_start, mixed, finer, ctx->batch_tc);
     }
-    const double busy = std::min(1.0, (double)bp.items.size() / std::max(1, bp.grid));
+    const double busy = std::min(1.0, (double)bp.items.size() / std::max(1, bp.workers()));
     const int S = a.n_rhs;
     const double single = (S / 4) * 1.1 + (S % 4) / 2 + (S % 2);  // single-job launches, in quadratures
     if (single * busy <= 1.05) return BIELCC_OK;

@@ -532,29 +532,44 @@ __global__ void __launch_bounds__(kBT, MIXED ? BIELCC_BATCH_MINB : 2) batch_far_
 // that D[(a, p), (s, re|im)] = sum_(c, b) W_ab(p, c) J_b(c, s) is one real GEMM
 // of M = 192 (two M = 128 MMAs, the second one's last 64 rows unused),
 // K = 48 per round and N = 2 S. FP32 operands are split into TF32 hi + lo and
-// each product is hi*hi + hi*lo + lo*hi, which keeps FP32-level accuracy. D
-// accumulates the chunk's 16 cells in tensor memory (FP32, as the CUDA-core
-// form accumulates them in registers) and is then added into the job's FP64
-// partial sums. A chunk's MMAs run while the warps evaluate the next round.
+// each product is hi*hi + hi*lo + lo*hi + lo*lo, which keeps FP32-level
+// accuracy. D accumulates the chunk's 16 cells in tensor memory (FP32, as the
+// CUDA-core form accumulates them in registers) and is then added into the
+// job's FP64 partial sums. A chunk's MMAs run while the warps evaluate the next
+// round.
+//
+// A CTA holds two such 8-warp groups, each with its own work item, shared
+// memory, named barrier, mbarriers and half of the CTA's 512 tensor-memory
+// columns: one CTA per SM, 16 warps, so that one group's barriers and loads
+// overlap the other group's moments. (Two 8-warp CTAs of ~110 KB fit one SM
+// by registers and shared memory, but measured only one of them was ever
+// resident per SM.)
 namespace tcb {
-constexpr int kThreads = 256;  // 8 warps
+constexpr int kGroups = 2;                          // independent 8-warp groups per CTA
+constexpr int kGroupThreads = 256;                  // 8 warps
+constexpr int kThreads = kGroups * kGroupThreads;   // the CTA
 constexpr int kRound = 8;      // cells per round: one per warp
 constexpr int kK = 6 * kRound; // K of a round
 constexpr int kRows = 192;     // (component, point)
 constexpr int kSmax = 64;      // right-hand sides held in tensor memory
 constexpr int kG = 16;         // right-hand sides per staged B group
-constexpr uint32_t kTmemCols = 256, kBlock2Col = 128;
+constexpr bool kLoLo = true;   // the lo*lo product too (4 MMAs per K step)
+constexpr uint32_t kTmemCols = 256, kBlock2Col = 128;   // per group
+constexpr uint32_t kTmemAlloc = kGroups * kTmemCols;    // per CTA (all 512 columns of the SM)
 constexpr uint32_t kAbytes = kRows * kK * 4;     // one of A hi / A lo
 constexpr uint32_t kBbytes = 2 * kG * kK * 4;    // one of B hi / B lo of one buffer
 constexpr uint32_t kSbo = (kK / 4) * 128;        // byte distance of 8-row groups
 constexpr int kNodes = kRound * 64;              // n_start <= 8
-// A hi, A lo, then B (2 buffers x hi, lo): the second M block of A lo reads
-// its 64 unused rows from the B buffers, which are larger than that.
+// per group: A hi, A lo, then B (2 buffers x hi, lo): the second M block of A
+// lo reads its 64 unused rows from the B buffers, which are larger than that.
 constexpr size_t kOffAl = kAbytes, kOffB = 2 * (size_t)kAbytes, kOffNodes = kOffB + 4 * (size_t)kBbytes;
 constexpr size_t kOffYY = kOffNodes + 16 * (size_t)kNodes, kOffCell = kOffYY + 4 * (size_t)kNodes;
 constexpr size_t kOffRho = kOffCell + 32 * kRound, kOffNear = kOffRho + 8 * kRound;
-constexpr size_t kSmem = kOffNear + kRound * 32;
+constexpr size_t kSmemGroup = kOffNear + kRound * 32;
+constexpr size_t kGroupStride = (kSmemGroup + 1023) & ~(size_t)1023;
+constexpr size_t kSmem = kGroups * kGroupStride;
 static_assert(64 * kK * 4 <= 4 * kBbytes, "the unused rows of the second M block must stay inside shared memory");
+static_assert(kSmem <= 232448 - 128, "two groups fit the opt-in shared memory of one CTA");
 // longest wait for one group of MMAs before the kernel gives up: 2 s of the
 // global timer, against microseconds of MMA work
 constexpr uint64_t kWaitNs = 2000000000ull;
@@ -614,8 +629,8 @@ BIELCC_D void tc_split64(double v, float& hi, float& lo) {
 
 // Stages B of right-hand sides s0 .. s0 + 15 for the round's cells (zeros for
 // missing cells and right-hand sides): rows 2 s + (re|im of the output).
-BIELCC_D void tc_stage_b(unsigned char* Bh, unsigned char* Bl, const JobDev& jb, int c0, int nc, int s0) {
-    for (int i = threadIdx.x; i < tcb::kRound * tcb::kG * 3; i += tcb::kThreads) {
+BIELCC_D void tc_stage_b(unsigned char* Bh, unsigned char* Bl, const JobDev& jb, int c0, int nc, int s0, int gt) {
+    for (int i = gt; i < tcb::kRound * tcb::kG * 3; i += tcb::kGroupThreads) {
         const int cl = i / (tcb::kG * 3), rem = i - cl * (tcb::kG * 3), sl = rem / 3, b = rem - sl * 3;
         const int s = s0 + sl;
         cplx v = mk(0., 0.);
@@ -648,15 +663,40 @@ BIELCC_D void tc_issue_group(uint32_t tmem, uint32_t sA, uint32_t sAl, uint32_t 
             umma::mma_tf32(d, ah, bh, id, !(first_round && ks == 0));
             umma::mma_tf32(d, ah, bl, id, true);
             umma::mma_tf32(d, al, bh, id, true);
+            if (tcb::kLoLo) umma::mma_tf32(d, al, bl, id, true);
         }
     }
 }
 
-__global__ void __launch_bounds__(tcb::kThreads, 2)
+// Barrier of one 8-warp group (named barrier `id`, kGroupThreads threads),
+// and the same barrier reducing a predicate with OR over the group.
+BIELCC_D void group_sync(int id) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(tcb::kGroupThreads) : "memory");
+}
+BIELCC_D bool group_or(int id, bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t"
+        ".reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, %2, %3, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t"
+        "}\n"
+        : "=r"(r)
+        : "r"((uint32_t)v), "r"(id), "r"(tcb::kGroupThreads)
+        : "memory");
+    return r != 0;
+}
+
+__global__ void __launch_bounds__(tcb::kThreads, 1)
     batch_far_tc_kernel(const JobDev* __restrict__ jobs, const BatchItem* __restrict__ items, int n_items,
                         int* __restrict__ counter, double analytic_calc, int n_start, int max_items,
                         long long* __restrict__ err) {
-    extern __shared__ __align__(128) unsigned char smem[];
+    extern __shared__ __align__(1024) unsigned char smem_all[];
+    const int grp = threadIdx.x / tcb::kGroupThreads;
+    const int gt = threadIdx.x - grp * tcb::kGroupThreads;  // thread of the group
+    const int bar_id = 1 + grp;                             // named barrier of the group (0: __syncthreads)
+    unsigned char* smem = smem_all + grp * tcb::kGroupStride;
     unsigned char* sAh = smem;
     unsigned char* sAl = smem + tcb::kOffAl;
     unsigned char* sB = smem + tcb::kOffB;  // buffer q: hi at 2 q kBbytes, lo at (2 q + 1) kBbytes
@@ -665,22 +705,29 @@ __global__ void __launch_bounds__(tcb::kThreads, 2)
     double4* s_cell = reinterpret_cast<double4*>(smem + tcb::kOffCell);
     double* s_rho = reinterpret_cast<double*>(smem + tcb::kOffRho);
     unsigned char* s_near = smem + tcb::kOffNear;
-    __shared__ uint64_t bar[2];
+    __shared__ uint64_t bars[tcb::kGroups][2];
     __shared__ uint32_t s_tmem;
-    __shared__ int s_item;
+    __shared__ int s_items[tcb::kGroups];
+    uint64_t* bar = bars[grp];
+    int& s_item = s_items[grp];
 
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int warp = gt >> 5, lane = gt & 31;  // warp of the group; warp % 4 = the SM warp's % 4
     const int nn = n_start * n_start;
     if (threadIdx.x == 0) {
-        umma::mbar_init(&bar[0], 1);
-        umma::mbar_init(&bar[1], 1);
+        for (int g = 0; g < tcb::kGroups; g++) {
+            umma::mbar_init(&bars[g][0], 1);
+            umma::mbar_init(&bars[g][1], 1);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 0) umma::tmem_alloc(&s_tmem, tcb::kTmemCols);
+    if (threadIdx.x < 32) {
+        umma::tmem_alloc(&s_tmem, tcb::kTmemAlloc);
+        umma::tmem_relinquish();
+    }
     umma::fence_before_sync();
     __syncthreads();
     umma::fence_after_sync();
-    const uint32_t tmem = s_tmem;
+    const uint32_t tmem = s_tmem + (uint32_t)grp * tcb::kTmemCols;
     const uint32_t uA = umma::smem_u32(sAh), uAl = umma::smem_u32(sAl), uB = umma::smem_u32(sB);
     // commits in flight per barrier (0 or 1) and the parity of the next phase to wait for
     int inflight[2] = {0, 0};
@@ -698,18 +745,18 @@ __global__ void __launch_bounds__(tcb::kThreads, 2)
     auto wait_all = [&]() -> bool {
         const bool ok0 = wait_one_local(0);
         const bool ok1 = wait_one_local(1);
-        return !__syncthreads_or(!(ok0 && ok1));
+        return !group_or(bar_id, !(ok0 && ok1));
     };
-    auto wait_one = [&](int q) -> bool { return !__syncthreads_or(!wait_one_local(q)); };
+    auto wait_one = [&](int q) -> bool { return !group_or(bar_id, !wait_one_local(q)); };
 
     // D of the last chunk, added to the partial sums once its MMAs completed
     bool pend = false, pend_first = false;
     int pend_range = 0;
 
     for (int taken = 0; taken < max_items && !abort; taken++) {
-        __syncthreads();
-        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
-        __syncthreads();
+        group_sync(bar_id);
+        if (gt == 0) s_item = atomicAdd(counter, 1);
+        group_sync(bar_id);
         const int it = s_item;
         if (it >= n_items) break;
         const BatchItem bi = items[it];
@@ -764,21 +811,21 @@ __global__ void __launch_bounds__(tcb::kThreads, 2)
                 const int rc0 = c0 + r * tcb::kRound;
                 const int nc = min(tcb::kRound, ce - rc0);
                 if (nc <= 0) break;
-                __syncthreads();  // the previous round's reads of the staged nodes are done
+                group_sync(bar_id);  // the previous round's reads of the staged nodes are done
                 {
                     const float4* src = jb.nodes32 + (size_t)rc0 * nn;
-                    for (int i = threadIdx.x; i < nc * nn; i += tcb::kThreads) {
+                    for (int i = gt; i < nc * nn; i += tcb::kGroupThreads) {
                         const float4 v = __ldg(src + i);
                         s_nodes[i] = v;
                         s_yy[i] = node_yy(v);
                     }
-                    for (int i = threadIdx.x; i < nc; i += tcb::kThreads) {
+                    for (int i = gt; i < nc; i += tcb::kGroupThreads) {
                         const CellGeo& gg = jb.geo[rc0 + i];
                         s_cell[i] = make_double4(gg.c[0], gg.c[1], gg.c[2], gg.diam);
                         s_rho[i] = (double)jb.rho32[rc0 + i];
                     }
                 }
-                __syncthreads();
+                group_sync(bar_id);
                 // phase A: the moments of cell `warp` of the round for this warp's 32 points
                 float mom[20];
 #pragma unroll
@@ -806,11 +853,11 @@ __global__ void __launch_bounds__(tcb::kThreads, 2)
                 umma::fence_after_sync();
                 if (pend) drain();
                 tc_write_a(sAh, sAl, lane, warp, mom);
-                tc_stage_b(sB, sB + tcb::kBbytes, jb, rc0, nc, 0);
-                if (G > 1) tc_stage_b(sB + 2 * tcb::kBbytes, sB + 3 * tcb::kBbytes, jb, rc0, nc, tcb::kG);
+                tc_stage_b(sB, sB + tcb::kBbytes, jb, rc0, nc, 0, gt);
+                if (G > 1) tc_stage_b(sB + 2 * tcb::kBbytes, sB + 3 * tcb::kBbytes, jb, rc0, nc, tcb::kG, gt);
                 umma::fence_async_smem();
                 umma::fence_before_sync();
-                __syncthreads();
+                group_sync(bar_id);
                 umma::fence_after_sync();
                 // near-cell mask: warp 0 owns the words of its points
                 if (warp == 0) {
@@ -832,13 +879,13 @@ __global__ void __launch_bounds__(tcb::kThreads, 2)
                         }
                         umma::fence_after_sync();
                         tc_stage_b(sB + 2 * q * tcb::kBbytes, sB + (2 * q + 1) * tcb::kBbytes, jb, rc0, nc,
-                                   g * tcb::kG);
+                                   g * tcb::kG, gt);
                         umma::fence_async_smem();
                         umma::fence_before_sync();
-                        __syncthreads();
+                        group_sync(bar_id);
                         umma::fence_after_sync();
                     }
-                    if (threadIdx.x == 0) {
+                    if (gt == 0) {
                         const int n = 2 * min(tcb::kG, Spad - g * tcb::kG);
                         tc_issue_group(tmem, uA, uAl, uB + 2 * q * tcb::kBbytes, uB + (2 * q + 1) * tcb::kBbytes, g, n,
                                        r == 0);
@@ -859,17 +906,17 @@ __global__ void __launch_bounds__(tcb::kThreads, 2)
         }
     }
     if (abort) {
-        if (threadIdx.x == 0) atomicExch(reinterpret_cast<unsigned long long*>(err), 1ull);
+        if (gt == 0) atomicExch(reinterpret_cast<unsigned long long*>(err), 1ull);
         // MMAs still in flight: wait for them (bounded) before the tensor memory is released
         for (int q = 0; q < 2; q++)
             if (inflight[q]) umma::mbar_wait(&bar[q], parity[q], tcb::kWaitNs);
     }
+    // both groups done: the first warp frees the CTA's tensor memory
     umma::fence_before_sync();
     __syncthreads();
-    if (warp == 0) {
+    if (threadIdx.x < 32) {
         umma::fence_after_sync();
-        umma::tmem_dealloc(tmem, tcb::kTmemCols);
-        umma::tmem_relinquish();
+        umma::tmem_dealloc(s_tmem, tcb::kTmemAlloc);
     }
 }
 
@@ -1073,7 +1120,6 @@ int batch_grid(bool mixed, bool tc) {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (tc) {
         cudaFuncSetAttribute(batch_far_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tcb::kSmem);
-        // the whole shared-memory carveout: two CTAs of ~110 KB share one SM
         cudaFuncSetAttribute(batch_far_tc_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
                              (int)cudaSharedmemCarveoutMaxShared);
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_far_tc_kernel, tcb::kThreads, tcb::kSmem) !=
@@ -1094,8 +1140,8 @@ int batch_grid(bool mixed, bool tc) {
             per = std::max(per, std::min(by_regs, by_smem));
         }
         cudaGetLastError();
-        // every resident CTA holds kTmemCols of the SM's 512 tensor-memory columns
-        per = std::min(per, 512 / (int)tcb::kTmemCols);
+        // every resident CTA holds kTmemAlloc of the SM's 512 tensor-memory columns
+        per = std::min(per, 512 / (int)tcb::kTmemAlloc);
         return sms * std::max(1, per);
     }
     size_t smem = mixed ? BatchCfg<true>::smem_bytes() : BatchCfg<false>::smem_bytes();
@@ -1130,6 +1176,7 @@ void plan_batch(BatchPlan& bp, const std::vector<JobDev>& jobs_in, int n_start, 
     bp.tc = mixed && allow_tc && n_start <= 8;
     for (const JobDev& j : jobs_in) bp.tc = bp.tc && j.n_rhs <= tcb::kSmax;
     bp.grid = batch_grid(mixed, bp.tc);
+    bp.per_cta = bp.tc ? tcb::kGroups : 1;
     const double nodes = (double)n_start * n_start;
     bp.items.clear();
     bp.pt_job.clear();
@@ -1169,7 +1216,8 @@ void plan_batch(BatchPlan& bp, const std::vector<JobDev>& jobs_in, int n_start, 
 
 void batch_make_preemptible(BatchPlan& bp) {
     bp.max_items = 1;
-    bp.grid = std::max<int>(1, (int)std::min<size_t>(bp.items.size(), (size_t)INT32_MAX));
+    const size_t ctas = (bp.items.size() + bp.per_cta - 1) / bp.per_cta;
+    bp.grid = std::max<int>(1, (int)std::min<size_t>(ctas, (size_t)INT32_MAX));
 }
 
 // Enqueues stage 1 (far kernel, near counting, scan) of a planned batch into

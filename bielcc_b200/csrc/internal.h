@@ -193,6 +193,8 @@ struct BatchPlan {
     // mixed batches whose jobs have at most 64 right-hand sides (n_start <= 8)
     // contract their moments on the tensor cores (batch_far_tc_kernel)
     bool tc = false;
+    int per_cta = 1;  // items a CTA works on at once (the tensor-core kernel's CTA holds two groups)
+    int workers() const { return grid * per_cta; }
 };
 // Turns a planned batch into one CTA per item (see BatchPlan::max_items).
 void batch_make_preemptible(BatchPlan& bp);
