@@ -59,8 +59,8 @@ def parse():
     ap.add_argument("--no-assembly", action="store_true", help="skip the 20,480-triangle assembly leg")
     ap.add_argument("--assembly-level", type=int, default=5, help="icosphere level of the assembly leg (5: 20,480)")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream leg")
-    ap.add_argument("--no-tensor-cores", action="store_true",
-                    help="mixed batches contract on the CUDA cores (bielcc_ctx_set_batch_tensor_cores(ctx, 0))")
+    ap.add_argument("--tensor-cores", action="store_true",
+                    help="mixed batches contract on the tensor cores (bielcc_ctx_set_batch_tensor_cores(ctx, 1))")
     ap.add_argument("--small", action="store_true",
                     help="reduced case for profiler captures: 2048-cell sphere x 5000 points (not a bench line)")
     ap.add_argument("--serve-requests", type=int, default=600)
@@ -263,20 +263,15 @@ def run_batched(args, ctx, torch, dev, stream, flush, fp64_single_rhs_value, pea
         return t / n
 
     # the same batch without the error report (no FP64 sample), and with the
-    # contraction on the CUDA cores instead of the tensor cores
+    # other form of the contraction (tensor cores <-> CUDA cores)
     ms_no_est = time_batch(steps, report=False)
-    ctx.set_batch_tensor_cores(False)
+    ctx.set_batch_tensor_cores(not args.tensor_cores)
     ctx.field_EH_batch(jobs, precision="mixed", stream=sc, report=False)  # warm-up of the other kernel
     ctx.stats(reset=True)
-    ms_cuda_cores = time_batch(max(1, min(steps, 2)), report=False)
-    ctas_cuda_cores = ctx.stats(reset=True)["far_ctas"]
+    ms_other = time_batch(max(1, min(steps, 2)), report=False)
+    ctas_other = ctx.stats(reset=True)["far_ctas"]
     other = [(E.clone(), H.clone()) for E, H in outs]
-    ctx.set_batch_tensor_cores(not args.no_tensor_cores)
-    if args.no_tensor_cores:  # `other` holds the tensor-core form then
-        ctx.set_batch_tensor_cores(True)
-        ctx.field_EH_batch(jobs, precision="mixed", stream=sc, report=False)
-        other = [(E.clone(), H.clone()) for E, H in outs]
-        ctx.set_batch_tensor_cores(False)
+    ctx.set_batch_tensor_cores(args.tensor_cores)
     # the batch planned once and replayed from its CUDA graph (fixed geometry, currents in place)
     plan = ctx.batch_plan(jobs, precision="mixed", stream=sc)
     torch.cuda.synchronize()
@@ -320,19 +315,22 @@ def run_batched(args, ctx, torch, dev, stream, flush, fp64_single_rhs_value, pea
         b.synchronize()
         ms64 += a.elapsed_time(b)
     ms64 /= steps64
-    num = den = num_o = 0.0
-    for (Em, Hm), (Eo, Ho), (E6, H6) in zip(mixed, other, outs):
-        num += float(torch.sum(torch.abs(Em - E6) ** 2) + torch.sum(torch.abs(Hm - H6) ** 2))
-        num_o += float(torch.sum(torch.abs(Eo - E6) ** 2) + torch.sum(torch.abs(Ho - H6) ** 2))
+    den = 0.0
+    for E6, H6 in outs:
         den += float(torch.sum(torch.abs(E6) ** 2) + torch.sum(torch.abs(H6) ** 2))
-    del mixed, other
     for m, _, _ in keep:
         m.close()
     value = rhs_pairs / (ms * 1e-3)
-    # The moments (the quadrature) bound the FP32 pipe; the contraction runs on
-    # the tensor cores: per 32-point tile, cell and group of 16 RHS, two M = 128
-    # MMAs of K = 6 and N = 2 min(16, S8 - 16 g) (S8 = S rounded up to 8), three
-    # TF32 products each. Time without the error report (no FP64 sample).
+    # Roofline of the whole launch against the measured FP32 FMA peak: 8320
+    # flops per (point, cell) quadrature (the moments) plus 114 per (point,
+    # cell, RHS) for the contraction on the CUDA cores. The tensor-core form
+    # runs the moments on the FP32 pipe and the contraction as 2 M = 128 MMAs
+    # of K = 6 and N = 2 min(16, S8 - 16 g) (S8 = S rounded up to 8) per 32-point
+    # tile, cell and group of 16 RHS, three TF32 products each. Times without the
+    # error report (no FP64 sample).
+    ms_cc, ms_tc = (ms_other, ms_no_est) if args.tensor_cores else (ms_no_est, ms_other)
+    ctas_cc, ctas_tc = (ctas_other, st["far_ctas"]) if args.tensor_cores else (st["far_ctas"], ctas_other)
+    out_cc, out_tc = (other, mixed) if args.tensor_cores else (mixed, other)
     tc_flops = 0.0
     for j in jobs_np:
         S = j["J"].shape[0]
@@ -340,39 +338,50 @@ def run_batched(args, ctx, torch, dev, stream, flush, fp64_single_rhs_value, pea
         n_sum = sum(2 * min(16, s8 - 16 * g) for g in range((S + 15) // 16))
         tiles = (len(j["pts"]) + 31) // 32
         tc_flops += tiles * len(j["cells"]) * 2 * 128 * 6 * n_sum * 3 * 2
-    quad = geo_pairs * FLOPS_PER_FAR_PAIR / (ms_no_est * 1e-3) / 1e12
     peak_tf32 = None
     try:
         mp = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
         peak_tf32 = mp["bf16_tflops"] / 2.0
     except Exception:
         pass
-    tc_achieved = tc_flops / (ms_no_est * 1e-3) / 1e12
-    roofline = {"bound": "fp32 CUDA-core pipe (the moments); the contraction runs on the tensor cores",
-                "kernel": "batch_far_tc_kernel (whole batch, one launch)",
-                "achieved": quad, "peak": peak32, "unit": "TFLOP/s", "frac": quad / peak32,
-                "flops": f"{FLOPS_PER_FAR_PAIR} per (point, cell) quadrature",
-                "peak_source": "measured FMA loop (bielcc_measure_fma_peak)",
-                "tensor": {"achieved": tc_achieved, "unit": "TFLOP/s (TF32, issued)",
-                           "peak": peak_tf32, "frac": tc_achieved / peak_tf32 if peak_tf32 else None,
-                           "peak_source": "half the measured dense bf16 rate (MEASURED_PEAKS.json bf16_tflops)",
-                           "flops": "2 M=128 MMAs x K=6 per (tile, cell) and 16-RHS group, 3 TF32 products"},
-                "cuda_core_form": {"achieved": (geo_pairs * FLOPS_PER_FAR_PAIR + rhs_pairs *
-                                                FLOPS_PER_RHS_CONTRACTION) / (ms_cuda_cores * 1e-3) / 1e12,
-                                   "flops": f"{FLOPS_PER_FAR_PAIR} per (point, cell) + "
-                                            f"{FLOPS_PER_RHS_CONTRACTION} per (point, cell, RHS)"}}
+    cc_achieved = (geo_pairs * FLOPS_PER_FAR_PAIR + rhs_pairs * FLOPS_PER_RHS_CONTRACTION) / (ms_cc * 1e-3) / 1e12
+    tc_moments = geo_pairs * FLOPS_PER_FAR_PAIR / (ms_tc * 1e-3) / 1e12
+    tc_achieved = tc_flops / (ms_tc * 1e-3) / 1e12
+
+    def rel_vs_fp64(outs_m):
+        num = 0.0
+        for (Em, Hm), (E6, H6) in zip(outs_m, outs):
+            num += float(torch.sum(torch.abs(Em - E6) ** 2) + torch.sum(torch.abs(Hm - H6) ** 2))
+        return (num / den) ** 0.5
+
+    roofline = {"bound": "fp32 CUDA-core pipe (the moments and, in the default form, the contraction)",
+                "kernel": "batch_far_tc_kernel (whole batch, one launch)" if args.tensor_cores
+                else "batch_far_kernel<MIXED=1> (whole batch, one launch)",
+                "achieved": tc_moments if args.tensor_cores else cc_achieved, "peak": peak32, "unit": "TFLOP/s",
+                "frac": (tc_moments if args.tensor_cores else cc_achieved) / peak32,
+                "flops": f"{FLOPS_PER_FAR_PAIR} per (point, cell) quadrature" + (
+                    "" if args.tensor_cores else f" + {FLOPS_PER_RHS_CONTRACTION} per (point, cell, RHS)"),
+                "peak_source": "measured FMA loop (bielcc_measure_fma_peak)"}
+    forms = {"cuda_cores": {"ms": ms_cc, "ctas": ctas_cc, "rel_l2_vs_fp64": rel_vs_fp64(out_cc),
+                            "achieved_tflops": cc_achieved, "frac_of_fp32_peak": cc_achieved / peak32},
+             "tensor_cores": {"ms": ms_tc, "ctas": ctas_tc, "rel_l2_vs_fp64": rel_vs_fp64(out_tc),
+                              "moments_tflops": tc_moments, "moments_frac_of_fp32_peak": tc_moments / peak32,
+                              "tensor_tflops_issued": tc_achieved, "tensor_peak": peak_tf32,
+                              "tensor_frac": tc_achieved / peak_tf32 if peak_tf32 else None,
+                              "tensor_peak_source": "half the measured dense bf16 rate (MEASURED_PEAKS.json)",
+                              "kernel": "batch_far_tc_kernel: tcgen05.mma kind::tf32, TF32 hi + lo, "
+                                        "two 8-warp groups per CTA"},
+             "tensor_core_speedup": ms_cc / ms_tc}
     return {"workload": f"{len(jobs_np)} meshes (spheroids, rounded cubes, tori), 200-20000 cells, k 0.5-20, "
                         f"1-64 PO RHS, 2000 far points each, seed 3",
             "value": value, "unit": "(point, cell, RHS) pairs/s", "geometry_pairs_per_s": geo_pairs / (ms * 1e-3),
             "ms_per_step": ms, "steps": steps, "rhs_pairs_per_step": rhs_pairs, "geometry_pairs_per_step": geo_pairs,
-            "rel_l2_vs_fp64": (num / den) ** 0.5, "autotuned_item_cost": item_cost, "roofline": roofline,
+            "rel_l2_vs_fp64": rel_vs_fp64(mixed), "autotuned_item_cost": item_cost, "roofline": roofline,
             "fp64_ms_per_step": ms64, "fp64_value": rhs_pairs / (ms64 * 1e-3),
             "mixed_over_fp64_batched": ms64 / ms,
             "est_rel_l2_reported": est_rel_l2, "ms_without_error_report": ms_no_est,
-            "contraction": "CUDA cores" if args.no_tensor_cores else "tensor cores (tcgen05 kind::tf32, TF32 hi+lo)",
-            "cuda_core_contraction_ms": ms_cuda_cores, "tensor_core_speedup": ms_cuda_cores / ms_no_est,
-            "far_ctas": st["far_ctas"], "cuda_core_far_ctas": ctas_cuda_cores,
-            "other_contraction_rel_l2_vs_fp64": (num_o / den) ** 0.5,
+            "contraction": "tensor cores (tcgen05 kind::tf32, TF32 hi+lo)" if args.tensor_cores else "CUDA cores",
+            "contraction_forms": forms, "far_ctas": st["far_ctas"],
             "over_plain_fp64_single_rhs": value / fp64_single_rhs_value,
             "sequential_single_job_ms": ms_seq, "batched_over_sequential": ms_seq / ms,
             "graph_replay_ms": ms_graph, "graph_replay_value": rhs_pairs / (ms_graph * 1e-3), "gpu_launches_per_step":
@@ -678,8 +687,8 @@ def run_ours(args, ws, rank, local):
     pairs_per_step = S * N * P
 
     ctx = gpu.Context(local)
-    if args.no_tensor_cores:
-        ctx.set_batch_tensor_cores(False)
+    if args.tensor_cores:
+        ctx.set_batch_tensor_cores(True)
     mesh = ctx.mesh(cells)
     Jd = torch.from_numpy(np.ascontiguousarray(J)).to(dev)
     Pd = torch.from_numpy(np.ascontiguousarray(pts)).to(dev)

@@ -98,7 +98,7 @@ struct bielcc_ctx_s {
     cudaEvent_t side_in = nullptr;
     cudaEvent_t side_out = nullptr;  // the side stream's error sample is complete
     DevBuf side_ws, side_pair_ws, side_io, side_scratch;
-    bool batch_tc = true;               // mixed batches contract on the tensor cores when they qualify
+    bool batch_tc = false;              // mixed batches contract on the tensor cores when they qualify
     long long* h_side_total = nullptr;  // pinned
     unsigned long long* h_nonfinite = nullptr;
     // counters / timing (bielcc_ctx_stats)

@@ -532,8 +532,8 @@ __global__ void __launch_bounds__(kBT, MIXED ? BIELCC_BATCH_MINB : 2) batch_far_
 // that D[(a, p), (s, re|im)] = sum_(c, b) W_ab(p, c) J_b(c, s) is one real GEMM
 // of M = 192 (two M = 128 MMAs, the second one's last 64 rows unused),
 // K = 48 per round and N = 2 S. FP32 operands are split into TF32 hi + lo and
-// each product is hi*hi + hi*lo + lo*hi + lo*lo, which keeps FP32-level
-// accuracy. D accumulates the chunk's 16 cells in tensor memory (FP32, as the
+// each product is hi*hi + hi*lo + lo*hi (lo*lo is below the operands' own
+// rounding: adding it left the measured error unchanged). D accumulates the chunk's 16 cells in tensor memory (FP32, as the
 // CUDA-core form accumulates them in registers) and is then added into the
 // job's FP64 partial sums. A chunk's MMAs run while the warps evaluate the next
 // round.
@@ -553,7 +553,7 @@ constexpr int kK = 6 * kRound; // K of a round
 constexpr int kRows = 192;     // (component, point)
 constexpr int kSmax = 64;      // right-hand sides held in tensor memory
 constexpr int kG = 16;         // right-hand sides per staged B group
-constexpr bool kLoLo = true;   // the lo*lo product too (4 MMAs per K step)
+constexpr bool kLoLo = false;  // the lo*lo product too (measured: no change of the error)
 constexpr uint32_t kTmemCols = 256, kBlock2Col = 128;   // per group
 constexpr uint32_t kTmemAlloc = kGroups * kTmemCols;    // per CTA (all 512 columns of the SM)
 constexpr uint32_t kAbytes = kRows * kK * 4;     // one of A hi / A lo

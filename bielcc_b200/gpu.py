@@ -256,7 +256,7 @@ class Context:
         _check(_lib.bielcc_ctx_set_timing(self.h, int(bool(on))))
 
     def set_batch_tensor_cores(self, on=True):
-        """Mixed batches contract moments and currents on the tensor cores (default) or the CUDA cores."""
+        """Mixed batches contract moments and currents on the tensor cores or on the CUDA cores (default)."""
         _check(_lib.bielcc_ctx_set_batch_tensor_cores(self.h, int(bool(on))))
 
     def stats(self, reset=False):

@@ -142,9 +142,10 @@ int bielcc_ctx_set_timing(bielcc_ctx ctx, int on);
  * batches, single-job calls routed as one-job batches) whose jobs have at most
  * 64 right-hand sides and n_start <= 8 contract their far moments with the
  * currents on the tensor cores (tcgen05, TF32 split into hi + lo, FP32
- * accumulation over 16 cells, FP64 across) when on = 1 (the default);
- * on = 0 keeps that contraction on the CUDA cores. No counterpart in the
- * reference. */
+ * accumulation over 16 cells, FP64 across) when on = 1; on = 0 (the default)
+ * keeps that contraction on the CUDA cores, which measured faster and more
+ * accurate on the batched workloads (the moments, not the contraction, bound
+ * both forms). No counterpart in the reference. */
 int bielcc_ctx_set_batch_tensor_cores(bielcc_ctx ctx, int on);
 int bielcc_ctx_stats(bielcc_ctx ctx, bielcc_stats* out, int reset);
 

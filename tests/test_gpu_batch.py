@@ -89,11 +89,20 @@ def test_batch_fallback_adaptive_and_autotune(gctx):
     assert c > 0
 
 
-def test_batch_plan_graph_replay_with_new_currents(gctx):
+@pytest.mark.parametrize("tensor_cores", [False, True])
+def test_batch_plan_graph_replay_with_new_currents(gctx, tensor_cores):
     """A planned batch replayed from its CUDA graph after the currents changed
     in place gives the same result as a fresh batched call with those
-    currents, and matches the oracle."""
+    currents, and matches the oracle; with either contraction."""
     torch = pytest.importorskip("torch")
+    gctx.set_batch_tensor_cores(tensor_cores)
+    try:
+        _plan_replay(torch, gctx)
+    finally:
+        gctx.set_batch_tensor_cores(False)
+
+
+def _plan_replay(torch, gctx):
     dev = torch.device("cuda:0")
     specs = _jobs(gctx, seed=7)
     tens, jspecs = [], []
@@ -189,7 +198,7 @@ def test_batch_tensor_core_contraction_matches_cuda_cores(gctx):
         gctx.set_batch_tensor_cores(False)
         cc, _ = _batch(torch, gctx, specs, "mixed")
     finally:
-        gctx.set_batch_tensor_cores(True)
+        gctx.set_batch_tensor_cores(False)
     assert rep.n_near_pairs > 0
     for sp, (E, H), (Ec, Hc) in zip(specs, tc, cc):
         assert rel_l2(E, Ec) < TOL_MIXED and rel_l2(H, Hc) < TOL_MIXED
