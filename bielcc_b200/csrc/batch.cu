@@ -50,6 +50,14 @@ constexpr int kBW = 4;    // warps
 #ifndef BIELCC_BATCH_MINB
 #define BIELCC_BATCH_MINB 3
 #endif
+// Mixed form: phase A two cells per warp at a time (TWO = 1) or one; RHS per
+// thread in phase B (R; SP a multiple of 4 R).
+#ifndef BIELCC_BATCH_TWO
+#define BIELCC_BATCH_TWO 1
+#endif
+#ifndef BIELCC_BATCH_R
+#define BIELCC_BATCH_R 4
+#endif
 constexpr int kSP = BIELCC_BATCH_SP;  // right-hand sides staged per pass (a multiple of kBW x R)
 // Unrolling of the one-cell and two-cell phase-A node loops. Three CTAs of
 // different jobs (different phase polynomials) share an SM's instruction
@@ -70,7 +78,7 @@ struct BatchCfg {
     using NodeT = typename std::conditional<MIXED, float4, double4>::type;
     static constexpr int CH = MIXED ? BIELCC_BATCH_CH32 : 8;            // cells per chunk (n_start <= 8)
     static constexpr int NODES = MIXED ? 64 * BIELCC_BATCH_CH32 : 512;  // staged nodes
-    static constexpr int R = MIXED ? 4 : 2;               // RHS per thread in phase B
+    static constexpr int R = MIXED ? BIELCC_BATCH_R : 2;  // RHS per thread in phase B
     // currents per (cell, RHS, component): FP32 (re, im, im, re) for the packed
     // contraction, FP64 (re, im)
     static constexpr int JW = MIXED ? 4 : 2;
@@ -80,6 +88,8 @@ struct BatchCfg {
                sizeof(double4) * CH + sizeof(double) * CH + CH * kBP + 64;
     }
 };
+static_assert(kSP % (kBW * BatchCfg<true>::R) == 0, "a phase-B pass covers whole groups of kBW x R RHS");
+
 
 // acc[12] += contraction of one cell's moments m[20] (a1r, a1i, t[6][2], g[3][2])
 // with the current J = (jr, ji): E = (A1 I + T) J, H = G x J. The caller has
@@ -429,7 +439,7 @@ __global__ void __launch_bounds__(kBT, MIXED ? BIELCC_BATCH_MINB : 2) batch_far_
             __syncthreads();
             // phase A: moments of cells warp, warp+4, ... for this warp's 32 points; the
             // mixed form takes them two at a time (cells cc and cc + 4)
-            if constexpr (MIXED) {
+            if constexpr (MIXED && BIELCC_BATCH_TWO) {
                 for (int cc = warp; cc < nc; cc += 2 * kBW) {
                     const int cb2 = cc + kBW;
                     const bool two = cb2 < nc;
@@ -692,7 +702,7 @@ __global__ void __launch_bounds__(tcb::kThreads, 1)
     batch_far_tc_kernel(const JobDev* __restrict__ jobs, const BatchItem* __restrict__ items, int n_items,
                         int* __restrict__ counter, double analytic_calc, int n_start, int max_items,
                         long long* __restrict__ err) {
-    extern __shared__ __align__(1024) unsigned char smem_all[];
+    extern __shared__ __align__(128) unsigned char smem_all[];
     const int grp = threadIdx.x / tcb::kGroupThreads;
     const int gt = threadIdx.x - grp * tcb::kGroupThreads;  // thread of the group
     const int bar_id = 1 + grp;                             // named barrier of the group (0: __syncthreads)

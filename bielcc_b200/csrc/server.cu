@@ -574,20 +574,33 @@ void complete_slot(bielcc_server_s* sv, Slot& sl) {
 std::vector<Req*> admit_locked(bielcc_server_s* sv) {
     std::vector<Req*> take;
     int64_t work = 0;
-    while (!sv->paused && !sv->queue.empty()) {
-        Req* r = sv->queue.front();
-        if (r->type == kAssemble && !take.empty()) break;
+    // With a cap on a batch's work, a request above a quarter of the cap is
+    // "large": it runs in a batch of its own, and small requests queued behind
+    // it (or behind an assembly) go ahead into the next batch instead of
+    // waiting for it (every request of a batch completes with the whole batch).
+    // The queue's head always goes into the batch, so nothing waits forever.
+    const int64_t large = sv->max_batch_pairs > 0 ? sv->max_batch_pairs / 4 : INT64_MAX;
+    for (auto it = sv->queue.begin(); !sv->paused && it != sv->queue.end();) {
+        Req* r = *it;
+        const bool alone = r->type == kAssemble || r->pairs > large;
+        if (alone && !take.empty()) {
+            if (sv->max_batch_pairs > 0) {
+                ++it;  // it waits for the next idle slot; smaller requests behind it go on
+                continue;
+            }
+            break;  // no cap: arrival order
+        }
         // a batch's length bounds the latency of every request in it: past the
         // cap, the rest waits for the next idle slot (an empty batch takes any one)
         if (sv->max_batch_pairs > 0 && !take.empty() && work + r->pairs > sv->max_batch_pairs) break;
         const bool fits = sv->reserved + r->bytes <= sv->budget;
-        if (!fits && !(sv->reserved == 0 && take.empty())) break;  // head of line waits for memory
-        sv->queue.pop_front();
+        if (!fits && !(sv->reserved == 0 && take.empty())) break;  // the first in line waits for memory
+        it = sv->queue.erase(it);
         sv->reserved += r->bytes;
         r->state = kRunning;
         work += r->pairs;
         take.push_back(r);
-        if (r->type == kAssemble || (int)take.size() >= sv->max_batch) break;
+        if (alone || (int)take.size() >= sv->max_batch) break;
     }
     if (!take.empty()) {
         sv->peak_reserved = std::max(sv->peak_reserved, sv->reserved);

@@ -593,8 +593,11 @@ int bielcc_server_set_preemptible(bielcc_server sv, int on);
 int bielcc_server_set_max_batch(bielcc_server sv, int max_batch);
 /* Most (point, cell, RHS) pairs one batch admits (0 = no cap, the default):
  * a batch's length bounds the latency of every request in it, so a cap keeps
- * large requests from lengthening the batches of small ones; a request larger
- * than the cap runs in a batch of its own. */
+ * large requests from lengthening the batches of small ones. With a cap, a
+ * request above a quarter of it (and every assembly request) runs in a batch
+ * of its own, and smaller field requests queued behind it are admitted past
+ * it into other slots' batches; the queue's first request always goes into
+ * the next batch. Without a cap, requests are admitted in arrival order. */
 int bielcc_server_set_max_batch_pairs(bielcc_server sv, int64_t pairs);
 /* paused = 1: queue requests without admitting any (running batches finish);
  * 0: resume. Lets a caller release a burst of requests as one batch. */

@@ -102,6 +102,34 @@ def test_server_small_requests_overtake_a_large_batch(gctx):
         sv.close()
 
 
+def test_server_cap_runs_a_large_request_alone(gctx):
+    """With a cap on a batch's pairs, a request above a quarter of the cap runs
+    in a batch of its own, and the small requests queued behind it go ahead
+    together on the other slot; each result is the same as alone."""
+    big_cells = W.uv_sphere(64, 128)
+    big = dict(mesh=gctx.mesh(big_cells), J=W.po_currents(big_cells, 2 * np.pi), k=2 * np.pi, mult=1.0,
+               pts=W.shell_points(20000, 2.0, 5.0, np.random.default_rng(0)))
+    small = _specs(gctx, 4)
+    sv = gpu.Server(gctx, n_slots=2, precision="mixed", max_batch_pairs=2 * 10**8)  # "large": > 5e7 pairs
+    try:
+        alone = [sv.wait(_submit(sv, sp))[2] for sp in small]
+        s0 = sv.stats()
+        sv.pause(True)
+        tb = _submit(sv, big)  # 1.6e8 pairs, first in line
+        ts = [_submit(sv, sp) for sp in small]
+        sv.pause(False)
+        res = [sv.wait(t) for t in ts]
+        st, lat_big, _ = sv.wait(tb)
+        assert st == 0 and all(r[0] == 0 for r in res)
+        for (_, _, out), a in zip(res, alone):
+            assert np.array_equal(out["E"], a["E"]) and np.array_equal(out["H"], a["H"])
+        s = sv.stats()
+        assert s["batches"] - s0["batches"] == 2 and s["max_batch"] == len(small)
+        assert max(r[1] for r in res) < lat_big
+    finally:
+        sv.close()
+
+
 def test_server_assembly_and_resident_currents(gctx):
     torch = pytest.importorskip("torch")
     specs = _specs(gctx, 4)
