@@ -51,7 +51,12 @@ constexpr int kBW = 4;    // warps
 #define BIELCC_BATCH_MINB 3
 #endif
 // Mixed form: phase A two cells per warp at a time (TWO = 1) or one; RHS per
-// thread in phase B (R; SP a multiple of 4 R).
+// thread in phase B (R; SP a multiple of 4 R). Measured on the 256-mesh batch
+// (cells / SP / CTAs per SM / TWO / R): 16 / 16 / 3 / 1 / 4 (164 registers)
+// 659 ms; 16 / 16 / 3 / 0 / 4 707 ms; 12 / 8 / 4 / 0 / 2 (128 registers)
+// 705 ms; 8 / 8 / 4 / 1 / 2 734 ms; 8 / 8 / 5 / 0 / 2 (96 registers, 20 warps
+// per SM) 865 ms: the two-cell node loop's second dependency chain is worth
+// more than extra warps.
 #ifndef BIELCC_BATCH_TWO
 #define BIELCC_BATCH_TWO 1
 #endif
