@@ -75,6 +75,8 @@ def parse():
                     help="largest mesh an assembly request draws (the config-5 mesh range)")
     ap.add_argument("--serve-asm-host-cells", type=int, default=2000,
                     help="assemblies of larger meshes write a caller-owned device matrix instead of host memory")
+    ap.add_argument("--serve-trace", default=None,
+                    help="write the served batches (bielcc_server_trace) and every request's latency to this JSON file")
     ap.add_argument("--serve-p99-target-ms", type=float, default=1000.0,
                     help="stated p99 latency objective of the serving stream")
     return ap.parse_args()
@@ -603,6 +605,12 @@ def run_serving(args, ctx, torch, dev, stream, item_cost):
             ready.release()
         th.join()
     st = sv.stats()
+    if args.serve_trace:
+        with open(args.serve_trace, "w") as fh:
+            json.dump({"batches": sv.trace(), "rate_per_s": rate,
+                       "requests": [{"request": i, "type": r["type"], "mesh": r["mesh"], "P": r.get("P"),
+                                     "S": r.get("S"), "arrival_s": r["t"] / rate, "latency_ms": res[i][1]}
+                                    for i, r in enumerate(reqs)]}, fh)
     sv.close()
     lat_f = [res[i][1] for i, r in enumerate(reqs) if r["type"] == "field"]
     lat_a = [res[i][1] for i, r in enumerate(reqs) if r["type"] == "assemble"]

@@ -250,6 +250,26 @@ class ServerStats(C.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_}
 
 
+class BatchTrace(C.Structure):
+    """bielcc_batch_trace: one served batch (times in ms from the first submission)."""
+    _fields_ = [
+        ("slot", C.c_int32),
+        ("n_requests", C.c_int32),
+        ("assembly", C.c_int32),
+        ("high_priority", C.c_int32),
+        ("pairs", C.c_int64),
+        ("first_ticket", C.c_int64),
+        ("admit_ms", C.c_double),
+        ("stage1_ms", C.c_double),
+        ("done_ms", C.c_double),
+        ("complete_ms", C.c_double),
+        ("oldest_wait_ms", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 class Stats(C.Structure):
     _fields_ = [
         ("kernel_launches", C.c_int64),

@@ -232,7 +232,10 @@ struct bielcc_server_s {
     double st_alloc = 0, st_copy = 0, st_plan = 0, st_launch = 0;  // parts of stage_in_s
     Clock::time_point t_first, t_last;
     bool any = false;
+    std::deque<bielcc_batch_trace> trace;  // the last kTraceCap batches
 };
+
+constexpr size_t kTraceCap = 4096;
 
 namespace {
 
@@ -626,6 +629,8 @@ bool admissible_locked(bielcc_server_s* sv) {
 void slot_loop(bielcc_server_s* sv, Slot* slp) {
     Slot& sl = *slp;
     cudaSetDevice(sv->device);
+    bielcc_batch_trace tr{};
+    Clock::time_point t_admit, t_stage1, t_done;
     for (;;) {
         std::vector<Req*> take;
         {
@@ -643,6 +648,18 @@ void slot_loop(bielcc_server_s* sv, Slot* slp) {
                 if (&o != &sl && o.state != kIdle && o.work > sl.work) overtake = true;
             sl.s = overtake ? sl.s_hi : sl.s_lo;
             if (overtake) sv->priority_batches++;
+            tr = bielcc_batch_trace{};
+            tr.slot = (int32_t)(slp - sv->slot_mem.get());
+            tr.n_requests = (int32_t)take.size();
+            tr.assembly = take[0]->type == kAssemble ? 1 : 0;
+            tr.high_priority = overtake ? 1 : 0;
+            tr.pairs = sl.work;
+            tr.first_ticket = take[0]->ticket;
+            t_admit = Clock::now();
+            for (const Req* r : take) {
+                const double w = std::chrono::duration<double, std::milli>(t_admit - r->t_submit).count();
+                tr.oldest_wait_ms = std::max(tr.oldest_wait_ms, w);
+            }
         }
         const auto t_in = Clock::now();
         cudaError_t e = take[0]->type == kField ? start_field_batch(sv, sl) : start_assemble(sv, sl);
@@ -653,6 +670,7 @@ void slot_loop(bielcc_server_s* sv, Slot* slp) {
             sv->stage_in_s += in_s;
         }
         if (e == cudaSuccess) e = cudaEventSynchronize(sl.ev_stage1);
+        t_stage1 = Clock::now();
         if (e == cudaSuccess && take[0]->type == kField &&
             (batch_timed_out(sl.h_total) || (sl.samp_on && batch_timed_out(sl.h_total + 4))))
             e = cudaErrorTimeout;  // a bounded wait in the far kernel ran out: the batch fails
@@ -667,6 +685,7 @@ void slot_loop(bielcc_server_s* sv, Slot* slp) {
             e = finish_batch(sv, sl, n_near, pb);
         }
         if (e == cudaSuccess) e = cudaEventSynchronize(sl.ev_done);
+        t_done = Clock::now();
         if (e == cudaSuccess) {
             float b = 0.f, t = 0.f;
             if (cudaEventElapsedTime(&b, sv->ev_ref, sl.ev_begin) == cudaSuccess &&
@@ -677,6 +696,17 @@ void slot_loop(bielcc_server_s* sv, Slot* slp) {
             cudaGetLastError();
             sl.state = kCompleting;
             complete_slot(sv, sl);
+            const auto t_complete = Clock::now();
+            std::lock_guard<std::mutex> g(sv->mu);
+            auto ms = [&](Clock::time_point t) {
+                return std::chrono::duration<double, std::milli>(t - sv->t_first).count();
+            };
+            tr.admit_ms = ms(t_admit);
+            tr.stage1_ms = ms(t_stage1);
+            tr.done_ms = ms(t_done);
+            tr.complete_ms = ms(t_complete);
+            if (sv->trace.size() >= kTraceCap) sv->trace.pop_front();
+            sv->trace.push_back(tr);
         } else {
             cudaGetLastError();
             cudaStreamSynchronize(sl.s);  // nothing of this batch may still write the pinned block
@@ -1053,9 +1083,19 @@ int bielcc_server_get_stats(bielcc_server sv, bielcc_server_stats* st, int reset
         sv->stage_in_s = sv->copy_out_s = 0;
         sv->st_alloc = sv->st_copy = sv->st_plan = sv->st_launch = 0;
         sv->spans.clear();
+        sv->trace.clear();
         sv->peak_reserved = sv->reserved;
         sv->any = false;
     }
+    return BIELCC_OK;
+}
+
+int bielcc_server_trace(bielcc_server sv, bielcc_batch_trace* out, int capacity, int* n_out) {
+    if (!sv || !n_out || capacity < 0 || (capacity > 0 && !out)) return set_api_error(BIELCC_ERR_ARG, "bad argument");
+    std::lock_guard<std::mutex> g(sv->mu);
+    const int n = std::min<int>(capacity, (int)sv->trace.size());
+    for (int i = 0; i < n; i++) out[i] = sv->trace[i];
+    *n_out = n;
     return BIELCC_OK;
 }
 

@@ -99,6 +99,7 @@ def load(path=LIB_PATH):
     d("bielcc_server_pause", [vp, C.c_int])
     d("bielcc_server_drain", [vp, C.c_double])
     d("bielcc_server_set_max_batch_pairs", [vp, C.c_int64])
+    d("bielcc_server_trace", [vp, C.POINTER(abi.BatchTrace), C.c_int, C.POINTER(C.c_int)])
     d("bielcc_server_get_stats", [vp, C.POINTER(abi.ServerStats), C.c_int])
     abi.declare_common(L, "bielcc_")
     if L.bielcc_abi_version() != abi.ABI_VERSION:
@@ -672,6 +673,13 @@ class Server:
 
     def drain(self, timeout=600.0):
         _check(_lib.bielcc_server_drain(self.h, float(timeout)))
+
+    def trace(self, capacity=4096):
+        """The last batches served (bielcc_server_trace), oldest first, as dicts."""
+        buf = (abi.BatchTrace * capacity)()
+        n = C.c_int(0)
+        _check(_lib.bielcc_server_trace(self.h, buf, capacity, C.byref(n)))
+        return [buf[i].as_dict() for i in range(n.value)]
 
     def stats(self, reset=False):
         st = abi.ServerStats()

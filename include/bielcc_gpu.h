@@ -619,6 +619,23 @@ int bielcc_server_cancel(bielcc_server sv, int64_t ticket);
 /* Blocks (at most timeout_s) until nothing is queued or running. */
 int bielcc_server_drain(bielcc_server sv, double timeout_s);
 int bielcc_server_get_stats(bielcc_server sv, bielcc_server_stats* out, int reset);
+/* Trace of the last batches the server ran (up to 4096, oldest first; reset
+ * with the statistics). Times are ms from the first submission since the
+ * last reset: when a slot admitted the batch, when its stage 1 (far kernel,
+ * near-pair count) and stage 2 had completed on the GPU, and when its results
+ * were in the callers' buffers. No counterpart in the reference. */
+typedef struct bielcc_batch_trace {
+    int32_t slot;
+    int32_t n_requests;
+    int32_t assembly;       /* 1: an assembly request */
+    int32_t high_priority;  /* launched on the slot's high-priority stream */
+    int64_t pairs;          /* (point, cell, RHS) pairs; N^2 for an assembly */
+    int64_t first_ticket;
+    double admit_ms, stage1_ms, done_ms, complete_ms;
+    double oldest_wait_ms;  /* longest time one of its requests had queued when the batch was admitted */
+} bielcc_batch_trace;
+/* Copies at most `capacity` records into out; *n_out = the number copied. */
+int bielcc_server_trace(bielcc_server sv, bielcc_batch_trace* out, int capacity, int* n_out);
 
 /* ---- solving the collocation system ------------------------------------
  * No counterpart in the reference (it assembles operators but has no solver).

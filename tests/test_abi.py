@@ -46,11 +46,13 @@ def test_ctypes_layouts_match_header():
     #include <stddef.h>
     #include "bielcc_gpu.h"
     int main(void) {
-      printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(bielcc_numparam), sizeof(bielcc_planewave),
+      printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(bielcc_numparam),
+             sizeof(bielcc_planewave),
              sizeof(bielcc_kernelparam), sizeof(bielcc_report), offsetof(bielcc_report, est_rel_l2),
              offsetof(bielcc_kernelparam, current), sizeof(bielcc_field_job), sizeof(bielcc_field_request),
              offsetof(bielcc_field_request, inc), sizeof(bielcc_assemble_request), sizeof(bielcc_server_stats),
-             offsetof(bielcc_server_stats, p50_ms));
+             offsetof(bielcc_server_stats, p50_ms), sizeof(bielcc_batch_trace), offsetof(bielcc_batch_trace, admit_ms),
+             sizeof(bielcc_stats));
       return 0; }
     '''
     with tempfile.TemporaryDirectory() as d:
@@ -62,7 +64,8 @@ def test_ctypes_layouts_match_header():
     assert sizes == [C.sizeof(abi.NumParam), C.sizeof(abi.PlaneWave), C.sizeof(abi.KernelParam),
                      C.sizeof(abi.Report), abi.Report.est_rel_l2.offset, abi.KernelParam.current.offset,
                      C.sizeof(abi.FieldJob), C.sizeof(abi.FieldRequest), abi.FieldRequest.inc.offset,
-                     C.sizeof(abi.AssembleRequest), C.sizeof(abi.ServerStats), abi.ServerStats.p50_ms.offset]
+                     C.sizeof(abi.AssembleRequest), C.sizeof(abi.ServerStats), abi.ServerStats.p50_ms.offset,
+                     C.sizeof(abi.BatchTrace), abi.BatchTrace.admit_ms.offset, C.sizeof(abi.Stats)]
 
 
 def test_no_device_fails_loudly():

@@ -126,6 +126,14 @@ def test_server_cap_runs_a_large_request_alone(gctx):
         s = sv.stats()
         assert s["batches"] - s0["batches"] == 2 and s["max_batch"] == len(small)
         assert max(r[1] for r in res) < lat_big
+        # the server's batch trace: the last two batches are the large request alone and the small ones
+        tr = sv.trace()[-2:]
+        assert sorted(b["n_requests"] for b in tr) == [1, len(small)]
+        assert {b["slot"] for b in tr} == {0, 1}
+        for b in tr:
+            assert 0 <= b["admit_ms"] <= b["stage1_ms"] <= b["done_ms"] <= b["complete_ms"]
+        big_b = next(b for b in tr if b["n_requests"] == 1)
+        assert big_b["pairs"] == len(big["pts"]) * len(big_cells) and big_b["assembly"] == 0
     finally:
         sv.close()
 
