@@ -221,6 +221,7 @@ struct bielcc_server_s {
     int64_t max_batch_pairs = 0;  // 0: no cap on a batch's (point, cell, RHS) pairs
     bool paused = false;
     bool preemptible = true;
+    bool overtake = true;  // a batch smaller than a running one goes to the high-priority stream
     cudaEvent_t ev_ref = nullptr;              // time origin of the batch spans
     std::vector<std::pair<double, double>> spans;  // [begin, end] ms of every batch on the GPU
     double item_cost = 4.0e6;
@@ -645,7 +646,7 @@ void slot_loop(bielcc_server_s* sv, Slot* slp) {
             for (const Req* r : take) sl.work += r->pairs;
             bool overtake = false;
             for (const Slot& o : slots_of(sv))
-                if (&o != &sl && o.state != kIdle && o.work > sl.work) overtake = true;
+                if (sv->overtake && &o != &sl && o.state != kIdle && o.work > sl.work) overtake = true;
             sl.s = overtake ? sl.s_hi : sl.s_lo;
             if (overtake) sv->priority_batches++;
             tr = bielcc_batch_trace{};
@@ -888,6 +889,13 @@ int bielcc_server_set_preemptible(bielcc_server sv, int on) {
     if (!sv) return set_api_error(BIELCC_ERR_ARG, "null argument");
     std::lock_guard<std::mutex> g(sv->mu);
     sv->preemptible = on != 0;
+    return BIELCC_OK;
+}
+
+int bielcc_server_set_overtake(bielcc_server sv, int on) {
+    if (!sv) return set_api_error(BIELCC_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> g(sv->mu);
+    sv->overtake = on != 0;
     return BIELCC_OK;
 }
 

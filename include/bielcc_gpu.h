@@ -589,6 +589,11 @@ int bielcc_server_reserve(bielcc_server sv, int64_t device_bytes, int64_t pinned
  * item and retires, so a batch on a higher-priority stream gets SMs at once;
  * 0: persistent CTAs (no overtaking inside a running batch). */
 int bielcc_server_set_preemptible(bielcc_server sv, int on);
+/* on = 1 (default): a batch smaller (in pairs) than one running on another
+ * slot is launched on its slot's high-priority stream and overtakes it;
+ * 0: every batch on the same priority, so the GPU serves the batches' CTAs in
+ * launch order. */
+int bielcc_server_set_overtake(bielcc_server sv, int on);
 /* Most requests one batch admits (default 64). */
 int bielcc_server_set_max_batch(bielcc_server sv, int max_batch);
 /* Most (point, cell, RHS) pairs one batch admits (0 = no cap, the default):
