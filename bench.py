@@ -75,8 +75,9 @@ def parse():
                     help="largest mesh an assembly request draws (the config-5 mesh range)")
     ap.add_argument("--serve-asm-host-cells", type=int, default=2000,
                     help="assemblies of larger meshes write a caller-owned device matrix instead of host memory")
-    ap.add_argument("--serve-fifo", action="store_true",
-                    help="no overtaking: every served batch at one stream priority (bielcc_server_set_overtake(sv, 0))")
+    ap.add_argument("--serve-overtake", action="store_true",
+                    help="smaller batches overtake larger running ones on a high-priority stream "
+                         "(bielcc_server_set_overtake(sv, 1)); default: every served batch at one priority")
     ap.add_argument("--serve-trace", default=None,
                     help="write the served batches (bielcc_server_trace) and every request's latency to this JSON file")
     ap.add_argument("--serve-p99-target-ms", type=float, default=1000.0,
@@ -562,7 +563,7 @@ def run_serving(args, ctx, torch, dev, stream, item_cost):
     sv = gpu.Server(ctx, n_slots=args.serve_slots, precision="mixed", item_cost=item_cost,
                     preemptible=not args.serve_persistent, max_batch=args.serve_max_batch,
                     reserve=(args.serve_reserve_gb << 30, 4 << 30),
-                    max_batch_pairs=int(args.serve_max_batch_pairs) or None, overtake=not args.serve_fifo)
+                    max_batch_pairs=int(args.serve_max_batch_pairs) or None, overtake=args.serve_overtake)
 
     def submit_asm(i, r):
         if r["mesh"] in asm_dev:
@@ -679,7 +680,7 @@ def run_serving(args, ctx, torch, dev, stream, item_cost):
         "failed": bad, "sampled_identical_to_offline": f"{same}/{len(ref)}",
         "sampled_mismatch": {"requests": bad_idx, "max_diff_over_max": worst},
         "unit": "(point, cell, RHS) pairs/s", "clocks": clk.summary(), "slo": slo,
-        "max_batch_pairs": args.serve_max_batch_pairs, "overtake": not args.serve_fifo,
+        "max_batch_pairs": args.serve_max_batch_pairs, "overtake": args.serve_overtake,
         "assembly_meshes": {"max_cells": args.serve_asm_max_cells, "device_output_above_cells":
                             args.serve_asm_host_cells, "largest_assembled": max([mh_n for mh_n in
                             [len(meshes[r["mesh"]]["cells"]) for r in asm]] or [0])},
