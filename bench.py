@@ -78,6 +78,8 @@ def parse():
     ap.add_argument("--serve-overtake", action="store_true",
                     help="smaller batches overtake larger running ones on a high-priority stream "
                          "(bielcc_server_set_overtake(sv, 1)); default: every served batch at one priority")
+    ap.add_argument("--serve-priority-pairs", type=float, default=0.0,
+                    help="served batches of at most this many pairs run at high priority (0: none)")
     ap.add_argument("--serve-trace", default=None,
                     help="write the served batches (bielcc_server_trace) and every request's latency to this JSON file")
     ap.add_argument("--serve-p99-target-ms", type=float, default=1000.0,
@@ -563,7 +565,8 @@ def run_serving(args, ctx, torch, dev, stream, item_cost):
     sv = gpu.Server(ctx, n_slots=args.serve_slots, precision="mixed", item_cost=item_cost,
                     preemptible=not args.serve_persistent, max_batch=args.serve_max_batch,
                     reserve=(args.serve_reserve_gb << 30, 4 << 30),
-                    max_batch_pairs=int(args.serve_max_batch_pairs) or None, overtake=args.serve_overtake)
+                    max_batch_pairs=int(args.serve_max_batch_pairs) or None, overtake=args.serve_overtake,
+                    priority_pairs=int(args.serve_priority_pairs))
 
     def submit_asm(i, r):
         if r["mesh"] in asm_dev:
@@ -681,6 +684,7 @@ def run_serving(args, ctx, torch, dev, stream, item_cost):
         "sampled_mismatch": {"requests": bad_idx, "max_diff_over_max": worst},
         "unit": "(point, cell, RHS) pairs/s", "clocks": clk.summary(), "slo": slo,
         "max_batch_pairs": args.serve_max_batch_pairs, "overtake": args.serve_overtake,
+        "priority_pairs": args.serve_priority_pairs,
         "assembly_meshes": {"max_cells": args.serve_asm_max_cells, "device_output_above_cells":
                             args.serve_asm_host_cells, "largest_assembled": max([mh_n for mh_n in
                             [len(meshes[r["mesh"]]["cells"]) for r in asm]] or [0])},

@@ -222,6 +222,7 @@ struct bielcc_server_s {
     bool paused = false;
     bool preemptible = true;
     bool overtake = true;  // a batch smaller than a running one goes to the high-priority stream
+    int64_t priority_pairs = 0;  // a batch of at most this many pairs goes to the high-priority stream (0: off)
     cudaEvent_t ev_ref = nullptr;              // time origin of the batch spans
     std::vector<std::pair<double, double>> spans;  // [begin, end] ms of every batch on the GPU
     double item_cost = 4.0e6;
@@ -644,7 +645,7 @@ void slot_loop(bielcc_server_s* sv, Slot* slp) {
             sl.state = kStage1;
             sl.work = 0;
             for (const Req* r : take) sl.work += r->pairs;
-            bool overtake = false;
+            bool overtake = sv->priority_pairs > 0 && sl.work <= sv->priority_pairs;
             for (const Slot& o : slots_of(sv))
                 if (sv->overtake && &o != &sl && o.state != kIdle && o.work > sl.work) overtake = true;
             sl.s = overtake ? sl.s_hi : sl.s_lo;
@@ -896,6 +897,13 @@ int bielcc_server_set_overtake(bielcc_server sv, int on) {
     if (!sv) return set_api_error(BIELCC_ERR_ARG, "null argument");
     std::lock_guard<std::mutex> g(sv->mu);
     sv->overtake = on != 0;
+    return BIELCC_OK;
+}
+
+int bielcc_server_set_priority_pairs(bielcc_server sv, int64_t pairs) {
+    if (!sv || pairs < 0) return set_api_error(BIELCC_ERR_ARG, "bad argument");
+    std::lock_guard<std::mutex> g(sv->mu);
+    sv->priority_pairs = pairs;
     return BIELCC_OK;
 }
 

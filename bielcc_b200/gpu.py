@@ -101,6 +101,7 @@ def load(path=LIB_PATH):
     d("bielcc_server_set_max_batch_pairs", [vp, C.c_int64])
     d("bielcc_server_trace", [vp, C.POINTER(abi.BatchTrace), C.c_int, C.POINTER(C.c_int)])
     d("bielcc_server_set_overtake", [vp, C.c_int])
+    d("bielcc_server_set_priority_pairs", [vp, C.c_int64])
     d("bielcc_server_get_stats", [vp, C.POINTER(abi.ServerStats), C.c_int])
     abi.declare_common(L, "bielcc_")
     if L.bielcc_abi_version() != abi.ABI_VERSION:
@@ -567,7 +568,8 @@ class Server:
     (status, latency_ms, outputs) once the request finished."""
 
     def __init__(self, ctx, hbm_budget=0, n_slots=2, numparam=None, precision="mixed", max_batch=None,
-                 item_cost=None, preemptible=True, reserve=None, max_batch_pairs=None, overtake=True):
+                 item_cost=None, preemptible=True, reserve=None, max_batch_pairs=None, overtake=True,
+                 priority_pairs=None):
         self.ctx = ctx
         np_ = numparam if numparam is not None else abi.NumParam.default()
         h = C.c_void_p()
@@ -583,6 +585,8 @@ class Server:
             _check(_lib.bielcc_server_set_item_cost(self.h, float(item_cost)))
         _check(_lib.bielcc_server_set_preemptible(self.h, int(bool(preemptible))))
         _check(_lib.bielcc_server_set_overtake(self.h, int(bool(overtake))))
+        if priority_pairs is not None:
+            _check(_lib.bielcc_server_set_priority_pairs(self.h, int(priority_pairs)))
         if reserve is not None:
             _check(_lib.bielcc_server_reserve(self.h, int(reserve[0]), int(reserve[1])))
 

@@ -594,6 +594,10 @@ int bielcc_server_set_preemptible(bielcc_server sv, int on);
  * 0: every batch on the same priority, so the GPU serves the batches' CTAs in
  * launch order. */
 int bielcc_server_set_overtake(bielcc_server sv, int on);
+/* A batch of at most `pairs` (point, cell, RHS) pairs (N^2 for an assembly)
+ * runs on its slot's high-priority stream whatever the overtake setting, so
+ * small requests get SMs within one work item's time (0 = off, the default). */
+int bielcc_server_set_priority_pairs(bielcc_server sv, int64_t pairs);
 /* Most requests one batch admits (default 64). */
 int bielcc_server_set_max_batch(bielcc_server sv, int max_batch);
 /* Most (point, cell, RHS) pairs one batch admits (0 = no cap, the default):
