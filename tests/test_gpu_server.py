@@ -138,6 +138,28 @@ def test_server_cap_runs_a_large_request_alone(gctx):
         sv.close()
 
 
+def test_server_priority_settings(gctx):
+    """Without overtaking, no batch takes the high-priority stream unless it is
+    within the priority threshold; results do not depend on the stream."""
+    specs = _specs(gctx, 5)
+    outs = {}
+    for overtake, prio in ((False, 0), (False, 10**9), (True, 0)):
+        sv = gpu.Server(gctx, n_slots=2, precision="mixed", overtake=overtake, priority_pairs=prio)
+        try:
+            res = [sv.wait(_submit(sv, sp)) for sp in specs]
+            assert all(r[0] == 0 for r in res)
+            s = sv.stats()
+            if not overtake:
+                assert s["priority_batches"] == (s["batches"] if prio else 0)
+            outs[(overtake, prio)] = [r[2] for r in res]
+        finally:
+            sv.close()
+    ref = outs[(False, 0)]
+    for k, v in outs.items():
+        for a, b in zip(v, ref):
+            assert np.array_equal(a["E"], b["E"]) and np.array_equal(a["H"], b["H"]), k
+
+
 def test_server_assembly_and_resident_currents(gctx):
     torch = pytest.importorskip("torch")
     specs = _specs(gctx, 4)
