@@ -35,7 +35,7 @@ extern "C" {
 #pragma GCC visibility push(default)
 #endif
 
-#define BIELCC_ABI_VERSION 2
+#define BIELCC_ABI_VERSION 3
 
 /* ---- status codes ---------------------------------------------------- */
 #define BIELCC_OK                 0
