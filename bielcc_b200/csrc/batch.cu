@@ -307,6 +307,89 @@ BIELCC_D void batch_moments2(const float4* ndA, const float* yyA, const float4* 
     store_moments<CK, float>(mb, PBr, PBi, dB, momB);
 }
 
+// Phase B of one chunk: the right-hand sides s0 + sb + warp + 4 j (j < R) of the
+// sp staged in s_j, contracted with the chunk's moments (s_mom[cc][20][32])
+// and added into the job's partial sums (stored by the item's first chunk).
+template <bool MIXED>
+BIELCC_D void batch_phase_b(const typename BatchCfg<MIXED>::F* s_mom, const typename BatchCfg<MIXED>::F* s_j, int nc,
+                            int s0, int sp, int warp, int lane, bool live, const JobDev& jb, int range, int S, int P,
+                            int p, bool first) {
+    using C = BatchCfg<MIXED>;
+    using F = typename C::F;
+    for (int sb = 0; sb < sp; sb += kBW * C::R) {
+        F acc[C::R][12];
+#pragma unroll
+        for (int j = 0; j < C::R; j++)
+#pragma unroll
+            for (int q = 0; q < 12; q++) acc[j][q] = 0;
+        for (int cc = 0; cc < nc; cc++) {
+            F m[20];
+#pragma unroll
+            for (int q = 0; q < 20; q++) m[q] = s_mom[(cc * 20 + q) * kBP + lane];
+            // A1 I + T: A1 onto the diagonal t_xx, t_yy, t_zz
+            m[2] += m[0];
+            m[3] += m[1];
+            m[8] += m[0];
+            m[9] += m[1];
+            m[12] += m[0];
+            m[13] += m[1];
+            if constexpr (MIXED) {
+                contract_packed_cell<C::R>(m, reinterpret_cast<const float4*>(s_j) + (size_t)cc * kSP * 3, sb + warp,
+                                           kBW, sp, acc);
+            } else {
+#pragma unroll
+                for (int j = 0; j < C::R; j++) {
+                    const int sl = sb + warp + kBW * j;
+                    if (sl < sp) {
+                        const F* jj = s_j + (size_t)(cc * kSP + sl) * 6;
+                        const F jr[3] = {jj[0], jj[2], jj[4]}, ji[3] = {jj[1], jj[3], jj[5]};
+                        contract12<F>(m, jr, ji, acc[j]);
+                    }
+                }
+            }
+        }
+        if (live) {
+#pragma unroll
+            for (int j = 0; j < C::R; j++) {
+                const int sl = sb + warp + kBW * j;
+                if (sl >= sp) continue;
+                double* dst = jb.partial + (((size_t)range * S + (s0 + sl)) * 12) * (size_t)P + p;
+                // one writer per address (this thread), so the adds land in chunk
+                // order: the fire-and-forget reduction (no load to wait for) gives
+                // the same sums as a load-add-store
+                if (first) {
+#pragma unroll
+                    for (int q = 0; q < 12; q++) dst[(size_t)q * P] = (double)acc[j][q];
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 12; q++) atomicAdd(dst + (size_t)q * P, (double)acc[j][q]);
+                }
+            }
+        }
+    }
+}
+
+// Stages the currents of RHS s0 .. s0 + sp - 1 of cells c0 .. c0 + nc - 1
+// (FP32 (re, im, im, re) for the packed contraction; FP64 (re, im)).
+template <bool MIXED>
+BIELCC_D void batch_stage_j(typename BatchCfg<MIXED>::F* s_j, const JobDev& jb, int c0, int nc, int s0, int sp,
+                            int tid) {
+    using C = BatchCfg<MIXED>;
+    using F = typename C::F;
+    const int N = jb.n_cells;
+    for (int i = tid; i < nc * sp * 3; i += kBT) {
+        const int cc = i / (sp * 3), rem = i - cc * sp * 3, sl = rem / 3, g = rem - sl * 3;
+        const cplx v = jb.J[((size_t)(s0 + sl) * N + (c0 + cc)) * 3 + g];
+        F* d = s_j + ((size_t)(cc * kSP + sl) * 3 + g) * C::JW;
+        d[0] = (F)v.re;
+        d[1] = (F)v.im;
+        if constexpr (MIXED) {
+            d[2] = (F)v.im;
+            d[3] = (F)v.re;
+        }
+    }
+}
+
 template <bool MIXED>
 __global__ void __launch_bounds__(kBT, MIXED ? BIELCC_BATCH_MINB : 2) batch_far_kernel(const JobDev* __restrict__ jobs,
                                                          const BatchItem* __restrict__ items, int n_items,
@@ -354,73 +437,9 @@ __global__ void __launch_bounds__(kBT, MIXED ? BIELCC_BATCH_MINB : 2) batch_far_
             // phase B: RHS s0 + sb + warp + 4 j (j < R) of the sp staged in s_j, contracted over
             // the chunk's cells and added into the job's partial sums
             auto phase_b = [&](int s0, int sp) {
-                for (int sb = 0; sb < sp; sb += kBW * C::R) {
-                    F acc[C::R][12];
-#pragma unroll
-                    for (int j = 0; j < C::R; j++)
-#pragma unroll
-                        for (int q = 0; q < 12; q++) acc[j][q] = 0;
-                    for (int cc = 0; cc < nc; cc++) {
-                        F m[20];
-#pragma unroll
-                        for (int q = 0; q < 20; q++) m[q] = s_mom[(cc * 20 + q) * kBP + lane];
-                        // A1 I + T: A1 onto the diagonal t_xx, t_yy, t_zz
-                        m[2] += m[0];
-                        m[3] += m[1];
-                        m[8] += m[0];
-                        m[9] += m[1];
-                        m[12] += m[0];
-                        m[13] += m[1];
-                        if constexpr (MIXED) {
-                            contract_packed_cell<C::R>(m, reinterpret_cast<const float4*>(s_j) + (size_t)cc * kSP * 3,
-                                                       sb + warp, kBW, sp, acc);
-                        } else {
-#pragma unroll
-                            for (int j = 0; j < C::R; j++) {
-                                const int sl = sb + warp + kBW * j;
-                                if (sl < sp) {
-                                    const F* jj = s_j + (size_t)(cc * kSP + sl) * 6;
-                                    const F jr[3] = {jj[0], jj[2], jj[4]}, ji[3] = {jj[1], jj[3], jj[5]};
-                                    contract12<F>(m, jr, ji, acc[j]);
-                                }
-                            }
-                        }
-                    }
-                    if (live) {
-#pragma unroll
-                        for (int j = 0; j < C::R; j++) {
-                            const int sl = sb + warp + kBW * j;
-                            if (sl >= sp) continue;
-                            double* dst =
-                                jb.partial + (((size_t)bi.range * S + (s0 + sl)) * 12) * (size_t)P + p;
-                            // one writer per address (this thread), so the adds land in chunk
-                            // order: the fire-and-forget reduction (no load to wait for) gives
-                            // the same sums as a load-add-store
-                            if (c0 == cb) {
-#pragma unroll
-                                for (int q = 0; q < 12; q++) dst[(size_t)q * P] = (double)acc[j][q];
-                            } else {
-#pragma unroll
-                                for (int q = 0; q < 12; q++) atomicAdd(dst + (size_t)q * P, (double)acc[j][q]);
-                            }
-                        }
-                    }
-                }
+                batch_phase_b<MIXED>(s_mom, s_j, nc, s0, sp, warp, lane, live, jb, bi.range, S, P, p, c0 == cb);
             };
-            // stage the currents of RHS s0 .. s0 + sp - 1
-            auto stage_j = [&](int s0, int sp) {
-                for (int i = threadIdx.x; i < nc * sp * 3; i += kBT) {
-                    const int cc = i / (sp * 3), rem = i - cc * sp * 3, sl = rem / 3, g = rem - sl * 3;
-                    const cplx v = jb.J[((size_t)(s0 + sl) * N + (c0 + cc)) * 3 + g];
-                    F* d = s_j + ((size_t)(cc * kSP + sl) * 3 + g) * C::JW;
-                    d[0] = (F)v.re;
-                    d[1] = (F)v.im;
-                    if constexpr (MIXED) {
-                        d[2] = (F)v.im;
-                        d[3] = (F)v.re;
-                    }
-                }
-            };
+            auto stage_j = [&](int s0, int sp) { batch_stage_j<MIXED>(s_j, jb, c0, nc, s0, sp, threadIdx.x); };
             __syncthreads();
             // stage node tables, cell rows and the first RHS pass's currents
             if constexpr (MIXED) {
@@ -525,6 +544,187 @@ __global__ void __launch_bounds__(kBT, MIXED ? BIELCC_BATCH_MINB : 2) batch_far_
                 stage_j(s0, min(kSP, S - s0));
                 __syncthreads();
                 phase_b(s0, min(kSP, S - s0));
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- split pipeline (mixed form)
+// The same items as batch_far_kernel<true> in two kernels per wave of items:
+// batch_moments_kernel evaluates the moments of every (point, cell) pair of
+// an item and writes them to an HBM buffer laid out as the fused kernel's
+// shared-memory chunk (cell, moment, point); batch_contract_kernel reads them
+// back a 16-cell chunk at a time and runs phase B unchanged. The moments
+// kernel holds no phase-B state, so it runs at more resident warps; the cell
+// pairing of the two-cell node loop (cells c, c + 4 of each 8) and the 16-cell
+// FP32 summation boundaries are the fused kernel's, so the results are
+// bit-identical to it. Only for n_start <= 8.
+#ifndef BIELCC_MOM_MINB
+#define BIELCC_MOM_MINB 4
+#endif
+constexpr int kMomCells = 8;                     // cells per moments block
+constexpr int kMomBlock = kMomCells * 20 * kBP;  // floats per block
+
+__global__ void __launch_bounds__(kBT, BIELCC_MOM_MINB)
+    batch_moments_kernel(const JobDev* __restrict__ jobs, const BatchItem* __restrict__ items, int n_items,
+                         int* __restrict__ counter, double analytic_calc, int n_start, int max_items,
+                         float* __restrict__ mom) {
+    __shared__ __align__(16) float4 s_nodes[kMomCells * 64];
+    __shared__ float s_yy[kMomCells * 64];
+    __shared__ double4 s_cell[kMomCells];
+    __shared__ double s_rho[kMomCells];
+    __shared__ unsigned char s_near[kMomCells * kBP];
+    __shared__ int s_item;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nn = n_start * n_start;
+
+    for (int taken = 0; taken < max_items; taken++) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int it = s_item;
+        if (it >= n_items) break;
+        const BatchItem bi = items[it];
+        const JobDev& jb = jobs[bi.job];
+        const int P = jb.n_pts, N = jb.n_cells;
+        const int p = bi.tile * kBP + lane;
+        const bool live = p < P;
+        double x[3] = {0., 0., 0.};
+        if (live)
+            for (int g = 0; g < 3; g++) x[g] = jb.pts[3 * (size_t)p + g];
+        const int cb = bi.range * jb.cells_per_range;
+        const int ce = min(N, cb + jb.cells_per_range);
+        const cplx k = jb.k;
+        const double k2r = k.re * k.re - k.im * k.im, k2i = 2.0 * k.re * k.im;
+        const bool ck = k.im != 0.0;
+        float* mo = mom + (size_t)bi.pad * kMomBlock;  // the item's blocks, in cell order
+        unsigned nbits = 0;
+
+        for (int c0 = cb; c0 < ce; c0 += kMomCells) {
+            const int nc = min(kMomCells, ce - c0);
+            __syncthreads();  // the previous chunk's reads of the staged nodes are done
+            {
+                const float4* src = jb.nodes32 + (size_t)c0 * nn;
+                for (int i = threadIdx.x; i < nc * nn; i += kBT) {
+                    const float4 v = __ldg(src + i);
+                    s_nodes[i] = v;
+                    s_yy[i] = node_yy(v);
+                }
+                for (int i = threadIdx.x; i < nc; i += kBT) {
+                    const CellGeo& gg = jb.geo[c0 + i];
+                    s_cell[i] = make_double4(gg.c[0], gg.c[1], gg.c[2], gg.diam);
+                    s_rho[i] = (double)jb.rho32[c0 + i];
+                }
+            }
+            __syncthreads();
+            // cells warp and warp + 4 of the block, two at a time (batch_far_kernel's pairing)
+            for (int cc = warp; cc < nc; cc += 2 * kBW) {
+                const int cb2 = cc + kBW;
+                const bool two = cb2 < nc;
+                const double4 ca = s_cell[cc], cbb = s_cell[two ? cb2 : cc];
+                const double cena[3] = {ca.x, ca.y, ca.z}, cenb[3] = {cbb.x, cbb.y, cbb.z};
+                double da, db;
+                const bool na = is_near(x, cena, ca.w, analytic_calc, &da);
+                const bool nb = is_near(x, cenb, cbb.w, analytic_calc, &db);
+                const bool fa = !na && live, fb = two && !nb && live;
+                s_near[cc * kBP + lane] = na ? 1 : 0;
+                if (two) s_near[cb2 * kBP + lane] = nb ? 1 : 0;
+                float moa[20], mob[20];
+#pragma unroll
+                for (int q = 0; q < 20; q++) moa[q] = mob[q] = 0.f;
+                const float4 *nda = s_nodes + cc * nn, *ndb = s_nodes + (two ? cb2 : cc) * nn;
+                const float *ya = s_yy + cc * nn, *yb = s_yy + (two ? cb2 : cc) * nn;
+                if (fa && fb) {
+                    if (ck) batch_moments2<true>(nda, ya, ndb, yb, nn, x, ca, da, s_rho[cc], cbb, db, s_rho[cb2], k,
+                                                 moa, mob);
+                    else batch_moments2<false>(nda, ya, ndb, yb, nn, x, ca, da, s_rho[cc], cbb, db, s_rho[cb2], k,
+                                               moa, mob);
+                } else if (fa || fb) {
+                    const float4* nd = fa ? nda : ndb;
+                    const float* yy = fa ? ya : yb;
+                    const double4 ci = fa ? ca : cbb;
+                    const double d = fa ? da : db, rho = s_rho[fa ? cc : cb2];
+                    float* mo1 = fa ? moa : mob;
+                    if (ck) batch_moments<true, true>(nd, yy, nn, x, ci, d, rho, k, k2r, k2i, mo1);
+                    else batch_moments<true, false>(nd, yy, nn, x, ci, d, rho, k, k2r, k2i, mo1);
+                }
+                float* da_ = mo + (size_t)(c0 - cb + cc) * 20 * kBP + lane;
+#pragma unroll
+                for (int q = 0; q < 20; q++) da_[q * kBP] = moa[q];
+                if (two) {
+                    float* db_ = mo + (size_t)(c0 - cb + cb2) * 20 * kBP + lane;
+#pragma unroll
+                    for (int q = 0; q < 20; q++) db_[q * kBP] = mob[q];
+                }
+            }
+            __syncthreads();
+            // near-cell mask: warp 0 owns the words of its points
+            if (warp == 0) {
+                for (int cc = 0; cc < nc; cc++) {
+                    const int c = c0 + cc;
+                    nbits |= (unsigned)s_near[cc * kBP + lane] << (c & 31);
+                    if ((c & 31) == 31 || c == ce - 1) {
+                        if (live) jb.mask[(size_t)(c >> 5) * P + p] = nbits;
+                        nbits = 0;
+                    }
+                }
+            }
+        }
+    }
+}
+
+// Phase B of the split pipeline: per 16-cell chunk of an item, its moments
+// (written by batch_moments_kernel) and the currents are staged and
+// contracted exactly as in batch_far_kernel<true>.
+constexpr int kConCells = 16;
+constexpr size_t kConSmem = sizeof(float) * kConCells * 20 * kBP + sizeof(float) * 4 * kConCells * kSP * 3;
+#ifndef BIELCC_CON_MINB
+#define BIELCC_CON_MINB 4
+#endif
+
+__global__ void __launch_bounds__(kBT, BIELCC_CON_MINB)
+    batch_contract_kernel(const JobDev* __restrict__ jobs, const BatchItem* __restrict__ items, int n_items,
+                          int* __restrict__ counter, int max_items, const float* __restrict__ mom) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    float* s_mom = (float*)smem;               // [16][20][kBP]
+    float* s_j = s_mom + kConCells * 20 * kBP;  // [16][kSP][3][4]
+    __shared__ int s_item;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    for (int taken = 0; taken < max_items; taken++) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int it = s_item;
+        if (it >= n_items) break;
+        const BatchItem bi = items[it];
+        const JobDev& jb = jobs[bi.job];
+        const int P = jb.n_pts, N = jb.n_cells, S = jb.n_rhs;
+        const int p = bi.tile * kBP + lane;
+        const bool live = p < P;
+        const int cb = bi.range * jb.cells_per_range;
+        const int ce = min(N, cb + jb.cells_per_range);
+        const float* mo = mom + (size_t)bi.pad * kMomBlock;
+
+        for (int c0 = cb; c0 < ce; c0 += kConCells) {
+            const int nc = min(kConCells, ce - c0);
+            __syncthreads();  // the previous chunk's phase B is done with s_mom and s_j
+            {
+                const float4* src = reinterpret_cast<const float4*>(mo + (size_t)(c0 - cb) * 20 * kBP);
+                float4* dst = reinterpret_cast<float4*>(s_mom);
+                for (int i = threadIdx.x; i < nc * 20 * kBP / 4; i += kBT) dst[i] = __ldcs(src + i);
+            }
+            batch_stage_j<true>(s_j, jb, c0, nc, 0, min(kSP, S), threadIdx.x);
+            __syncthreads();
+            batch_phase_b<true>(s_mom, s_j, nc, 0, min(kSP, S), warp, lane, live, jb, bi.range, S, P, p, c0 == cb);
+            // further RHS passes reuse the chunk's moments in shared memory
+            for (int s0 = kSP; s0 < S; s0 += kSP) {
+                __syncthreads();
+                batch_stage_j<true>(s_j, jb, c0, nc, s0, min(kSP, S - s0), threadIdx.x);
+                __syncthreads();
+                batch_phase_b<true>(s_mom, s_j, nc, s0, min(kSP, S - s0), warp, lane, live, jb, bi.range, S, P, p,
+                                    c0 == cb);
             }
         }
     }
@@ -1170,6 +1370,22 @@ int batch_grid(bool mixed, bool tc) {
     return sms * std::max(1, per);
 }
 
+size_t moments_block_bytes() { return (size_t)kMomBlock * sizeof(float); }
+
+// Resident CTAs of the split pipeline's two kernels (dynamic shared memory
+// opted in once).
+void split_grids(int& grid_mom, int& grid_con) {
+    int dev = 0, sms = 148, pm = 1, pc = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaFuncSetAttribute(batch_contract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kConSmem);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pm, batch_moments_kernel, kBT, 0) != cudaSuccess) pm = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pc, batch_contract_kernel, kBT, kConSmem) != cudaSuccess) pc = 1;
+    cudaGetLastError();
+    grid_mom = sms * std::max(1, pm);
+    grid_con = sms * std::max(1, pc);
+}
+
 // Cuts every job into items (32-point tile, range of cells). The range length
 // depends only on the job itself and on `item_cost` (estimated node
 // evaluations per item, a per-context autotuned constant), never on the other
@@ -1185,7 +1401,7 @@ int batch_cells_per_range(int n_cells, int n_rhs, int n_start, double item_cost)
 }
 
 void plan_batch(BatchPlan& bp, const std::vector<JobDev>& jobs_in, int n_start, bool mixed, double item_cost,
-                bool allow_tc) {
+                bool allow_tc, size_t split_cap) {
     bp.jobs = jobs_in;
     bp.mixed = mixed;
     bp.tc = mixed && allow_tc && n_start <= 8;
@@ -1227,12 +1443,79 @@ void plan_batch(BatchPlan& bp, const std::vector<JobDev>& jobs_in, int n_start, 
     const size_t T = bp.total_pts;
     bp.ws_bytes += al256(bp.jobs.size() * sizeof(JobDev)) + al256(bp.items.size() * sizeof(BatchItem)) +
                    al256(T * sizeof(int)) + 2 * al256((T + 1) * sizeof(long long)) + 3 * 256;
+    // split pipeline: waves of consecutive (sorted) items whose moments fit the buffer
+    bp.split = mixed && !bp.tc && n_start <= 8 && split_cap > 0 && !bp.items.empty();
+    bp.waves.clear();
+    bp.mom_blocks = 0;
+    if (bp.split) {
+        const size_t cap = std::max<size_t>(1, split_cap / (kMomBlock * sizeof(float)));
+        size_t used = 0;
+        int w0 = 0;
+        for (size_t i = 0; i < bp.items.size(); i++) {
+            BatchItem& it = bp.items[i];
+            const JobDev& j = bp.jobs[it.job];
+            const int cells = std::min(j.cells_per_range, j.n_cells - it.range * j.cells_per_range);
+            const size_t blocks = (size_t)(cells + kMomCells - 1) / kMomCells;
+            if (used + blocks > cap && (int)i > w0) {
+                bp.waves.emplace_back(w0, (int)i);
+                w0 = (int)i;
+                used = 0;
+            }
+            it.pad = (int)used;
+            used += blocks;
+            bp.mom_blocks = std::max(bp.mom_blocks, used);
+        }
+        bp.waves.emplace_back(w0, (int)bp.items.size());
+        bp.ws_bytes += al256(bp.mom_blocks * kMomBlock * sizeof(float)) + al256(2 * bp.waves.size() * sizeof(int));
+        split_grids(bp.grid_mom, bp.grid_con);
+    }
 }
 
 void batch_make_preemptible(BatchPlan& bp) {
     bp.max_items = 1;
     const size_t ctas = (bp.items.size() + bp.per_cta - 1) / bp.per_cta;
     bp.grid = std::max<int>(1, (int)std::min<size_t>(ctas, (size_t)INT32_MAX));
+}
+
+// The far-field launches of a planned batch: the fused kernel (or its
+// tensor-core form), or per wave the moments kernel (when `moments`) and the
+// contraction kernel. Resets the work counters first.
+static cudaError_t launch_far(BatchPlan& bp, const BatchDevPtrs& d, double analytic_calc, int n_start, bool moments,
+                       cudaStream_t s, int* launches) {
+    *launches = 0;
+    cudaError_t e = cudaMemsetAsync(d.counter, 0, sizeof(int), s);
+    if (e == cudaSuccess && bp.split) e = cudaMemsetAsync(d.wave_counters, 0, 2 * bp.waves.size() * sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    const int n_items = (int)bp.items.size();
+    if (n_items == 0) return cudaSuccess;
+    if (bp.split) {
+        for (size_t w = 0; w < bp.waves.size(); w++) {
+            const int b = bp.waves[w].first, n = bp.waves[w].second - bp.waves[w].first;
+            const int gm = bp.max_items == 1 ? n : std::min(bp.grid_mom, n);
+            const int gc = bp.max_items == 1 ? n : std::min(bp.grid_con, n);
+            if (moments) {
+                batch_moments_kernel<<<gm, kBT, 0, s>>>(d.jobs, d.items + b, n, d.wave_counters + 2 * w,
+                                                        analytic_calc, n_start, bp.max_items, d.mom);
+                *launches += 1;
+            }
+            batch_contract_kernel<<<gc, kBT, kConSmem, s>>>(d.jobs, d.items + b, n, d.wave_counters + 2 * w + 1,
+                                                             bp.max_items, d.mom);
+            *launches += 1;
+        }
+        return cudaGetLastError();
+    }
+    const size_t smem = bp.mixed ? BatchCfg<true>::smem_bytes() : BatchCfg<false>::smem_bytes();
+    if (bp.tc)
+        batch_far_tc_kernel<<<bp.grid, tcb::kThreads, tcb::kSmem, s>>>(d.jobs, d.items, n_items, d.counter,
+                                                                      analytic_calc, n_start, bp.max_items, d.err);
+    else if (bp.mixed)
+        batch_far_kernel<true><<<bp.grid, kBT, smem, s>>>(d.jobs, d.items, n_items, d.counter, analytic_calc, n_start,
+                                                         bp.max_items);
+    else
+        batch_far_kernel<false><<<bp.grid, kBT, smem, s>>>(d.jobs, d.items, n_items, d.counter, analytic_calc,
+                                                          n_start, bp.max_items);
+    *launches = 1;
+    return cudaGetLastError();
 }
 
 // Enqueues stage 1 (far kernel, near counting, scan) of a planned batch into
@@ -1263,31 +1546,26 @@ cudaError_t batch_stage1(BatchPlan& bp, void* ws, double analytic_calc, int n_st
     d.err = d.total + 1;
     w += 256;
     d.counter = (int*)w;
+    w += 256;
+    if (bp.split) {
+        d.mom = (float*)w;
+        w += al256(bp.mom_blocks * kMomBlock * sizeof(float));
+        d.wave_counters = (int*)w;
+    }
     cudaError_t e = cudaMemcpyAsync(d.jobs, bp.jobs.data(), bp.jobs.size() * sizeof(JobDev), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess && !bp.items.empty())
         e = cudaMemcpyAsync(d.items, bp.items.data(), bp.items.size() * sizeof(BatchItem), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess && T) e = cudaMemcpyAsync(d.pt_job, bp.pt_job.data(), T * sizeof(int), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(d.counter, 0, sizeof(int), s);
     if (e == cudaSuccess) e = cudaMemsetAsync(d.total, 0, 2 * sizeof(long long), s);
     if (e != cudaSuccess) return e;
-    const size_t smem = bp.mixed ? BatchCfg<true>::smem_bytes() : BatchCfg<false>::smem_bytes();
-    const int n_items = (int)bp.items.size();
-    if (n_items > 0) {
-        if (bp.tc)
-            batch_far_tc_kernel<<<bp.grid, tcb::kThreads, tcb::kSmem, s>>>(d.jobs, d.items, n_items, d.counter,
-                                                                          analytic_calc, n_start, bp.max_items, d.err);
-        else if (bp.mixed)
-            batch_far_kernel<true><<<bp.grid, kBT, smem, s>>>(d.jobs, d.items, n_items, d.counter, analytic_calc,
-                                                             n_start, bp.max_items);
-        else
-            batch_far_kernel<false><<<bp.grid, kBT, smem, s>>>(d.jobs, d.items, n_items, d.counter, analytic_calc,
-                                                              n_start, bp.max_items);
-    }
+    int lf = 0;
+    e = launch_far(bp, d, analytic_calc, n_start, true, s, &lf);
+    if (e != cudaSuccess) return e;
     const int tb = (int)((T + 127) / 128);
     if (T) batch_near_count_kernel<<<tb, 128, 0, s>>>(d.jobs, d.pt_job, (int)T, d.counts);
     scan_kernel<<<1, 1024, 0, s>>>(d.counts, (int)T, d.offs, d.total);
     *out = d;
-    *launches = (n_items > 0 ? 1 : 0) + (T ? 1 : 0) + 1;
+    *launches = lf + (T ? 1 : 0) + 1;
     return cudaGetLastError();
 }
 
@@ -1338,21 +1616,11 @@ cudaError_t batch_stage2(BatchPlan& bp, const BatchDevPtrs& d, long long n_near,
 cudaError_t batch_replay(BatchPlan& bp, const BatchDevPtrs& d, long long n_near, void* pair_ws, double analytic_calc,
                          int n_start, cudaStream_t s) {
     const size_t T = bp.total_pts;
-    cudaError_t e = cudaMemsetAsync(d.counter, 0, sizeof(int), s);
+    // one wave: the moments left in the buffer by the first evaluation depend
+    // on geometry, points and k only, so the replay contracts them again
+    int lf = 0;
+    cudaError_t e = launch_far(bp, d, analytic_calc, n_start, !(bp.split && bp.waves.size() == 1), s, &lf);
     if (e != cudaSuccess) return e;
-    const size_t smem = bp.mixed ? BatchCfg<true>::smem_bytes() : BatchCfg<false>::smem_bytes();
-    const int n_items = (int)bp.items.size();
-    if (n_items > 0) {
-        if (bp.tc)
-            batch_far_tc_kernel<<<bp.grid, tcb::kThreads, tcb::kSmem, s>>>(d.jobs, d.items, n_items, d.counter,
-                                                                          analytic_calc, n_start, bp.max_items, d.err);
-        else if (bp.mixed)
-            batch_far_kernel<true><<<bp.grid, kBT, smem, s>>>(d.jobs, d.items, n_items, d.counter, analytic_calc,
-                                                             n_start, bp.max_items);
-        else
-            batch_far_kernel<false><<<bp.grid, kBT, smem, s>>>(d.jobs, d.items, n_items, d.counter, analytic_calc,
-                                                              n_start, bp.max_items);
-    }
     if (T) {
         const cplx* moments = nullptr;
         const int* pair_cell = nullptr;

@@ -11,6 +11,8 @@
 struct bielcc_ctx_s;  // the C ABI's context (api.cu)
 // Whether the context's mixed batches may use the tensor-core contraction (api.cu).
 bool ctx_batch_tensor_cores(bielcc_ctx_s* ctx);
+// moments-buffer cap of the split pipeline (0: the fused kernel)
+size_t ctx_batch_split_cap(bielcc_ctx_s* ctx);
 
 namespace bielcc_gpu {
 
@@ -195,6 +197,13 @@ struct BatchPlan {
     bool tc = false;
     int per_cta = 1;  // items a CTA works on at once (the tensor-core kernel's CTA holds two groups)
     int workers() const { return grid * per_cta; }
+    // split pipeline (mixed, n_start <= 8): per wave [first, last) of the
+    // sorted items, batch_moments_kernel then batch_contract_kernel, through a
+    // moments buffer of mom_blocks blocks (BatchItem::pad = the item's first block)
+    bool split = false;
+    std::vector<std::pair<int, int>> waves;
+    size_t mom_blocks = 0;
+    int grid_mom = 0, grid_con = 0;
 };
 // Turns a planned batch into one CTA per item (see BatchPlan::max_items).
 void batch_make_preemptible(BatchPlan& bp);
@@ -208,6 +217,8 @@ struct BatchDevPtrs {
     long long* total;
     long long* err;  // nonzero: a bounded wait in the far kernel ran out (next to total)
     int* counter;
+    float* mom = nullptr;           // split pipeline: the moments buffer
+    int* wave_counters = nullptr;   // split pipeline: two work counters per wave
 };
 // Copies the near-pair count into h[0] and the far kernel's status into h[3]
 // (a 64-byte pinned block; h[1] may hold another count).
@@ -219,8 +230,13 @@ inline bool batch_timed_out(const long long* h) { return h[3] != 0; }
 int batch_cells_per_range(int n_cells, int n_rhs, int n_start, double item_cost);
 // allow_tc: mixed batches that qualify run the tensor-core contraction
 // (bielcc_ctx_set_batch_tensor_cores); otherwise the CUDA-core kernel.
+// split_cap > 0: mixed batches with n_start <= 8 (and no tensor-core
+// contraction) run the split pipeline with a moments buffer of at most
+// split_cap bytes (waves of items); 0: the fused kernel.
 void plan_batch(BatchPlan& bp, const std::vector<JobDev>& jobs, int n_start, bool mixed, double item_cost,
-                bool allow_tc = true);
+                bool allow_tc = true, size_t split_cap = 0);
+// bytes of one moments block of the split pipeline (8 cells x 20 moments x 32 points, FP32)
+size_t moments_block_bytes();
 cudaError_t batch_stage1(BatchPlan& bp, void* ws, double analytic_calc, int n_start, bool ck, cudaStream_t s,
                          BatchDevPtrs* out, int* launches);
 size_t batch_pair_ws_bytes(long long n_near);

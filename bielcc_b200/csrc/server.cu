@@ -187,6 +187,7 @@ struct Slot {
     AssembleLaunch asl{};
     size_t out_base = 0, out_total = 0, nan_off = 0;
     int64_t extra = 0;  // reservation correction once the near count is known
+    int64_t mom_res = 0;  // reservation of the batch's moments buffer (split pipeline)
     // error sample of a mixed field batch (estimate.cu): per request min(P, 32)
     // points and min(S, 4) right-hand sides in FP64, after the main stage 1
     bool samp_on = false;
@@ -238,6 +239,8 @@ struct bielcc_server_s {
 };
 
 constexpr size_t kTraceCap = 4096;
+// largest moments buffer of one served batch (split pipeline): larger batches run in waves
+constexpr size_t kServeMomCap = (size_t)1 << 30;
 
 namespace {
 
@@ -286,8 +289,8 @@ void fail_slot_locked(bielcc_server_s* sv, Slot& sl, int code) {
         sv->reserved -= r->bytes;
         sv->failed++;
     }
-    sv->reserved -= sl.extra;
-    sl.extra = 0;
+    sv->reserved -= sl.extra + sl.mom_res;
+    sl.extra = sl.mom_res = 0;
     sv->running -= (int)sl.reqs.size();
     sl.reqs.clear();
     sl.state = kIdle;
@@ -385,8 +388,13 @@ cudaError_t start_field_batch(bielcc_server_s* sv, Slot& sl) {
     }
     auto t3 = Clock::now();
     plan_batch(sl.bp, jd, sv->np.n_start, sv->precision == BIELCC_PREC_MIXED, sv->item_cost,
-               ctx_batch_tensor_cores(sv->ctx));
+               ctx_batch_tensor_cores(sv->ctx), std::min<size_t>(ctx_batch_split_cap(sv->ctx), kServeMomCap));
     if (sv->preemptible) batch_make_preemptible(sl.bp);
+    if (sl.bp.split) {  // the moments buffer counts against the budget until the batch completes
+        std::lock_guard<std::mutex> g(sv->mu);
+        sl.mom_res = (int64_t)(sl.bp.mom_blocks * moments_block_bytes());
+        sv->reserved += sl.mom_res;
+    }
     auto t4 = Clock::now();
     e = sl.ws.ensure(sl.bp.ws_bytes, sl.s);
     if (e != cudaSuccess) return e;
@@ -564,8 +572,8 @@ void complete_slot(bielcc_server_s* sv, Slot& sl) {
         if (r->type == kField) sv->pairs_done += r->pairs;
         sv->lat_ms.push_back(std::chrono::duration<double, std::milli>(now - r->t_submit).count());
     }
-    sv->reserved -= sl.extra;
-    sl.extra = 0;
+    sv->reserved -= sl.extra + sl.mom_res;
+    sl.extra = sl.mom_res = 0;
     sv->t_last = now;
     sv->running -= (int)sl.reqs.size();
     sl.reqs.clear();

@@ -147,6 +147,14 @@ int bielcc_ctx_set_timing(bielcc_ctx ctx, int on);
  * accurate on the batched workloads (the moments, not the contraction, bound
  * both forms). No counterpart in the reference. */
 int bielcc_ctx_set_batch_tensor_cores(bielcc_ctx ctx, int on);
+/* Mixed-precision batches with n_start <= 8 (and the CUDA-core contraction)
+ * run as two kernels per wave of work items: the far moments of every
+ * (point, cell) pair into a device buffer of at most moments_bytes (default
+ * 16 GiB, part of the context's workspace), then their contraction with the
+ * currents. Results are bit-identical to the fused kernel (moments_bytes = 0).
+ * A batch plan whose moments fit one wave replays only the contraction. No
+ * counterpart in the reference. */
+int bielcc_ctx_set_batch_split(bielcc_ctx ctx, int64_t moments_bytes);
 int bielcc_ctx_stats(bielcc_ctx ctx, bielcc_stats* out, int reset);
 
 /* Measured FMA throughput (TFLOP/s, 2 flops per FMA) of the current device's

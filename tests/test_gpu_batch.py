@@ -89,17 +89,23 @@ def test_batch_fallback_adaptive_and_autotune(gctx):
     assert c > 0
 
 
-@pytest.mark.parametrize("tensor_cores", [False, True])
-def test_batch_plan_graph_replay_with_new_currents(gctx, tensor_cores):
+SPLIT_DEFAULT = 16 << 30
+
+
+@pytest.mark.parametrize("mode", ["split, one wave", "split, many waves", "fused", "tensor cores"])
+def test_batch_plan_graph_replay_with_new_currents(gctx, mode):
     """A planned batch replayed from its CUDA graph after the currents changed
     in place gives the same result as a fresh batched call with those
-    currents, and matches the oracle; with either contraction."""
+    currents, and matches the oracle: the split pipeline (a plan of one wave
+    replays only the contraction), the fused kernel, the tensor-core form."""
     torch = pytest.importorskip("torch")
-    gctx.set_batch_tensor_cores(tensor_cores)
+    gctx.set_batch_tensor_cores(mode == "tensor cores")
+    gctx.set_batch_split({"split, one wave": SPLIT_DEFAULT, "split, many waves": 100_000}.get(mode, 0))
     try:
         _plan_replay(torch, gctx)
     finally:
         gctx.set_batch_tensor_cores(False)
+        gctx.set_batch_split(SPLIT_DEFAULT)
 
 
 def _plan_replay(torch, gctx):
@@ -210,3 +216,37 @@ def test_batch_tensor_core_contraction_matches_cuda_cores(gctx):
     out, _ = _batch(torch, gctx, [big], "mixed")
     Eo, Ho = oracle.field_EH(big["cells"], big["J"][::23], big["k"], big["pts"], mult=big["mult"])
     assert rel_l2(out[0][0][::23], Eo) < TOL_MIXED and rel_l2(out[0][1][::23], Ho) < TOL_MIXED
+
+
+@pytest.mark.parametrize("cap", [SPLIT_DEFAULT, 200_000])
+def test_batch_split_pipeline_equals_fused_kernel(gctx, cap):
+    """The split pipeline (moments to a device buffer, then the contraction;
+    one wave, or many waves of a small buffer) gives bit-identical results to
+    the fused kernel: 1 to 70 right-hand sides, quads and triangles, real and
+    complex k, near points."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(21)
+    meshes = [W.uv_sphere(8, 16), W.perturbed_icosphere(2, seed=5), W.torus(24, 8), W.rounded_cube(6, 0.1, 1.0),
+              W.triangulate(W.uv_sphere(6, 12))]
+    specs = []
+    for i, cells in enumerate(meshes):
+        k = [2.0, 6.0, complex(3.0, 0.3), 9.0, 4.0][i]
+        S = [1, 5, 17, 33, 70][i]
+        ext = float(np.max(np.linalg.norm(cells.reshape(-1, 3), axis=1)))
+        pts = np.concatenate([W.shell_points(45 + 7 * i, 1.6 * ext, 3 * ext, rng),
+                              W.near_points(cells, 5, 0.02, 0.2, rng)])
+        specs.append(dict(mesh=gctx.mesh(cells), cells=cells, J=W.po_currents(cells, abs(k), directions=S, seed=i),
+                          pts=pts, k=k, mult=complex(0.5, 1.0)))
+    try:
+        gctx.set_batch_split(0)
+        fused, _ = _batch(torch, gctx, specs, "mixed")
+        gctx.set_batch_split(cap)
+        split, rep = _batch(torch, gctx, specs, "mixed")
+    finally:
+        gctx.set_batch_split(SPLIT_DEFAULT)
+    assert rep.n_near_pairs > 0
+    for (E, H), (Ef, Hf) in zip(split, fused):
+        assert np.array_equal(E, Ef) and np.array_equal(H, Hf)
+    sp = specs[2]
+    Eo, Ho = oracle.field_EH(sp["cells"], sp["J"][:2], sp["k"], sp["pts"], mult=sp["mult"])
+    assert rel_l2(split[2][0][:2], Eo) < TOL_MIXED and rel_l2(split[2][1][:2], Ho) < TOL_MIXED
