@@ -187,7 +187,6 @@ struct Slot {
     AssembleLaunch asl{};
     size_t out_base = 0, out_total = 0, nan_off = 0;
     int64_t extra = 0;  // reservation correction once the near count is known
-    int64_t mom_res = 0;  // reservation of the batch's moments buffer (split pipeline)
     // error sample of a mixed field batch (estimate.cu): per request min(P, 32)
     // points and min(S, 4) right-hand sides in FP64, after the main stage 1
     bool samp_on = false;
@@ -257,9 +256,11 @@ int64_t near_estimate(int64_t pts, int64_t cells) {
 }
 
 // Device bytes of a field request inside a batch: inputs, outputs, the
-// job's partial sums and near mask (as plan_batch lays them out) and the
-// near-pair estimate. The item size is read under the server lock.
-int64_t field_bytes(const Req& r, int n_start, double item_cost) {
+// job's partial sums and near mask (as plan_batch lays them out), the
+// near-pair estimate and, for the split pipeline (mom_cap > 0), its share of
+// the batch's moments buffer (at most the buffer's cap, so the batch's buffer
+// never exceeds its requests' sum). The item size is read under the server lock.
+int64_t field_bytes(const Req& r, int n_start, double item_cost, int64_t mom_cap) {
     const int64_t S = r.f.n_rhs, P = r.f.n_pts, N = r.mesh->n_cells;
     const int64_t in = (r.f.J_dev ? 0 : al(S * N * 48)) + al(P * 24);
     const int64_t out = al(S * P * 3 * (r.f.out_c64 ? 8 : 16) * (r.f.H ? 2 : 1)) + 8;
@@ -270,7 +271,12 @@ int64_t field_bytes(const Req& r, int n_start, double item_cost) {
     const int64_t Q = std::min<int64_t>(P, 32), Ss = std::min<int64_t>(S, 4);
     const int64_t samp = 3 * al(Q * 24 + Ss * Q * 96) + al((ranges + 1) * Ss * 12 * Q * 8) + al(words * Q * 4) +
                          al(Q * 8 * 216) + 1024;
-    return in + out + ws + samp + r.near_est;
+    int64_t mom = 0;
+    if (mom_cap > 0) {
+        const int64_t blocks = (P + 31) / 32 * ((N + 7) / 8 + ranges);
+        mom = std::min<int64_t>(mom_cap, blocks * (int64_t)moments_block_bytes());
+    }
+    return in + out + ws + samp + r.near_est + mom;
 }
 
 int64_t assemble_bytes(const Req& r) {
@@ -289,8 +295,8 @@ void fail_slot_locked(bielcc_server_s* sv, Slot& sl, int code) {
         sv->reserved -= r->bytes;
         sv->failed++;
     }
-    sv->reserved -= sl.extra + sl.mom_res;
-    sl.extra = sl.mom_res = 0;
+    sv->reserved -= sl.extra;
+    sl.extra = 0;
     sv->running -= (int)sl.reqs.size();
     sl.reqs.clear();
     sl.state = kIdle;
@@ -390,11 +396,7 @@ cudaError_t start_field_batch(bielcc_server_s* sv, Slot& sl) {
     plan_batch(sl.bp, jd, sv->np.n_start, sv->precision == BIELCC_PREC_MIXED, sv->item_cost,
                ctx_batch_tensor_cores(sv->ctx), std::min<size_t>(ctx_batch_split_cap(sv->ctx), kServeMomCap));
     if (sv->preemptible) batch_make_preemptible(sl.bp);
-    if (sl.bp.split) {  // the moments buffer counts against the budget until the batch completes
-        std::lock_guard<std::mutex> g(sv->mu);
-        sl.mom_res = (int64_t)(sl.bp.mom_blocks * moments_block_bytes());
-        sv->reserved += sl.mom_res;
-    }
+
     auto t4 = Clock::now();
     e = sl.ws.ensure(sl.bp.ws_bytes, sl.s);
     if (e != cudaSuccess) return e;
@@ -572,8 +574,8 @@ void complete_slot(bielcc_server_s* sv, Slot& sl) {
         if (r->type == kField) sv->pairs_done += r->pairs;
         sv->lat_ms.push_back(std::chrono::duration<double, std::milli>(now - r->t_submit).count());
     }
-    sv->reserved -= sl.extra + sl.mom_res;
-    sl.extra = sl.mom_res = 0;
+    sv->reserved -= sl.extra;
+    sl.extra = 0;
     sv->t_last = now;
     sv->running -= (int)sl.reqs.size();
     sl.reqs.clear();
@@ -956,7 +958,10 @@ int bielcc_server_submit_field(bielcc_server sv, const bielcc_field_request* req
         std::lock_guard<std::mutex> g(sv->mu);
         item_cost = sv->item_cost;
     }
-    r->bytes = field_bytes(*r, sv->np.n_start, item_cost);
+    const int64_t mom_cap = sv->precision == BIELCC_PREC_MIXED && sv->np.n_start <= 8 && !ctx_batch_tensor_cores(sv->ctx)
+                                ? (int64_t)std::min<size_t>(ctx_batch_split_cap(sv->ctx), kServeMomCap)
+                                : 0;
+    r->bytes = field_bytes(*r, sv->np.n_start, item_cost, mom_cap);
     r->pairs = (int64_t)req->n_pts * r->mesh->n_cells * req->n_rhs;
     return submit(sv, r, ticket);
 }

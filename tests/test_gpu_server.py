@@ -208,8 +208,9 @@ def test_server_budget_cancel_and_errors(gctx):
         assert s["rejected"] == 1 and s["cancelled"] == 1
         assert 0 < s["peak_bytes_reserved"] <= s["budget"]
         # requests that do not fit the budget together run one after another
-        # far points (no near pairs on this coarse mesh), ~2.5 MB reserved each: two exceed the budget
-        pts = W.shell_points(900, 8.0, 10.0, np.random.default_rng(2))
+        # far points (no near pairs on this coarse mesh), ~2.7 MB reserved each (with the share of
+        # the moments buffer): two exceed the budget
+        pts = W.shell_points(300, 8.0, 10.0, np.random.default_rng(2))
         sv.pause(True)
         ta = sv.submit_field(sp["mesh"], sp["J"], pts, sp["k"])
         tb = sv.submit_field(sp["mesh"], sp["J"], pts, sp["k"])
