@@ -903,10 +903,15 @@ BIELCC_D bool group_or(int id, bool v) {
     return r != 0;
 }
 
+// BUF = true: the contraction kernel of the split pipeline with this
+// contraction: the moments of each round come from batch_moments_kernel's
+// buffer `mom` (read once, streaming) instead of being evaluated here, and the
+// near mask is already written.
+template <bool BUF>
 __global__ void __launch_bounds__(tcb::kThreads, 1)
     batch_far_tc_kernel(const JobDev* __restrict__ jobs, const BatchItem* __restrict__ items, int n_items,
                         int* __restrict__ counter, double analytic_calc, int n_start, int max_items,
-                        long long* __restrict__ err) {
+                        long long* __restrict__ err, const float* __restrict__ mom) {
     extern __shared__ __align__(128) unsigned char smem_all[];
     const int grp = threadIdx.x / tcb::kGroupThreads;
     const int gt = threadIdx.x - grp * tcb::kGroupThreads;  // thread of the group
@@ -980,13 +985,14 @@ __global__ void __launch_bounds__(tcb::kThreads, 1)
         const int p = bi.tile * kBP + lane;
         const bool live = p < P;
         double x[3] = {0., 0., 0.};
-        if (live)
+        if (!BUF && live)
             for (int g = 0; g < 3; g++) x[g] = jb.pts[3 * (size_t)p + g];
         const int cb = bi.range * jb.cells_per_range;
         const int ce = min(N, cb + jb.cells_per_range);
         const cplx k = jb.k;
         const double k2r = k.re * k.re - k.im * k.im, k2i = 2.0 * k.re * k.im;
         const bool ck = k.im != 0.0;
+        const float* mo = BUF ? mom + (size_t)bi.pad * kMomBlock : nullptr;
         const int G = (S + tcb::kG - 1) / tcb::kG;
         const int Spad = (S + 7) & ~7;
         unsigned nbits = 0;
@@ -1026,8 +1032,8 @@ __global__ void __launch_bounds__(tcb::kThreads, 1)
                 const int rc0 = c0 + r * tcb::kRound;
                 const int nc = min(tcb::kRound, ce - rc0);
                 if (nc <= 0) break;
-                group_sync(bar_id);  // the previous round's reads of the staged nodes are done
-                {
+                if constexpr (!BUF) {
+                    group_sync(bar_id);  // the previous round's reads of the staged nodes are done
                     const float4* src = jb.nodes32 + (size_t)rc0 * nn;
                     for (int i = gt; i < nc * nn; i += tcb::kGroupThreads) {
                         const float4 v = __ldg(src + i);
@@ -1039,13 +1045,19 @@ __global__ void __launch_bounds__(tcb::kThreads, 1)
                         s_cell[i] = make_double4(gg.c[0], gg.c[1], gg.c[2], gg.diam);
                         s_rho[i] = (double)jb.rho32[rc0 + i];
                     }
+                    group_sync(bar_id);
                 }
-                group_sync(bar_id);
                 // phase A: the moments of cell `warp` of the round for this warp's 32 points
                 float mom[20];
 #pragma unroll
                 for (int q = 0; q < 20; q++) mom[q] = 0.f;
-                if (warp < nc) {
+                if constexpr (BUF) {
+                    if (warp < nc) {
+                        const float* src = mo + (size_t)(rc0 - cb + warp) * 20 * kBP + lane;
+#pragma unroll
+                        for (int q = 0; q < 20; q++) mom[q] = __ldcs(src + q * kBP);
+                    }
+                } else if (warp < nc) {
                     const double4 ci = s_cell[warp];
                     const double cen[3] = {ci.x, ci.y, ci.z};
                     double d;
@@ -1075,7 +1087,7 @@ __global__ void __launch_bounds__(tcb::kThreads, 1)
                 group_sync(bar_id);
                 umma::fence_after_sync();
                 // near-cell mask: warp 0 owns the words of its points
-                if (warp == 0) {
+                if (!BUF && warp == 0) {
                     for (int cc = 0; cc < nc; cc++) {
                         const int c = rc0 + cc;
                         nbits |= (unsigned)s_near[cc * 32 + lane] << (c & 31);
@@ -1334,11 +1346,12 @@ int batch_grid(bool mixed, bool tc) {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (tc) {
-        cudaFuncSetAttribute(batch_far_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tcb::kSmem);
-        cudaFuncSetAttribute(batch_far_tc_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             (int)cudaSharedmemCarveoutMaxShared);
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_far_tc_kernel, tcb::kThreads, tcb::kSmem) !=
-            cudaSuccess) {
+        for (const void* f : {(const void*)batch_far_tc_kernel<false>, (const void*)batch_far_tc_kernel<true>}) {
+            cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tcb::kSmem);
+            cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+        }
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_far_tc_kernel<false>, tcb::kThreads,
+                                                          tcb::kSmem) != cudaSuccess) {
             cudaGetLastError();
             per = 1;
         }
@@ -1346,7 +1359,7 @@ int batch_grid(bool mixed, bool tc) {
         // occupancy query can assume a smaller carveout than the launch gets
         cudaFuncAttributes fa{};
         int regs_sm = 65536, smem_sm = 0, resv = 0;
-        if (cudaFuncGetAttributes(&fa, batch_far_tc_kernel) == cudaSuccess &&
+        if (cudaFuncGetAttributes(&fa, batch_far_tc_kernel<false>) == cudaSuccess &&
             cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev) == cudaSuccess &&
             cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) == cudaSuccess &&
             cudaDeviceGetAttribute(&resv, cudaDevAttrReservedSharedMemoryPerBlock, dev) == cudaSuccess) {
@@ -1444,7 +1457,7 @@ void plan_batch(BatchPlan& bp, const std::vector<JobDev>& jobs_in, int n_start, 
     bp.ws_bytes += al256(bp.jobs.size() * sizeof(JobDev)) + al256(bp.items.size() * sizeof(BatchItem)) +
                    al256(T * sizeof(int)) + 2 * al256((T + 1) * sizeof(long long)) + 3 * 256;
     // split pipeline: waves of consecutive (sorted) items whose moments fit the buffer
-    bp.split = mixed && !bp.tc && n_start <= 8 && split_cap > 0 && !bp.items.empty();
+    bp.split = mixed && n_start <= 8 && split_cap > 0 && !bp.items.empty();
     bp.waves.clear();
     bp.mom_blocks = 0;
     if (bp.split) {
@@ -1468,6 +1481,10 @@ void plan_batch(BatchPlan& bp, const std::vector<JobDev>& jobs_in, int n_start, 
         bp.waves.emplace_back(w0, (int)bp.items.size());
         bp.ws_bytes += al256(bp.mom_blocks * kMomBlock * sizeof(float)) + al256(2 * bp.waves.size() * sizeof(int));
         split_grids(bp.grid_mom, bp.grid_con);
+        if (bp.tc) bp.grid_con = bp.grid;  // the tensor-core contraction: one CTA of two groups per SM
+        // the moments kernel sets the pace: planning counts its CTAs
+        bp.grid = bp.grid_mom;
+        bp.per_cta = 1;
     }
 }
 
@@ -1492,22 +1509,28 @@ static cudaError_t launch_far(BatchPlan& bp, const BatchDevPtrs& d, double analy
         for (size_t w = 0; w < bp.waves.size(); w++) {
             const int b = bp.waves[w].first, n = bp.waves[w].second - bp.waves[w].first;
             const int gm = bp.max_items == 1 ? n : std::min(bp.grid_mom, n);
-            const int gc = bp.max_items == 1 ? n : std::min(bp.grid_con, n);
+            const int gc = bp.max_items == 1 ? (bp.tc ? (n + tcb::kGroups - 1) / tcb::kGroups : n)
+                                             : std::min(bp.grid_con, n);
             if (moments) {
                 batch_moments_kernel<<<gm, kBT, 0, s>>>(d.jobs, d.items + b, n, d.wave_counters + 2 * w,
                                                         analytic_calc, n_start, bp.max_items, d.mom);
                 *launches += 1;
             }
-            batch_contract_kernel<<<gc, kBT, kConSmem, s>>>(d.jobs, d.items + b, n, d.wave_counters + 2 * w + 1,
-                                                             bp.max_items, d.mom);
+            if (bp.tc)
+                batch_far_tc_kernel<true><<<gc, tcb::kThreads, tcb::kSmem, s>>>(
+                    d.jobs, d.items + b, n, d.wave_counters + 2 * w + 1, analytic_calc, n_start, bp.max_items, d.err,
+                    d.mom);
+            else
+                batch_contract_kernel<<<gc, kBT, kConSmem, s>>>(d.jobs, d.items + b, n, d.wave_counters + 2 * w + 1,
+                                                                 bp.max_items, d.mom);
             *launches += 1;
         }
         return cudaGetLastError();
     }
     const size_t smem = bp.mixed ? BatchCfg<true>::smem_bytes() : BatchCfg<false>::smem_bytes();
     if (bp.tc)
-        batch_far_tc_kernel<<<bp.grid, tcb::kThreads, tcb::kSmem, s>>>(d.jobs, d.items, n_items, d.counter,
-                                                                      analytic_calc, n_start, bp.max_items, d.err);
+        batch_far_tc_kernel<false><<<bp.grid, tcb::kThreads, tcb::kSmem, s>>>(
+            d.jobs, d.items, n_items, d.counter, analytic_calc, n_start, bp.max_items, d.err, nullptr);
     else if (bp.mixed)
         batch_far_kernel<true><<<bp.grid, kBT, smem, s>>>(d.jobs, d.items, n_items, d.counter, analytic_calc, n_start,
                                                          bp.max_items);

@@ -92,15 +92,17 @@ def test_batch_fallback_adaptive_and_autotune(gctx):
 SPLIT_DEFAULT = 16 << 30
 
 
-@pytest.mark.parametrize("mode", ["split, one wave", "split, many waves", "fused", "tensor cores"])
+@pytest.mark.parametrize("mode", ["split, one wave", "split, many waves", "fused", "tensor cores",
+                                  "split, tensor cores"])
 def test_batch_plan_graph_replay_with_new_currents(gctx, mode):
     """A planned batch replayed from its CUDA graph after the currents changed
     in place gives the same result as a fresh batched call with those
     currents, and matches the oracle: the split pipeline (a plan of one wave
     replays only the contraction), the fused kernel, the tensor-core form."""
     torch = pytest.importorskip("torch")
-    gctx.set_batch_tensor_cores(mode == "tensor cores")
-    gctx.set_batch_split({"split, one wave": SPLIT_DEFAULT, "split, many waves": 100_000}.get(mode, 0))
+    gctx.set_batch_tensor_cores("tensor cores" in mode)
+    gctx.set_batch_split({"split, one wave": SPLIT_DEFAULT, "split, many waves": 100_000,
+                          "split, tensor cores": SPLIT_DEFAULT}.get(mode, 0))
     try:
         _plan_replay(torch, gctx)
     finally:
@@ -218,12 +220,14 @@ def test_batch_tensor_core_contraction_matches_cuda_cores(gctx):
     assert rel_l2(out[0][0][::23], Eo) < TOL_MIXED and rel_l2(out[0][1][::23], Ho) < TOL_MIXED
 
 
+@pytest.mark.parametrize("tensor_cores", [False, True])
 @pytest.mark.parametrize("cap", [SPLIT_DEFAULT, 200_000])
-def test_batch_split_pipeline_equals_fused_kernel(gctx, cap):
-    """The split pipeline (moments to a device buffer, then the contraction;
-    one wave, or many waves of a small buffer) gives bit-identical results to
-    the fused kernel: 1 to 70 right-hand sides, quads and triangles, real and
-    complex k, near points."""
+def test_batch_split_pipeline_equals_fused_kernel(gctx, cap, tensor_cores):
+    """The split pipeline (moments to a device buffer, then the contraction on
+    the CUDA or the tensor cores; one wave, or many waves of a small buffer)
+    gives bit-identical results to the fused kernel of the same contraction:
+    1 to 70 right-hand sides (the tensor cores: up to 64), quads and
+    triangles, real and complex k, near points."""
     torch = pytest.importorskip("torch")
     rng = np.random.default_rng(21)
     meshes = [W.uv_sphere(8, 16), W.perturbed_icosphere(2, seed=5), W.torus(24, 8), W.rounded_cube(6, 0.1, 1.0),
@@ -231,19 +235,21 @@ def test_batch_split_pipeline_equals_fused_kernel(gctx, cap):
     specs = []
     for i, cells in enumerate(meshes):
         k = [2.0, 6.0, complex(3.0, 0.3), 9.0, 4.0][i]
-        S = [1, 5, 17, 33, 70][i]
+        S = [1, 5, 17, 33, 64 if tensor_cores else 70][i]
         ext = float(np.max(np.linalg.norm(cells.reshape(-1, 3), axis=1)))
         pts = np.concatenate([W.shell_points(45 + 7 * i, 1.6 * ext, 3 * ext, rng),
                               W.near_points(cells, 5, 0.02, 0.2, rng)])
         specs.append(dict(mesh=gctx.mesh(cells), cells=cells, J=W.po_currents(cells, abs(k), directions=S, seed=i),
                           pts=pts, k=k, mult=complex(0.5, 1.0)))
     try:
+        gctx.set_batch_tensor_cores(tensor_cores)
         gctx.set_batch_split(0)
         fused, _ = _batch(torch, gctx, specs, "mixed")
         gctx.set_batch_split(cap)
         split, rep = _batch(torch, gctx, specs, "mixed")
     finally:
         gctx.set_batch_split(SPLIT_DEFAULT)
+        gctx.set_batch_tensor_cores(False)
     assert rep.n_near_pairs > 0
     for (E, H), (Ef, Hf) in zip(split, fused):
         assert np.array_equal(E, Ef) and np.array_equal(H, Hf)
