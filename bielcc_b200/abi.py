@@ -5,7 +5,7 @@ shared object exporting functions with these argument layouts.
 """
 import ctypes as C
 
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 OK = 0
 ERR_ARG = -1

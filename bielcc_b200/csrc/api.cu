@@ -99,7 +99,10 @@ struct bielcc_ctx_s {
     cudaEvent_t side_out = nullptr;  // the side stream's error sample is complete
     DevBuf side_ws, side_pair_ws, side_io, side_scratch;
     bool batch_tc = false;              // mixed batches contract on the tensor cores when they qualify
-    size_t batch_split = (size_t)16 << 30;  // moments-buffer cap of the split pipeline (0: fused kernel)
+    // moments-buffer cap of the split pipeline (0: never split). Batch plans
+    // split when their moments fit one wave; every batch only with split_all.
+    size_t batch_split = (size_t)16 << 30;
+    bool batch_split_all = false;
     long long* h_side_total = nullptr;  // pinned
     unsigned long long* h_nonfinite = nullptr;
     // counters / timing (bielcc_ctx_stats)
@@ -200,7 +203,7 @@ struct WsSet {
 }  // namespace
 
 bool ctx_batch_tensor_cores(bielcc_ctx_s* ctx) { return ctx->batch_tc; }
-size_t ctx_batch_split_cap(bielcc_ctx_s* ctx) { return ctx->batch_split; }
+size_t ctx_batch_split_cap(bielcc_ctx_s* ctx) { return ctx->batch_split_all ? ctx->batch_split : 0; }
 
 namespace {
 
@@ -268,13 +271,14 @@ int field_device_batched(bielcc_ctx ctx, const FieldArgs& a, cudaStream_t s, bie
     d.H = a.H;
     BatchPlan bp;
     const bool mixed = a.precision == BIELCC_PREC_MIXED;
-    plan_batch(bp, std::vector<JobDev>{d}, a.np.n_start, mixed, ctx->batch_item_cost, ctx->batch_tc, ctx->batch_split);
+    const size_t split = ctx_batch_split_cap(ctx);
+    plan_batch(bp, std::vector<JobDev>{d}, a.np.n_start, mixed, ctx->batch_item_cost, ctx->batch_tc, split);
     // The tuned item size suits batches of many jobs; one job alone is cut
     // finer (up to its range limit) when its items would leave resident CTAs idle.
     if ((int)bp.items.size() < 2 * bp.workers()) {
         const double finer = std::max(1.0e5, ctx->batch_item_cost * bp.items.size() / (2.0 * bp.workers()));
         if (finer < ctx->batch_item_cost)
-            plan_batch(bp, std::vector<JobDev>{d}, a.np.n_start, mixed, finer, ctx->batch_tc, ctx->batch_split);
+            plan_batch(bp, std::vector<JobDev>{d}, a.np.n_start, mixed, finer, ctx->batch_tc, split);
     }
     const double busy = std::min(1.0, (double)bp.items.size() / std::max(1, bp.workers()));
     const int S = a.n_rhs;
@@ -584,11 +588,12 @@ int bielcc_ctx_set_batch_tensor_cores(bielcc_ctx ctx, int on) {
     return BIELCC_OK;
 }
 
-int bielcc_ctx_set_batch_split(bielcc_ctx ctx, int64_t moments_bytes) {
+int bielcc_ctx_set_batch_split(bielcc_ctx ctx, int64_t moments_bytes, int all_batches) {
     TRY(enter(ctx));
     if (moments_bytes < 0) return set_error(BIELCC_ERR_ARG, "negative moments buffer size");
     std::lock_guard<std::mutex> g(ctx->mu);
     ctx->batch_split = (size_t)moments_bytes;
+    ctx->batch_split_all = all_batches != 0;
     return BIELCC_OK;
 }
 
@@ -1091,7 +1096,7 @@ int field_batch_locked(bielcc_ctx ctx, int n_jobs, const bielcc_field_job* jobs,
     if (precision == BIELCC_PREC_MIXED && want_est && n_jobs > 0)
         TRY(batch_est_begin(ctx, jd, jobs, n, ck, item_cost, s, es));
     BatchPlan bp;
-    plan_batch(bp, jd, n.n_start, precision == BIELCC_PREC_MIXED, item_cost, ctx->batch_tc, ctx->batch_split);
+    plan_batch(bp, jd, n.n_start, precision == BIELCC_PREC_MIXED, item_cost, ctx->batch_tc, ctx_batch_split_cap(ctx));
     TRY(ctx->ws.ensure(bp.ws_bytes));
     TRY(ctx->scratch_small.ensure(256));
     BatchDevPtrs d;
@@ -1200,8 +1205,14 @@ int bielcc_batch_plan_create(bielcc_ctx ctx, int n_jobs, const bielcc_field_job*
     cudaError_t e = cudaSuccess;
     int l1 = 0, l2 = 0;
     if (rc == BIELCC_OK) {
-        plan_batch(p->bp, jd, n.n_start, precision == BIELCC_PREC_MIXED, ctx->batch_item_cost, ctx->batch_tc,
-                   ctx->batch_split);
+        // A plan keeps the moments only when they fit one wave of the buffer:
+        // its replays then run the contraction alone. Over several waves a
+        // replay would evaluate every moment again, so it runs the fused kernel
+        // (unless every batch is set to split).
+        const bool mixed = precision == BIELCC_PREC_MIXED;
+        plan_batch(p->bp, jd, n.n_start, mixed, ctx->batch_item_cost, ctx->batch_tc, ctx->batch_split);
+        if (p->bp.split && p->bp.waves.size() > 1 && !ctx->batch_split_all)
+            plan_batch(p->bp, jd, n.n_start, mixed, ctx->batch_item_cost, ctx->batch_tc, 0);
         e = cudaMalloc(&p->ws, p->bp.ws_bytes);
         if (e == cudaSuccess) e = batch_stage1(p->bp, p->ws, n.analytic_calc, n.n_start, ck, s, &p->d, &l1);
         if (e == cudaSuccess) e = batch_status_to_host(p->d, ctx->h_total, s);

@@ -11,7 +11,8 @@
 struct bielcc_ctx_s;  // the C ABI's context (api.cu)
 // Whether the context's mixed batches may use the tensor-core contraction (api.cu).
 bool ctx_batch_tensor_cores(bielcc_ctx_s* ctx);
-// moments-buffer cap of the split pipeline (0: the fused kernel)
+// moments-buffer cap of the split pipeline for one-shot and served batches
+// (0: the fused kernel; nonzero only when the context sets every batch to split)
 size_t ctx_batch_split_cap(bielcc_ctx_s* ctx);
 
 namespace bielcc_gpu {
@@ -230,9 +231,9 @@ inline bool batch_timed_out(const long long* h) { return h[3] != 0; }
 int batch_cells_per_range(int n_cells, int n_rhs, int n_start, double item_cost);
 // allow_tc: mixed batches that qualify run the tensor-core contraction
 // (bielcc_ctx_set_batch_tensor_cores); otherwise the CUDA-core kernel.
-// split_cap > 0: mixed batches with n_start <= 8 (and no tensor-core
-// contraction) run the split pipeline with a moments buffer of at most
-// split_cap bytes (waves of items); 0: the fused kernel.
+// split_cap > 0: mixed batches with n_start <= 8 run the split pipeline with
+// a moments buffer of at most split_cap bytes (waves of items); 0: the fused
+// kernel.
 void plan_batch(BatchPlan& bp, const std::vector<JobDev>& jobs, int n_start, bool mixed, double item_cost,
                 bool allow_tc = true, size_t split_cap = 0);
 // bytes of one moments block of the split pipeline (8 cells x 20 moments x 32 points, FP32)

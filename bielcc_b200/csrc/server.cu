@@ -958,7 +958,8 @@ int bielcc_server_submit_field(bielcc_server sv, const bielcc_field_request* req
         std::lock_guard<std::mutex> g(sv->mu);
         item_cost = sv->item_cost;
     }
-    const int64_t mom_cap = sv->precision == BIELCC_PREC_MIXED && sv->np.n_start <= 8 && !ctx_batch_tensor_cores(sv->ctx)
+    // served batches split only when the context sets every batch to split
+    const int64_t mom_cap = sv->precision == BIELCC_PREC_MIXED && sv->np.n_start <= 8
                                 ? (int64_t)std::min<size_t>(ctx_batch_split_cap(sv->ctx), kServeMomCap)
                                 : 0;
     r->bytes = field_bytes(*r, sv->np.n_start, item_cost, mom_cap);

@@ -80,7 +80,7 @@ def load(path=LIB_PATH):
     d("bielcc_batch_plan_destroy", [vp])
     d("bielcc_ctx_set_timing", [vp, C.c_int])
     d("bielcc_ctx_set_batch_tensor_cores", [vp, C.c_int])
-    d("bielcc_ctx_set_batch_split", [vp, C.c_int64])
+    d("bielcc_ctx_set_batch_split", [vp, C.c_int64, C.c_int])
     d("bielcc_medium_at", [C.POINTER(abi.Material), C.c_double, C.POINTER(abi.Medium)])
     d("bielcc_planewave_in_medium", [C.POINTER(abi.Medium), C.c_double, C.POINTER(C.c_double),
                                      C.POINTER(C.c_double), C.c_int, C.c_int, C.POINTER(abi.PlaneWave)])
@@ -263,9 +263,11 @@ class Context:
         """Mixed batches contract moments and currents on the tensor cores or on the CUDA cores (default)."""
         _check(_lib.bielcc_ctx_set_batch_tensor_cores(self.h, int(bool(on))))
 
-    def set_batch_split(self, moments_bytes):
-        """Moments-buffer cap (bytes) of the split batched pipeline; 0 runs the fused kernel."""
-        _check(_lib.bielcc_ctx_set_batch_split(self.h, int(moments_bytes)))
+    def set_batch_split(self, moments_bytes, all_batches=False):
+        """Moments-buffer cap (bytes) of the split batched pipeline: batch plans
+        whose moments fit one wave keep them and replay only the contraction;
+        all_batches splits every mixed batch; 0 always runs the fused kernel."""
+        _check(_lib.bielcc_ctx_set_batch_split(self.h, int(moments_bytes), int(bool(all_batches))))
 
     def stats(self, reset=False):
         st = abi.Stats()

@@ -35,7 +35,7 @@ extern "C" {
 #pragma GCC visibility push(default)
 #endif
 
-#define BIELCC_ABI_VERSION 3
+#define BIELCC_ABI_VERSION 4
 
 /* ---- status codes ---------------------------------------------------- */
 #define BIELCC_OK                 0
@@ -147,14 +147,25 @@ int bielcc_ctx_set_timing(bielcc_ctx ctx, int on);
  * accurate on the batched workloads (the moments, not the contraction, bound
  * both forms). No counterpart in the reference. */
 int bielcc_ctx_set_batch_tensor_cores(bielcc_ctx ctx, int on);
-/* Mixed-precision batches with n_start <= 8 (and the CUDA-core contraction)
- * run as two kernels per wave of work items: the far moments of every
- * (point, cell) pair into a device buffer of at most moments_bytes (default
- * 16 GiB, part of the context's workspace), then their contraction with the
- * currents. Results are bit-identical to the fused kernel (moments_bytes = 0).
- * A batch plan whose moments fit one wave replays only the contraction. No
- * counterpart in the reference. */
-int bielcc_ctx_set_batch_split(bielcc_ctx ctx, int64_t moments_bytes);
+/* The split pipeline of mixed-precision batches (n_start <= 8): two kernels
+ * per wave of work items, the far moments of every (point, cell) pair into a
+ * device buffer of at most moments_bytes, then their contraction with the
+ * currents (on the CUDA cores, or on the tensor cores when
+ * bielcc_ctx_set_batch_tensor_cores is on).
+ *   - Batch plans (bielcc_batch_plan_create) use it when their moments fit
+ *     one wave of moments_bytes (default 16 GiB, held by the plan): the
+ *     moments depend on geometry and k only, so a replay with new currents
+ *     runs the contraction alone. Other plans run the fused kernel.
+ *   - all_batches = 1 also splits one-shot batches (bielcc_field_EH_batch,
+ *     single-job calls routed as one-job batches, served batches) and plans
+ *     of several waves; measured no faster than the fused kernel there
+ *     (0.99-1.04x), so the default is 0.
+ *   - moments_bytes = 0 never splits.
+ * With the CUDA-core contraction the results are bit-identical to the fused
+ * kernel; with the tensor-core contraction they agree with the fused
+ * tensor-core kernel within the mixed-precision tolerance (the moments kernel
+ * pairs cells in its node loop). No counterpart in the reference. */
+int bielcc_ctx_set_batch_split(bielcc_ctx ctx, int64_t moments_bytes, int all_batches);
 int bielcc_ctx_stats(bielcc_ctx ctx, bielcc_stats* out, int reset);
 
 /* Measured FMA throughput (TFLOP/s, 2 flops per FMA) of the current device's

@@ -97,12 +97,15 @@ SPLIT_DEFAULT = 16 << 30
 def test_batch_plan_graph_replay_with_new_currents(gctx, mode):
     """A planned batch replayed from its CUDA graph after the currents changed
     in place gives the same result as a fresh batched call with those
-    currents, and matches the oracle: the split pipeline (a plan of one wave
-    replays only the contraction), the fused kernel, the tensor-core form."""
+    currents, and matches the oracle: the split pipeline (a plan of one wave,
+    the default, keeps its moments and replays only the contraction, and the
+    fresh call runs the fused kernel; a plan of many waves with every batch
+    split), the fused kernel, the tensor-core forms."""
     torch = pytest.importorskip("torch")
     gctx.set_batch_tensor_cores("tensor cores" in mode)
-    gctx.set_batch_split({"split, one wave": SPLIT_DEFAULT, "split, many waves": 100_000,
-                          "split, tensor cores": SPLIT_DEFAULT}.get(mode, 0))
+    cap, every = {"split, one wave": (SPLIT_DEFAULT, False), "split, many waves": (100_000, True),
+                  "split, tensor cores": (SPLIT_DEFAULT, True)}.get(mode, (0, False))
+    gctx.set_batch_split(cap, all_batches=every)
     try:
         _plan_replay(torch, gctx)
     finally:
@@ -225,9 +228,13 @@ def test_batch_tensor_core_contraction_matches_cuda_cores(gctx):
 def test_batch_split_pipeline_equals_fused_kernel(gctx, cap, tensor_cores):
     """The split pipeline (moments to a device buffer, then the contraction on
     the CUDA or the tensor cores; one wave, or many waves of a small buffer)
-    gives bit-identical results to the fused kernel of the same contraction:
-    1 to 70 right-hand sides (the tensor cores: up to 64), quads and
-    triangles, real and complex k, near points."""
+    against the fused kernel of the same contraction: 1 to 70 right-hand sides
+    (the tensor cores: up to 64), quads and triangles, real and complex k,
+    near points. With the CUDA-core contraction the results are bit-identical.
+    The fused tensor-core kernel evaluates one cell per warp with that cell's
+    own phase polynomial, while the moments kernel pairs cells c and c + 4 of
+    each block under the polynomial of the larger phase range, so the
+    tensor-core forms agree within the mixed tolerance, not bit for bit."""
     torch = pytest.importorskip("torch")
     rng = np.random.default_rng(21)
     meshes = [W.uv_sphere(8, 16), W.perturbed_icosphere(2, seed=5), W.torus(24, 8), W.rounded_cube(6, 0.1, 1.0),
@@ -245,14 +252,17 @@ def test_batch_split_pipeline_equals_fused_kernel(gctx, cap, tensor_cores):
         gctx.set_batch_tensor_cores(tensor_cores)
         gctx.set_batch_split(0)
         fused, _ = _batch(torch, gctx, specs, "mixed")
-        gctx.set_batch_split(cap)
+        gctx.set_batch_split(cap, all_batches=True)
         split, rep = _batch(torch, gctx, specs, "mixed")
     finally:
         gctx.set_batch_split(SPLIT_DEFAULT)
         gctx.set_batch_tensor_cores(False)
     assert rep.n_near_pairs > 0
     for (E, H), (Ef, Hf) in zip(split, fused):
-        assert np.array_equal(E, Ef) and np.array_equal(H, Hf)
+        if tensor_cores:
+            assert rel_l2(E, Ef) < TOL_MIXED and rel_l2(H, Hf) < TOL_MIXED
+        else:
+            assert np.array_equal(E, Ef) and np.array_equal(H, Hf)
     sp = specs[2]
     Eo, Ho = oracle.field_EH(sp["cells"], sp["J"][:2], sp["k"], sp["pts"], mult=sp["mult"])
     assert rel_l2(split[2][0][:2], Eo) < TOL_MIXED and rel_l2(split[2][1][:2], Ho) < TOL_MIXED
