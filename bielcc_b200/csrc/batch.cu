@@ -128,12 +128,15 @@ BIELCC_D void contract12(const F* m, const F* jr, const F* ji, F* acc) {
 // the RHS sl = sl0 + step * j (j < R, sl < sp), two lanes of a packed
 // fma.rn.f32x2 per complex multiply-add: (mr + i mi)(jr + i ji) =
 // (mr, mr) * (jr, ji) + (-mi, mi) * (ji, jr). The currents are staged as
-// (re, im, im, re), so both operand pairs come from one 128-bit load.
+// (re, im, im, re), so both operand pairs come from one 128-bit load. The
+// accumulators are (re, im) pairs: E x, y, z then H x, y, z. ALL: every one of
+// the R right-hand sides is staged (no per-RHS test, so the R RHS's
+// multiply-add chains interleave freely).
 BIELCC_D float2 f2(float v) { return make_float2(v, v); }
 
-template <int R>
+template <int R, bool ALL>
 BIELCC_D void contract_packed_cell(const float* m, const float4* __restrict__ sj, int sl0, int step, int sp,
-                                   float (&acc)[R][12]) {
+                                   float2 (&acc)[R][6]) {
     float2 P[9], Q[9];  // T (6 entries), G (3): (mr, mr), (-mi, mi)
 #pragma unroll
     for (int q = 0; q < 6; q++) {
@@ -152,7 +155,7 @@ BIELCC_D void contract_packed_cell(const float* m, const float4* __restrict__ sj
 #pragma unroll
     for (int j = 0; j < R; j++) {
         const int sl = sl0 + step * j;
-        if (sl >= sp) continue;
+        if (!ALL && sl >= sp) continue;
         const float4* jj = sj + (size_t)sl * 3;
         float2 jp[3], js[3];
 #pragma unroll
@@ -163,27 +166,39 @@ BIELCC_D void contract_packed_cell(const float* m, const float4* __restrict__ sj
         }
 #pragma unroll
         for (int a = 0; a < 3; a++) {
-            float2 e = make_float2(acc[j][2 * a], acc[j][2 * a + 1]);
+            float2 e = acc[j][a];
 #pragma unroll
             for (int b = 0; b < 3; b++) {
                 e = __ffma2_rn(P[ti[a][b]], jp[b], e);
                 e = __ffma2_rn(Q[ti[a][b]], js[b], e);
             }
-            acc[j][2 * a] = e.x;
-            acc[j][2 * a + 1] = e.y;
+            acc[j][a] = e;
         }
 #pragma unroll
         for (int a = 0; a < 3; a++) {  // H_a = G_b J_c - G_c J_b
             const int b = (a + 1) % 3, c = (a + 2) % 3;
-            float2 h = make_float2(acc[j][6 + 2 * a], acc[j][7 + 2 * a]);
+            float2 h = acc[j][3 + a];
             h = __ffma2_rn(P[6 + b], jp[c], h);
             h = __ffma2_rn(Q[6 + b], js[c], h);
             h = __ffma2_rn(NP[c], jp[b], h);
             h = __ffma2_rn(NQ[c], js[b], h);
-            acc[j][6 + 2 * a] = h.x;
-            acc[j][7 + 2 * a] = h.y;
+            acc[j][3 + a] = h;
         }
     }
+}
+
+// One cell's 20 moments from the staged chunk (s_mom[cc][20][32]), A1 folded
+// onto T's diagonal (t_xx, t_yy, t_zz): W = A1 I + T.
+template <typename F>
+BIELCC_D void load_cell_moments(const F* s_mom, int cc, int lane, F (&m)[20]) {
+#pragma unroll
+    for (int q = 0; q < 20; q++) m[q] = s_mom[(cc * 20 + q) * kBP + lane];
+    m[2] += m[0];
+    m[3] += m[1];
+    m[8] += m[0];
+    m[9] += m[1];
+    m[12] += m[0];
+    m[13] += m[1];
 }
 
 // Moments of one cell, real-k form finished, times e^{ik r0} into mom[20];
@@ -310,6 +325,8 @@ BIELCC_D void batch_moments2(const float4* ndA, const float* yyA, const float4* 
 // Phase B of one chunk: the right-hand sides s0 + sb + warp + 4 j (j < R) of the
 // sp staged in s_j, contracted with the chunk's moments (s_mom[cc][20][32])
 // and added into the job's partial sums (stored by the item's first chunk).
+// A warp whose R right-hand sides are all staged runs the contraction without
+// per-RHS tests; a warp with none skips the chunk.
 template <bool MIXED>
 BIELCC_D void batch_phase_b(const typename BatchCfg<MIXED>::F* s_mom, const typename BatchCfg<MIXED>::F* s_j, int nc,
                             int s0, int sp, int warp, int lane, bool live, const JobDev& jb, int range, int S, int P,
@@ -317,29 +334,64 @@ BIELCC_D void batch_phase_b(const typename BatchCfg<MIXED>::F* s_mom, const type
     using C = BatchCfg<MIXED>;
     using F = typename C::F;
     for (int sb = 0; sb < sp; sb += kBW * C::R) {
-        F acc[C::R][12];
+        const int sl0 = sb + warp;
+        if (sl0 >= sp) break;  // warp-uniform: no staged RHS left for this warp
+        if constexpr (MIXED) {
+            float2 acc[C::R][6];
 #pragma unroll
-        for (int j = 0; j < C::R; j++)
+            for (int j = 0; j < C::R; j++)
 #pragma unroll
-            for (int q = 0; q < 12; q++) acc[j][q] = 0;
-        for (int cc = 0; cc < nc; cc++) {
-            F m[20];
-#pragma unroll
-            for (int q = 0; q < 20; q++) m[q] = s_mom[(cc * 20 + q) * kBP + lane];
-            // A1 I + T: A1 onto the diagonal t_xx, t_yy, t_zz
-            m[2] += m[0];
-            m[3] += m[1];
-            m[8] += m[0];
-            m[9] += m[1];
-            m[12] += m[0];
-            m[13] += m[1];
-            if constexpr (MIXED) {
-                contract_packed_cell<C::R>(m, reinterpret_cast<const float4*>(s_j) + (size_t)cc * kSP * 3, sb + warp,
-                                           kBW, sp, acc);
+                for (int q = 0; q < 6; q++) acc[j][q] = make_float2(0.f, 0.f);
+            const float4* sj = reinterpret_cast<const float4*>(s_j);
+            if (sl0 + kBW * (C::R - 1) < sp) {
+                for (int cc = 0; cc < nc; cc++) {
+                    float m[20];
+                    load_cell_moments<float>(s_mom, cc, lane, m);
+                    contract_packed_cell<C::R, true>(m, sj + (size_t)cc * kSP * 3, sl0, kBW, sp, acc);
+                }
             } else {
+                for (int cc = 0; cc < nc; cc++) {
+                    float m[20];
+                    load_cell_moments<float>(s_mom, cc, lane, m);
+                    contract_packed_cell<C::R, false>(m, sj + (size_t)cc * kSP * 3, sl0, kBW, sp, acc);
+                }
+            }
+            if (live) {
 #pragma unroll
                 for (int j = 0; j < C::R; j++) {
-                    const int sl = sb + warp + kBW * j;
+                    const int sl = sl0 + kBW * j;
+                    if (sl >= sp) continue;
+                    double* dst = jb.partial + (((size_t)range * S + (s0 + sl)) * 12) * (size_t)P + p;
+                    // one writer per address (this thread), so the adds land in chunk
+                    // order: the fire-and-forget reduction (no load to wait for) gives
+                    // the same sums as a load-add-store
+                    if (first) {
+#pragma unroll
+                        for (int q = 0; q < 6; q++) {
+                            dst[(size_t)(2 * q) * P] = (double)acc[j][q].x;
+                            dst[(size_t)(2 * q + 1) * P] = (double)acc[j][q].y;
+                        }
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < 6; q++) {
+                            atomicAdd(dst + (size_t)(2 * q) * P, (double)acc[j][q].x);
+                            atomicAdd(dst + (size_t)(2 * q + 1) * P, (double)acc[j][q].y);
+                        }
+                    }
+                }
+            }
+        } else {
+            F acc[C::R][12];
+#pragma unroll
+            for (int j = 0; j < C::R; j++)
+#pragma unroll
+                for (int q = 0; q < 12; q++) acc[j][q] = 0;
+            for (int cc = 0; cc < nc; cc++) {
+                F m[20];
+                load_cell_moments<F>(s_mom, cc, lane, m);
+#pragma unroll
+                for (int j = 0; j < C::R; j++) {
+                    const int sl = sl0 + kBW * j;
                     if (sl < sp) {
                         const F* jj = s_j + (size_t)(cc * kSP + sl) * 6;
                         const F jr[3] = {jj[0], jj[2], jj[4]}, ji[3] = {jj[1], jj[3], jj[5]};
@@ -347,22 +399,19 @@ BIELCC_D void batch_phase_b(const typename BatchCfg<MIXED>::F* s_mom, const type
                     }
                 }
             }
-        }
-        if (live) {
+            if (live) {
 #pragma unroll
-            for (int j = 0; j < C::R; j++) {
-                const int sl = sb + warp + kBW * j;
-                if (sl >= sp) continue;
-                double* dst = jb.partial + (((size_t)range * S + (s0 + sl)) * 12) * (size_t)P + p;
-                // one writer per address (this thread), so the adds land in chunk
-                // order: the fire-and-forget reduction (no load to wait for) gives
-                // the same sums as a load-add-store
-                if (first) {
+                for (int j = 0; j < C::R; j++) {
+                    const int sl = sl0 + kBW * j;
+                    if (sl >= sp) continue;
+                    double* dst = jb.partial + (((size_t)range * S + (s0 + sl)) * 12) * (size_t)P + p;
+                    if (first) {
 #pragma unroll
-                    for (int q = 0; q < 12; q++) dst[(size_t)q * P] = (double)acc[j][q];
-                } else {
+                        for (int q = 0; q < 12; q++) dst[(size_t)q * P] = (double)acc[j][q];
+                    } else {
 #pragma unroll
-                    for (int q = 0; q < 12; q++) atomicAdd(dst + (size_t)q * P, (double)acc[j][q]);
+                        for (int q = 0; q < 12; q++) atomicAdd(dst + (size_t)q * P, (double)acc[j][q]);
+                    }
                 }
             }
         }
@@ -380,12 +429,12 @@ BIELCC_D void batch_stage_j(typename BatchCfg<MIXED>::F* s_j, const JobDev& jb, 
     for (int i = tid; i < nc * sp * 3; i += kBT) {
         const int cc = i / (sp * 3), rem = i - cc * sp * 3, sl = rem / 3, g = rem - sl * 3;
         const cplx v = jb.J[((size_t)(s0 + sl) * N + (c0 + cc)) * 3 + g];
-        F* d = s_j + ((size_t)(cc * kSP + sl) * 3 + g) * C::JW;
-        d[0] = (F)v.re;
-        d[1] = (F)v.im;
-        if constexpr (MIXED) {
-            d[2] = (F)v.im;
-            d[3] = (F)v.re;
+        const size_t e = (size_t)(cc * kSP + sl) * 3 + g;
+        if constexpr (MIXED) {  // one 128-bit store: (re, im, im, re)
+            const float re = (float)v.re, im = (float)v.im;
+            reinterpret_cast<float4*>(s_j)[e] = make_float4(re, im, im, re);
+        } else {
+            reinterpret_cast<double2*>(s_j)[e] = make_double2(v.re, v.im);
         }
     }
 }
@@ -674,6 +723,12 @@ __global__ void __launch_bounds__(kBT, BIELCC_MOM_MINB)
     }
 }
 
+// Bulk prefetch of [p, p + bytes) into L2 (p and bytes multiples of 16; a hint:
+// no completion to wait for).
+BIELCC_D void prefetch_l2_bulk(const void* p, unsigned bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 // Phase B of the split pipeline: per 16-cell chunk of an item, its moments
 // (written by batch_moments_kernel) and the currents are staged and
 // contracted exactly as in batch_far_kernel<true>.
@@ -717,6 +772,11 @@ __global__ void __launch_bounds__(kBT, BIELCC_CON_MINB)
             }
             batch_stage_j<true>(s_j, jb, c0, nc, 0, min(kSP, S), threadIdx.x);
             __syncthreads();
+            // the next chunk of the item streams from HBM into L2 while this one is contracted
+            if (threadIdx.x == 0 && c0 + kConCells < ce) {
+                const int nc2 = min(kConCells, ce - c0 - kConCells);
+                prefetch_l2_bulk(mo + (size_t)(c0 + kConCells - cb) * 20 * kBP, (unsigned)(nc2 * 20 * kBP * sizeof(float)));
+            }
             batch_phase_b<true>(s_mom, s_j, nc, 0, min(kSP, S), warp, lane, live, jb, bi.range, S, P, p, c0 == cb);
             // further RHS passes reuse the chunk's moments in shared memory
             for (int s0 = kSP; s0 < S; s0 += kSP) {
