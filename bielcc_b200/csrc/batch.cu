@@ -152,37 +152,46 @@ BIELCC_D void contract_packed_cell(const float* m, const float4* __restrict__ sj
         NQ[q] = make_float2(m[15 + 2 * q], -m[15 + 2 * q]);
     }
     const int ti[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+    // Component b of the currents of all R right-hand sides at a time: every
+    // accumulator takes one multiply-add in turn, so consecutive multiply-adds
+    // into one accumulator are 12 (E) or 8 (H) instructions apart.
 #pragma unroll
-    for (int j = 0; j < R; j++) {
-        const int sl = sl0 + step * j;
-        if (!ALL && sl >= sp) continue;
-        const float4* jj = sj + (size_t)sl * 3;
-        float2 jp[3], js[3];
+    for (int b = 0; b < 3; b++) {
+        float2 jp[R], js[R];
 #pragma unroll
-        for (int b = 0; b < 3; b++) {
-            const float4 v = jj[b];
-            jp[b] = make_float2(v.x, v.y);
-            js[b] = make_float2(v.z, v.w);
+        for (int j = 0; j < R; j++) {
+            if (!ALL && sl0 + step * j >= sp) continue;
+            const float4 v = sj[(size_t)(sl0 + step * j) * 3 + b];
+            jp[j] = make_float2(v.x, v.y);
+            js[j] = make_float2(v.z, v.w);
+        }
+        // E_a += W_ab J_b: the (mr, mr) halves, then the (-mi, mi) halves
+#pragma unroll
+        for (int j = 0; j < R; j++) {
+            if (!ALL && sl0 + step * j >= sp) continue;
+#pragma unroll
+            for (int a = 0; a < 3; a++) acc[j][a] = __ffma2_rn(P[ti[a][b]], jp[j], acc[j][a]);
         }
 #pragma unroll
-        for (int a = 0; a < 3; a++) {
-            float2 e = acc[j][a];
+        for (int j = 0; j < R; j++) {
+            if (!ALL && sl0 + step * j >= sp) continue;
 #pragma unroll
-            for (int b = 0; b < 3; b++) {
-                e = __ffma2_rn(P[ti[a][b]], jp[b], e);
-                e = __ffma2_rn(Q[ti[a][b]], js[b], e);
-            }
-            acc[j][a] = e;
+            for (int a = 0; a < 3; a++) acc[j][a] = __ffma2_rn(Q[ti[a][b]], js[j], acc[j][a]);
+        }
+        // H_a = G_(a+1) J_(a+2) - G_(a+2) J_(a+1): J_b adds G_(b+2) J_b to
+        // H_(b+1) and takes G_(b+1) J_b from H_(b+2)
+        const int a1 = (b + 1) % 3, a2 = (b + 2) % 3;
+#pragma unroll
+        for (int j = 0; j < R; j++) {
+            if (!ALL && sl0 + step * j >= sp) continue;
+            acc[j][3 + a1] = __ffma2_rn(P[6 + a2], jp[j], acc[j][3 + a1]);
+            acc[j][3 + a2] = __ffma2_rn(NP[a1], jp[j], acc[j][3 + a2]);
         }
 #pragma unroll
-        for (int a = 0; a < 3; a++) {  // H_a = G_b J_c - G_c J_b
-            const int b = (a + 1) % 3, c = (a + 2) % 3;
-            float2 h = acc[j][3 + a];
-            h = __ffma2_rn(P[6 + b], jp[c], h);
-            h = __ffma2_rn(Q[6 + b], js[c], h);
-            h = __ffma2_rn(NP[c], jp[b], h);
-            h = __ffma2_rn(NQ[c], js[b], h);
-            acc[j][3 + a] = h;
+        for (int j = 0; j < R; j++) {
+            if (!ALL && sl0 + step * j >= sp) continue;
+            acc[j][3 + a1] = __ffma2_rn(Q[6 + a2], js[j], acc[j][3 + a1]);
+            acc[j][3 + a2] = __ffma2_rn(NQ[a1], js[j], acc[j][3 + a2]);
         }
     }
 }
