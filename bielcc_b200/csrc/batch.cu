@@ -336,38 +336,42 @@ BIELCC_D void batch_moments2(const float4* ndA, const float* yyA, const float4* 
 // and added into the job's partial sums (stored by the item's first chunk).
 // A warp whose R right-hand sides are all staged runs the contraction without
 // per-RHS tests; a warp with none skips the chunk.
-template <bool MIXED>
+// R: right-hand sides per thread; SP: right-hand sides per staged pass (the
+// stride of s_j). Neither changes any sum: each RHS's chunk sum takes its
+// cells in order, whatever the grouping.
+template <bool MIXED, int R = BatchCfg<MIXED>::R, int SP = kSP>
 BIELCC_D void batch_phase_b(const typename BatchCfg<MIXED>::F* s_mom, const typename BatchCfg<MIXED>::F* s_j, int nc,
                             int s0, int sp, int warp, int lane, bool live, const JobDev& jb, int range, int S, int P,
                             int p, bool first) {
     using C = BatchCfg<MIXED>;
     using F = typename C::F;
-    for (int sb = 0; sb < sp; sb += kBW * C::R) {
+    static_assert(SP % (kBW * R) == 0, "a phase-B pass covers whole groups of kBW x R RHS");
+    for (int sb = 0; sb < sp; sb += kBW * R) {
         const int sl0 = sb + warp;
         if (sl0 >= sp) break;  // warp-uniform: no staged RHS left for this warp
         if constexpr (MIXED) {
-            float2 acc[C::R][6];
+            float2 acc[R][6];
 #pragma unroll
-            for (int j = 0; j < C::R; j++)
+            for (int j = 0; j < R; j++)
 #pragma unroll
                 for (int q = 0; q < 6; q++) acc[j][q] = make_float2(0.f, 0.f);
             const float4* sj = reinterpret_cast<const float4*>(s_j);
-            if (sl0 + kBW * (C::R - 1) < sp) {
+            if (sl0 + kBW * (R - 1) < sp) {
                 for (int cc = 0; cc < nc; cc++) {
                     float m[20];
                     load_cell_moments<float>(s_mom, cc, lane, m);
-                    contract_packed_cell<C::R, true>(m, sj + (size_t)cc * kSP * 3, sl0, kBW, sp, acc);
+                    contract_packed_cell<R, true>(m, sj + (size_t)cc * SP * 3, sl0, kBW, sp, acc);
                 }
             } else {
                 for (int cc = 0; cc < nc; cc++) {
                     float m[20];
                     load_cell_moments<float>(s_mom, cc, lane, m);
-                    contract_packed_cell<C::R, false>(m, sj + (size_t)cc * kSP * 3, sl0, kBW, sp, acc);
+                    contract_packed_cell<R, false>(m, sj + (size_t)cc * SP * 3, sl0, kBW, sp, acc);
                 }
             }
             if (live) {
 #pragma unroll
-                for (int j = 0; j < C::R; j++) {
+                for (int j = 0; j < R; j++) {
                     const int sl = sl0 + kBW * j;
                     if (sl >= sp) continue;
                     double* dst = jb.partial + (((size_t)range * S + (s0 + sl)) * 12) * (size_t)P + p;
@@ -390,19 +394,19 @@ BIELCC_D void batch_phase_b(const typename BatchCfg<MIXED>::F* s_mom, const type
                 }
             }
         } else {
-            F acc[C::R][12];
+            F acc[R][12];
 #pragma unroll
-            for (int j = 0; j < C::R; j++)
+            for (int j = 0; j < R; j++)
 #pragma unroll
                 for (int q = 0; q < 12; q++) acc[j][q] = 0;
             for (int cc = 0; cc < nc; cc++) {
                 F m[20];
                 load_cell_moments<F>(s_mom, cc, lane, m);
 #pragma unroll
-                for (int j = 0; j < C::R; j++) {
+                for (int j = 0; j < R; j++) {
                     const int sl = sl0 + kBW * j;
                     if (sl < sp) {
-                        const F* jj = s_j + (size_t)(cc * kSP + sl) * 6;
+                        const F* jj = s_j + (size_t)(cc * SP + sl) * 6;
                         const F jr[3] = {jj[0], jj[2], jj[4]}, ji[3] = {jj[1], jj[3], jj[5]};
                         contract12<F>(m, jr, ji, acc[j]);
                     }
@@ -410,7 +414,7 @@ BIELCC_D void batch_phase_b(const typename BatchCfg<MIXED>::F* s_mom, const type
             }
             if (live) {
 #pragma unroll
-                for (int j = 0; j < C::R; j++) {
+                for (int j = 0; j < R; j++) {
                     const int sl = sl0 + kBW * j;
                     if (sl >= sp) continue;
                     double* dst = jb.partial + (((size_t)range * S + (s0 + sl)) * 12) * (size_t)P + p;
@@ -428,8 +432,9 @@ BIELCC_D void batch_phase_b(const typename BatchCfg<MIXED>::F* s_mom, const type
 }
 
 // Stages the currents of RHS s0 .. s0 + sp - 1 of cells c0 .. c0 + nc - 1
-// (FP32 (re, im, im, re) for the packed contraction; FP64 (re, im)).
-template <bool MIXED>
+// (FP32 (re, im, im, re) for the packed contraction; FP64 (re, im)); SP: the
+// staging stride in right-hand sides.
+template <bool MIXED, int SP = kSP>
 BIELCC_D void batch_stage_j(typename BatchCfg<MIXED>::F* s_j, const JobDev& jb, int c0, int nc, int s0, int sp,
                             int tid) {
     using C = BatchCfg<MIXED>;
@@ -438,7 +443,7 @@ BIELCC_D void batch_stage_j(typename BatchCfg<MIXED>::F* s_j, const JobDev& jb, 
     for (int i = tid; i < nc * sp * 3; i += kBT) {
         const int cc = i / (sp * 3), rem = i - cc * sp * 3, sl = rem / 3, g = rem - sl * 3;
         const cplx v = jb.J[((size_t)(s0 + sl) * N + (c0 + cc)) * 3 + g];
-        const size_t e = (size_t)(cc * kSP + sl) * 3 + g;
+        const size_t e = (size_t)(cc * SP + sl) * 3 + g;
         if constexpr (MIXED) {  // one 128-bit store: (re, im, im, re)
             const float re = (float)v.re, im = (float)v.im;
             reinterpret_cast<float4*>(s_j)[e] = make_float4(re, im, im, re);
@@ -741,18 +746,26 @@ BIELCC_D void prefetch_l2_bulk(const void* p, unsigned bytes) {
 // Phase B of the split pipeline: per 16-cell chunk of an item, its moments
 // (written by batch_moments_kernel) and the currents are staged and
 // contracted exactly as in batch_far_kernel<true>.
+// It holds no phase-A state, so it can afford more right-hand sides per thread
+// (kConR, staged kConSP at a time) than the fused kernel: each cell's moments
+// are loaded from shared memory once per kConR RHS.
 constexpr int kConCells = 16;
-constexpr size_t kConSmem = sizeof(float) * kConCells * 20 * kBP + sizeof(float) * 4 * kConCells * kSP * 3;
+#ifndef BIELCC_CON_R
+#define BIELCC_CON_R 4
+#endif
 #ifndef BIELCC_CON_MINB
 #define BIELCC_CON_MINB 4
 #endif
+constexpr int kConR = BIELCC_CON_R;
+constexpr int kConSP = kBW * kConR * (kSP / (kBW * BatchCfg<true>::R) > 1 ? kSP / (kBW * BatchCfg<true>::R) : 1);
+constexpr size_t kConSmem = sizeof(float) * kConCells * 20 * kBP + sizeof(float) * 4 * kConCells * kConSP * 3;
 
 __global__ void __launch_bounds__(kBT, BIELCC_CON_MINB)
     batch_contract_kernel(const JobDev* __restrict__ jobs, const BatchItem* __restrict__ items, int n_items,
                           int* __restrict__ counter, int max_items, const float* __restrict__ mom) {
     extern __shared__ __align__(16) unsigned char smem[];
     float* s_mom = (float*)smem;               // [16][20][kBP]
-    float* s_j = s_mom + kConCells * 20 * kBP;  // [16][kSP][3][4]
+    float* s_j = s_mom + kConCells * 20 * kBP;  // [16][kConSP][3][4]
     __shared__ int s_item;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
@@ -779,21 +792,22 @@ __global__ void __launch_bounds__(kBT, BIELCC_CON_MINB)
                 float4* dst = reinterpret_cast<float4*>(s_mom);
                 for (int i = threadIdx.x; i < nc * 20 * kBP / 4; i += kBT) dst[i] = __ldcs(src + i);
             }
-            batch_stage_j<true>(s_j, jb, c0, nc, 0, min(kSP, S), threadIdx.x);
+            batch_stage_j<true, kConSP>(s_j, jb, c0, nc, 0, min(kConSP, S), threadIdx.x);
             __syncthreads();
             // the next chunk of the item streams from HBM into L2 while this one is contracted
             if (threadIdx.x == 0 && c0 + kConCells < ce) {
                 const int nc2 = min(kConCells, ce - c0 - kConCells);
                 prefetch_l2_bulk(mo + (size_t)(c0 + kConCells - cb) * 20 * kBP, (unsigned)(nc2 * 20 * kBP * sizeof(float)));
             }
-            batch_phase_b<true>(s_mom, s_j, nc, 0, min(kSP, S), warp, lane, live, jb, bi.range, S, P, p, c0 == cb);
+            batch_phase_b<true, kConR, kConSP>(s_mom, s_j, nc, 0, min(kConSP, S), warp, lane, live, jb, bi.range, S,
+                                               P, p, c0 == cb);
             // further RHS passes reuse the chunk's moments in shared memory
-            for (int s0 = kSP; s0 < S; s0 += kSP) {
+            for (int s0 = kConSP; s0 < S; s0 += kConSP) {
                 __syncthreads();
-                batch_stage_j<true>(s_j, jb, c0, nc, s0, min(kSP, S - s0), threadIdx.x);
+                batch_stage_j<true, kConSP>(s_j, jb, c0, nc, s0, min(kConSP, S - s0), threadIdx.x);
                 __syncthreads();
-                batch_phase_b<true>(s_mom, s_j, nc, s0, min(kSP, S - s0), warp, lane, live, jb, bi.range, S, P, p,
-                                    c0 == cb);
+                batch_phase_b<true, kConR, kConSP>(s_mom, s_j, nc, s0, min(kConSP, S - s0), warp, lane, live, jb,
+                                                   bi.range, S, P, p, c0 == cb);
             }
         }
     }
