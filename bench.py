@@ -61,6 +61,7 @@ def parse():
     ap.add_argument("--no-assembly", action="store_true", help="skip the 20,480-triangle assembly leg")
     ap.add_argument("--assembly-level", type=int, default=5, help="icosphere level of the assembly leg (5: 20,480)")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream leg")
+    ap.add_argument("--no-adaptive", action="store_true", help="skip the adaptive-quadrature (p_max = 2) leg")
     ap.add_argument("--tensor-cores", action="store_true",
                     help="mixed batches contract on the tensor cores (bielcc_ctx_set_batch_tensor_cores(ctx, 1))")
     ap.add_argument("--small", action="store_true",
@@ -463,6 +464,73 @@ def run_plan_moments_kept(ctx, torch, stream, flush, jobs_np, specs, outs, steps
             "replay_speedup": ms_fresh / ms_replay, "replay_identical_to_fresh_batch": identical,
             "what": "plan of the first jobs whose far moments fit 16 GiB; a replay contracts the kept moments "
                     "with the currents in place and finalizes"}
+
+
+def run_adaptive(ctx, torch, dev, stream, flush, wl, cpu_threads):
+    """Adaptive quadrature, p_max = 2 (the reference's refinement loop), on the
+    headline geometry: the 8192-quad sphere, k = 2 pi, every 10th point of the
+    headline set (1800 far, 200 near-field), 1 RHS. With p_max = 2 a far pair's
+    result is the pass at 2 n_start, so the far part runs on the table-driven
+    kernels at n = 16 (256 nodes per cell); near pairs take the full
+    refinement schedule. GPU FP64 and mixed are timed with CUDA events on
+    device buffers; the compiled reference times a 22-point sample on the host
+    cores, and the GPU's FP64 result is checked against it there."""
+    import oracle
+    from bielcc_b200 import abi
+
+    cells, J, k, pts_all = wl["cells"], wl["J"], wl["k"], wl["pts"]
+    pts = np.ascontiguousarray(np.concatenate([pts_all[:18000:10], pts_all[18000::10]]))
+    npm = abi.NumParam.default(p_max=2, p_max_seg=2)
+    mesh = ctx.mesh(cells)
+    P, S, N = len(pts), J.shape[0], len(cells)
+    Jd = torch.from_numpy(np.ascontiguousarray(J)).to(dev)
+    Pd = torch.from_numpy(pts).to(dev)
+    Ed = torch.empty((S, P, 3), dtype=torch.complex128, device=dev)
+    Hd = torch.empty_like(Ed)
+    sc = stream.cuda_stream
+
+    def timed(prec, n):
+        def call():
+            ctx.field_EH_device(mesh, Jd.data_ptr(), k, Pd.data_ptr(), Ed.data_ptr(), Hd.data_ptr(), S, P,
+                                numparam=npm, precision=prec, stream=sc, report=False)
+        call()  # warm-up (and the n = 16 node tables)
+        t = 0.0
+        for _ in range(n):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            call()
+            b.record(stream)
+            b.synchronize()
+            t += a.elapsed_time(b)
+        return t / n
+
+    ms64 = timed("fp64", 3)
+    E64, H64 = Ed.cpu().numpy(), Hd.cpu().numpy()
+    msmx = timed("mixed", 3)
+    Em, Hm = Ed.cpu().numpy(), Hd.cpu().numpy()
+    rel_mx = float(np.sqrt((np.sum(np.abs(Em - E64) ** 2) + np.sum(np.abs(Hm - H64) ** 2)) /
+                           (np.sum(np.abs(E64) ** 2) + np.sum(np.abs(H64) ** 2))))
+    idx = list(range(20)) + [1800, 1801]  # 20 far + 2 near-field points
+    which = "ref" if oracle.available("ref") else "port"
+    t0 = time.perf_counter()
+    Eo, Ho = oracle.field_EH(cells, J, k, pts[idx], npm, n_threads=cpu_threads, which=which)
+    dt = time.perf_counter() - t0
+    rel_ref = float(np.sqrt((np.sum(np.abs(E64[:, idx] - Eo) ** 2) + np.sum(np.abs(H64[:, idx] - Ho) ** 2)) /
+                            (np.sum(np.abs(Eo) ** 2) + np.sum(np.abs(Ho) ** 2))))
+    mesh.close()
+    pairs = P * N * S
+    cpu_value = len(idx) * N * S / dt
+    return {"workload": f"sphere{N}_k2pi, {P} points (1800 far, 200 near-field), 1 RHS, p_max = 2 "
+                        "(n_start 8, n_start_seg 10, p_max_seg 2)",
+            "unit": "pairs/s", "value": pairs / (msmx * 1e-3), "ms": msmx, "rel_l2_vs_fp64": rel_mx,
+            "fp64_value": pairs / (ms64 * 1e-3), "fp64_ms": ms64,
+            "fp64_rel_l2_vs_cpu_reference": rel_ref,
+            "cpu_reference": {"value": cpu_value, "unit": "pairs/s", "cores": cpu_threads,
+                              "kind": "reference" if which == "ref" else "port",
+                              "sample": f"{len(idx)} points (2 near-field) x {N} cells x {S} RHS, {dt:.1f} s"},
+            "far_pass": "table-driven far kernels at n = 16 (the pass p_max = 2 returns)"}
 
 
 def run_assembly(args, ctx, torch, dev, stream, flush):
@@ -902,6 +970,9 @@ def run_ours(args, ws, rank, local):
     assembly = None
     if not args.no_assembly:
         assembly = run_assembly(args, ctx, torch, dev, stream, flush)
+    adaptive = None
+    if not args.no_adaptive and not args.small and rank == 0:
+        adaptive = run_adaptive(ctx, torch, dev, stream, flush, wl, os.cpu_count() or 1)
     serving = None
     if not args.no_serving and rank == 0:
         serving = run_serving(args, ctx, torch, dev, stream, batched["autotuned_item_cost"] if batched else None)
@@ -940,6 +1011,7 @@ def run_ours(args, ws, rank, local):
         "near_pairs_per_step": int(last["rep"].n_near_pairs),
         "batched": batched,
         "assembly": assembly,
+        "adaptive": adaptive,
         "serving": serving,
     }
     if rank == 0:

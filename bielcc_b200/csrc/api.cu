@@ -325,7 +325,7 @@ int field_begin(bielcc_ctx ctx, const FieldArgs& a, cudaStream_t s, bielcc_repor
     p->a = a;
     TRY(field_device_batched(ctx, a, s, rep, d_nonfinite, &p->batched, w));
     if (p->batched) return BIELCC_OK;
-    TRY(ensure_tables(a.m, a.np.n_start, s));
+    TRY(ensure_tables(a.m, far_split_n(a.np), s));
     FieldLaunch& f = p->f;
     f.mesh = a.m;
     f.pts = a.pts;
@@ -444,7 +444,7 @@ int est_single_begin(bielcc_ctx ctx, const FieldArgs& a, cudaStream_t s, SingleE
     j.H = H_out;
     j.Eq = e.full ? e.Ec : e.Eq;
     j.Hq = H_out ? (e.full ? e.Hc : e.Hq) : nullptr;
-    TRY(ensure_tables(a.m, a.np.n_start, s));
+    TRY(ensure_tables(a.m, far_split_n(a.np), s));
     TRY_CUDA(cudaEventRecord(ctx->side_in, s));  // inputs and node tables on the device
     TRY_CUDA(cudaStreamWaitEvent(ctx->side, ctx->side_in, 0));
     TRY_CUDA(cudaMemcpyAsync(e.d_job, &j, sizeof(j), cudaMemcpyHostToDevice, ctx->side));
@@ -1587,7 +1587,7 @@ int bielcc_assemble_K_device(bielcc_ctx ctx, bielcc_mesh mesh, double k_re, doub
     if (!A_dev) return set_error(BIELCC_ERR_ARG, "null matrix");
     cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
     TRY(ws_acquire(ctx, s));
-    TRY(ensure_tables(m, n.n_start, s));
+    TRY(ensure_tables(m, far_split_n(n), s));
     AssembleLaunch a{m, mk(k_re, k_im), n, layout, out_c64 ? 1 : 0, precision, A_dev};
     TRY(ctx->ws.ensure(assemble_ws_base_bytes(a)));
     TRY(ctx->scratch_small.ensure(256));

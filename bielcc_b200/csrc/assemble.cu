@@ -339,7 +339,7 @@ __global__ void __launch_bounds__(kAsmThreads, (!CK && MIXED) ? BIELCC_ASM_MINB 
     }
 }
 
-// Far entries with adaptive refinement (p_max > 1): K_RotRot_Far's
+// Far entries with adaptive refinement (p_max > 2): K_RotRot_Far's
 // convergence depends on the current, so each column basis vector runs its
 // own adaptive quadrature (generic per-pair code, nodes on the fly).
 __global__ void assemble_far_adaptive_kernel(AsmArgs a, const double* __restrict__ verts, int nv, DNP np) {
@@ -576,7 +576,7 @@ size_t assemble_ws_base_bytes(const AssembleLaunch& a) {
 
 // The far kernel writes the near mask (and count / fill read it) unless the
 // adaptive far kernel runs, which tests pairs on its own.
-static bool uses_mask(const AssembleLaunch& a) { return a.np.p_max <= 1; }
+static bool uses_mask(const AssembleLaunch& a) { return !far_adaptive(a.np); }
 
 static AsmArgs make_args(const AssembleLaunch& a) {
     const MeshDev& m = *a.mesh;
@@ -586,7 +586,7 @@ static AsmArgs make_args(const AssembleLaunch& a) {
     g.nodes64 = m.nodes64;
     g.nodes32 = m.nodes32;
     g.rho32 = m.rho32;
-    g.nn = a.np.n_start * a.np.n_start;
+    g.nn = far_split_n(a.np) * far_split_n(a.np);
     g.k = a.k;
     g.analytic_calc = a.np.analytic_calc;
     g.m = a.layout == 1 ? 3 : 2;
@@ -628,10 +628,12 @@ cudaError_t assemble_stage1(const AssembleLaunch& a, void* ws, long long* d_tota
     int tiles = (N + kAsmThreads - 1) / kAsmThreads;
     bool ck = a.k.im != 0.;
     // column splits in whole 32-column words, so every mask word has one writer
-    int splits = choose_cell_splits(tiles, N, asm_slots(ck, a.precision == 1, a.np.p_max > 1), N);
+    if (!far_adaptive(a.np) && m.table_n != far_split_n(a.np))
+        return cudaErrorInvalidValue;  // node tables of another split: the caller builds far_split_n's
+    int splits = choose_cell_splits(tiles, N, asm_slots(ck, a.precision == 1, far_adaptive(a.np)), N);
     g.cols_per_split = round_cells_per_split(N, splits);
     dim3 grid(tiles, splits);
-    if (a.np.p_max > 1) {
+    if (far_adaptive(a.np)) {
         DNP np{a.np.eps, a.np.rs, a.np.rs_seg, a.np.analytic_calc, a.np.n_start, a.np.n_start_seg, a.np.p_max,
                a.np.p_max_seg};
         assemble_far_adaptive_kernel<<<grid, kAsmThreads, 0, s>>>(g, m.verts, m.nv, np);

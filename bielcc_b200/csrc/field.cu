@@ -328,7 +328,7 @@ __global__ void BIELCC_FAR_BOUNDS(NRHS, CK, MIXED) far_kernel(FarArgs a) {
     }
 }
 
-// Far pairs with adaptive refinement (p_max > 1): the reference's
+// Far pairs with adaptive refinement (p_max > 2): the reference's
 // convergence test of K_RotRot_Far runs on F_RotRotSimplePot_H . J, so the
 // refinement depth depends on the current; one RHS per launch, generic
 // per-pair quadrature with nodes generated on the fly (ops.cuh). R_Rot_Colloc
@@ -627,7 +627,7 @@ size_t field_ws_base_bytes(const FieldLaunch& f, int* splits_out, size_t partial
     const int N = f.mesh->n_cells;
     const size_t P = f.n_pts;
     const size_t per_split = (size_t)f.n_rhs * 12 * P * sizeof(double);
-    const int slots = far_slots(f.n_rhs, f.k.im != 0.0, f.precision == 1, f.np.p_max > 1);
+    const int slots = far_slots(f.n_rhs, f.k.im != 0.0, f.precision == 1, far_adaptive(f.np));
     const int max_splits = (int)std::max<size_t>(1, partial_cap / std::max<size_t>(1, per_split));
     const int splits = choose_cell_splits(tiles, N, slots, max_splits);
     *splits_out = splits;
@@ -676,7 +676,7 @@ cudaError_t field_stage1(const FieldLaunch& f, void* ws, int splits, long long* 
     a.nodes64 = m.nodes64;
     a.nodes32 = m.nodes32;
     a.rho32 = m.rho32;
-    a.nn = f.np.n_start * f.np.n_start;
+    a.nn = far_split_n(f.np) * far_split_n(f.np);
     a.J = reinterpret_cast<const cplx*>(f.J);
     a.n_rhs = f.n_rhs;
     a.rhs0 = 0;
@@ -690,7 +690,9 @@ cudaError_t field_stage1(const FieldLaunch& f, void* ws, int splits, long long* 
     bool mixed = f.precision == 1;
     int nl = 0;
     if (far_begin) cudaEventRecord(far_begin, s);
-    if (tiles > 0 && f.np.p_max > 1) {
+    if (tiles > 0 && !far_adaptive(f.np) && m.table_n != far_split_n(f.np))
+        return cudaErrorInvalidValue;  // node tables of another split: the caller builds far_split_n's
+    if (tiles > 0 && far_adaptive(f.np)) {
         DNP np{f.np.eps, f.np.rs, f.np.rs_seg, f.np.analytic_calc, f.np.n_start, f.np.n_start_seg, f.np.p_max,
                f.np.p_max_seg};
         for (int r = 0; r < f.n_rhs; r++, nl++) {

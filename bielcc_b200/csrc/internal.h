@@ -22,6 +22,18 @@ struct NumParamH {
     int n_start, n_start_seg, p_max, p_max_seg;
 };
 
+// Node split of the far pass. The reference's adaptive quadrature
+// (IntegralUniversalPnt, integral_universal.h:58-119 quads, :160-219
+// triangles) returns the last pass it computed once p_max passes are spent,
+// and the far operators run it with the smoothing radius at its floor
+// (K_RotRot_Far, K.h:293-295; R_Rot_Colloc, R.h:101-102), so it never halves.
+// With p_max = 2 a far pair's result is therefore the pass at 2 n_start,
+// whatever the convergence test decides: the table-driven far kernels
+// evaluate that pass alone. p_max >= 3 keeps the per-pair convergence test
+// (the adaptive far kernels). Near pairs always take the full schedule.
+inline int far_split_n(const NumParamH& np) { return np.p_max == 2 ? 2 * np.n_start : np.n_start; }
+inline bool far_adaptive(const NumParamH& np) { return np.p_max > 2; }
+
 // Device-resident mesh with its per-cell geometry and cached node tables.
 struct MeshDev {
     int nv = 0, n_cells = 0;

@@ -81,7 +81,8 @@ extern "C" int bielcc_field_EH_noalloc(int n_vert, int n_cells, const double* ce
     cudaStream_t s = (cudaStream_t)stream;
 
     // carve the static array: cell rows, node tables, then the field workspace
-    const size_t N = n_cells, nn = (size_t)n.n_start * n.n_start;
+    // node tables of the far pass's split (2 n_start when p_max = 2)
+    const size_t N = n_cells, nn = (size_t)far_split_n(n) * far_split_n(n);
     MeshDev m;
     m.nv = n_vert;
     m.n_cells = n_cells;
@@ -98,7 +99,7 @@ extern "C" int bielcc_field_EH_noalloc(int n_vert, int n_cells, const double* ce
     off += b_n32;
     m.rho32 = (float*)(sp + off);
     off += b_rho;
-    m.table_n = n.n_start;
+    m.table_n = far_split_n(n);
 
     FieldLaunch f;
     f.mesh = &m;
@@ -143,7 +144,7 @@ extern "C" int bielcc_field_EH_noalloc(int n_vert, int n_cells, const double* ce
 
     cudaError_t e = launch_cell_geometry(m.verts, n_vert, n_cells, m.geo, s);
     if (e == cudaSuccess)
-        e = launch_node_tables(m.verts, m.geo, n_vert, n_cells, n.n_start, m.nodes64, m.nodes32, m.rho32, s);
+        e = launch_node_tables(m.verts, m.geo, n_vert, n_cells, far_split_n(n), m.nodes64, m.nodes32, m.rho32, s);
     int l1 = 0, lf = 0, l2 = 0;
     if (e == cudaSuccess) e = field_stage1(f, ws, splits, d_total, s, &l1, nullptr, nullptr, &lf);
     long long n_near = 0;  // pageable host copy: no pinned staging is allocated

@@ -294,7 +294,8 @@ int bielcc_field_EH_full_device(bielcc_ctx ctx, bielcc_mesh mesh, int n_rhs,
  * loading the library holds until exit. Sizes whose scratch exceeds 64 MiB are
  * rejected with BIELCC_ERR_ARG and a message giving the bytes needed. The
  * scratch is, in bytes (each term rounded up to 256):
- *   per cell:  128 + 48 n_start^2 + 4        (3204 B = 3.1 KiB at n_start = 8)
+ *   per cell:  128 + 48 n^2 + 4              (3204 B = 3.1 KiB at n = 8; n is
+ *                                             n_start, or 2 n_start when p_max = 2)
  *   per point: 96 n_rhs per cell split + 96 n_rhs (near sums) + 16
  *              + 4 ceil(n_cells / 32)        (near-cell mask: 1 KiB per point
  *                                             at 8192 cells)

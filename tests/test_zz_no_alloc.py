@@ -46,7 +46,8 @@ def test_noalloc_matches_allocating_entry_point_twice():
     Jd = torch.from_numpy(np.ascontiguousarray(J)).to(dev)
     np_ = abi.NumParam.default()
 
-    def run_both(pts, precision):
+    def run_both(pts, precision, numparam=None):
+        nparam = np_ if numparam is None else numparam
         Pd = torch.from_numpy(np.ascontiguousarray(pts)).to(dev)
         shape = (1, len(pts), 3)
         Ea = torch.zeros(shape, dtype=torch.complex128, device=dev)
@@ -54,9 +55,9 @@ def test_noalloc_matches_allocating_entry_point_twice():
         Eb = torch.full(shape, complex(7.0, 7.0), dtype=torch.complex128, device=dev)
         Hb = torch.full(shape, complex(7.0, 7.0), dtype=torch.complex128, device=dev)
         ctx.field_EH_device(mesh, Jd.data_ptr(), k, Pd.data_ptr(), Ea.data_ptr(), Ha.data_ptr(), 1, len(pts),
-                            inc=inc, precision=precision, stream=stream.cuda_stream)
+                            inc=inc, numparam=nparam, precision=precision, stream=stream.cuda_stream)
         rep = abi.Report()
-        rc = noalloc(4, len(cells), Cd.data_ptr(), 1, Jd.data_ptr(), k, 0.0, 1.0, 0.0, C.byref(inc), C.byref(np_),
+        rc = noalloc(4, len(cells), Cd.data_ptr(), 1, Jd.data_ptr(), k, 0.0, 1.0, 0.0, C.byref(inc), C.byref(nparam),
                      len(pts), Pd.data_ptr(), Eb.data_ptr(), Hb.data_ptr(), gpu.PREC[precision], stream.cuda_stream,
                      C.byref(rep))
         assert rc == 0, L.bielcc_last_error().decode()
@@ -76,6 +77,12 @@ def test_noalloc_matches_allocating_entry_point_twice():
     (Ea, Ha), (Eb, Hb), rep = run_both(pts2, "mixed")
     assert rep.n_near_pairs > 0
     assert rel_l2(Eb, Ea) < TOL_MIXED and rel_l2(Hb, Ha) < TOL_MIXED
+
+    # call 3: adaptive quadrature with p_max = 2, whose far pass runs at 2 n_start
+    # (node tables four times larger in the static array)
+    np2 = abi.NumParam.default(p_max=2, p_max_seg=2)
+    (Ea, Ha), (Eb, Hb), rep = run_both(pts2, "fp64", np2)
+    assert rel_l2(Eb, Ea) < TOL_FP64 and rel_l2(Hb, Ha) < TOL_FP64
 
     mesh.close()
     ctx.close()
