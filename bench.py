@@ -61,7 +61,7 @@ def parse():
     ap.add_argument("--no-assembly", action="store_true", help="skip the 20,480-triangle assembly leg")
     ap.add_argument("--assembly-level", type=int, default=5, help="icosphere level of the assembly leg (5: 20,480)")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream leg")
-    ap.add_argument("--no-adaptive", action="store_true", help="skip the adaptive-quadrature (p_max = 2) leg")
+    ap.add_argument("--no-adaptive", action="store_true", help="skip the adaptive-quadrature (p_max = 2 and 3) leg")
     ap.add_argument("--tensor-cores", action="store_true",
                     help="mixed batches contract on the tensor cores (bielcc_ctx_set_batch_tensor_cores(ctx, 1))")
     ap.add_argument("--small", action="store_true",
@@ -467,20 +467,21 @@ def run_plan_moments_kept(ctx, torch, stream, flush, jobs_np, specs, outs, steps
 
 
 def run_adaptive(ctx, torch, dev, stream, flush, wl, cpu_threads):
-    """Adaptive quadrature, p_max = 2 (the reference's refinement loop), on the
-    headline geometry: the 8192-quad sphere, k = 2 pi, every 10th point of the
-    headline set (1800 far, 200 near-field), 1 RHS. With p_max = 2 a far pair's
-    result is the pass at 2 n_start, so the far part runs on the table-driven
-    kernels at n = 16 (256 nodes per cell); near pairs take the full
-    refinement schedule. GPU FP64 and mixed are timed with CUDA events on
-    device buffers; the compiled reference times a 22-point sample on the host
-    cores, and the GPU's FP64 result is checked against it there."""
+    """Adaptive quadrature (the reference's refinement loop) on the headline
+    geometry: the 8192-quad sphere, k = 2 pi, every 10th point of the headline
+    set (1800 far, 200 near-field), 1 RHS, at p_max = 2 and 3 (n_start 8,
+    n_start_seg 10, p_max_seg 2). With p_max = 2 a far pair's result is the pass
+    at 2 n_start (table-driven far kernels at n = 16); with p_max = 3 every far
+    pair's convergence test runs on the passes at 8 and 16 and the failing pairs
+    take the whole loop in the refinement kernel. Near pairs take the full
+    schedule. GPU FP64 and mixed are timed with CUDA events on device buffers;
+    the compiled reference times a 22-point sample on the host cores, and the
+    GPU's FP64 result is checked against it there."""
     import oracle
     from bielcc_b200 import abi
 
     cells, J, k, pts_all = wl["cells"], wl["J"], wl["k"], wl["pts"]
     pts = np.ascontiguousarray(np.concatenate([pts_all[:18000:10], pts_all[18000::10]]))
-    npm = abi.NumParam.default(p_max=2, p_max_seg=2)
     mesh = ctx.mesh(cells)
     P, S, N = len(pts), J.shape[0], len(cells)
     Jd = torch.from_numpy(np.ascontiguousarray(J)).to(dev)
@@ -488,49 +489,55 @@ def run_adaptive(ctx, torch, dev, stream, flush, wl, cpu_threads):
     Ed = torch.empty((S, P, 3), dtype=torch.complex128, device=dev)
     Hd = torch.empty_like(Ed)
     sc = stream.cuda_stream
-
-    def timed(prec, n):
-        def call():
-            ctx.field_EH_device(mesh, Jd.data_ptr(), k, Pd.data_ptr(), Ed.data_ptr(), Hd.data_ptr(), S, P,
-                                numparam=npm, precision=prec, stream=sc, report=False)
-        call()  # warm-up (and the n = 16 node tables)
-        t = 0.0
-        for _ in range(n):
-            flush.zero_()
-            a = torch.cuda.Event(enable_timing=True)
-            b = torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            call()
-            b.record(stream)
-            b.synchronize()
-            t += a.elapsed_time(b)
-        return t / n
-
-    ms64 = timed("fp64", 3)
-    E64, H64 = Ed.cpu().numpy(), Hd.cpu().numpy()
-    msmx = timed("mixed", 3)
-    Em, Hm = Ed.cpu().numpy(), Hd.cpu().numpy()
-    rel_mx = float(np.sqrt((np.sum(np.abs(Em - E64) ** 2) + np.sum(np.abs(Hm - H64) ** 2)) /
-                           (np.sum(np.abs(E64) ** 2) + np.sum(np.abs(H64) ** 2))))
-    idx = list(range(20)) + [1800, 1801]  # 20 far + 2 near-field points
     which = "ref" if oracle.available("ref") else "port"
-    t0 = time.perf_counter()
-    Eo, Ho = oracle.field_EH(cells, J, k, pts[idx], npm, n_threads=cpu_threads, which=which)
-    dt = time.perf_counter() - t0
-    rel_ref = float(np.sqrt((np.sum(np.abs(E64[:, idx] - Eo) ** 2) + np.sum(np.abs(H64[:, idx] - Ho) ** 2)) /
-                            (np.sum(np.abs(Eo) ** 2) + np.sum(np.abs(Ho) ** 2))))
-    mesh.close()
+    idx = list(range(20)) + [1800, 1801]  # 20 far + 2 near-field points
     pairs = P * N * S
-    cpu_value = len(idx) * N * S / dt
-    return {"workload": f"sphere{N}_k2pi, {P} points (1800 far, 200 near-field), 1 RHS, p_max = 2 "
-                        "(n_start 8, n_start_seg 10, p_max_seg 2)",
-            "unit": "pairs/s", "value": pairs / (msmx * 1e-3), "ms": msmx, "rel_l2_vs_fp64": rel_mx,
+
+    def rel(a, b, c, d):
+        return float(np.sqrt((np.sum(np.abs(a - c) ** 2) + np.sum(np.abs(b - d) ** 2)) /
+                             (np.sum(np.abs(c) ** 2) + np.sum(np.abs(d) ** 2))))
+
+    out = {"workload": f"sphere{N}_k2pi, {P} points (1800 far, 200 near-field), 1 RHS, n_start 8, n_start_seg 10, "
+                       "p_max_seg 2", "unit": "pairs/s"}
+    for p_max in (2, 3):
+        npm = abi.NumParam.default(p_max=p_max, p_max_seg=2)
+
+        def timed(prec, n):
+            def call():
+                ctx.field_EH_device(mesh, Jd.data_ptr(), k, Pd.data_ptr(), Ed.data_ptr(), Hd.data_ptr(), S, P,
+                                    numparam=npm, precision=prec, stream=sc, report=False)
+            call()  # warm-up (and the node tables)
+            t = 0.0
+            for _ in range(n):
+                flush.zero_()
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                call()
+                b.record(stream)
+                b.synchronize()
+                t += a.elapsed_time(b)
+            return t / n
+
+        ms64 = timed("fp64", 3)
+        E64, H64 = Ed.cpu().numpy(), Hd.cpu().numpy()
+        msmx = timed("mixed", 3)
+        Em, Hm = Ed.cpu().numpy(), Hd.cpu().numpy()
+        t0 = time.perf_counter()
+        Eo, Ho = oracle.field_EH(cells, J, k, pts[idx], npm, n_threads=cpu_threads, which=which)
+        dt = time.perf_counter() - t0
+        out[f"p_max_{p_max}"] = {
+            "value": pairs / (msmx * 1e-3), "ms": msmx, "rel_l2_vs_fp64": rel(Em, Hm, E64, H64),
             "fp64_value": pairs / (ms64 * 1e-3), "fp64_ms": ms64,
-            "fp64_rel_l2_vs_cpu_reference": rel_ref,
-            "cpu_reference": {"value": cpu_value, "unit": "pairs/s", "cores": cpu_threads,
+            "fp64_rel_l2_vs_cpu_reference": rel(E64[:, idx], H64[:, idx], Eo, Ho),
+            "cpu_reference": {"value": len(idx) * N * S / dt, "unit": "pairs/s", "cores": cpu_threads,
                               "kind": "reference" if which == "ref" else "port",
-                              "sample": f"{len(idx)} points (2 near-field) x {N} cells x {S} RHS, {dt:.1f} s"},
-            "far_pass": "table-driven far kernels at n = 16 (the pass p_max = 2 returns)"}
+                              "sample": f"{len(idx)} points (2 near-field) x {N} cells x {S} RHS, {dt:.1f} s"}}
+    mesh.close()
+    out["far_pass"] = ("p_max = 2: table-driven far kernels at n = 16 (the pass the loop returns); p_max = 3: "
+                       "convergence test on the passes at 8 and 16 for every far pair, the pass at 16 where it "
+                       "holds, the whole loop for the rest")
+    return out
 
 
 def run_assembly(args, ctx, torch, dev, stream, flush):

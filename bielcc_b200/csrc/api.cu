@@ -158,6 +158,10 @@ void free_mesh(MeshDev* m) {
     cudaFree(m->nodes64);
     cudaFree(m->nodes32);
     cudaFree(m->rho32);
+    cudaFree(m->nodes64_lo);
+    cudaFree(m->nodes64_hi);
+    cudaFree(m->nodes32_hi);
+    cudaFree(m->rho32_hi);
     delete m;
 }
 
@@ -177,6 +181,40 @@ int ensure_tables(MeshDev* m, int n, cudaStream_t s) {
     TRY_CUDA(cudaMalloc(&m->rho32, (size_t)m->n_cells * sizeof(float) + 16));
     TRY_CUDA(launch_node_tables(m->verts, m->geo, m->nv, m->n_cells, n, m->nodes64, m->nodes32, m->rho32, s));
     m->table_n = n;
+    return BIELCC_OK;
+}
+
+// The far pass's node tables (far_split_n) and, for p_max >= 3, the FP64
+// table at n_start that the convergence test compares against and, for
+// p_max = 3, the tables at 4 n_start of the third pass.
+int ensure_far_tables(MeshDev* m, const NumParamH& np, cudaStream_t s) {
+    TRY(ensure_tables(m, far_split_n(np), s));
+    if (far_adaptive(np) && (m->table_lo_n != np.n_start || !m->nodes64_lo)) {
+        cudaFree(m->nodes64_lo);
+        m->nodes64_lo = nullptr;
+        m->table_lo_n = 0;
+        TRY_CUDA(cudaMalloc(&m->nodes64_lo, (size_t)np.n_start * np.n_start * m->n_cells * sizeof(double4) + 16));
+        TRY_CUDA(launch_node_tables(m->verts, m->geo, m->nv, m->n_cells, np.n_start, m->nodes64_lo, nullptr, nullptr,
+                                    s));
+        m->table_lo_n = np.n_start;
+    }
+    const int n3 = 4 * np.n_start;
+    if (far_third_pass(np) && (m->table_hi_n != n3 || !m->nodes64_hi)) {
+        cudaFree(m->nodes64_hi);
+        cudaFree(m->nodes32_hi);
+        cudaFree(m->rho32_hi);
+        m->nodes64_hi = nullptr;
+        m->nodes32_hi = nullptr;
+        m->rho32_hi = nullptr;
+        m->table_hi_n = 0;
+        const size_t nn = (size_t)n3 * n3 * m->n_cells;
+        TRY_CUDA(cudaMalloc(&m->nodes64_hi, nn * sizeof(double4) + 16));
+        TRY_CUDA(cudaMalloc(&m->nodes32_hi, nn * sizeof(float4) + 16));
+        TRY_CUDA(cudaMalloc(&m->rho32_hi, (size_t)m->n_cells * sizeof(float) + 16));
+        TRY_CUDA(launch_node_tables(m->verts, m->geo, m->nv, m->n_cells, n3, m->nodes64_hi, m->nodes32_hi,
+                                    m->rho32_hi, s));
+        m->table_hi_n = n3;
+    }
     return BIELCC_OK;
 }
 
@@ -325,7 +363,7 @@ int field_begin(bielcc_ctx ctx, const FieldArgs& a, cudaStream_t s, bielcc_repor
     p->a = a;
     TRY(field_device_batched(ctx, a, s, rep, d_nonfinite, &p->batched, w));
     if (p->batched) return BIELCC_OK;
-    TRY(ensure_tables(a.m, far_split_n(a.np), s));
+    TRY(ensure_far_tables(a.m, a.np, s));
     FieldLaunch& f = p->f;
     f.mesh = a.m;
     f.pts = a.pts;
@@ -444,7 +482,7 @@ int est_single_begin(bielcc_ctx ctx, const FieldArgs& a, cudaStream_t s, SingleE
     j.H = H_out;
     j.Eq = e.full ? e.Ec : e.Eq;
     j.Hq = H_out ? (e.full ? e.Hc : e.Hq) : nullptr;
-    TRY(ensure_tables(a.m, far_split_n(a.np), s));
+    TRY(ensure_far_tables(a.m, a.np, s));
     TRY_CUDA(cudaEventRecord(ctx->side_in, s));  // inputs and node tables on the device
     TRY_CUDA(cudaStreamWaitEvent(ctx->side, ctx->side_in, 0));
     TRY_CUDA(cudaMemcpyAsync(e.d_job, &j, sizeof(j), cudaMemcpyHostToDevice, ctx->side));
@@ -620,6 +658,8 @@ int bielcc_ctx_mem_used(bielcc_ctx ctx, int64_t* bytes) {
         const MeshDev* m = kv.second;
         b += (int64_t)m->n_cells * (m->nv * 3 * 8 + sizeof(CellGeo));
         if (m->table_n) b += (int64_t)m->n_cells * m->table_n * m->table_n * (32 + 16) + 4 * m->n_cells;
+        if (m->table_lo_n) b += (int64_t)m->n_cells * m->table_lo_n * m->table_lo_n * 32;
+        if (m->table_hi_n) b += (int64_t)m->n_cells * m->table_hi_n * m->table_hi_n * (32 + 16) + 4 * m->n_cells;
     }
     *bytes = b;
     return BIELCC_OK;

@@ -95,12 +95,28 @@ struct FarArgs {
     double* partial;      // [split][S][12][P]
     unsigned* nearmask;   // [ceil(N/32)][P]: bit c%32 of word c/32 set iff (p, c) is near
 };
+// p_max >= 3, the far kernel's marks-reading variant: the integrals that failed
+// the convergence test at the second pass, grad F per pair [ceil(N/32)][P] and
+// F . J per RHS [S][ceil(N/32)][P]; take_marked 0 adds the integrals that
+// passed, 1 the ones that failed. (A separate type: the plain variants keep
+// FarArgs' parameter block, whose size the FP64 kernel's register allocation
+// follows.)
+struct FarArgsMarks : FarArgs {
+    const unsigned* markG;
+    const unsigned* markK;
+    int take_marked;
+};
+template <bool MARKS>
+using FarArgsOf = typename std::conditional<MARKS, FarArgsMarks, FarArgs>::type;
 
 // Contract one cell's moments (times the phase P = pr + i pi) with the RHS
 // currents and add into the FP64 accumulators acc[r][12] =
 // (Ex, Ey, Ez, Hx, Hy, Hz) x (re, im).
+// takeE: bit r adds RHS r's E; takeH: the H of every RHS (convergence-test
+// marks, p_max >= 3; all set otherwise).
 template <int NRHS, typename F>
-BIELCC_D void contract(const Moments<F>& m, F pr, F pi, const cplx (*sj)[3], bool zeroR, double (*acc)[12]) {
+BIELCC_D void contract(const Moments<F>& m, F pr, F pi, const cplx (*sj)[3], bool zeroR, double (*acc)[12],
+                       unsigned takeE = ~0u, bool takeH = true) {
     // moments x phase
     F A1r = m.a1r * pr - m.a1i * pi, A1i = m.a1r * pi + m.a1i * pr;
     F T[6][2], G[3][2];
@@ -132,10 +148,12 @@ BIELCC_D void contract(const Moments<F>& m, F pr, F pi, const cplx (*sj)[3], boo
                 er += t[0] * jr[b] - t[1] * ji[b];
                 ei += t[0] * ji[b] + t[1] * jr[b];
             }
-            acc[rr][2 * a] += (double)er;
-            acc[rr][2 * a + 1] += (double)ei;
+            if ((takeE >> rr) & 1u) {
+                acc[rr][2 * a] += (double)er;
+                acc[rr][2 * a + 1] += (double)ei;
+            }
         }
-        if (!zeroR) {
+        if (!zeroR && takeH) {
 #pragma unroll
             for (int a = 0; a < 3; a++) {
                 int b = (a + 1) % 3, c = (a + 2) % 3;  // (G x J)_a = G_b J_c - G_c J_b
@@ -148,9 +166,11 @@ BIELCC_D void contract(const Moments<F>& m, F pr, F pi, const cplx (*sj)[3], boo
     }
 }
 
-// The far kernel. MIXED = false: FP64 nodes; true: FP32 nodes.
-template <int NRHS, bool CK, bool MIXED>
-__global__ void BIELCC_FAR_BOUNDS(NRHS, CK, MIXED) far_kernel(FarArgs a) {
+// The far kernel. MIXED = false: FP64 nodes; true: FP32 nodes. MARKS: the
+// convergence-test marks of p_max >= 3 select the integrals this pass adds
+// (FarArgs::markG / markK); the other variants read no marks.
+template <int NRHS, bool CK, bool MIXED, bool MARKS = false>
+__global__ void BIELCC_FAR_BOUNDS(NRHS, CK, MIXED) far_kernel(FarArgsOf<MARKS> a) {
     using NodeT = typename std::conditional<MIXED, float4, double4>::type;
     __shared__ __align__(16) NodeT s_nodes[kStageNodes];
     __shared__ float s_yy[MIXED ? kStageNodes : 1];  // |y - centre|^2 of the staged nodes (mixed form)
@@ -181,6 +201,8 @@ __global__ void BIELCC_FAR_BOUNDS(NRHS, CK, MIXED) far_kernel(FarArgs a) {
     Moments<F> m;
     m.zero();
     bool far = false, zeroR = false;
+    unsigned takeE = ~0u;  // convergence-test marks (p_max >= 3): the RHS whose E this pass adds
+    bool takeH = true;     // and whether it adds H
     unsigned nbits = 0;  // near bits of the current 32-cell word
     // mixed-form per-pair state
     PairF32 pf{};
@@ -235,6 +257,20 @@ __global__ void BIELCC_FAR_BOUNDS(NRHS, CK, MIXED) far_kernel(FarArgs a) {
                     double cen[3] = {ci.x, ci.y, ci.z}, d;
                     const bool nr = is_near(x, cen, ci.w, a.analytic_calc, &d);
                     far = !nr && live;
+                    if constexpr (MARKS) {
+                      if (far) {  // each integral's convergence test decides which pass adds it
+                        const int c = c0 + cc, nw = (a.n_cells + 31) >> 5;
+                        const size_t wi = (size_t)(c >> 5) * a.n_pts + p;
+                        const bool want = a.take_marked != 0;
+                        takeH = (((a.markG[wi] >> (c & 31)) & 1u) != 0) == want;
+                        takeE = 0u;
+                        for (int rr = 0; rr < NRHS && a.rhs0 + rr < a.n_rhs; rr++) {
+                            const unsigned mk = a.markK[(size_t)(a.rhs0 + rr) * nw * a.n_pts + wi];
+                            if ((((mk >> (c & 31)) & 1u) != 0) == want) takeE |= 1u << rr;
+                        }
+                        far = takeE != 0u || takeH;
+                      }
+                    }
                     zeroR = d < kMachineZero;  // R_Rot_Colloc: R = 0 at the cell centre
                     m.zero();
                     const int c = c0 + cc;
@@ -311,8 +347,14 @@ __global__ void BIELCC_FAR_BOUNDS(NRHS, CK, MIXED) far_kernel(FarArgs a) {
                 }
                 if (k0 + kc == nn && far) {
                     if (!CK) m.finish_real_k();
-                    if constexpr (MIXED) contract<NRHS, float>(m, (float)P0r, (float)P0i, s_j[cc], zeroR, acc);
-                    else contract<NRHS, double>(m, P0r, P0i, s_j[cc], zeroR, acc);
+                    if constexpr (MARKS) {
+                        if constexpr (MIXED)
+                            contract<NRHS, float>(m, (float)P0r, (float)P0i, s_j[cc], zeroR, acc, takeE, takeH);
+                        else contract<NRHS, double>(m, P0r, P0i, s_j[cc], zeroR, acc, takeE, takeH);
+                    } else {
+                        if constexpr (MIXED) contract<NRHS, float>(m, (float)P0r, (float)P0i, s_j[cc], zeroR, acc);
+                        else contract<NRHS, double>(m, P0r, P0i, s_j[cc], zeroR, acc);
+                    }
                 }
             }
         }
@@ -328,49 +370,186 @@ __global__ void BIELCC_FAR_BOUNDS(NRHS, CK, MIXED) far_kernel(FarArgs a) {
     }
 }
 
-// Far pairs with adaptive refinement (p_max > 2): the reference's
-// convergence test of K_RotRot_Far runs on F_RotRotSimplePot_H . J, so the
-// refinement depth depends on the current; one RHS per launch, generic
-// per-pair quadrature with nodes generated on the fly (ops.cuh). R_Rot_Colloc
-// is J-independent (moment G). Writes the same raw partials as far_kernel.
-__global__ void far_adaptive_kernel(FarArgs a, const double* __restrict__ verts, int nv, DNP np) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+// ---------------------------------------------------------------- adaptive far pairs (p_max >= 3)
+// The reference's loop (integral_universal.h:58-119) stops at the first pass
+// after the first whose squared L2 change is below eps^2, else returns its last
+// pass. far_refine_decide_kernel runs that test between the passes at n_start
+// and 2 n_start for every far pair, from node tables: K_RotRot_Far's integral
+// of F_RotRotSimplePot_H . J for every right-hand side (K.h:288-301) and
+// R_Rot_Colloc's integral of grad F (R.h:89-111; none at the cell centre).
+// Each integral is tested on its own, as the reference runs one loop per
+// integral: an integral that passes takes the pass at 2 n_start (far_kernel
+// with take_marked = 0); one that fails is marked (markG per pair, markK per
+// pair and RHS) and takes the pass at 4 n_start when p_max = 3 (far_kernel
+// with take_marked = 1 on those tables), else the whole loop in
+// far_refine_sum_kernel.
+
+// One pass of the FP64 far node loop over a cell's node table row (far_kernel's
+// FP64 arithmetic: the phase split below |k| rho = 0.5, else sincos per node).
+template <bool CK>
+BIELCC_D void far_pass_f64(Moments<double>& m, const double4* __restrict__ nd, int nn, const double* x, cplx k,
+                           double k2r, double k2i, double r0, bool split, int td) {
+    m.zero();
+    if (split) {
+#define BIELCC_PASS64(TD_)                                                                              \
+    for (int i = 0; i < nn; i++) {                                                                      \
+        const double4 v = nd[i];                                                                \
+        far_node_f64<CK, true, TD_>(m, x[0] - v.x, x[1] - v.y, x[2] - v.z, v.w, k, k2r, k2i, r0);       \
+    }
+        switch (td) {
+            case 2: BIELCC_PASS64(2) break;
+            case 1: BIELCC_PASS64(1) break;
+            default: BIELCC_PASS64(0) break;
+        }
+#undef BIELCC_PASS64
+    } else {
+        for (int i = 0; i < nn; i++) {
+            const double4 v = nd[i];
+            far_node_f64<CK, false>(m, x[0] - v.x, x[1] - v.y, x[2] - v.z, v.w, k, k2r, k2i, r0);
+        }
+    }
+    if (!CK) m.finish_real_k();
+}
+
+// Raw integrals of one pass (before the 1/4pi of K_RotRot_Far / R_Rot_Colloc),
+// times the phase P: K = A1 J + T J, G = grad F.
+BIELCC_D void far_raw_K(const Moments<double>& m, double pr, double pi, const cplx* j, cplx* K) {
+    const int ti[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+    for (int a = 0; a < 3; a++) {
+        cplx e = mk(m.a1r, m.a1i) * j[a];
+        for (int b = 0; b < 3; b++) e = e + mk(m.t[ti[a][b]][0], m.t[ti[a][b]][1]) * j[b];
+        K[a] = e * mk(pr, pi);
+    }
+}
+
+// The reference's squared change: sum of |res - prev|^2 with |.| taken first
+// (integral_universal.h:96-99).
+BIELCC_D double far_delta2(const cplx* a, const cplx* b) {
+    double d = 0.;
+    for (int g = 0; g < 3; g++) {
+        const double t = sqrt(cabs2(a[g] - b[g]));
+        d += t * t;
+    }
+    return d;
+}
+
+// markK must be zero on entry (set bits only); markG is written in full.
+__global__ void far_refine_decide_kernel(FarArgs a, const double4* __restrict__ lo, int nn_lo, double eps2,
+                                         unsigned* __restrict__ markG, unsigned* __restrict__ markK) {
+    const int p = blockIdx.x * kFarThreads + threadIdx.x;
     if (p >= a.n_pts) return;
-    const int rhs = a.rhs0;
-    double x[3] = {a.pts[3 * (size_t)p], a.pts[3 * (size_t)p + 1], a.pts[3 * (size_t)p + 2]};
+    const double x[3] = {a.pts[3 * (size_t)p], a.pts[3 * (size_t)p + 1], a.pts[3 * (size_t)p + 2]};
     const int cb = blockIdx.y * a.cells_per_split;
     const int ce = min(a.n_cells, cb + a.cells_per_split);
-    double acc[12];
-    for (int q = 0; q < 12; q++) acc[q] = 0.;
-    unsigned nbits = 0;
+    const bool ck = a.k.im != 0.0;
+    const double k2r = a.k.re * a.k.re - a.k.im * a.k.im, k2i = 2.0 * a.k.re * a.k.im;
+    const int nw = (a.n_cells + 31) >> 5;
+    unsigned nbits = 0, gbits = 0;
     for (int c = cb; c < ce; c++) {
         const CellGeo& gg = a.geo[c];
         double d;
         const bool nr = is_near(x, gg.c, gg.diam, a.analytic_calc, &d);
+        bool gfail = false;
+        if (!nr) {
+            const double th64 = fabs(a.k.re) * (double)a.rho32[c] * (1.0 + 1e-6);
+            const bool split = !ck && th64 <= 0.5;
+            const int td = th64 <= 0.125 ? 2 : (th64 <= 0.25 ? 1 : 0);
+            double pr = 1.0, pi = 0.0;
+            if (split) sincos(a.k.re * d, &pi, &pr);
+            Moments<double> m0, m1;
+            if (ck) {
+                far_pass_f64<true>(m0, lo + (size_t)c * nn_lo, nn_lo, x, a.k, k2r, k2i, d, false, 0);
+                far_pass_f64<true>(m1, a.nodes64 + (size_t)c * a.nn, a.nn, x, a.k, k2r, k2i, d, false, 0);
+            } else {
+                far_pass_f64<false>(m0, lo + (size_t)c * nn_lo, nn_lo, x, a.k, k2r, k2i, d, split, td);
+                far_pass_f64<false>(m1, a.nodes64 + (size_t)c * a.nn, a.nn, x, a.k, k2r, k2i, d, split, td);
+            }
+            if (!(d < kMachineZero)) {  // R_Rot_Colloc integrates grad F away from the centre only
+                cplx g0[3], g1[3];
+                for (int q = 0; q < 3; q++) {
+                    g0[q] = mk(m0.g[q][0], m0.g[q][1]) * mk(pr, pi);
+                    g1[q] = mk(m1.g[q][0], m1.g[q][1]) * mk(pr, pi);
+                }
+                gfail = !(far_delta2(g1, g0) < eps2);
+            }
+            for (int s = 0; s < a.n_rhs; s++) {
+                const cplx* j = a.J + ((size_t)s * a.n_cells + c) * 3;
+                const cplx jj[3] = {j[0], j[1], j[2]};
+                cplx k0[3], k1[3];
+                far_raw_K(m0, pr, pi, jj, k0);
+                far_raw_K(m1, pr, pi, jj, k1);
+                if (!(far_delta2(k1, k0) < eps2))
+                    atomicOr(markK + ((size_t)s * nw + (c >> 5)) * a.n_pts + p, 1u << (c & 31));
+            }
+        }
         nbits |= (nr ? 1u : 0u) << (c & 31);
+        gbits |= (gfail ? 1u : 0u) << (c & 31);
         if ((c & 31) == 31 || c == ce - 1) {
             if (a.nearmask) a.nearmask[(size_t)(c >> 5) * a.n_pts + p] = nbits;
-            nbits = 0;
+            markG[(size_t)(c >> 5) * a.n_pts + p] = gbits;
+            nbits = gbits = 0;
         }
-        if (nr) continue;
+    }
+}
+
+// p_max > 3: the integrals that failed the test, through the whole loop
+// (integral_cell, ops.cuh: the reference's passes, test and budget), one warp
+// per (point, RHS): F . J where markK is set, grad F where markG is set. In
+// round r lane l takes the point's marked cell of rank 32 r + l (cell order;
+// each lane walks the mask words with its own cursor), so the lanes run their
+// loops side by side; lane sums are in cell order and combined by a fixed xor
+// butterfly. Writes the raw E, H sums (before 1/4pi) of every point, zero
+// without marked cells, into the partial-sum slot `out` [S][12][P].
+__global__ void far_refine_sum_kernel(FarArgs a, const unsigned* __restrict__ markG, const unsigned* __restrict__ markK,
+                                      const double* __restrict__ verts, int nv, DNP np, double* __restrict__ out) {
+    const int p = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    const int s = blockIdx.y;
+    if (p >= a.n_pts) return;  // whole warps
+    const size_t P = a.n_pts;
+    const int n_words = (a.n_cells + 31) / 32;
+    const unsigned* mK = markK + (size_t)s * n_words * P;
+    const double x[3] = {a.pts[3 * (size_t)p], a.pts[3 * (size_t)p + 1], a.pts[3 * (size_t)p + 2]};
+    double v[12];
+#pragma unroll
+    for (int q = 0; q < 12; q++) v[q] = 0.;
+    int w = 0;
+    unsigned bits = n_words > 0 ? (markG[p] | mK[p]) : 0u;
+    long long base = 0;  // rank of the first flagged cell of word w
+    for (long long t = lane;; t += 32) {
+        while (w < n_words && base + __popc(bits) <= t) {
+            base += __popc(bits);
+            w++;
+            bits = w < n_words ? (markG[(size_t)w * P + p] | mK[(size_t)w * P + p]) : 0u;
+        }
+        const bool have = w < n_words;
+        if (!__any_sync(0xffffffffu, have)) break;
+        if (!have) continue;
+        unsigned b = bits;
+        for (long long r = base; r < t; r++) b &= b - 1;  // drop the lower-ranked cells of the word
+        const int c = w * 32 + __ffs(b) - 1;
+        const bool doK = (mK[(size_t)w * P + p] >> (c & 31)) & 1u, doG = (markG[(size_t)w * P + p] >> (c & 31)) & 1u;
         DCell cl;
         cl.nv = nv;
-        for (int v = 0; v < nv; v++)
-            for (int g = 0; g < 3; g++) cl.v[v][g] = verts[((size_t)c * nv + v) * 3 + g];
-        const cplx* j = a.J + ((size_t)rhs * a.n_cells + c) * 3;
+        for (int vv = 0; vv < nv; vv++)
+            for (int g = 0; g < 3; g++) cl.v[vv][g] = verts[((size_t)c * nv + vv) * 3 + g];
+        const cplx* j = a.J + ((size_t)s * a.n_cells + c) * 3;
         DKP kp;
         dkp_zero(kp);
         kp.smoothR = kMachineZero;
         kp.smoothRMin = kMachineZero;
         kp.k = a.k;
         for (int g = 0; g < 3; g++) kp.current[g] = j[g];
-        cplx K[3];
-        integral_cell<cplx>(F_ROTROTSIMPLEPOT_H, x, cl, kp, 3, np.n_start, np.p_max, np.eps, K);
-        for (int g = 0; g < 3; g++) {
-            acc[2 * g] += K[g].re;
-            acc[2 * g + 1] += K[g].im;
+        if (doK) {
+            cplx K[3];
+            integral_cell<cplx>(F_ROTROTSIMPLEPOT_H, x, cl, kp, 3, np.n_start, np.p_max, np.eps, K);
+            for (int g = 0; g < 3; g++) {
+                v[2 * g] += K[g].re;
+                v[2 * g + 1] += K[g].im;
+            }
         }
-        if (!(d < kMachineZero)) {  // R_Rot_Colloc: 0 at the cell centre
+        double d;
+        is_near(x, a.geo[c].c, a.geo[c].diam, a.analytic_calc, &d);
+        if (doG && !(d < kMachineZero)) {  // R_Rot_Colloc: 0 at the cell centre
             DKP kr;
             dkp_zero(kr);
             kr.smoothR = kMachineZero;
@@ -380,14 +559,22 @@ __global__ void far_adaptive_kernel(FarArgs a, const double* __restrict__ verts,
             integral_cell<cplx>(F_GRADSIMPLEPOT_H, x, cl, kr, 3, np.n_start, np.p_max, np.eps, G);
             ccross_cc(G, jj, h);
             for (int g = 0; g < 3; g++) {
-                acc[6 + 2 * g] += h[g].re;
-                acc[6 + 2 * g + 1] += h[g].im;
+                v[6 + 2 * g] += h[g].re;
+                v[7 + 2 * g] += h[g].im;
             }
         }
     }
-    const size_t P = a.n_pts;
-    double* dst = a.partial + (((size_t)blockIdx.y * a.n_rhs + rhs) * 12) * P + p;
-    for (int q = 0; q < 12; q++) dst[(size_t)q * P] = acc[q];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+        for (int q = 0; q < 12; q++) v[q] += __shfl_xor_sync(0xffffffffu, v[q], off);
+    if (lane < 12) {
+        double r = v[0];
+#pragma unroll
+        for (int q = 1; q < 12; q++)
+            if (lane == q) r = v[q];
+        out[((size_t)s * 12 + lane) * P + p] = r;
+    }
 }
 
 // ---------------------------------------------------------------- near classification
@@ -594,22 +781,26 @@ __global__ void finalize_kernel(FinalArgs a) {
 // ---------------------------------------------------------------- host launchers
 static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 static size_t mask_words(int n_cells) { return (size_t)(n_cells + 31) / 32; }
+// Partial-sum slots [slot][S][12][P]: one per cell split; with p_max = 3 as
+// many again for the third pass of the pairs that fail the convergence test;
+// with p_max > 3 one more for the pairs that take the whole refinement loop.
+static int partial_slots(const FieldLaunch& f, int splits) {
+    return splits + (far_third_pass(f.np) ? splits : (far_adaptive(f.np) ? 1 : 0));
+}
 // Resident CTAs (whole GPU) of the far-kernel variant a launch starts with:
-// NRHS 4 / 2 / 1 (the first RHS chunk), real / complex k, FP64 / mixed, or
-// the adaptive kernel.
-static int far_slots(int n_rhs, bool ck, bool mixed, bool adaptive) {
-    static std::atomic<int> cache[2][2][3][2];
+// NRHS 4 / 2 / 1 (the first RHS chunk), real / complex k, FP64 / mixed.
+static int far_slots(int n_rhs, bool ck, bool mixed) {
+    static std::atomic<int> cache[2][3][2];
     const int ri = n_rhs >= 4 ? 0 : (n_rhs >= 2 ? 1 : 2);
-    std::atomic<int>& c = cache[adaptive][ck][ri][mixed];
+    std::atomic<int>& c = cache[ck][ri][mixed];
     int v = c.load(std::memory_order_relaxed);
     if (v) return v;
     int dev = 0, sms = 148, per = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const void* fn;
-    if (adaptive) fn = (const void*)far_adaptive_kernel;
 #define BIELCC_FK(R, C, M) (const void*)far_kernel<R, C, M>
-    else if (ri == 0) fn = ck ? (mixed ? BIELCC_FK(4, true, true) : BIELCC_FK(4, true, false))
+    if (ri == 0) fn = ck ? (mixed ? BIELCC_FK(4, true, true) : BIELCC_FK(4, true, false))
                               : (mixed ? BIELCC_FK(4, false, true) : BIELCC_FK(4, false, false));
     else if (ri == 1) fn = ck ? (mixed ? BIELCC_FK(2, true, true) : BIELCC_FK(2, true, false))
                               : (mixed ? BIELCC_FK(2, false, true) : BIELCC_FK(2, false, false));
@@ -627,18 +818,29 @@ size_t field_ws_base_bytes(const FieldLaunch& f, int* splits_out, size_t partial
     const int N = f.mesh->n_cells;
     const size_t P = f.n_pts;
     const size_t per_split = (size_t)f.n_rhs * 12 * P * sizeof(double);
-    const int slots = far_slots(f.n_rhs, f.k.im != 0.0, f.precision == 1, far_adaptive(f.np));
+    const int slots = far_slots(f.n_rhs, f.k.im != 0.0, f.precision == 1);
     const int max_splits = (int)std::max<size_t>(1, partial_cap / std::max<size_t>(1, per_split));
     const int splits = choose_cell_splits(tiles, N, slots, max_splits);
     *splits_out = splits;
-    return align256((size_t)splits * per_split) + 2 * align256((P + 1) * sizeof(long long)) +
+    return align256((size_t)partial_slots(f, splits) * per_split) + 2 * align256((P + 1) * sizeof(long long)) +
            align256(sizeof(long long)) + align256(mask_words(N) * P * sizeof(unsigned)) +
-           align256((size_t)f.n_rhs * 12 * P * sizeof(double));
+           align256((size_t)f.n_rhs * 12 * P * sizeof(double)) +
+           (far_adaptive(f.np) ? align256((size_t)(1 + f.n_rhs) * mask_words(N) * P * sizeof(unsigned)) : 0);
 }
 
 template <int NRHS, bool CK, bool MIXED>
 static void launch_far_t(const FarArgs& a, int tiles, int splits, cudaStream_t s) {
     far_kernel<NRHS, CK, MIXED><<<dim3(tiles, splits), kFarThreads, 0, s>>>(a);
+}
+
+// p_max >= 3: one RHS per launch of the marks-reading variant.
+template <bool CK, bool MIXED>
+static int launch_far_marks(FarArgsMarks a, int tiles, int splits, cudaStream_t s) {
+    for (int r = 0; r < a.n_rhs; r++) {
+        a.rhs0 = r;
+        far_kernel<1, CK, MIXED, true><<<dim3(tiles, splits), kFarThreads, 0, s>>>(a);
+    }
+    return a.n_rhs;
 }
 
 template <bool CK, bool MIXED>
@@ -660,13 +862,17 @@ cudaError_t field_stage1(const FieldLaunch& f, void* ws, int splits, long long* 
     const size_t P = f.n_pts;
     char* w = (char*)ws;
     double* partial = (double*)w;
-    w += align256((size_t)splits * f.n_rhs * 12 * P * sizeof(double));
+    w += align256((size_t)partial_slots(f, splits) * f.n_rhs * 12 * P * sizeof(double));
     long long* counts = (long long*)w;
     w += align256((P + 1) * sizeof(long long));
     long long* offs = (long long*)w;
     w += align256((P + 1) * sizeof(long long)) + align256(sizeof(long long));
     unsigned* mask = (unsigned*)w;
     const int n_words = (int)mask_words(m.n_cells);
+    w += align256(mask_words(m.n_cells) * P * sizeof(unsigned)) + align256((size_t)f.n_rhs * 12 * P * sizeof(double));
+    // p_max >= 3, after the near sums: the marks of grad F, then of F . J per RHS
+    unsigned* markG = far_adaptive(f.np) ? (unsigned*)w : nullptr;
+    unsigned* markK = markG ? markG + mask_words(m.n_cells) * P : nullptr;
 
     FarArgs a;
     a.pts = f.pts;
@@ -689,19 +895,51 @@ cudaError_t field_stage1(const FieldLaunch& f, void* ws, int splits, long long* 
     bool ck = f.k.im != 0.0;
     bool mixed = f.precision == 1;
     int nl = 0;
-    if (far_begin) cudaEventRecord(far_begin, s);
-    if (tiles > 0 && !far_adaptive(f.np) && m.table_n != far_split_n(f.np))
+    if (tiles > 0 && m.table_n != far_split_n(f.np))
         return cudaErrorInvalidValue;  // node tables of another split: the caller builds far_split_n's
+    if (tiles > 0 && far_adaptive(f.np) && (m.table_lo_n != f.np.n_start || !m.nodes64_lo))
+        return cudaErrorInvalidValue;  // no n_start table for the convergence test
+    if (tiles > 0 && far_third_pass(f.np) && (m.table_hi_n != 4 * f.np.n_start || !m.nodes64_hi))
+        return cudaErrorInvalidValue;  // no 4 n_start tables for the third pass
+    if (far_begin) cudaEventRecord(far_begin, s);
     if (tiles > 0 && far_adaptive(f.np)) {
+        // the convergence test of every far pair's integrals; the failing ones are marked
+        cudaError_t e = cudaMemsetAsync(markK, 0, (size_t)f.n_rhs * n_words * P * sizeof(unsigned), s);
+        if (e != cudaSuccess) return e;
+        far_refine_decide_kernel<<<dim3(tiles, splits), kFarThreads, 0, s>>>(
+            a, m.nodes64_lo, f.np.n_start * f.np.n_start, f.np.eps * f.np.eps, markG, markK);
+        nl++;
+    }
+    FarArgsMarks am;
+    static_cast<FarArgs&>(am) = a;
+    am.markG = markG;
+    am.markK = markK;
+    am.take_marked = 0;
+    if (tiles > 0 && markG) {  // the integrals that passed: the pass at 2 n_start
+        if (mixed) nl += ck ? launch_far_marks<true, true>(am, tiles, splits, s) : launch_far_marks<false, true>(am, tiles, splits, s);
+        else nl += ck ? launch_far_marks<true, false>(am, tiles, splits, s) : launch_far_marks<false, false>(am, tiles, splits, s);
+    } else if (tiles > 0) {
+        if (mixed) nl += ck ? launch_far_rhs<true, true>(a, tiles, splits, s) : launch_far_rhs<false, true>(a, tiles, splits, s);
+        else nl += ck ? launch_far_rhs<true, false>(a, tiles, splits, s) : launch_far_rhs<false, false>(a, tiles, splits, s);
+    }
+    if (tiles > 0 && far_third_pass(f.np)) {
+        // p_max = 3: the marked pairs return the third pass, at 4 n_start, into
+        // their own partial slots
+        FarArgsMarks a3 = am;
+        a3.nodes64 = m.nodes64_hi;
+        a3.nodes32 = m.nodes32_hi;
+        a3.rho32 = m.rho32_hi;
+        a3.nn = 16 * f.np.n_start * f.np.n_start;
+        a3.partial = partial + (size_t)splits * f.n_rhs * 12 * P;
+        a3.take_marked = 1;
+        if (mixed) nl += ck ? launch_far_marks<true, true>(a3, tiles, splits, s) : launch_far_marks<false, true>(a3, tiles, splits, s);
+        else nl += ck ? launch_far_marks<true, false>(a3, tiles, splits, s) : launch_far_marks<false, false>(a3, tiles, splits, s);
+    } else if (tiles > 0 && f.n_rhs > 0 && far_adaptive(f.np)) {
         DNP np{f.np.eps, f.np.rs, f.np.rs_seg, f.np.analytic_calc, f.np.n_start, f.np.n_start_seg, f.np.p_max,
                f.np.p_max_seg};
-        for (int r = 0; r < f.n_rhs; r++, nl++) {
-            a.rhs0 = r;
-            far_adaptive_kernel<<<dim3(tiles, splits), kFarThreads, 0, s>>>(a, m.verts, m.nv, np);
-        }
-    } else if (tiles > 0) {
-        if (mixed) nl = ck ? launch_far_rhs<true, true>(a, tiles, splits, s) : launch_far_rhs<false, true>(a, tiles, splits, s);
-        else nl = ck ? launch_far_rhs<true, false>(a, tiles, splits, s) : launch_far_rhs<false, false>(a, tiles, splits, s);
+        far_refine_sum_kernel<<<dim3((f.n_pts + 7) / 8, f.n_rhs), 256, 0, s>>>(
+            a, markG, markK, m.verts, m.nv, np, partial + (size_t)splits * f.n_rhs * 12 * P);
+        nl++;
     }
     if (far_end) cudaEventRecord(far_end, s);
     if (tiles > 0) near_count_kernel<<<tiles, kFarThreads, 0, s>>>(mask, n_words, f.n_pts, counts);
@@ -718,7 +956,7 @@ cudaError_t field_stage2(const FieldLaunch& f, void* ws, int splits, long long n
     const size_t P = f.n_pts;
     char* w = (char*)ws;
     double* partial = (double*)w;
-    w += align256((size_t)splits * f.n_rhs * 12 * P * sizeof(double));
+    w += align256((size_t)partial_slots(f, splits) * f.n_rhs * 12 * P * sizeof(double));
     w += align256((P + 1) * sizeof(long long));
     long long* offs = (long long*)w;
     w += align256((P + 1) * sizeof(long long)) + align256(sizeof(long long));
@@ -752,7 +990,7 @@ cudaError_t field_stage2(const FieldLaunch& f, void* ws, int splits, long long n
     fa.n_pts = f.n_pts;
     fa.n_rhs = f.n_rhs;
     fa.n_cells = m.n_cells;
-    fa.splits = splits;
+    fa.splits = partial_slots(f, splits);
     fa.partial = partial;
     fa.offs = n_near > 0 ? offs : nullptr;
     fa.near = near;
@@ -768,7 +1006,7 @@ cudaError_t field_stage2(const FieldLaunch& f, void* ws, int splits, long long n
     fa.H = f.H;
     fa.nonfinite = d_nonfinite;
     if (tiles > 0 && f.n_rhs > 0) {
-        if (splits > 32) finalize_kernel<true><<<dim3((f.n_pts + 7) / 8, f.n_rhs), 256, 0, s>>>(fa);
+        if (fa.splits > 32) finalize_kernel<true><<<dim3((f.n_pts + 7) / 8, f.n_rhs), 256, 0, s>>>(fa);
         else finalize_kernel<false><<<dim3(tiles, f.n_rhs), kFarThreads, 0, s>>>(fa);
         *launches += 1;
     }

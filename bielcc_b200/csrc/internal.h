@@ -24,15 +24,21 @@ struct NumParamH {
 
 // Node split of the far pass. The reference's adaptive quadrature
 // (IntegralUniversalPnt, integral_universal.h:58-119 quads, :160-219
-// triangles) returns the last pass it computed once p_max passes are spent,
-// and the far operators run it with the smoothing radius at its floor
+// triangles) stops at the first pass after the first whose squared L2 change
+// is below eps^2, and returns the last pass it computed once p_max passes are
+// spent; the far operators run it with the smoothing radius at its floor
 // (K_RotRot_Far, K.h:293-295; R_Rot_Colloc, R.h:101-102), so it never halves.
-// With p_max = 2 a far pair's result is therefore the pass at 2 n_start,
-// whatever the convergence test decides: the table-driven far kernels
-// evaluate that pass alone. p_max >= 3 keeps the per-pair convergence test
-// (the adaptive far kernels). Near pairs always take the full schedule.
-inline int far_split_n(const NumParamH& np) { return np.p_max == 2 ? 2 * np.n_start : np.n_start; }
+// So a far pair's result is the pass at 2 n_start when p_max = 2 (whatever the
+// test decides), and also when p_max >= 3 and the test passes at that pass.
+// The table-driven far kernels evaluate that pass. With p_max >= 3 a first
+// kernel runs the test for every far pair (passes at n_start and 2 n_start);
+// the pairs that fail it (far_adaptive) take the full loop in a kernel of their
+// own. Near pairs always take the full schedule.
+inline int far_split_n(const NumParamH& np) { return np.p_max >= 2 ? 2 * np.n_start : np.n_start; }
 inline bool far_adaptive(const NumParamH& np) { return np.p_max > 2; }
+// p_max = 3: the pairs that fail the test return the third pass (4 n_start)
+// with no further test, so they too run the table-driven far kernels.
+inline bool far_third_pass(const NumParamH& np) { return np.p_max == 3; }
 
 // Device-resident mesh with its per-cell geometry and cached node tables.
 struct MeshDev {
@@ -45,6 +51,15 @@ struct MeshDev {
     double4* nodes64 = nullptr;  // [N][n*n]
     float4* nodes32 = nullptr;   // [N][n*n]
     float* rho32 = nullptr;      // [N] max |node - centre|
+    // p_max >= 3: the FP64 table at n_start (table_lo_n) of the convergence test
+    int table_lo_n = 0;
+    double4* nodes64_lo = nullptr;  // [N][n_start^2]
+    // p_max = 3: the tables at 4 n_start (table_hi_n), the last pass, which
+    // the pairs that fail the test take
+    int table_hi_n = 0;
+    double4* nodes64_hi = nullptr;
+    float4* nodes32_hi = nullptr;
+    float* rho32_hi = nullptr;
     size_t bytes = 0;
 };
 

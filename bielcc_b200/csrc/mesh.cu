@@ -60,6 +60,7 @@ __global__ void cell_geometry_kernel(const double* __restrict__ verts, int nv, i
 // triangle: lower then upper sub-triangle per (i, j), :166-193). FP64 rows
 // hold (y, weight); FP32 rows hold (y - centre, weight). Triangle weights are
 // area / n / n (the reference scales the sum once; same value up to rounding).
+// out32 and rho32 may be null (an FP64-only table).
 __global__ void node_table_kernel(const double* __restrict__ verts, const CellGeo* __restrict__ geo, int nv,
                                   int n_cells, int n, double4* __restrict__ out64, float4* __restrict__ out32,
                                   float* __restrict__ rho32) {
@@ -75,7 +76,7 @@ __global__ void node_table_kernel(const double* __restrict__ verts, const CellGe
     auto emit = [&](const double* y, double w) {
         out64[base + idx] = make_double4(y[0], y[1], y[2], w);
         float dx = (float)(y[0] - ctr[0]), dy = (float)(y[1] - ctr[1]), dz = (float)(y[2] - ctr[2]);
-        out32[base + idx] = make_float4(dx, dy, dz, (float)w);
+        if (out32) out32[base + idx] = make_float4(dx, dy, dz, (float)w);
         rmax = fmaxf(rmax, sqrtf(dx * dx + dy * dy + dz * dz));
         idx++;
     };
@@ -110,7 +111,7 @@ __global__ void node_table_kernel(const double* __restrict__ verts, const CellGe
                 }
             }
     }
-    rho32[c] = rmax;
+    if (rho32) rho32[c] = rmax;
 }
 
 cudaError_t launch_cell_geometry(const double* verts, int nv, int n_cells, CellGeo* geo, cudaStream_t s) {

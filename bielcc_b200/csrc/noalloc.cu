@@ -100,6 +100,21 @@ extern "C" int bielcc_field_EH_noalloc(int n_vert, int n_cells, const double* ce
     m.rho32 = (float*)(sp + off);
     off += b_rho;
     m.table_n = far_split_n(n);
+    if (far_adaptive(n)) {  // p_max >= 3: the FP64 table at n_start of the convergence test
+        m.nodes64_lo = (double4*)(sp + off);
+        off += al(N * (size_t)n.n_start * n.n_start * sizeof(double4));
+        m.table_lo_n = n.n_start;
+    }
+    if (far_third_pass(n)) {  // p_max = 3: the tables at 4 n_start of the third pass
+        const size_t nn3 = (size_t)16 * n.n_start * n.n_start;
+        m.nodes64_hi = (double4*)(sp + off);
+        off += al(N * nn3 * sizeof(double4));
+        m.nodes32_hi = (float4*)(sp + off);
+        off += al(N * nn3 * sizeof(float4));
+        m.rho32_hi = (float*)(sp + off);
+        off += al(N * sizeof(float));
+        m.table_hi_n = 4 * n.n_start;
+    }
 
     FieldLaunch f;
     f.mesh = &m;
@@ -145,6 +160,11 @@ extern "C" int bielcc_field_EH_noalloc(int n_vert, int n_cells, const double* ce
     cudaError_t e = launch_cell_geometry(m.verts, n_vert, n_cells, m.geo, s);
     if (e == cudaSuccess)
         e = launch_node_tables(m.verts, m.geo, n_vert, n_cells, far_split_n(n), m.nodes64, m.nodes32, m.rho32, s);
+    if (e == cudaSuccess && m.nodes64_lo)
+        e = launch_node_tables(m.verts, m.geo, n_vert, n_cells, n.n_start, m.nodes64_lo, nullptr, nullptr, s);
+    if (e == cudaSuccess && m.nodes64_hi)
+        e = launch_node_tables(m.verts, m.geo, n_vert, n_cells, m.table_hi_n, m.nodes64_hi, m.nodes32_hi, m.rho32_hi,
+                               s);
     int l1 = 0, lf = 0, l2 = 0;
     if (e == cudaSuccess) e = field_stage1(f, ws, splits, d_total, s, &l1, nullptr, nullptr, &lf);
     long long n_near = 0;  // pageable host copy: no pinned staging is allocated

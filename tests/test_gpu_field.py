@@ -67,13 +67,14 @@ def test_sphere8192_near_and_far_subset(gctx):
 
 
 @pytest.mark.parametrize("n_start,n_seg,p_max", [(4, 5, 1), (10, 12, 1), (20, 10, 1), (4, 6, 2), (8, 10, 2),
-                                                  (3, 4, 3)])
+                                                  (3, 4, 3), (8, 10, 3), (4, 5, 4)])
 def test_quadrature_splits_and_adaptive(gctx, n_start, n_seg, p_max):
     """Node tiles that fill one stage partially (n=4), several cells per stage
     (n=10), chunked cells (n=20: 400 nodes > one stage) and adaptive refinement:
-    p_max = 2 runs the far pairs through the table-driven kernels at 2 n_start
-    (FP64 and mixed), p_max = 3 through the per-pair adaptive kernel, against
-    the oracle's full refinement loop."""
+    p_max = 2 runs the far pairs through the table-driven kernels at 2 n_start;
+    p_max >= 3 tests convergence between the passes at n_start and 2 n_start
+    for every far pair and runs the failing ones through the whole loop. FP64
+    and mixed, against the oracle's full refinement loop."""
     cells = W.uv_sphere(8, 16)
     J = W.po_currents(cells, 4.0, directions=3, seed=5)
     rng = np.random.default_rng(n_start)
@@ -83,9 +84,29 @@ def test_quadrature_splits_and_adaptive(gctx, n_start, n_seg, p_max):
     E, H, _ = gctx.field_EH(m, J, 4.0, pts, numparam=npm)
     Eo, Ho = oracle.field_EH(cells, J, 4.0, pts, npm)
     assert rel_l2(E, Eo) < TOL_FP64 and rel_l2(H, Ho) < TOL_FP64
-    if p_max <= 2:
-        Em, Hm, _ = gctx.field_EH(m, J, 4.0, pts, numparam=npm, precision="mixed")
-        assert rel_l2(Em, Eo) < TOL_MIXED and rel_l2(Hm, Ho) < TOL_MIXED
+    Em, Hm, _ = gctx.field_EH(m, J, 4.0, pts, numparam=npm, precision="mixed")
+    assert rel_l2(Em, Eo) < TOL_MIXED and rel_l2(Hm, Ho) < TOL_MIXED
+
+
+@pytest.mark.parametrize("p_max", [3, 4])
+@pytest.mark.parametrize("eps", [1e-14, 1e3])
+def test_adaptive_far_refinement_paths(gctx, eps, p_max):
+    """Every far pair failing the convergence test at the second pass (eps =
+    1e-14: with p_max = 3 all take the third pass from the 4 n_start tables,
+    with p_max = 4 the whole loop in the refinement kernel) and none failing
+    (eps = 1e3: all take the pass at 2 n_start); triangles and quads, complex
+    k, 3 RHS; FP64 against the oracle's loop."""
+    rng = np.random.default_rng(8)
+    for cells, k in ((W.uv_sphere(6, 12), 3.0), (W.perturbed_icosphere(1, seed=3), complex(2.5, 0.4))):
+        J = W.po_currents(cells, abs(k), directions=3, seed=2)
+        pts = np.concatenate([W.sphere_points(20, 2.0, 7), W.near_points(cells, 6, 0.02, 0.4, rng)])
+        npm = abi.NumParam.default(n_start=3, n_start_seg=4, p_max=p_max, p_max_seg=2)
+        npm.eps = eps
+        m = gctx.mesh(cells)
+        E, H, _ = gctx.field_EH(m, J, k, pts, numparam=npm)
+        Eo, Ho = oracle.field_EH(cells, J, k, pts, npm)
+        assert rel_l2(E, Eo) < TOL_FP64 and rel_l2(H, Ho) < TOL_FP64
+        m.close()
 
 
 def test_multi_rhs_chunks_and_large_k(gctx):

@@ -84,6 +84,11 @@ def test_noalloc_matches_allocating_entry_point_twice():
     (Ea, Ha), (Eb, Hb), rep = run_both(pts2, "fp64", np2)
     assert rel_l2(Eb, Ea) < TOL_FP64 and rel_l2(Hb, Ha) < TOL_FP64
 
+    # call 4: p_max = 3 (the n_start table of the convergence test joins the array)
+    np3 = abi.NumParam.default(p_max=3, p_max_seg=2)
+    (Ea, Ha), (Eb, Hb), rep = run_both(pts2, "fp64", np3)
+    assert rel_l2(Eb, Ea) < TOL_FP64 and rel_l2(Hb, Ha) < TOL_FP64
+
     mesh.close()
     ctx.close()
 
