@@ -295,10 +295,16 @@ int bielcc_field_EH_full_device(bielcc_ctx ctx, bielcc_mesh mesh, int n_rhs,
  * rejected with BIELCC_ERR_ARG and a message giving the bytes needed. The
  * scratch is, in bytes (each term rounded up to 256):
  *   per cell:  128 + 48 n^2 + 4              (3204 B = 3.1 KiB at n = 8; n is
- *                                             n_start, or 2 n_start when p_max = 2)
+ *                                             n_start for p_max = 1, else
+ *                                             2 n_start)
+ *              + 32 n_start^2                (p_max >= 3)
+ *              + 48 (4 n_start)^2 + 4        (p_max = 3)
  *   per point: 96 n_rhs per cell split + 96 n_rhs (near sums) + 16
  *              + 4 ceil(n_cells / 32)        (near-cell mask: 1 KiB per point
  *                                             at 8192 cells)
+ *              + 4 ceil(n_cells / 32) (1 + n_rhs) and one more cell split
+ *                                            (p_max >= 3: test marks; p_max = 3
+ *                                             doubles the cell splits)
  *   per near pair: 216
  * The far partial sums take at most half of what is left after the cells and
  * a one-split workspace; the cell-split count is capped to fit. Every call
