@@ -1627,7 +1627,7 @@ int bielcc_assemble_K_device(bielcc_ctx ctx, bielcc_mesh mesh, double k_re, doub
     if (!A_dev) return set_error(BIELCC_ERR_ARG, "null matrix");
     cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
     TRY(ws_acquire(ctx, s));
-    TRY(ensure_tables(m, far_split_n(n), s));
+    TRY(ensure_far_tables(m, n, s));
     AssembleLaunch a{m, mk(k_re, k_im), n, layout, out_c64 ? 1 : 0, precision, A_dev};
     TRY(ctx->ws.ensure(assemble_ws_base_bytes(a)));
     TRY(ctx->scratch_small.ensure(256));

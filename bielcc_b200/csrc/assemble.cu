@@ -42,6 +42,18 @@ struct AsmArgs {
     unsigned* mask;  // [ceil(N/32)][N] near bits of (row i, column word) written by the far kernel, or null
 };
 
+// p_max >= 3, the far kernel's marks-reading variant: mark[b] [ceil(N/32)][N]
+// is set for the (row, column) blocks whose column-b integral failed the
+// convergence test at the second pass; take_marked 0 writes the columns that
+// passed, 1 the ones that failed. (A separate type, so that the plain
+// variants keep AsmArgs' parameter block.)
+struct AsmArgsMarks : AsmArgs {
+    const unsigned* mark;
+    int take_marked;
+};
+template <bool MARKS>
+using AsmArgsOf = typename std::conditional<MARKS, AsmArgsMarks, AsmArgs>::type;
+
 BIELCC_D bool asm_is_near(const double* x, const CellGeo& g, double analytic_calc, double* d) {
     *d = dist3_rn(x, g.c);
     return *d < __dmul_rn(analytic_calc, g.diam);
@@ -53,7 +65,8 @@ BIELCC_D bool asm_is_near(const double* x, const CellGeo& g, double analytic_cal
 // block stays in registers.
 template <int M>
 BIELCC_D void write_block_m(const AsmArgs& a, int i, int j, const double (&Kr)[3][3], const double (&Ki)[3][3],
-                            const double* ti1, const double* ti2, const double* tj1, const double* tj2) {
+                            const double* ti1, const double* ti2, const double* tj1, const double* tj2,
+                            unsigned cols = ~0u) {
     const size_t dim = (size_t)M * a.n_cells;
 #pragma unroll
     for (int aa = 0; aa < M; aa++) {
@@ -82,11 +95,13 @@ BIELCC_D void write_block_m(const AsmArgs& a, int i, int j, const double (&Kr)[3
         if (a.c64) {
             float2* dst = reinterpret_cast<float2*>(a.A) + off;
 #pragma unroll
-            for (int b = 0; b < M; b++) dst[b] = make_float2((float)rv[b][0], (float)rv[b][1]);
+            for (int b = 0; b < M; b++)
+                if ((cols >> b) & 1u) dst[b] = make_float2((float)rv[b][0], (float)rv[b][1]);
         } else {
             double2* dst = reinterpret_cast<double2*>(a.A) + off;
 #pragma unroll
-            for (int b = 0; b < M; b++) dst[b] = make_double2(rv[b][0], rv[b][1]);
+            for (int b = 0; b < M; b++)
+                if ((cols >> b) & 1u) dst[b] = make_double2(rv[b][0], rv[b][1]);
         }
     }
 }
@@ -95,9 +110,12 @@ BIELCC_D void write_block_m(const AsmArgs& a, int i, int j, const double (&Kr)[3
 // K = A1 I + T with T symmetric (xx, xy, xz, yy, yz, zz), projected on the two
 // cells' tangents (M = 2: u_b = K t_b, A_ab = t_a . u_b) or kept Cartesian
 // (M = 3), times ph = e^{ik r0} / 4pi.
+// cols: bit b writes column b of the block (the convergence-test passes of
+// p_max >= 3; all otherwise).
 template <int M>
 BIELCC_D void write_block_f32(const AsmArgs& a, int i, int j, float a1r, float a1i, const float (&t)[6][2], float phr,
-                              float phi, const float (&ti)[2][3], const double* tj1, const double* tj2) {
+                              float phi, const float (&ti)[2][3], const double* tj1, const double* tj2,
+                              unsigned cols = ~0u) {
     const size_t dim = (size_t)M * a.n_cells;
     const int sym[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
     float kr[6], ki[6];
@@ -142,19 +160,22 @@ BIELCC_D void write_block_f32(const AsmArgs& a, int i, int j, float a1r, float a
         if (a.c64) {
             float2* dst = reinterpret_cast<float2*>(a.A) + off;
 #pragma unroll
-            for (int b = 0; b < M; b++) dst[b] = make_float2(out[aa][b][0], out[aa][b][1]);
+            for (int b = 0; b < M; b++)
+                if ((cols >> b) & 1u) dst[b] = make_float2(out[aa][b][0], out[aa][b][1]);
         } else {
             double2* dst = reinterpret_cast<double2*>(a.A) + off;
 #pragma unroll
-            for (int b = 0; b < M; b++) dst[b] = make_double2(out[aa][b][0], out[aa][b][1]);
+            for (int b = 0; b < M; b++)
+                if ((cols >> b) & 1u) dst[b] = make_double2(out[aa][b][0], out[aa][b][1]);
         }
     }
 }
 
 BIELCC_D void write_block(const AsmArgs& a, int i, int j, const double (&Kr)[3][3], const double (&Ki)[3][3],
-                          const double* ti1, const double* ti2, const double* tj1, const double* tj2) {
-    if (a.m == 2) write_block_m<2>(a, i, j, Kr, Ki, ti1, ti2, tj1, tj2);
-    else write_block_m<3>(a, i, j, Kr, Ki, ti1, ti2, tj1, tj2);
+                          const double* ti1, const double* ti2, const double* tj1, const double* tj2,
+                          unsigned cols = ~0u) {
+    if (a.m == 2) write_block_m<2>(a, i, j, Kr, Ki, ti1, ti2, tj1, tj2, cols);
+    else write_block_m<3>(a, i, j, Kr, Ki, ti1, ti2, tj1, tj2, cols);
 }
 
 // Minimum resident CTAs per SM asked of the real-k mixed far kernel (0: the
@@ -163,8 +184,9 @@ BIELCC_D void write_block(const AsmArgs& a, int i, int j, const double (&Kr)[3][
 #ifndef BIELCC_ASM_MINB
 #define BIELCC_ASM_MINB 5
 #endif
-template <bool CK, bool MIXED>
-__global__ void __launch_bounds__(kAsmThreads, (!CK && MIXED) ? BIELCC_ASM_MINB : 0) assemble_far_kernel(AsmArgs a) {
+template <bool CK, bool MIXED, bool MARKS = false>
+__global__ void __launch_bounds__(kAsmThreads, (!CK && MIXED) ? BIELCC_ASM_MINB : 0)
+    assemble_far_kernel(AsmArgsOf<MARKS> a) {
     using NodeT = typename std::conditional<MIXED, float4, double4>::type;
     __shared__ __align__(16) NodeT s_nodes[kAsmStageNodes];
     __shared__ float s_yy[MIXED ? kAsmStageNodes : 1];  // |y - centre|^2 of the staged nodes (mixed form)
@@ -187,6 +209,7 @@ __global__ void __launch_bounds__(kAsmThreads, (!CK && MIXED) ? BIELCC_ASM_MINB 
     using F = typename std::conditional<MIXED, float, double>::type;
     F a1r = 0, a1i = 0, t[6][2];
     bool far = false;
+    unsigned cols = ~0u;  // MARKS: the block columns this pass writes
     PairF32 pf{};
     const KF32 kf = KF32::make(a.k.re, a.k.im);
     // the row cell's tangents in FP32 (mixed-form block projection)
@@ -232,6 +255,18 @@ __global__ void __launch_bounds__(kAsmThreads, (!CK && MIXED) ? BIELCC_ASM_MINB 
                     double d;
                     const bool nr = asm_is_near(x, gj, a.analytic_calc, &d);
                     far = live && !nr;
+                    if constexpr (MARKS) {
+                        if (far) {
+                            const int c = c0 + cc;
+                            const size_t wi = (size_t)(c >> 5) * a.n_cells + i;
+                            const size_t plane = (size_t)((a.n_cells + 31) >> 5) * a.n_cells;
+                            cols = 0u;
+                            for (int b = 0; b < a.m; b++)
+                                if ((((a.mark[b * plane + wi] >> (c & 31)) & 1u) != 0) == (a.take_marked != 0))
+                                    cols |= 1u << b;
+                            far = cols != 0u;
+                        }
+                    }
                     if (a.mask) {
                         const int c = c0 + cc;
                         nbits |= (nr ? 1u : 0u) << (c & 31);
@@ -318,8 +353,13 @@ __global__ void __launch_bounds__(kAsmThreads, (!CK && MIXED) ? BIELCC_ASM_MINB 
                     if constexpr (MIXED) {
                         if constexpr (!CK) finish_real_k<F>(a1r, a1i, t);
                         const float phr = (float)(P0r * kInvFourPi), phi = (float)(P0i * kInvFourPi);
-                        if (a.m == 2) write_block_f32<2>(a, i, c0 + cc, a1r, a1i, t, phr, phi, tif, gj.t1, gj.t2);
-                        else write_block_f32<3>(a, i, c0 + cc, a1r, a1i, t, phr, phi, tif, gj.t1, gj.t2);
+                        if constexpr (MARKS) {
+                            if (a.m == 2) write_block_f32<2>(a, i, c0 + cc, a1r, a1i, t, phr, phi, tif, gj.t1, gj.t2, cols);
+                            else write_block_f32<3>(a, i, c0 + cc, a1r, a1i, t, phr, phi, tif, gj.t1, gj.t2, cols);
+                        } else {
+                            if (a.m == 2) write_block_f32<2>(a, i, c0 + cc, a1r, a1i, t, phr, phi, tif, gj.t1, gj.t2);
+                            else write_block_f32<3>(a, i, c0 + cc, a1r, a1i, t, phr, phi, tif, gj.t1, gj.t2);
+                        }
                     } else {
                         // K = (A1 I + T) * P0 / 4pi
                         const int ti[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
@@ -331,7 +371,8 @@ __global__ void __launch_bounds__(kAsmThreads, (!CK && MIXED) ? BIELCC_ASM_MINB 
                                 Kr[p][q] = (vr * P0r - vi * P0i) * kInvFourPi;
                                 Ki[p][q] = (vr * P0i + vi * P0r) * kInvFourPi;
                             }
-                        write_block(a, i, c0 + cc, Kr, Ki, gi.t1, gi.t2, gj.t1, gj.t2);
+                        if constexpr (MARKS) write_block(a, i, c0 + cc, Kr, Ki, gi.t1, gi.t2, gj.t1, gj.t2, cols);
+                        else write_block(a, i, c0 + cc, Kr, Ki, gi.t1, gi.t2, gj.t1, gj.t2);
                     }
                 }
             }
@@ -339,26 +380,129 @@ __global__ void __launch_bounds__(kAsmThreads, (!CK && MIXED) ? BIELCC_ASM_MINB 
     }
 }
 
-// Far entries with adaptive refinement (p_max > 2): K_RotRot_Far's
-// convergence depends on the current, so each column basis vector runs its
-// own adaptive quadrature (generic per-pair code, nodes on the fly).
-__global__ void assemble_far_adaptive_kernel(AsmArgs a, const double* __restrict__ verts, int nv, DNP np) {
+// ---------------------------------------------------------------- adaptive far blocks (p_max >= 3)
+// The reference runs one refinement loop per matrix column: K_RotRot_Far
+// (K.h:288-301) of the column's basis current J_b (tau_b of the column cell, or
+// e_b) at the row cell's centre, which stops at the first pass after the first
+// whose squared change is below eps^2 (integral_universal.h:58-119), else
+// returns its last pass. asm_refine_decide_kernel runs the test at the second
+// pass for every far block and column from the FP64 node tables at n_start and
+// 2 n_start, writes the near mask, and marks the failing columns in
+// mark[b]. The marks-reading far kernel then writes the columns that passed
+// from the 2 n_start tables and, with p_max = 3, the failing ones from the
+// 4 n_start tables; with p_max > 3 the failing ones run the whole loop in
+// assemble_far_refine_kernel.
+
+// One FP64 pass over a cell's node table row (the field kernels' FP64 node,
+// K moments only), finished and ready for K = (A1 I + T) J.
+template <bool CK>
+BIELCC_D void asm_pass_f64(Moments<double>& m, const double4* __restrict__ nd, int nn, const double* x, cplx k,
+                           double k2r, double k2i, double r0, bool split) {
+    m.zero();
+    if (split) {
+        for (int q = 0; q < nn; q++) {
+            const double4 v = nd[q];
+            far_node_f64<CK, true>(m, x[0] - v.x, x[1] - v.y, x[2] - v.z, v.w, k, k2r, k2i, r0);
+        }
+    } else {
+        for (int q = 0; q < nn; q++) {
+            const double4 v = nd[q];
+            far_node_f64<CK, false>(m, x[0] - v.x, x[1] - v.y, x[2] - v.z, v.w, k, k2r, k2i, r0);
+        }
+    }
+    if (!CK) m.finish_real_k();
+}
+
+// The squared change of column b's raw integral (A1 J + T J) P0 between two
+// passes, |.| taken first as in integral_universal.h:96-99.
+BIELCC_D double asm_delta2(const Moments<double>& m0, const Moments<double>& m1, const double* J, double pr,
+                           double pi) {
+    const int ti[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+    double d = 0.;
+    for (int p = 0; p < 3; p++) {
+        double e0r = m0.a1r * J[p], e0i = m0.a1i * J[p], e1r = m1.a1r * J[p], e1i = m1.a1i * J[p];
+        for (int q = 0; q < 3; q++) {
+            e0r += m0.t[ti[p][q]][0] * J[q];
+            e0i += m0.t[ti[p][q]][1] * J[q];
+            e1r += m1.t[ti[p][q]][0] * J[q];
+            e1i += m1.t[ti[p][q]][1] * J[q];
+        }
+        const cplx k0 = mk(e0r, e0i) * mk(pr, pi), k1 = mk(e1r, e1i) * mk(pr, pi);
+        const double t = sqrt(cabs2(k1 - k0));
+        d += t * t;
+    }
+    return d;
+}
+
+__global__ void asm_refine_decide_kernel(AsmArgs a, const double4* __restrict__ lo, int nn_lo, double eps2,
+                                         unsigned* __restrict__ mark) {
+    const int i = blockIdx.x * kAsmThreads + threadIdx.x;
+    if (i >= a.n_cells) return;
+    const CellGeo gi = a.geo[i];
+    const double* x = gi.c;
+    const int cb = blockIdx.y * a.cols_per_split;
+    const int ce = min(a.n_cells, cb + a.cols_per_split);
+    const bool ck = a.k.im != 0.0;
+    const double k2r = a.k.re * a.k.re - a.k.im * a.k.im, k2i = 2.0 * a.k.re * a.k.im;
+    const size_t plane = (size_t)((a.n_cells + 31) >> 5) * a.n_cells;
+    unsigned nbits = 0, mb[3] = {0u, 0u, 0u};
+    for (int j = cb; j < ce; j++) {
+        const CellGeo& gj = a.geo[j];
+        double d;
+        const bool nr = asm_is_near(x, gj, a.analytic_calc, &d);
+        if (!nr) {
+            const bool split = !ck && fabs(a.k.re) * (double)a.rho32[j] * (1.0 + 1e-6) <= 0.5;
+            double pr = 1.0, pi = 0.0;
+            if (split) sincos(a.k.re * d, &pi, &pr);
+            Moments<double> m0, m1;
+            if (ck) {
+                asm_pass_f64<true>(m0, lo + (size_t)j * nn_lo, nn_lo, x, a.k, k2r, k2i, d, false);
+                asm_pass_f64<true>(m1, a.nodes64 + (size_t)j * a.nn, a.nn, x, a.k, k2r, k2i, d, false);
+            } else {
+                asm_pass_f64<false>(m0, lo + (size_t)j * nn_lo, nn_lo, x, a.k, k2r, k2i, d, split);
+                asm_pass_f64<false>(m1, a.nodes64 + (size_t)j * a.nn, a.nn, x, a.k, k2r, k2i, d, split);
+            }
+            for (int b = 0; b < a.m; b++) {
+                double J[3];
+                for (int g = 0; g < 3; g++) J[g] = a.m == 3 ? (g == b ? 1. : 0.) : (b == 0 ? gj.t1[g] : gj.t2[g]);
+                if (!(asm_delta2(m0, m1, J, pr, pi) < eps2)) mb[b] |= 1u << (j & 31);
+            }
+        }
+        nbits |= (nr ? 1u : 0u) << (j & 31);
+        if ((j & 31) == 31 || j == ce - 1) {
+            const size_t wi = (size_t)(j >> 5) * a.n_cells + i;
+            if (a.mask) a.mask[wi] = nbits;
+            for (int b = 0; b < a.m; b++) mark[b * plane + wi] = mb[b];
+            nbits = 0;
+            mb[0] = mb[1] = mb[2] = 0u;
+        }
+    }
+}
+
+// p_max > 3: the marked (row, column, basis) far entries through the whole
+// loop (integral_cell, ops.cuh: nodes on the fly).
+__global__ void assemble_far_refine_kernel(AsmArgs a, const unsigned* __restrict__ mark, const double* __restrict__ verts,
+                                           int nv, DNP np) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n_cells) return;
     const CellGeo gi = a.geo[i];
     const int cb = blockIdx.y * a.cols_per_split;
     const int ce = min(a.n_cells, cb + a.cols_per_split);
+    const int m = a.m;
+    const size_t plane = (size_t)((a.n_cells + 31) >> 5) * a.n_cells;
     for (int j = cb; j < ce; j++) {
+        const size_t wi = (size_t)(j >> 5) * a.n_cells + i;
+        unsigned cols = 0u;
+        for (int b = 0; b < m; b++) cols |= ((mark[b * plane + wi] >> (j & 31)) & 1u) << b;
+        if (!cols) continue;
         const CellGeo& gj = a.geo[j];
-        double d;
-        if (asm_is_near(gi.c, gj, a.analytic_calc, &d)) continue;
         DCell cl;
         cl.nv = nv;
         for (int v = 0; v < nv; v++)
             for (int g = 0; g < 3; g++) cl.v[v][g] = verts[((size_t)j * nv + v) * 3 + g];
-        const int m = a.m;
         cplx v[3][3];  // v[b] = K[J_b], J_b = tau_b(j) (TAU2) or e_b (FULL3)
         for (int b = 0; b < m; b++) {
+            if (!((cols >> b) & 1u)) continue;
             DKP kp;
             dkp_zero(kp);
             kp.smoothR = kMachineZero;
@@ -372,6 +516,7 @@ __global__ void assemble_far_adaptive_kernel(AsmArgs a, const double* __restrict
         for (int aa = 0; aa < m; aa++) {
             size_t off = ((size_t)i * m + aa) * dim + (size_t)j * m;
             for (int b = 0; b < m; b++) {
+                if (!((cols >> b) & 1u)) continue;
                 cplx e = m == 3 ? v[b][aa]
                                 : (aa == 0 ? v[b][0] * gi.t1[0] + v[b][1] * gi.t1[1] + v[b][2] * gi.t1[2]
                                            : v[b][0] * gi.t2[0] + v[b][1] * gi.t2[1] + v[b][2] * gi.t2[2]);
@@ -569,14 +714,18 @@ __global__ void asm_error_sum_kernel(const double2* __restrict__ part, int n, do
 
 static size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
 
+// Column blocks of the (row, column word) marks of p_max >= 3: one per basis vector.
+static int asm_mark_planes(const AssembleLaunch& a) { return far_adaptive(a.np) ? (a.layout == 1 ? 3 : 2) : 0; }
+
 size_t assemble_ws_base_bytes(const AssembleLaunch& a) {
     size_t N = a.mesh->n_cells;
-    return 2 * al256((N + 1) * sizeof(long long)) + al256((N + 31) / 32 * N * sizeof(unsigned)) + 256;
+    return 2 * al256((N + 1) * sizeof(long long)) + al256((N + 31) / 32 * N * sizeof(unsigned)) + 256 +
+           al256((size_t)asm_mark_planes(a) * ((N + 31) / 32) * N * sizeof(unsigned));
 }
 
-// The far kernel writes the near mask (and count / fill read it) unless the
-// adaptive far kernel runs, which tests pairs on its own.
-static bool uses_mask(const AssembleLaunch& a) { return !far_adaptive(a.np); }
+// The near mask is written by the far kernel (p_max <= 2) or the decision
+// kernel (p_max >= 3); count / fill read it.
+static bool uses_mask(const AssembleLaunch&) { return true; }
 
 static AsmArgs make_args(const AssembleLaunch& a) {
     const MeshDev& m = *a.mesh;
@@ -597,19 +746,18 @@ static AsmArgs make_args(const AssembleLaunch& a) {
 }
 
 // Resident CTAs (whole GPU) of the far assembly kernel variant.
-static int asm_slots(bool ck, bool mixed, bool adaptive) {
-    static std::atomic<int> cache[2][2][2];
-    std::atomic<int>& c = cache[adaptive][ck][mixed];
+static int asm_slots(bool ck, bool mixed) {
+    static std::atomic<int> cache[2][2];
+    std::atomic<int>& c = cache[ck][mixed];
     int v = c.load(std::memory_order_relaxed);
     if (v) return v;
     int dev = 0, sms = 148, per = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const void* fn = adaptive ? (const void*)assemble_far_adaptive_kernel
-                              : (ck ? (mixed ? (const void*)assemble_far_kernel<true, true>
-                                             : (const void*)assemble_far_kernel<true, false>)
-                                    : (mixed ? (const void*)assemble_far_kernel<false, true>
-                                             : (const void*)assemble_far_kernel<false, false>));
+    const void* fn = ck ? (mixed ? (const void*)assemble_far_kernel<true, true>
+                                 : (const void*)assemble_far_kernel<true, false>)
+                        : (mixed ? (const void*)assemble_far_kernel<false, true>
+                                 : (const void*)assemble_far_kernel<false, false>);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, kAsmThreads, 0);
     v = std::max(1, sms * std::max(1, per));
     c.store(v, std::memory_order_relaxed);
@@ -628,15 +776,49 @@ cudaError_t assemble_stage1(const AssembleLaunch& a, void* ws, long long* d_tota
     int tiles = (N + kAsmThreads - 1) / kAsmThreads;
     bool ck = a.k.im != 0.;
     // column splits in whole 32-column words, so every mask word has one writer
-    if (!far_adaptive(a.np) && m.table_n != far_split_n(a.np))
+    if (m.table_n != far_split_n(a.np))
         return cudaErrorInvalidValue;  // node tables of another split: the caller builds far_split_n's
-    int splits = choose_cell_splits(tiles, N, asm_slots(ck, a.precision == 1, far_adaptive(a.np)), N);
+    if (far_adaptive(a.np) && (m.table_lo_n != a.np.n_start || !m.nodes64_lo))
+        return cudaErrorInvalidValue;  // no n_start table for the convergence test
+    if (far_third_pass(a.np) && (m.table_hi_n != 4 * a.np.n_start || !m.nodes64_hi))
+        return cudaErrorInvalidValue;  // no 4 n_start tables for the third pass
+    int splits = choose_cell_splits(tiles, N, asm_slots(ck, a.precision == 1), N);
     g.cols_per_split = round_cells_per_split(N, splits);
     dim3 grid(tiles, splits);
     if (far_adaptive(a.np)) {
-        DNP np{a.np.eps, a.np.rs, a.np.rs_seg, a.np.analytic_calc, a.np.n_start, a.np.n_start_seg, a.np.p_max,
-               a.np.p_max_seg};
-        assemble_far_adaptive_kernel<<<grid, kAsmThreads, 0, s>>>(g, m.verts, m.nv, np);
+        unsigned* mark = (unsigned*)((char*)mask + al256((size_t)n_words * N * sizeof(unsigned)) + 256);
+        asm_refine_decide_kernel<<<grid, kAsmThreads, 0, s>>>(g, m.nodes64_lo, a.np.n_start * a.np.n_start,
+                                                              a.np.eps * a.np.eps, mark);
+        AsmArgsMarks gm;
+        static_cast<AsmArgs&>(gm) = g;
+        gm.mask = nullptr;  // written by the decision kernel
+        gm.mark = mark;
+        gm.take_marked = 0;  // the columns that passed: the pass at 2 n_start
+        if (a.precision == 1) {
+            if (ck) assemble_far_kernel<true, true, true><<<grid, kAsmThreads, 0, s>>>(gm);
+            else assemble_far_kernel<false, true, true><<<grid, kAsmThreads, 0, s>>>(gm);
+        } else {
+            if (ck) assemble_far_kernel<true, false, true><<<grid, kAsmThreads, 0, s>>>(gm);
+            else assemble_far_kernel<false, false, true><<<grid, kAsmThreads, 0, s>>>(gm);
+        }
+        if (far_third_pass(a.np)) {  // p_max = 3: the failing columns return the pass at 4 n_start
+            gm.nodes64 = m.nodes64_hi;
+            gm.nodes32 = m.nodes32_hi;
+            gm.rho32 = m.rho32_hi;
+            gm.nn = 16 * a.np.n_start * a.np.n_start;
+            gm.take_marked = 1;
+            if (a.precision == 1) {
+                if (ck) assemble_far_kernel<true, true, true><<<grid, kAsmThreads, 0, s>>>(gm);
+                else assemble_far_kernel<false, true, true><<<grid, kAsmThreads, 0, s>>>(gm);
+            } else {
+                if (ck) assemble_far_kernel<true, false, true><<<grid, kAsmThreads, 0, s>>>(gm);
+                else assemble_far_kernel<false, false, true><<<grid, kAsmThreads, 0, s>>>(gm);
+            }
+        } else {
+            DNP np{a.np.eps, a.np.rs, a.np.rs_seg, a.np.analytic_calc, a.np.n_start, a.np.n_start_seg, a.np.p_max,
+                   a.np.p_max_seg};
+            assemble_far_refine_kernel<<<grid, kAsmThreads, 0, s>>>(g, mark, m.verts, m.nv, np);
+        }
     } else if (a.precision == 1) {
         if (ck) assemble_far_kernel<true, true><<<grid, kAsmThreads, 0, s>>>(g);
         else assemble_far_kernel<false, true><<<grid, kAsmThreads, 0, s>>>(g);
