@@ -279,8 +279,8 @@ struct FieldArgs {
 int field_device_batched(bielcc_ctx ctx, const FieldArgs& a, cudaStream_t s, bielcc_report* rep,
                          unsigned long long* d_nonfinite, bool* done, const WsSet& w) {
     *done = false;
-    if (a.n_rhs <= 2 || a.np.p_max > 1 || a.np.n_start > kBatchMaxNStart || a.n_pts == 0) return BIELCC_OK;
-    TRY(ensure_tables(a.m, a.np.n_start, s));
+    if (a.n_rhs <= 2 || far_adaptive(a.np) || far_split_n(a.np) > kBatchMaxNStart || a.n_pts == 0) return BIELCC_OK;
+    TRY(ensure_tables(a.m, far_split_n(a.np), s));
     JobDev d;
     memset(&d, 0, sizeof(d));
     d.geo = a.m->geo;
@@ -310,13 +310,13 @@ int field_device_batched(bielcc_ctx ctx, const FieldArgs& a, cudaStream_t s, bie
     BatchPlan bp;
     const bool mixed = a.precision == BIELCC_PREC_MIXED;
     const size_t split = ctx_batch_split_cap(ctx);
-    plan_batch(bp, std::vector<JobDev>{d}, a.np.n_start, mixed, ctx->batch_item_cost, ctx->batch_tc, split);
+    plan_batch(bp, std::vector<JobDev>{d}, far_split_n(a.np), mixed, ctx->batch_item_cost, ctx->batch_tc, split);
     // The tuned item size suits batches of many jobs; one job alone is cut
     // finer (up to its range limit) when its items would leave resident CTAs idle.
     if ((int)bp.items.size() < 2 * bp.workers()) {
         const double finer = std::max(1.0e5, ctx->batch_item_cost * bp.items.size() / (2.0 * bp.workers()));
         if (finer < ctx->batch_item_cost)
-            plan_batch(bp, std::vector<JobDev>{d}, a.np.n_start, mixed, finer, ctx->batch_tc, split);
+            plan_batch(bp, std::vector<JobDev>{d}, far_split_n(a.np), mixed, finer, ctx->batch_tc, split);
     }
     const double busy = std::min(1.0, (double)bp.items.size() / std::max(1, bp.workers()));
     const int S = a.n_rhs;
@@ -325,7 +325,7 @@ int field_device_batched(bielcc_ctx ctx, const FieldArgs& a, cudaStream_t s, bie
     TRY(w.ws->ensure(bp.ws_bytes));
     BatchDevPtrs dp;
     int l1 = 0, l2 = 0;
-    TRY_CUDA(batch_stage1(bp, w.ws->p, a.np.analytic_calc, a.np.n_start, a.k.im != 0., s, &dp, &l1));
+    TRY_CUDA(batch_stage1(bp, w.ws->p, a.np.analytic_calc, far_split_n(a.np), a.k.im != 0., s, &dp, &l1));
     TRY_CUDA(batch_status_to_host(dp, w.h_total, s));
     TRY_CUDA(cudaStreamSynchronize(s));
     if (batch_timed_out(w.h_total)) return set_error(BIELCC_ERR_TIMEOUT, "batched far kernel: a bounded wait ran out");
@@ -964,7 +964,7 @@ int jobs_to_dev(int n_jobs, const bielcc_field_job* jobs, const std::vector<Mesh
     for (int i = 0; i < n_jobs; i++) {
         const bielcc_field_job& j = jobs[i];
         MeshDev* m = meshes[i];
-        TRY(ensure_tables(m, n.n_start, s));
+        TRY(ensure_tables(m, far_split_n(n), s));
         JobDev& d = jd[i];
         memset(&d, 0, sizeof(d));
         d.geo = m->geo;
@@ -1080,9 +1080,9 @@ int batch_est_begin(bielcc_ctx ctx, const std::vector<JobDev>& jd, const bielcc_
     TRY_CUDA(cudaStreamWaitEvent(ctx->side, ctx->side_in, 0));
     TRY_CUDA(cudaMemcpyAsync(e.d_ej, e.ej.data(), jd.size() * sizeof(ErrJob), cudaMemcpyHostToDevice, ctx->side));
     TRY_CUDA(err_gather(e.d_ej, e.n_jobs, e.spts, ctx->side));
-    plan_batch(e.bp, e.js, n.n_start, false, item_cost, false);
+    plan_batch(e.bp, e.js, far_split_n(n), false, item_cost, false);
     TRY(ctx->side_ws.ensure(e.bp.ws_bytes));
-    TRY_CUDA(batch_stage1(e.bp, ctx->side_ws.p, n.analytic_calc, n.n_start, ck, ctx->side, &e.d, &e.l1));
+    TRY_CUDA(batch_stage1(e.bp, ctx->side_ws.p, n.analytic_calc, far_split_n(n), ck, ctx->side, &e.d, &e.l1));
     TRY_CUDA(batch_status_to_host(e.d, ctx->h_side_total, ctx->side));
     return BIELCC_OK;
 }
@@ -1110,7 +1110,9 @@ int field_batch_locked(bielcc_ctx ctx, int n_jobs, const bielcc_field_job* jobs,
     TRY(check_jobs(ctx, n_jobs, jobs, meshes));
     if (report) memset(report, 0, sizeof(*report));
     TRY(ws_acquire(ctx, s));
-    if (n.p_max > 1 || n.n_start > kBatchMaxNStart) {  // outside the batched kernel: one call per job
+    // p_max >= 3 (the convergence-test marks) and far splits beyond the batched
+    // kernel's staging run outside it: one call per job
+    if (far_adaptive(n) || far_split_n(n) > kBatchMaxNStart) {
         for (int i = 0; i < n_jobs; i++) {
             const bielcc_field_job& j = jobs[i];
             FieldArgs a{meshes[i], j.n_rhs, j.J_dev, mk(j.k_re, j.k_im), mk(j.mult_re, j.mult_im), &j.inc, n,
@@ -1136,12 +1138,13 @@ int field_batch_locked(bielcc_ctx ctx, int n_jobs, const bielcc_field_job* jobs,
     if (precision == BIELCC_PREC_MIXED && want_est && n_jobs > 0)
         TRY(batch_est_begin(ctx, jd, jobs, n, ck, item_cost, s, es));
     BatchPlan bp;
-    plan_batch(bp, jd, n.n_start, precision == BIELCC_PREC_MIXED, item_cost, ctx->batch_tc, ctx_batch_split_cap(ctx));
+    plan_batch(bp, jd, far_split_n(n), precision == BIELCC_PREC_MIXED, item_cost, ctx->batch_tc,
+               ctx_batch_split_cap(ctx));
     TRY(ctx->ws.ensure(bp.ws_bytes));
     TRY(ctx->scratch_small.ensure(256));
     BatchDevPtrs d;
     int l1 = 0, l2 = 0;
-    TRY_CUDA(batch_stage1(bp, ctx->ws.p, n.analytic_calc, n.n_start, ck, s, &d, &l1));
+    TRY_CUDA(batch_stage1(bp, ctx->ws.p, n.analytic_calc, far_split_n(n), ck, s, &d, &l1));
     TRY_CUDA(batch_status_to_host(d, ctx->h_total, s));
     TRY_CUDA(cudaStreamSynchronize(s));
     if (batch_timed_out(ctx->h_total)) return set_error(BIELCC_ERR_TIMEOUT, "batched far kernel: a bounded wait ran out");
@@ -1228,8 +1231,10 @@ int bielcc_batch_plan_create(bielcc_ctx ctx, int n_jobs, const bielcc_field_job*
         return set_error(BIELCC_ERR_ARG, "unknown precision %d", precision);
     NumParamH n = to_np(np);
     TRY(check_np(n));
-    if (n.p_max > 1 || n.n_start > kBatchMaxNStart)
-        return set_error(BIELCC_ERR_UNSUPPORTED, "batch plans run the batched kernel: p_max = 1, n_start <= 22");
+    if (far_adaptive(n) || far_split_n(n) > kBatchMaxNStart)
+        return set_error(BIELCC_ERR_UNSUPPORTED,
+                         "batch plans run the batched kernel: p_max <= 2 and a far split (n_start, 2 n_start "
+                         "for p_max = 2) of at most 22");
     std::lock_guard<std::mutex> g(ctx->mu);
     cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
     std::vector<MeshDev*> meshes;
@@ -1250,11 +1255,11 @@ int bielcc_batch_plan_create(bielcc_ctx ctx, int n_jobs, const bielcc_field_job*
         // replay would evaluate every moment again, so it runs the fused kernel
         // (unless every batch is set to split).
         const bool mixed = precision == BIELCC_PREC_MIXED;
-        plan_batch(p->bp, jd, n.n_start, mixed, ctx->batch_item_cost, ctx->batch_tc, ctx->batch_split);
+        plan_batch(p->bp, jd, far_split_n(n), mixed, ctx->batch_item_cost, ctx->batch_tc, ctx->batch_split);
         if (p->bp.split && p->bp.waves.size() > 1 && !ctx->batch_split_all)
-            plan_batch(p->bp, jd, n.n_start, mixed, ctx->batch_item_cost, ctx->batch_tc, 0);
+            plan_batch(p->bp, jd, far_split_n(n), mixed, ctx->batch_item_cost, ctx->batch_tc, 0);
         e = cudaMalloc(&p->ws, p->bp.ws_bytes);
-        if (e == cudaSuccess) e = batch_stage1(p->bp, p->ws, n.analytic_calc, n.n_start, ck, s, &p->d, &l1);
+        if (e == cudaSuccess) e = batch_stage1(p->bp, p->ws, n.analytic_calc, far_split_n(n), ck, s, &p->d, &l1);
         if (e == cudaSuccess) e = batch_status_to_host(p->d, ctx->h_total, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e == cudaSuccess && batch_timed_out(ctx->h_total))
@@ -1273,7 +1278,7 @@ int bielcc_batch_plan_create(bielcc_ctx ctx, int n_jobs, const bielcc_field_job*
     if (rc == BIELCC_OK && e == cudaSuccess) {
         e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
-            cudaError_t e1 = batch_replay(p->bp, p->d, p->n_near, p->pair_ws, n.analytic_calc, n.n_start, cs);
+            cudaError_t e1 = batch_replay(p->bp, p->d, p->n_near, p->pair_ws, n.analytic_calc, far_split_n(n), cs);
             cudaError_t e2 = cudaStreamEndCapture(cs, &p->graph);
             e = e1 != cudaSuccess ? e1 : e2;
         }

@@ -393,7 +393,7 @@ cudaError_t start_field_batch(bielcc_server_s* sv, Slot& sl) {
         d.nonfinite = (unsigned long long*)(dev + sl.nan_off) + i;
     }
     auto t3 = Clock::now();
-    plan_batch(sl.bp, jd, sv->np.n_start, sv->precision == BIELCC_PREC_MIXED, sv->item_cost,
+    plan_batch(sl.bp, jd, far_split_n(sv->np), sv->precision == BIELCC_PREC_MIXED, sv->item_cost,
                ctx_batch_tensor_cores(sv->ctx), std::min<size_t>(ctx_batch_split_cap(sv->ctx), kServeMomCap));
     if (sv->preemptible) batch_make_preemptible(sl.bp);
 
@@ -402,7 +402,7 @@ cudaError_t start_field_batch(bielcc_server_s* sv, Slot& sl) {
     if (e != cudaSuccess) return e;
     auto t5 = Clock::now();
     int launches = 0;
-    e = batch_stage1(sl.bp, sl.ws.p, sv->np.analytic_calc, sv->np.n_start, false, sl.s, &sl.d, &launches);
+    e = batch_stage1(sl.bp, sl.ws.p, sv->np.analytic_calc, far_split_n(sv->np), false, sl.s, &sl.d, &launches);
     if (e == cudaSuccess) e = batch_status_to_host(sl.d, sl.h_total, sl.s);
     if (e == cudaSuccess && sl.samp_on) {  // the error sample: gather, FP64 stage 1 (status in h_total[4], [7])
         char* sb = dev + sl.samp_off;
@@ -442,12 +442,12 @@ cudaError_t start_field_batch(bielcc_server_s* sv, Slot& sl) {
         e = cudaMemcpyAsync(sl.samp_ej, ej.data(), n * sizeof(ErrJob), cudaMemcpyHostToDevice, sl.s);
         if (e == cudaSuccess) e = err_gather(sl.samp_ej, (int)n, spts, sl.s);
         if (e == cudaSuccess) {
-            plan_batch(sl.samp_bp, js, sv->np.n_start, false, sv->item_cost, false);
+            plan_batch(sl.samp_bp, js, far_split_n(sv->np), false, sv->item_cost, false);
             e = sl.samp_ws.ensure(sl.samp_bp.ws_bytes, sl.s);
         }
         int l = 0;
         if (e == cudaSuccess)
-            e = batch_stage1(sl.samp_bp, sl.samp_ws.p, sv->np.analytic_calc, sv->np.n_start, false, sl.s, &sl.samp_d,
+            e = batch_stage1(sl.samp_bp, sl.samp_ws.p, sv->np.analytic_calc, far_split_n(sv->np), false, sl.s, &sl.samp_d,
                              &l);
         if (e == cudaSuccess) e = batch_status_to_host(sl.samp_d, sl.h_total + 4, sl.s);
     }
@@ -777,9 +777,11 @@ int bielcc_server_create(bielcc_ctx ctx, int64_t hbm_budget, int n_slots, const 
     NumParamH n{1e-6, 2.0, 2.0, 3.0, 8, 10, 1, 1};
     if (np) n = NumParamH{np->eps, np->rs, np->rs_seg, np->analytic_calc, np->n_start, np->n_start_seg, np->p_max,
                           np->p_max_seg};
-    if (n.p_max != 1 || n.n_start < 1 || n.n_start > kBatchMaxNStart || n.n_start_seg < 1 || n.p_max_seg < 1 ||
-        n.p_max_seg > 20)
-        return set_api_error(BIELCC_ERR_UNSUPPORTED, "the server runs the batched kernel: p_max = 1, 1 <= n_start <= 22");
+    if (n.p_max < 1 || far_adaptive(n) || n.n_start < 1 || far_split_n(n) > kBatchMaxNStart || n.n_start_seg < 1 ||
+        n.p_max_seg < 1 || n.p_max_seg > 20)
+        return set_api_error(BIELCC_ERR_UNSUPPORTED,
+                             "the server runs the batched kernel: p_max <= 2, far split (n_start, 2 n_start for "
+                             "p_max = 2) of at most 22");
     bielcc_server_s* sv = new (std::nothrow) bielcc_server_s;
     if (!sv) return set_api_error(BIELCC_ERR_OOM, "out of host memory");
     sv->ctx = ctx;
@@ -947,7 +949,7 @@ int bielcc_server_submit_field(bielcc_server sv, const bielcc_field_request* req
     if (!r) return set_api_error(BIELCC_ERR_OOM, "out of host memory");
     r->type = kField;
     r->f = *req;
-    int rc = server_mesh(sv->ctx, req->mesh, sv->np.n_start, &r->mesh);
+    int rc = server_mesh(sv->ctx, req->mesh, far_split_n(sv->np), &r->mesh);
     if (rc != BIELCC_OK) {
         delete r;
         return rc;
@@ -959,10 +961,10 @@ int bielcc_server_submit_field(bielcc_server sv, const bielcc_field_request* req
         item_cost = sv->item_cost;
     }
     // served batches split only when the context sets every batch to split
-    const int64_t mom_cap = sv->precision == BIELCC_PREC_MIXED && sv->np.n_start <= 8
+    const int64_t mom_cap = sv->precision == BIELCC_PREC_MIXED && far_split_n(sv->np) <= 8
                                 ? (int64_t)std::min<size_t>(ctx_batch_split_cap(sv->ctx), kServeMomCap)
                                 : 0;
-    r->bytes = field_bytes(*r, sv->np.n_start, item_cost, mom_cap);
+    r->bytes = field_bytes(*r, far_split_n(sv->np), item_cost, mom_cap);
     r->pairs = (int64_t)req->n_pts * r->mesh->n_cells * req->n_rhs;
     return submit(sv, r, ticket);
 }
@@ -976,7 +978,7 @@ int bielcc_server_submit_assemble(bielcc_server sv, const bielcc_assemble_reques
     if (!r) return set_api_error(BIELCC_ERR_OOM, "out of host memory");
     r->type = kAssemble;
     r->a = *req;
-    int rc = server_mesh(sv->ctx, req->mesh, sv->np.n_start, &r->mesh);
+    int rc = server_mesh(sv->ctx, req->mesh, far_split_n(sv->np), &r->mesh);
     if (rc != BIELCC_OK) {
         delete r;
         return rc;

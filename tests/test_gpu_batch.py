@@ -70,11 +70,14 @@ def test_batch_job_alone_equals_in_mix(gctx):
 def test_batch_fallback_adaptive_and_autotune(gctx):
     torch = pytest.importorskip("torch")
     specs = _jobs(gctx, seed=5)[:2]
-    npm = abi.NumParam.default(n_start=4, n_start_seg=5, p_max=2, p_max_seg=2)
-    outs, _ = _batch(torch, gctx, specs, "fp64", numparam=npm)
-    for sp, (E, H) in zip(specs, outs):
-        Eo, Ho = oracle.field_EH(sp["cells"], sp["J"], sp["k"], sp["pts"], npm, mult=sp["mult"])
-        assert rel_l2(E, Eo) < TOL_FP64 and rel_l2(H, Ho) < TOL_FP64
+    # p_max = 2 runs the batched kernel's far pass at 2 n_start; p_max = 3 one call per job
+    for pm in (2, 3):
+        npm = abi.NumParam.default(n_start=4, n_start_seg=5, p_max=pm, p_max_seg=2)
+        for precision, tol in (("fp64", TOL_FP64), ("mixed", TOL_MIXED)):
+            outs, _ = _batch(torch, gctx, specs, precision, numparam=npm)
+            for sp, (E, H) in zip(specs, outs):
+                Eo, Ho = oracle.field_EH(sp["cells"], sp["J"], sp["k"], sp["pts"], npm, mult=sp["mult"])
+                assert rel_l2(E, Eo) < tol and rel_l2(H, Ho) < tol
     dev = torch.device("cuda:0")
     keep = []
     s2 = []

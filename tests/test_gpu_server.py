@@ -52,6 +52,28 @@ def test_server_results_match_oracle(gctx, precision, tol):
         sv.close()
 
 
+@pytest.mark.parametrize("precision,tol", [("fp64", TOL_FP64), ("mixed", TOL_MIXED)])
+def test_server_adaptive_p_max2(gctx, precision, tol):
+    """A server with p_max = 2: served batches run the batched kernel's far pass
+    at 2 n_start (the pass the reference's loop returns) and the full schedule
+    for near pairs; results against the oracle's loop. p_max = 3 needs the
+    convergence-test marks, which the batched kernel does not read: refused."""
+    specs = _specs(gctx, 5)[:3]
+    npm = abi.NumParam.default(n_start=4, n_start_seg=5, p_max=2, p_max_seg=2)
+    sv = gpu.Server(gctx, n_slots=2, numparam=npm, precision=precision)
+    try:
+        tickets = [_submit(sv, sp, out_c64=False) for sp in specs]
+        for sp, t in zip(specs, tickets):
+            st, _, out = sv.wait(t)
+            assert st == 0
+            Eo, Ho = oracle.field_EH(sp["cells"], sp["J"], sp["k"], sp["pts"], npm, mult=sp["mult"])
+            assert rel_l2(out["E"], Eo) < tol and rel_l2(out["H"], Ho) < tol
+    finally:
+        sv.close()
+    with pytest.raises(gpu.BielccError):
+        gpu.Server(gctx, n_slots=1, numparam=abi.NumParam.default(p_max=3), precision=precision)
+
+
 def test_server_request_alone_equals_in_mix(gctx):
     specs = _specs(gctx, 2)
     sv = gpu.Server(gctx, n_slots=3, precision="mixed")
