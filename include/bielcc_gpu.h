@@ -370,7 +370,8 @@ int bielcc_batch_autotune(bielcc_ctx ctx, int n_jobs, const bielcc_field_job* jo
  * persistent far kernel, finalize) is captured once in a CUDA graph, which
  * bielcc_batch_plan_launch replays on a stream: no host planning, no host
  * round trip, 3 graph nodes. Results are identical to bielcc_field_EH_batch
- * with the same J. p_max must be 1 and n_start <= 22. The plan owns its
+ * with the same J. p_max must be 1 or 2 and the far pass's split (n_start,
+ * or 2 n_start when p_max = 2) at most 22. The plan owns its
  * device memory; the jobs' buffers must outlive it. No counterpart in the
  * reference. */
 typedef struct bielcc_batch_plan_s* bielcc_batch_plan;
@@ -597,7 +598,8 @@ typedef struct bielcc_server_stats {
 } bielcc_server_stats;
 
 /* hbm_budget <= 0 selects 150 GiB. np: NULL for the defaults; the server runs
- * the batched kernel, so np->p_max must be 1 and np->n_start <= 22. The
+ * the batched kernel, so np->p_max must be 1 or 2 and the far pass's split
+ * (np->n_start, or 2 np->n_start when p_max = 2) at most 22. The
  * server maps a quarter of its budget (at most half the free device memory)
  * into its memory pool at creation. */
 int bielcc_server_create(bielcc_ctx ctx, int64_t hbm_budget, int n_slots, const bielcc_numparam* np,
