@@ -954,7 +954,7 @@ def run_ours(args, ws, rank, local):
     # DRAM bytes per far-kernel launch: a constant read from the ncu capture
     # summarised in profiles/ (ncu does not run inside the bench)
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "far_kernel_mixed_sphere8192.md")
+    tpath = os.path.join(ROOT, "profiles", "far_kernel_traffic_sphere8192.md")
     if os.path.exists(tpath):
         import re
 
@@ -1006,8 +1006,8 @@ def run_ours(args, ws, rank, local):
         "roofline": {"bound": "fp32 CUDA-core pipe (no tensor-core or HBM bound: compute-only kernel)",
                      "kernel": "far_kernel<1,false,true>", "achieved": achieved, "peak": peak32, "unit": "TFLOP/s",
                      "frac": achieved / peak32 if peak32 else None, "traffic": traffic,
-                     "traffic_source": "ncu capture of the same launch summarised in "
-                                       "profiles/far_kernel_mixed_sphere8192.md (a constant from that capture, "
+                     "traffic_source": "one-pass ncu capture of the same full-size launch summarised in "
+                                       "profiles/far_kernel_traffic_sphere8192.md (a constant from that capture, "
                                        "not measured in this run)",
                      "algorithmic_flops_per_launch": far_flops, "far_ms_per_launch": far_ms,
                      "peak_source": "measured FMA loop (bielcc_measure_fma_peak); MEASURED_PEAKS.json has no FP32 "
