@@ -74,6 +74,18 @@ constexpr int kSP = BIELCC_BATCH_SP;  // right-hand sides staged per pass (a mul
 #ifndef BIELCC_BATCH_U2
 #define BIELCC_BATCH_U2 1
 #endif
+// FP64 form: unrolling of the node loop and resident CTAs per SM asked of the
+// kernel. Measured on 64 meshes of the batched workload (unroll / CTAs per SM):
+// 1 / 3 (168 registers, no spills) 284 ms; 2 / 3 284 ms; 4 / 3 322-327 ms;
+// 1 / 2 (206 registers) 338 ms; 8 / 2 388 ms; 8 / 3 436 ms; 16 / 3 491 ms.
+// Unrolling costs instruction-cache misses (CTAs of different jobs share an
+// SM); a third CTA hides the FP64 latency better.
+#ifndef BIELCC_BATCH64_UNROLL
+#define BIELCC_BATCH64_UNROLL 1
+#endif
+#ifndef BIELCC_BATCH64_MINB
+#define BIELCC_BATCH64_MINB 3
+#endif
 #define BIELCC_PRAGMA_STR(x) #x
 #define BIELCC_UNROLL(n) _Pragma(BIELCC_PRAGMA_STR(unroll n))
 
@@ -283,11 +295,13 @@ BIELCC_D void batch_moments(const typename BatchCfg<MIXED>::NodeT* nd, const flo
             sincos(k.re * d, &sn, &cs);
             P0r = cs;
             P0i = sn;
+            BIELCC_UNROLL(BIELCC_BATCH64_UNROLL)
             for (int i = 0; i < nn; i++) {
                 const double4 v = nd[i];
                 far_node_f64<CK, true>(m, x[0] - v.x, x[1] - v.y, x[2] - v.z, v.w, k, k2r, k2i, d);
             }
         } else {
+            BIELCC_UNROLL(BIELCC_BATCH64_UNROLL)
             for (int i = 0; i < nn; i++) {
                 const double4 v = nd[i];
                 far_node_f64<CK, false>(m, x[0] - v.x, x[1] - v.y, x[2] - v.z, v.w, k, k2r, k2i, d);
@@ -454,7 +468,7 @@ BIELCC_D void batch_stage_j(typename BatchCfg<MIXED>::F* s_j, const JobDev& jb, 
 }
 
 template <bool MIXED>
-__global__ void __launch_bounds__(kBT, MIXED ? BIELCC_BATCH_MINB : 2) batch_far_kernel(const JobDev* __restrict__ jobs,
+__global__ void __launch_bounds__(kBT, MIXED ? BIELCC_BATCH_MINB : BIELCC_BATCH64_MINB) batch_far_kernel(const JobDev* __restrict__ jobs,
                                                          const BatchItem* __restrict__ items, int n_items,
                                                          int* __restrict__ counter, double analytic_calc, int n_start,
                                                          int max_items) {
