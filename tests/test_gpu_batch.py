@@ -96,7 +96,7 @@ SPLIT_DEFAULT = 16 << 30
 
 
 @pytest.mark.parametrize("mode", ["split, one wave", "split, many waves", "fused", "tensor cores",
-                                  "split, tensor cores"])
+                                  "split, tensor cores", "fused, p_max 2"])
 def test_batch_plan_graph_replay_with_new_currents(gctx, mode):
     """A planned batch replayed from its CUDA graph after the currents changed
     in place gives the same result as a fresh batched call with those
@@ -109,14 +109,15 @@ def test_batch_plan_graph_replay_with_new_currents(gctx, mode):
     cap, every = {"split, one wave": (SPLIT_DEFAULT, False), "split, many waves": (100_000, True),
                   "split, tensor cores": (SPLIT_DEFAULT, True)}.get(mode, (0, False))
     gctx.set_batch_split(cap, all_batches=every)
+    npm = abi.NumParam.default(n_start=4, n_start_seg=5, p_max=2, p_max_seg=2) if "p_max 2" in mode else None
     try:
-        _plan_replay(torch, gctx)
+        _plan_replay(torch, gctx, npm)
     finally:
         gctx.set_batch_tensor_cores(False)
         gctx.set_batch_split(SPLIT_DEFAULT)
 
 
-def _plan_replay(torch, gctx):
+def _plan_replay(torch, gctx, npm=None):
     dev = torch.device("cuda:0")
     specs = _jobs(gctx, seed=7)
     tens, jspecs = [], []
@@ -131,10 +132,10 @@ def _plan_replay(torch, gctx):
                            H=Hd.data_ptr(), k=sp["k"], mult=sp["mult"]))
     jobs = gctx.make_jobs(jspecs)
     sc = torch.cuda.current_stream().cuda_stream
-    plan = gctx.batch_plan(jobs, precision="mixed", stream=sc)
+    plan = gctx.batch_plan(jobs, numparam=npm, precision="mixed", stream=sc)
     torch.cuda.synchronize()
     first = [(E.clone(), H.clone()) for _, _, E, H in tens]
-    fresh, _ = _batch(torch, gctx, specs, "mixed")
+    fresh, _ = _batch(torch, gctx, specs, "mixed", numparam=npm)
     for (E, H), (Ef, Hf) in zip(first, fresh):
         assert np.array_equal(E.cpu().numpy(), Ef) and np.array_equal(H.cpu().numpy(), Hf)
     # new currents in place, then replay the graph (twice: replays are repeatable)
@@ -144,11 +145,11 @@ def _plan_replay(torch, gctx):
     for _ in range(2):
         plan.launch(stream=sc)
     torch.cuda.synchronize()
-    fresh, _ = _batch(torch, gctx, specs, "mixed")
+    fresh, _ = _batch(torch, gctx, specs, "mixed", numparam=npm)
     for sp, (_, _, E, H), (Ef, Hf) in zip(specs, tens, fresh):
         E, H = E.cpu().numpy(), H.cpu().numpy()
         assert np.array_equal(E, Ef) and np.array_equal(H, Hf)
-        Eo, Ho = oracle.field_EH(sp["cells"], sp["J"], sp["k"], sp["pts"], mult=sp["mult"])
+        Eo, Ho = oracle.field_EH(sp["cells"], sp["J"], sp["k"], sp["pts"], npm, mult=sp["mult"])
         assert rel_l2(E, Eo) < TOL_MIXED and rel_l2(H, Ho) < TOL_MIXED
     assert plan.report.n_near_pairs > 0
     plan.close()
