@@ -147,6 +147,17 @@ int run() {
     bielcc_gpu::GetFieldE_Ideal(mesh, jE, mult, einc, bielcc::PlaneWaveFieldE<double>, np, pts, Eg);
     report("GetFieldE_Ideal (128 quads, " + std::to_string(pts.size()) + " pts)",
            rel(&Eg[0][0], &Er[0][0], 3 * pts.size()));
+    // adaptive refinement: p_max = 2 (the far pass at 2 n_start) and 3 (the
+    // per-integral convergence test and the third pass)
+    {
+        bielcc::NumParam np2(1e-6, 2, 2, 3, 8, 10, 2, 2);
+        for (const bielcc::NumParam* npa : {&np2, &np3}) {
+            std::vector<std::array<cd, 3>> Ra(pts.size()), Ga(pts.size());
+            bielcc::GetFieldE_Ideal(mesh, jE, mult, einc, bielcc::PlaneWaveFieldE<double>, *npa, pts, Ra);
+            bielcc_gpu::GetFieldE_Ideal(mesh, jE, mult, einc, bielcc::PlaneWaveFieldE<double>, *npa, pts, Ga);
+            report("GetFieldE_Ideal, p_max " + std::to_string(npa->p_max), rel(&Ga[0][0], &Ra[0][0], 3 * pts.size()));
+        }
+    }
     // more currents than cells: the extra ones are ignored, as in the reference loop
     std::vector<std::array<cd, 3>> jLong = jE;
     jLong.push_back({cd(1e3, 0), cd(1e3, 0), cd(1e3, 0)});
