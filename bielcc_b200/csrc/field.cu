@@ -384,6 +384,14 @@ __global__ void BIELCC_FAR_BOUNDS(NRHS, CK, MIXED) far_kernel(FarArgsOf<MARKS> a
 // with take_marked = 1 on those tables), else the whole loop in
 // far_refine_sum_kernel.
 
+// Unrolling of the decision kernel's node loops (the node rows come from
+// global memory: unrolled, their loads issue ahead of the arithmetic).
+// 2000 x 8192 at p_max = 3, mixed / FP64: x1 ~92 / 131 ms, x4 88.3 / 129.3 ms,
+// x8 88.4 / 127.9 ms.
+#ifndef BIELCC_DECIDE_UNROLL
+#define BIELCC_DECIDE_UNROLL 8
+#endif
+
 // One pass of the FP64 far node loop over a cell's node table row (far_kernel's
 // FP64 arithmetic: the phase split below |k| rho = 0.5, else sincos per node).
 template <bool CK>
@@ -392,7 +400,7 @@ BIELCC_D void far_pass_f64(Moments<double>& m, const double4* __restrict__ nd, i
     m.zero();
     if (split) {
 #define BIELCC_PASS64(TD_)                                                                              \
-    for (int i = 0; i < nn; i++) {                                                                      \
+    BIELCC_FAR_PRAGMA(BIELCC_DECIDE_UNROLL) for (int i = 0; i < nn; i++) {                              \
         const double4 v = nd[i];                                                                \
         far_node_f64<CK, true, TD_>(m, x[0] - v.x, x[1] - v.y, x[2] - v.z, v.w, k, k2r, k2i, r0);       \
     }
@@ -403,7 +411,7 @@ BIELCC_D void far_pass_f64(Moments<double>& m, const double4* __restrict__ nd, i
         }
 #undef BIELCC_PASS64
     } else {
-        for (int i = 0; i < nn; i++) {
+        BIELCC_FAR_PRAGMA(BIELCC_DECIDE_UNROLL) for (int i = 0; i < nn; i++) {
             const double4 v = nd[i];
             far_node_f64<CK, false>(m, x[0] - v.x, x[1] - v.y, x[2] - v.z, v.w, k, k2r, k2i, r0);
         }
