@@ -442,11 +442,19 @@ BIELCC_D double far_delta2(const cplx* a, const cplx* b) {
 }
 
 // markK must be zero on entry (set bits only); markG is written in full.
+// STAGED: the CTA stages each cell's two node rows in shared memory
+// ((nn_lo + nn) double4, dynamic) before its threads use them; otherwise every
+// thread reads them from global memory (rows too long to stage).
+template <bool STAGED>
 __global__ void far_refine_decide_kernel(FarArgs a, const double4* __restrict__ lo, int nn_lo, double eps2,
                                          unsigned* __restrict__ markG, unsigned* __restrict__ markK) {
+    extern __shared__ double4 s_rows[];  // STAGED: [nn_lo] then [nn] of the current cell
     const int p = blockIdx.x * kFarThreads + threadIdx.x;
-    if (p >= a.n_pts) return;
-    const double x[3] = {a.pts[3 * (size_t)p], a.pts[3 * (size_t)p + 1], a.pts[3 * (size_t)p + 2]};
+    const bool live = p < a.n_pts;
+    if (!STAGED && !live) return;
+    double x[3] = {0., 0., 0.};
+    if (live)
+        for (int g = 0; g < 3; g++) x[g] = a.pts[3 * (size_t)p + g];
     const int cb = blockIdx.y * a.cells_per_split;
     const int ce = min(a.n_cells, cb + a.cells_per_split);
     const bool ck = a.k.im != 0.0;
@@ -454,6 +462,17 @@ __global__ void far_refine_decide_kernel(FarArgs a, const double4* __restrict__ 
     const int nw = (a.n_cells + 31) >> 5;
     unsigned nbits = 0, gbits = 0;
     for (int c = cb; c < ce; c++) {
+        const double4* row_lo = lo + (size_t)c * nn_lo;
+        const double4* row_hi = a.nodes64 + (size_t)c * a.nn;
+        if constexpr (STAGED) {
+            __syncthreads();  // the previous cell's rows are no longer read
+            for (int i = threadIdx.x; i < nn_lo; i += kFarThreads) s_rows[i] = row_lo[i];
+            for (int i = threadIdx.x; i < a.nn; i += kFarThreads) s_rows[nn_lo + i] = row_hi[i];
+            __syncthreads();
+            row_lo = s_rows;
+            row_hi = s_rows + nn_lo;
+            if (!live) continue;  // after the barriers: every thread stages
+        }
         const CellGeo& gg = a.geo[c];
         double d;
         const bool nr = is_near(x, gg.c, gg.diam, a.analytic_calc, &d);
@@ -466,11 +485,11 @@ __global__ void far_refine_decide_kernel(FarArgs a, const double4* __restrict__ 
             if (split) sincos(a.k.re * d, &pi, &pr);
             Moments<double> m0, m1;
             if (ck) {
-                far_pass_f64<true>(m0, lo + (size_t)c * nn_lo, nn_lo, x, a.k, k2r, k2i, d, false, 0);
-                far_pass_f64<true>(m1, a.nodes64 + (size_t)c * a.nn, a.nn, x, a.k, k2r, k2i, d, false, 0);
+                far_pass_f64<true>(m0, row_lo, nn_lo, x, a.k, k2r, k2i, d, false, 0);
+                far_pass_f64<true>(m1, row_hi, a.nn, x, a.k, k2r, k2i, d, false, 0);
             } else {
-                far_pass_f64<false>(m0, lo + (size_t)c * nn_lo, nn_lo, x, a.k, k2r, k2i, d, split, td);
-                far_pass_f64<false>(m1, a.nodes64 + (size_t)c * a.nn, a.nn, x, a.k, k2r, k2i, d, split, td);
+                far_pass_f64<false>(m0, row_lo, nn_lo, x, a.k, k2r, k2i, d, split, td);
+                far_pass_f64<false>(m1, row_hi, a.nn, x, a.k, k2r, k2i, d, split, td);
             }
             if (!(d < kMachineZero)) {  // R_Rot_Colloc integrates grad F away from the centre only
                 cplx g0[3], g1[3];
@@ -914,8 +933,14 @@ cudaError_t field_stage1(const FieldLaunch& f, void* ws, int splits, long long* 
         // the convergence test of every far pair's integrals; the failing ones are marked
         cudaError_t e = cudaMemsetAsync(markK, 0, (size_t)f.n_rhs * n_words * P * sizeof(unsigned), s);
         if (e != cudaSuccess) return e;
-        far_refine_decide_kernel<<<dim3(tiles, splits), kFarThreads, 0, s>>>(
-            a, m.nodes64_lo, f.np.n_start * f.np.n_start, f.np.eps * f.np.eps, markG, markK);
+        const int nn_lo = f.np.n_start * f.np.n_start;
+        const size_t rows = (size_t)(nn_lo + a.nn) * sizeof(double4);
+        if (rows <= 48 * 1024)
+            far_refine_decide_kernel<true><<<dim3(tiles, splits), kFarThreads, rows, s>>>(
+                a, m.nodes64_lo, nn_lo, f.np.eps * f.np.eps, markG, markK);
+        else
+            far_refine_decide_kernel<false><<<dim3(tiles, splits), kFarThreads, 0, s>>>(
+                a, m.nodes64_lo, nn_lo, f.np.eps * f.np.eps, markG, markK);
         nl++;
     }
     FarArgsMarks am;
