@@ -400,11 +400,13 @@ BIELCC_D void asm_pass_f64(Moments<double>& m, const double4* __restrict__ nd, i
                            double k2r, double k2i, double r0, bool split) {
     m.zero();
     if (split) {
+#pragma unroll 8
         for (int q = 0; q < nn; q++) {
             const double4 v = nd[q];
             far_node_f64<CK, true>(m, x[0] - v.x, x[1] - v.y, x[2] - v.z, v.w, k, k2r, k2i, r0);
         }
     } else {
+#pragma unroll 8
         for (int q = 0; q < nn; q++) {
             const double4 v = nd[q];
             far_node_f64<CK, false>(m, x[0] - v.x, x[1] - v.y, x[2] - v.z, v.w, k, k2r, k2i, r0);
@@ -434,11 +436,17 @@ BIELCC_D double asm_delta2(const Moments<double>& m0, const Moments<double>& m1,
     return d;
 }
 
+// STAGED: the CTA stages each column cell's two node rows in shared memory
+// ((nn_lo + nn) double4, dynamic); otherwise every thread reads them from
+// global memory (rows too long to stage).
+template <bool STAGED>
 __global__ void asm_refine_decide_kernel(AsmArgs a, const double4* __restrict__ lo, int nn_lo, double eps2,
                                          unsigned* __restrict__ mark) {
+    extern __shared__ double4 s_rows[];
     const int i = blockIdx.x * kAsmThreads + threadIdx.x;
-    if (i >= a.n_cells) return;
-    const CellGeo gi = a.geo[i];
+    const bool live = i < a.n_cells;
+    if (!STAGED && !live) return;
+    const CellGeo gi = a.geo[live ? i : 0];
     const double* x = gi.c;
     const int cb = blockIdx.y * a.cols_per_split;
     const int ce = min(a.n_cells, cb + a.cols_per_split);
@@ -447,6 +455,17 @@ __global__ void asm_refine_decide_kernel(AsmArgs a, const double4* __restrict__ 
     const size_t plane = (size_t)((a.n_cells + 31) >> 5) * a.n_cells;
     unsigned nbits = 0, mb[3] = {0u, 0u, 0u};
     for (int j = cb; j < ce; j++) {
+        const double4* row_lo = lo + (size_t)j * nn_lo;
+        const double4* row_hi = a.nodes64 + (size_t)j * a.nn;
+        if constexpr (STAGED) {
+            __syncthreads();  // the previous column's rows are no longer read
+            for (int q = threadIdx.x; q < nn_lo; q += kAsmThreads) s_rows[q] = row_lo[q];
+            for (int q = threadIdx.x; q < a.nn; q += kAsmThreads) s_rows[nn_lo + q] = row_hi[q];
+            __syncthreads();
+            row_lo = s_rows;
+            row_hi = s_rows + nn_lo;
+            if (!live) continue;  // after the barriers: every thread stages
+        }
         const CellGeo& gj = a.geo[j];
         double d;
         const bool nr = asm_is_near(x, gj, a.analytic_calc, &d);
@@ -456,11 +475,11 @@ __global__ void asm_refine_decide_kernel(AsmArgs a, const double4* __restrict__ 
             if (split) sincos(a.k.re * d, &pi, &pr);
             Moments<double> m0, m1;
             if (ck) {
-                asm_pass_f64<true>(m0, lo + (size_t)j * nn_lo, nn_lo, x, a.k, k2r, k2i, d, false);
-                asm_pass_f64<true>(m1, a.nodes64 + (size_t)j * a.nn, a.nn, x, a.k, k2r, k2i, d, false);
+                asm_pass_f64<true>(m0, row_lo, nn_lo, x, a.k, k2r, k2i, d, false);
+                asm_pass_f64<true>(m1, row_hi, a.nn, x, a.k, k2r, k2i, d, false);
             } else {
-                asm_pass_f64<false>(m0, lo + (size_t)j * nn_lo, nn_lo, x, a.k, k2r, k2i, d, split);
-                asm_pass_f64<false>(m1, a.nodes64 + (size_t)j * a.nn, a.nn, x, a.k, k2r, k2i, d, split);
+                asm_pass_f64<false>(m0, row_lo, nn_lo, x, a.k, k2r, k2i, d, split);
+                asm_pass_f64<false>(m1, row_hi, a.nn, x, a.k, k2r, k2i, d, split);
             }
             for (int b = 0; b < a.m; b++) {
                 double J[3];
@@ -787,8 +806,14 @@ cudaError_t assemble_stage1(const AssembleLaunch& a, void* ws, long long* d_tota
     dim3 grid(tiles, splits);
     if (far_adaptive(a.np)) {
         unsigned* mark = (unsigned*)((char*)mask + al256((size_t)n_words * N * sizeof(unsigned)) + 256);
-        asm_refine_decide_kernel<<<grid, kAsmThreads, 0, s>>>(g, m.nodes64_lo, a.np.n_start * a.np.n_start,
-                                                              a.np.eps * a.np.eps, mark);
+        const int nn_lo = a.np.n_start * a.np.n_start;
+        const size_t rows = (size_t)(nn_lo + g.nn) * sizeof(double4);
+        if (rows <= 48 * 1024)
+            asm_refine_decide_kernel<true><<<grid, kAsmThreads, rows, s>>>(g, m.nodes64_lo, nn_lo, a.np.eps * a.np.eps,
+                                                                           mark);
+        else
+            asm_refine_decide_kernel<false><<<grid, kAsmThreads, 0, s>>>(g, m.nodes64_lo, nn_lo, a.np.eps * a.np.eps,
+                                                                         mark);
         AsmArgsMarks gm;
         static_cast<AsmArgs&>(gm) = g;
         gm.mask = nullptr;  // written by the decision kernel
