@@ -56,18 +56,26 @@ def test_server_results_match_oracle(gctx, precision, tol):
 def test_server_adaptive_p_max2(gctx, precision, tol):
     """A server with p_max = 2: served batches run the batched kernel's far pass
     at 2 n_start (the pass the reference's loop returns) and the full schedule
-    for near pairs; results against the oracle's loop. p_max = 3 needs the
+    for near pairs; results against the oracle's loop. A served assembly request
+    equals the direct call with the same parameters. p_max = 3 needs the
     convergence-test marks, which the batched kernel does not read: refused."""
     specs = _specs(gctx, 5)[:3]
     npm = abi.NumParam.default(n_start=4, n_start_seg=5, p_max=2, p_max_seg=2)
     sv = gpu.Server(gctx, n_slots=2, numparam=npm, precision=precision)
     try:
         tickets = [_submit(sv, sp, out_c64=False) for sp in specs]
+        c64 = precision == "mixed"
+        ta = sv.submit_assemble(specs[1]["mesh"], 4.0, layout="tau2", out_c64=c64)
         for sp, t in zip(specs, tickets):
             st, _, out = sv.wait(t)
             assert st == 0
             Eo, Ho = oracle.field_EH(sp["cells"], sp["J"], sp["k"], sp["pts"], npm, mult=sp["mult"])
             assert rel_l2(out["E"], Eo) < tol and rel_l2(out["H"], Ho) < tol
+        st, _, out = sv.wait(ta)
+        assert st == 0
+        A_direct, _ = gctx.assemble_K(specs[1]["mesh"], 4.0, numparam=npm, layout=abi.LAYOUT_TAU2, c64=c64,
+                                      precision=precision)
+        assert np.array_equal(out["A"], A_direct)
     finally:
         sv.close()
     with pytest.raises(gpu.BielccError):
