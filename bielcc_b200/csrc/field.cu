@@ -378,10 +378,11 @@ __global__ void BIELCC_FAR_BOUNDS(NRHS, CK, MIXED) far_kernel(FarArgsOf<MARKS> a
 // of F_RotRotSimplePot_H . J for every right-hand side (K.h:288-301) and
 // R_Rot_Colloc's integral of grad F (R.h:89-111; none at the cell centre).
 // Each integral is tested on its own, as the reference runs one loop per
-// integral: an integral that passes takes the pass at 2 n_start (far_kernel
-// with take_marked = 0); one that fails is marked (markG per pair, markK per
-// pair and RHS) and takes the pass at 4 n_start when p_max = 3 (far_kernel
-// with take_marked = 1 on those tables), else the whole loop in
+// integral: an integral that passes returns the pass at 2 n_start, which the
+// decision kernel has just run for the test and adds to the split sums itself
+// (in FP64, in the mixed form too); one that fails is marked (markG per pair,
+// markK per pair and RHS) and takes the pass at 4 n_start when p_max = 3
+// (far_kernel with take_marked = 1 on those tables), else the whole loop in
 // far_refine_sum_kernel.
 
 // Unrolling of the decision kernel's node loops (the node rows come from
@@ -441,7 +442,8 @@ BIELCC_D double far_delta2(const cplx* a, const cplx* b) {
     return d;
 }
 
-// markK must be zero on entry (set bits only); markG is written in full.
+// markK and this split's slot of a.partial must be zero on entry (set bits
+// only; the passing integrals are added); markG is written in full.
 // STAGED: the CTA stages each cell's two node rows in shared memory
 // ((nn_lo + nn) double4, dynamic) before its threads use them; otherwise every
 // thread reads them from global memory (rows too long to stage).
@@ -460,6 +462,7 @@ __global__ void far_refine_decide_kernel(FarArgs a, const double4* __restrict__ 
     const bool ck = a.k.im != 0.0;
     const double k2r = a.k.re * a.k.re - a.k.im * a.k.im, k2i = 2.0 * a.k.re * a.k.im;
     const int nw = (a.n_cells + 31) >> 5;
+    const size_t P = a.n_pts;
     unsigned nbits = 0, gbits = 0;
     for (int c = cb; c < ce; c++) {
         const double4* row_lo = lo + (size_t)c * nn_lo;
@@ -491,8 +494,10 @@ __global__ void far_refine_decide_kernel(FarArgs a, const double4* __restrict__ 
                 far_pass_f64<false>(m0, row_lo, nn_lo, x, a.k, k2r, k2i, d, split, td);
                 far_pass_f64<false>(m1, row_hi, a.nn, x, a.k, k2r, k2i, d, split, td);
             }
-            if (!(d < kMachineZero)) {  // R_Rot_Colloc integrates grad F away from the centre only
-                cplx g0[3], g1[3];
+            const bool zeroR = d < kMachineZero;  // R_Rot_Colloc integrates grad F away from the centre only
+            cplx g1[3];
+            if (!zeroR) {
+                cplx g0[3];
                 for (int q = 0; q < 3; q++) {
                     g0[q] = mk(m0.g[q][0], m0.g[q][1]) * mk(pr, pi);
                     g1[q] = mk(m1.g[q][0], m1.g[q][1]) * mk(pr, pi);
@@ -505,8 +510,23 @@ __global__ void far_refine_decide_kernel(FarArgs a, const double4* __restrict__ 
                 cplx k0[3], k1[3];
                 far_raw_K(m0, pr, pi, jj, k0);
                 far_raw_K(m1, pr, pi, jj, k1);
-                if (!(far_delta2(k1, k0) < eps2))
-                    atomicOr(markK + ((size_t)s * nw + (c >> 5)) * a.n_pts + p, 1u << (c & 31));
+                const bool kfail = !(far_delta2(k1, k0) < eps2);
+                if (kfail) atomicOr(markK + ((size_t)s * nw + (c >> 5)) * a.n_pts + p, 1u << (c & 31));
+                // the integrals that passed return the pass at 2 n_start: added
+                // here, in cell order, to this split's raw sums (the thread owns them)
+                double* dst = a.partial + ((size_t)blockIdx.y * a.n_rhs + s) * 12 * P + p;
+                if (!kfail)
+                    for (int q = 0; q < 3; q++) {
+                        dst[(size_t)(2 * q) * P] += k1[q].re;
+                        dst[(size_t)(2 * q + 1) * P] += k1[q].im;
+                    }
+                if (!zeroR && !gfail)
+                    for (int q = 0; q < 3; q++) {  // (G x J)_q = G_b J_c - G_c J_b
+                        const int b = (q + 1) % 3, cc = (q + 2) % 3;
+                        const cplx h = g1[b] * jj[cc] - g1[cc] * jj[b];
+                        dst[(size_t)(6 + 2 * q) * P] += h.re;
+                        dst[(size_t)(6 + 2 * q + 1) * P] += h.im;
+                    }
             }
         }
         nbits |= (nr ? 1u : 0u) << (c & 31);
@@ -930,8 +950,10 @@ cudaError_t field_stage1(const FieldLaunch& f, void* ws, int splits, long long* 
         return cudaErrorInvalidValue;  // no 4 n_start tables for the third pass
     if (far_begin) cudaEventRecord(far_begin, s);
     if (tiles > 0 && far_adaptive(f.np)) {
-        // the convergence test of every far pair's integrals; the failing ones are marked
+        // the convergence test of every far pair's integrals; the failing ones
+        // are marked, the passing ones added to the split sums (slots [0, splits))
         cudaError_t e = cudaMemsetAsync(markK, 0, (size_t)f.n_rhs * n_words * P * sizeof(unsigned), s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(partial, 0, (size_t)splits * f.n_rhs * 12 * P * sizeof(double), s);
         if (e != cudaSuccess) return e;
         const int nn_lo = f.np.n_start * f.np.n_start;
         const size_t rows = (size_t)(nn_lo + a.nn) * sizeof(double4);
@@ -947,11 +969,7 @@ cudaError_t field_stage1(const FieldLaunch& f, void* ws, int splits, long long* 
     static_cast<FarArgs&>(am) = a;
     am.markG = markG;
     am.markK = markK;
-    am.take_marked = 0;
-    if (tiles > 0 && markG) {  // the integrals that passed: the pass at 2 n_start
-        if (mixed) nl += ck ? launch_far_marks<true, true>(am, tiles, splits, s) : launch_far_marks<false, true>(am, tiles, splits, s);
-        else nl += ck ? launch_far_marks<true, false>(am, tiles, splits, s) : launch_far_marks<false, false>(am, tiles, splits, s);
-    } else if (tiles > 0) {
+    if (tiles > 0 && !markG) {
         if (mixed) nl += ck ? launch_far_rhs<true, true>(a, tiles, splits, s) : launch_far_rhs<false, true>(a, tiles, splits, s);
         else nl += ck ? launch_far_rhs<true, false>(a, tiles, splits, s) : launch_far_rhs<false, false>(a, tiles, splits, s);
     }
