@@ -97,8 +97,9 @@ struct FarArgs {
 };
 // p_max >= 3, the far kernel's marks-reading variant: the integrals that failed
 // the convergence test at the second pass, grad F per pair [ceil(N/32)][P] and
-// F . J per RHS [S][ceil(N/32)][P]; take_marked 0 adds the integrals that
-// passed, 1 the ones that failed. (A separate type: the plain variants keep
+// F . J per RHS [S][ceil(N/32)][P]; take_marked 1 adds the integrals that
+// failed (the third pass, at 4 n_start), 0 the ones that passed (which the
+// decision kernel adds itself on the field path). (A separate type: the plain variants keep
 // FarArgs' parameter block, whose size the FP64 kernel's register allocation
 // follows.)
 struct FarArgsMarks : FarArgs {
