@@ -542,12 +542,15 @@ __global__ void far_refine_decide_kernel(FarArgs a, const double4* __restrict__ 
 
 // p_max > 3: the integrals that failed the test, through the whole loop
 // (integral_cell, ops.cuh: the reference's passes, test and budget), one warp
-// per (point, RHS): F . J where markK is set, grad F where markG is set. In
-// round r lane l takes the point's marked cell of rank 32 r + l (cell order;
-// each lane walks the mask words with its own cursor), so the lanes run their
-// loops side by side; lane sums are in cell order and combined by a fixed xor
-// butterfly. Writes the raw E, H sums (before 1/4pi) of every point, zero
-// without marked cells, into the partial-sum slot `out` [S][12][P].
+// per (point, RHS, range of mask words): F . J where markK is set, grad F where
+// markG is set. In round r lane l takes the range's marked cell of rank
+// 32 r + l (cell order; each lane walks the mask words with its own cursor), so
+// the lanes run their loops side by side; lane sums are in cell order and
+// combined by a fixed xor butterfly. The marked cells gather on the few
+// near-field points, so gridDim.z ranges per point give the GPU that many more
+// warps. Writes the raw E, H sums (before 1/4pi) of every point and range,
+// zero without marked cells, into partial-sum slot blockIdx.z of `out`
+// [gridDim.z][S][12][P].
 __global__ void far_refine_sum_kernel(FarArgs a, const unsigned* __restrict__ markG, const unsigned* __restrict__ markK,
                                       const double* __restrict__ verts, int nv, DNP np, double* __restrict__ out) {
     const int p = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
@@ -555,21 +558,25 @@ __global__ void far_refine_sum_kernel(FarArgs a, const unsigned* __restrict__ ma
     if (p >= a.n_pts) return;  // whole warps
     const size_t P = a.n_pts;
     const int n_words = (a.n_cells + 31) / 32;
+    // this warp's range of mask words (blockIdx.z of gridDim.z parts) and output slot
+    const int wpp = (n_words + gridDim.z - 1) / gridDim.z;
+    const int w_end = min(n_words, (int)(blockIdx.z + 1) * wpp);
+    out += (size_t)blockIdx.z * a.n_rhs * 12 * P;
     const unsigned* mK = markK + (size_t)s * n_words * P;
     const double x[3] = {a.pts[3 * (size_t)p], a.pts[3 * (size_t)p + 1], a.pts[3 * (size_t)p + 2]};
     double v[12];
 #pragma unroll
     for (int q = 0; q < 12; q++) v[q] = 0.;
-    int w = 0;
-    unsigned bits = n_words > 0 ? (markG[p] | mK[p]) : 0u;
-    long long base = 0;  // rank of the first flagged cell of word w
+    int w = blockIdx.z * wpp;
+    unsigned bits = w < w_end ? (markG[(size_t)w * P + p] | mK[(size_t)w * P + p]) : 0u;
+    long long base = 0;  // rank (within the range) of the first flagged cell of word w
     for (long long t = lane;; t += 32) {
-        while (w < n_words && base + __popc(bits) <= t) {
+        while (w < w_end && base + __popc(bits) <= t) {
             base += __popc(bits);
             w++;
-            bits = w < n_words ? (markG[(size_t)w * P + p] | mK[(size_t)w * P + p]) : 0u;
+            bits = w < w_end ? (markG[(size_t)w * P + p] | mK[(size_t)w * P + p]) : 0u;
         }
-        const bool have = w < n_words;
+        const bool have = w < w_end;
         if (!__any_sync(0xffffffffu, have)) break;
         if (!have) continue;
         unsigned b = bits;
@@ -829,11 +836,16 @@ __global__ void finalize_kernel(FinalArgs a) {
 // ---------------------------------------------------------------- host launchers
 static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 static size_t mask_words(int n_cells) { return (size_t)(n_cells + 31) / 32; }
+// Mask-word ranges per point of far_refine_sum_kernel (p_max > 3).
+static int refine_parts(const FieldLaunch& f) {
+    return (int)std::min<size_t>(8, std::max<size_t>(1, mask_words(f.mesh->n_cells)));
+}
 // Partial-sum slots [slot][S][12][P]: one per cell split; with p_max = 3 as
 // many again for the third pass of the pairs that fail the convergence test;
-// with p_max > 3 one more for the pairs that take the whole refinement loop.
+// with p_max > 3 one per mask-word range of the pairs that take the whole
+// refinement loop.
 static int partial_slots(const FieldLaunch& f, int splits) {
-    return splits + (far_third_pass(f.np) ? splits : (far_adaptive(f.np) ? 1 : 0));
+    return splits + (far_third_pass(f.np) ? splits : (far_adaptive(f.np) ? refine_parts(f) : 0));
 }
 // Resident CTAs (whole GPU) of the far-kernel variant a launch starts with:
 // NRHS 4 / 2 / 1 (the first RHS chunk), real / complex k, FP64 / mixed.
@@ -1001,7 +1013,7 @@ cudaError_t field_stage1(const FieldLaunch& f, void* ws, int splits, long long* 
     } else if (tiles > 0 && f.n_rhs > 0 && far_adaptive(f.np)) {
         DNP np{f.np.eps, f.np.rs, f.np.rs_seg, f.np.analytic_calc, f.np.n_start, f.np.n_start_seg, f.np.p_max,
                f.np.p_max_seg};
-        far_refine_sum_kernel<<<dim3((f.n_pts + 7) / 8, f.n_rhs), 256, 0, s>>>(
+        far_refine_sum_kernel<<<dim3((f.n_pts + 7) / 8, f.n_rhs, refine_parts(f)), 256, 0, s>>>(
             a, markG, markK, m.verts, m.nv, np, partial + (size_t)splits * f.n_rhs * 12 * P);
         nl++;
     }

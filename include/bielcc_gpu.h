@@ -302,9 +302,9 @@ int bielcc_field_EH_full_device(bielcc_ctx ctx, bielcc_mesh mesh, int n_rhs,
  *   per point: 96 n_rhs per cell split + 96 n_rhs (near sums) + 16
  *              + 4 ceil(n_cells / 32)        (near-cell mask: 1 KiB per point
  *                                             at 8192 cells)
- *              + 4 ceil(n_cells / 32) (1 + n_rhs) and one more cell split
- *                                            (p_max >= 3: test marks; p_max = 3
- *                                             doubles the cell splits)
+ *              + 4 ceil(n_cells / 32) (1 + n_rhs) (p_max >= 3: test marks)
+ *              and the cell splits again (p_max = 3), or
+ *              min(8, ceil(n_cells / 32)) more (p_max > 3)
  *   per near pair: 216
  * The far partial sums take at most half of what is left after the cells and
  * a one-split workspace; the cell-split count is capped to fit. Every call
